@@ -1,0 +1,371 @@
+"""Benchmark: placements/s of the per-placement field solve on the 1M-tet 10-tissue sphere head.
+
+Workload: 8-shell sphere of radius 90 mm with an eye and a muscle cap, Kuhn
+lattice at 2.63 mm (1.0M tetrahedra, 0.18M nodes; a 1.5 mm lattice reaches 1M tetrahedra only at
+a 51 mm radius, so the lattice is coarsened to keep a head-sized sphere), +-0.2 mm seeded node jitter;
+figure-8 coil of 2 x 2048 dipoles; 8 placements on a 15-degree grid of the upper hemisphere solved as
+one block (block_k = 8) to relative residual 1e-8. A step is one block of 8 placements: coil
+placement, dA/dt, right-hand side, block PCG, E reconstruction and gray-matter summary.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|plain]
+
+Prints one JSON line (rank 0). ``value`` is device-timed with CUDA events on the library's stream,
+inputs resident in HBM, L2 flushed between steps; ``e2e`` goes through the host C ABI call
+(cunibs_solve_block) with host buffers, timed by the wall clock around the synchronous call.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from cunibs_b200.synthetic import EIGHT_SHELLS, EYE_CAP, MUSCLE_CAP, figure8_coil, sphere_head  # noqa: E402
+
+METRIC = "placements/s @1M tets, rel.res 1e-8: learned+mixed vs plain FP64 PCG, same B200"
+TOL = 1e-8
+K_BLOCK = 8
+
+
+def workload():
+    mesh = sphere_head(2.63, 90.0, EIGHT_SHELLS, (EYE_CAP, MUSCLE_CAP), jitter_mm=0.2, seed=0)
+    coil = figure8_coil(2048)
+    sites = []
+    for th, ph in [(0, 0), (15, 0), (15, 90), (15, 180), (15, 270), (30, 45), (30, 135), (30, 225)]:
+        t, f = np.radians(th), np.radians(ph)
+        c = 90.0 * np.array([np.sin(t) * np.cos(f), np.sin(t) * np.sin(f), np.cos(t)])
+        sites.append((c, c + 50.0 * np.array([-np.sin(f), np.cos(f), 0.0])))
+    return mesh, coil, sites
+
+
+def config_dict(mesh, extra=None):
+    d = {"workload": "1M-tet 10-tissue sphere head (configs[1])", "n_tets": int(mesh.n_tets),
+         "n_nodes": int(mesh.n_nodes), "lattice_mm": 2.63, "radius_mm": 90.0, "dipoles": 4096, "block_k": K_BLOCK,
+         "placements_per_step": K_BLOCK, "tolerance": TOL}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int) -> None:
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+        self.t = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[2:6]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float]:
+    """Algorithmic bytes of one PCG iteration and of one FP64 refinement step at block width K.
+
+    Unique bytes each kernel must move, no reuse credit. v_b/v_x: value/vector bytes, 4 in the
+    mixed inner iteration, 8 in the plain one. On level l with n rows, nnz entries, a prolongator of
+    pnnz entries and nc coarse rows:
+      SpMV      nnz*(v_b+4) + 4*(n+1) + 2*v_x*K*n      (values, columns, row pointers, x and y)
+      Chebyshev SpMV + 4*n + 4*v_x*K*n                  (+ dinv; x_cur, x_prev, b, out)
+      residual  SpMV + 3*v_x*K*n
+      restrict  pnnz*(v_b+4) + 4*(nc+1) + v_x*K*(n+nc) (+ the fused first coarse step: dinv, x)
+      prolong   pnnz*(v_b+4) + 4*(n+1) + v_x*K*(nc+2n) (x_f read and written)
+      coarse    v_b*nc^2 + 2*v_x*K*nc
+    and the PCG body's BLAS-1 passes count each (n, K) vector read or written once.
+    """
+    vb = vx = 4 if precision == "mixed" else 8
+    sizes = ctx.levels()
+    L = ctx.n_levels
+    deg = 2
+    total = 0.0
+    for lev in range(L):
+        n, nc = sizes[lev], sizes[lev + 1]
+        nnz = ctx.array("a_col", lev).shape[0]
+        pnnz = ctx.array("p_col", lev).shape[0]
+        spmv = nnz * (vb + 4) + 4 * (n + 1) + 2 * vx * K * n
+        cheb = spmv + 4 * n + 4 * vx * K * n
+        if lev == 0:
+            total += 4 * n + 2 * vx * K * n  # zero-guess first step x = a0*dinv*b
+        total += (deg - 1) * cheb + spmv + 3 * vx * K * n
+        total += pnnz * (vb + 4) + 4 * (nc + 1) + vx * K * (n + nc)
+        if lev + 1 < L:
+            total += 4 * nc + vx * K * nc
+        total += pnnz * (vb + 4) + 4 * (n + 1) + vx * K * (nc + 2 * n)
+        total += deg * cheb
+    nc = ctx.coarse_rows
+    total += vb * nc * nc + 2 * vx * K * nc
+    n0 = sizes[0]
+    nnz0 = ctx.array("a_col", 0).shape[0] if L > 0 else 0
+    total += nnz0 * (vb + 4) + 4 * (n0 + 1) + 2 * vx * K * n0  # Ap = A p (+ p.Ap)
+    total += 6 * vx * K * n0  # x += a p, r -= a Ap (+ ||r||)
+    total += 2 * vx * K * n0  # r.z
+    total += 3 * vx * K * n0  # p = z + b p
+    outer = nnz0 * 12 + 4 * (n0 + 1) + (8 + 8 + 4) * K * n0 + 20 * K * n0  # B - A X in FP64; X += d
+    return float(total), float(outer)
+
+
+def run_ours(args) -> dict:
+    import torch
+
+    from cunibs_b200 import _native
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist_mod.init_process_group("nccl", timeout=timedelta(seconds=300))
+        dist = dist_mod
+
+    mesh, coil, sites = workload()
+    p = _native.default_params()
+    p.device = local
+    p.tolerance = TOL
+    p.precision = _native.PREC_MIXED if args.precision == "mixed" else _native.PREC_PLAIN_FP64
+    t0 = time.perf_counter()
+    ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
+    setup_s = time.perf_counter() - t0
+    ctx.set_timing(True)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+
+    centers = np.stack([c for c, _ in sites])
+    handles = np.stack([h for _, h in sites])
+    dists = np.full(K_BLOCK, 4.0)
+    dev = torch.device("cuda", local)
+    d_pos = torch.tensor(coil.positions_m, dtype=torch.float64, device=dev)
+    d_mom = torch.tensor(coil.moments, dtype=torch.float64, device=dev)
+    d_c = torch.tensor(centers, dtype=torch.float64, device=dev)
+    d_h = torch.tensor(handles, dtype=torch.float64, device=dev)
+    d_d = torch.tensor(dists, dtype=torch.float64, device=dev)
+    d_T = torch.empty((K_BLOCK, 16), dtype=torch.float64, device=dev)
+    d_S = torch.empty((K_BLOCK, 16), dtype=torch.float64, device=dev)
+    outs = {"transforms": d_T.data_ptr(), "summary": d_S.data_ptr()}
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        return ctx.solve_block_device(d_pos.data_ptr(), d_mom.data_ptr(), coil.n_dipoles, d_c.data_ptr(),
+                                      d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, outs)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    launches0 = _native.kernel_launches()
+    stage_sum = np.zeros(5)
+    iters = []
+    outers = []
+    step_ms = []
+    with ClockSampler(local) as clocks:
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                ev0 = torch.cuda.Event(enable_timing=True)
+                ev1 = torch.cuda.Event(enable_timing=True)
+                ev0.record(stream)
+            it, outer = step()
+            with torch.cuda.stream(stream):
+                ev1.record(stream)
+            ev1.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+            stage_sum += ctx.stage_times()
+            iters.append(it)
+            outers.append(outer)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+    launches = _native.kernel_launches() - launches0
+    total_ms = float(sum(step_ms))
+    if dist is not None:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    value = world * args.steps * K_BLOCK / (total_ms / 1e3)
+
+    # End to end through the host C ABI (host buffers in and out).
+    e2e_ms = []
+    for _ in range(max(1, min(args.steps, 5))):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        res = ctx.solve_block(coil, centers, handles, dists, 1e6)
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    e2e_value = world * K_BLOCK / (statistics.median(e2e_ms) / 1e3)
+    h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
+    d2h = res["transform"].nbytes + res["summary"].nbytes + res["iterations"].nbytes + res["relative_residual"].nbytes
+
+    # Roofline of the SpMV-dominated iteration (solve stage).
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    per_it, per_outer = solve_bytes_per_iteration(ctx, K_BLOCK, args.precision)
+    mean_iters = float(np.mean(iters))
+    mean_outer = float(np.mean(outers))
+    solve_ms = stage_sum[3] / args.steps
+    solve_bytes = per_it * mean_iters + per_outer * mean_outer
+    achieved = solve_bytes / (solve_ms / 1e3) / 1e9
+    traffic = None
+    tp = ROOT / "profiles" / "solve_traffic.json"
+    if tp.exists():
+        traffic = json.loads(tp.read_text()).get("bytes_per_solve")
+    n_nodes = mesh.n_nodes
+    dadt_ms = stage_sum[1] / args.steps
+    pair_evals = n_nodes * coil.n_dipoles * K_BLOCK
+    line = {
+        "metric": METRIC,
+        "value": round(value, 3),
+        "unit": "placements/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(total_ms / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 (FP32 PCG/V-cycle/dA-dt) with f64 refinement" if args.precision == "mixed" else "f64",
+        "data": "synthetic: seeded sphere head and figure-8 coil",
+        "config": config_dict(mesh, {"precision": args.precision, "l2": "flushed (256 MB write) between steps",
+                                     "parallelism": f"replicas x{world}"}),
+        "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "block PCG solve stage (SpMV-dominated iteration)",
+                     "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
+                     "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
+                     "bytes_per_iteration": per_it, "iterations": mean_iters, "outer_steps": mean_outer,
+                     "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
+        "stages_ms": {k: round(v / args.steps, 4) for k, v in
+                      zip(["place", "dadt", "rhs", "solve", "post"], stage_sum)},
+        "dadt": {"pair_evals_per_step": int(pair_evals), "ms": round(dadt_ms, 4),
+                 "gpair_per_s": round(pair_evals / (dadt_ms / 1e3) / 1e9, 2)},
+        "setup_s": round(setup_s, 3),
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(mesh, coil, sites)
+    if dist is not None:
+        dist.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def cpu_baseline(mesh, coil, sites, n_place=1) -> dict:
+    """The FP64 CPU restatement (oracle/) on this host's cores: one placement of the same workload."""
+    from oracle import Oracle
+
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    orc = Oracle(mesh)
+    setup = time.perf_counter() - t0
+    c = np.stack([s[0] for s in sites[:n_place]])
+    h = np.stack([s[1] for s in sites[:n_place]])
+    t1 = time.perf_counter()
+    orc.solve(coil, c, h, np.full(n_place, 4.0), 1e6, tolerance=TOL)
+    dt = time.perf_counter() - t1
+    return {"value": round(n_place / dt, 4), "unit": "placements/s", "cores": threads, "kind": "port",
+            "sample": f"{n_place} placement(s) of the same workload, FP64 AMG-PCG to 1e-8 (setup {setup:.1f} s excluded)"}
+
+
+def run_reference(args) -> dict | None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    mesh, coil, sites = workload()
+    from oracle import Oracle
+
+    threads = os.cpu_count() or 1
+    orc = Oracle(mesh)
+    c = np.stack([s[0] for s in sites])
+    h = np.stack([s[1] for s in sites])
+    for i in range(args.warmup):
+        j = i % len(sites)
+        orc.solve(coil, c[j:j + 1], h[j:j + 1], [4.0], 1e6, tolerance=TOL)
+    times = []
+    for i in range(args.steps):
+        j = i % len(sites)
+        t1 = time.perf_counter()
+        orc.solve(coil, c[j:j + 1], h[j:j + 1], [4.0], 1e6, tolerance=TOL)
+        times.append(time.perf_counter() - t1)
+    value = len(times) / sum(times)
+    return {
+        "metric": METRIC, "value": round(value, 4), "unit": "placements/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
+        "data": "synthetic: seeded sphere head and figure-8 coil", "config": config_dict(mesh),
+        "cpu_baseline": {"value": round(value, 4), "unit": "placements/s", "cores": threads, "kind": "port",
+                         "sample": "one placement per step (the workload's 8 sites in turn), FP64 AMG-PCG to 1e-8"},
+        "e2e": {"value": round(value, 4), "unit": "placements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    line = run_reference(args) if args.impl == "reference" else run_ours(args)
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,354 @@
+"""ctypes binding of the C ABI in include/cunibs_b200.h (libcunibs_b200.so).
+
+The library is built in-tree (cunibs_b200/_lib). There is no fallback: if it is missing or cannot
+be loaded, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcunibs_b200.so"
+_lib: C.CDLL | None = None
+
+OK, EINVAL, ENOMEM, ECUDA, ENOCONV, ETIMEOUT, EINTERNAL = range(7)
+PREC_DEFAULT, PREC_PLAIN_FP64, PREC_MIXED = 0, 1, 2
+SUMMARY_LEN = 16
+
+_vp = C.c_void_p
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("device", C.c_int),
+        ("min_coarse_rows", C.c_int),
+        ("max_levels", C.c_int),
+        ("agg_rounds", C.c_int),
+        ("cheby_degree", C.c_int),
+        ("cheby_lower_ratio", C.c_double),
+        ("tolerance", C.c_double),
+        ("max_iters", C.c_int),
+        ("precision", C.c_int),
+        ("inner_reduction", C.c_double),
+        ("inner_max_iters", C.c_int),
+        ("iters_per_sync", C.c_int),
+    ]
+
+
+class Info(C.Structure):
+    _fields_ = [
+        ("n_nodes", C.c_int),
+        ("n_tets", C.c_int),
+        ("n_skin", C.c_int),
+        ("n_gray_matter", C.c_int),
+        ("stiffness_nnz", C.c_longlong),
+        ("ground_node", C.c_int),
+        ("n_levels", C.c_int),
+        ("coarse_rows", C.c_int),
+    ]
+
+
+class SolveOpts(C.Structure):
+    _fields_ = [
+        ("block_width", C.c_int),
+        ("precision", C.c_int),
+        ("tolerance", C.c_double),
+        ("max_iters", C.c_int),
+    ]
+
+
+class BlockOut(C.Structure):
+    _fields_ = [
+        ("transforms", _vp),
+        ("summary", _vp),
+        ("iterations", _vp),
+        ("relres", _vp),
+        ("magnE", _vp),
+        ("E", _vp),
+        ("v", _vp),
+        ("total_iterations", C.c_int),
+        ("outer_steps", C.c_int),
+    ]
+
+
+class NativeError(RuntimeError):
+    """A failure reported by the native library (status code in ``.code``)."""
+
+    def __init__(self, code: int, message: str) -> None:
+        super().__init__(message)
+        self.code = code
+
+
+class ConvergenceFailure(NativeError):
+    pass
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def load() -> C.CDLL:
+    """Load the native library; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise ImportError(
+            f"{_LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+            "or `make -C cunibs_b200/csrc`"
+        )
+    lib = C.CDLL(str(_LIB_PATH))
+    ip = C.POINTER(C.c_int)
+    dp = C.POINTER(C.c_double)
+    fp = C.POINTER(C.c_float)
+    sig = {
+        "cunibs_version": ([], C.c_int),
+        "cunibs_last_error": ([], C.c_char_p),
+        "cunibs_params_default": ([C.POINTER(Params)], C.c_int),
+        "cunibs_context_create": ([dp, C.c_int, ip, ip, C.c_int, ip, C.c_int, C.POINTER(Params), C.POINTER(_vp)], C.c_int),
+        "cunibs_context_destroy": ([_vp], C.c_int),
+        "cunibs_context_info": ([_vp, C.POINTER(Info)], C.c_int),
+        "cunibs_context_mesh": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "cunibs_context_levels": ([_vp, ip, C.c_int], C.c_int),
+        "cunibs_solve_block": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), C.POINTER(BlockOut)], C.c_int),
+        "cunibs_solve_block_device": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), C.POINTER(BlockOut)], C.c_int),
+        "cunibs_context_set_conductivity": ([_vp, dp], C.c_int),
+        "cunibs_context_array": ([_vp, C.c_char_p, C.c_int, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
+        "cunibs_context_place": ([_vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
+        "cunibs_context_dadt": ([_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp], C.c_int),
+        "cunibs_context_solve": ([_vp, _vp, _vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, _vp, _vp, _vp], C.c_int),
+        "cunibs_context_vcycle": ([_vp, _vp, _vp, C.c_int, C.c_int], C.c_int),
+        "cunibs_select_size4": ([C.c_int, ip, ip, fp, ip, ip], C.c_int),
+        "cunibs_context_summary": ([_vp, _vp, C.c_int, _vp], C.c_int),
+        "cunibs_context_set_timing": ([_vp, C.c_int], C.c_int),
+        "cunibs_context_stage_times": ([_vp, dp, C.c_int], C.c_int),
+        "cunibs_context_stream": ([_vp, C.POINTER(_vp)], C.c_int),
+        "cunibs_kernel_launches": ([], C.c_longlong),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc == OK:
+        return
+    msg = load().cunibs_last_error().decode(errors="replace")
+    if rc == EINVAL:
+        raise ValueError(msg)
+    if rc == ENOCONV:
+        raise ConvergenceFailure(rc, msg)
+    if rc == ENOMEM:
+        raise MemoryError(msg)
+    raise NativeError(rc, msg)
+
+
+def _p(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(_vp)
+
+
+def _ip(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def default_params() -> Params:
+    p = Params()
+    check(load().cunibs_params_default(C.byref(p)))
+    return p
+
+
+# Names of the int32 arrays cunibs_context_array serves; the rest are float64.
+_INT_ARRAYS = {
+    "node_perm", "tet_perm", "tet_nodes", "tet_tags", "skin_tris", "n2c_ptr", "n2c_idx", "stiff_ptr",
+    "stiff_col", "gm_index", "a_ptr", "a_col", "agg", "p_ptr", "p_col", "coarse_ptr", "coarse_col",
+}
+
+
+class Context:
+    """One subject's device state: a handle from cunibs_context_create."""
+
+    def __init__(self, nodes_mm, tet_nodes, tet_tags, skin_tris, params: Params | None = None) -> None:
+        lib = load()
+        nodes = np.ascontiguousarray(nodes_mm, dtype=np.float64).reshape(-1, 3)
+        tets = np.ascontiguousarray(tet_nodes, dtype=np.int32).reshape(-1, 4)
+        tags = np.ascontiguousarray(tet_tags, dtype=np.int32).reshape(-1)
+        skin = np.ascontiguousarray(skin_tris, dtype=np.int32).reshape(-1, 3)
+        if skin.size == 0:
+            skin = np.zeros((1, 3), np.int32)[:0]
+        h = _vp()
+        prm = params if params is not None else default_params()
+        check(lib.cunibs_context_create(
+            nodes.ctypes.data_as(C.POINTER(C.c_double)), nodes.shape[0], _ip(tets), _ip(tags), tets.shape[0],
+            _ip(skin) if skin.shape[0] else None, skin.shape[0], C.byref(prm), C.byref(h)))
+        self._h = h
+        self._lib = lib
+        self.params = prm
+        info = Info()
+        check(lib.cunibs_context_info(h, C.byref(info)))
+        self.n_nodes = info.n_nodes
+        self.n_tets = info.n_tets
+        self.n_skin = info.n_skin
+        self.n_gray_matter = info.n_gray_matter
+        self.stiffness_nnz = info.stiffness_nnz
+        self.ground_node = info.ground_node
+        self.n_levels = info.n_levels
+        self.coarse_rows = info.coarse_rows
+
+    def close(self) -> None:
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.cunibs_context_destroy(h)
+            self._h = _vp()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter teardown
+            pass
+
+    @property
+    def handle(self):
+        if not self._h.value:
+            raise ValueError("the context has been freed")
+        return self._h
+
+    def mesh(self):
+        nodes = np.empty((self.n_nodes, 3))
+        tets = np.empty((self.n_tets, 4), np.int32)
+        tags = np.empty(self.n_tets, np.int32)
+        skin = np.empty((max(self.n_skin, 1), 3), np.int32)
+        node_perm = np.empty(self.n_nodes, np.int32)
+        tet_perm = np.empty(self.n_tets, np.int32)
+        check(self._lib.cunibs_context_mesh(self.handle, _p(nodes), _p(tets), _p(tags), _p(skin), _p(node_perm), _p(tet_perm)))
+        return nodes, tets, tags, skin[: self.n_skin], node_perm, tet_perm
+
+    def levels(self) -> list[int]:
+        out = np.empty(64, np.int32)
+        check(self._lib.cunibs_context_levels(self.handle, _ip(out), 64))
+        return out[: self.n_levels + 1].tolist()
+
+    def array(self, name: str, level: int = -1) -> np.ndarray:
+        n = C.c_longlong()
+        check(self._lib.cunibs_context_array(self.handle, name.encode(), level, None, 0, C.byref(n)))
+        dt = np.int32 if name in _INT_ARRAYS else np.float64
+        out = np.empty(n.value, dt)
+        check(self._lib.cunibs_context_array(self.handle, name.encode(), level, _p(out), n.value, C.byref(n)))
+        return out
+
+    def place(self, centers, handles, dists):
+        centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
+        k = centers.shape[0]
+        handles_a = None if handles is None else np.ascontiguousarray(handles, np.float64).reshape(-1, 3)
+        dists = np.ascontiguousarray(dists, np.float64).reshape(-1)
+        T = np.empty((k, 4, 4))
+        deg = np.empty(k, np.int32)
+        check(self._lib.cunibs_context_place(self.handle, _p(centers), _p(handles_a), _p(dists), k, _p(T), _p(deg)))
+        return T, deg
+
+    def dadt(self, coil, transforms, didt) -> np.ndarray:
+        T = np.ascontiguousarray(transforms, np.float64).reshape(-1, 16)
+        k = T.shape[0]
+        pos = np.ascontiguousarray(coil.positions_m, np.float64)
+        mom = np.ascontiguousarray(coil.moments, np.float64)
+        out = np.empty((k, self.n_nodes, 3), np.float32)
+        check(self._lib.cunibs_context_dadt(self.handle, _p(pos), _p(mom), pos.shape[0], _p(T), k, float(didt), _p(out)))
+        return out
+
+    def solve(self, B, k, width, precision=PREC_DEFAULT, tolerance=0.0, max_iters=0, x0=None):
+        B = np.ascontiguousarray(B, np.float64)
+        X = np.empty_like(B)
+        it = np.empty(k, np.int32)
+        rel = np.empty(k)
+        x0a = None if x0 is None else np.ascontiguousarray(x0, np.float64)
+        check(self._lib.cunibs_context_solve(self.handle, _p(B), _p(X), k, width, precision, float(tolerance),
+                                             int(max_iters), _p(x0a), _p(it), _p(rel)))
+        return X, it, rel
+
+    def vcycle(self, r, fp32=False) -> np.ndarray:
+        r = np.ascontiguousarray(r, np.float64)
+        k = 1 if r.ndim == 1 else r.shape[1]
+        z = np.empty_like(r)
+        check(self._lib.cunibs_context_vcycle(self.handle, _p(r), _p(z), k, int(bool(fp32))))
+        return z
+
+    def summary(self, magnE) -> np.ndarray:
+        m = np.ascontiguousarray(magnE, np.float32).reshape(-1, self.n_tets)
+        out = np.empty((m.shape[0], SUMMARY_LEN))
+        check(self._lib.cunibs_context_summary(self.handle, _p(m), m.shape[0], _p(out)))
+        return out
+
+    def set_timing(self, on: bool = True) -> None:
+        check(self._lib.cunibs_context_set_timing(self.handle, int(bool(on))))
+
+    def stage_times(self) -> np.ndarray:
+        ms = np.empty(5)
+        check(self._lib.cunibs_context_stage_times(self.handle, ms.ctypes.data_as(C.POINTER(C.c_double)), 5))
+        return ms
+
+    def stream(self) -> int:
+        out = _vp()
+        check(self._lib.cunibs_context_stream(self.handle, C.byref(out)))
+        return int(out.value or 0)
+
+    def solve_block_device(self, pos, mom, n_dip, centers, handles, dists, k, didt, out_ptrs, *, block_width=0,
+                           precision=PREC_DEFAULT, tolerance=0.0, max_iters=0) -> tuple[int, int]:
+        """cunibs_solve_block_device on raw device pointers (ints); out_ptrs maps output names to pointers."""
+        out = BlockOut(out_ptrs.get("transforms"), out_ptrs.get("summary"), out_ptrs.get("iterations"),
+                       out_ptrs.get("relres"), out_ptrs.get("magnE"), out_ptrs.get("E"), out_ptrs.get("v"), 0, 0)
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters))
+        check(self._lib.cunibs_solve_block_device(self.handle, pos, mom, int(n_dip), centers, handles, dists, int(k),
+                                                  float(didt), C.byref(opts), C.byref(out)))
+        return out.total_iterations, out.outer_steps
+
+    def set_conductivity(self, sigma_by_tag) -> None:
+        s = np.ascontiguousarray(sigma_by_tag, np.float64).reshape(11)
+        check(self._lib.cunibs_context_set_conductivity(self.handle, s.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def solve_block(self, coil, centers, handles, dists, didt, *, block_width=0, precision=PREC_DEFAULT,
+                    tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False) -> dict:
+        """One block of k placements through cunibs_solve_block (host buffers in and out)."""
+        centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
+        k = centers.shape[0]
+        handles = np.ascontiguousarray(handles, np.float64).reshape(-1, 3)
+        dists = np.ascontiguousarray(dists, np.float64).reshape(-1)
+        pos = np.ascontiguousarray(coil.positions_m, np.float64)
+        mom = np.ascontiguousarray(coil.moments, np.float64)
+        res = {
+            "transform": np.empty((k, 4, 4)),
+            "summary": np.empty((k, SUMMARY_LEN)),
+            "iterations": np.empty(k, np.int32),
+            "relative_residual": np.empty(k),
+            "magnE": np.empty((k, self.n_tets), np.float32) if magnitude else None,
+            "E": np.empty((k, self.n_tets, 3), np.float32) if vectors else None,
+            "v": np.empty((k, self.n_nodes)) if potential else None,
+        }
+        out = BlockOut(_p(res["transform"]), _p(res["summary"]), _p(res["iterations"]), _p(res["relative_residual"]),
+                       _p(res["magnE"]), _p(res["E"]), _p(res["v"]), 0, 0)
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters))
+        check(self._lib.cunibs_solve_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
+                                           _p(dists), k, float(didt), C.byref(opts), C.byref(out)))
+        res["total_iterations"] = out.total_iterations
+        res["outer_steps"] = out.outer_steps
+        return res
+
+
+def kernel_launches() -> int:
+    return int(load().cunibs_kernel_launches())
+
+
+def select_size4(row_ptr, col_idx, values):
+    lib = load()
+    rp = np.ascontiguousarray(row_ptr, np.int32)
+    n = rp.shape[0] - 1
+    agg = np.empty(max(n, 1), np.int32)
+    nc = C.c_int()
+    ci = np.ascontiguousarray(col_idx, np.int32)
+    va = np.ascontiguousarray(values, np.float32)
+    check(lib.cunibs_select_size4(n, _ip(rp), _ip(ci), va.ctypes.data_as(C.POINTER(C.c_float)), _ip(agg), C.byref(nc)))
+    return agg[:n], nc.value

@@ -1,0 +1,573 @@
+// The C ABI (include/cunibs_b200.h): context lifetime, the block solve, stage-level entry points.
+#include <cstring>
+#include <string>
+
+#include "../../include/cunibs_b200.h"
+#include "internal.hpp"
+
+using namespace cunibs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+int guarded(F&& f) {
+    try {
+        f();
+        return CUNIBS_OK;
+    } catch (const Error& e) {
+        g_last_error = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_last_error = "host allocation failed";
+        return CUNIBS_ENOMEM;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return CUNIBS_EINTERNAL;
+    }
+}
+
+void require(bool ok, const char* msg) {
+    if (!ok) fail(kEInval, msg);
+}
+
+int to_internal_precision(int p) {
+    if (p == CUNIBS_PREC_PLAIN_FP64) return kPlainFp64;
+    if (p == CUNIBS_PREC_MIXED) return kMixed;
+    fail(kEInval, "precision must be CUNIBS_PREC_PLAIN_FP64 or CUNIBS_PREC_MIXED");
+}
+
+int pad_width(int k) {
+    for (int w : {1, 2, 4, 8, 16})
+        if (w >= k) return w;
+    fail(kEInval, "at most 16 placements per block");
+}
+
+}  // namespace
+
+struct cunibs_context {
+    int device = 0;
+    Params prm;
+    cudaStream_t stream = nullptr;
+    Mesh mesh;
+    Hierarchy hier;
+    SolverPtr solver;
+    SummaryWork sw;
+    // Block workspace, grown on demand.
+    DevArray<double> pos, mom, centers, handles, dists, T, B, X, summary, v;
+    DevArray<int> deg;
+    DevArray<unsigned char> dip_packed;
+    DevArray<float> dadt_nodes, dadt_elm, magn, E;
+    // Stage timing (CUDA events on the context stream), enabled by cunibs_context_set_timing.
+    bool timing = false;
+    cudaEvent_t ev[6] = {};
+    double stage_ms[5] = {};
+
+    void mark(int i) {
+        if (timing) CUNIBS_CHECK(cudaEventRecord(ev[i], stream));
+    }
+
+    void rebuild_hierarchy() {
+        solver.reset();
+        DevCsr<double> a0;
+        reduce_grounded(mesh, a0, stream);
+        build_hierarchy(hier, a0, prm, stream);
+        solver = make_solver(hier, prm);
+    }
+
+    ~cunibs_context() {
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        solver.reset();
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        CUNIBS_CHECK(cudaSetDevice(dev));
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+Params resolve(const cunibs_context* c, const cunibs_solve_opts* o) {
+    Params p = c->prm;
+    if (o) {
+        if (o->precision != CUNIBS_PREC_DEFAULT) p.precision = to_internal_precision(o->precision);
+        if (o->tolerance > 0) p.tolerance = o->tolerance;
+        if (o->max_iters > 0) p.max_iters = o->max_iters;
+    }
+    return p;
+}
+
+// The block solve on device-resident inputs; outputs land in the context's workspace.
+void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, int n_dip, const double* centers,
+                     const double* handles, const double* dists, int k, double didt, const cunibs_solve_opts* opts,
+                     SolveStats& st, bool want_E, int& K_out) {
+    require(k >= 1, "need at least one placement");
+    require(n_dip >= 1, "the coil needs at least one dipole");
+    const int K = (opts && opts->block_width > 0) ? opts->block_width : pad_width(k);
+    require(K >= k, "block_width must be at least the number of placements");
+    K_out = K;
+    const Params prm = resolve(c, opts);
+    Mesh& m = c->mesh;
+    cudaStream_t s = c->stream;
+    const int n_red = m.n_nodes - 1;
+    c->T.reserve(16 * static_cast<std::size_t>(k));
+    c->deg.reserve(k);
+    c->mark(0);
+    place_transforms(m, centers, handles, dists, k, c->T.get(), c->deg.get(), s);
+    std::vector<int> deg(k);
+    CUNIBS_CHECK(cudaMemcpyAsync(deg.data(), c->deg.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, s));
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    for (int i = 0; i < k; ++i)
+        if (handles != nullptr && deg[i])
+            fail(kEInval, "degenerate coil placement at index " + std::to_string(i) + " of " + std::to_string(k) +
+                              ": the handle lies on the outward scalp normal through the projected centre, so the "
+                              "coil's rotation about the normal is undefined");
+    c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
+    prep_dipoles(pos, mom, n_dip, c->T.get(), k, c->dip_packed.get(), s);
+    c->dadt_nodes.reserve(static_cast<std::size_t>(m.n_nodes) * 3 * k);
+    c->mark(1);
+    dadt_nodes(m, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, c->T.get(), k, didt, c->dadt_nodes.get(),
+               s);
+    c->mark(2);
+    c->dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
+    dadt_elements(m, c->dadt_nodes.get(), k, c->dadt_elm.get(), s);
+    c->B.reserve(static_cast<std::size_t>(n_red) * K);
+    c->X.reserve(static_cast<std::size_t>(n_red) * K);
+    rhs_block(m, c->dadt_elm.get(), k, K, c->B.get(), s);
+    c->mark(3);
+    solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, prm, s, st);
+    // Columns that missed tolerance: one FP64 retry from their current iterate, then an error
+    // (the rebuild-then-retry contract of fem/solve.py:528-551).
+    std::vector<int> missed;
+    for (int i = 0; i < k; ++i)
+        if (!(st.col_rel[i] <= prm.tolerance)) missed.push_back(i);
+    if (!missed.empty()) {
+        Params retry = prm;
+        retry.precision = kPlainFp64;
+        SolveStats st2;
+        solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, retry, s, st2, c->X.get());
+        for (int i : missed) {
+            st.col_iters[i] += st2.col_iters[i];
+            st.col_rel[i] = st2.col_rel[i];
+            if (!(st2.col_rel[i] <= prm.tolerance)) {
+                fail(kENoConv, "PCG did not converge (column " + std::to_string(i) + " of the block): " +
+                                   std::to_string(st.col_iters[i]) + " iterations, relative residual " +
+                                   std::to_string(st2.col_rel[i]) + " > tolerance " + std::to_string(prm.tolerance));
+            }
+        }
+        st.iterations += st2.iterations;
+    }
+    c->mark(4);
+    c->magn.reserve(static_cast<std::size_t>(m.n_tets) * k);
+    if (want_E) c->E.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
+    reconstruct_block(m, c->X.get(), k, K, c->dadt_elm.get(), want_E ? c->E.get() : nullptr, c->magn.get(), s);
+    c->summary.reserve(static_cast<std::size_t>(kSummaryLen) * k);
+    gm_summary(m, c->magn.get(), k, c->summary.get(), c->sw, s);
+    c->mark(5);
+    if (c->timing) {
+        CUNIBS_CHECK(cudaEventSynchronize(c->ev[5]));
+        for (int i = 0; i < 5; ++i) {
+            float ms = 0.0f;
+            CUNIBS_CHECK(cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]));
+            c->stage_ms[i] = ms;
+        }
+    }
+}
+
+void copy_out(void* dst, const void* src, std::size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
+    if (dst && bytes) CUNIBS_CHECK(cudaMemcpyAsync(dst, src, bytes, kind, s));
+}
+
+}  // namespace
+
+extern "C" {
+
+int cunibs_version(void) { return 1; }
+
+const char* cunibs_last_error(void) { return g_last_error.c_str(); }
+
+int cunibs_params_default(cunibs_params* out) {
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        const Params p;
+        out->device = 0;
+        out->min_coarse_rows = p.min_coarse_rows;
+        out->max_levels = p.max_levels;
+        out->agg_rounds = p.agg_rounds;
+        out->cheby_degree = p.cheby_degree;
+        out->cheby_lower_ratio = p.cheby_lower_ratio;
+        out->tolerance = p.tolerance;
+        out->max_iters = p.max_iters;
+        out->precision = CUNIBS_PREC_MIXED;
+        out->inner_reduction = p.inner_reduction;
+        out->inner_max_iters = p.inner_max_iters;
+        out->iters_per_sync = p.iters_per_sync;
+    });
+}
+
+int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_nodes, const int* tet_tags, int n_tets,
+                          const int* skin_tris, int n_skin, const cunibs_params* params, cunibs_context** out) {
+    return guarded([&] {
+        require(out != nullptr, "out is NULL");
+        *out = nullptr;
+        require(nodes_mm && tet_nodes && tet_tags, "mesh arrays must not be NULL");
+        require(n_skin == 0 || skin_tris != nullptr, "skin_tris is NULL");
+        cunibs_params p;
+        if (params) p = *params;
+        else cunibs_params_default(&p);
+        auto c = std::make_unique<cunibs_context>();
+        c->device = p.device;
+        DeviceGuard dg(c->device);
+        c->prm.min_coarse_rows = p.min_coarse_rows;
+        c->prm.max_levels = p.max_levels;
+        c->prm.agg_rounds = p.agg_rounds;
+        c->prm.cheby_degree = p.cheby_degree;
+        c->prm.cheby_lower_ratio = p.cheby_lower_ratio;
+        c->prm.tolerance = p.tolerance;
+        c->prm.max_iters = p.max_iters;
+        c->prm.precision = to_internal_precision(p.precision == CUNIBS_PREC_DEFAULT ? CUNIBS_PREC_MIXED : p.precision);
+        c->prm.inner_reduction = p.inner_reduction;
+        c->prm.inner_max_iters = p.inner_max_iters;
+        c->prm.iters_per_sync = p.iters_per_sync > 0 ? p.iters_per_sync : 4;
+        require(c->prm.tolerance > 0 && c->prm.max_iters > 0, "tolerance and max_iters must be positive");
+        CUNIBS_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        build_mesh(c->mesh, nodes_mm, n_nodes, tet_nodes, tet_tags, n_tets, skin_tris, n_skin, c->stream);
+        c->rebuild_hierarchy();
+        *out = c.release();
+    });
+}
+
+int cunibs_context_destroy(cunibs_context* ctx) {
+    return guarded([&] {
+        if (!ctx) return;
+        DeviceGuard dg(ctx->device);
+        CUNIBS_CHECK(cudaStreamSynchronize(ctx->stream));
+        delete ctx;
+    });
+}
+
+int cunibs_context_info(const cunibs_context* c, cunibs_info* out) {
+    return guarded([&] {
+        require(c && out, "NULL argument");
+        out->n_nodes = c->mesh.n_nodes;
+        out->n_tets = c->mesh.n_tets;
+        out->n_skin = c->mesh.n_skin;
+        out->n_gray_matter = c->mesh.n_gm;
+        out->stiffness_nnz = c->mesh.k_nnz;
+        out->ground_node = c->mesh.ground;
+        out->n_levels = static_cast<int>(c->hier.levels.size());
+        out->coarse_rows = c->hier.nc;
+    });
+}
+
+int cunibs_context_mesh(const cunibs_context* c, double* nodes_mm, int* tet_nodes, int* tet_tags, int* skin_tris,
+                        int* node_perm, int* tet_perm) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        DeviceGuard dg(c->device);
+        const Mesh& m = c->mesh;
+        cudaStream_t s = c->stream;
+        copy_out(nodes_mm, m.nodes.get(), sizeof(double) * 3 * m.n_nodes, cudaMemcpyDeviceToHost, s);
+        copy_out(tet_nodes, m.tets.get(), sizeof(int) * 4 * static_cast<std::size_t>(m.n_tets), cudaMemcpyDeviceToHost, s);
+        copy_out(tet_tags, m.tags.get(), sizeof(int) * m.n_tets, cudaMemcpyDeviceToHost, s);
+        copy_out(skin_tris, m.skin.get(), sizeof(int) * 3 * m.n_skin, cudaMemcpyDeviceToHost, s);
+        copy_out(node_perm, m.node_perm.get(), sizeof(int) * m.n_nodes, cudaMemcpyDeviceToHost, s);
+        copy_out(tet_perm, m.tet_perm.get(), sizeof(int) * m.n_tets, cudaMemcpyDeviceToHost, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+int cunibs_context_levels(const cunibs_context* c, int* sizes, int cap) {
+    return guarded([&] {
+        require(c && sizes, "NULL argument");
+        const std::size_t n = c->hier.sizes.size();
+        require(cap >= static_cast<int>(n), "sizes buffer too small");
+        for (std::size_t i = 0; i < n; ++i) sizes[i] = c->hier.sizes[i];
+    });
+}
+
+int cunibs_solve_block(cunibs_context* c, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                       const double* centers_mm, const double* handles_mm, const double* dists_mm, int k, double didt,
+                       const cunibs_solve_opts* opts, cunibs_block_out* out) {
+    return guarded([&] {
+        require(c && out, "NULL argument");
+        require(dip_pos_m && dip_moment && centers_mm && handles_mm && dists_mm, "input arrays must not be NULL");
+        require(out->transforms && out->summary, "out->transforms and out->summary are required");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        c->pos.upload(dip_pos_m, 3 * static_cast<std::size_t>(n_dip), s);
+        c->mom.upload(dip_moment, 3 * static_cast<std::size_t>(n_dip), s);
+        c->centers.upload(centers_mm, 3 * static_cast<std::size_t>(k), s);
+        c->handles.upload(handles_mm, 3 * static_cast<std::size_t>(k), s);
+        c->dists.upload(dists_mm, static_cast<std::size_t>(k), s);
+        SolveStats st;
+        int K = 0;
+        solve_block_dev(c, c->pos.get(), c->mom.get(), n_dip, c->centers.get(), c->handles.get(), c->dists.get(), k,
+                        didt, opts, st, out->E != nullptr, K);
+        const Mesh& m = c->mesh;
+        copy_out(out->transforms, c->T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToHost, s);
+        copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToHost, s);
+        copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
+        copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
+        if (out->v) {
+            c->v.reserve(static_cast<std::size_t>(m.n_nodes) * k);
+            scatter_potential(m, c->X.get(), k, K, c->v.get(), s);
+            copy_out(out->v, c->v.get(), sizeof(double) * static_cast<std::size_t>(m.n_nodes) * k, cudaMemcpyDeviceToHost, s);
+        }
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        for (int i = 0; i < k; ++i) {
+            if (out->iterations) out->iterations[i] = st.col_iters[i];
+            if (out->relres) out->relres[i] = st.col_rel[i];
+        }
+        out->total_iterations = st.iterations;
+        out->outer_steps = st.outer_steps;
+    });
+}
+
+int cunibs_solve_block_device(cunibs_context* c, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                              const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
+                              double didt, const cunibs_solve_opts* opts, cunibs_block_out* out) {
+    return guarded([&] {
+        require(c && out, "NULL argument");
+        require(out->transforms && out->summary, "out->transforms and out->summary are required");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        SolveStats st;
+        int K = 0;
+        solve_block_dev(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k, didt, opts, st,
+                        out->E != nullptr, K);
+        const Mesh& m = c->mesh;
+        copy_out(out->transforms, c->T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToDevice, s);
+        copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToDevice, s);
+        copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
+        copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
+        if (out->v) scatter_potential(m, c->X.get(), k, K, out->v, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        if (out->iterations)
+            CUNIBS_CHECK(cudaMemcpy(out->iterations, st.col_iters.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
+        if (out->relres)
+            CUNIBS_CHECK(cudaMemcpy(out->relres, st.col_rel.data(), sizeof(double) * k, cudaMemcpyHostToDevice));
+        out->total_iterations = st.iterations;
+        out->outer_steps = st.outer_steps;
+    });
+}
+
+int cunibs_context_set_conductivity(cunibs_context* c, const double* sigma_by_tag) {
+    return guarded([&] {
+        require(c && sigma_by_tag, "NULL argument");
+        for (int t = 1; t <= 10; ++t) require(sigma_by_tag[t] > 0.0, "conductivities must be positive");
+        DeviceGuard dg(c->device);
+        assemble_stiffness(c->mesh, sigma_by_tag, c->stream);
+        c->rebuild_hierarchy();
+    });
+}
+
+int cunibs_context_array(const cunibs_context* c, const char* name, int level, void* out, long long cap,
+                         long long* len) {
+    return guarded([&] {
+        require(c && name && len, "NULL argument");
+        DeviceGuard dg(c->device);
+        const Mesh& m = c->mesh;
+        const Hierarchy& h = c->hier;
+        const std::string n(name);
+        const void* src = nullptr;
+        std::size_t count = 0, elem = 4;
+        auto pick = [&](const void* p, std::size_t cnt, std::size_t es) {
+            src = p;
+            count = cnt;
+            elem = es;
+        };
+        const bool lv_ok = level >= 0 && level < static_cast<int>(h.levels.size());
+        if (n == "node_perm") pick(m.node_perm.get(), m.n_nodes, 4);
+        else if (n == "tet_perm") pick(m.tet_perm.get(), m.n_tets, 4);
+        else if (n == "tet_nodes") pick(m.tets.get(), 4 * static_cast<std::size_t>(m.n_tets), 4);
+        else if (n == "tet_tags") pick(m.tags.get(), m.n_tets, 4);
+        else if (n == "skin_tris") pick(m.skin.get(), 3 * static_cast<std::size_t>(m.n_skin), 4);
+        else if (n == "n2c_ptr") pick(m.n2c_ptr.get(), m.n_nodes + 1, 4);
+        else if (n == "n2c_idx") pick(m.n2c_idx.get(), 4 * static_cast<std::size_t>(m.n_tets), 4);
+        else if (n == "stiff_ptr") pick(m.k_ptr.get(), m.n_nodes + 1, 4);
+        else if (n == "stiff_col") pick(m.k_col.get(), m.k_nnz, 4);
+        else if (n == "gm_index") pick(m.gm_index.get(), m.n_gm, 4);
+        else if (n == "nodes_mm") pick(m.nodes.get(), 3 * static_cast<std::size_t>(m.n_nodes), 8);
+        else if (n == "g") pick(m.g.get(), 12 * static_cast<std::size_t>(m.n_tets), 8);
+        else if (n == "vols") pick(m.vols.get(), m.n_tets, 8);
+        else if (n == "bary") pick(m.bary.get(), 3 * static_cast<std::size_t>(m.n_tets), 8);
+        else if (n == "stiff_val") pick(m.k_val.get(), m.k_nnz, 8);
+        else if (n == "skin_normals") pick(m.skin_normals.get(), 3 * static_cast<std::size_t>(m.n_skin), 8);
+        else if (n == "coarse_ptr") pick(h.coarse.ptr.get(), h.nc + 1, 4);
+        else if (n == "coarse_col") pick(h.coarse.col.get(), h.coarse.nnz, 4);
+        else if (n == "coarse_val") pick(h.coarse.val.get(), h.coarse.nnz, 8);
+        else if (n == "coarse_inv") pick(h.coarse_inv.get(), static_cast<std::size_t>(h.nc) * h.nc, 8);
+        else if (lv_ok && n == "a_ptr") pick(h.levels[level].a.ptr.get(), h.levels[level].n + 1, 4);
+        else if (lv_ok && n == "a_col") pick(h.levels[level].a.col.get(), h.levels[level].a.nnz, 4);
+        else if (lv_ok && n == "a_val") pick(h.levels[level].a.val.get(), h.levels[level].a.nnz, 8);
+        else if (lv_ok && n == "agg") pick(h.levels[level].agg.get(), h.levels[level].n, 4);
+        else if (lv_ok && n == "p_ptr") pick(h.levels[level].p.ptr.get(), h.levels[level].n + 1, 4);
+        else if (lv_ok && n == "p_col") pick(h.levels[level].p.col.get(), h.levels[level].p.nnz, 4);
+        else if (lv_ok && n == "p_val") pick(h.levels[level].p.val.get(), h.levels[level].p.nnz, 8);
+        else if (lv_ok && n == "dinv") pick(h.levels[level].dinv.get(), h.levels[level].n, 8);
+        else fail(kEInval, "unknown array name or level: " + n);
+        *len = static_cast<long long>(count);
+        if (out && count) {
+            const std::size_t nb = std::min<std::size_t>(count, static_cast<std::size_t>(cap)) * elem;
+            CUNIBS_CHECK(cudaMemcpy(out, src, nb, cudaMemcpyDeviceToHost));
+        }
+    });
+}
+
+int cunibs_context_place(cunibs_context* c, const double* centers_mm, const double* handles_mm, const double* dists_mm,
+                         int k, double* transforms, int* degenerate) {
+    return guarded([&] {
+        require(c && centers_mm && dists_mm && transforms, "NULL argument");
+        require(k >= 1, "need at least one placement");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        c->centers.upload(centers_mm, 3 * static_cast<std::size_t>(k), s);
+        if (handles_mm) c->handles.upload(handles_mm, 3 * static_cast<std::size_t>(k), s);
+        c->dists.upload(dists_mm, k, s);
+        c->T.reserve(16 * static_cast<std::size_t>(k));
+        c->deg.reserve(k);
+        place_transforms(c->mesh, c->centers.get(), handles_mm ? c->handles.get() : nullptr, c->dists.get(), k,
+                         c->T.get(), c->deg.get(), s);
+        copy_out(transforms, c->T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToHost, s);
+        copy_out(degenerate, c->deg.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+int cunibs_context_dadt(cunibs_context* c, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                        const double* transforms, int k, double didt, float* out) {
+    return guarded([&] {
+        require(c && dip_pos_m && dip_moment && transforms && out, "NULL argument");
+        require(k >= 1 && n_dip >= 1, "need at least one transform and one dipole");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        c->pos.upload(dip_pos_m, 3 * static_cast<std::size_t>(n_dip), s);
+        c->mom.upload(dip_moment, 3 * static_cast<std::size_t>(n_dip), s);
+        DevArray<double> T;
+        T.upload(transforms, 16 * static_cast<std::size_t>(k), s);
+        c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
+        prep_dipoles(c->pos.get(), c->mom.get(), n_dip, T.get(), k, c->dip_packed.get(), s);
+        c->dadt_nodes.reserve(static_cast<std::size_t>(c->mesh.n_nodes) * 3 * k);
+        dadt_nodes(c->mesh, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, T.get(), k, didt,
+                   c->dadt_nodes.get(), s);
+        copy_out(out, c->dadt_nodes.get(), sizeof(float) * 3 * static_cast<std::size_t>(c->mesh.n_nodes) * k,
+                 cudaMemcpyDeviceToHost, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+int cunibs_context_solve(cunibs_context* c, const double* B, double* X, int k, int width, int precision,
+                         double tolerance, int max_iters, const double* x0, int* iterations, double* relres) {
+    return guarded([&] {
+        require(c && B && X, "NULL argument");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        const std::size_t nk = static_cast<std::size_t>(c->mesh.n_nodes - 1) * width;
+        DevArray<double> dB, dX, dX0;
+        dB.upload(B, nk, s);
+        dX.resize(nk);
+        if (x0) dX0.upload(x0, nk, s);
+        cunibs_solve_opts o{};
+        o.precision = precision;
+        o.tolerance = tolerance;
+        o.max_iters = max_iters;
+        const Params prm = resolve(c, &o);
+        SolveStats st;
+        solver_solve(*c->solver, dB.get(), dX.get(), k, width, prm, s, st, x0 ? dX0.get() : nullptr);
+        dX.download(X, nk, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        for (int i = 0; i < k; ++i) {
+            if (iterations) iterations[i] = st.col_iters[i];
+            if (relres) relres[i] = st.col_rel[i];
+        }
+    });
+}
+
+int cunibs_context_vcycle(cunibs_context* c, const double* r, double* z, int k, int fp32) {
+    return guarded([&] {
+        require(c && r && z, "NULL argument");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        const std::size_t nk = static_cast<std::size_t>(c->mesh.n_nodes - 1) * k;
+        DevArray<double> dr, dz(nk);
+        dr.upload(r, nk, s);
+        solver_vcycle(*c->solver, dr.get(), dz.get(), k, fp32 != 0, s);
+        dz.download(z, nk, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+int cunibs_select_size4(int n, const int* row_ptr, const int* col_idx, const float* values, int* aggregates,
+                        int* n_coarse) {
+    return guarded([&] {
+        require(n >= 0 && row_ptr && aggregates && n_coarse, "NULL argument");
+        cudaStream_t s = nullptr;
+        CUNIBS_CHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        struct StreamDel {
+            cudaStream_t s;
+            ~StreamDel() { cudaStreamDestroy(s); }
+        } del{s};
+        const int nnz = row_ptr[n];
+        DevArray<int> rp, ci, agg(n > 0 ? n : 1);
+        DevArray<float> va;
+        rp.upload(row_ptr, n + 1, s);
+        ci.upload(col_idx, nnz, s);
+        va.upload(values, nnz, s);
+        *n_coarse = select_size4(n, rp.get(), ci.get(), va.get(), agg.get(), s);
+        agg.download(aggregates, n, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+int cunibs_context_summary(cunibs_context* c, const float* magnE, int k, double* summary) {
+    return guarded([&] {
+        require(c && magnE && summary && k >= 1, "NULL argument");
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        DevArray<float> dm;
+        dm.upload(magnE, static_cast<std::size_t>(c->mesh.n_tets) * k, s);
+        DevArray<double> out(static_cast<std::size_t>(kSummaryLen) * k);
+        gm_summary(c->mesh, dm.get(), k, out.get(), c->sw, s);
+        out.download(summary, static_cast<std::size_t>(kSummaryLen) * k, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    });
+}
+
+int cunibs_context_set_timing(cunibs_context* c, int on) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        DeviceGuard dg(c->device);
+        if (on && !c->ev[0])
+            for (cudaEvent_t& e : c->ev) CUNIBS_CHECK(cudaEventCreate(&e));
+        c->timing = on != 0;
+    });
+}
+
+int cunibs_context_stage_times(const cunibs_context* c, double* ms, int cap) {
+    return guarded([&] {
+        require(c && ms && cap >= 5, "NULL argument or cap < 5");
+        for (int i = 0; i < 5; ++i) ms[i] = c->stage_ms[i];
+    });
+}
+
+int cunibs_context_stream(const cunibs_context* c, void** stream) {
+    return guarded([&] {
+        require(c && stream, "NULL argument");
+        *stream = c->stream;
+    });
+}
+
+long long cunibs_kernel_launches(void) { return launch_counter().load(); }
+
+}  // extern "C"

@@ -1,0 +1,227 @@
+// Coil dA/dt at the mesh nodes, its element average, and the k-wide FEM right-hand side.
+//
+// dA/dt(r) = didt * mu0/4pi * sum_j m_j x (r - s_j) / |r - s_j|^3   (fem/placement.py:279-317).
+//
+// The N-body sum is the hot part: N nodes x D dipoles x k placements pair evaluations. Each block
+// stages a tile of one placement's dipoles in shared memory (positions and moments already rotated
+// into the head frame and centred on the coil origin in FP64, then rounded to FP32, as the reference
+// does to keep |r - s|^2 free of cancellation), and every thread carries four nodes as two float2
+// pairs so the arithmetic issues as sm_100 packed FP32 instructions (FFMA2/FADD2/FMUL2): two node
+// evaluations per instruction. The difference r - s is formed directly rather than through
+// |r|^2 + |s|^2 - 2 r.s, which costs no more here and loses nothing to cancellation.
+#include <cstdint>
+
+#include "internal.hpp"
+
+namespace cunibs {
+namespace {
+
+constexpr int kDadtThreads = 128;
+constexpr int kDipTile = 256;
+
+// One placement's dipoles in the head frame, centred on the coil origin, each component stored
+// twice so a shared-memory load yields a ready float2 broadcast: {s,s}, {m,m} per axis.
+struct __align__(16) DipolePacked {
+    float2 sx, sy, sz, mx, my, mz;
+};
+
+// Per (placement, dipole): s' = R pos (metres), m' = R mom, where R is the transform's rotation.
+// The translation cancels against the centring at the coil origin.
+__global__ void prep_dipoles_kernel(const double* __restrict__ pos, const double* __restrict__ mom, int n_dip,
+                                    const double* __restrict__ T, int k, DipolePacked* __restrict__ out) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<long>(n_dip) * k) return;
+    const int p = static_cast<int>(q / n_dip);
+    const int j = static_cast<int>(q % n_dip);
+    const double* R = T + 16 * static_cast<long>(p);
+    double s[3], m[3];
+    for (int a = 0; a < 3; ++a) {
+        s[a] = R[4 * a] * pos[3 * j] + R[4 * a + 1] * pos[3 * j + 1] + R[4 * a + 2] * pos[3 * j + 2];
+        m[a] = R[4 * a] * mom[3 * j] + R[4 * a + 1] * mom[3 * j + 1] + R[4 * a + 2] * mom[3 * j + 2];
+    }
+    DipolePacked d;
+    d.sx = make_float2(static_cast<float>(s[0]), static_cast<float>(s[0]));
+    d.sy = make_float2(static_cast<float>(s[1]), static_cast<float>(s[1]));
+    d.sz = make_float2(static_cast<float>(s[2]), static_cast<float>(s[2]));
+    d.mx = make_float2(static_cast<float>(m[0]), static_cast<float>(m[0]));
+    d.my = make_float2(static_cast<float>(m[1]), static_cast<float>(m[1]));
+    d.mz = make_float2(static_cast<float>(m[2]), static_cast<float>(m[2]));
+    out[q] = d;
+}
+
+__device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
+
+// grid = (ceil(N / (4*threads)), k). Node i of this thread: base + {0, 1, 2, 3} * stride, paired
+// as (0, 1) and (2, 3) into float2 lanes.
+__global__ void __launch_bounds__(kDadtThreads) dadt_kernel(const double* __restrict__ nodes_mm, int n_nodes,
+                                                            const DipolePacked* __restrict__ dip, int n_dip,
+                                                            const double* __restrict__ T, float scale,
+                                                            float* __restrict__ out) {
+    __shared__ DipolePacked tile[kDipTile];
+    const int p = blockIdx.y;
+    const double* Tp = T + 16 * static_cast<long>(p);
+    const double ox = Tp[3] * 1e-3, oy = Tp[7] * 1e-3, oz = Tp[11] * 1e-3;
+    const int stride = gridDim.x * blockDim.x;
+    const int base = blockIdx.x * blockDim.x + threadIdx.x;
+    int node[4];
+    float rxs[4], rys[4], rzs[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        node[u] = base + u * stride;
+        const int i = node[u] < n_nodes ? node[u] : n_nodes - 1;
+        rxs[u] = static_cast<float>(nodes_mm[3 * static_cast<long>(i)] * 1e-3 - ox);
+        rys[u] = static_cast<float>(nodes_mm[3 * static_cast<long>(i) + 1] * 1e-3 - oy);
+        rzs[u] = static_cast<float>(nodes_mm[3 * static_cast<long>(i) + 2] * 1e-3 - oz);
+    }
+    const float2 rx0 = make_float2(rxs[0], rxs[1]), ry0 = make_float2(rys[0], rys[1]), rz0 = make_float2(rzs[0], rzs[1]);
+    const float2 rx1 = make_float2(rxs[2], rxs[3]), ry1 = make_float2(rys[2], rys[3]), rz1 = make_float2(rzs[2], rzs[3]);
+    float2 ax0 = make_float2(0.f, 0.f), ay0 = ax0, az0 = ax0, ax1 = ax0, ay1 = ax0, az1 = ax0;
+    const DipolePacked* dp = dip + static_cast<long>(p) * n_dip;
+    for (int t0 = 0; t0 < n_dip; t0 += kDipTile) {
+        const int nt = min(kDipTile, n_dip - t0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nt; j += blockDim.x) tile[j] = dp[t0 + j];
+        __syncthreads();
+#pragma unroll 2
+        for (int j = 0; j < nt; ++j) {
+            const DipolePacked d = tile[j];
+            // pair 0
+            {
+                const float2 dx = __fadd2_rn(rx0, f2neg(d.sx));
+                const float2 dy = __fadd2_rn(ry0, f2neg(d.sy));
+                const float2 dz = __fadd2_rn(rz0, f2neg(d.sz));
+                float2 d2 = __fmul2_rn(dx, dx);
+                d2 = __ffma2_rn(dy, dy, d2);
+                d2 = __ffma2_rn(dz, dz, d2);
+                const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+                const float2 w = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+                const float2 cx = __ffma2_rn(d.my, dz, __fmul2_rn(f2neg(d.mz), dy));
+                const float2 cy = __ffma2_rn(d.mz, dx, __fmul2_rn(f2neg(d.mx), dz));
+                const float2 cz = __ffma2_rn(d.mx, dy, __fmul2_rn(f2neg(d.my), dx));
+                ax0 = __ffma2_rn(w, cx, ax0);
+                ay0 = __ffma2_rn(w, cy, ay0);
+                az0 = __ffma2_rn(w, cz, az0);
+            }
+            // pair 1
+            {
+                const float2 dx = __fadd2_rn(rx1, f2neg(d.sx));
+                const float2 dy = __fadd2_rn(ry1, f2neg(d.sy));
+                const float2 dz = __fadd2_rn(rz1, f2neg(d.sz));
+                float2 d2 = __fmul2_rn(dx, dx);
+                d2 = __ffma2_rn(dy, dy, d2);
+                d2 = __ffma2_rn(dz, dz, d2);
+                const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+                const float2 w = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+                const float2 cx = __ffma2_rn(d.my, dz, __fmul2_rn(f2neg(d.mz), dy));
+                const float2 cy = __ffma2_rn(d.mz, dx, __fmul2_rn(f2neg(d.mx), dz));
+                const float2 cz = __ffma2_rn(d.mx, dy, __fmul2_rn(f2neg(d.my), dx));
+                ax1 = __ffma2_rn(w, cx, ax1);
+                ay1 = __ffma2_rn(w, cy, ay1);
+                az1 = __ffma2_rn(w, cz, az1);
+            }
+        }
+    }
+    const float ax[4] = {ax0.x, ax0.y, ax1.x, ax1.y};
+    const float ay[4] = {ay0.x, ay0.y, ay1.x, ay1.y};
+    const float az[4] = {az0.x, az0.y, az1.x, az1.y};
+    float* o = out + static_cast<long>(p) * n_nodes * 3;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        if (node[u] < n_nodes) {
+            o[3 * static_cast<long>(node[u])] = scale * ax[u];
+            o[3 * static_cast<long>(node[u]) + 1] = scale * ay[u];
+            o[3 * static_cast<long>(node[u]) + 2] = scale * az[u];
+        }
+    }
+}
+
+// dadt_elm[p][e] = 1/4 sum of the four nodal values (dadt_element.cu:6-31).
+__global__ void element_average_kernel(const float* __restrict__ nodal, const int* __restrict__ tets, int n_nodes,
+                                       int n_tets, int k, float* __restrict__ elm) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<long>(n_tets) * k) return;
+    const int p = static_cast<int>(q / n_tets);
+    const int e = static_cast<int>(q % n_tets);
+    const int4 tn = reinterpret_cast<const int4*>(tets)[e];
+    const float* v = nodal + static_cast<long>(p) * n_nodes * 3;
+    float* o = elm + static_cast<long>(p) * n_tets * 3;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        o[3 * static_cast<long>(e) + a] =
+            0.25f * (v[3 * static_cast<long>(tn.x) + a] + v[3 * static_cast<long>(tn.y) + a] +
+                     v[3 * static_cast<long>(tn.z) + a] + v[3 * static_cast<long>(tn.w) + a]);
+}
+
+// b_red[r][c] = sum over the corners of node i of neg_vc[e] * (dadt_elm[c][e] . g[corner]),
+// accumulated in FP64 in node2corner order; node i = r, skipping the grounded node. Columns past
+// k repeat column k-1 (the padding of a partial block).
+template <int K>
+__global__ void __launch_bounds__(64 * K) rhs_kernel(const float* __restrict__ elm, const float* __restrict__ g32,
+                                                     const float* __restrict__ neg_vc, const int* __restrict__ ptr,
+                                                     const int* __restrict__ idx, int n_nodes, int n_tets, int k,
+                                                     int ground, double* __restrict__ b_red) {
+    const int r = blockIdx.x * 64 + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (r >= n_nodes - 1) return;
+    const int i = r + (r >= ground ? 1 : 0);
+    const int src = c < k ? c : k - 1;
+    const float* el = elm + static_cast<long>(src) * n_tets * 3;
+    double acc = 0.0;
+    for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
+        const int corner = idx[q];
+        const int e = corner >> 2;
+        const float* gc = g32 + 3 * static_cast<long>(corner);
+        const double d = static_cast<double>(el[3 * static_cast<long>(e)]) * gc[0] +
+                         static_cast<double>(el[3 * static_cast<long>(e) + 1]) * gc[1] +
+                         static_cast<double>(el[3 * static_cast<long>(e) + 2]) * gc[2];
+        acc += static_cast<double>(neg_vc[e]) * d;
+    }
+    b_red[static_cast<long>(r) * K + c] = acc;
+}
+
+}  // namespace
+
+void prep_dipoles(const double* pos, const double* mom, int n_dip, const double* transforms_dev, int k, void* out,
+                  cudaStream_t s) {
+    const long total = static_cast<long>(n_dip) * k;
+    prep_dipoles_kernel<<<grid_for(total), kBlock, 0, s>>>(pos, mom, n_dip, transforms_dev, k,
+                                                           static_cast<DipolePacked*>(out)); count_launch();
+    CUNIBS_LAUNCH_CHECK("prep dipoles");
+}
+
+std::size_t packed_dipole_bytes() { return sizeof(DipolePacked); }
+
+void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k, double didt,
+                float* out, cudaStream_t s) {
+    const int per_block = 4 * kDadtThreads;
+    const dim3 grid((m.n_nodes + per_block - 1) / per_block, k);
+    dadt_kernel<<<grid, kDadtThreads, 0, s>>>(m.nodes.get(), m.n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
+                                             n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out); count_launch();
+    CUNIBS_LAUNCH_CHECK("dadt");
+}
+
+void dadt_elements(const Mesh& m, const float* nodal, int k, float* elm, cudaStream_t s) {
+    const long total = static_cast<long>(m.n_tets) * k;
+    element_average_kernel<<<grid_for(total), kBlock, 0, s>>>(nodal, m.tets.get(), m.n_nodes, m.n_tets, k, elm); count_launch();
+    CUNIBS_LAUNCH_CHECK("dadt element average");
+}
+
+void rhs_block(const Mesh& m, const float* elm, int k, int K, double* b_red, cudaStream_t s) {
+    const unsigned g = (m.n_nodes - 1 + 63) / 64;
+    auto go = [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        rhs_kernel<KK><<<g, 64 * KK, 0, s>>>(elm, m.g32.get(), m.neg_vc32.get(), m.n2c_ptr.get(), m.n2c_idx.get(),
+                                             m.n_nodes, m.n_tets, k, m.ground, b_red); count_launch();
+    };
+    switch (K) {
+        case 1: go(std::integral_constant<int, 1>{}); break;
+        case 2: go(std::integral_constant<int, 2>{}); break;
+        case 4: go(std::integral_constant<int, 4>{}); break;
+        case 8: go(std::integral_constant<int, 8>{}); break;
+        case 16: go(std::integral_constant<int, 16>{}); break;
+        default: fail(kEInval, "block width must be one of {1, 2, 4, 8, 16}");
+    }
+    CUNIBS_LAUNCH_CHECK("rhs");
+}
+
+}  // namespace cunibs

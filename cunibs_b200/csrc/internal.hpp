@@ -1,0 +1,164 @@
+// Internal declarations shared by the cunibs_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <array>
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+
+namespace cunibs {
+
+// Solver precision modes.
+enum Precision : int {
+    kPlainFp64 = 0,   // FP64 PCG over an FP64 V-cycle: the plain method
+    kMixed = 1,       // FP32 PCG + FP32 V-cycle inside FP64 iterative refinement
+    kFp64CgFp32Mg = 2 // FP64 PCG over an FP32 V-cycle (the reference's own split)
+};
+
+struct Params {
+    int min_coarse_rows = 128;
+    int max_levels = 50;
+    int agg_rounds = 2;
+    int cheby_degree = 2;
+    double cheby_lower_ratio = 12.0;
+    double tolerance = 1e-6;
+    int max_iters = 2000;
+    int precision = kMixed;
+    double inner_reduction = 1e-4;  // inner FP32 PCG stops at this residual reduction
+    int inner_max_iters = 60;
+    int iters_per_sync = 4;         // PCG iterations launched between host convergence checks
+};
+
+struct Cheby {
+    int degree = 2;
+    double alpha0 = 0.0;
+    double c_cur[8] = {};
+    double c_prev[8] = {};
+    double alpha[8] = {};
+};
+
+Cheby make_cheby(int degree, double lower_ratio);
+
+// One level of the smoothed-aggregation hierarchy. FP64 values are the built operator; the FP32
+// copies (rounded once) are what the mixed-precision V-cycle streams.
+struct Level {
+    int n = 0;
+    int n_coarse = 0;
+    DevCsr<double> a;
+    DevArray<float> a32;
+    DevArray<double> dinv;
+    DevArray<float> dinv32;
+    DevArray<int> agg;
+    DevCsr<double> p;
+    DevArray<float> p32;
+    DevCsr<double> r;
+    DevArray<float> r32;
+};
+
+struct Hierarchy {
+    std::vector<Level> levels;
+    DevCsr<double> coarse;
+    int nc = 0;
+    DevArray<double> coarse_inv;   // dense (nc, nc), FP64 from a Cholesky factorisation
+    DevArray<float> coarse_inv32;
+    std::vector<int> sizes;
+    Cheby cheby;
+};
+
+// Per-subject device state, laid out along the Morton curve.
+struct Mesh {
+    int n_nodes = 0;
+    int n_tets = 0;
+    int n_skin = 0;
+    DevArray<double> nodes;     // (N,3) mm
+    DevArray<int> tets;         // (M,4)
+    DevArray<int> tags;         // (M)
+    DevArray<int> skin;         // (S,3)
+    DevArray<int> node_perm;    // sorted position -> input node
+    DevArray<int> tet_perm;     // sorted position -> input tet
+    DevArray<double> g;         // (M,4,3) FP64, 1/m
+    DevArray<float> g32;        // (M,4,3)
+    DevArray<double> vols;      // (M) m^3
+    DevArray<float> vols32;
+    DevArray<double> cond;      // (M) S/m
+    DevArray<float> neg_vc32;   // -(vol*sigma) in FP32
+    DevArray<double> bary;      // (M,3) mm
+    DevArray<int> n2c_ptr;      // (N+1)
+    DevArray<int> n2c_idx;      // (4M) corner ids
+    DevArray<double> skin_normals;  // (S,3)
+    // Stiffness pattern and the element-contribution map that assembles it.
+    DevArray<int> k_ptr;        // (N+1)
+    DevArray<int> k_col;        // (nnz)
+    DevArray<int> contrib_ptr;  // (nnz+1) into contrib_idx
+    DevArray<int> contrib_idx;  // (16M) e*16 + i*4 + j, ascending e within each entry
+    DevArray<double> k_val;     // (nnz) FP64
+    long k_nnz = 0;
+    int ground = 0;
+    // Gray-matter slice (tag 2): element index, FP32 volumes, barycentres.
+    DevArray<int> gm_index;
+    int n_gm = 0;
+};
+
+// Setup stages (setup_mesh.cu).
+void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, const int* tags, int n_tets,
+                const int* skin, int n_skin, cudaStream_t s);
+void assemble_stiffness(Mesh& m, const double* sigma_by_tag /* 11 entries or null */, cudaStream_t s);
+void reduce_grounded(const Mesh& m, DevCsr<double>& out, cudaStream_t s);
+
+// Hierarchy (setup_amg.cu).
+int select_size4(int n, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s);
+void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& p, cudaStream_t s);
+void spgemm(const DevCsr<double>& A, const DevCsr<double>& B, DevCsr<double>& C, cudaStream_t s);
+void transpose(const DevCsr<double>& A, DevCsr<double>& T, cudaStream_t s);
+void l1_dinv(const DevCsr<double>& a, DevArray<double>& dinv, cudaStream_t s);
+
+// Solver (solve.cu).
+struct SolveStats {
+    std::vector<int> col_iters;
+    std::vector<double> col_rel;
+    int iterations = 0;
+    int outer_steps = 0;
+};
+class Solver;
+struct SolverDeleter {
+    void operator()(Solver* s) const;
+};
+using SolverPtr = std::unique_ptr<Solver, SolverDeleter>;
+SolverPtr make_solver(const Hierarchy& h, const Params& p);
+void solver_solve(Solver& sv, const double* B, double* X, int k, int k_pad, const Params& p, cudaStream_t s,
+                  SolveStats& stats, const double* X0 = nullptr);
+void solver_vcycle(Solver& sv, const double* r, double* z, int k, bool fp32, cudaStream_t s);
+
+// Coil and right-hand side (coil.cu).
+void place_transforms(const Mesh& m, const double* centers, const double* handles, const double* dists, int k,
+                      double* transforms_dev, int* degenerate_dev, cudaStream_t s);
+std::size_t packed_dipole_bytes();
+// Rotates the coil's dipoles into each placement's head frame: (k, n_dip) packed records.
+void prep_dipoles(const double* pos, const double* mom, int n_dip, const double* transforms_dev, int k, void* out,
+                  cudaStream_t s);
+void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k, double didt,
+                float* out /* (k, N, 3) */, cudaStream_t s);
+void dadt_elements(const Mesh& m, const float* dadt_nodes, int k, float* dadt_elm /* (k, M, 3) */, cudaStream_t s);
+void rhs_block(const Mesh& m, const float* dadt_elm, int k, int k_pad, double* b_red /* (N-1, k_pad) */,
+               cudaStream_t s);
+
+// Post-processing (post.cu).
+void reconstruct_block(const Mesh& m, const double* x_red /* (N-1,k_pad) */, int k, int k_pad,
+                       const float* dadt_elm, float* E /* (k,M,3) or null */, float* magnE /* (k,M) */,
+                       cudaStream_t s);
+void scatter_potential(const Mesh& m, const double* x_red, int k, int k_pad, double* v /* (k,N) */, cudaStream_t s);
+constexpr int kSummaryLen = 16;
+struct SummaryWork {
+    DevArray<float> keys, keys_s;
+    DevArray<int> vals, vals_s, offsets;
+    DevArray<double> w_sorted, cw, tile_tot;
+    DevArray<unsigned char> temp;
+};
+void gm_summary(const Mesh& m, const float* magnE, int k, double* summary_dev /* (k,16) */, SummaryWork& w,
+                cudaStream_t s);
+
+}  // namespace cunibs

@@ -1,0 +1,318 @@
+// Post-processing of a solved block: E = -grad v - dA/dt per tetrahedron, the potential on the full
+// node set, and the gray-matter summary metrics.
+//
+// Reference behaviour restated: reconstruct.cu:36-76 (FP64 accumulation of grad v, FP32 output),
+// fem/solve.py:939-941 (grounded node carries v = 0), metrics.py:58-243 (volume-weighted
+// peak/location, centre of gravity, mean/std, p50/p95/p99/p99.9 at midpoint positions with linear
+// interpolation, focality at 0.5 and 0.75 of p99.9). The percentiles come from a stable segmented
+// radix sort of each placement's gray-matter |E| (keys = |E|, values = element slot) and a
+// fixed-order tiled prefix sum of the sorted volumes, so the ranks are integer-exact and the
+// cumulative weights reproduce run to run.
+#include <cub/cub.cuh>
+
+#include "internal.hpp"
+
+namespace cunibs {
+namespace {
+
+// One thread per (tet, column): E = -sum_i v[n_i] g_i - dadt_elm (FP64 accumulation).
+__global__ void reconstruct_kernel(const double* __restrict__ x_red, int K, int ground, const int* __restrict__ tets,
+                                   const float* __restrict__ g32, const float* __restrict__ elm, int n_tets, int k,
+                                   float* __restrict__ E, float* __restrict__ magn) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<long>(n_tets) * k) return;
+    const int c = static_cast<int>(q / n_tets);
+    const int e = static_cast<int>(q % n_tets);
+    const int4 tn = reinterpret_cast<const int4*>(tets)[e];
+    const int nd[4] = {tn.x, tn.y, tn.z, tn.w};
+    const float* ge = g32 + 12 * static_cast<long>(e);
+    double gx = 0.0, gy = 0.0, gz = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int node = nd[i];
+        const double vi = (node == ground) ? 0.0 : x_red[static_cast<long>(node - (node > ground ? 1 : 0)) * K + c];
+        gx += vi * static_cast<double>(ge[3 * i]);
+        gy += vi * static_cast<double>(ge[3 * i + 1]);
+        gz += vi * static_cast<double>(ge[3 * i + 2]);
+    }
+    const float* el = elm + static_cast<long>(c) * n_tets * 3 + 3 * static_cast<long>(e);
+    const double ex = -gx - static_cast<double>(el[0]);
+    const double ey = -gy - static_cast<double>(el[1]);
+    const double ez = -gz - static_cast<double>(el[2]);
+    if (E != nullptr) {
+        float* o = E + static_cast<long>(c) * n_tets * 3 + 3 * static_cast<long>(e);
+        o[0] = static_cast<float>(ex);
+        o[1] = static_cast<float>(ey);
+        o[2] = static_cast<float>(ez);
+    }
+    magn[static_cast<long>(c) * n_tets + e] = static_cast<float>(sqrt(ex * ex + ey * ey + ez * ez));
+}
+
+__global__ void scatter_kernel(const double* __restrict__ x_red, int K, int ground, int n_nodes, int k,
+                               double* __restrict__ v) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<long>(n_nodes) * k) return;
+    const int c = static_cast<int>(q / n_nodes);
+    const int i = static_cast<int>(q % n_nodes);
+    v[q] = (i == ground) ? 0.0 : x_red[static_cast<long>(i - (i > ground ? 1 : 0)) * K + c];
+}
+
+__global__ void gm_gather_kernel(const float* __restrict__ magn, const int* __restrict__ gm, int n_gm, int n_tets, int k,
+                                 float* __restrict__ keys, int* __restrict__ vals, int* __restrict__ offsets) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q <= k) {
+        if (q <= k) offsets[q] = static_cast<int>(q * n_gm);
+    }
+    if (q >= static_cast<long>(n_gm) * k) return;
+    const int c = static_cast<int>(q / n_gm);
+    const int i = static_cast<int>(q % n_gm);
+    keys[q] = magn[static_cast<long>(c) * n_tets + gm[i]];
+    vals[q] = i;
+}
+
+constexpr int kScanTile = 1024;
+
+// Inclusive scan of the sorted FP64 volumes within each tile of each placement's segment: a
+// sequential walk per 8-element thread strip, then a fixed tree over the strips.
+__global__ void tile_scan_kernel(const int* __restrict__ sorted_idx, const int* __restrict__ gm,
+                                 const float* __restrict__ vols32, int n_gm, double* __restrict__ w_sorted,
+                                 double* __restrict__ cw, double* __restrict__ tile_tot) {
+    constexpr int kPer = kScanTile / 128;
+    __shared__ double strip[128];
+    const int c = blockIdx.y;
+    const int tile = blockIdx.x;
+    const long base = static_cast<long>(c) * n_gm;
+    const int start = tile * kScanTile + threadIdx.x * kPer;
+    double local[kPer];
+    double run = 0.0;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int i = start + u;
+        double w = 0.0;
+        if (i < n_gm) {
+            w = static_cast<double>(vols32[gm[sorted_idx[base + i]]]);
+            w_sorted[base + i] = w;
+        }
+        run += w;
+        local[u] = run;
+    }
+    strip[threadIdx.x] = run;
+    __syncthreads();
+    // Exclusive prefix of the strip totals, Hillis-Steele over 128 entries (fixed order).
+    for (int off = 1; off < 128; off <<= 1) {
+        const double add = (threadIdx.x >= off) ? strip[threadIdx.x - off] : 0.0;
+        __syncthreads();
+        strip[threadIdx.x] += add;
+        __syncthreads();
+    }
+    const double before = (threadIdx.x > 0) ? strip[threadIdx.x - 1] : 0.0;
+#pragma unroll
+    for (int u = 0; u < kPer; ++u) {
+        const int i = start + u;
+        if (i < n_gm) cw[base + i] = before + local[u];
+    }
+    if (threadIdx.x == 127) tile_tot[static_cast<long>(c) * gridDim.x + tile] = strip[127];
+}
+
+// Adds the (sequentially scanned) totals of earlier tiles.
+__global__ void tile_offset_kernel(double* __restrict__ cw, const double* __restrict__ tile_tot, int n_gm, int tiles) {
+    __shared__ double off;
+    const int c = blockIdx.y;
+    const int tile = blockIdx.x;
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int t = 0; t < tile; ++t) s += tile_tot[static_cast<long>(c) * tiles + t];
+        off = s;
+    }
+    __syncthreads();
+    if (tile == 0) return;
+    const long base = static_cast<long>(c) * n_gm;
+    for (int i = tile * kScanTile + threadIdx.x; i < min(n_gm, (tile + 1) * kScanTile); i += blockDim.x)
+        cw[base + i] += off;
+}
+
+// interp(q, pos, v) with pos_i = (cw_i - w_i/2) / cw_last (metrics.py:82-95, numpy.interp).
+__device__ double quantile(double q, const float* __restrict__ v, const double* __restrict__ w,
+                           const double* __restrict__ cw, int n) {
+    const double total = cw[n - 1];
+    auto pos = [&](int i) { return (cw[i] - 0.5 * w[i]) / total; };
+    if (q <= pos(0)) return v[0];
+    if (q >= pos(n - 1)) return v[n - 1];
+    int lo = 0, hi = n - 1;  // pos(lo) <= q < pos(hi)
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pos(mid) <= q) lo = mid;
+        else hi = mid;
+    }
+    const double x0 = pos(lo), x1 = pos(lo + 1);
+    const double slope = (static_cast<double>(v[lo + 1]) - static_cast<double>(v[lo])) / (x1 - x0);
+    return slope * (q - x0) + static_cast<double>(v[lo]);
+}
+
+// One block per placement: peak/argmax, sums for mean/CoG, then variance; thread 0 finishes the
+// percentiles and focality from the sorted arrays.
+__global__ void summary_kernel(const float* __restrict__ magn, const int* __restrict__ gm, int n_gm, int n_tets,
+                               const float* __restrict__ vols32, const double* __restrict__ bary,
+                               const float* __restrict__ sorted_keys, const double* __restrict__ w_sorted,
+                               const double* __restrict__ cw, double* __restrict__ out) {
+    constexpr int kT = 512;
+    __shared__ double sv[kT], sw[kT], swm[kT], sx[kT], sy[kT], sz[kT];
+    __shared__ int si[kT];
+    __shared__ double mean_sh;
+    const int c = blockIdx.x;
+    const float* m = magn + static_cast<long>(c) * n_tets;
+    double best = -1.0;
+    int bi = 0x7fffffff;
+    double w_s = 0.0, wm_s = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    for (int i = threadIdx.x; i < n_gm; i += kT) {
+        const int e = gm[i];
+        const double mv = m[e];
+        const double w = vols32[e];
+        if (mv > best) {
+            best = mv;
+            bi = i;
+        }
+        w_s += w;
+        const double ww = w * mv;
+        wm_s += ww;
+        cx += ww * bary[3 * static_cast<long>(e)];
+        cy += ww * bary[3 * static_cast<long>(e) + 1];
+        cz += ww * bary[3 * static_cast<long>(e) + 2];
+    }
+    sv[threadIdx.x] = best;
+    si[threadIdx.x] = bi;
+    sw[threadIdx.x] = w_s;
+    swm[threadIdx.x] = wm_s;
+    sx[threadIdx.x] = cx;
+    sy[threadIdx.x] = cy;
+    sz[threadIdx.x] = cz;
+    __syncthreads();
+    for (int off = kT / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) {
+            const int o = threadIdx.x + off;
+            if (sv[o] > sv[threadIdx.x] || (sv[o] == sv[threadIdx.x] && si[o] < si[threadIdx.x])) {
+                sv[threadIdx.x] = sv[o];
+                si[threadIdx.x] = si[o];
+            }
+            sw[threadIdx.x] += sw[o];
+            swm[threadIdx.x] += swm[o];
+            sx[threadIdx.x] += sx[o];
+            sy[threadIdx.x] += sy[o];
+            sz[threadIdx.x] += sz[o];
+        }
+        __syncthreads();
+    }
+    double* o = out + static_cast<long>(c) * kSummaryLen;
+    if (threadIdx.x == 0) {
+        const int e = gm[si[0]];
+        o[0] = sv[0];
+        o[1] = bary[3 * static_cast<long>(e)];
+        o[2] = bary[3 * static_cast<long>(e) + 1];
+        o[3] = bary[3 * static_cast<long>(e) + 2];
+        o[4] = sx[0] / swm[0];
+        o[5] = sy[0] / swm[0];
+        o[6] = sz[0] / swm[0];
+        o[7] = sw[0];
+        mean_sh = swm[0] / sw[0];
+        o[8] = mean_sh;
+    }
+    __syncthreads();
+    const double mean = mean_sh;
+    const double wtot = sw[0];
+    __syncthreads();
+    double var = 0.0;
+    for (int i = threadIdx.x; i < n_gm; i += kT) {
+        const int e = gm[i];
+        const double d = static_cast<double>(m[e]) - mean;
+        var += static_cast<double>(vols32[e]) * d * d;
+    }
+    sv[threadIdx.x] = var;
+    __syncthreads();
+    for (int off = kT / 2; off > 0; off >>= 1) {
+        if (threadIdx.x < off) sv[threadIdx.x] += sv[threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        o[9] = sqrt(sv[0] / wtot);
+        const long base = static_cast<long>(c) * n_gm;
+        const float* v = sorted_keys + base;
+        const double* w = w_sorted + base;
+        const double* cwp = cw + base;
+        const double qs[4] = {static_cast<double>(0.5f), static_cast<double>(0.95f), static_cast<double>(0.99f),
+                              static_cast<double>(0.999f)};
+        for (int j = 0; j < 4; ++j) o[10 + j] = quantile(qs[j], v, w, cwp, n_gm);
+        const double fr[2] = {0.5, 0.75};
+        for (int f = 0; f < 2; ++f) {
+            const double thr = fr[f] * o[13];
+            // First sorted slot with |E| >= thr; everything from there on is stimulated.
+            int lo = 0, hi = n_gm;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (static_cast<double>(v[mid]) >= thr) hi = mid;
+                else lo = mid + 1;
+            }
+            o[14 + f] = (lo == 0) ? cwp[n_gm - 1] : (cwp[n_gm - 1] - cwp[lo - 1]);
+        }
+    }
+}
+
+__global__ void nan_fill_kernel(double* out, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = NAN;
+}
+
+}  // namespace
+
+void reconstruct_block(const Mesh& m, const double* x_red, int k, int K, const float* elm, float* E, float* magnE,
+                       cudaStream_t s) {
+    const long total = static_cast<long>(m.n_tets) * k;
+    reconstruct_kernel<<<grid_for(total), kBlock, 0, s>>>(x_red, K, m.ground, m.tets.get(), m.g32.get(), elm, m.n_tets,
+                                                          k, E, magnE); count_launch();
+    CUNIBS_LAUNCH_CHECK("reconstruct");
+}
+
+void scatter_potential(const Mesh& m, const double* x_red, int k, int K, double* v, cudaStream_t s) {
+    const long total = static_cast<long>(m.n_nodes) * k;
+    scatter_kernel<<<grid_for(total), kBlock, 0, s>>>(x_red, K, m.ground, m.n_nodes, k, v); count_launch();
+    CUNIBS_LAUNCH_CHECK("scatter potential");
+}
+
+void gm_summary_impl(const Mesh& m, const float* magnE, int k, double* out, SummaryWork& w, cudaStream_t s) {
+    const int n = m.n_gm;
+    if (n == 0) {
+        nan_fill_kernel<<<grid_for(k * kSummaryLen), kBlock, 0, s>>>(out, k * kSummaryLen); count_launch();
+        return;
+    }
+    const long total = static_cast<long>(n) * k;
+    w.keys.reserve(total);
+    w.keys_s.reserve(total);
+    w.vals.reserve(total);
+    w.vals_s.reserve(total);
+    w.offsets.reserve(k + 1);
+    w.w_sorted.reserve(total);
+    w.cw.reserve(total);
+    const int tiles = (n + kScanTile - 1) / kScanTile;
+    w.tile_tot.reserve(static_cast<std::size_t>(tiles) * k);
+    gm_gather_kernel<<<grid_for(std::max<long>(total, k + 1)), kBlock, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, k,
+                                                                            w.keys.get(), w.vals.get(), w.offsets.get()); count_launch();
+    std::size_t bytes = 0;
+    CUNIBS_CHECK(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, bytes, w.keys.get(), w.keys_s.get(), w.vals.get(),
+                                                         w.vals_s.get(), static_cast<int>(total), k, w.offsets.get(),
+                                                         w.offsets.get() + 1, 0, 32, s));
+    w.temp.reserve(bytes ? bytes : 1);
+    CUNIBS_CHECK(cub::DeviceSegmentedRadixSort::SortPairs(w.temp.get(), bytes, w.keys.get(), w.keys_s.get(),
+                                                         w.vals.get(), w.vals_s.get(), static_cast<int>(total), k,
+                                                         w.offsets.get(), w.offsets.get() + 1, 0, 32, s));
+    tile_scan_kernel<<<dim3(tiles, k), 128, 0, s>>>(w.vals_s.get(), m.gm_index.get(), m.vols32.get(), n,
+                                                   w.w_sorted.get(), w.cw.get(), w.tile_tot.get()); count_launch();
+    tile_offset_kernel<<<dim3(tiles, k), 256, 0, s>>>(w.cw.get(), w.tile_tot.get(), n, tiles); count_launch();
+    summary_kernel<<<k, 512, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, m.vols32.get(), m.bary.get(),
+                                     w.keys_s.get(), w.w_sorted.get(), w.cw.get(), out); count_launch();
+    CUNIBS_LAUNCH_CHECK("gm summary");
+}
+
+void gm_summary(const Mesh& m, const float* magnE, int k, double* summary_dev, SummaryWork& w, cudaStream_t s) {
+    gm_summary_impl(m, magnE, k, summary_dev, w, s);
+}
+
+}  // namespace cunibs

@@ -1,0 +1,842 @@
+// Block PCG with a smoothed-aggregation V-cycle, for k right-hand sides in lockstep.
+//
+// Two precisions share one set of kernels, templated on the arithmetic type T:
+//   * plain: FP64 PCG over an FP64 V-cycle (the baseline method).
+//   * mixed: FP64 iterative refinement. Each outer step forms the true residual B - A X in FP64,
+//     then an inner PCG in FP32 (FP32 matrix values, FP32 vectors, FP32 V-cycle; FP64 inner
+//     products) reduces it by `inner_reduction`, and X += correction in FP64.
+//
+// Layout: every dense operand is row-major (n, K), so a mesh node's K values are contiguous. Every
+// row-parallel kernel runs on tiles of kTileRows rows with K lanes per row (lane = column): a lane
+// walks its row's nonzeros in CSR order, so each column's sum has the same order whatever K is.
+// Column reductions are two-stage and fixed-order (rows of a tile sequentially, then tiles in a
+// fixed tree by the grid's last block), so a placement's answer is bitwise independent of the block
+// width and of the other placements in its block. A column that meets its tolerance freezes
+// (alpha = beta = 0) on the device, which keeps the iteration body identical from launch to launch
+// and lets it replay as a CUDA graph with the convergence test read back only every few iterations.
+//
+// Reference semantics restated: solver.cpp:84-198 (lockstep k-RHS PCG, per-column freeze,
+// ||r||/||b|| <= tol), block_cg.cu:188-226 (freeze via alpha = beta = 0), vcycle.cu:560-648
+// (cycle order: Chebyshev pre-smooth from zero, residual, restrict; dense coarse solve; prolongate,
+// Chebyshev post-smooth).
+#include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+
+#include "internal.hpp"
+
+namespace cunibs {
+namespace {
+
+constexpr int kTileRows = 64;
+
+template <int K>
+constexpr int tile_threads() {
+    return kTileRows * K;
+}
+
+int n_tiles(int n) { return (n + kTileRows - 1) / kTileRows; }
+
+// --- deterministic column reductions ---------------------------------------------------------
+
+// Writes this block's per-column partial (rows of the tile summed in order) to partials[c][tile].
+template <int K>
+__device__ __forceinline__ void tile_partial(double v, double* __restrict__ partials, int tiles) {
+    __shared__ double sh[kTileRows][K];
+    const int slot = threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    sh[slot][c] = v;
+    __syncthreads();
+    if (threadIdx.x < K) {
+        double s = 0.0;
+#pragma unroll 8
+        for (int r = 0; r < kTileRows; ++r) s += sh[r][threadIdx.x];
+        partials[static_cast<long>(threadIdx.x) * tiles + blockIdx.x] = s;
+        __threadfence();
+    }
+}
+
+// True in the last block to finish; that block then owns the final reduction. It resets the
+// arrival counter, which no other block touches again in this launch.
+__device__ __forceinline__ bool last_block(unsigned* counter) {
+    __shared__ bool is_last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned prev = atomicAdd(counter, 1u);
+        is_last = (prev == gridDim.x - 1);
+        if (is_last) *counter = 0u;
+    }
+    __syncthreads();
+    return is_last;
+}
+
+// In the last block: total[c] = fixed tree over kTileRows strided sums of the tile partials.
+template <int K>
+__device__ __forceinline__ void final_reduce(const double* __restrict__ partials, int tiles, double* total) {
+    __shared__ double sh[kTileRows][K];
+    const int slot = threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double acc = 0.0;
+    for (int t = slot; t < tiles; t += kTileRows) acc += __ldcg(partials + static_cast<long>(c) * tiles + t);
+    sh[slot][c] = acc;
+    __syncthreads();
+#pragma unroll
+    for (int off = kTileRows / 2; off > 0; off >>= 1) {
+        if (slot < off) sh[slot][c] += sh[slot + off][c];
+        __syncthreads();
+    }
+    if (threadIdx.x < K) total[threadIdx.x] = sh[0][threadIdx.x];
+    __syncthreads();
+}
+
+template <typename T>
+__device__ __forceinline__ T row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
+                                     const T* __restrict__ val, const T* __restrict__ x, int row, int c, int K) {
+    T s = T(0);
+    const int e = ptr[row + 1];
+    for (int p = ptr[row]; p < e; ++p) s += val[p] * x[static_cast<long>(col[p]) * K + c];
+    return s;
+}
+
+// --- V-cycle kernels ---------------------------------------------------------------------
+
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) jz_kernel(int n, const T* __restrict__ dinv, const T* __restrict__ b,
+                                                               T alpha0, T* __restrict__ x) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row < n) x[static_cast<long>(row) * K + c] = alpha0 * dinv[row] * b[static_cast<long>(row) * K + c];
+}
+
+// out = c_cur*x_cur + c_prev*x_prev + alpha*dinv*(b - A x_cur). out may alias x_prev (read only
+// at this row), never x_cur.
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) cheby_kernel(int n, const int* __restrict__ ptr,
+                                                                  const int* __restrict__ col, const T* __restrict__ val,
+                                                                  const T* __restrict__ dinv, const T* __restrict__ b,
+                                                                  const T* __restrict__ x_cur, const T* x_prev, T c_cur,
+                                                                  T c_prev, T alpha, T* out) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= n) return;
+    const T s = row_dot<T>(ptr, col, val, x_cur, row, c, K);
+    const long q = static_cast<long>(row) * K + c;
+    const T cur = x_cur[q];
+    const T prev = x_prev[q];
+    const T rhs = b[q];
+    out[q] = c_cur * cur + c_prev * prev + alpha * dinv[row] * (rhs - s);
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) residual_kernel(int n, const int* __restrict__ ptr,
+                                                                     const int* __restrict__ col,
+                                                                     const T* __restrict__ val, const T* __restrict__ x,
+                                                                     const T* __restrict__ b, T* __restrict__ r) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= n) return;
+    const long q = static_cast<long>(row) * K + c;
+    r[q] = b[q] - row_dot<T>(ptr, col, val, x, row, c, K);
+}
+
+// b_c = R r_f; with dinv_c given, also the coarse level's first smoothing step x_c = alpha0*dinv*b_c.
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) restrict_kernel(int nc, const int* __restrict__ ptr,
+                                                                     const int* __restrict__ col,
+                                                                     const T* __restrict__ val, const T* __restrict__ rf,
+                                                                     T* __restrict__ bc, const T* __restrict__ dinv_c,
+                                                                     T alpha0, T* __restrict__ xc) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= nc) return;
+    const T s = row_dot<T>(ptr, col, val, rf, row, c, K);
+    const long q = static_cast<long>(row) * K + c;
+    bc[q] = s;
+    if (dinv_c != nullptr) xc[q] = alpha0 * dinv_c[row] * s;
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) prolong_kernel(int n, const int* __restrict__ ptr,
+                                                                    const int* __restrict__ col,
+                                                                    const T* __restrict__ val, const T* __restrict__ xc,
+                                                                    T* __restrict__ xf) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= n) return;
+    xf[static_cast<long>(row) * K + c] += row_dot<T>(ptr, col, val, xc, row, c, K);
+}
+
+// x = Ainv b for the dense coarsest operator: a warp per row, lanes striding the row, a fixed
+// shuffle tree per column.
+template <typename T, int K>
+__global__ void coarse_gemv_kernel(int nc, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
+    const int lane = threadIdx.x % kWarp;
+    T acc[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = T(0);
+    if (row < nc) {
+        for (int j = lane; j < nc; j += kWarp) {
+            const T a = inv[static_cast<long>(row) * nc + j];
+#pragma unroll
+            for (int c = 0; c < K; ++c) acc[c] += a * b[static_cast<long>(j) * K + c];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < K; ++c) acc[c] = group_sum<kWarp>(acc[c]);
+    if (row < nc && lane == 0) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) x[static_cast<long>(row) * K + c] = acc[c];
+    }
+}
+
+// --- PCG kernels -------------------------------------------------------------------------
+
+// ||x_c||^2 per column into out[c].
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) norm2_kernel(int n, const T* __restrict__ x, double* partials,
+                                                                  unsigned* counter, double* __restrict__ out) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double v = 0.0;
+    if (row < n) {
+        const double xv = static_cast<double>(x[static_cast<long>(row) * K + c]);
+        v = xv * xv;
+    }
+    tile_partial<K>(v, partials, gridDim.x);
+    if (last_block(counter)) {
+        __shared__ double tot[K];
+        final_reduce<K>(partials, gridDim.x, tot);
+        if (threadIdx.x < K) out[threadIdx.x] = tot[threadIdx.x];
+    }
+}
+
+// Ap = A p; pAp per column; alpha = rz / pAp (0 on a frozen column).
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
+    int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
+    const T* __restrict__ p, T* __restrict__ ap, double* partials, unsigned* counter, const double* __restrict__ rz,
+    const int* __restrict__ frozen, double* __restrict__ alpha) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double v = 0.0;
+    if (row < n) {
+        const T s = row_dot<T>(ptr, col, val, p, row, c, K);
+        const long q = static_cast<long>(row) * K + c;
+        ap[q] = s;
+        v = static_cast<double>(p[q]) * static_cast<double>(s);
+    }
+    tile_partial<K>(v, partials, gridDim.x);
+    if (last_block(counter)) {
+        __shared__ double tot[K];
+        final_reduce<K>(partials, gridDim.x, tot);
+        if (threadIdx.x < K) {
+            const int cc = threadIdx.x;
+            alpha[cc] = frozen[cc] ? 0.0 : rz[cc] / tot[cc];
+        }
+    }
+}
+
+// x += alpha p; r -= alpha Ap; rr = ||r||^2. A column freezes when sqrt(rr) <= tol*sqrt(ref[c]);
+// the iteration it froze at and its relative residual are recorded on the device.
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
+    int n, const double* __restrict__ alpha, const T* __restrict__ p, const T* __restrict__ ap, T* __restrict__ x,
+    T* __restrict__ r, double* partials, unsigned* counter, const double* __restrict__ ref, double tol,
+    int* __restrict__ frozen, int* __restrict__ iter_counter, int* __restrict__ conv_iter, double* __restrict__ rel_out,
+    int record) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double v = 0.0;
+    if (row < n) {
+        const long q = static_cast<long>(row) * K + c;
+        const T a = static_cast<T>(alpha[c]);
+        x[q] += a * p[q];
+        const T rn = r[q] - a * ap[q];
+        r[q] = rn;
+        v = static_cast<double>(rn) * static_cast<double>(rn);
+    }
+    tile_partial<K>(v, partials, gridDim.x);
+    if (last_block(counter)) {
+        __shared__ double tot[K];
+        final_reduce<K>(partials, gridDim.x, tot);
+        const int it = *iter_counter + 1;
+        if (threadIdx.x < K) {
+            const int cc = threadIdx.x;
+            const double rel = sqrt(tot[cc]) / sqrt(ref[cc]);
+            if (!frozen[cc]) {
+                if (record) rel_out[cc] = rel;
+                if (rel <= tol) {
+                    frozen[cc] = 1;
+                    if (record) conv_iter[cc] = it;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) *iter_counter = it;
+    }
+}
+
+// rz_new = r . z; beta = rz_new / rz (0 on a frozen column); rz = rz_new.
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) dot_beta_kernel(int n, const T* __restrict__ r,
+                                                                     const T* __restrict__ z, double* partials,
+                                                                     unsigned* counter, double* __restrict__ rz,
+                                                                     const int* __restrict__ frozen,
+                                                                     double* __restrict__ beta) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double v = 0.0;
+    if (row < n) {
+        const long q = static_cast<long>(row) * K + c;
+        v = static_cast<double>(r[q]) * static_cast<double>(z[q]);
+    }
+    tile_partial<K>(v, partials, gridDim.x);
+    if (last_block(counter)) {
+        __shared__ double tot[K];
+        final_reduce<K>(partials, gridDim.x, tot);
+        if (threadIdx.x < K) {
+            const int cc = threadIdx.x;
+            beta[cc] = frozen[cc] ? 0.0 : tot[cc] / rz[cc];
+            rz[cc] = tot[cc];
+        }
+    }
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) update_p_kernel(int n, const double* __restrict__ beta,
+                                                                     const T* __restrict__ z, T* __restrict__ p) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= n) return;
+    const long q = static_cast<long>(row) * K + c;
+    p[q] = z[q] + static_cast<T>(beta[c]) * p[q];
+}
+
+// Mixed refinement outer step: R = B - A X in FP64; r32 = (float)R; per column the true relative
+// residual, the outer freeze, and the inner solve's reference norm and starting freeze.
+template <int K>
+__global__ void __launch_bounds__(tile_threads<K>()) true_residual_kernel(
+    int n, const int* __restrict__ ptr, const int* __restrict__ col, const double* __restrict__ val,
+    const double* __restrict__ B, const double* __restrict__ X, float* __restrict__ r32, double* partials,
+    unsigned* counter, const double* __restrict__ ref_sq, double tol, int* __restrict__ outer_conv,
+    int* __restrict__ inner_frozen, double* __restrict__ rr0, const int* __restrict__ iter_counter,
+    int* __restrict__ conv_iter, double* __restrict__ rel_out) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double v = 0.0;
+    if (row < n) {
+        const long q = static_cast<long>(row) * K + c;
+        const double rv = B[q] - row_dot<double>(ptr, col, val, X, row, c, K);
+        const float rf = static_cast<float>(rv);
+        r32[q] = rf;
+        v = static_cast<double>(rf) * static_cast<double>(rf);
+    }
+    tile_partial<K>(v, partials, gridDim.x);
+    if (last_block(counter)) {
+        __shared__ double tot[K];
+        final_reduce<K>(partials, gridDim.x, tot);
+        if (threadIdx.x < K) {
+            const int cc = threadIdx.x;
+            const double rel = sqrt(tot[cc]) / sqrt(ref_sq[cc]);
+            if (!outer_conv[cc]) {
+                rel_out[cc] = rel;
+                if (rel <= tol) {
+                    outer_conv[cc] = 1;
+                    conv_iter[cc] = *iter_counter;
+                }
+            }
+            inner_frozen[cc] = outer_conv[cc];
+            rr0[cc] = tot[cc];
+        }
+    }
+}
+
+// FP64 residual R = B - A X for a warm start of the plain solve.
+template <int K>
+__global__ void __launch_bounds__(tile_threads<K>()) residual64_kernel(int n, const int* __restrict__ ptr,
+                                                                       const int* __restrict__ col,
+                                                                       const double* __restrict__ val,
+                                                                       const double* __restrict__ B,
+                                                                       const double* __restrict__ X,
+                                                                       double* __restrict__ R) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= n) return;
+    const long q = static_cast<long>(row) * K + c;
+    R[q] = B[q] - row_dot<double>(ptr, col, val, X, row, c, K);
+}
+
+template <int K>
+__global__ void __launch_bounds__(tile_threads<K>()) add_correction_kernel(int n, double* __restrict__ X,
+                                                                           const float* __restrict__ d) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (row >= n) return;
+    const long q = static_cast<long>(row) * K + c;
+    X[q] += static_cast<double>(d[q]);
+}
+
+}  // namespace
+
+// Per-precision V-cycle workspace.
+template <typename T>
+struct VWork {
+    std::vector<DevArray<T>> x, r, b;
+    DevArray<T> cb, cx;
+};
+
+class Solver {
+  public:
+    const Hierarchy* h = nullptr;
+    int n = 0;
+    int kcap = 0;
+    cudaStream_t stream = nullptr;
+    // FP64 CG / outer workspace (n, kcap)
+    DevArray<double> B, X, R, P, AP, Z;
+    // FP32 inner workspace
+    DevArray<float> d32, r32, p32, ap32, z32;
+    VWork<float> v32;
+    VWork<double> v64;
+    // Per-column scalars.
+    DevArray<double> rz, alpha, beta, ref_sq, rr0, rel, partials;
+    DevArray<int> frozen, outer_conv, conv_iter, iter_counter;
+    DevArray<unsigned> counter;
+    int* h_flags = nullptr;   // pinned
+    double* h_dbl = nullptr;  // pinned
+    std::map<std::tuple<int, int, int>, std::pair<cudaGraphExec_t, long long>> graphs;
+
+    ~Solver() {
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.first);
+        if (h_flags) cudaFreeHost(h_flags);
+        if (h_dbl) cudaFreeHost(h_dbl);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void ensure(int K) {
+        if (kcap >= K) return;
+        for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.first);
+        graphs.clear();
+        const std::size_t nk = static_cast<std::size_t>(n) * K;
+        for (auto* a : {&B, &X, &R, &P, &AP, &Z}) a->resize(nk);
+        for (auto* a : {&d32, &r32, &p32, &ap32, &z32}) a->resize(nk);
+        const std::size_t L = h->levels.size();
+        v32.x.resize(L);
+        v32.r.resize(L);
+        v32.b.resize(L);
+        v64.x.resize(L);
+        v64.r.resize(L);
+        v64.b.resize(L);
+        for (std::size_t l = 0; l < L; ++l) {
+            const std::size_t m = static_cast<std::size_t>(h->levels[l].n) * K;
+            v32.x[l].resize(m);
+            v32.r[l].resize(m);
+            v64.x[l].resize(m);
+            v64.r[l].resize(m);
+            if (l > 0) {
+                v32.b[l].resize(m);
+                v64.b[l].resize(m);
+            }
+        }
+        const std::size_t mc = static_cast<std::size_t>(h->nc) * K;
+        v32.cb.resize(mc);
+        v32.cx.resize(mc);
+        v64.cb.resize(mc);
+        v64.cx.resize(mc);
+        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel}) a->resize(K);
+        for (auto* a : {&frozen, &outer_conv, &conv_iter}) a->resize(K);
+        iter_counter.resize(1);
+        counter.resize(1);
+        counter.zero(stream);
+        partials.resize(static_cast<std::size_t>(n_tiles(n)) * K);
+        if (h_flags) cudaFreeHost(h_flags);
+        if (h_dbl) cudaFreeHost(h_dbl);
+        CUNIBS_CHECK(cudaMallocHost(&h_flags, sizeof(int) * 4 * K));
+        CUNIBS_CHECK(cudaMallocHost(&h_dbl, sizeof(double) * 4 * K));
+        kcap = K;
+        CUNIBS_CHECK(cudaStreamSynchronize(stream));
+    }
+
+    // Level accessors per precision.
+    template <typename T>
+    const T* lval(int l) const;
+    template <typename T>
+    const T* ldinv(int l) const;
+    template <typename T>
+    const T* pval(int l) const;
+    template <typename T>
+    const T* rval(int l) const;
+    template <typename T>
+    const T* cinv() const;
+    template <typename T>
+    VWork<T>& vw();
+
+    template <typename T, int K>
+    void vcycle(const T* b, T* z);
+    template <typename T, int K>
+    void pcg_tail(T* r, T* z, T* p);
+    template <typename T, int K>
+    void pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
+                       const double* ref, int record);
+    template <int K>
+    void solve_plain(int k, const Params& prm, SolveStats& st, bool warm);
+    template <int K>
+    void solve_mixed(int k, const Params& prm, SolveStats& st);
+
+    template <typename Body>
+    void run_graph(std::tuple<int, int, int> key, Body&& body) {
+        auto it = graphs.find(key);
+        if (it == graphs.end()) {
+            cudaGraph_t g = nullptr;
+            // Captured launches do not execute; the replays below count the graph's kernels.
+            const long long before = launch_counter().load();
+            CUNIBS_CHECK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+            body();
+            const cudaError_t end = cudaStreamEndCapture(stream, &g);
+            launch_counter().store(before);
+            if (end != cudaSuccess || g == nullptr) {
+                if (g) cudaGraphDestroy(g);
+                (void)cudaGetLastError();
+                body();  // capture failed: run eagerly
+                return;
+            }
+            std::size_t n_nodes = 0;
+            CUNIBS_CHECK(cudaGraphGetNodes(g, nullptr, &n_nodes));
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t inst = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (inst != cudaSuccess) {
+                (void)cudaGetLastError();
+                body();
+                return;
+            }
+            it = graphs.emplace(key, std::make_pair(ex, static_cast<long long>(n_nodes))).first;
+        }
+        CUNIBS_CHECK(cudaGraphLaunch(it->second.first, stream));
+        count_launch(it->second.second);
+    }
+};
+
+template <>
+const float* Solver::lval<float>(int l) const { return h->levels[l].a32.get(); }
+template <>
+const double* Solver::lval<double>(int l) const { return h->levels[l].a.val.get(); }
+template <>
+const float* Solver::ldinv<float>(int l) const { return h->levels[l].dinv32.get(); }
+template <>
+const double* Solver::ldinv<double>(int l) const { return h->levels[l].dinv.get(); }
+template <>
+const float* Solver::pval<float>(int l) const { return h->levels[l].p32.get(); }
+template <>
+const double* Solver::pval<double>(int l) const { return h->levels[l].p.val.get(); }
+template <>
+const float* Solver::rval<float>(int l) const { return h->levels[l].r32.get(); }
+template <>
+const double* Solver::rval<double>(int l) const { return h->levels[l].r.val.get(); }
+template <>
+const float* Solver::cinv<float>() const { return h->coarse_inv32.get(); }
+template <>
+const double* Solver::cinv<double>() const { return h->coarse_inv.get(); }
+template <>
+VWork<float>& Solver::vw<float>() { return v32; }
+template <>
+VWork<double>& Solver::vw<double>() { return v64; }
+
+template <typename T, int K>
+void Solver::vcycle(const T* b, T* z) {
+    const Hierarchy& H = *h;
+    const Cheby& ch = H.cheby;
+    const int L = static_cast<int>(H.levels.size());
+    VWork<T>& w = vw<T>();
+    constexpr int TT = tile_threads<K>();
+    cudaStream_t s = stream;
+    if (L == 0) {
+        coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(), b, z); count_launch();
+        return;
+    }
+    const int deg = ch.degree;
+    const bool odd = (deg % 2) != 0;
+    // One Chebyshev sweep of `deg` steps (vcycle.cu:585-617 buffer discipline). x0 == nullptr is a
+    // zero initial guess whose first step, x = alpha0*dinv*b, the caller has already written into
+    // `first`. Otherwise step 0 reads x0 and writes `first`; later steps alternate, writing over
+    // the buffer that holds x_{i-1}, which the step kernel reads only at the row it writes.
+    auto sweep = [&](int l, const T* bi, T* x0, T* first, T* other, T* final_out) {
+        const Level& lv = H.levels[l];
+        const unsigned g = n_tiles(lv.n);
+        auto target = [&](int st) -> T* {
+            if (st + 1 == deg && final_out) return final_out;
+            return (st % 2) ? other : first;
+        };
+        T* cur;
+        T* prev;
+        if (x0 == nullptr) {
+            cur = first;
+            prev = first;
+        } else {
+            T* out = target(0);
+            cheby_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, x0,
+                                               x0, T(1), T(0), static_cast<T>(ch.alpha0), out); count_launch();
+            prev = x0;
+            cur = out;
+        }
+        for (int st = 1; st < deg; ++st) {
+            T* out = target(st);
+            const T cp = (st == 1 && x0 == nullptr) ? T(0) : static_cast<T>(ch.c_prev[st - 1]);
+            cheby_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur,
+                                               prev, static_cast<T>(ch.c_cur[st - 1]), cp,
+                                               static_cast<T>(ch.alpha[st - 1]), out); count_launch();
+            prev = cur;
+            cur = out;
+        }
+        return cur;
+    };
+    // Down-sweep.
+    for (int l = 0; l < L; ++l) {
+        const Level& lv = H.levels[l];
+        const T* bi = (l == 0) ? b : w.b[l].get();
+        T* first = odd ? w.x[l].get() : w.r[l].get();
+        T* other = odd ? w.r[l].get() : w.x[l].get();
+        const unsigned g = n_tiles(lv.n);
+        if (l == 0) {
+            jz_kernel<T, K><<<g, TT, 0, s>>>(lv.n, ldinv<T>(0), bi, static_cast<T>(ch.alpha0), first);
+            count_launch();
+        }
+        sweep(l, bi, nullptr, first, other, nullptr);
+        residual_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi,
+                                               w.r[l].get()); count_launch();
+        const bool next_is_level = (l + 1 < L);
+        T* nb = next_is_level ? w.b[l + 1].get() : w.cb.get();
+        T* nx = nullptr;
+        const T* nd = nullptr;
+        if (next_is_level) {
+            const bool nodd = odd;
+            nx = nodd ? w.x[l + 1].get() : w.r[l + 1].get();
+            nd = ldinv<T>(l + 1);
+        }
+        restrict_kernel<T, K><<<n_tiles(lv.n_coarse), TT, 0, s>>>(lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(),
+                                                                  rval<T>(l), w.r[l].get(), nb, nd,
+                                                                  static_cast<T>(ch.alpha0), nx); count_launch();
+    }
+    coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(),
+                                                                                                 w.cb.get(), w.cx.get()); count_launch();
+    // Up-sweep.
+    const T* xc = w.cx.get();
+    for (int l = L - 1; l >= 0; --l) {
+        const Level& lv = H.levels[l];
+        const T* bi = (l == 0) ? b : w.b[l].get();
+        const unsigned g = n_tiles(lv.n);
+        prolong_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get()); count_launch();
+        // The level's smoothed correction stays wherever its sweep left it; the next finer
+        // prolongation reads it from there.
+        xc = sweep(l, bi, w.x[l].get(), w.r[l].get(), w.x[l].get(), (l == 0) ? z : nullptr);
+    }
+}
+
+template <typename T, int K>
+void Solver::pcg_tail(T* r, T* z, T* p) {
+    constexpr int TT = tile_threads<K>();
+    const unsigned g = n_tiles(n);
+    vcycle<T, K>(r, z);
+    dot_beta_kernel<T, K><<<g, TT, 0, stream>>>(n, r, z, partials.get(), counter.get(), rz.get(), frozen.get(), beta.get()); count_launch();
+    update_p_kernel<T, K><<<g, TT, 0, stream>>>(n, beta.get(), z, p); count_launch();
+}
+
+template <typename T, int K>
+void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
+                           const double* ref, int record) {
+    constexpr int TT = tile_threads<K>();
+    const unsigned g = n_tiles(n);
+    spmv_alpha_kernel<T, K><<<g, TT, 0, stream>>>(n, ptr, col, val, p, ap, partials.get(), counter.get(), rz.get(),
+                                                  frozen.get(), alpha.get()); count_launch();
+    update_xr_kernel<T, K><<<g, TT, 0, stream>>>(n, alpha.get(), p, ap, x, r, partials.get(), counter.get(), ref, tol,
+                                                 frozen.get(), iter_counter.get(), conv_iter.get(), rel.get(), record); count_launch();
+    pcg_tail<T, K>(r, z, p);
+}
+
+template <int K>
+void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
+    constexpr int TT = tile_threads<K>();
+    const unsigned g = n_tiles(n);
+    cudaStream_t s = stream;
+    const DevCsr<double>& A = h->levels.empty() ? h->coarse : h->levels[0].a;
+    const std::size_t nk = static_cast<std::size_t>(n) * K;
+    norm2_kernel<double, K><<<g, TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
+    if (warm) {
+        residual64_kernel<K><<<g, TT, 0, s>>>(n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), R.get()); count_launch();
+    } else {
+        X.zero(s);
+        CUNIBS_CHECK(cudaMemcpyAsync(R.get(), B.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    frozen.zero(s);
+    iter_counter.zero(s);
+    P.zero(s);
+    CUNIBS_CHECK(cudaMemcpyAsync(h_dbl, ref_sq.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    for (int c = 0; c < k; ++c)
+        if (!(h_dbl[c] > 0.0)) fail(kEInval, "zero right-hand side column " + std::to_string(c));
+    std::vector<int> init_iters(K, prm.max_iters);
+    CUNIBS_CHECK(cudaMemcpyAsync(conv_iter.get(), init_iters.data(), sizeof(int) * K, cudaMemcpyHostToDevice, s));
+    rel.zero(s);
+    pcg_tail<double, K>(R.get(), Z.get(), P.get());
+    int it = 0;
+    while (it < prm.max_iters) {
+        const int m = std::min(prm.iters_per_sync, prm.max_iters - it);
+        for (int j = 0; j < m; ++j) {
+            run_graph({0, K, 0}, [&] {
+                pcg_iteration<double, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(),
+                                         Z.get(), prm.tolerance, ref_sq.get(), 1);
+            });
+        }
+        it += m;
+        CUNIBS_CHECK(cudaMemcpyAsync(h_flags, frozen.get(), sizeof(int) * K, cudaMemcpyDeviceToHost, s));
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        bool all = true;
+        for (int c = 0; c < k; ++c) all = all && h_flags[c];
+        if (all) break;
+    }
+    st.iterations = it;
+    st.outer_steps = 1;
+}
+
+template <int K>
+void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
+    constexpr int TT = tile_threads<K>();
+    const unsigned g = n_tiles(n);
+    cudaStream_t s = stream;
+    const DevCsr<double>& A = h->levels.empty() ? h->coarse : h->levels[0].a;
+    const float* A32 = h->levels.empty() ? nullptr : h->levels[0].a32.get();
+    DevArray<float> coarse32;
+    if (A32 == nullptr) fail(kEInval, "mixed precision needs at least one AMG level");
+    norm2_kernel<double, K><<<g, TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
+    outer_conv.zero(s);
+    iter_counter.zero(s);
+    CUNIBS_CHECK(cudaMemcpyAsync(h_dbl, ref_sq.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    for (int c = 0; c < k; ++c)
+        if (!(h_dbl[c] > 0.0)) fail(kEInval, "zero right-hand side column " + std::to_string(c));
+    std::vector<int> init_iters(K, prm.max_iters);
+    CUNIBS_CHECK(cudaMemcpyAsync(conv_iter.get(), init_iters.data(), sizeof(int) * K, cudaMemcpyHostToDevice, s));
+    rel.zero(s);
+    int total_inner = 0;
+    int outer = 0;
+    const int max_outer = 64;
+    for (; outer < max_outer; ++outer) {
+        true_residual_kernel<K><<<g, TT, 0, s>>>(n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), r32.get(),
+                                                 partials.get(), counter.get(), ref_sq.get(), prm.tolerance,
+                                                 outer_conv.get(), frozen.get(), rr0.get(), iter_counter.get(),
+                                                 conv_iter.get(), rel.get()); count_launch();
+        CUNIBS_CHECK(cudaMemcpyAsync(h_flags, outer_conv.get(), sizeof(int) * K, cudaMemcpyDeviceToHost, s));
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        bool all = true;
+        for (int c = 0; c < k; ++c) all = all && h_flags[c];
+        if (all || total_inner >= prm.max_iters) break;
+        d32.zero(s);
+        p32.zero(s);
+        pcg_tail<float, K>(r32.get(), z32.get(), p32.get());
+        int it = 0;
+        const int cap = std::min(prm.inner_max_iters, prm.max_iters - total_inner);
+        while (it < cap) {
+            const int m = std::min(prm.iters_per_sync, cap - it);
+            for (int j = 0; j < m; ++j) {
+                run_graph({1, K, 0}, [&] {
+                    pcg_iteration<float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
+                                            z32.get(), prm.inner_reduction, rr0.get(), 0);
+                });
+            }
+            it += m;
+            CUNIBS_CHECK(cudaMemcpyAsync(h_flags, frozen.get(), sizeof(int) * K, cudaMemcpyDeviceToHost, s));
+            CUNIBS_CHECK(cudaStreamSynchronize(s));
+            bool done = true;
+            for (int c = 0; c < k; ++c) done = done && h_flags[c];
+            if (done) break;
+        }
+        total_inner += it;
+        add_correction_kernel<K><<<g, TT, 0, s>>>(n, X.get(), d32.get()); count_launch();
+    }
+    st.iterations = total_inner;
+    st.outer_steps = outer + 1;
+}
+
+void SolverDeleter::operator()(Solver* s) const { delete s; }
+
+SolverPtr make_solver(const Hierarchy& h, const Params& p) {
+    (void)p;
+    SolverPtr sv(new Solver());
+    sv->h = &h;
+    sv->n = h.levels.empty() ? h.nc : h.levels[0].n;
+    CUNIBS_CHECK(cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking));
+    return sv;
+}
+
+template <typename F>
+void dispatch_k(int K, F&& f) {
+    switch (K) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 16: f(std::integral_constant<int, 16>{}); break;
+        default: fail(kEInval, "block width must be one of {1, 2, 4, 8, 16}");
+    }
+}
+
+void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, const Params& prm, cudaStream_t s,
+                  SolveStats& st, const double* X0) {
+    if (k < 1 || k > K) fail(kEInval, "k must be in [1, block width]");
+    dispatch_k(K, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        sv.ensure(KK);
+        // Join the caller's stream.
+        cudaEvent_t ev;
+        CUNIBS_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CUNIBS_CHECK(cudaEventRecord(ev, s));
+        CUNIBS_CHECK(cudaStreamWaitEvent(sv.stream, ev, 0));
+        const std::size_t nk = static_cast<std::size_t>(sv.n) * KK;
+        CUNIBS_CHECK(cudaMemcpyAsync(sv.B.get(), Bin, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
+        if (X0) CUNIBS_CHECK(cudaMemcpyAsync(sv.X.get(), X0, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
+        else sv.X.zero(sv.stream);
+        if (prm.precision == kMixed) sv.solve_mixed<KK>(k, prm, st);
+        else sv.solve_plain<KK>(k, prm, st, X0 != nullptr);
+        CUNIBS_CHECK(cudaMemcpyAsync(Xout, sv.X.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
+        CUNIBS_CHECK(cudaMemcpyAsync(sv.h_flags, sv.conv_iter.get(), sizeof(int) * KK, cudaMemcpyDeviceToHost, sv.stream));
+        CUNIBS_CHECK(cudaMemcpyAsync(sv.h_dbl, sv.rel.get(), sizeof(double) * KK, cudaMemcpyDeviceToHost, sv.stream));
+        CUNIBS_CHECK(cudaEventRecord(ev, sv.stream));
+        CUNIBS_CHECK(cudaStreamWaitEvent(s, ev, 0));
+        CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
+        cudaEventDestroy(ev);
+        st.col_iters.assign(sv.h_flags, sv.h_flags + k);
+        st.col_rel.assign(sv.h_dbl, sv.h_dbl + k);
+    });
+}
+
+void solver_vcycle(Solver& sv, const double* r, double* z, int k, bool fp32, cudaStream_t s) {
+    (void)fp32;
+    dispatch_k(k, [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        sv.ensure(KK);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        const std::size_t nk = static_cast<std::size_t>(sv.n) * KK;
+        if (fp32) {
+            // r (FP64) -> FP32, cycle, back to FP64.
+            std::vector<double> hr(nk);
+            CUNIBS_CHECK(cudaMemcpy(hr.data(), r, nk * sizeof(double), cudaMemcpyDeviceToHost));
+            std::vector<float> hf(hr.begin(), hr.end());
+            CUNIBS_CHECK(cudaMemcpy(sv.r32.get(), hf.data(), nk * sizeof(float), cudaMemcpyHostToDevice));
+            sv.vcycle<float, KK>(sv.r32.get(), sv.z32.get());
+            CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
+            CUNIBS_CHECK(cudaMemcpy(hf.data(), sv.z32.get(), nk * sizeof(float), cudaMemcpyDeviceToHost));
+            std::vector<double> hz(hf.begin(), hf.end());
+            CUNIBS_CHECK(cudaMemcpy(z, hz.data(), nk * sizeof(double), cudaMemcpyHostToDevice));
+        } else {
+            CUNIBS_CHECK(cudaMemcpyAsync(sv.R.get(), r, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
+            sv.vcycle<double, KK>(sv.R.get(), sv.Z.get());
+            CUNIBS_CHECK(cudaMemcpyAsync(z, sv.Z.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
+            CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
+        }
+        CUNIBS_LAUNCH_CHECK("vcycle");
+    });
+}
+
+}  // namespace cunibs

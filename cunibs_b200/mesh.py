@@ -105,7 +105,10 @@ class _Reader:
         return text
 
     def expect(self, marker: str) -> None:
+        # A binary block may be followed by its own newline before the closing marker.
         found = self.line()
+        while found == "" and self.pos < len(self.data):
+            found = self.line()
         if found != marker:
             raise _fail(self.path, f"expected {marker}, found {found!r}")
 

@@ -41,3 +41,264 @@ class Placement:
         object.__setattr__(self, "center_mm", center)
         object.__setattr__(self, "handle_mm", handle)
         object.__setattr__(self, "distance_mm", distance)
+
+
+import threading  # noqa: E402
+from collections.abc import Iterator, Sequence  # noqa: E402
+from dataclasses import field  # noqa: E402
+from pathlib import Path  # noqa: E402
+from typing import Literal  # noqa: E402
+
+from . import _native, metrics  # noqa: E402
+from .coil import Coil  # noqa: E402
+from .fem import (  # noqa: E402
+    DEFAULT_MAX_ITERS,
+    DEFAULT_TOLERANCE,
+    MAX_BLOCK,
+    SolverConvergenceError,
+    validate_recovery,
+)
+from .mesh import HeadMesh, load_mesh  # noqa: E402
+
+_FORMAT_VERSION = 1
+Precision = Literal["mixed", "plain"]
+
+
+@dataclass(frozen=True)
+class _Retain:
+    magnitude: bool
+    vectors: bool
+    potential: bool
+    nodal: bool = False
+
+
+def _sites(placements, method: str) -> list[Placement]:
+    if isinstance(placements, Placement):
+        raise TypeError(f"{method}() takes a sequence of placements; wrap a single one in a list, or use simulate().")
+    sites = list(placements)
+    for s in sites:
+        if not isinstance(s, Placement):
+            raise TypeError(f"{method}() takes Placement objects, got {type(s).__name__}")
+    return sites
+
+
+class Subject:
+    """A head mesh and its reusable GPU solver state (reference simulation.py:169-546).
+
+    ``tolerance`` is the PCG stopping criterion ||r||/||b|| (the reference's DEFAULT_TOLERANCE is
+    1e-6). ``precision`` selects "mixed" (FP32 PCG and V-cycle inside FP64 refinement, the default)
+    or "plain" (FP64 throughout).
+    """
+
+    def __init__(self, mesh: HeadMesh, *, tolerance: float = DEFAULT_TOLERANCE, max_iters: int = DEFAULT_MAX_ITERS,
+                 precision: Precision = "mixed", device: int = 0) -> None:
+        if precision not in ("mixed", "plain"):
+            raise ValueError("precision must be 'mixed' or 'plain'")
+        self._mesh = mesh
+        self._ctx: _native.Context | None = None
+        self._ordered: HeadMesh | None = None
+        self._host_metrics: tuple[np.ndarray, np.ndarray, np.ndarray] | None = None
+        self._tolerance = float(tolerance)
+        self._max_iters = int(max_iters)
+        self._precision = precision
+        self._device = int(device)
+        self._lock = threading.RLock()
+
+    @classmethod
+    def from_mesh(cls, mesh_file: str | Path, **kwargs) -> Subject:
+        return cls(load_mesh(mesh_file), **kwargs)
+
+    def free(self) -> None:
+        """Release the device state; it is rebuilt lazily on the next call."""
+        with self._lock:
+            if self._ctx is not None:
+                self._ctx.close()
+            self._ctx = None
+            self._ordered = None
+            self._host_metrics = None
+
+    def __enter__(self) -> Subject:
+        return self
+
+    def __exit__(self, *exc: object) -> None:
+        self.free()
+
+    @property
+    def context(self) -> _native.Context:
+        with self._lock:
+            if self._ctx is None:
+                p = _native.default_params()
+                p.tolerance = self._tolerance
+                p.max_iters = self._max_iters
+                p.precision = _native.PREC_MIXED if self._precision == "mixed" else _native.PREC_PLAIN_FP64
+                p.device = self._device
+                m = self._mesh
+                self._ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris, p)
+            return self._ctx
+
+    @property
+    def mesh(self) -> HeadMesh:
+        """The mesh in the Morton order every result array is indexed by."""
+        with self._lock:
+            if self._ordered is None:
+                nodes, tets, tags, skin, _, _ = self.context.mesh()
+                self._ordered = HeadMesh(nodes, tets, tags, skin)
+            return self._ordered
+
+    def _host_metric_inputs(self) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        with self._lock:
+            if self._host_metrics is None:
+                ctx = self.context
+                vols = ctx.array("vols").astype(np.float32)
+                self._host_metrics = (vols, ctx.array("tet_tags"), ctx.array("bary").reshape(-1, 3))
+            return self._host_metrics
+
+    def _iter_reduced(self, coil: Coil, sites: Sequence[Placement], didt: float, block_k: int | None,
+                      retain: _Retain, recovery: str) -> Iterator[FieldResult]:
+        ctx = self.context
+        chunk_k = MAX_BLOCK if block_k is None else max(1, min(MAX_BLOCK, int(block_k)))
+        for start in range(0, len(sites), chunk_k):
+            chunk = sites[start : start + chunk_k]
+            centers = np.stack([s.center_mm for s in chunk])
+            handles = np.stack([s.handle_mm for s in chunk])
+            dists = np.array([s.distance_mm for s in chunk])
+            try:
+                out = ctx.solve_block(coil, centers, handles, dists, didt, magnitude=retain.magnitude,
+                                      vectors=retain.vectors, potential=retain.potential)
+            except _native.ConvergenceFailure as exc:
+                raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
+            host = self._host_metric_inputs() if retain.magnitude else None
+            for i, site in enumerate(chunk):
+                yield FieldResult(
+                    summary=metrics.from_summary_row(out["summary"][i]),
+                    magnE=out["magnE"][i] if retain.magnitude else None,
+                    E=out["E"][i] if retain.vectors else None,
+                    v=out["v"][i] if retain.potential else None,
+                    transform=out["transform"][i],
+                    placement=site,
+                    coil_name=coil.name,
+                    didt=float(didt),
+                    vols=host[0] if host else None,
+                    tet_tags=host[1] if host else None,
+                    barycenters_mm=host[2] if host else None,
+                    recovery=recovery,
+                    iterations=int(out["iterations"][i]),
+                    relative_residual=float(out["relative_residual"][i]),
+                )
+
+    def iter_simulate(self, coil: Coil, placements: Sequence[Placement], didt: float = 1e6, *,
+                      magnitude: bool = False, vectors: bool = False, potential: bool = False,
+                      nodal: bool = False, recovery: str = "raw", block_k: int | None = None) -> Iterator[FieldResult]:
+        """Stream one FieldResult per placement, in order, solving blocks of ``block_k`` together.
+
+        A placement's result does not depend on ``block_k`` or on which placements share its
+        block. Arguments are validated here, before the first result is requested.
+        """
+        sites = _sites(placements, "iter_simulate")
+        recovery = validate_recovery(recovery)
+        if nodal:
+            raise ValueError("nodal=True needs a recovered nodal field, which this build does not produce yet")
+        if recovery != "raw":
+            raise ValueError(f"recovery={recovery!r} is not available in this build; use recovery='raw'")
+        if not isinstance(coil, Coil):
+            raise TypeError("coil must be a cunibs_b200.Coil")
+        retain = _Retain(bool(magnitude), bool(vectors), bool(potential), bool(nodal))
+        return self._iter_reduced(coil, sites, float(didt), block_k, retain, recovery)
+
+    def simulate(self, coil: Coil, placement: Placement, didt: float = 1e6, *, magnitude: bool = False,
+                 vectors: bool = False, potential: bool = False, nodal: bool = False, recovery: str = "raw",
+                 block_k: int | None = None) -> FieldResult:
+        if not isinstance(placement, Placement):
+            raise TypeError("simulate() takes a single Placement; use iter_simulate() for a sequence.")
+        (result,) = self.iter_simulate(coil, [placement], didt, magnitude=magnitude, vectors=vectors,
+                                       potential=potential, nodal=nodal, recovery=recovery, block_k=block_k)
+        return result
+
+
+@dataclass
+class FieldResult:
+    """Gray-matter metrics for one placement plus whichever full-volume arrays were retained
+    (reference simulation.py:668-870). Arrays are NumPy, in the subject's Morton order."""
+
+    summary: metrics.FieldMetrics
+    magnE: npt.NDArray[np.float32] | None
+    E: npt.NDArray[np.float32] | None
+    v: npt.NDArray[np.float64] | None
+    transform: npt.NDArray[np.float64]
+    placement: Placement
+    coil_name: str
+    didt: float
+    vols: npt.NDArray[np.float32] | None
+    tet_tags: npt.NDArray[np.int32] | None
+    barycenters_mm: npt.NDArray[np.float64] | None
+    recovery: str = "raw"
+    iterations: int = 0
+    relative_residual: float = 0.0
+    _summaries: dict = field(default_factory=dict, repr=False)
+
+    def _require_magnitude(self, what: str) -> np.ndarray:
+        if self.magnE is None:
+            raise ValueError(f"{what} needs the per-element |E|, which this result did not retain. Re-run with magnitude=True.")
+        return self.magnE
+
+    def peak_magnE(self, region: metrics.Region = "gray_matter") -> float:
+        return self.summary_for(region)["peak_magnE"]
+
+    def peak_location_mm(self, region: metrics.Region = "gray_matter") -> np.ndarray:
+        return self.summary_for(region)["peak_location_mm"]
+
+    def center_of_gravity_mm(self, region: metrics.Region = "gray_matter") -> np.ndarray:
+        return self.summary_for(region)["center_of_gravity_mm"]
+
+    def focality(self, frac: float = 0.5, region: metrics.Region = "gray_matter") -> float:
+        key = f"{frac:g}"
+        s = self.summary_for(region)
+        if key in s["focality_m3"]:
+            return s["focality_m3"][key]
+        m = self._require_magnitude(f"focality at frac={key}")
+        return metrics.focality(m, self.vols, metrics.region_mask(self.tet_tags, region), frac)
+
+    def summary_for(self, region: metrics.Region) -> metrics.FieldMetrics:
+        if region == self.summary["region"]:
+            return self.summary
+        if region not in self._summaries:
+            m = self._require_magnitude(f"metrics for region {region!r}")
+            self._summaries[region] = metrics.compute_metrics(m, self.vols, self.barycenters_mm, self.tet_tags, region=region)
+        return self._summaries[region]
+
+    def save(self, path: str | Path) -> None:
+        """Write the result to a self-contained ``.npz`` (arrays not retained are absent)."""
+        arrays = {k: getattr(self, k) for k in ("magnE", "E", "v", "vols", "tet_tags", "barycenters_mm")
+                  if getattr(self, k) is not None}
+        s = self.summary
+        np.savez_compressed(
+            Path(path), transform=self.transform, format_version=_FORMAT_VERSION, recovery=self.recovery,
+            coil_name=self.coil_name, didt=self.didt, placement_center_mm=self.placement.center_mm,
+            placement_handle_mm=self.placement.handle_mm, placement_distance_mm=self.placement.distance_mm,
+            summary_region=s["region"], summary_peak_magnE=s["peak_magnE"],
+            summary_peak_location_mm=s["peak_location_mm"], summary_center_of_gravity_mm=s["center_of_gravity_mm"],
+            summary_region_volume_m3=s["region_volume_m3"],
+            summary_focality_keys=np.array(list(s["focality_m3"])), summary_focality_vals=np.array(list(s["focality_m3"].values())),
+            summary_dist_keys=np.array(list(s["distribution"])), summary_dist_vals=np.array(list(s["distribution"].values())),
+            iterations=self.iterations, relative_residual=self.relative_residual, **arrays)
+
+    @classmethod
+    def load(cls, path: str | Path) -> FieldResult:
+        with np.load(Path(path), allow_pickle=False) as z:
+            if int(z["format_version"]) != _FORMAT_VERSION:
+                raise ValueError(f"{path}: file format version {int(z['format_version'])} is not readable (expected {_FORMAT_VERSION}).")
+            opt = lambda k: np.asarray(z[k]) if k in z.files else None  # noqa: E731
+            summary: metrics.FieldMetrics = {
+                "region": str(z["summary_region"]),
+                "peak_magnE": float(z["summary_peak_magnE"]),
+                "peak_location_mm": np.asarray(z["summary_peak_location_mm"]),
+                "center_of_gravity_mm": np.asarray(z["summary_center_of_gravity_mm"]),
+                "region_volume_m3": float(z["summary_region_volume_m3"]),
+                "focality_m3": {str(k): float(v) for k, v in zip(z["summary_focality_keys"], z["summary_focality_vals"])},
+                "distribution": {str(k): float(v) for k, v in zip(z["summary_dist_keys"], z["summary_dist_vals"])},
+            }
+            return cls(summary=summary, magnE=opt("magnE"), E=opt("E"), v=opt("v"), transform=np.asarray(z["transform"]),
+                       placement=Placement(z["placement_center_mm"], z["placement_handle_mm"], float(z["placement_distance_mm"])),
+                       coil_name=str(z["coil_name"]), didt=float(z["didt"]), vols=opt("vols"), tet_tags=opt("tet_tags"),
+                       barycenters_mm=opt("barycenters_mm"), recovery=str(z["recovery"]),
+                       iterations=int(z["iterations"]), relative_residual=float(z["relative_residual"]))

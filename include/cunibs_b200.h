@@ -1,0 +1,199 @@
+/* cunibs_b200 -- C ABI of the B200-native per-placement TMS field solve.
+ *
+ * The reference (cuNIBS 0.4.0) exposes this path through a nanobind module,
+ * cunibs.solver._solver_ext (src/cunibs/solver/bindings.cpp:30-676), driven from Python by
+ * fem/solve.py:690-746 (build_context) and fem/solve.py:865-979 (solve_placements_block). This
+ * library replaces that boundary with plain C: opaque handles, pointers and sizes, int status codes.
+ * Every entry point returns CUNIBS_OK (0) or an error code; cunibs_last_error() returns the message
+ * of the calling thread's last failure.
+ *
+ * Arrays are C-contiguous. Unless an entry point says "device", pointers are host memory and the
+ * call copies in and out itself; it returns after results are in the caller's buffers.
+ * A context is not thread-safe; callers serialise use of one handle.
+ */
+#ifndef CUNIBS_B200_H
+#define CUNIBS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference raises ValueError (invalid_argument) and RuntimeError
+ * (bindings.cpp:52-56) and, for a missed tolerance, SolverConvergenceError (fem/solve.py:368-392). */
+#define CUNIBS_OK 0
+#define CUNIBS_EINVAL 1
+#define CUNIBS_ENOMEM 2
+#define CUNIBS_ECUDA 3
+#define CUNIBS_ENOCONV 4
+#define CUNIBS_ETIMEOUT 5
+#define CUNIBS_EINTERNAL 6
+
+/* Solver precision. */
+#define CUNIBS_PREC_DEFAULT 0    /* per-call option: use the context's precision */
+#define CUNIBS_PREC_PLAIN_FP64 1 /* FP64 PCG over an FP64 V-cycle */
+#define CUNIBS_PREC_MIXED 2      /* FP32 PCG + FP32 V-cycle inside FP64 iterative refinement */
+
+/* Summary layout, one row of CUNIBS_SUMMARY_LEN doubles per placement (metrics.py:28-37,209-243). */
+#define CUNIBS_SUMMARY_PEAK 0       /* peak |E| in gray matter, V/m */
+#define CUNIBS_SUMMARY_PEAK_LOC 1   /* 3 values: barycentre of the peak element, mm */
+#define CUNIBS_SUMMARY_COG 4        /* 3 values: volume*|E| weighted centre of gravity, mm */
+#define CUNIBS_SUMMARY_VOLUME 7     /* gray-matter volume, m^3 */
+#define CUNIBS_SUMMARY_MEAN 8
+#define CUNIBS_SUMMARY_STD 9
+#define CUNIBS_SUMMARY_P50 10
+#define CUNIBS_SUMMARY_P95 11
+#define CUNIBS_SUMMARY_P99 12
+#define CUNIBS_SUMMARY_P999 13
+#define CUNIBS_SUMMARY_FOCALITY_50 14 /* volume with |E| >= 0.5 * p99.9, m^3 */
+#define CUNIBS_SUMMARY_FOCALITY_75 15
+#define CUNIBS_SUMMARY_LEN 16
+
+typedef struct cunibs_context cunibs_context;
+
+typedef struct {
+    int device;               /* CUDA device ordinal */
+    int min_coarse_rows;      /* AggregationParams.min_coarse_rows (fem/solve.py:146) = 128 */
+    int max_levels;           /* AggregationParams.max_levels = 50 */
+    int agg_rounds;           /* AggregationParams.rounds = 2 */
+    int cheby_degree;         /* SmootherParams.degree (fem/solve.py:167) = 2 */
+    double cheby_lower_ratio; /* SmootherParams.lower_ratio = 12 */
+    double tolerance;         /* ||r||/||b|| stopping criterion; DEFAULT_TOLERANCE = 1e-6 (fem/solve.py:56) */
+    int max_iters;            /* DEFAULT_MAX_ITERS = 2000 */
+    int precision;            /* CUNIBS_PREC_* */
+    double inner_reduction;   /* mixed: residual reduction of each inner FP32 solve */
+    int inner_max_iters;      /* mixed: iteration cap of each inner FP32 solve */
+    int iters_per_sync;       /* PCG iterations launched between host convergence checks */
+} cunibs_params;
+
+typedef struct {
+    int n_nodes;
+    int n_tets;
+    int n_skin;
+    int n_gray_matter;
+    long long stiffness_nnz;
+    int ground_node; /* in the context's (Morton) node order */
+    int n_levels;    /* AMG levels above the dense coarse solve */
+    int coarse_rows;
+} cunibs_info;
+
+/* Per-call options of a block solve. Zero-initialise for the context defaults. */
+typedef struct {
+    int block_width;   /* padded width; 0 = smallest of {1,2,4,8,16} >= k */
+    int precision;     /* CUNIBS_PREC_DEFAULT or a CUNIBS_PREC_* override */
+    double tolerance;  /* <= 0: context default */
+    int max_iters;     /* <= 0: context default */
+} cunibs_solve_opts;
+
+/* Outputs of a block solve of k placements. Required: transforms, summary. Optional (NULL to
+ * skip): iterations, relres, magnE (k, n_tets), E (k, n_tets, 3), v (k, n_nodes). All in the
+ * context's node and element order (cunibs_context_mesh returns it). */
+typedef struct {
+    double* transforms; /* (k, 4, 4) coil-to-head affines, mm */
+    double* summary;    /* (k, CUNIBS_SUMMARY_LEN) gray-matter metrics */
+    int* iterations;    /* (k) PCG iterations at which each column met tolerance */
+    double* relres;     /* (k) final relative residual per column */
+    float* magnE;       /* (k, n_tets) */
+    float* E;           /* (k, n_tets, 3) */
+    double* v;          /* (k, n_nodes) potential, grounded node = 0 */
+    int total_iterations; /* filled: iterations the block ran */
+    int outer_steps;      /* filled: FP64 refinement steps (mixed) */
+} cunibs_block_out;
+
+int cunibs_version(void);
+const char* cunibs_last_error(void);
+int cunibs_params_default(cunibs_params* out);
+
+/* Builds a subject's solver state (replaces build_context, fem/solve.py:690-746): Morton layout,
+ * P1 gradients and volumes (rejecting zero or non-finite volumes), conductivity lookup (rejecting
+ * unknown tags), stiffness assembly, grounding of the lowest-z node, the SA-AMG hierarchy, skin
+ * normals. tet_tags use the tissue table 1..10; skin_tris are the scalp triangles (tag 1005). */
+int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_nodes, const int* tet_tags,
+                          int n_tets, const int* skin_tris, int n_skin, const cunibs_params* params,
+                          cunibs_context** out);
+int cunibs_context_destroy(cunibs_context* ctx);
+int cunibs_context_info(const cunibs_context* ctx, cunibs_info* out);
+
+/* The context's Morton-ordered mesh; any pointer may be NULL. node_perm[i] / tet_perm[e] give the
+ * input index of node i / tet e (fem/solve.py:645-662). */
+int cunibs_context_mesh(const cunibs_context* ctx, double* nodes_mm, int* tet_nodes, int* tet_tags, int* skin_tris,
+                        int* node_perm, int* tet_perm);
+
+/* Hierarchy row counts, finest first then the dense coarse level (n_levels + 1 entries). */
+int cunibs_context_levels(const cunibs_context* ctx, int* sizes, int cap);
+
+/* Solves k placements as one block (replaces solve_placements_block, fem/solve.py:865-979, with
+ * Subject._reduce_chunk's summary, simulation.py:330-376). dip_pos_m/dip_moment: (n_dip, 3) in the
+ * coil frame. centers_mm/handles_mm: (k, 3); dists_mm: (k). A handle on the scalp normal is
+ * CUNIBS_EINVAL; a column that misses tolerance after one FP64 retry is CUNIBS_ENOCONV with the
+ * column in the message. */
+int cunibs_solve_block(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                       const double* centers_mm, const double* handles_mm, const double* dists_mm, int k, double didt,
+                       const cunibs_solve_opts* opts, cunibs_block_out* out);
+
+/* Same, with every input and output pointer in device memory of the context's GPU (outputs are
+ * written there; nothing is copied to the host). Returns after the work is complete. */
+int cunibs_solve_block_device(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                              const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
+                              double didt, const cunibs_solve_opts* opts, cunibs_block_out* out);
+
+/* Re-assembles the stiffness with a new conductivity per tissue tag (sigma_by_tag[0..10], S/m;
+ * index = tag) and rebuilds the AMG hierarchy: the per-sample step of a conductivity Monte Carlo
+ * (uq/conductivity/run.py:324-361). */
+int cunibs_context_set_conductivity(cunibs_context* ctx, const double* sigma_by_tag);
+
+/* --- stage-level entry points (the reference's kernel exports, bindings.cpp) --------------- */
+
+/* Copies a named internal array to host memory. name / dtype:
+ *   int32:   "node_perm" "tet_perm" "tet_nodes" "tet_tags" "skin_tris" "n2c_ptr" "n2c_idx"
+ *            "stiff_ptr" "stiff_col" "gm_index" and per level "a_ptr" "a_col" "agg" "p_ptr" "p_col"
+ *            "coarse_ptr" "coarse_col"
+ *   float64: "nodes_mm" "g" "vols" "bary" "stiff_val" "skin_normals" "coarse_val" "coarse_inv"
+ *            and per level "a_val" "p_val" "dinv"
+ * *len receives the element count; at most cap elements are written. */
+int cunibs_context_array(const cunibs_context* ctx, const char* name, int level, void* out, long long cap,
+                         long long* len);
+
+/* Coil frames for k targets (place.cu:246-273 semantics); degenerate[i] = 1 where the handle left
+ * the in-plane axis undefined. handles may be NULL. */
+int cunibs_context_place(cunibs_context* ctx, const double* centers_mm, const double* handles_mm,
+                         const double* dists_mm, int k, double* transforms, int* degenerate);
+
+/* dA/dt at the context's nodes for k given transforms: out (k, n_nodes, 3) (dadt.cu semantics). */
+int cunibs_context_dadt(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                        const double* transforms, int k, double didt, float* out);
+
+/* Solves the grounded system for k right-hand sides B (n_nodes-1, width), width in {1,2,4,8,16};
+ * X receives the solution in the same layout. x0 may be NULL. */
+int cunibs_context_solve(cunibs_context* ctx, const double* B, double* X, int k, int width, int precision,
+                         double tolerance, int max_iters, const double* x0, int* iterations, double* relres);
+
+/* One V-cycle z = M r on the grounded system, k columns row-major (n_nodes-1, k); fp32 selects the
+ * FP32 hierarchy. */
+int cunibs_context_vcycle(cunibs_context* ctx, const double* r, double* z, int k, int fp32);
+
+/* SIZE_4 pairwise aggregation of one FP32 CSR matrix (select_size4, aggregate.cu:368-472).
+ * aggregates: (n) out; *n_coarse receives the aggregate count. */
+int cunibs_select_size4(int n, const int* row_ptr, const int* col_idx, const float* values, int* aggregates,
+                        int* n_coarse);
+
+/* Gray-matter summary of one |E| field on the context's elements (RegionSlice.summarize). */
+int cunibs_context_summary(cunibs_context* ctx, const float* magnE, int k, double* summary);
+
+/* --- measurement ------------------------------------------------------------------------ */
+
+/* With timing on, each block solve records CUDA events on the context's stream between its stages
+ * and cunibs_context_stage_times returns the last call's milliseconds: [0] placement and dipole
+ * rotation, [1] dA/dt, [2] element average + right-hand side, [3] linear solve, [4] E + summary. */
+int cunibs_context_set_timing(cunibs_context* ctx, int on);
+int cunibs_context_stage_times(const cunibs_context* ctx, double* ms, int cap);
+
+/* The context's CUDA stream (a cudaStream_t), on which every block solve's work is ordered. */
+int cunibs_context_stream(const cunibs_context* ctx, void** stream);
+
+/* Kernels this process has enqueued through the library so far (graph replays count their nodes). */
+long long cunibs_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

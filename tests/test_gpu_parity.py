@@ -1,0 +1,219 @@
+"""CUDA path vs the CPU oracle, through the C ABI. Needs a B200.
+
+Integer stages (Morton layout, CSR pattern, aggregation) must match bit for bit; the setup
+stages compiled without FMA contraction (gradients, stiffness, hierarchy operators, placement) must
+match exactly too; the field must match the FP64 oracle within the stated tolerances.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cunibs_b200 import Placement, Subject, _native
+from cunibs_b200.synthetic import figure8_coil, sphere_head
+from oracle import Oracle, oracle_dadt, oracle_select_size4, oracle_summary
+
+pytestmark = pytest.mark.gpu
+
+GM_REL_L2 = 1e-5  # relative L2 of |E| over gray matter, GPU vs FP64 oracle
+PEAK_REL = 1e-5   # peak |E| relative
+
+
+@pytest.fixture(scope="module")
+def patch_pair(patch_mesh):
+    m = patch_mesh
+    return _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris), Oracle(m)
+
+
+@pytest.fixture(scope="module")
+def sphere_mesh():
+    return sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+
+
+@pytest.fixture(scope="module")
+def sphere_pair(sphere_mesh):
+    m = sphere_mesh
+    return _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris), Oracle(m)
+
+
+@pytest.mark.parametrize("which", ["patch_pair", "sphere_pair"])
+def test_layout_and_operator_bit_exact(which, request):
+    ctx, orc = request.getfixturevalue(which)
+    for name in ("node_perm", "tet_perm", "tet_nodes", "tet_tags", "skin_tris", "n2c_ptr", "n2c_idx", "stiff_ptr",
+                 "stiff_col"):
+        np.testing.assert_array_equal(ctx.array(name), orc.i32(name), err_msg=name)
+    for name in ("nodes_mm", "g", "vols", "bary", "stiff_val", "skin_normals"):
+        np.testing.assert_array_equal(ctx.array(name), orc.f64(name), err_msg=name)
+    assert ctx.ground_node == int(orc.i32("ground")[0])
+
+
+@pytest.mark.parametrize("which", ["patch_pair", "sphere_pair"])
+def test_hierarchy_bit_exact(which, request):
+    ctx, orc = request.getfixturevalue(which)
+    assert ctx.levels() == orc.i32("level_sizes").tolist()
+    for lev in range(ctx.n_levels):
+        for name in ("a_ptr", "a_col", "agg", "p_ptr", "p_col"):
+            np.testing.assert_array_equal(ctx.array(name, lev), orc.i32(name, lev), err_msg=f"{name}[{lev}]")
+        for name in ("a_val", "p_val", "dinv"):
+            np.testing.assert_array_equal(ctx.array(name, lev), orc.f64(name, lev), err_msg=f"{name}[{lev}]")
+    np.testing.assert_array_equal(ctx.array("coarse_col"), orc.i32("coarse_col"))
+    np.testing.assert_array_equal(ctx.array("coarse_val"), orc.f64("coarse_val"))
+    inv_g, inv_o = ctx.array("coarse_inv"), orc.f64("coarse_inv")
+    assert np.abs(inv_g - inv_o).max() <= 1e-12 * np.abs(inv_o).max()
+
+
+def test_patch_hierarchy_matches_reference_pin(patch_pair, pins):
+    ctx, _ = patch_pair
+    assert ctx.levels() == pins["patch_hierarchy_sizes"]["value"]
+
+
+def test_select_size4_bit_exact_on_level_operators(patch_pair):
+    ctx, orc = patch_pair
+    ptr, col, val = orc.i32("a_ptr", 0), orc.i32("a_col", 0), orc.f64("a_val", 0).astype(np.float32)
+    agg_g, nc_g = _native.select_size4(ptr, col, val)
+    agg_o, nc_o = oracle_select_size4(ptr, col, val)
+    assert nc_g == nc_o
+    np.testing.assert_array_equal(agg_g, agg_o)
+
+
+@pytest.mark.parametrize("fp32,tol", [(False, 1e-11), (True, 2e-5)])
+def test_vcycle_matches_oracle(sphere_pair, fp32, tol):
+    ctx, orc = sphere_pair
+    rng = np.random.default_rng(0)
+    r = rng.standard_normal((ctx.n_nodes - 1, 4))
+    z_g = ctx.vcycle(r, fp32=fp32)
+    z_o = orc.vcycle(r)
+    for c in range(4):
+        assert np.linalg.norm(z_g[:, c] - z_o[:, c]) / np.linalg.norm(z_o[:, c]) <= tol
+
+
+def test_placement_matches_oracle(patch_pair, patch_placement):
+    ctx, orc = patch_pair
+    p = patch_placement
+    centers = np.stack([p.center_mm, p.center_mm + [3.0, -2.0, 0.0]])
+    handles = centers + [0.0, 50.0, 0.0]
+    T_g, deg_g = ctx.place(centers, handles, [4.0, 6.0])
+    T_o, deg_o = orc.place(centers, handles, [4.0, 6.0])
+    np.testing.assert_array_equal(T_g, T_o)
+    np.testing.assert_array_equal(deg_g, deg_o)
+    # A handle straight along the outward normal leaves the frame undefined.
+    normal = -T_g[0, :3, 2]
+    proj = T_g[0, :3, 3] - 4.0 * normal
+    _, deg = ctx.place(centers[:1], (proj + 30 * normal)[None], [4.0])
+    assert deg[0] == 1
+
+
+def test_dadt_matches_fp64_oracle(patch_pair, d70_coil, patch_placement):
+    ctx, orc = patch_pair
+    p = patch_placement
+    T, _ = ctx.place(p.center_mm[None], p.handle_mm[None], [p.distance_mm])
+    got = ctx.dadt(d70_coil, T, 1e6)[0].astype(np.float64)
+    want = oracle_dadt(d70_coil, T[0], 1e6, ctx.array("nodes_mm").reshape(-1, 3))
+    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 2e-6
+    assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("precision", [_native.PREC_PLAIN_FP64, _native.PREC_MIXED])
+def test_linear_solve_matches_oracle_direct(sphere_pair, precision):
+    ctx, orc = sphere_pair
+    n = ctx.n_nodes - 1
+    rng = np.random.default_rng(5)
+    B = rng.standard_normal((n, 4))
+    X, it, rel = ctx.solve(B, 4, 4, precision=precision, tolerance=1e-10, max_iters=500)
+    assert (rel <= 1e-10).all() and (it > 0).all()
+    # Residual in FP64 against the oracle's assembled operator.
+    ptr, col, val = orc.i32("a_ptr", 0), orc.i32("a_col", 0), orc.f64("a_val", 0)
+    rows = np.repeat(np.arange(n), np.diff(ptr))
+    for c in range(4):
+        ax = np.zeros(n)
+        np.add.at(ax, rows, val * X[col, c])
+        assert np.linalg.norm(B[:, c] - ax) / np.linalg.norm(B[:, c]) <= 2e-10
+
+
+def _compare_block(subject, orc, coil, sites, tol=1e-10):
+    res = list(subject.iter_simulate(coil, sites, magnitude=True, block_k=8))
+    ref = orc.solve(coil, np.stack([s.center_mm for s in sites]), np.stack([s.handle_mm for s in sites]),
+                    [s.distance_mm for s in sites], 1e6, tolerance=tol)
+    tags = subject.mesh.tet_tags
+    gm = tags == 2
+    for i, r in enumerate(res):
+        a, b = r.magnE.astype(np.float64)[gm], ref["magnE"][i].astype(np.float64)[gm]
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert rel <= GM_REL_L2, f"placement {i}: GM rel-L2 {rel:.2e}"
+        assert abs(r.peak_magnE() - ref["summary"][i][0]) <= PEAK_REL * ref["summary"][i][0]
+        np.testing.assert_allclose(r.transform, ref["transform"][i], rtol=0, atol=1e-12)
+    return res, ref
+
+
+@pytest.mark.parametrize("precision", ["mixed", "plain"])
+def test_patch_end_to_end_vs_oracle_and_reference_pin(patch_mesh, d70_coil, patch_placement, pins, precision):
+    subj = Subject(patch_mesh, tolerance=1e-10, precision=precision)
+    orc = Oracle(patch_mesh)
+    p = patch_placement
+    sites = [p, Placement(p.center_mm + [5.0, 3.0, -1.0], p.handle_mm + [5.0, 3.0, -1.0])]
+    res, _ = _compare_block(subj, orc, d70_coil, sites)
+    pin = pins["patch_peak_magnE_raw"]
+    assert res[0].peak_magnE() == pytest.approx(pin["value"], rel=pin["rel"])
+    np.testing.assert_allclose(res[0].peak_location_mm(), pins["patch_peak_location_mm"]["value"], atol=2.0)
+    subj.free()
+
+
+def test_sphere_block_vs_oracle(sphere_mesh):
+    subj = Subject(sphere_mesh, tolerance=1e-10)
+    coil = figure8_coil(128)
+    sites = []
+    for th, ph in [(0, 0), (15, 0), (15, 90), (30, 180), (30, 270)]:
+        t, f = np.radians(th), np.radians(ph)
+        c = 90 * np.array([np.sin(t) * np.cos(f), np.sin(t) * np.sin(f), np.cos(t)])
+        sites.append(Placement(c, c + 50 * np.array([-np.sin(f), np.cos(f), 0.0])))
+    _compare_block(subj, Oracle(sphere_mesh), coil, sites)
+    subj.free()
+
+
+def test_block_width_and_batch_invariance_bitwise(sphere_mesh):
+    """A placement's result is bitwise independent of block_k and of its block-mates."""
+    subj = Subject(sphere_mesh, tolerance=1e-8)
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    sites = [Placement(top + [dx, 0, 0], top + [dx, 50, 0]) for dx in (0.0, 10.0, -12.0)]
+    runs = {bk: list(subj.iter_simulate(coil, sites, magnitude=True, potential=True, block_k=bk)) for bk in (1, 2, 4, 8)}
+    for bk in (2, 4, 8):
+        for i in range(3):
+            np.testing.assert_array_equal(runs[bk][i].magnE, runs[1][i].magnE)
+            np.testing.assert_array_equal(runs[bk][i].v, runs[1][i].v)
+            assert runs[bk][i].summary["peak_magnE"] == runs[1][i].summary["peak_magnE"]
+    alone = subj.simulate(coil, sites[2], magnitude=True)
+    np.testing.assert_array_equal(alone.magnE, runs[8][2].magnE)
+    again = list(subj.iter_simulate(coil, sites, magnitude=True, block_k=8))
+    for i in range(3):
+        np.testing.assert_array_equal(again[i].magnE, runs[8][i].magnE)
+    subj.free()
+
+
+def test_gpu_summary_matches_oracle_summary(sphere_pair):
+    ctx, orc = sphere_pair
+    rng = np.random.default_rng(2)
+    m = rng.gamma(2.0, 0.3, size=(2, ctx.n_tets)).astype(np.float32)
+    m[1, :50] = m[1].max()  # ties at the top
+    got = ctx.summary(m)
+    vols32 = orc.f64("vols").astype(np.float32)
+    for i in range(2):
+        want = oracle_summary(m[i], vols32, orc.f64("bary").reshape(-1, 3), orc.i32("tet_tags"))
+        np.testing.assert_allclose(got[i], want, rtol=1e-10, atol=0)
+
+
+def test_invalid_inputs_raise(sphere_mesh):
+    subj = Subject(sphere_mesh)
+    coil = figure8_coil(16)
+    top = np.array([0.0, 0.0, 90.0])
+    with pytest.raises(ValueError, match="zero right-hand side"):
+        subj.simulate(coil, Placement(top, top + [0, 50, 0]), didt=0.0)
+    with pytest.raises(ValueError, match="degenerate"):
+        subj.simulate(coil, Placement(top, top + [0, 0, 50]))
+    subj.free()
+    with pytest.raises(ValueError, match="volume"):
+        from cunibs_b200.mesh import HeadMesh
+
+        bad = HeadMesh([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], [[0, 1, 2, 3]], [2], [[0, 1, 2]])
+        _native.Context(bad.nodes_mm, bad.tet_nodes, bad.tet_tags, bad.skin_tris)
