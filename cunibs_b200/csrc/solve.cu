@@ -634,6 +634,12 @@ void Solver::vcycle(const T* b, T* z) {
     }
 }
 
+// Before a first tail: p = 0 and rz = 1, so beta is finite and p becomes z.
+__global__ void fill_kernel(double* v, int n, double x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = x;
+}
+
 template <typename T, int K>
 void Solver::pcg_tail(T* r, T* z, T* p) {
     constexpr int TT = tile_threads<K>();
@@ -679,6 +685,8 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     std::vector<int> init_iters(K, prm.max_iters);
     CUNIBS_CHECK(cudaMemcpyAsync(conv_iter.get(), init_iters.data(), sizeof(int) * K, cudaMemcpyHostToDevice, s));
     rel.zero(s);
+    fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
+    count_launch();
     pcg_tail<double, K>(R.get(), Z.get(), P.get());
     int it = 0;
     while (it < prm.max_iters) {
@@ -734,6 +742,8 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
         if (all || total_inner >= prm.max_iters) break;
         d32.zero(s);
         p32.zero(s);
+        fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
+        count_launch();
         pcg_tail<float, K>(r32.get(), z32.get(), p32.get());
         int it = 0;
         const int cap = std::min(prm.inner_max_iters, prm.max_iters - total_inner);

@@ -209,8 +209,11 @@ def test_invalid_inputs_raise(sphere_mesh):
     top = np.array([0.0, 0.0, 90.0])
     with pytest.raises(ValueError, match="zero right-hand side"):
         subj.simulate(coil, Placement(top, top + [0, 50, 0]), didt=0.0)
+    T, _ = subj.context.place(top[None], (top + [0, 50, 0])[None], [4.0])
+    normal = -T[0, :3, 2]
+    proj = T[0, :3, 3] - 4.0 * normal
     with pytest.raises(ValueError, match="degenerate"):
-        subj.simulate(coil, Placement(top, top + [0, 0, 50]))
+        subj.simulate(coil, Placement(top, proj + 30.0 * normal))
     subj.free()
     with pytest.raises(ValueError, match="volume"):
         from cunibs_b200.mesh import HeadMesh
