@@ -57,7 +57,7 @@ struct cunibs_context {
     // Block workspace, grown on demand.
     DevArray<double> pos, mom, centers, handles, dists, T, B, X, summary, v;
     DevArray<int> deg;
-    DevArray<unsigned char> dip_packed;
+    DevArray<unsigned char> dip_packed, zdip_packed;
     DevArray<float> dadt_nodes, dadt_elm, magn, E;
     // Stage timing (CUDA events on the context stream), enabled by cunibs_context_set_timing.
     bool timing = false;
@@ -123,21 +123,30 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
     c->T.reserve(16 * static_cast<std::size_t>(k));
     c->deg.reserve(k);
     c->mark(0);
+    c->deg.reserve(k + 1);
     place_transforms(m, centers, handles, dists, k, c->T.get(), c->deg.get(), s);
-    std::vector<int> deg(k);
-    CUNIBS_CHECK(cudaMemcpyAsync(deg.data(), c->deg.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, s));
+    c->zdip_packed.reserve(packed_zdipole_bytes() * static_cast<std::size_t>(n_dip));
+    prep_zdipoles(pos, mom, n_dip, c->zdip_packed.get(), c->deg.get() + k, s);
+    std::vector<int> deg(k + 1);
+    CUNIBS_CHECK(cudaMemcpyAsync(deg.data(), c->deg.get(), sizeof(int) * (k + 1), cudaMemcpyDeviceToHost, s));
     CUNIBS_CHECK(cudaStreamSynchronize(s));
+    const bool zcoil = deg[k] == 0;
     for (int i = 0; i < k; ++i)
         if (handles != nullptr && deg[i])
             fail(kEInval, "degenerate coil placement at index " + std::to_string(i) + " of " + std::to_string(k) +
                               ": the handle lies on the outward scalp normal through the projected centre, so the "
                               "coil's rotation about the normal is undefined");
-    c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
-    prep_dipoles(pos, mom, n_dip, c->T.get(), k, c->dip_packed.get(), s);
     c->dadt_nodes.reserve(static_cast<std::size_t>(m.n_nodes) * 3 * k);
-    c->mark(1);
-    dadt_nodes(m, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, c->T.get(), k, didt, c->dadt_nodes.get(),
-               s);
+    if (zcoil) {
+        c->mark(1);
+        dadt_nodes_zcoil(m, c->zdip_packed.get(), n_dip, c->T.get(), k, didt, c->dadt_nodes.get(), s);
+    } else {
+        c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
+        prep_dipoles(pos, mom, n_dip, c->T.get(), k, c->dip_packed.get(), s);
+        c->mark(1);
+        dadt_nodes(m, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, c->T.get(), k, didt,
+                   c->dadt_nodes.get(), s);
+    }
     c->mark(2);
     c->dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
     dadt_elements(m, c->dadt_nodes.get(), k, c->dadt_elm.get(), s);
@@ -456,11 +465,21 @@ int cunibs_context_dadt(cunibs_context* c, const double* dip_pos_m, const double
         c->mom.upload(dip_moment, 3 * static_cast<std::size_t>(n_dip), s);
         DevArray<double> T;
         T.upload(transforms, 16 * static_cast<std::size_t>(k), s);
-        c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
-        prep_dipoles(c->pos.get(), c->mom.get(), n_dip, T.get(), k, c->dip_packed.get(), s);
+        DevArray<int> flag(1);
+        c->zdip_packed.reserve(packed_zdipole_bytes() * static_cast<std::size_t>(n_dip));
+        prep_zdipoles(c->pos.get(), c->mom.get(), n_dip, c->zdip_packed.get(), flag.get(), s);
+        int general = 0;
+        CUNIBS_CHECK(cudaMemcpyAsync(&general, flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
         c->dadt_nodes.reserve(static_cast<std::size_t>(c->mesh.n_nodes) * 3 * k);
-        dadt_nodes(c->mesh, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, T.get(), k, didt,
-                   c->dadt_nodes.get(), s);
+        if (general == 0) {
+            dadt_nodes_zcoil(c->mesh, c->zdip_packed.get(), n_dip, T.get(), k, didt, c->dadt_nodes.get(), s);
+        } else {
+            c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
+            prep_dipoles(c->pos.get(), c->mom.get(), n_dip, T.get(), k, c->dip_packed.get(), s);
+            dadt_nodes(c->mesh, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, T.get(), k, didt,
+                       c->dadt_nodes.get(), s);
+        }
         copy_out(out, c->dadt_nodes.get(), sizeof(float) * 3 * static_cast<std::size_t>(c->mesh.n_nodes) * k,
                  cudaMemcpyDeviceToHost, s);
         CUNIBS_CHECK(cudaStreamSynchronize(s));

@@ -28,7 +28,7 @@ struct Params {
     double tolerance = 1e-6;
     int max_iters = 2000;
     int precision = kMixed;
-    double inner_reduction = 1e-4;  // inner FP32 PCG stops at this residual reduction
+    double inner_reduction = 1e-6;  // smallest residual reduction asked of one inner FP32 solve
     int inner_max_iters = 60;
     int iters_per_sync = 4;         // PCG iterations launched between host convergence checks
 };
@@ -57,7 +57,13 @@ struct Level {
     DevArray<float> p32;
     DevCsr<double> r;
     DevArray<float> r32;
+    // Threads per row of the V-cycle kernels on A, P and R, from each operator's shape.
+    int tpr_a = 1, tpr_p = 1, tpr_r = 1;
 };
+
+// Threads per row for an SpMV-shaped kernel over n_rows rows and nnz entries: one lane per row
+// while the rows alone fill the GPU, otherwise enough lanes that each walks about 8 entries.
+int choose_tpr(int n_rows, long nnz);
 
 struct Hierarchy {
     std::vector<Level> levels;
@@ -142,6 +148,15 @@ void prep_dipoles(const double* pos, const double* mom, int n_dip, const double*
                   cudaStream_t s);
 void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k, double didt,
                 float* out /* (k, N, 3) */, cudaStream_t s);
+// Coils whose moments all point along the coil's own z axis (every figure-8 and circular coil
+// model) take a cheaper path evaluated in each placement's coil frame. general_flag_dev receives 0
+// when the coil qualifies, 1 when some moment has an in-plane component; zpacked has room for
+// packed_zdipole_bytes() * n_dip.
+std::size_t packed_zdipole_bytes();
+void prep_zdipoles(const double* pos, const double* mom, int n_dip, void* zpacked, int* general_flag_dev,
+                   cudaStream_t s);
+void dadt_nodes_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
+                      float* out /* (k, N, 3) */, cudaStream_t s);
 void dadt_elements(const Mesh& m, const float* dadt_nodes, int k, float* dadt_elm /* (k, M, 3) */, cudaStream_t s);
 void rhs_block(const Mesh& m, const float* dadt_elm, int k, int k_pad, double* b_red /* (N-1, k_pad) */,
                cudaStream_t s);

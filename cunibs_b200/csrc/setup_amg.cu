@@ -626,6 +626,15 @@ void l1_dinv(const DevCsr<double>& a, DevArray<double>& dinv, cudaStream_t s) {
     CUNIBS_LAUNCH_CHECK("l1 dinv");
 }
 
+int choose_tpr(int n_rows, long nnz) {
+    if (n_rows <= 0) return 1;
+    if (n_rows >= 65536) return 1;
+    const double per = static_cast<double>(nnz) / n_rows;
+    int t = 1;
+    while (t < 32 && per / t > 8.0) t *= 2;
+    return t;
+}
+
 Cheby make_cheby(int degree, double lower_ratio) {
     if (degree < 1 || degree > 8) fail(kEInval, "Chebyshev degree must be in [1, 8]");
     if (!(lower_ratio > 1.0)) fail(kEInval, "Chebyshev lower_ratio must exceed 1");
@@ -678,6 +687,9 @@ void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& prm, cudaSt
         to_f32(L.dinv, L.n, L.dinv32, s);
         to_f32(L.p.val, L.p.nnz, L.p32, s);
         to_f32(L.r.val, L.r.nnz, L.r32, s);
+        L.tpr_a = choose_tpr(L.n, L.a.nnz);
+        L.tpr_p = choose_tpr(L.n, L.p.nnz);
+        L.tpr_r = choose_tpr(L.n_coarse, L.r.nnz);
         h.levels.push_back(std::move(L));
         a = std::move(next);
         h.sizes.push_back(a.n);

@@ -37,25 +37,9 @@ constexpr int tile_threads() {
 }
 
 int n_tiles(int n) { return (n + kTileRows - 1) / kTileRows; }
+__device__ __forceinline__ int n_tiles_dev(int n) { return (n + kTileRows - 1) / kTileRows; }
 
 // --- deterministic column reductions ---------------------------------------------------------
-
-// Writes this block's per-column partial (rows of the tile summed in order) to partials[c][tile].
-template <int K>
-__device__ __forceinline__ void tile_partial(double v, double* __restrict__ partials, int tiles) {
-    __shared__ double sh[kTileRows][K];
-    const int slot = threadIdx.x / K;
-    const int c = threadIdx.x % K;
-    sh[slot][c] = v;
-    __syncthreads();
-    if (threadIdx.x < K) {
-        double s = 0.0;
-#pragma unroll 8
-        for (int r = 0; r < kTileRows; ++r) s += sh[r][threadIdx.x];
-        partials[static_cast<long>(threadIdx.x) * tiles + blockIdx.x] = s;
-        __threadfence();
-    }
-}
 
 // True in the last block to finish; that block then owns the final reduction. It resets the
 // arrival counter, which no other block touches again in this launch.
@@ -101,6 +85,61 @@ __device__ __forceinline__ T row_dot(const int* __restrict__ ptr, const int* __r
 }
 
 // --- V-cycle kernels ---------------------------------------------------------------------
+//
+// A row group is TPR x K threads: K lanes per column-slot (lane = column, so a nonzero's K values
+// are one coalesced read) times TPR sub-lanes that stride the row's nonzeros. TPR is chosen per
+// operator from its shape alone (choose_tpr), never from K, and the TPR partial sums are combined
+// in shared memory by a sequential walk over the sub-lanes: the summation order of every column is
+// then fixed by the operator, which keeps a placement's answer bitwise independent of the block
+// width.
+
+template <int K, int TPR>
+struct Group {
+    static constexpr int kThreads = TPR * K;
+    static constexpr int kRows = kThreads >= 256 ? 1 : 256 / kThreads;
+    static constexpr int kBlock = kRows * kThreads;
+};
+
+template <typename T, int K, int TPR>
+struct RowSlot {
+    int row;  // global row
+    int r;    // row within the block
+    int sub;  // sub-lane
+    int c;    // column
+    __device__ __forceinline__ RowSlot() {
+        const int t = threadIdx.x;
+        r = t / Group<K, TPR>::kThreads;
+        sub = (t / K) % TPR;
+        c = t % K;
+        row = blockIdx.x * Group<K, TPR>::kRows + r;
+    }
+};
+
+// Row-times-block for one (row, column): each sub-lane sums its strided share of the row, then
+// sub-lane 0 adds the shares in order. Every thread of the block must call this.
+template <typename T, int K, int TPR>
+__device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
+                                           const T* __restrict__ val, const T* __restrict__ x,
+                                           const RowSlot<T, K, TPR>& s, bool valid) {
+    T acc = T(0);
+    if (valid) {
+        const int e = ptr[s.row + 1];
+        for (int p = ptr[s.row] + s.sub; p < e; p += TPR) acc += val[p] * x[static_cast<long>(col[p]) * K + s.c];
+    }
+    if constexpr (TPR == 1) {
+        return acc;
+    } else {
+        __shared__ T sh[Group<K, TPR>::kRows][TPR][K];
+        sh[s.r][s.sub][s.c] = acc;
+        __syncthreads();
+        T tot = T(0);
+        if (s.sub == 0) {
+#pragma unroll
+            for (int q = 0; q < TPR; ++q) tot += sh[s.r][q][s.c];
+        }
+        return tot;
+    }
+}
 
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) jz_kernel(int n, const T* __restrict__ dinv, const T* __restrict__ b,
@@ -112,60 +151,81 @@ __global__ void __launch_bounds__(tile_threads<K>()) jz_kernel(int n, const T* _
 
 // out = c_cur*x_cur + c_prev*x_prev + alpha*dinv*(b - A x_cur). out may alias x_prev (read only
 // at this row), never x_cur.
-template <typename T, int K>
-__global__ void __launch_bounds__(tile_threads<K>()) cheby_kernel(int n, const int* __restrict__ ptr,
-                                                                  const int* __restrict__ col, const T* __restrict__ val,
-                                                                  const T* __restrict__ dinv, const T* __restrict__ b,
-                                                                  const T* __restrict__ x_cur, const T* x_prev, T c_cur,
-                                                                  T c_prev, T alpha, T* out) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
-    const int c = threadIdx.x % K;
-    if (row >= n) return;
-    const T s = row_dot<T>(ptr, col, val, x_cur, row, c, K);
-    const long q = static_cast<long>(row) * K + c;
+template <typename T, int K, int TPR>
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) cheby_kernel(
+    int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
+    const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ x_cur, const T* x_prev, T c_cur,
+    T c_prev, T alpha, T* out) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < n;
+    const T ax = group_row_dot<T, K, TPR>(ptr, col, val, x_cur, s, valid);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.c;
     const T cur = x_cur[q];
     const T prev = x_prev[q];
     const T rhs = b[q];
-    out[q] = c_cur * cur + c_prev * prev + alpha * dinv[row] * (rhs - s);
+    out[q] = c_cur * cur + c_prev * prev + alpha * dinv[s.row] * (rhs - ax);
 }
 
-template <typename T, int K>
-__global__ void __launch_bounds__(tile_threads<K>()) residual_kernel(int n, const int* __restrict__ ptr,
-                                                                     const int* __restrict__ col,
-                                                                     const T* __restrict__ val, const T* __restrict__ x,
-                                                                     const T* __restrict__ b, T* __restrict__ r) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
-    const int c = threadIdx.x % K;
-    if (row >= n) return;
-    const long q = static_cast<long>(row) * K + c;
-    r[q] = b[q] - row_dot<T>(ptr, col, val, x, row, c, K);
+template <typename T, int K, int TPR>
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) residual_kernel(int n, const int* __restrict__ ptr,
+                                                                         const int* __restrict__ col,
+                                                                         const T* __restrict__ val,
+                                                                         const T* __restrict__ x,
+                                                                         const T* __restrict__ b, T* __restrict__ r) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < n;
+    const T ax = group_row_dot<T, K, TPR>(ptr, col, val, x, s, valid);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.c;
+    r[q] = b[q] - ax;
 }
 
 // b_c = R r_f; with dinv_c given, also the coarse level's first smoothing step x_c = alpha0*dinv*b_c.
-template <typename T, int K>
-__global__ void __launch_bounds__(tile_threads<K>()) restrict_kernel(int nc, const int* __restrict__ ptr,
-                                                                     const int* __restrict__ col,
-                                                                     const T* __restrict__ val, const T* __restrict__ rf,
-                                                                     T* __restrict__ bc, const T* __restrict__ dinv_c,
-                                                                     T alpha0, T* __restrict__ xc) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
-    const int c = threadIdx.x % K;
-    if (row >= nc) return;
-    const T s = row_dot<T>(ptr, col, val, rf, row, c, K);
-    const long q = static_cast<long>(row) * K + c;
-    bc[q] = s;
-    if (dinv_c != nullptr) xc[q] = alpha0 * dinv_c[row] * s;
+template <typename T, int K, int TPR>
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) restrict_kernel(int nc, const int* __restrict__ ptr,
+                                                                         const int* __restrict__ col,
+                                                                         const T* __restrict__ val,
+                                                                         const T* __restrict__ rf, T* __restrict__ bc,
+                                                                         const T* __restrict__ dinv_c, T alpha0,
+                                                                         T* __restrict__ xc) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < nc;
+    const T v = group_row_dot<T, K, TPR>(ptr, col, val, rf, s, valid);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.c;
+    bc[q] = v;
+    if (dinv_c != nullptr) xc[q] = alpha0 * dinv_c[s.row] * v;
 }
 
-template <typename T, int K>
-__global__ void __launch_bounds__(tile_threads<K>()) prolong_kernel(int n, const int* __restrict__ ptr,
-                                                                    const int* __restrict__ col,
-                                                                    const T* __restrict__ val, const T* __restrict__ xc,
-                                                                    T* __restrict__ xf) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
-    const int c = threadIdx.x % K;
-    if (row >= n) return;
-    xf[static_cast<long>(row) * K + c] += row_dot<T>(ptr, col, val, xc, row, c, K);
+template <typename T, int K, int TPR>
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) prolong_kernel(int n, const int* __restrict__ ptr,
+                                                                        const int* __restrict__ col,
+                                                                        const T* __restrict__ val,
+                                                                        const T* __restrict__ xc, T* __restrict__ xf) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < n;
+    const T v = group_row_dot<T, K, TPR>(ptr, col, val, xc, s, valid);
+    if (!valid || s.sub != 0) return;
+    xf[static_cast<long>(s.row) * K + s.c] += v;
+}
+
+template <int K, typename F>
+void dispatch_tpr(int tpr, F&& f) {
+    switch (tpr) {
+        case 1: f(std::integral_constant<int, 1>{}); break;
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 4: f(std::integral_constant<int, 4>{}); break;
+        case 8: f(std::integral_constant<int, 8>{}); break;
+        case 16: f(std::integral_constant<int, 16>{}); break;
+        case 32: f(std::integral_constant<int, 32>{}); break;
+        default: fail(kEInternal, "threads-per-row must be a power of two up to 32");
+    }
+}
+
+template <int K, int TPR>
+unsigned group_grid(int n) {
+    return static_cast<unsigned>((n + Group<K, TPR>::kRows - 1) / Group<K, TPR>::kRows);
 }
 
 // x = Ainv b for the dense coarsest operator: a warp per row, lanes striding the row, a fixed
@@ -193,19 +253,49 @@ __global__ void coarse_gemv_kernel(int nc, const T* __restrict__ inv, const T* _
 }
 
 // --- PCG kernels -------------------------------------------------------------------------
+//
+// Column reductions run over a grid of at most kMaxReduceBlocks blocks that stride the 64-row
+// tiles; each thread keeps a running sum of its rows, a block combines its 64 row slots by a fixed
+// tree, and the last block to finish adds the block partials by a fixed tree. The grid size is a
+// function of n alone, so every column is summed in the same order whatever the block width.
+
+constexpr int kMaxReduceBlocks = 592;
+
+// Per-block partial of each column into partials[c * gridDim.x + blockIdx.x].
+template <int K>
+__device__ __forceinline__ void block_partial(double v, double* __restrict__ partials) {
+    __shared__ double sh[kTileRows][K];
+    const int slot = threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    sh[slot][c] = v;
+    __syncthreads();
+#pragma unroll
+    for (int off = kTileRows / 2; off > 0; off >>= 1) {
+        if (slot < off) sh[slot][c] += sh[slot + off][c];
+        __syncthreads();
+    }
+    if (threadIdx.x < K) {
+        partials[static_cast<long>(threadIdx.x) * gridDim.x + blockIdx.x] = sh[0][threadIdx.x];
+        __threadfence();
+    }
+}
 
 // ||x_c||^2 per column into out[c].
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) norm2_kernel(int n, const T* __restrict__ x, double* partials,
                                                                   unsigned* counter, double* __restrict__ out) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
+    const int tiles = n_tiles_dev(n);
     double v = 0.0;
-    if (row < n) {
-        const double xv = static_cast<double>(x[static_cast<long>(row) * K + c]);
-        v = xv * xv;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int row = t * kTileRows + slot;
+        if (row < n) {
+            const double xv = static_cast<double>(x[static_cast<long>(row) * K + c]);
+            v += xv * xv;
+        }
     }
-    tile_partial<K>(v, partials, gridDim.x);
+    block_partial<K>(v, partials);
     if (last_block(counter)) {
         __shared__ double tot[K];
         final_reduce<K>(partials, gridDim.x, tot);
@@ -219,16 +309,20 @@ __global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
     const T* __restrict__ p, T* __restrict__ ap, double* partials, unsigned* counter, const double* __restrict__ rz,
     const int* __restrict__ frozen, double* __restrict__ alpha) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
+    const int tiles = n_tiles_dev(n);
     double v = 0.0;
-    if (row < n) {
-        const T s = row_dot<T>(ptr, col, val, p, row, c, K);
-        const long q = static_cast<long>(row) * K + c;
-        ap[q] = s;
-        v = static_cast<double>(p[q]) * static_cast<double>(s);
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int row = t * kTileRows + slot;
+        if (row < n) {
+            const T s = row_dot<T>(ptr, col, val, p, row, c, K);
+            const long q = static_cast<long>(row) * K + c;
+            ap[q] = s;
+            v += static_cast<double>(p[q]) * static_cast<double>(s);
+        }
     }
-    tile_partial<K>(v, partials, gridDim.x);
+    block_partial<K>(v, partials);
     if (last_block(counter)) {
         __shared__ double tot[K];
         final_reduce<K>(partials, gridDim.x, tot);
@@ -239,26 +333,34 @@ __global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
     }
 }
 
-// x += alpha p; r -= alpha Ap; rr = ||r||^2. A column freezes when sqrt(rr) <= tol*sqrt(ref[c]);
-// the iteration it froze at and its relative residual are recorded on the device.
+// x += alpha p; r -= alpha Ap; rr = ||r||^2. A column freezes when sqrt(rr) <= tol_c*sqrt(ref[c])
+// (tol_c = tol_vec[c] when given, else tol); the iteration it froze at and its relative residual
+// are recorded on the device. With z0 given, also writes the V-cycle's first smoothing step
+// z0 = alpha0*dinv*r from the new residual.
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
     int n, const double* __restrict__ alpha, const T* __restrict__ p, const T* __restrict__ ap, T* __restrict__ x,
     T* __restrict__ r, double* partials, unsigned* counter, const double* __restrict__ ref, double tol,
-    int* __restrict__ frozen, int* __restrict__ iter_counter, int* __restrict__ conv_iter, double* __restrict__ rel_out,
-    int record) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const double* __restrict__ tol_vec, int* __restrict__ frozen, int* __restrict__ iter_counter,
+    int* __restrict__ conv_iter, double* __restrict__ rel_out, int record, const T* __restrict__ dinv, T alpha0,
+    T* __restrict__ z0) {
+    const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
+    const int tiles = n_tiles_dev(n);
+    const T a = static_cast<T>(alpha[c]);
     double v = 0.0;
-    if (row < n) {
-        const long q = static_cast<long>(row) * K + c;
-        const T a = static_cast<T>(alpha[c]);
-        x[q] += a * p[q];
-        const T rn = r[q] - a * ap[q];
-        r[q] = rn;
-        v = static_cast<double>(rn) * static_cast<double>(rn);
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int row = t * kTileRows + slot;
+        if (row < n) {
+            const long q = static_cast<long>(row) * K + c;
+            x[q] += a * p[q];
+            const T rn = r[q] - a * ap[q];
+            r[q] = rn;
+            if (z0 != nullptr) z0[q] = alpha0 * dinv[row] * rn;
+            v += static_cast<double>(rn) * static_cast<double>(rn);
+        }
     }
-    tile_partial<K>(v, partials, gridDim.x);
+    block_partial<K>(v, partials);
     if (last_block(counter)) {
         __shared__ double tot[K];
         final_reduce<K>(partials, gridDim.x, tot);
@@ -266,9 +368,10 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
         if (threadIdx.x < K) {
             const int cc = threadIdx.x;
             const double rel = sqrt(tot[cc]) / sqrt(ref[cc]);
+            const double tc = tol_vec ? tol_vec[cc] : tol;
             if (!frozen[cc]) {
                 if (record) rel_out[cc] = rel;
-                if (rel <= tol) {
+                if (rel <= tc) {
                     frozen[cc] = 1;
                     if (record) conv_iter[cc] = it;
                 }
@@ -279,6 +382,18 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
     }
 }
 
+// Finishes the beta update in the last block: rz_new = sum; beta = rz_new / rz (0 when frozen).
+template <int K>
+__device__ __forceinline__ void finish_beta(double* partials, double* rz, const int* frozen, double* beta) {
+    __shared__ double tot[K];
+    final_reduce<K>(partials, gridDim.x, tot);
+    if (threadIdx.x < K) {
+        const int cc = threadIdx.x;
+        beta[cc] = frozen[cc] ? 0.0 : tot[cc] / rz[cc];
+        rz[cc] = tot[cc];
+    }
+}
+
 // rz_new = r . z; beta = rz_new / rz (0 on a frozen column); rz = rz_new.
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) dot_beta_kernel(int n, const T* __restrict__ r,
@@ -286,23 +401,46 @@ __global__ void __launch_bounds__(tile_threads<K>()) dot_beta_kernel(int n, cons
                                                                      unsigned* counter, double* __restrict__ rz,
                                                                      const int* __restrict__ frozen,
                                                                      double* __restrict__ beta) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
+    const int tiles = n_tiles_dev(n);
     double v = 0.0;
-    if (row < n) {
-        const long q = static_cast<long>(row) * K + c;
-        v = static_cast<double>(r[q]) * static_cast<double>(z[q]);
-    }
-    tile_partial<K>(v, partials, gridDim.x);
-    if (last_block(counter)) {
-        __shared__ double tot[K];
-        final_reduce<K>(partials, gridDim.x, tot);
-        if (threadIdx.x < K) {
-            const int cc = threadIdx.x;
-            beta[cc] = frozen[cc] ? 0.0 : tot[cc] / rz[cc];
-            rz[cc] = tot[cc];
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int row = t * kTileRows + slot;
+        if (row < n) {
+            const long q = static_cast<long>(row) * K + c;
+            v += static_cast<double>(r[q]) * static_cast<double>(z[q]);
         }
     }
+    block_partial<K>(v, partials);
+    if (last_block(counter)) finish_beta<K>(partials, rz, frozen, beta);
+}
+
+// The V-cycle's last Chebyshev step on the finest level (one lane per row), fused with r . z:
+// z = c_cur*x_cur + c_prev*x_prev + alpha*dinv*(r - A x_cur), then beta as in dot_beta_kernel.
+template <typename T, int K>
+__global__ void __launch_bounds__(tile_threads<K>()) cheby_dot_kernel(
+    int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
+    const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ x_cur, const T* __restrict__ x_prev,
+    T c_cur, T c_prev, T alpha, T* __restrict__ z, double* partials, unsigned* counter, double* __restrict__ rz,
+    const int* __restrict__ frozen, double* __restrict__ beta) {
+    const int slot = threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    const int tiles = n_tiles_dev(n);
+    double v = 0.0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int row = t * kTileRows + slot;
+        if (row < n) {
+            const T s = row_dot<T>(ptr, col, val, x_cur, row, c, K);
+            const long q = static_cast<long>(row) * K + c;
+            const T rhs = b[q];
+            const T out = c_cur * x_cur[q] + c_prev * x_prev[q] + alpha * dinv[row] * (rhs - s);
+            z[q] = out;
+            v += static_cast<double>(rhs) * static_cast<double>(out);
+        }
+    }
+    block_partial<K>(v, partials);
+    if (last_block(counter)) finish_beta<K>(partials, rz, frozen, beta);
 }
 
 template <typename T, int K>
@@ -316,25 +454,31 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_p_kernel(int n, cons
 }
 
 // Mixed refinement outer step: R = B - A X in FP64; r32 = (float)R; per column the true relative
-// residual, the outer freeze, and the inner solve's reference norm and starting freeze.
+// residual, the outer freeze, the inner solve's reference norm, its starting freeze, and the
+// inner target: reduce the residual by eta = max(eta_min, 0.3 * tol / rel), just enough (with a
+// margin) for the next outer step to meet tol.
 template <int K>
 __global__ void __launch_bounds__(tile_threads<K>()) true_residual_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ B, const double* __restrict__ X, float* __restrict__ r32, double* partials,
-    unsigned* counter, const double* __restrict__ ref_sq, double tol, int* __restrict__ outer_conv,
-    int* __restrict__ inner_frozen, double* __restrict__ rr0, const int* __restrict__ iter_counter,
-    int* __restrict__ conv_iter, double* __restrict__ rel_out) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    unsigned* counter, const double* __restrict__ ref_sq, double tol, double eta_min, int* __restrict__ outer_conv,
+    int* __restrict__ inner_frozen, double* __restrict__ rr0, double* __restrict__ eta,
+    const int* __restrict__ iter_counter, int* __restrict__ conv_iter, double* __restrict__ rel_out) {
+    const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
+    const int tiles = n_tiles_dev(n);
     double v = 0.0;
-    if (row < n) {
-        const long q = static_cast<long>(row) * K + c;
-        const double rv = B[q] - row_dot<double>(ptr, col, val, X, row, c, K);
-        const float rf = static_cast<float>(rv);
-        r32[q] = rf;
-        v = static_cast<double>(rf) * static_cast<double>(rf);
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int row = t * kTileRows + slot;
+        if (row < n) {
+            const long q = static_cast<long>(row) * K + c;
+            const double rv = B[q] - row_dot<double>(ptr, col, val, X, row, c, K);
+            const float rf = static_cast<float>(rv);
+            r32[q] = rf;
+            v += static_cast<double>(rf) * static_cast<double>(rf);
+        }
     }
-    tile_partial<K>(v, partials, gridDim.x);
+    block_partial<K>(v, partials);
     if (last_block(counter)) {
         __shared__ double tot[K];
         final_reduce<K>(partials, gridDim.x, tot);
@@ -350,6 +494,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) true_residual_kernel(
             }
             inner_frozen[cc] = outer_conv[cc];
             rr0[cc] = tot[cc];
+            eta[cc] = fmax(eta_min, fmin(0.1, 0.3 * tol / rel));
         }
     }
 }
@@ -379,6 +524,8 @@ __global__ void __launch_bounds__(tile_threads<K>()) add_correction_kernel(int n
     X[q] += static_cast<double>(d[q]);
 }
 
+int reduce_grid(int n) { return std::min(n_tiles(n), kMaxReduceBlocks); }
+
 }  // namespace
 
 // Per-precision V-cycle workspace.
@@ -401,7 +548,7 @@ class Solver {
     VWork<float> v32;
     VWork<double> v64;
     // Per-column scalars.
-    DevArray<double> rz, alpha, beta, ref_sq, rr0, rel, partials;
+    DevArray<double> rz, alpha, beta, ref_sq, rr0, rel, eta, partials;
     DevArray<int> frozen, outer_conv, conv_iter, iter_counter;
     DevArray<unsigned> counter;
     int* h_flags = nullptr;   // pinned
@@ -445,12 +592,12 @@ class Solver {
         v32.cx.resize(mc);
         v64.cb.resize(mc);
         v64.cx.resize(mc);
-        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel}) a->resize(K);
+        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta}) a->resize(K);
         for (auto* a : {&frozen, &outer_conv, &conv_iter}) a->resize(K);
         iter_counter.resize(1);
         counter.resize(1);
         counter.zero(stream);
-        partials.resize(static_cast<std::size_t>(n_tiles(n)) * K);
+        partials.resize(static_cast<std::size_t>(kMaxReduceBlocks) * K);
         if (h_flags) cudaFreeHost(h_flags);
         if (h_dbl) cudaFreeHost(h_dbl);
         CUNIBS_CHECK(cudaMallocHost(&h_flags, sizeof(int) * 4 * K));
@@ -473,13 +620,21 @@ class Solver {
     template <typename T>
     VWork<T>& vw();
 
+    // z = M b. jz_done: the finest level's first smoothing step is already in its buffer (fused into
+    // the PCG update). dot: fuse r . z and the beta update into the last step (finest level, one lane
+    // per row); returns whether it did.
     template <typename T, int K>
-    void vcycle(const T* b, T* z);
+    bool vcycle(const T* b, T* z, bool jz_done = false, bool dot = false);
+    template <typename T>
+    T* first0() {
+        VWork<T>& w = vw<T>();
+        return (h->cheby.degree % 2) ? w.x[0].get() : w.r[0].get();
+    }
     template <typename T, int K>
-    void pcg_tail(T* r, T* z, T* p);
+    void pcg_tail(T* r, T* z, T* p, bool jz_done);
     template <typename T, int K>
     void pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
-                       const double* ref, int record);
+                       const double* tol_vec, const double* ref, int record);
     template <int K>
     void solve_plain(int k, const Params& prm, SolveStats& st, bool warm);
     template <int K>
@@ -545,7 +700,7 @@ template <>
 VWork<double>& Solver::vw<double>() { return v64; }
 
 template <typename T, int K>
-void Solver::vcycle(const T* b, T* z) {
+bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     const Hierarchy& H = *h;
     const Cheby& ch = H.cheby;
     const int L = static_cast<int>(H.levels.size());
@@ -554,17 +709,25 @@ void Solver::vcycle(const T* b, T* z) {
     cudaStream_t s = stream;
     if (L == 0) {
         coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(), b, z); count_launch();
-        return;
+        return false;
     }
+    const bool fuse_dot = dot && H.levels[0].tpr_a == 1;
     const int deg = ch.degree;
     const bool odd = (deg % 2) != 0;
     // One Chebyshev sweep of `deg` steps (vcycle.cu:585-617 buffer discipline). x0 == nullptr is a
     // zero initial guess whose first step, x = alpha0*dinv*b, the caller has already written into
     // `first`. Otherwise step 0 reads x0 and writes `first`; later steps alternate, writing over
     // the buffer that holds x_{i-1}, which the step kernel reads only at the row it writes.
-    auto sweep = [&](int l, const T* bi, T* x0, T* first, T* other, T* final_out) {
+    auto launch_cheby = [&](int l, const T* bi, const T* cur, const T* prev, T cc, T cp, T al, T* out) {
         const Level& lv = H.levels[l];
-        const unsigned g = n_tiles(lv.n);
+        dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
+            constexpr int TPR = decltype(tc)::value;
+            cheby_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
+                lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al, out);
+        });
+        count_launch();
+    };
+    auto sweep = [&](int l, const T* bi, T* x0, T* first, T* other, T* final_out) {
         auto target = [&](int st) -> T* {
             if (st + 1 == deg && final_out) return final_out;
             return (st % 2) ? other : first;
@@ -576,17 +739,25 @@ void Solver::vcycle(const T* b, T* z) {
             prev = first;
         } else {
             T* out = target(0);
-            cheby_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, x0,
-                                               x0, T(1), T(0), static_cast<T>(ch.alpha0), out); count_launch();
+            launch_cheby(l, bi, x0, x0, T(1), T(0), static_cast<T>(ch.alpha0), out);
             prev = x0;
             cur = out;
         }
         for (int st = 1; st < deg; ++st) {
             T* out = target(st);
             const T cp = (st == 1 && x0 == nullptr) ? T(0) : static_cast<T>(ch.c_prev[st - 1]);
-            cheby_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur,
-                                               prev, static_cast<T>(ch.c_cur[st - 1]), cp,
-                                               static_cast<T>(ch.alpha[st - 1]), out); count_launch();
+            if (fuse_dot && l == 0 && final_out != nullptr && st + 1 == deg) {
+                const Level& lv = H.levels[0];
+                cheby_dot_kernel<T, K><<<reduce_grid(lv.n), TT, 0, s>>>(
+                    lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(0), ldinv<T>(0), bi, cur, prev,
+                    static_cast<T>(ch.c_cur[st - 1]), cp, static_cast<T>(ch.alpha[st - 1]), out, partials.get(),
+                    counter.get(), rz.get(), frozen.get(), beta.get());
+                count_launch();
+                prev = cur;
+                cur = out;
+                continue;
+            }
+            launch_cheby(l, bi, cur, prev, static_cast<T>(ch.c_cur[st - 1]), cp, static_cast<T>(ch.alpha[st - 1]), out);
             prev = cur;
             cur = out;
         }
@@ -599,13 +770,17 @@ void Solver::vcycle(const T* b, T* z) {
         T* first = odd ? w.x[l].get() : w.r[l].get();
         T* other = odd ? w.r[l].get() : w.x[l].get();
         const unsigned g = n_tiles(lv.n);
-        if (l == 0) {
+        if (l == 0 && !jz_done) {
             jz_kernel<T, K><<<g, TT, 0, s>>>(lv.n, ldinv<T>(0), bi, static_cast<T>(ch.alpha0), first);
             count_launch();
         }
         sweep(l, bi, nullptr, first, other, nullptr);
-        residual_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi,
-                                               w.r[l].get()); count_launch();
+        dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
+            constexpr int TPR = decltype(tc)::value;
+            residual_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
+                lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
+        });
+        count_launch();
         const bool next_is_level = (l + 1 < L);
         T* nb = next_is_level ? w.b[l + 1].get() : w.cb.get();
         T* nx = nullptr;
@@ -615,9 +790,13 @@ void Solver::vcycle(const T* b, T* z) {
             nx = nodd ? w.x[l + 1].get() : w.r[l + 1].get();
             nd = ldinv<T>(l + 1);
         }
-        restrict_kernel<T, K><<<n_tiles(lv.n_coarse), TT, 0, s>>>(lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(),
-                                                                  rval<T>(l), w.r[l].get(), nb, nd,
-                                                                  static_cast<T>(ch.alpha0), nx); count_launch();
+        dispatch_tpr<K>(lv.tpr_r, [&](auto tc) {
+            constexpr int TPR = decltype(tc)::value;
+            restrict_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n_coarse), Group<K, TPR>::kBlock, 0, s>>>(
+                lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(), rval<T>(l), w.r[l].get(), nb, nd,
+                static_cast<T>(ch.alpha0), nx);
+        });
+        count_launch();
     }
     coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(),
                                                                                                  w.cb.get(), w.cx.get()); count_launch();
@@ -626,12 +805,18 @@ void Solver::vcycle(const T* b, T* z) {
     for (int l = L - 1; l >= 0; --l) {
         const Level& lv = H.levels[l];
         const T* bi = (l == 0) ? b : w.b[l].get();
-        const unsigned g = n_tiles(lv.n);
-        prolong_kernel<T, K><<<g, TT, 0, s>>>(lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get()); count_launch();
+        dispatch_tpr<K>(lv.tpr_p, [&](auto tc) {
+            constexpr int TPR = decltype(tc)::value;
+            prolong_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
+                lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
+        });
+        count_launch();
         // The level's smoothed correction stays wherever its sweep left it; the next finer
         // prolongation reads it from there.
         xc = sweep(l, bi, w.x[l].get(), w.r[l].get(), w.x[l].get(), (l == 0) ? z : nullptr);
     }
+    // The fused step exists only when the sweep has a step after its first (degree >= 2).
+    return fuse_dot && deg >= 2;
 }
 
 // Before a first tail: p = 0 and rz = 1, so beta is finite and p becomes z.
@@ -641,24 +826,33 @@ __global__ void fill_kernel(double* v, int n, double x) {
 }
 
 template <typename T, int K>
-void Solver::pcg_tail(T* r, T* z, T* p) {
+void Solver::pcg_tail(T* r, T* z, T* p, bool jz_done) {
     constexpr int TT = tile_threads<K>();
-    const unsigned g = n_tiles(n);
-    vcycle<T, K>(r, z);
-    dot_beta_kernel<T, K><<<g, TT, 0, stream>>>(n, r, z, partials.get(), counter.get(), rz.get(), frozen.get(), beta.get()); count_launch();
-    update_p_kernel<T, K><<<g, TT, 0, stream>>>(n, beta.get(), z, p); count_launch();
+    const bool fused = vcycle<T, K>(r, z, jz_done, true);
+    if (!fused) {
+        dot_beta_kernel<T, K><<<reduce_grid(n), TT, 0, stream>>>(n, r, z, partials.get(), counter.get(), rz.get(),
+                                                                frozen.get(), beta.get());
+        count_launch();
+    }
+    update_p_kernel<T, K><<<n_tiles(n), TT, 0, stream>>>(n, beta.get(), z, p);
+    count_launch();
 }
 
 template <typename T, int K>
 void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
-                           const double* ref, int record) {
+                           const double* tol_vec, const double* ref, int record) {
     constexpr int TT = tile_threads<K>();
-    const unsigned g = n_tiles(n);
+    const unsigned g = reduce_grid(n);
     spmv_alpha_kernel<T, K><<<g, TT, 0, stream>>>(n, ptr, col, val, p, ap, partials.get(), counter.get(), rz.get(),
-                                                  frozen.get(), alpha.get()); count_launch();
-    update_xr_kernel<T, K><<<g, TT, 0, stream>>>(n, alpha.get(), p, ap, x, r, partials.get(), counter.get(), ref, tol,
-                                                 frozen.get(), iter_counter.get(), conv_iter.get(), rel.get(), record); count_launch();
-    pcg_tail<T, K>(r, z, p);
+                                                  frozen.get(), alpha.get());
+    count_launch();
+    const bool has_levels = !h->levels.empty();
+    update_xr_kernel<T, K><<<g, TT, 0, stream>>>(
+        n, alpha.get(), p, ap, x, r, partials.get(), counter.get(), ref, tol, tol_vec, frozen.get(), iter_counter.get(),
+        conv_iter.get(), rel.get(), record, has_levels ? ldinv<T>(0) : nullptr, static_cast<T>(h->cheby.alpha0),
+        has_levels ? first0<T>() : nullptr);
+    count_launch();
+    pcg_tail<T, K>(r, z, p, has_levels);
 }
 
 template <int K>
@@ -668,7 +862,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     cudaStream_t s = stream;
     const DevCsr<double>& A = h->levels.empty() ? h->coarse : h->levels[0].a;
     const std::size_t nk = static_cast<std::size_t>(n) * K;
-    norm2_kernel<double, K><<<g, TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
+    norm2_kernel<double, K><<<reduce_grid(n), TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
     if (warm) {
         residual64_kernel<K><<<g, TT, 0, s>>>(n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), R.get()); count_launch();
     } else {
@@ -687,14 +881,14 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     rel.zero(s);
     fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
     count_launch();
-    pcg_tail<double, K>(R.get(), Z.get(), P.get());
+    pcg_tail<double, K>(R.get(), Z.get(), P.get(), false);
     int it = 0;
     while (it < prm.max_iters) {
         const int m = std::min(prm.iters_per_sync, prm.max_iters - it);
         for (int j = 0; j < m; ++j) {
             run_graph({0, K, 0}, [&] {
                 pcg_iteration<double, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(),
-                                         Z.get(), prm.tolerance, ref_sq.get(), 1);
+                                         Z.get(), prm.tolerance, nullptr, ref_sq.get(), 1);
             });
         }
         it += m;
@@ -717,7 +911,7 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
     const float* A32 = h->levels.empty() ? nullptr : h->levels[0].a32.get();
     DevArray<float> coarse32;
     if (A32 == nullptr) fail(kEInval, "mixed precision needs at least one AMG level");
-    norm2_kernel<double, K><<<g, TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
+    norm2_kernel<double, K><<<reduce_grid(n), TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
     outer_conv.zero(s);
     iter_counter.zero(s);
     CUNIBS_CHECK(cudaMemcpyAsync(h_dbl, ref_sq.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
@@ -731,10 +925,11 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
     int outer = 0;
     const int max_outer = 64;
     for (; outer < max_outer; ++outer) {
-        true_residual_kernel<K><<<g, TT, 0, s>>>(n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), r32.get(),
-                                                 partials.get(), counter.get(), ref_sq.get(), prm.tolerance,
-                                                 outer_conv.get(), frozen.get(), rr0.get(), iter_counter.get(),
-                                                 conv_iter.get(), rel.get()); count_launch();
+        true_residual_kernel<K><<<reduce_grid(n), TT, 0, s>>>(
+            n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), r32.get(), partials.get(), counter.get(),
+            ref_sq.get(), prm.tolerance, prm.inner_reduction, outer_conv.get(), frozen.get(), rr0.get(), eta.get(),
+            iter_counter.get(), conv_iter.get(), rel.get());
+        count_launch();
         CUNIBS_CHECK(cudaMemcpyAsync(h_flags, outer_conv.get(), sizeof(int) * K, cudaMemcpyDeviceToHost, s));
         CUNIBS_CHECK(cudaStreamSynchronize(s));
         bool all = true;
@@ -744,7 +939,7 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
         p32.zero(s);
         fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
         count_launch();
-        pcg_tail<float, K>(r32.get(), z32.get(), p32.get());
+        pcg_tail<float, K>(r32.get(), z32.get(), p32.get(), false);
         int it = 0;
         const int cap = std::min(prm.inner_max_iters, prm.max_iters - total_inner);
         while (it < cap) {
@@ -752,7 +947,7 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
             for (int j = 0; j < m; ++j) {
                 run_graph({1, K, 0}, [&] {
                     pcg_iteration<float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
-                                            z32.get(), prm.inner_reduction, rr0.get(), 0);
+                                            z32.get(), 0.0, eta.get(), rr0.get(), 0);
                 });
             }
             it += m;

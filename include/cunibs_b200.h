@@ -60,7 +60,7 @@ typedef struct {
     double tolerance;         /* ||r||/||b|| stopping criterion; DEFAULT_TOLERANCE = 1e-6 (fem/solve.py:56) */
     int max_iters;            /* DEFAULT_MAX_ITERS = 2000 */
     int precision;            /* CUNIBS_PREC_* */
-    double inner_reduction;   /* mixed: residual reduction of each inner FP32 solve */
+    double inner_reduction;   /* mixed: smallest residual reduction asked of one inner FP32 solve */
     int inner_max_iters;      /* mixed: iteration cap of each inner FP32 solve */
     int iters_per_sync;       /* PCG iterations launched between host convergence checks */
 } cunibs_params;
@@ -158,7 +158,8 @@ int cunibs_context_array(const cunibs_context* ctx, const char* name, int level,
 int cunibs_context_place(cunibs_context* ctx, const double* centers_mm, const double* handles_mm,
                          const double* dists_mm, int k, double* transforms, int* degenerate);
 
-/* dA/dt at the context's nodes for k given transforms: out (k, n_nodes, 3) (dadt.cu semantics). */
+/* dA/dt at the context's nodes for k given transforms: out (k, n_nodes, 3) (dadt.cu semantics).
+ * Coils whose moments all lie along the coil's z axis take the coil-frame path. */
 int cunibs_context_dadt(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
                         const double* transforms, int k, double didt, float* out);
 

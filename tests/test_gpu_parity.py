@@ -104,14 +104,25 @@ def test_placement_matches_oracle(patch_pair, patch_placement):
     assert deg[0] == 1
 
 
-def test_dadt_matches_fp64_oracle(patch_pair, d70_coil, patch_placement):
+@pytest.mark.parametrize("general", [False, True])
+def test_dadt_matches_fp64_oracle(patch_pair, d70_coil, patch_placement, general):
+    """Both dipole paths: the D70's z-moments (coil-frame path) and a tilted copy (general path)."""
+    from cunibs_b200.coil import Coil
+
     ctx, orc = patch_pair
     p = patch_placement
-    T, _ = ctx.place(p.center_mm[None], p.handle_mm[None], [p.distance_mm])
-    got = ctx.dadt(d70_coil, T, 1e6)[0].astype(np.float64)
-    want = oracle_dadt(d70_coil, T[0], 1e6, ctx.array("nodes_mm").reshape(-1, 3))
-    assert np.linalg.norm(got - want) / np.linalg.norm(want) <= 2e-6
-    assert np.abs(got - want).max() <= 1e-5 * np.abs(want).max()
+    coil = d70_coil
+    if general:
+        c, s_ = np.cos(0.3), np.sin(0.3)
+        rot = np.array([[c, 0, s_], [0, 1, 0], [-s_, 0, c]])
+        coil = Coil(d70_coil.positions_m, d70_coil.moments @ rot.T)
+    T, _ = ctx.place(np.stack([p.center_mm, p.center_mm + [4.0, 0, 0]]), np.stack([p.handle_mm, p.handle_mm + [4.0, 0, 0]]),
+                     [p.distance_mm, 6.0])
+    got = ctx.dadt(coil, T, 1e6).astype(np.float64)
+    for i in range(2):
+        want = oracle_dadt(coil, T[i], 1e6, ctx.array("nodes_mm").reshape(-1, 3))
+        assert np.linalg.norm(got[i] - want) / np.linalg.norm(want) <= 2e-6
+        assert np.abs(got[i] - want).max() <= 1e-5 * np.abs(want).max()
 
 
 @pytest.mark.parametrize("precision", [_native.PREC_PLAIN_FP64, _native.PREC_MIXED])
