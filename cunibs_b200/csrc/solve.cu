@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
     T* __restrict__ r, double* partials, unsigned* counter, const double* __restrict__ ref, double tol,
     const double* __restrict__ tol_vec, int* __restrict__ frozen, int* __restrict__ iter_counter,
     int* __restrict__ conv_iter, double* __restrict__ rel_out, int record, const T* __restrict__ dinv, T alpha0,
-    T* __restrict__ z0) {
+    T* __restrict__ z0, cudaGraphConditionalHandle loop, int use_loop, const int* __restrict__ cap) {
     const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
     const int tiles = n_tiles_dev(n);
@@ -378,7 +378,16 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) *iter_counter = it;
+        if (threadIdx.x == 0) {
+            *iter_counter = it;
+            // Inside a device-side WHILE graph: run another iteration unless every column has
+            // frozen or the iteration budget is spent.
+            if (use_loop) {
+                bool all = true;
+                for (int cc = 0; cc < K; ++cc) all = all && frozen[cc];
+                cudaGraphSetConditional(loop, (!all && it < *cap) ? 1u : 0u);
+            }
+        }
     }
 }
 
@@ -595,6 +604,7 @@ class Solver {
         for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta}) a->resize(K);
         for (auto* a : {&frozen, &outer_conv, &conv_iter}) a->resize(K);
         iter_counter.resize(1);
+        cap.resize(1);
         counter.resize(1);
         counter.zero(stream);
         partials.resize(static_cast<std::size_t>(kMaxReduceBlocks) * K);
@@ -632,9 +642,73 @@ class Solver {
     }
     template <typename T, int K>
     void pcg_tail(T* r, T* z, T* p, bool jz_done);
+    void set_cap(int v) {
+        h_flags[0] = v;
+        CUNIBS_CHECK(cudaMemcpyAsync(cap.get(), h_flags, sizeof(int), cudaMemcpyHostToDevice, stream));
+    }
     template <typename T, int K>
     void pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
-                       const double* tol_vec, const double* ref, int record);
+                       const double* tol_vec, const double* ref, int record, cudaGraphConditionalHandle loop = 0,
+                       int use_loop = 0);
+    DevArray<int> cap;
+    // Device-side loop: body(handle) is captured once into the body of a conditional WHILE node and
+    // replayed until a kernel in it clears the condition. Returns false when the driver cannot
+    // build such a graph (the caller then loops on the host).
+    template <typename Body>
+    bool run_while(std::tuple<int, int, int> key, Body&& body, long long* nodes_out) {
+        auto it = graphs.find(key);
+        if (it == graphs.end()) {
+            if (while_unsupported) return false;
+            cudaGraph_t g = nullptr;
+            if (cudaGraphCreate(&g, 0) != cudaSuccess) return fail_while();
+            cudaGraphConditionalHandle handle;
+            if (cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail_while();
+            }
+            cudaGraphNodeParams np = {};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = handle;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            cudaGraphNode_t node;
+            if (cudaGraphAddNode(&node, g, nullptr, 0, &np) != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail_while();
+            }
+            cudaGraph_t bodyg = np.conditional.phGraph_out[0];
+            const long long before = launch_counter().load();
+            if (cudaStreamBeginCaptureToGraph(stream, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+                cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail_while();
+            }
+            body(handle);
+            cudaGraph_t captured = nullptr;
+            const cudaError_t end = cudaStreamEndCapture(stream, &captured);
+            launch_counter().store(before);
+            if (end != cudaSuccess) {
+                cudaGraphDestroy(g);
+                return fail_while();
+            }
+            std::size_t n_nodes = 0;
+            CUNIBS_CHECK(cudaGraphGetNodes(bodyg, nullptr, &n_nodes));
+            cudaGraphExec_t ex = nullptr;
+            const cudaError_t inst = cudaGraphInstantiate(&ex, g, 0);
+            cudaGraphDestroy(g);
+            if (inst != cudaSuccess) return fail_while();
+            it = graphs.emplace(key, std::make_pair(ex, static_cast<long long>(n_nodes))).first;
+        }
+        CUNIBS_CHECK(cudaGraphLaunch(it->second.first, stream));
+        *nodes_out = it->second.second;
+        return true;
+    }
+    bool while_unsupported = false;
+    bool fail_while() {
+        (void)cudaGetLastError();
+        while_unsupported = true;
+        return false;
+    }
     template <int K>
     void solve_plain(int k, const Params& prm, SolveStats& st, bool warm);
     template <int K>
@@ -840,7 +914,8 @@ void Solver::pcg_tail(T* r, T* z, T* p, bool jz_done) {
 
 template <typename T, int K>
 void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
-                           const double* tol_vec, const double* ref, int record) {
+                           const double* tol_vec, const double* ref, int record, cudaGraphConditionalHandle loop,
+                           int use_loop) {
     constexpr int TT = tile_threads<K>();
     const unsigned g = reduce_grid(n);
     spmv_alpha_kernel<T, K><<<g, TT, 0, stream>>>(n, ptr, col, val, p, ap, partials.get(), counter.get(), rz.get(),
@@ -850,7 +925,7 @@ void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T
     update_xr_kernel<T, K><<<g, TT, 0, stream>>>(
         n, alpha.get(), p, ap, x, r, partials.get(), counter.get(), ref, tol, tol_vec, frozen.get(), iter_counter.get(),
         conv_iter.get(), rel.get(), record, has_levels ? ldinv<T>(0) : nullptr, static_cast<T>(h->cheby.alpha0),
-        has_levels ? first0<T>() : nullptr);
+        has_levels ? first0<T>() : nullptr, loop, use_loop, cap.get());
     count_launch();
     pcg_tail<T, K>(r, z, p, has_levels);
 }
@@ -883,7 +958,19 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     count_launch();
     pcg_tail<double, K>(R.get(), Z.get(), P.get(), false);
     int it = 0;
-    while (it < prm.max_iters) {
+    set_cap(prm.max_iters);
+    long long nodes = 0;
+    const bool device_loop = run_while({2, K, 0}, [&](cudaGraphConditionalHandle hnd) {
+        pcg_iteration<double, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(), Z.get(),
+                                 prm.tolerance, nullptr, ref_sq.get(), 1, hnd, 1);
+    }, &nodes);
+    if (device_loop) {
+        CUNIBS_CHECK(cudaMemcpyAsync(h_flags, iter_counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        it = h_flags[0];
+        count_launch(nodes * it);
+    }
+    while (!device_loop && it < prm.max_iters) {
         const int m = std::min(prm.iters_per_sync, prm.max_iters - it);
         for (int j = 0; j < m; ++j) {
             run_graph({0, K, 0}, [&] {
@@ -941,9 +1028,21 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
         count_launch();
         pcg_tail<float, K>(r32.get(), z32.get(), p32.get(), false);
         int it = 0;
-        const int cap = std::min(prm.inner_max_iters, prm.max_iters - total_inner);
-        while (it < cap) {
-            const int m = std::min(prm.iters_per_sync, cap - it);
+        const int cap_n = std::min(prm.inner_max_iters, prm.max_iters - total_inner);
+        set_cap(total_inner + cap_n);
+        long long nodes = 0;
+        const bool device_loop = run_while({3, K, 0}, [&](cudaGraphConditionalHandle hnd) {
+            pcg_iteration<float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
+                                    z32.get(), 0.0, eta.get(), rr0.get(), 0, hnd, 1);
+        }, &nodes);
+        if (device_loop) {
+            CUNIBS_CHECK(cudaMemcpyAsync(h_flags, iter_counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+            CUNIBS_CHECK(cudaStreamSynchronize(s));
+            it = h_flags[0] - total_inner;
+            count_launch(nodes * it);
+        }
+        while (!device_loop && it < cap_n) {
+            const int m = std::min(prm.iters_per_sync, cap_n - it);
             for (int j = 0; j < m; ++j) {
                 run_graph({1, K, 0}, [&] {
                     pcg_iteration<float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
