@@ -61,8 +61,8 @@ struct Level {
     int tpr_a = 1, tpr_p = 1, tpr_r = 1;
 };
 
-// Threads per row for an SpMV-shaped kernel over n_rows rows and nnz entries: one lane per row
-// while the rows alone fill the GPU, otherwise enough lanes that each walks about 8 entries.
+// Lanes per row for an SpMV-shaped kernel over n_rows rows and nnz entries: enough that each lane
+// walks about four entries (a power of two up to 32).
 int choose_tpr(int n_rows, long nnz);
 
 struct Hierarchy {

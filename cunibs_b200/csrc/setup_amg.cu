@@ -628,10 +628,9 @@ void l1_dinv(const DevCsr<double>& a, DevArray<double>& dinv, cudaStream_t s) {
 
 int choose_tpr(int n_rows, long nnz) {
     if (n_rows <= 0) return 1;
-    if (n_rows >= 65536) return 1;
     const double per = static_cast<double>(nnz) / n_rows;
     int t = 1;
-    while (t < 32 && per / t > 8.0) t *= 2;
+    while (t < 32 && per / t > 4.0) t *= 2;
     return t;
 }
 
