@@ -630,7 +630,7 @@ int choose_tpr(int n_rows, long nnz) {
     if (n_rows <= 0) return 1;
     const double per = static_cast<double>(nnz) / n_rows;
     int t = 1;
-    while (t < 32 && per / t > 4.0) t *= 2;
+    while (t < 32 && per / t > 8.0) t *= 2;
     return t;
 }
 

@@ -56,50 +56,23 @@ __device__ __forceinline__ bool last_block(unsigned* counter) {
     return is_last;
 }
 
-// In the last block: total[c] = a fixed tree over 64 strided sums of the block partials. Works
-// for any block size.
+// In the last block: total[c] = fixed tree over kTileRows strided sums of the tile partials.
 template <int K>
-__device__ __forceinline__ void final_reduce(const double* __restrict__ partials, int nblocks, double* total) {
+__device__ __forceinline__ void final_reduce(const double* __restrict__ partials, int tiles, double* total) {
     __shared__ double sh[kTileRows][K];
-    for (int idx = threadIdx.x; idx < kTileRows * K; idx += blockDim.x) {
-        const int slot = idx / K;
-        const int c = idx % K;
-        double acc = 0.0;
-        for (int t = slot; t < nblocks; t += kTileRows) acc += __ldcg(partials + static_cast<long>(c) * nblocks + t);
-        sh[slot][c] = acc;
-    }
+    const int slot = threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    double acc = 0.0;
+    for (int t = slot; t < tiles; t += kTileRows) acc += __ldcg(partials + static_cast<long>(c) * tiles + t);
+    sh[slot][c] = acc;
     __syncthreads();
 #pragma unroll
     for (int off = kTileRows / 2; off > 0; off >>= 1) {
-        for (int idx = threadIdx.x; idx < off * K; idx += blockDim.x) sh[idx / K][idx % K] += sh[idx / K + off][idx % K];
+        if (slot < off) sh[slot][c] += sh[slot + off][c];
         __syncthreads();
     }
     if (threadIdx.x < K) total[threadIdx.x] = sh[0][threadIdx.x];
     __syncthreads();
-}
-
-// Block partial for the row-vector kernels: the owner lane of each (row slot, column) contributes
-// its running sum over the block's tiles; a fixed tree over the ROWS slots follows.
-template <int K, int ROWS, int TPR>
-__device__ __forceinline__ void block_partial_rows(const double (&part)[K], double* __restrict__ partials) {
-    __shared__ double sh[ROWS][K];
-    const int r = threadIdx.x / TPR;
-    const int sub = threadIdx.x % TPR;
-    for (int idx = threadIdx.x; idx < ROWS * K; idx += blockDim.x) sh[idx / K][idx % K] = 0.0;
-    __syncthreads();
-#pragma unroll
-    for (int c = 0; c < K; ++c)
-        if (c % TPR == sub) sh[r][c] = part[c];
-    __syncthreads();
-#pragma unroll
-    for (int off = ROWS / 2; off > 0; off >>= 1) {
-        for (int idx = threadIdx.x; idx < off * K; idx += blockDim.x) sh[idx / K][idx % K] += sh[idx / K + off][idx % K];
-        __syncthreads();
-    }
-    if (threadIdx.x < K) {
-        partials[static_cast<long>(threadIdx.x) * gridDim.x + blockIdx.x] = sh[0][threadIdx.x];
-        __threadfence();
-    }
 }
 
 template <typename T>
@@ -111,73 +84,83 @@ __device__ __forceinline__ T row_dot(const int* __restrict__ ptr, const int* __r
     return s;
 }
 
-// --- SpMV-shaped kernels -------------------------------------------------------------------
+// --- V-cycle kernels ---------------------------------------------------------------------
 //
-// A row belongs to TPR adjacent lanes of one warp; each lane strides the row's nonzeros and carries
-// all K columns, loading a nonzero's K-wide block of x as vector loads. The TPR partial sums are
-// combined by an XOR butterfly, after which every lane of the group holds the same totals (each
-// pair of lanes adds the same two values, and addition is commutative), and lane `sub` finishes
-// the columns c with c % TPR == sub. TPR is chosen per operator from its shape alone (choose_tpr),
-// never from K, so each column's summation order is fixed by the operator and a placement's answer
-// is bitwise independent of the block width.
+// A row group is TPR x K threads: K lanes per column-slot (lane = column, so a nonzero's K values
+// are one coalesced read) times TPR sub-lanes that stride the row's nonzeros. TPR is chosen per
+// operator from its shape alone (choose_tpr), never from K, and the TPR partial sums are combined
+// in shared memory by a sequential walk over the sub-lanes: the summation order of every column is
+// then fixed by the operator, which keeps a placement's answer bitwise independent of the block
+// width.
 
-template <int TPR>
-struct RowTile {
-    static constexpr int kRows = TPR <= 16 ? 64 : 32;
-    static constexpr int kThreads = kRows * TPR;
+template <int K, int TPR>
+struct Group {
+    static constexpr int kThreads = TPR * K;
+    static constexpr int kRows = kThreads >= 256 ? 1 : 256 / kThreads;
+    static constexpr int kBlock = kRows * kThreads;
 };
 
-template <typename T, int K>
-__device__ __forceinline__ void load_vec(const T* __restrict__ p, T (&v)[K]) {
-    if constexpr (sizeof(T) == 4 && K % 4 == 0) {
+template <typename T, int K, int TPR>
+struct RowSlot {
+    int row;  // global row
+    int r;    // row within the block
+    int sub;  // sub-lane
+    int c;    // column
+    __device__ __forceinline__ RowSlot() {
+        const int t = threadIdx.x;
+        r = t / Group<K, TPR>::kThreads;
+        sub = (t / K) % TPR;
+        c = t % K;
+        row = blockIdx.x * Group<K, TPR>::kRows + r;
+    }
+};
+
+// Row-times-block for one (row, column): each sub-lane sums its strided share of the row, then the
+// shares are combined in a fixed order: by an XOR butterfly over the sub-lanes when a row group fits
+// in a warp (every sub-lane ends with the same total, since each pair adds the same two values and
+// addition is commutative), otherwise by sub-lane 0 walking them in shared memory. Either way the
+// order depends on TPR alone. Every thread of the block must call this.
+template <typename T, int K, int TPR, int ROWS>
+__device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
+                                           const T* __restrict__ val, const T* __restrict__ x, int row, int r,
+                                           int sub, int c, bool valid) {
+    T acc = T(0);
+    if (valid) {
+        const int e = ptr[row + 1];
+        for (int p = ptr[row] + sub; p < e; p += TPR) acc += val[p] * x[static_cast<long>(col[p]) * K + c];
+    }
+    if constexpr (TPR == 1) {
+        return acc;
+    } else if constexpr (TPR * K <= kWarp) {
 #pragma unroll
-        for (int b = 0; b < K / 4; ++b) {
-            const float4 t = __ldg(reinterpret_cast<const float4*>(p) + b);
-            v[4 * b] = t.x;
-            v[4 * b + 1] = t.y;
-            v[4 * b + 2] = t.z;
-            v[4 * b + 3] = t.w;
-        }
-    } else if constexpr (sizeof(T) == 4 && K == 2) {
-        const float2 t = __ldg(reinterpret_cast<const float2*>(p));
-        v[0] = t.x;
-        v[1] = t.y;
-    } else if constexpr (sizeof(T) == 8 && K % 2 == 0) {
-#pragma unroll
-        for (int b = 0; b < K / 2; ++b) {
-            const double2 t = __ldg(reinterpret_cast<const double2*>(p) + b);
-            v[2 * b] = t.x;
-            v[2 * b + 1] = t.y;
-        }
+        for (int off = TPR / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off * K);
+        return acc;
     } else {
+        __shared__ T sh[ROWS][TPR][K];
+        sh[r][sub][c] = acc;
+        __syncthreads();
+        T tot = T(0);
+        if (sub == 0) {
 #pragma unroll
-        for (int c = 0; c < K; ++c) v[c] = __ldg(p + c);
+            for (int q = 0; q < TPR; ++q) tot += sh[r][q][c];
+        }
+        __syncthreads();
+        return tot;
     }
 }
 
-// Every lane of the block must call this (the butterfly is a full-warp shuffle).
 template <typename T, int K, int TPR>
-__device__ __forceinline__ void row_spmv(const int* __restrict__ ptr, const int* __restrict__ col,
-                                         const T* __restrict__ val, const T* __restrict__ x, int row, bool valid,
-                                         int sub, T (&acc)[K]) {
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = T(0);
-    if (valid) {
-        const int e = ptr[row + 1];
-        for (int p = ptr[row] + sub; p < e; p += TPR) {
-            const T v = val[p];
-            T xv[K];
-            load_vec<T, K>(x + static_cast<long>(col[p]) * K, xv);
-#pragma unroll
-            for (int c = 0; c < K; ++c) acc[c] += v * xv[c];
-        }
-    }
-#pragma unroll
-    for (int off = TPR / 2; off > 0; off >>= 1) {
-#pragma unroll
-        for (int c = 0; c < K; ++c) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off, TPR);
-    }
+__device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
+                                           const T* __restrict__ val, const T* __restrict__ x,
+                                           const RowSlot<T, K, TPR>& s, bool valid) {
+    return group_row_dot<T, K, TPR, Group<K, TPR>::kRows>(ptr, col, val, x, s.row, s.r, s.sub, s.c, valid);
 }
+
+// Reducing kernels tile the rows 64/TPR at a time so a block is always 64*K threads.
+template <int TPR>
+struct ReduceTile {
+    static constexpr int kRows = kTileRows / TPR;
+};
 
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) jz_kernel(int n, const T* __restrict__ dinv, const T* __restrict__ b,
@@ -187,85 +170,65 @@ __global__ void __launch_bounds__(tile_threads<K>()) jz_kernel(int n, const T* _
     if (row < n) x[static_cast<long>(row) * K + c] = alpha0 * dinv[row] * b[static_cast<long>(row) * K + c];
 }
 
-// out = c_cur*x_cur + c_prev*x_prev + alpha*dinv*(b - A x_cur). out may alias x_prev (each entry is
-// read and written by the same lane), never x_cur.
+// out = c_cur*x_cur + c_prev*x_prev + alpha*dinv*(b - A x_cur). out may alias x_prev (read only
+// at this row), never x_cur.
 template <typename T, int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) cheby_kernel(
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) cheby_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
     const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ x_cur, const T* x_prev, T c_cur,
     T c_prev, T alpha, T* out) {
-    const int sub = threadIdx.x % TPR;
-    const int row = blockIdx.x * RowTile<TPR>::kRows + threadIdx.x / TPR;
-    const bool valid = row < n;
-    T ax[K];
-    row_spmv<T, K, TPR>(ptr, col, val, x_cur, row, valid, sub, ax);
-    if (!valid) return;
-    const T d = alpha * dinv[row];
-    const long base = static_cast<long>(row) * K;
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        if (c % TPR == sub) out[base + c] = c_cur * x_cur[base + c] + c_prev * x_prev[base + c] + d * (b[base + c] - ax[c]);
-    }
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < n;
+    const T ax = group_row_dot<T, K, TPR>(ptr, col, val, x_cur, s, valid);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.c;
+    const T cur = x_cur[q];
+    const T prev = x_prev[q];
+    const T rhs = b[q];
+    out[q] = c_cur * cur + c_prev * prev + alpha * dinv[s.row] * (rhs - ax);
 }
 
 template <typename T, int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) residual_kernel(int n, const int* __restrict__ ptr,
-                                                                          const int* __restrict__ col,
-                                                                          const T* __restrict__ val,
-                                                                          const T* __restrict__ x,
-                                                                          const T* __restrict__ b, T* __restrict__ r) {
-    const int sub = threadIdx.x % TPR;
-    const int row = blockIdx.x * RowTile<TPR>::kRows + threadIdx.x / TPR;
-    const bool valid = row < n;
-    T ax[K];
-    row_spmv<T, K, TPR>(ptr, col, val, x, row, valid, sub, ax);
-    if (!valid) return;
-    const long base = static_cast<long>(row) * K;
-#pragma unroll
-    for (int c = 0; c < K; ++c)
-        if (c % TPR == sub) r[base + c] = b[base + c] - ax[c];
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) residual_kernel(int n, const int* __restrict__ ptr,
+                                                                         const int* __restrict__ col,
+                                                                         const T* __restrict__ val,
+                                                                         const T* __restrict__ x,
+                                                                         const T* __restrict__ b, T* __restrict__ r) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < n;
+    const T ax = group_row_dot<T, K, TPR>(ptr, col, val, x, s, valid);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.c;
+    r[q] = b[q] - ax;
 }
 
 // b_c = R r_f; with dinv_c given, also the coarse level's first smoothing step x_c = alpha0*dinv*b_c.
 template <typename T, int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) restrict_kernel(int nc, const int* __restrict__ ptr,
-                                                                          const int* __restrict__ col,
-                                                                          const T* __restrict__ val,
-                                                                          const T* __restrict__ rf, T* __restrict__ bc,
-                                                                          const T* __restrict__ dinv_c, T alpha0,
-                                                                          T* __restrict__ xc) {
-    const int sub = threadIdx.x % TPR;
-    const int row = blockIdx.x * RowTile<TPR>::kRows + threadIdx.x / TPR;
-    const bool valid = row < nc;
-    T v[K];
-    row_spmv<T, K, TPR>(ptr, col, val, rf, row, valid, sub, v);
-    if (!valid) return;
-    const long base = static_cast<long>(row) * K;
-    const T d = dinv_c != nullptr ? alpha0 * dinv_c[row] : T(0);
-#pragma unroll
-    for (int c = 0; c < K; ++c) {
-        if (c % TPR == sub) {
-            bc[base + c] = v[c];
-            if (dinv_c != nullptr) xc[base + c] = d * v[c];
-        }
-    }
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) restrict_kernel(int nc, const int* __restrict__ ptr,
+                                                                         const int* __restrict__ col,
+                                                                         const T* __restrict__ val,
+                                                                         const T* __restrict__ rf, T* __restrict__ bc,
+                                                                         const T* __restrict__ dinv_c, T alpha0,
+                                                                         T* __restrict__ xc) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < nc;
+    const T v = group_row_dot<T, K, TPR>(ptr, col, val, rf, s, valid);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.c;
+    bc[q] = v;
+    if (dinv_c != nullptr) xc[q] = alpha0 * dinv_c[s.row] * v;
 }
 
 template <typename T, int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) prolong_kernel(int n, const int* __restrict__ ptr,
-                                                                         const int* __restrict__ col,
-                                                                         const T* __restrict__ val,
-                                                                         const T* __restrict__ xc, T* __restrict__ xf) {
-    const int sub = threadIdx.x % TPR;
-    const int row = blockIdx.x * RowTile<TPR>::kRows + threadIdx.x / TPR;
-    const bool valid = row < n;
-    T v[K];
-    row_spmv<T, K, TPR>(ptr, col, val, xc, row, valid, sub, v);
-    if (!valid) return;
-    const long base = static_cast<long>(row) * K;
-#pragma unroll
-    for (int c = 0; c < K; ++c)
-        if (c % TPR == sub) xf[base + c] += v[c];
+__global__ void __launch_bounds__(Group<K, TPR>::kBlock) prolong_kernel(int n, const int* __restrict__ ptr,
+                                                                        const int* __restrict__ col,
+                                                                        const T* __restrict__ val,
+                                                                        const T* __restrict__ xc, T* __restrict__ xf) {
+    const RowSlot<T, K, TPR> s;
+    const bool valid = s.row < n;
+    const T v = group_row_dot<T, K, TPR>(ptr, col, val, xc, s, valid);
+    if (!valid || s.sub != 0) return;
+    xf[static_cast<long>(s.row) * K + s.c] += v;
 }
 
 template <int K, typename F>
@@ -281,9 +244,9 @@ void dispatch_tpr(int tpr, F&& f) {
     }
 }
 
-template <int TPR>
-unsigned row_grid(int n) {
-    return static_cast<unsigned>((n + RowTile<TPR>::kRows - 1) / RowTile<TPR>::kRows);
+template <int K, int TPR>
+unsigned group_grid(int n) {
+    return static_cast<unsigned>((n + Group<K, TPR>::kRows - 1) / Group<K, TPR>::kRows);
 }
 
 // x = Ainv b for the dense coarsest operator: a warp per row, lanes striding the row, a fixed
@@ -363,33 +326,27 @@ __global__ void __launch_bounds__(tile_threads<K>()) norm2_kernel(int n, const T
 
 // Ap = A p; pAp per column; alpha = rz / pAp (0 on a frozen column).
 template <typename T, int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) spmv_alpha_kernel(
+__global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
     const T* __restrict__ p, T* __restrict__ ap, double* partials, unsigned* counter, const double* __restrict__ rz,
     const int* __restrict__ frozen, double* __restrict__ alpha) {
-    constexpr int ROWS = RowTile<TPR>::kRows;
-    const int sub = threadIdx.x % TPR;
+    constexpr int ROWS = ReduceTile<TPR>::kRows;
+    const int r = threadIdx.x / (TPR * K);
+    const int sub = (threadIdx.x / K) % TPR;
+    const int c = threadIdx.x % K;
     const int tiles = (n + ROWS - 1) / ROWS;
-    double part[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) part[c] = 0.0;
+    double v = 0.0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int row = t * ROWS + threadIdx.x / TPR;
+        const int row = t * ROWS + r;
         const bool valid = row < n;
-        T s[K];
-        row_spmv<T, K, TPR>(ptr, col, val, p, row, valid, sub, s);
-        if (valid) {
-            const long base = static_cast<long>(row) * K;
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                if (c % TPR == sub) {
-                    ap[base + c] = s[c];
-                    part[c] += static_cast<double>(p[base + c]) * static_cast<double>(s[c]);
-                }
-            }
+        const T s = group_row_dot<T, K, TPR, ROWS>(ptr, col, val, p, row, r, sub, c, valid);
+        if (valid && sub == 0) {
+            const long q = static_cast<long>(row) * K + c;
+            ap[q] = s;
+            v += static_cast<double>(p[q]) * static_cast<double>(s);
         }
     }
-    block_partial_rows<K, ROWS, TPR>(part, partials);
+    block_partial<K>(v, partials);
     if (last_block(counter)) {
         __shared__ double tot[K];
         final_reduce<K>(partials, gridDim.x, tot);
@@ -495,37 +452,30 @@ __global__ void __launch_bounds__(tile_threads<K>()) dot_beta_kernel(int n, cons
 // The V-cycle's last Chebyshev step on the finest level fused with r . z:
 // z = c_cur*x_cur + c_prev*x_prev + alpha*dinv*(r - A x_cur), then beta as in dot_beta_kernel.
 template <typename T, int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) cheby_dot_kernel(
+__global__ void __launch_bounds__(tile_threads<K>()) cheby_dot_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
     const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ x_cur, const T* __restrict__ x_prev,
     T c_cur, T c_prev, T alpha, T* __restrict__ z, double* partials, unsigned* counter, double* __restrict__ rz,
     const int* __restrict__ frozen, double* __restrict__ beta) {
-    constexpr int ROWS = RowTile<TPR>::kRows;
-    const int sub = threadIdx.x % TPR;
+    constexpr int ROWS = ReduceTile<TPR>::kRows;
+    const int r = threadIdx.x / (TPR * K);
+    const int sub = (threadIdx.x / K) % TPR;
+    const int c = threadIdx.x % K;
     const int tiles = (n + ROWS - 1) / ROWS;
-    double part[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) part[c] = 0.0;
+    double v = 0.0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int row = t * ROWS + threadIdx.x / TPR;
+        const int row = t * ROWS + r;
         const bool valid = row < n;
-        T ax[K];
-        row_spmv<T, K, TPR>(ptr, col, val, x_cur, row, valid, sub, ax);
-        if (valid) {
-            const long base = static_cast<long>(row) * K;
-            const T d = alpha * dinv[row];
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                if (c % TPR == sub) {
-                    const T rhs = b[base + c];
-                    const T out = c_cur * x_cur[base + c] + c_prev * x_prev[base + c] + d * (rhs - ax[c]);
-                    z[base + c] = out;
-                    part[c] += static_cast<double>(rhs) * static_cast<double>(out);
-                }
-            }
+        const T s = group_row_dot<T, K, TPR, ROWS>(ptr, col, val, x_cur, row, r, sub, c, valid);
+        if (valid && sub == 0) {
+            const long q = static_cast<long>(row) * K + c;
+            const T rhs = b[q];
+            const T out = c_cur * x_cur[q] + c_prev * x_prev[q] + alpha * dinv[row] * (rhs - s);
+            z[q] = out;
+            v += static_cast<double>(rhs) * static_cast<double>(out);
         }
     }
-    block_partial_rows<K, ROWS, TPR>(part, partials);
+    block_partial<K>(v, partials);
     if (last_block(counter)) finish_beta<K>(partials, rz, frozen, beta);
 }
 
@@ -544,36 +494,30 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_p_kernel(int n, cons
 // inner target: reduce the residual by eta = max(eta_min, 0.3 * tol / rel), just enough (with a
 // margin) for the next outer step to meet tol.
 template <int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) true_residual_kernel(
+__global__ void __launch_bounds__(tile_threads<K>()) true_residual_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const double* __restrict__ val,
     const double* __restrict__ B, const double* __restrict__ X, float* __restrict__ r32, double* partials,
     unsigned* counter, const double* __restrict__ ref_sq, double tol, double eta_min, int* __restrict__ outer_conv,
     int* __restrict__ inner_frozen, double* __restrict__ rr0, double* __restrict__ eta,
     const int* __restrict__ iter_counter, int* __restrict__ conv_iter, double* __restrict__ rel_out) {
-    constexpr int ROWS = RowTile<TPR>::kRows;
-    const int sub = threadIdx.x % TPR;
+    constexpr int ROWS = ReduceTile<TPR>::kRows;
+    const int r = threadIdx.x / (TPR * K);
+    const int sub = (threadIdx.x / K) % TPR;
+    const int c = threadIdx.x % K;
     const int tiles = (n + ROWS - 1) / ROWS;
-    double part[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) part[c] = 0.0;
+    double v = 0.0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
-        const int row = t * ROWS + threadIdx.x / TPR;
+        const int row = t * ROWS + r;
         const bool valid = row < n;
-        double ax[K];
-        row_spmv<double, K, TPR>(ptr, col, val, X, row, valid, sub, ax);
-        if (valid) {
-            const long base = static_cast<long>(row) * K;
-#pragma unroll
-            for (int c = 0; c < K; ++c) {
-                if (c % TPR == sub) {
-                    const float rf = static_cast<float>(B[base + c] - ax[c]);
-                    r32[base + c] = rf;
-                    part[c] += static_cast<double>(rf) * static_cast<double>(rf);
-                }
-            }
+        const double ax = group_row_dot<double, K, TPR, ROWS>(ptr, col, val, X, row, r, sub, c, valid);
+        if (valid && sub == 0) {
+            const long q = static_cast<long>(row) * K + c;
+            const float rf = static_cast<float>(B[q] - ax);
+            r32[q] = rf;
+            v += static_cast<double>(rf) * static_cast<double>(rf);
         }
     }
-    block_partial_rows<K, ROWS, TPR>(part, partials);
+    block_partial<K>(v, partials);
     if (last_block(counter)) {
         __shared__ double tot[K];
         final_reduce<K>(partials, gridDim.x, tot);
@@ -596,22 +540,22 @@ __global__ void __launch_bounds__(RowTile<TPR>::kThreads) true_residual_kernel(
 
 // FP64 residual R = B - A X for a warm start of the plain solve.
 template <int K, int TPR>
-__global__ void __launch_bounds__(RowTile<TPR>::kThreads) residual64_kernel(int n, const int* __restrict__ ptr,
-                                                                            const int* __restrict__ col,
-                                                                            const double* __restrict__ val,
-                                                                            const double* __restrict__ B,
-                                                                            const double* __restrict__ X,
-                                                                            double* __restrict__ R) {
-    const int sub = threadIdx.x % TPR;
-    const int row = blockIdx.x * RowTile<TPR>::kRows + threadIdx.x / TPR;
+__global__ void __launch_bounds__(tile_threads<K>()) residual64_kernel(int n, const int* __restrict__ ptr,
+                                                                       const int* __restrict__ col,
+                                                                       const double* __restrict__ val,
+                                                                       const double* __restrict__ B,
+                                                                       const double* __restrict__ X,
+                                                                       double* __restrict__ R) {
+    constexpr int ROWS = ReduceTile<TPR>::kRows;
+    const int r = threadIdx.x / (TPR * K);
+    const int sub = (threadIdx.x / K) % TPR;
+    const int c = threadIdx.x % K;
+    const int row = blockIdx.x * ROWS + r;
     const bool valid = row < n;
-    double ax[K];
-    row_spmv<double, K, TPR>(ptr, col, val, X, row, valid, sub, ax);
-    if (!valid) return;
-    const long base = static_cast<long>(row) * K;
-#pragma unroll
-    for (int c = 0; c < K; ++c)
-        if (c % TPR == sub) R[base + c] = B[base + c] - ax[c];
+    const double ax = group_row_dot<double, K, TPR, ROWS>(ptr, col, val, X, row, r, sub, c, valid);
+    if (!valid || sub != 0) return;
+    const long q = static_cast<long>(row) * K + c;
+    R[q] = B[q] - ax;
 }
 
 template <int K>
@@ -627,7 +571,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) add_correction_kernel(int n
 int reduce_grid(int n) { return std::min(n_tiles(n), kMaxReduceBlocks); }
 template <int TPR>
 int reduce_grid_rows(int n) {
-    return std::min((n + RowTile<TPR>::kRows - 1) / RowTile<TPR>::kRows, kMaxReduceBlocks);
+    return std::min((n + ReduceTile<TPR>::kRows - 1) / ReduceTile<TPR>::kRows, kMaxReduceBlocks);
 }
 
 }  // namespace
@@ -737,8 +681,12 @@ class Solver {
     }
     template <typename T, int K>
     void pcg_tail(T* r, T* z, T* p, bool jz_done);
-    // Threads per row on the finest operator (the PCG's own matrix).
-    int tpr0() const { return h->levels.empty() ? choose_tpr(h->nc, h->coarse.nnz) : h->levels[0].tpr_a; }
+    // Sub-lanes per row on the finest operator (the PCG's own matrix), capped where the reducing
+    // kernels' 64/TPR-row tiles need at least four rows.
+    int tpr0() const {
+        const int t = h->levels.empty() ? choose_tpr(h->nc, h->coarse.nnz) : h->levels[0].tpr_a;
+        return t > 16 ? 16 : t;
+    }
     void set_cap(int v) {
         h_flags[0] = v;
         CUNIBS_CHECK(cudaMemcpyAsync(cap.get(), h_flags, sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -882,7 +830,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(), b, z); count_launch();
         return false;
     }
-    const bool fuse_dot = dot;
+    const bool fuse_dot = dot && H.levels[0].tpr_a <= 16;
     const int deg = ch.degree;
     const bool odd = (deg % 2) != 0;
     // One Chebyshev sweep of `deg` steps (vcycle.cu:585-617 buffer discipline). x0 == nullptr is a
@@ -893,7 +841,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         const Level& lv = H.levels[l];
         dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            cheby_kernel<T, K, TPR><<<row_grid<TPR>(lv.n), RowTile<TPR>::kThreads, 0, s>>>(
+            cheby_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
                 lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al, out);
         });
         count_launch();
@@ -921,7 +869,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
                 const Level& lv = H.levels[0];
                 dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
                     constexpr int TPR = decltype(tc)::value;
-                    cheby_dot_kernel<T, K, TPR><<<reduce_grid_rows<TPR>(lv.n), RowTile<TPR>::kThreads, 0, s>>>(
+                    cheby_dot_kernel<T, K, TPR><<<reduce_grid_rows<TPR>(lv.n), TT, 0, s>>>(
                         lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(0), ldinv<T>(0), bi, cur, prev,
                         static_cast<T>(ch.c_cur[st - 1]), cp, static_cast<T>(ch.alpha[st - 1]), out, partials.get(),
                         counter.get(), rz.get(), frozen.get(), beta.get());
@@ -951,7 +899,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         sweep(l, bi, nullptr, first, other, nullptr);
         dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            residual_kernel<T, K, TPR><<<row_grid<TPR>(lv.n), RowTile<TPR>::kThreads, 0, s>>>(
+            residual_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
                 lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
         });
         count_launch();
@@ -966,7 +914,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         }
         dispatch_tpr<K>(lv.tpr_r, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            restrict_kernel<T, K, TPR><<<row_grid<TPR>(lv.n_coarse), RowTile<TPR>::kThreads, 0, s>>>(
+            restrict_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n_coarse), Group<K, TPR>::kBlock, 0, s>>>(
                 lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(), rval<T>(l), w.r[l].get(), nb, nd,
                 static_cast<T>(ch.alpha0), nx);
         });
@@ -981,7 +929,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         const T* bi = (l == 0) ? b : w.b[l].get();
         dispatch_tpr<K>(lv.tpr_p, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            prolong_kernel<T, K, TPR><<<row_grid<TPR>(lv.n), RowTile<TPR>::kThreads, 0, s>>>(
+            prolong_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
                 lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
         });
         count_launch();
@@ -1020,7 +968,7 @@ void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T
     const unsigned g = reduce_grid(n);
     dispatch_tpr<K>(tpr0(), [&](auto tc) {
         constexpr int TPR = decltype(tc)::value;
-        spmv_alpha_kernel<T, K, TPR><<<reduce_grid_rows<TPR>(n), RowTile<TPR>::kThreads, 0, stream>>>(
+        spmv_alpha_kernel<T, K, TPR><<<reduce_grid_rows<TPR>(n), TT, 0, stream>>>(
             n, ptr, col, val, p, ap, partials.get(), counter.get(), rz.get(), frozen.get(), alpha.get());
     });
     count_launch();
@@ -1044,7 +992,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     if (warm) {
         dispatch_tpr<K>(tpr0(), [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            residual64_kernel<K, TPR><<<row_grid<TPR>(n), RowTile<TPR>::kThreads, 0, s>>>(
+            residual64_kernel<K, TPR><<<(n + ReduceTile<TPR>::kRows - 1) / ReduceTile<TPR>::kRows, TT, 0, s>>>(
                 n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), R.get());
         });
         count_launch();
@@ -1122,7 +1070,7 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
     for (; outer < max_outer; ++outer) {
         dispatch_tpr<K>(tpr0(), [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            true_residual_kernel<K, TPR><<<reduce_grid_rows<TPR>(n), RowTile<TPR>::kThreads, 0, s>>>(
+            true_residual_kernel<K, TPR><<<reduce_grid_rows<TPR>(n), TT, 0, s>>>(
                 n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), r32.get(), partials.get(), counter.get(),
                 ref_sq.get(), prm.tolerance, prm.inner_reduction, outer_conv.get(), frozen.get(), rr0.get(), eta.get(),
                 iter_counter.get(), conv_iter.get(), rel.get());
