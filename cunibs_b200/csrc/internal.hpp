@@ -61,8 +61,8 @@ struct Level {
     int tpr_a = 1, tpr_p = 1, tpr_r = 1;
 };
 
-// Sub-lanes per row for an SpMV-shaped kernel over n_rows rows and nnz entries: enough that each
-// walks about eight entries (a power of two up to 32).
+// Sub-lanes per row for an SpMV-shaped kernel over n_rows rows and nnz entries: one while the rows
+// alone fill the GPU, otherwise enough that each walks about eight entries (a power of two up to 32).
 int choose_tpr(int n_rows, long nnz);
 
 struct Hierarchy {

@@ -116,10 +116,11 @@ struct RowSlot {
 };
 
 // Row-times-block for one (row, column): each sub-lane sums its strided share of the row, then the
-// shares are combined in a fixed order: by an XOR butterfly over the sub-lanes when a row group fits
-// in a warp (every sub-lane ends with the same total, since each pair adds the same two values and
-// addition is commutative), otherwise by sub-lane 0 walking them in shared memory. Either way the
-// order depends on TPR alone. Every thread of the block must call this.
+// shares are combined by one fixed pairing tree ((s0+s4)+(s2+s6))+((s1+s5)+(s3+s7)) for TPR = 8:
+// as an XOR butterfly over the sub-lanes when a row group fits in a warp (every sub-lane ends with
+// the same total, since each pair adds the same two values and addition is commutative), otherwise
+// by sub-lane 0 in shared memory. The tree depends on TPR alone, never on K. Every thread of the
+// block must call this.
 template <typename T, int K, int TPR, int ROWS>
 __device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
                                            const T* __restrict__ val, const T* __restrict__ x, int row, int r,
@@ -136,13 +137,20 @@ __device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const in
         for (int off = TPR / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off * K);
         return acc;
     } else {
+        // The same pairing tree as the butterfly above, so the two paths agree bit for bit.
         __shared__ T sh[ROWS][TPR][K];
         sh[r][sub][c] = acc;
         __syncthreads();
         T tot = T(0);
         if (sub == 0) {
+            T a[TPR];
 #pragma unroll
-            for (int q = 0; q < TPR; ++q) tot += sh[r][q][c];
+            for (int q = 0; q < TPR; ++q) a[q] = sh[r][q][c];
+#pragma unroll
+            for (int off = TPR / 2; off > 0; off >>= 1)
+#pragma unroll
+                for (int q = 0; q < off; ++q) a[q] = a[q] + a[q + off];
+            tot = a[0];
         }
         __syncthreads();
         return tot;
