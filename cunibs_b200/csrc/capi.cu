@@ -46,6 +46,8 @@ int pad_width(int k) {
 
 }  // namespace
 
+void cunibs::set_last_error(const std::string& message) { g_last_error = message; }
+
 struct cunibs_context {
     int device = 0;
     Params prm;

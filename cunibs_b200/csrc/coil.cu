@@ -200,6 +200,15 @@ void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double*
     CUNIBS_LAUNCH_CHECK("dadt");
 }
 
+void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
+                    const double* transforms_dev, int k, double didt, float* out, cudaStream_t s) {
+    const int per_block = 4 * kDadtThreads;
+    const dim3 grid((n_nodes + per_block - 1) / per_block, k);
+    dadt_kernel<<<grid, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
+                                             n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out);
+    count_launch();
+}
+
 void dadt_elements(const Mesh& m, const float* nodal, int k, float* elm, cudaStream_t s) {
     const long total = static_cast<long>(m.n_tets) * k;
     element_average_kernel<<<grid_for(total), kBlock, 0, s>>>(nodal, m.tets.get(), m.n_nodes, m.n_tets, k, elm); count_launch();

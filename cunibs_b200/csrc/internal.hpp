@@ -6,6 +6,7 @@
 #include <array>
 #include <cstdint>
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "common.cuh"
@@ -158,6 +159,12 @@ void prep_zdipoles(const double* pos, const double* mom, int n_dip, void* zpacke
 void dadt_nodes_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
                       float* out /* (k, N, 3) */, cudaStream_t s);
 void dadt_elements(const Mesh& m, const float* dadt_nodes, int k, float* dadt_elm /* (k, M, 3) */, cudaStream_t s);
+// The general-moment dA/dt on raw device node coordinates (no Mesh), packed records from prep_dipoles.
+void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
+                    const double* transforms_dev, int k, double didt, float* out, cudaStream_t s);
+
+// Records the calling thread's message for cunibs_last_error.
+void set_last_error(const std::string& message);
 void rhs_block(const Mesh& m, const float* dadt_elm, int k, int k_pad, double* b_red /* (N-1, k_pad) */,
                cudaStream_t s);
 

@@ -180,6 +180,27 @@ int cunibs_select_size4(int n, const int* row_ptr, const int* col_idx, const flo
 /* Gray-matter summary of one |E| field on the context's elements (RegionSlice.summarize). */
 int cunibs_context_summary(cunibs_context* ctx, const float* magnE, int k, double* summary);
 
+/* --- without device allocation ------------------------------------------------------------
+ *
+ * No counterpart in the reference. For callers that cannot have the library allocate GPU memory --
+ * for example a process whose device memory is already reserved by another framework's caching
+ * allocator, or code held to a fixed memory budget set up in advance.
+ *
+ * cunibs_dadt_noalloc computes the same dA/dt as cunibs_context_dadt's general-moment path, for k
+ * placements: nodes_mm (n_nodes, 3), dip_pos_m and dip_moment (n_dip, 3) in the coil frame,
+ * transforms (k, 4, 4) and out (k, n_nodes, 3) are all device pointers on the current device, and the
+ * work is queued on `stream` (a cudaStream_t; NULL is the legacy default stream). The function
+ * allocates nothing: its scratch -- k * n_dip rotated dipole records -- is a fixed array of
+ * CUNIBS_DADT_NOALLOC_MAX_RECORDS records (768 KiB) compiled into the library, which every GPU that
+ * loads the library holds until the process exits. Larger k * n_dip is rejected with CUNIBS_EINVAL.
+ * The first call on a device looks up that array's device address (a one-time cudaGetSymbolAddress,
+ * made with the device current); make that first call before any stream capture. All calls share
+ * the one array, so calls that may overlap on the GPU (different streams, or different host
+ * threads) race on it: order them on one stream. */
+#define CUNIBS_DADT_NOALLOC_MAX_RECORDS 16384
+int cunibs_dadt_noalloc(const double* nodes_mm, int n_nodes, const double* dip_pos_m, const double* dip_moment,
+                        int n_dip, const double* transforms, int k, double didt, float* out, void* stream);
+
 /* --- measurement ------------------------------------------------------------------------ */
 
 /* With timing on, each block solve records CUDA events on the context's stream between its stages
