@@ -1,6 +1,6 @@
 """Benchmark: placements/s of the per-placement field solve on the 1M-tet 10-tissue sphere head.
 
-Workload (BASELINE configs[1]): 8-shell sphere of radius 90 mm with an eye and a muscle cap, Kuhn
+Workload: 8-shell sphere of radius 90 mm with an eye and a muscle cap, Kuhn
 lattice at 2.63 mm (1.0M tetrahedra, 0.18M nodes; a 1.5 mm lattice reaches 1M tetrahedra only at
 a 51 mm radius, so the lattice is coarsened to keep a head-sized sphere), +-0.2 mm seeded node jitter;
 figure-8 coil of 2 x 2048 dipoles; 8 placements on a 15-degree grid of the upper hemisphere solved as
@@ -50,7 +50,7 @@ def workload():
 
 
 def config_dict(mesh, extra=None):
-    d = {"workload": "1M-tet 10-tissue sphere head (configs[1])", "n_tets": int(mesh.n_tets),
+    d = {"workload": "1M-tet 10-tissue sphere head, 8 placements x 2x2048-dipole figure-8", "n_tets": int(mesh.n_tets),
          "n_nodes": int(mesh.n_nodes), "lattice_mm": 2.63, "radius_mm": 90.0, "dipoles": 4096, "block_k": K_BLOCK,
          "placements_per_step": K_BLOCK, "tolerance": TOL}
     if extra:

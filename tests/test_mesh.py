@@ -76,7 +76,7 @@ def test_sphere_head_tags_and_orientation():
 
 
 def test_small_workload_size_matches_config():
-    """64^3 lattice at 3 mm clipped to 90 mm: ~0.68M tets / 0.12M nodes (BASELINE configs[0])."""
+    """64^3 lattice at 3 mm clipped to 90 mm: ~0.68M tets / 0.12M nodes."""
     m = sphere_head(3.0, 90.0, cells=64)
     assert 600_000 < m.n_tets < 700_000 and 100_000 < m.n_nodes < 130_000
 
