@@ -5,7 +5,8 @@ lattice at 2.63 mm (1.0M tetrahedra, 0.18M nodes; a 1.5 mm lattice reaches 1M te
 a 51 mm radius, so the lattice is coarsened to keep a head-sized sphere), +-0.2 mm seeded node jitter;
 figure-8 coil of 2 x 2048 dipoles; 8 placements on a 15-degree grid of the upper hemisphere solved as
 one block (block_k = 8) to relative residual 1e-8. A step is one block of 8 placements: coil
-placement, dA/dt, right-hand side, block PCG, E reconstruction and gray-matter summary.
+placement, dA/dt, right-hand side, block PCG, field recovery (harmonic by default, as Subject.simulate)
+and gray-matter summary.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|plain]
 
@@ -201,7 +202,7 @@ def run_ours(args) -> dict:
 
     def step():
         return ctx.solve_block_device(d_pos.data_ptr(), d_mom.data_ptr(), coil.n_dipoles, d_c.data_ptr(),
-                                      d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, outs)
+                                      d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, outs, recovery=args.recovery)
 
     for _ in range(args.warmup):
         step()
@@ -245,7 +246,7 @@ def run_ours(args) -> dict:
     for _ in range(max(1, min(args.steps, 5))):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        res = ctx.solve_block(coil, centers, handles, dists, 1e6)
+        res = ctx.solve_block(coil, centers, handles, dists, 1e6, recovery=args.recovery)
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     e2e_value = world * K_BLOCK / (statistics.median(e2e_ms) / 1e3)
     h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
@@ -280,7 +281,8 @@ def run_ours(args) -> dict:
         "vs_baseline": None,
         "dtype": "f32 (FP32 PCG/V-cycle/dA-dt) with f64 refinement" if args.precision == "mixed" else "f64",
         "data": "synthetic: seeded sphere head and figure-8 coil",
-        "config": config_dict(mesh, {"precision": args.precision, "l2": "flushed (256 MB write) between steps",
+        "config": config_dict(mesh, {"precision": args.precision, "recovery": args.recovery,
+                                     "l2": "flushed (256 MB write) between steps",
                                      "parallelism": f"replicas x{world}"}),
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -298,24 +300,26 @@ def run_ours(args) -> dict:
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(mesh, coil, sites)
+        line["cpu_baseline"] = cpu_baseline(mesh, coil, sites, args.recovery)
     if dist is not None:
         dist.destroy_process_group()
     return line if rank == 0 else None
 
 
-def cpu_baseline(mesh, coil, sites, n_place=1) -> dict:
+def cpu_baseline(mesh, coil, sites, recovery, n_place=1) -> dict:
     """The FP64 CPU restatement (oracle/) on this host's cores: one placement of the same workload."""
     from oracle import Oracle
 
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
     orc = Oracle(mesh)
+    if recovery != "raw":
+        orc.recovery(recovery)  # per-subject setup, like the operator build
     setup = time.perf_counter() - t0
     c = np.stack([s[0] for s in sites[:n_place]])
     h = np.stack([s[1] for s in sites[:n_place]])
     t1 = time.perf_counter()
-    orc.solve(coil, c, h, np.full(n_place, 4.0), 1e6, tolerance=TOL)
+    orc.solve(coil, c, h, np.full(n_place, 4.0), 1e6, tolerance=TOL, recovery=recovery)
     dt = time.perf_counter() - t1
     return {"value": round(n_place / dt, 4), "unit": "placements/s", "cores": threads, "kind": "port",
             "sample": f"{n_place} placement(s) of the same workload, FP64 AMG-PCG to 1e-8 (setup {setup:.1f} s excluded)"}
@@ -330,23 +334,26 @@ def run_reference(args) -> dict | None:
 
     threads = os.cpu_count() or 1
     orc = Oracle(mesh)
+    if args.recovery != "raw":
+        orc.recovery(args.recovery)
     c = np.stack([s[0] for s in sites])
     h = np.stack([s[1] for s in sites])
     for i in range(args.warmup):
         j = i % len(sites)
-        orc.solve(coil, c[j:j + 1], h[j:j + 1], [4.0], 1e6, tolerance=TOL)
+        orc.solve(coil, c[j:j + 1], h[j:j + 1], [4.0], 1e6, tolerance=TOL, recovery=args.recovery)
     times = []
     for i in range(args.steps):
         j = i % len(sites)
         t1 = time.perf_counter()
-        orc.solve(coil, c[j:j + 1], h[j:j + 1], [4.0], 1e6, tolerance=TOL)
+        orc.solve(coil, c[j:j + 1], h[j:j + 1], [4.0], 1e6, tolerance=TOL, recovery=args.recovery)
         times.append(time.perf_counter() - t1)
     value = len(times) / sum(times)
     return {
         "metric": METRIC, "value": round(value, 4), "unit": "placements/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")),
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * sum(times) / len(times), 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "impl": "reference",
-        "data": "synthetic: seeded sphere head and figure-8 coil", "config": config_dict(mesh),
+        "data": "synthetic: seeded sphere head and figure-8 coil",
+        "config": config_dict(mesh, {"precision": "f64", "recovery": args.recovery}),
         "cpu_baseline": {"value": round(value, 4), "unit": "placements/s", "cores": threads, "kind": "port",
                          "sample": "one placement per step (the workload's 8 sites in turn), FP64 AMG-PCG to 1e-8"},
         "e2e": {"value": round(value, 4), "unit": "placements/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -360,6 +367,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
+    ap.add_argument("--recovery", choices=["harmonic", "spr_tissue", "spr_global", "raw"], default="harmonic")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     line = run_reference(args) if args.impl == "reference" else run_ours(args)

@@ -16,6 +16,7 @@ _lib: C.CDLL | None = None
 
 OK, EINVAL, ENOMEM, ECUDA, ENOCONV, ETIMEOUT, EINTERNAL = range(7)
 PREC_DEFAULT, PREC_PLAIN_FP64, PREC_MIXED = 0, 1, 2
+RECOVERY_CODES = {"raw": 0, "spr_global": 1, "spr_tissue": 2, "harmonic": 3}
 SUMMARY_LEN = 16
 
 _vp = C.c_void_p
@@ -57,6 +58,17 @@ class SolveOpts(C.Structure):
         ("precision", C.c_int),
         ("tolerance", C.c_double),
         ("max_iters", C.c_int),
+        ("recovery", C.c_int),
+    ]
+
+
+class RecoveryInfo(C.Structure):
+    _fields_ = [
+        ("mode", C.c_int),
+        ("n_slots", C.c_int),
+        ("nnz", C.c_longlong),
+        ("n_fallback", C.c_int),
+        ("n_undetermined", C.c_int),
     ]
 
 
@@ -71,6 +83,7 @@ class BlockOut(C.Structure):
         ("v", _vp),
         ("total_iterations", C.c_int),
         ("outer_steps", C.c_int),
+        ("E_slots", _vp),
     ]
 
 
@@ -123,6 +136,9 @@ def load() -> C.CDLL:
         "cunibs_context_vcycle": ([_vp, _vp, _vp, C.c_int, C.c_int], C.c_int),
         "cunibs_select_size4": ([C.c_int, ip, ip, fp, ip, ip], C.c_int),
         "cunibs_context_summary": ([_vp, _vp, C.c_int, _vp], C.c_int),
+        "cunibs_context_recovery": ([_vp, C.c_int, C.POINTER(RecoveryInfo)], C.c_int),
+        "cunibs_context_recovery_array": ([_vp, C.c_int, C.c_char_p, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
+        "cunibs_context_recover": ([_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "cunibs_context_set_timing": ([_vp, C.c_int], C.c_int),
         "cunibs_context_stage_times": ([_vp, dp, C.c_int], C.c_int),
         "cunibs_context_stream": ([_vp, C.POINTER(_vp)], C.c_int),
@@ -283,6 +299,39 @@ class Context:
         check(self._lib.cunibs_context_summary(self.handle, _p(m), m.shape[0], _p(out)))
         return out
 
+    def recovery(self, mode: str) -> dict:
+        """Build (once) the recovery operator of ``mode`` and return its counts."""
+        info = RecoveryInfo()
+        check(self._lib.cunibs_context_recovery(self.handle, RECOVERY_CODES[mode], C.byref(info)))
+        return {"mode": mode, "n_slots": info.n_slots, "nnz": info.nnz, "n_fallback": info.n_fallback,
+                "n_undetermined": info.n_undetermined}
+
+    def recovery_array(self, mode: str, name: str) -> np.ndarray:
+        code = RECOVERY_CODES[mode]
+        n = C.c_longlong()
+        check(self._lib.cunibs_context_recovery_array(self.handle, code, name.encode(), None, 0, C.byref(n)))
+        out = np.empty(n.value, np.float32 if name == "w" else np.int32)
+        check(self._lib.cunibs_context_recovery_array(self.handle, code, name.encode(), _p(out), n.value, C.byref(n)))
+        return out.reshape(-1, 3) if (name == "w" and mode == "harmonic") else out
+
+    def recover(self, mode: str, *, v=None, dadt_nodes=None, elements=None):
+        """cunibs_context_recover on host data: (E_slots (k,S,3), E (k,M,3), magnE (k,M))."""
+        info = self.recovery(mode)
+        va = da = ea = None
+        if mode == "harmonic":
+            va = np.ascontiguousarray(v, np.float64).reshape(-1, self.n_nodes)
+            da = np.ascontiguousarray(dadt_nodes, np.float32).reshape(-1, self.n_nodes, 3)
+            k = va.shape[0]
+        else:
+            ea = np.ascontiguousarray(elements, np.float32).reshape(-1, self.n_tets, 3)
+            k = ea.shape[0]
+        slots = np.empty((k, info["n_slots"], 3), np.float32)
+        E = np.empty((k, self.n_tets, 3), np.float32)
+        mag = np.empty((k, self.n_tets), np.float32)
+        check(self._lib.cunibs_context_recover(self.handle, RECOVERY_CODES[mode], k, _p(va), _p(da), _p(ea),
+                                               _p(slots), _p(E), _p(mag)))
+        return slots, E, mag
+
     def set_timing(self, on: bool = True) -> None:
         check(self._lib.cunibs_context_set_timing(self.handle, int(bool(on))))
 
@@ -297,11 +346,12 @@ class Context:
         return int(out.value or 0)
 
     def solve_block_device(self, pos, mom, n_dip, centers, handles, dists, k, didt, out_ptrs, *, block_width=0,
-                           precision=PREC_DEFAULT, tolerance=0.0, max_iters=0) -> tuple[int, int]:
+                           precision=PREC_DEFAULT, tolerance=0.0, max_iters=0, recovery="raw") -> tuple[int, int]:
         """cunibs_solve_block_device on raw device pointers (ints); out_ptrs maps output names to pointers."""
         out = BlockOut(out_ptrs.get("transforms"), out_ptrs.get("summary"), out_ptrs.get("iterations"),
-                       out_ptrs.get("relres"), out_ptrs.get("magnE"), out_ptrs.get("E"), out_ptrs.get("v"), 0, 0)
-        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters))
+                       out_ptrs.get("relres"), out_ptrs.get("magnE"), out_ptrs.get("E"), out_ptrs.get("v"), 0, 0,
+                       out_ptrs.get("E_slots"))
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery])
         check(self._lib.cunibs_solve_block_device(self.handle, pos, mom, int(n_dip), centers, handles, dists, int(k),
                                                   float(didt), C.byref(opts), C.byref(out)))
         return out.total_iterations, out.outer_steps
@@ -311,7 +361,8 @@ class Context:
         check(self._lib.cunibs_context_set_conductivity(self.handle, s.ctypes.data_as(C.POINTER(C.c_double))))
 
     def solve_block(self, coil, centers, handles, dists, didt, *, block_width=0, precision=PREC_DEFAULT,
-                    tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False) -> dict:
+                    tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False,
+                    recovery="raw", nodal=False) -> dict:
         """One block of k placements through cunibs_solve_block (host buffers in and out)."""
         centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
         k = centers.shape[0]
@@ -327,10 +378,15 @@ class Context:
             "magnE": np.empty((k, self.n_tets), np.float32) if magnitude else None,
             "E": np.empty((k, self.n_tets, 3), np.float32) if vectors else None,
             "v": np.empty((k, self.n_nodes)) if potential else None,
+            "E_slots": None,
         }
+        if nodal:
+            if recovery == "raw":
+                raise ValueError("nodal=True needs a recovery mode")
+            res["E_slots"] = np.empty((k, self.recovery(recovery)["n_slots"], 3), np.float32)
         out = BlockOut(_p(res["transform"]), _p(res["summary"]), _p(res["iterations"]), _p(res["relative_residual"]),
-                       _p(res["magnE"]), _p(res["E"]), _p(res["v"]), 0, 0)
-        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters))
+                       _p(res["magnE"]), _p(res["E"]), _p(res["v"]), 0, 0, _p(res["E_slots"]))
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery])
         check(self._lib.cunibs_solve_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
                                            _p(dists), k, float(didt), C.byref(opts), C.byref(out)))
         res["total_iterations"] = out.total_iterations

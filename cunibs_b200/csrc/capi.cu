@@ -61,6 +61,9 @@ struct cunibs_context {
     DevArray<int> deg;
     DevArray<unsigned char> dip_packed, zdip_packed;
     DevArray<float> dadt_nodes, dadt_elm, magn, E;
+    // Field-recovery operators, built on first use per mode, and their block workspace.
+    std::unique_ptr<RecoveryOp> rec[4];
+    DevArray<float> e_slots, e_raw;
     // Stage timing (CUDA events on the context stream), enabled by cunibs_context_set_timing.
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -68,6 +71,17 @@ struct cunibs_context {
 
     void mark(int i) {
         if (timing) CUNIBS_CHECK(cudaEventRecord(ev[i], stream));
+    }
+
+    RecoveryOp& recovery(int mode) {
+        if (mode < kRecSprGlobal || mode > kRecHarmonic) fail(kEInval, "unknown recovery mode " + std::to_string(mode));
+        if (!rec[mode]) {
+            auto op = std::make_unique<RecoveryOp>();
+            build_recovery(mesh, *op, mode, stream);
+            CUNIBS_CHECK(cudaStreamSynchronize(stream));
+            rec[mode] = std::move(op);
+        }
+        return *rec[mode];
     }
 
     void rebuild_hierarchy() {
@@ -119,6 +133,9 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
     require(K >= k, "block_width must be at least the number of placements");
     K_out = K;
     const Params prm = resolve(c, opts);
+    const int rec_mode = opts ? opts->recovery : kRecRaw;
+    require(rec_mode >= kRecRaw && rec_mode <= kRecHarmonic, "unknown recovery mode");
+    RecoveryOp* op = rec_mode == kRecRaw ? nullptr : &c->recovery(rec_mode);
     Mesh& m = c->mesh;
     cudaStream_t s = c->stream;
     const int n_red = m.n_nodes - 1;
@@ -181,7 +198,20 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
     c->mark(4);
     c->magn.reserve(static_cast<std::size_t>(m.n_tets) * k);
     if (want_E) c->E.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
-    reconstruct_block(m, c->X.get(), k, K, c->dadt_elm.get(), want_E ? c->E.get() : nullptr, c->magn.get(), s);
+    if (op == nullptr) {
+        reconstruct_block(m, c->X.get(), k, K, c->dadt_elm.get(), want_E ? c->E.get() : nullptr, c->magn.get(), s);
+    } else {
+        // The potential-consuming mode never forms the raw field (fem/solve.py:943-965).
+        const float* e_elem = nullptr;
+        if (rec_mode != kRecHarmonic) {
+            c->e_raw.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
+            reconstruct_block(m, c->X.get(), k, K, c->dadt_elm.get(), c->e_raw.get(), c->magn.get(), s);
+            e_elem = c->e_raw.get();
+        }
+        c->e_slots.reserve(static_cast<std::size_t>(op->n_slots) * 3 * k);
+        apply_recovery(m, *op, c->X.get(), K, c->dadt_nodes.get(), e_elem, k, c->e_slots.get(),
+                       want_E ? c->E.get() : nullptr, c->magn.get(), s);
+    }
     c->summary.reserve(static_cast<std::size_t>(kSummaryLen) * k);
     gm_summary(m, c->magn.get(), k, c->summary.get(), c->sw, s);
     c->mark(5);
@@ -197,6 +227,13 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
 
 void copy_out(void* dst, const void* src, std::size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
     if (dst && bytes) CUNIBS_CHECK(cudaMemcpyAsync(dst, src, bytes, kind, s));
+}
+
+// Bytes of the recovered slot field of a block solved with these options (0 for the raw field).
+std::size_t slot_bytes(const cunibs_context* c, const cunibs_solve_opts* opts, int k) {
+    const int mode = opts ? opts->recovery : kRecRaw;
+    if (mode == kRecRaw || !c->rec[mode]) return 0;
+    return sizeof(float) * 3 * static_cast<std::size_t>(c->rec[mode]->n_slots) * k;
 }
 
 }  // namespace
@@ -330,6 +367,7 @@ int cunibs_solve_block(cunibs_context* c, const double* dip_pos_m, const double*
         copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToHost, s);
         copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
         copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
+        copy_out(out->E_slots, c->e_slots.get(), slot_bytes(c, opts, k), cudaMemcpyDeviceToHost, s);
         if (out->v) {
             c->v.reserve(static_cast<std::size_t>(m.n_nodes) * k);
             scatter_potential(m, c->X.get(), k, K, c->v.get(), s);
@@ -362,6 +400,7 @@ int cunibs_solve_block_device(cunibs_context* c, const double* dip_pos_m, const 
         copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToDevice, s);
         copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
         copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
+        copy_out(out->E_slots, c->e_slots.get(), slot_bytes(c, opts, k), cudaMemcpyDeviceToDevice, s);
         if (out->v) scatter_potential(m, c->X.get(), k, K, out->v, s);
         CUNIBS_CHECK(cudaStreamSynchronize(s));
         if (out->iterations)
@@ -433,6 +472,103 @@ int cunibs_context_array(const cunibs_context* c, const char* name, int level, v
             const std::size_t nb = std::min<std::size_t>(count, static_cast<std::size_t>(cap)) * elem;
             CUNIBS_CHECK(cudaMemcpy(out, src, nb, cudaMemcpyDeviceToHost));
         }
+    });
+}
+
+int cunibs_context_recovery(cunibs_context* c, int mode, cunibs_recovery_info* out) {
+    return guarded([&] {
+        require(c && out, "NULL argument");
+        DeviceGuard dg(c->device);
+        const RecoveryOp& op = c->recovery(mode);
+        out->mode = mode;
+        out->n_slots = op.n_slots;
+        out->nnz = op.mode == kRecSprGlobal ? 4LL * c->mesh.n_tets : static_cast<long long>(op.nnz);
+        out->n_fallback = op.n_fallback;
+        out->n_undetermined = op.n_undetermined;
+    });
+}
+
+int cunibs_context_recovery_array(cunibs_context* c, int mode, const char* name, void* out, long long cap,
+                                  long long* len) {
+    return guarded([&] {
+        require(c && name && len, "NULL argument");
+        DeviceGuard dg(c->device);
+        const RecoveryOp& op = c->recovery(mode);
+        const Mesh& m = c->mesh;
+        const bool nodes = mode == kRecSprGlobal, harmonic = mode == kRecHarmonic;
+        const std::string n(name);
+        const std::size_t nc = 4 * static_cast<std::size_t>(m.n_tets);
+        std::vector<unsigned char> host;
+        const void* src = nullptr;
+        std::size_t count = 0, elem = 4;
+        auto pick = [&](const void* p, std::size_t cnt) {
+            src = p;
+            count = cnt;
+        };
+        if (n == "ptr") pick(nodes ? m.n2c_ptr.get() : op.ptr.get(), op.n_slots + 1);
+        else if (n == "idx") pick(nodes ? m.n2c_idx.get() : (harmonic ? op.pidx.get() : op.idx.get()),
+                                  harmonic ? op.nnz : nc);
+        else if (n == "slot_of_corner") pick(recovery_slot_of_corner(m, op), nc);
+        else if (n == "slot_node") pick(op.slot_node.get(), op.n_slots);
+        else if (n == "slot_tag") pick(op.slot_tag.get(), nodes ? 0 : op.n_slots);
+        else if (n == "status") pick(op.status.get(), harmonic ? op.n_slots : 0);
+        else if (n == "is_boundary") pick(op.is_boundary.get(), harmonic ? 0 : m.n_nodes);
+        else if (n == "w" && !harmonic) pick(op.w.get(), nc);
+        else if (n == "w") {
+            // Unpacked from the {w_x, w_y, w_z, node} records: (nnz, 3).
+            std::vector<float4> packed(op.nnz);
+            CUNIBS_CHECK(cudaMemcpy(packed.data(), op.wq.get(), sizeof(float4) * op.nnz, cudaMemcpyDeviceToHost));
+            host.resize(sizeof(float) * 3 * op.nnz);
+            float* f = reinterpret_cast<float*>(host.data());
+            for (std::int64_t i = 0; i < op.nnz; ++i) {
+                f[3 * i] = packed[i].x;
+                f[3 * i + 1] = packed[i].y;
+                f[3 * i + 2] = packed[i].z;
+            }
+            count = 3 * static_cast<std::size_t>(op.nnz);
+        } else fail(kEInval, "unknown recovery array name: " + n);
+        *len = static_cast<long long>(count);
+        if (out && count) {
+            const std::size_t nb = std::min<std::size_t>(count, static_cast<std::size_t>(cap)) * elem;
+            if (src) CUNIBS_CHECK(cudaMemcpy(out, src, nb, cudaMemcpyDeviceToHost));
+            else std::memcpy(out, host.data(), nb);
+        }
+    });
+}
+
+int cunibs_context_recover(cunibs_context* c, int mode, int k, const double* v, const float* dadt_nodes,
+                           const float* E_elem, float* E_slots, float* E, float* magnE) {
+    return guarded([&] {
+        require(c && E_slots && magnE, "NULL argument");
+        require(k >= 1 && k <= 16, "k must be in [1, 16]");
+        DeviceGuard dg(c->device);
+        RecoveryOp& op = c->recovery(mode);
+        const Mesh& m = c->mesh;
+        cudaStream_t s = c->stream;
+        DevArray<double> x;
+        DevArray<float> da, ee, slots(static_cast<std::size_t>(op.n_slots) * 3 * k),
+            mag(static_cast<std::size_t>(m.n_tets) * k), Ed;
+        if (E) Ed.resize(static_cast<std::size_t>(m.n_tets) * 3 * k);
+        if (mode == kRecHarmonic) {
+            require(v && dadt_nodes, "harmonic recovery reads v and dadt_nodes");
+            // (k, N) potentials into the solver's grounded row-major (N-1, k) layout.
+            std::vector<double> red(static_cast<std::size_t>(m.n_nodes - 1) * k);
+            for (int col = 0; col < k; ++col)
+                for (int i = 0, r = 0; i < m.n_nodes; ++i) {
+                    if (i == m.ground) continue;
+                    red[static_cast<std::size_t>(r++) * k + col] = v[static_cast<std::size_t>(col) * m.n_nodes + i];
+                }
+            x.upload(red.data(), red.size(), s);
+            da.upload(dadt_nodes, static_cast<std::size_t>(m.n_nodes) * 3 * k, s);
+        } else {
+            require(E_elem != nullptr, "SPR recovery reads E_elem");
+            ee.upload(E_elem, static_cast<std::size_t>(m.n_tets) * 3 * k, s);
+        }
+        apply_recovery(m, op, x.get(), k, da.get(), ee.get(), k, slots.get(), E ? Ed.get() : nullptr, mag.get(), s);
+        copy_out(E_slots, slots.get(), sizeof(float) * slots.size(), cudaMemcpyDeviceToHost, s);
+        copy_out(magnE, mag.get(), sizeof(float) * mag.size(), cudaMemcpyDeviceToHost, s);
+        if (E) copy_out(E, Ed.get(), sizeof(float) * Ed.size(), cudaMemcpyDeviceToHost, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
     });
 }
 

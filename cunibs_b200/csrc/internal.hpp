@@ -183,4 +183,28 @@ struct SummaryWork {
 void gm_summary(const Mesh& m, const float* magnE, int k, double* summary_dev /* (k,16) */, SummaryWork& w,
                 cudaStream_t s);
 
+// Field recovery (recovery.cu). Modes match CUNIBS_RECOVERY_*.
+enum RecoveryMode : int { kRecRaw = 0, kRecSprGlobal = 1, kRecSprTissue = 2, kRecHarmonic = 3 };
+
+struct RecoveryOp {
+    int mode = kRecRaw;
+    int n_slots = 0;
+    std::int64_t nnz = 0;
+    // SPR rows: corner ids per slot (spr_global uses the mesh's node-to-corner CSR instead).
+    DevArray<int> ptr, idx;
+    DevArray<float> w;          // SPR: one weight per corner entry
+    // Harmonic rows (ptr is then the patch CSR): patch node per entry and {w_x, w_y, w_z, node}.
+    DevArray<int> pidx;
+    DevArray<float4> wq;
+    DevArray<int> slot_of_corner;  // (4M); spr_global samples through the mesh's own tets
+    DevArray<int> slot_node, slot_tag, status, is_boundary;
+    int n_fallback = 0, n_undetermined = 0;
+};
+void build_recovery(const Mesh& m, RecoveryOp& op, int mode, cudaStream_t s);
+const int* recovery_slot_of_corner(const Mesh& m, const RecoveryOp& op);
+// Recovered E on slots (k, n_slots, 3) and at the barycentres: E (k,M,3) or null, magn (k,M).
+// Harmonic reads the solver block x_red (N-1, K) and dadt_nodes (k,N,3); SPR reads e_elem (k,M,3).
+void apply_recovery(const Mesh& m, const RecoveryOp& op, const double* x_red, int K, const float* dadt_nodes,
+                    const float* e_elem, int k, float* e_slots, float* E, float* magn, cudaStream_t s);
+
 }  // namespace cunibs

@@ -19,6 +19,7 @@
 // ||r||/||b|| <= tol), block_cg.cu:188-226 (freeze via alpha = beta = 0), vcycle.cu:560-648
 // (cycle order: Chebyshev pre-smooth from zero, residual, restrict; dense coarse solve; prolongate,
 // Chebyshev post-smooth).
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -1137,6 +1138,10 @@ SolverPtr make_solver(const Hierarchy& h, const Params& p) {
     SolverPtr sv(new Solver());
     sv->h = &h;
     sv->n = h.levels.empty() ? h.nc : h.levels[0].n;
+    // CUNIBS_SOLVER_HOST_LOOP=1 runs the same iteration graphs under a host loop instead of a
+    // device-side WHILE node, for profilers that do not step into conditional graph bodies.
+    const char* host_loop = std::getenv("CUNIBS_SOLVER_HOST_LOOP");
+    sv->while_unsupported = host_loop != nullptr && host_loop[0] == '1';
     CUNIBS_CHECK(cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking));
     return sv;
 }

@@ -98,6 +98,8 @@ class Subject:
         self._ctx: _native.Context | None = None
         self._ordered: HeadMesh | None = None
         self._host_metrics: tuple[np.ndarray, np.ndarray, np.ndarray] | None = None
+        self._host_slots: dict[str, tuple[np.ndarray, np.ndarray | None]] = {}
+        self._host_tets: np.ndarray | None = None
         self._tolerance = float(tolerance)
         self._max_iters = int(max_iters)
         self._precision = precision
@@ -116,6 +118,8 @@ class Subject:
             self._ctx = None
             self._ordered = None
             self._host_metrics = None
+            self._host_slots.clear()
+            self._host_tets = None
 
     def __enter__(self) -> Subject:
         return self
@@ -153,21 +157,50 @@ class Subject:
                 self._host_metrics = (vols, ctx.array("tet_tags"), ctx.array("bary").reshape(-1, 3))
             return self._host_metrics
 
+    def _host_slot_maps(self, recovery: str) -> tuple[np.ndarray, np.ndarray | None]:
+        """Host (slot_node, slot_tag) of a recovery mode, shared by every result it produces."""
+        with self._lock:
+            if recovery not in self._host_slots:
+                ctx = self.context
+                tags = ctx.recovery_array(recovery, "slot_tag")
+                self._host_slots[recovery] = (ctx.recovery_array(recovery, "slot_node"),
+                                              tags if recovery != "spr_global" else None)
+            return self._host_slots[recovery]
+
+    def _host_tet_nodes(self) -> np.ndarray:
+        with self._lock:
+            if self._host_tets is None:
+                self._host_tets = self.context.array("tet_nodes").reshape(-1, 4)
+            return self._host_tets
+
+    def recovery_operator(self, recovery: str) -> dict:
+        """Build (once) and describe the patch weights of ``recovery`` (slot and fallback counts)."""
+        recovery = validate_recovery(recovery)
+        if recovery == "raw":
+            raise ValueError("The raw mode has no recovery operator to build.")
+        with self._lock:
+            return self.context.recovery(recovery)
+
     def _iter_reduced(self, coil: Coil, sites: Sequence[Placement], didt: float, block_k: int | None,
                       retain: _Retain, recovery: str) -> Iterator[FieldResult]:
         ctx = self.context
         chunk_k = MAX_BLOCK if block_k is None else max(1, min(MAX_BLOCK, int(block_k)))
+        slot_node, slot_tag = self._host_slot_maps(recovery) if retain.nodal else (None, None)
+        # Per-node slots need the connectivity to say which nodes a region touches.
+        tet_nodes = self._host_tet_nodes() if retain.nodal and slot_tag is None else None
         for start in range(0, len(sites), chunk_k):
             chunk = sites[start : start + chunk_k]
             centers = np.stack([s.center_mm for s in chunk])
             handles = np.stack([s.handle_mm for s in chunk])
             dists = np.array([s.distance_mm for s in chunk])
             try:
-                out = ctx.solve_block(coil, centers, handles, dists, didt, magnitude=retain.magnitude,
-                                      vectors=retain.vectors, potential=retain.potential)
+                with self._lock:
+                    out = ctx.solve_block(coil, centers, handles, dists, didt, magnitude=retain.magnitude,
+                                          vectors=retain.vectors, potential=retain.potential, recovery=recovery,
+                                          nodal=retain.nodal)
             except _native.ConvergenceFailure as exc:
                 raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
-            host = self._host_metric_inputs() if retain.magnitude else None
+            host = self._host_metric_inputs() if (retain.magnitude or retain.nodal) else None
             for i, site in enumerate(chunk):
                 yield FieldResult(
                     summary=metrics.from_summary_row(out["summary"][i]),
@@ -184,29 +217,38 @@ class Subject:
                     recovery=recovery,
                     iterations=int(out["iterations"][i]),
                     relative_residual=float(out["relative_residual"][i]),
+                    n_nodes=ctx.n_nodes if retain.nodal else None,
+                    E_slots=out["E_slots"][i] if retain.nodal else None,
+                    slot_node=slot_node,
+                    slot_tag=slot_tag,
+                    tet_nodes=tet_nodes,
                 )
 
     def iter_simulate(self, coil: Coil, placements: Sequence[Placement], didt: float = 1e6, *,
                       magnitude: bool = False, vectors: bool = False, potential: bool = False,
-                      nodal: bool = False, recovery: str = "raw", block_k: int | None = None) -> Iterator[FieldResult]:
+                      nodal: bool = False, recovery: str = "harmonic", block_k: int | None = None) -> Iterator[FieldResult]:
         """Stream one FieldResult per placement, in order, solving blocks of ``block_k`` together.
 
         A placement's result does not depend on ``block_k`` or on which placements share its
-        block. Arguments are validated here, before the first result is requested.
+        block. ``recovery`` selects how the reported field is derived from the solve ("harmonic",
+        the default; "spr_tissue", "spr_global" or "raw"); ``nodal`` keeps the recovered field on its
+        slots (read it with :meth:`FieldResult.nodal_field`). Arguments are validated here, before
+        the first result is requested.
         """
         sites = _sites(placements, "iter_simulate")
         recovery = validate_recovery(recovery)
-        if nodal:
-            raise ValueError("nodal=True needs a recovered nodal field, which this build does not produce yet")
-        if recovery != "raw":
-            raise ValueError(f"recovery={recovery!r} is not available in this build; use recovery='raw'")
+        if nodal and recovery == "raw":
+            raise ValueError(
+                "nodal=True needs a recovery mode: the raw per-tetrahedron field has no nodal form. "
+                "Drop recovery='raw' to take the default, or name another mode."
+            )
         if not isinstance(coil, Coil):
             raise TypeError("coil must be a cunibs_b200.Coil")
         retain = _Retain(bool(magnitude), bool(vectors), bool(potential), bool(nodal))
         return self._iter_reduced(coil, sites, float(didt), block_k, retain, recovery)
 
     def simulate(self, coil: Coil, placement: Placement, didt: float = 1e6, *, magnitude: bool = False,
-                 vectors: bool = False, potential: bool = False, nodal: bool = False, recovery: str = "raw",
+                 vectors: bool = False, potential: bool = False, nodal: bool = False, recovery: str = "harmonic",
                  block_k: int | None = None) -> FieldResult:
         if not isinstance(placement, Placement):
             raise TypeError("simulate() takes a single Placement; use iter_simulate() for a sequence.")
@@ -234,7 +276,41 @@ class FieldResult:
     recovery: str = "raw"
     iterations: int = 0
     relative_residual: float = 0.0
+    n_nodes: int | None = None
+    E_slots: npt.NDArray[np.float32] | None = None
+    slot_node: npt.NDArray[np.int32] | None = None
+    slot_tag: npt.NDArray[np.int32] | None = None
+    tet_nodes: npt.NDArray[np.int32] | None = None
     _summaries: dict = field(default_factory=dict, repr=False)
+
+    def nodal_field(self, region: metrics.Region = "gray_matter") -> npt.NDArray[np.float32]:
+        """The recovered field at the mesh nodes on ``region``'s side of any boundary
+        (reference simulation.py:709-747): ``(n_nodes, 3)``, NaN where ``region`` does not reach.
+
+        For the tissue-restricted modes the field lives on (node, tissue) slots and is two-valued
+        at a conductivity jump, so ``region="all"`` is rejected for them.
+        """
+        if self.E_slots is None or self.slot_node is None or self.n_nodes is None:
+            raise ValueError("nodal_field needs the recovered nodal field, which this result did not retain. "
+                             "Re-run with nodal=True.")
+        if self.slot_tag is not None and region == "all":
+            raise ValueError(f"nodal_field(region='all') is ambiguous for recovery={self.recovery!r}: its field is "
+                             "two-valued at a tissue boundary, so a node there has one value per tissue. "
+                             "Name a tissue label instead.")
+        if self.slot_tag is not None:
+            keep = self.slot_tag == metrics.region_tag(region)
+        elif region == "all":
+            keep = slice(None)
+        else:
+            if self.tet_nodes is None or self.tet_tags is None:
+                raise ValueError("nodal_field for a specific region needs the mesh connectivity, which this result "
+                                 "did not retain. Re-run with nodal=True.")
+            touched = np.zeros(self.n_nodes, dtype=bool)
+            touched[self.tet_nodes[metrics.region_mask(self.tet_tags, region)]] = True
+            keep = touched[self.slot_node]
+        out = np.full((self.n_nodes, 3), np.nan, dtype=np.float32)
+        out[self.slot_node[keep]] = self.E_slots[keep]
+        return out
 
     def _require_magnitude(self, what: str) -> np.ndarray:
         if self.magnE is None:
@@ -268,8 +344,11 @@ class FieldResult:
 
     def save(self, path: str | Path) -> None:
         """Write the result to a self-contained ``.npz`` (arrays not retained are absent)."""
-        arrays = {k: getattr(self, k) for k in ("magnE", "E", "v", "vols", "tet_tags", "barycenters_mm")
+        arrays = {k: getattr(self, k) for k in ("magnE", "E", "v", "vols", "tet_tags", "barycenters_mm", "E_slots",
+                                                  "slot_node", "slot_tag", "tet_nodes")
                   if getattr(self, k) is not None}
+        if self.n_nodes is not None:
+            arrays["n_nodes"] = np.int64(self.n_nodes)
         s = self.summary
         np.savez_compressed(
             Path(path), transform=self.transform, format_version=_FORMAT_VERSION, recovery=self.recovery,
@@ -301,4 +380,6 @@ class FieldResult:
                        placement=Placement(z["placement_center_mm"], z["placement_handle_mm"], float(z["placement_distance_mm"])),
                        coil_name=str(z["coil_name"]), didt=float(z["didt"]), vols=opt("vols"), tet_tags=opt("tet_tags"),
                        barycenters_mm=opt("barycenters_mm"), recovery=str(z["recovery"]),
-                       iterations=int(z["iterations"]), relative_residual=float(z["relative_residual"]))
+                       iterations=int(z["iterations"]), relative_residual=float(z["relative_residual"]),
+                       n_nodes=int(z["n_nodes"]) if "n_nodes" in z.files else None, E_slots=opt("E_slots"),
+                       slot_node=opt("slot_node"), slot_tag=opt("slot_tag"), tet_nodes=opt("tet_nodes"))

@@ -33,6 +33,15 @@ extern "C" {
 #define CUNIBS_PREC_PLAIN_FP64 1 /* FP64 PCG over an FP64 V-cycle */
 #define CUNIBS_PREC_MIXED 2      /* FP32 PCG + FP32 V-cycle inside FP64 iterative refinement */
 
+/* Field recovery: how the reported E is derived from the solve (fem/recovery.py:74-113).
+ * RAW is the per-tetrahedron field; SPR_GLOBAL a linear patch fit per node; SPR_TISSUE the same per
+ * (node, tissue) slot; HARMONIC the potential fitted per (node, tissue) slot in harmonic
+ * polynomials and differentiated, plus the exact nodal dA/dt (the reference's default). */
+#define CUNIBS_RECOVERY_RAW 0
+#define CUNIBS_RECOVERY_SPR_GLOBAL 1
+#define CUNIBS_RECOVERY_SPR_TISSUE 2
+#define CUNIBS_RECOVERY_HARMONIC 3
+
 /* Summary layout, one row of CUNIBS_SUMMARY_LEN doubles per placement (metrics.py:28-37,209-243). */
 #define CUNIBS_SUMMARY_PEAK 0       /* peak |E| in gray matter, V/m */
 #define CUNIBS_SUMMARY_PEAK_LOC 1   /* 3 values: barycentre of the peak element, mm */
@@ -82,6 +91,7 @@ typedef struct {
     int precision;     /* CUNIBS_PREC_DEFAULT or a CUNIBS_PREC_* override */
     double tolerance;  /* <= 0: context default */
     int max_iters;     /* <= 0: context default */
+    int recovery;      /* CUNIBS_RECOVERY_*; 0 = raw. magnE, E and the summary describe this field */
 } cunibs_solve_opts;
 
 /* Outputs of a block solve of k placements. Required: transforms, summary. Optional (NULL to
@@ -97,7 +107,16 @@ typedef struct {
     double* v;          /* (k, n_nodes) potential, grounded node = 0 */
     int total_iterations; /* filled: iterations the block ran */
     int outer_steps;      /* filled: FP64 refinement steps (mixed) */
+    float* E_slots;     /* (k, n_slots, 3) recovered field on its slots (NULL to skip; recovery only) */
 } cunibs_block_out;
+
+typedef struct {
+    int mode;
+    int n_slots;        /* nodes (SPR_GLOBAL) or (node, tissue) pairs */
+    long long nnz;      /* operator entries: corners (SPR) or patch nodes (HARMONIC) */
+    int n_fallback;     /* SPR: slots on the volume average; HARMONIC: slots below the harmonic rungs */
+    int n_undetermined; /* HARMONIC: slots with no gradient (E = -dA/dt there) */
+} cunibs_recovery_info;
 
 int cunibs_version(void);
 const char* cunibs_last_error(void);
@@ -176,6 +195,24 @@ int cunibs_context_vcycle(cunibs_context* ctx, const double* r, double* z, int k
  * aggregates: (n) out; *n_coarse receives the aggregate count. */
 int cunibs_select_size4(int n, const int* row_ptr, const int* col_idx, const float* values, int* aggregates,
                         int* n_coarse);
+
+/* Builds (once per context and mode) and describes a recovery operator (build_recovery_operator,
+ * fem/recovery.py:445-453): slot maps, patches, the boundary marks and the patch weights. */
+int cunibs_context_recovery(cunibs_context* ctx, int mode, cunibs_recovery_info* out);
+
+/* Copies an array of a recovery operator to host memory. int32: "ptr" (n_slots+1), "idx" (corner ids
+ * for SPR, patch nodes for HARMONIC), "slot_of_corner" (4*n_tets), "slot_node", "slot_tag" (empty
+ * for SPR_GLOBAL), "status" (HARMONIC: rung per slot, 0 cubic .. 3 none), "is_boundary" (SPR, per
+ * node); float32: "w" (SPR: one per entry; HARMONIC: 3 per entry). */
+int cunibs_context_recovery_array(cunibs_context* ctx, int mode, const char* name, void* out, long long cap,
+                                  long long* len);
+
+/* Applies a recovery operator to k columns of caller data (apply_recovery_into,
+ * fem/recovery.py:482-525): HARMONIC reads v (k, n_nodes) float64 (the grounded node is taken as 0)
+ * and dadt_nodes (k, n_nodes, 3); SPR reads E_elem (k, n_tets, 3). Writes E_slots (k, n_slots, 3),
+ * E (k, n_tets, 3; may be NULL) and magnE (k, n_tets). */
+int cunibs_context_recover(cunibs_context* ctx, int mode, int k, const double* v, const float* dadt_nodes,
+                           const float* E_elem, float* E_slots, float* E, float* magnE);
 
 /* Gray-matter summary of one |E| field on the context's elements (RegionSlice.summarize). */
 int cunibs_context_summary(cunibs_context* ctx, const float* magnE, int k, double* summary);

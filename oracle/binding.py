@@ -14,6 +14,7 @@ _LIB_PATH = _HERE / "_build" / "liboracle.so"
 _lib: C.CDLL | None = None
 
 SUMMARY_LEN = 16
+RECOVERY_CODES = {"raw": 0, "spr_global": 1, "spr_tissue": 2, "harmonic": 3}
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
@@ -62,7 +63,11 @@ def _load() -> C.CDLL:
     lib.orc_vcycle_apply.argtypes = [C.c_void_p, _dp, _dp, C.c_int]
     vp = C.c_void_p
     lib.orc_solve.argtypes = [C.c_void_p, _dp, _dp, C.c_int, _dp, _dp, _dp, C.c_int, C.c_double, C.c_double, C.c_int,
-                              vp, vp, vp, vp, vp, vp, vp, C.c_char_p, C.c_int]
+                              C.c_int, vp, vp, vp, vp, vp, vp, vp, C.c_char_p, C.c_int]
+    lib.orc_recovery_build.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_int]
+    lib.orc_recovery_i32.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.c_long)]
+    lib.orc_recovery_w.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.c_long)]
+    lib.orc_recovery_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
     lib.orc_select_size4.argtypes = [C.c_int, _ip, _ip, _fp, _ip]
     lib.orc_select_size4.restype = C.c_int
     lib.orc_l1_dinv_f32.argtypes = [C.c_int, _ip, _ip, _fp, _fp]
@@ -142,7 +147,46 @@ class Oracle:
             raise ValueError("placement failed")
         return T.reshape(k, 4, 4), deg
 
-    def solve(self, coil, centers, handles, dists, didt=1e6, tolerance=1e-10, max_iters=2000):
+    def recovery(self, mode: str) -> dict:
+        """Build (once) and return a recovery operator's arrays and counts."""
+        code = RECOVERY_CODES[mode]
+        err = C.create_string_buffer(512)
+        if self._lib.orc_recovery_build(self._h, code, err, 512) != 0:
+            raise ValueError(err.value.decode())
+        out = {}
+        for name in ("ptr", "idx", "slot_of_corner", "slot_node", "slot_tag", "status", "is_boundary", "counts"):
+            p = C.POINTER(C.c_int)()
+            n = C.c_long()
+            if self._lib.orc_recovery_i32(self._h, code, name.encode(), C.byref(p), C.byref(n)) != 0:
+                raise KeyError(name)
+            out[name] = np.ctypeslib.as_array(p, shape=(n.value,)).copy() if n.value else np.empty(0, np.int32)
+        pw = C.POINTER(C.c_float)()
+        n = C.c_long()
+        self._lib.orc_recovery_w(self._h, code, C.byref(pw), C.byref(n))
+        w = np.ctypeslib.as_array(pw, shape=(n.value,)).copy() if n.value else np.empty(0, np.float32)
+        out["w"] = w.reshape(-1, 3) if mode == "harmonic" else w
+        out["n_slots"], out["n_fallback"], out["n_undetermined"] = (int(x) for x in out.pop("counts"))
+        return out
+
+    def recovery_apply(self, mode: str, *, v=None, dadt_nodes=None, elements=None):
+        """The CUDA apply kernels' arithmetic on given inputs: (E_slots, E, magnE), k columns."""
+        code = RECOVERY_CODES[mode]
+        op = self.recovery(mode)
+        if mode == "harmonic":
+            v = np.ascontiguousarray(v, np.float64).reshape(-1, self.n_nodes)
+            dadt_nodes = np.ascontiguousarray(dadt_nodes, np.float32).reshape(-1, self.n_nodes, 3)
+            k = v.shape[0]
+        else:
+            elements = np.ascontiguousarray(elements, np.float32).reshape(-1, self.n_tets, 3)
+            k = elements.shape[0]
+        slots = np.empty((k, op["n_slots"], 3), np.float32)
+        E = np.empty((k, self.n_tets, 3), np.float32)
+        mag = np.empty((k, self.n_tets), np.float32)
+        self._lib.orc_recovery_apply(self._h, code, k, _ptr(v), _ptr(dadt_nodes), _ptr(elements), _ptr(slots),
+                                     _ptr(E), _ptr(mag))
+        return slots, E, mag
+
+    def solve(self, coil, centers, handles, dists, didt=1e6, tolerance=1e-10, max_iters=2000, recovery="raw"):
         """Full pipeline for k placements; returns a dict of per-placement arrays."""
         centers = np.ascontiguousarray(centers, dtype=np.float64).reshape(-1, 3)
         handles = np.ascontiguousarray(handles, dtype=np.float64).reshape(-1, 3)
@@ -159,7 +203,7 @@ class Oracle:
         rel = np.empty(k)
         err = C.create_string_buffer(512)
         rc = self._lib.orc_solve(self._h, pos, mom, pos.shape[0], centers, handles, dists, k, float(didt), float(tolerance),
-                                 int(max_iters), _ptr(T), _ptr(v), _ptr(mag), _ptr(E), _ptr(S), _ptr(it), _ptr(rel), err, 512)
+                                 int(max_iters), RECOVERY_CODES[recovery], _ptr(T), _ptr(v), _ptr(mag), _ptr(E), _ptr(S), _ptr(it), _ptr(rel), err, 512)
         if rc != 0:
             raise ValueError(err.value.decode())
         return {"transform": T.reshape(k, 4, 4), "v": v, "magnE": mag, "E": E, "summary": S, "iterations": it, "relative_residual": rel}

@@ -81,6 +81,17 @@ struct Ctx {
     vector<int> gm_index;
     // Flattened per-level views for the getters.
     vector<int> level_sizes;
+    // Field-recovery operators, built on demand, indexed by mode (ORC_REC_*).
+    struct Recovery {
+        bool built = false;
+        vector<int> ptr, idx;             // slot CSR over corners (SPR) or patch nodes (harmonic)
+        vector<float> w;                  // SPR: one weight per entry; harmonic: three per entry
+        vector<int> slot_of_corner;       // (4M) slot each corner samples back from
+        vector<int> slot_node, slot_tag;  // (n_slots); slot_tag empty when slots are nodes
+        vector<int> status;               // harmonic: rung per slot
+        vector<int> is_boundary;          // SPR: per node
+        vector<int> counts;               // n_slots, n_fallback, n_undetermined
+    } rec[4];
 };
 
 // --- small helpers -----------------------------------------------------------------------
@@ -1031,6 +1042,386 @@ void summary_impl(const float* magnE, const float* vols, const double* bary, con
     }
 }
 
+// --- field recovery (fem/recovery.py:1-552; recovery.cu:1-774) ------------------------------
+//
+// Modes: 1 "spr_global" (a patch per node over every incident tetrahedron), 2 "spr_tissue" (a
+// patch per (node, tissue) slot), 3 "harmonic" (potential fitted per (node, tissue) slot in the
+// harmonic-polynomial space, then differentiated). Every accumulation below walks its CSR in
+// order and names each fused multiply-add, so the weights are the same IEEE values the CUDA
+// build kernels produce; the apply mirrors reproduce the CUDA apply kernels bit for bit.
+
+using Recovery = Ctx::Recovery;
+
+constexpr int kMinPatchNodes = 16;         // recovery.py:246-250 (_MIN_PATCH_NODES)
+constexpr double kMaxLebesgue = 8.0;       // recovery.cu:32-35
+constexpr double kMaxGradAmp = 50.0;       // recovery.cu:37-43
+
+// Slots = (node, tissue) pairs: corners stably sorted by node * stride + tag (recovery.py:186-225).
+void tissue_slots(const Ctx& c, Recovery& r) {
+    const int M = c.n_tets;
+    int max_tag = 0;
+    for (int e = 0; e < M; ++e) max_tag = std::max(max_tag, c.tags[e]);
+    const long stride = max_tag + 1;
+    vector<long> key(4 * static_cast<size_t>(M));
+    for (long q = 0; q < 4L * M; ++q) key[q] = c.tets[q] * stride + c.tags[q >> 2];
+    const vector<int> order = stable_argsort(key);
+    r.ptr.clear();
+    r.idx.assign(order.begin(), order.end());
+    r.slot_of_corner.assign(4 * static_cast<size_t>(M), 0);
+    r.slot_node.clear();
+    r.slot_tag.clear();
+    for (long i = 0; i < 4L * M; ++i) {
+        const long k = key[order[i]];
+        if (i == 0 || k != key[order[i - 1]]) {
+            r.ptr.push_back(static_cast<int>(i));
+            r.slot_node.push_back(static_cast<int>(k / stride));
+            r.slot_tag.push_back(static_cast<int>(k % stride));
+        }
+        r.slot_of_corner[order[i]] = static_cast<int>(r.slot_node.size()) - 1;
+    }
+    r.ptr.push_back(static_cast<int>(4L * M));
+}
+
+// Nodes on a face that exactly one tetrahedron owns (recovery.cu:46-110).
+vector<int> outer_boundary(const Ctx& c) {
+    const int M = c.n_tets;
+    struct Face {
+        int a, b, c;
+        bool operator<(const Face& o) const {
+            return a != o.a ? a < o.a : (b != o.b ? b < o.b : c < o.c);
+        }
+        bool operator==(const Face& o) const { return a == o.a && b == o.b && c == o.c; }
+    };
+    vector<Face> faces;
+    faces.reserve(4 * static_cast<size_t>(M));
+    for (int e = 0; e < M; ++e)
+        for (int skip = 0; skip < 4; ++skip) {
+            int v[3], m = 0;
+            for (int i = 0; i < 4; ++i)
+                if (i != skip) v[m++] = c.tets[4 * e + i];
+            std::sort(v, v + 3);
+            faces.push_back({v[0], v[1], v[2]});
+        }
+    std::sort(faces.begin(), faces.end());
+    vector<int> mark(c.n_nodes, 0);
+    for (size_t i = 0; i < faces.size();) {
+        size_t j = i + 1;
+        while (j < faces.size() && faces[j] == faces[i]) ++j;
+        if (j - i == 1) mark[faces[i].a] = mark[faces[i].b] = mark[faces[i].c] = 1;
+        i = j;
+    }
+    return mark;
+}
+
+// Cholesky of the lower triangle of an n x n SPD matrix (row-major, n <= 16); false on a pivot at
+// or below 1e-12 * A[0][0] (recovery.cu:119-152 pivot rule).
+bool chol_factor(const double* A, int n, double* L) {
+    const double floor_pivot = 1e-12 * A[0];
+    for (int j = 0; j < n; ++j) {
+        double d = A[j * n + j];
+        for (int k = 0; k < j; ++k) d = d - L[j * n + k] * L[j * n + k];
+        if (!(d > floor_pivot)) return false;
+        L[j * n + j] = std::sqrt(d);
+        for (int i = j + 1; i < n; ++i) {
+            double s = A[i * n + j];
+            for (int k = 0; k < j; ++k) s = s - L[i * n + k] * L[j * n + k];
+            L[i * n + j] = s / L[j * n + j];
+        }
+    }
+    return true;
+}
+
+// Row `row` of A^-1 from the factor: forward then backward substitution against e_row.
+void chol_unit_solve(const double* L, int n, int row, double* z) {
+    double y[16];
+    for (int i = 0; i < n; ++i) {
+        double s = (i == row) ? 1.0 : 0.0;
+        for (int k = 0; k < i; ++k) s = s - L[i * n + k] * y[k];
+        y[i] = s / L[i * n + i];
+    }
+    for (int i = n - 1; i >= 0; --i) {
+        double s = y[i];
+        for (int k = i + 1; k < n; ++k) s = s - L[k * n + i] * z[k];
+        z[i] = s / L[i * n + i];
+    }
+}
+
+// SPR weights, one slot at a time (recovery.cu:166-283): linear fit over the barycentres of the
+// slot's corners in the node-centred frame [1, (b - x_n)/h]; boundary slots, ill-posed fits and
+// fits with sum|w| > 8 take the volume-weighted average.
+void spr_weights(const Ctx& c, Recovery& r, bool node_slots) {
+    const int S = static_cast<int>(r.ptr.size()) - 1;
+    r.w.assign(r.idx.size(), 0.0f);
+    int fallbacks = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(+ : fallbacks)
+    for (int s = 0; s < S; ++s) {
+        const int node = node_slots ? s : r.slot_node[s];
+        const int begin = r.ptr[s], end = r.ptr[s + 1], count = end - begin;
+        if (count <= 0) continue;
+        const double* xn = &c.nodes[3 * static_cast<size_t>(node)];
+        bool fit = count >= 4 && !r.is_boundary[node];
+        double h = 1.0;
+        if (fit) {
+            h = 0.0;
+            for (int p = begin; p < end; ++p) {
+                const double* b = &c.bary[3 * static_cast<size_t>(r.idx[p] >> 2)];
+                for (int a = 0; a < 3; ++a) h = std::max(h, std::fabs(b[a] - xn[a]));
+            }
+            fit = h > 0.0;
+        }
+        double z[4] = {1.0, 0.0, 0.0, 0.0};
+        auto basis = [&](int p, double* q) {
+            const double* b = &c.bary[3 * static_cast<size_t>(r.idx[p] >> 2)];
+            q[0] = 1.0;
+            for (int a = 0; a < 3; ++a) q[1 + a] = (b[a] - xn[a]) / h;
+        };
+        auto weight = [&](const double* q) {
+            double acc = 0.0;
+            for (int i = 0; i < 4; ++i) acc = std::fma(z[i], q[i], acc);
+            return acc;
+        };
+        if (fit) {
+            double A[16] = {}, L[16] = {};
+            for (int p = begin; p < end; ++p) {
+                double q[4];
+                basis(p, q);
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j <= i; ++j) A[i * 4 + j] = std::fma(q[i], q[j], A[i * 4 + j]);
+            }
+            fit = chol_factor(A, 4, L);
+            if (fit) chol_unit_solve(L, 4, 0, z);
+        }
+        if (fit) {
+            double leb = 0.0;
+            for (int p = begin; p < end; ++p) {
+                double q[4];
+                basis(p, q);
+                leb = leb + std::fabs(weight(q));
+            }
+            fit = leb <= kMaxLebesgue;
+        }
+        if (!fit) {
+            ++fallbacks;
+            double total = 0.0;
+            for (int p = begin; p < end; ++p) total = total + static_cast<double>(c.vols_f32[r.idx[p] >> 2]);
+            const bool by_volume = total > 0.0;
+            const double inv = by_volume ? 1.0 / total : 1.0 / static_cast<double>(count);
+            for (int p = begin; p < end; ++p) {
+                const double num = by_volume ? static_cast<double>(c.vols_f32[r.idx[p] >> 2]) : 1.0;
+                r.w[p] = static_cast<float>(num * inv);
+            }
+            continue;
+        }
+        for (int p = begin; p < end; ++p) {
+            double q[4];
+            basis(p, q);
+            r.w[p] = static_cast<float>(weight(q));
+        }
+    }
+    r.counts = {S, fallbacks, 0};
+}
+
+// Harmonic bases in the scaled frame (recovery.cu:285-362): 16 cubic, 9 quadratic, 4 linear terms.
+int eval_basis(int rung, double u, double v, double t, double* p) {
+    p[0] = 1.0;
+    p[1] = u;
+    p[2] = v;
+    p[3] = t;
+    if (rung == 2) return 4;
+    p[4] = u * u - v * v;
+    p[5] = v * v - t * t;
+    p[6] = u * v;
+    p[7] = u * t;
+    p[8] = v * t;
+    if (rung == 1) return 9;
+    const double uu = u * u, vv = v * v, tt = t * t;
+    p[9] = t * (2.0 * tt - 3.0 * uu - 3.0 * vv);
+    p[10] = u * (4.0 * tt - uu - vv);
+    p[11] = v * (4.0 * tt - uu - vv);
+    p[12] = t * (uu - vv);
+    p[13] = u * v * t;
+    p[14] = u * (uu - 3.0 * vv);
+    p[15] = v * (3.0 * uu - vv);
+    return 16;
+}
+
+// Patches: the distinct nodes of a slot's own tetrahedra, grown to the union of its neighbours'
+// rings where that holds fewer than 16 nodes (recovery.py:253-312; pattern.cu:86-138).
+void harmonic_patches(const Ctx& c, Recovery& r) {
+    const int S = static_cast<int>(r.slot_node.size());
+    int max_tag = 0;
+    for (int t : r.slot_tag) max_tag = std::max(max_tag, t);
+    const long stride = max_tag + 1;
+    vector<vector<int>> ring(S);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int s = 0; s < S; ++s) {
+        vector<int>& out = ring[s];
+        for (int p = r.ptr[s]; p < r.ptr[s + 1]; ++p) {
+            const int e = r.idx[p] >> 2;
+            for (int i = 0; i < 4; ++i) out.push_back(c.tets[4 * e + i]);
+        }
+        std::sort(out.begin(), out.end());
+        out.erase(std::unique(out.begin(), out.end()), out.end());
+    }
+    vector<long> slot_key(S);
+    for (int s = 0; s < S; ++s) slot_key[s] = r.slot_node[s] * stride + r.slot_tag[s];
+    vector<vector<int>> patch(S);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int s = 0; s < S; ++s) {
+        if (static_cast<int>(ring[s].size()) >= kMinPatchNodes) {
+            patch[s] = ring[s];
+            continue;
+        }
+        vector<int> out;
+        for (int m : ring[s]) {
+            const long key = m * stride + r.slot_tag[s];
+            const int nb = static_cast<int>(std::lower_bound(slot_key.begin(), slot_key.end(), key) - slot_key.begin());
+            out.insert(out.end(), ring[nb].begin(), ring[nb].end());
+        }
+        std::sort(out.begin(), out.end());
+        out.erase(std::unique(out.begin(), out.end()), out.end());
+        patch[s] = std::move(out);
+    }
+    r.ptr.assign(S + 1, 0);
+    for (int s = 0; s < S; ++s) r.ptr[s + 1] = r.ptr[s] + static_cast<int>(patch[s].size());
+    r.idx.resize(r.ptr[S]);
+    for (int s = 0; s < S; ++s) std::copy(patch[s].begin(), patch[s].end(), r.idx.begin() + r.ptr[s]);
+}
+
+// One rung of the potential fit over slot s (recovery.cu:364-511): normal matrix accumulated over
+// the patch in order, Cholesky, rows 1..3 of the inverse, gradient weights w = grad / h. Accepted
+// when max_c sum_p |grad_c| <= 50, that sum taken as 32 strided partials (entry p to partial
+// (p - begin) % 32) folded by halving.
+bool harmonic_rung(const double* xm, const int* pidx, int begin, int end, const double* xn, double h, int rung,
+                   float* w) {
+    static const int kMin[3] = {20, 9, 4};
+    const int n = rung == 0 ? 16 : (rung == 1 ? 9 : 4);
+    if (end - begin < kMin[rung]) return false;
+    double A[256] = {}, L[256] = {}, q[16];
+    auto eval = [&](int p) {
+        const double* x = &xm[3 * static_cast<size_t>(pidx[p])];
+        eval_basis(rung, (x[0] - xn[0]) / h, (x[1] - xn[1]) / h, (x[2] - xn[2]) / h, q);
+    };
+    for (int p = begin; p < end; ++p) {
+        eval(p);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j <= i; ++j) A[i * n + j] = std::fma(q[i], q[j], A[i * n + j]);
+    }
+    if (!chol_factor(A, n, L)) return false;
+    double z[3][16];
+    for (int cdir = 0; cdir < 3; ++cdir) chol_unit_solve(L, n, cdir + 1, z[cdir]);
+    double part[3][32] = {};
+    for (int p = begin; p < end; ++p) {
+        eval(p);
+        for (int cdir = 0; cdir < 3; ++cdir) {
+            double g = 0.0;
+            for (int i = 0; i < n; ++i) g = std::fma(z[cdir][i], q[i], g);
+            part[cdir][(p - begin) % 32] = part[cdir][(p - begin) % 32] + std::fabs(g);
+            w[3 * static_cast<size_t>(p) + cdir] = static_cast<float>(g / h);
+        }
+    }
+    double worst = 0.0;
+    for (int cdir = 0; cdir < 3; ++cdir) {
+        for (int off = 16; off >= 1; off >>= 1)
+            for (int l = 0; l < off; ++l) part[cdir][l] = part[cdir][l] + part[cdir][l + off];
+        worst = std::max(worst, part[cdir][0]);
+    }
+    return worst <= kMaxGradAmp;
+}
+
+void harmonic_weights(const Ctx& c, Recovery& r) {
+    const int S = static_cast<int>(r.slot_node.size());
+    vector<double> xm(c.nodes.size());
+    for (size_t i = 0; i < xm.size(); ++i) xm[i] = c.nodes[i] * 1e-3;
+    r.w.assign(3 * r.idx.size(), 0.0f);
+    r.status.assign(S, 3);
+#pragma omp parallel for schedule(dynamic, 128)
+    for (int s = 0; s < S; ++s) {
+        const int begin = r.ptr[s], end = r.ptr[s + 1];
+        const double* xn = &xm[3 * static_cast<size_t>(r.slot_node[s])];
+        double h = 0.0;
+        for (int p = begin; p < end; ++p)
+            for (int a = 0; a < 3; ++a) h = std::max(h, std::fabs(xm[3 * static_cast<size_t>(r.idx[p]) + a] - xn[a]));
+        int rung = 3;
+        if (h > 0.0) {
+            for (int t = 0; t < 3 && rung == 3; ++t)
+                if (harmonic_rung(xm.data(), r.idx.data(), begin, end, xn, h, t, r.w.data())) rung = t;
+        }
+        if (rung == 3)
+            for (int p = begin; p < end; ++p) r.w[3 * p] = r.w[3 * p + 1] = r.w[3 * p + 2] = 0.0f;
+        r.status[s] = rung;
+    }
+    int fb = 0, und = 0;
+    for (int st : r.status) {
+        fb += st >= 2;
+        und += st == 3;
+    }
+    r.counts = {S, fb, und};
+}
+
+void build_recovery(Ctx& c, int mode) {
+    if (mode < 1 || mode > 3) throw std::invalid_argument("unknown recovery mode");
+    Recovery& r = c.rec[mode];
+    if (r.built) return;
+    r = Recovery();
+    if (mode == 1) {
+        r.ptr = c.n2c_ptr;
+        r.idx = c.n2c_idx;
+        r.slot_of_corner = c.tets;
+        r.slot_node.resize(c.n_nodes);
+        std::iota(r.slot_node.begin(), r.slot_node.end(), 0);
+        r.is_boundary = outer_boundary(c);
+        spr_weights(c, r, true);
+    } else if (mode == 2) {
+        tissue_slots(c, r);
+        r.is_boundary = outer_boundary(c);
+        // A node touching more than one tissue is on each tissue's submesh boundary (recovery.py:127-158).
+        for (size_t s = 1; s < r.slot_node.size(); ++s)
+            if (r.slot_node[s] == r.slot_node[s - 1]) r.is_boundary[r.slot_node[s]] = 1;
+        spr_weights(c, r, false);
+    } else {
+        tissue_slots(c, r);
+        harmonic_patches(c, r);
+        harmonic_weights(c, r);
+    }
+    r.built = true;
+}
+
+// Apply, FP64 ground truth on slots, then sampled at the barycentres (recovery.cu:513-687).
+// Harmonic: E_s = -sum_p w_p v_m - dA/dt(x_node); SPR: E_s = sum_p w_p E_e.
+void apply_recovery_f64(const Ctx& c, int mode, const double* v, const double* dadt_nodes, const double* E_elem,
+                        vector<double>& slots, float* magn, double* E_out) {
+    const Recovery& r = c.rec[mode];
+    const int S = static_cast<int>(r.ptr.size()) - 1;
+    slots.assign(3 * static_cast<size_t>(S), 0.0);
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < S; ++s) {
+        double acc[3] = {0.0, 0.0, 0.0};
+        for (int p = r.ptr[s]; p < r.ptr[s + 1]; ++p) {
+            if (mode == 3) {
+                const double vm = v[r.idx[p]];
+                for (int a = 0; a < 3; ++a) acc[a] = std::fma(static_cast<double>(r.w[3 * static_cast<size_t>(p) + a]), vm, acc[a]);
+            } else {
+                const double* ee = &E_elem[3 * static_cast<size_t>(r.idx[p] >> 2)];
+                for (int a = 0; a < 3; ++a) acc[a] = std::fma(static_cast<double>(r.w[p]), ee[a], acc[a]);
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            slots[3 * static_cast<size_t>(s) + a] =
+                mode == 3 ? -acc[a] - dadt_nodes[3 * static_cast<size_t>(r.slot_node[s]) + a] : acc[a];
+    }
+#pragma omp parallel for schedule(static)
+    for (int e = 0; e < c.n_tets; ++e) {
+        double sx[3] = {0.0, 0.0, 0.0};
+        for (int i = 0; i < 4; ++i)
+            for (int a = 0; a < 3; ++a) sx[a] = sx[a] + slots[3 * static_cast<size_t>(r.slot_of_corner[4 * e + i]) + a];
+        for (int a = 0; a < 3; ++a) sx[a] = sx[a] * 0.25;
+        if (E_out)
+            for (int a = 0; a < 3; ++a) E_out[3 * static_cast<size_t>(e) + a] = sx[a];
+        magn[e] = static_cast<float>(std::sqrt(sx[0] * sx[0] + sx[1] * sx[1] + sx[2] * sx[2]));
+    }
+}
+
 void set_err(char* err, int len, const std::string& msg) {
     if (err && len > 0) std::snprintf(err, static_cast<size_t>(len), "%s", msg.c_str());
 }
@@ -1274,10 +1665,12 @@ void orc_weighted_quantiles(const double* values, const double* weights, int n, 
 
 int orc_solve(void* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
               const double* centers_mm, const double* handles_mm, const double* dists_mm, int k, double didt,
-              double tolerance, int max_iters, double* transforms, double* v_out, float* magnE_out,
+              double tolerance, int max_iters, int recovery, double* transforms, double* v_out, float* magnE_out,
               float* E_out, double* summary, int* iters, double* relres, char* err, int err_len) {
     Ctx* c = static_cast<Ctx*>(ctx);
     try {
+        if (recovery != ORC_REC_RAW) build_recovery(*c, recovery);
+        vector<double> rec_slots, rec_E;
         const int N = c->n_nodes, M = c->n_tets;
         vector<double> T(16), dadt(3 * static_cast<size_t>(N)), elm(3 * static_cast<size_t>(M)), b(N);
         vector<double> v(N), E(3 * static_cast<size_t>(M));
@@ -1329,6 +1722,11 @@ int orc_solve(void* ctx, const double* dip_pos_m, const double* dip_moment, int 
                 for (int a = 0; a < 3; ++a) E[3 * static_cast<size_t>(e) + a] = ee[a];
                 mag[e] = static_cast<float>(std::sqrt(ee[0] * ee[0] + ee[1] * ee[1] + ee[2] * ee[2]));
             }
+            if (recovery != ORC_REC_RAW) {
+                rec_E.resize(3 * static_cast<size_t>(M));
+                apply_recovery_f64(*c, recovery, v.data(), dadt.data(), E.data(), rec_slots, mag.data(), rec_E.data());
+                E.swap(rec_E);
+            }
             if (magnE_out) std::copy(mag.begin(), mag.end(), magnE_out + static_cast<size_t>(p) * M);
             if (E_out)
                 for (size_t i = 0; i < 3 * static_cast<size_t>(M); ++i)
@@ -1342,6 +1740,89 @@ int orc_solve(void* ctx, const double* dip_pos_m, const double* dip_moment, int 
         set_err(err, err_len, ex.what());
         return -1;
     }
+}
+
+int orc_recovery_build(void* ctx, int mode, char* err, int err_len) {
+    try {
+        build_recovery(*static_cast<Ctx*>(ctx), mode);
+        return 0;
+    } catch (const std::exception& ex) {
+        set_err(err, err_len, ex.what());
+        return -1;
+    }
+}
+
+int orc_recovery_i32(void* ctx, int mode, const char* name, const int** ptr, long* len) {
+    Ctx* c = static_cast<Ctx*>(ctx);
+    if (mode < 1 || mode > 3 || !c->rec[mode].built) return -1;
+    const Recovery& r = c->rec[mode];
+    const std::string n(name);
+    const vector<int>* v = nullptr;
+    if (n == "ptr") v = &r.ptr;
+    else if (n == "idx") v = &r.idx;
+    else if (n == "slot_of_corner") v = &r.slot_of_corner;
+    else if (n == "slot_node") v = &r.slot_node;
+    else if (n == "slot_tag") v = &r.slot_tag;
+    else if (n == "status") v = &r.status;
+    else if (n == "is_boundary") v = &r.is_boundary;
+    else if (n == "counts") v = &r.counts;
+    if (!v) return -1;
+    *ptr = v->data();
+    *len = static_cast<long>(v->size());
+    return 0;
+}
+
+int orc_recovery_w(void* ctx, int mode, const float** ptr, long* len) {
+    Ctx* c = static_cast<Ctx*>(ctx);
+    if (mode < 1 || mode > 3 || !c->rec[mode].built) return -1;
+    *ptr = c->rec[mode].w.data();
+    *len = static_cast<long>(c->rec[mode].w.size());
+    return 0;
+}
+
+int orc_recovery_apply(void* ctx, int mode, int k, const double* v, const float* dadt_nodes, const float* E_elem,
+                       float* E_slots, float* E_out, float* magn) {
+    Ctx* c = static_cast<Ctx*>(ctx);
+    if (mode < 1 || mode > 3 || !c->rec[mode].built) return -1;
+    const Recovery& r = c->rec[mode];
+    const int S = static_cast<int>(r.ptr.size()) - 1, N = c->n_nodes, M = c->n_tets;
+    for (int col = 0; col < k; ++col) {
+        float* slots = E_slots + static_cast<size_t>(col) * S * 3;
+#pragma omp parallel for schedule(static)
+        for (int s = 0; s < S; ++s) {
+            if (mode == 3) {
+                const double* vc = v + static_cast<size_t>(col) * N;
+                const float* da = dadt_nodes + (static_cast<size_t>(col) * N + r.slot_node[s]) * 3;
+                double acc[3] = {0.0, 0.0, 0.0};
+                for (int p = r.ptr[s]; p < r.ptr[s + 1]; ++p) {
+                    const double vm = vc[r.idx[p]];
+                    for (int a = 0; a < 3; ++a)
+                        acc[a] = std::fma(static_cast<double>(r.w[3 * static_cast<size_t>(p) + a]), vm, acc[a]);
+                }
+                for (int a = 0; a < 3; ++a) slots[3 * static_cast<size_t>(s) + a] = static_cast<float>(-acc[a] - static_cast<double>(da[a]));
+            } else {
+                const float* ec = E_elem + static_cast<size_t>(col) * M * 3;
+                float acc[3] = {0.0f, 0.0f, 0.0f};
+                for (int p = r.ptr[s]; p < r.ptr[s + 1]; ++p) {
+                    const float* ee = ec + 3 * static_cast<size_t>(r.idx[p] >> 2);
+                    for (int a = 0; a < 3; ++a) acc[a] = std::fma(r.w[p], ee[a], acc[a]);
+                }
+                for (int a = 0; a < 3; ++a) slots[3 * static_cast<size_t>(s) + a] = acc[a];
+            }
+        }
+#pragma omp parallel for schedule(static)
+        for (int e = 0; e < M; ++e) {
+            double sx[3] = {0.0, 0.0, 0.0};
+            for (int i = 0; i < 4; ++i)
+                for (int a = 0; a < 3; ++a)
+                    sx[a] = sx[a] + static_cast<double>(slots[3 * static_cast<size_t>(r.slot_of_corner[4 * e + i]) + a]);
+            for (int a = 0; a < 3; ++a) sx[a] = sx[a] * 0.25;
+            if (E_out)
+                for (int a = 0; a < 3; ++a) E_out[(static_cast<size_t>(col) * M + e) * 3 + a] = static_cast<float>(sx[a]);
+            magn[static_cast<size_t>(col) * M + e] = static_cast<float>(std::sqrt(sx[0] * sx[0] + sx[1] * sx[1] + sx[2] * sx[2]));
+        }
+    }
+    return 0;
 }
 
 }  // extern "C"

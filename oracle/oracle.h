@@ -59,12 +59,16 @@ int orc_n_levels(void* ctx);
 /* One V-cycle application z = M r on the reduced system, k right-hand sides, row-major (n, k). */
 int orc_vcycle_apply(void* ctx, const double* r, double* z, int k);
 
-/* Full per-placement pipeline for k placements. Outputs (any may be NULL):
+/* Field recovery modes (fem/recovery.py:74-113). */
+enum { ORC_REC_RAW = 0, ORC_REC_SPR_GLOBAL = 1, ORC_REC_SPR_TISSUE = 2, ORC_REC_HARMONIC = 3 };
+
+/* Full per-placement pipeline for k placements. recovery selects the reported field (ORC_REC_*);
+ * the recovered field is FP64 on slots (recovery weights are FP32, as the reference stores them). Outputs (any may be NULL):
  * transforms (k,16), v (k, n_nodes) potential per placement, magnE (k, n_tets), E (k, n_tets, 3),
  * summary (k, ORC_SUMMARY_LEN), iters (k), relres (k). Returns 0 or -1 (err filled). */
 int orc_solve(void* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
               const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
-              double didt, double tolerance, int max_iters, double* transforms, double* v,
+              double didt, double tolerance, int max_iters, int recovery, double* transforms, double* v,
               float* magnE, float* E, double* summary, int* iters, double* relres, char* err,
               int err_len);
 
@@ -82,6 +86,20 @@ void orc_summary(const float* magnE, const float* vols, const double* barycenter
                  const int* tet_tags, int n_tets, int region_tag, double* out);
 void orc_weighted_quantiles(const double* values, const double* weights, int n, const double* qs,
                             int nq, double* out);
+
+/* Recovery operator of a mode, built once per context: the slot CSR (ptr, idx), slot maps,
+ * weights (SPR: one per corner entry; harmonic: three per patch entry), the harmonic rung per
+ * slot (status), the boundary marks of the SPR modes (is_boundary), and counts = (n_slots,
+ * n_fallback, n_undetermined). */
+int orc_recovery_build(void* ctx, int mode, char* err, int err_len);
+int orc_recovery_i32(void* ctx, int mode, const char* name, const int** ptr, long* len);
+int orc_recovery_w(void* ctx, int mode, const float** ptr, long* len);
+
+/* Applies a built operator to k columns with the CUDA apply kernels' arithmetic: harmonic reads
+ * v (k, n_nodes) f64 and dadt_nodes (k, n_nodes, 3) f32; SPR reads E_elem (k, n_tets, 3) f32.
+ * Writes E_slots (k, n_slots, 3), E_out (k, n_tets, 3; may be NULL) and magn (k, n_tets). */
+int orc_recovery_apply(void* ctx, int mode, int k, const double* v, const float* dadt_nodes, const float* E_elem,
+                       float* E_slots, float* E_out, float* magn);
 
 #ifdef __cplusplus
 }

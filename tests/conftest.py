@@ -79,3 +79,11 @@ def cube_mesh():
     tets = np.array([[0, 1, 3, 7], [0, 3, 2, 7], [0, 2, 6, 7], [0, 6, 4, 7], [0, 4, 5, 7], [0, 5, 1, 7]], np.int32)
     nodes = corners * 100.0
     return HeadMesh(nodes, tets, np.full(6, 2, np.int32), boundary_faces(tets, nodes))
+
+
+@pytest.fixture(scope="session")
+def single_tissue_ball():
+    """A one-tag (gray matter) jittered Kuhn ball, ~6k tets."""
+    from cunibs_b200.synthetic import sphere_head
+
+    return sphere_head(5.0, 40.0, shells=((1.0, 2),), jitter_mm=0.4, seed=4)

@@ -142,10 +142,10 @@ def test_linear_solve_matches_oracle_direct(sphere_pair, precision):
         assert np.linalg.norm(B[:, c] - ax) / np.linalg.norm(B[:, c]) <= 2e-10
 
 
-def _compare_block(subject, orc, coil, sites, tol=1e-10):
-    res = list(subject.iter_simulate(coil, sites, magnitude=True, block_k=8))
+def _compare_block(subject, orc, coil, sites, tol=1e-10, recovery="raw"):
+    res = list(subject.iter_simulate(coil, sites, magnitude=True, block_k=8, recovery=recovery))
     ref = orc.solve(coil, np.stack([s.center_mm for s in sites]), np.stack([s.handle_mm for s in sites]),
-                    [s.distance_mm for s in sites], 1e6, tolerance=tol)
+                    [s.distance_mm for s in sites], 1e6, tolerance=tol, recovery=recovery)
     tags = subject.mesh.tet_tags
     gm = tags == 2
     for i, r in enumerate(res):
@@ -182,21 +182,23 @@ def test_sphere_block_vs_oracle(sphere_mesh):
     subj.free()
 
 
-def test_block_width_and_batch_invariance_bitwise(sphere_mesh):
+@pytest.mark.parametrize("recovery", ["raw", "harmonic", "spr_tissue"])
+def test_block_width_and_batch_invariance_bitwise(sphere_mesh, recovery):
     """A placement's result is bitwise independent of block_k and of its block-mates."""
     subj = Subject(sphere_mesh, tolerance=1e-8)
     coil = figure8_coil(64)
     top = np.array([0.0, 0.0, 90.0])
     sites = [Placement(top + [dx, 0, 0], top + [dx, 50, 0]) for dx in (0.0, 10.0, -12.0)]
-    runs = {bk: list(subj.iter_simulate(coil, sites, magnitude=True, potential=True, block_k=bk)) for bk in (1, 2, 4, 8)}
+    kw = dict(magnitude=True, recovery=recovery)
+    runs = {bk: list(subj.iter_simulate(coil, sites, potential=True, block_k=bk, **kw)) for bk in (1, 2, 4, 8)}
     for bk in (2, 4, 8):
         for i in range(3):
             np.testing.assert_array_equal(runs[bk][i].magnE, runs[1][i].magnE)
             np.testing.assert_array_equal(runs[bk][i].v, runs[1][i].v)
             assert runs[bk][i].summary["peak_magnE"] == runs[1][i].summary["peak_magnE"]
-    alone = subj.simulate(coil, sites[2], magnitude=True)
+    alone = subj.simulate(coil, sites[2], **kw)
     np.testing.assert_array_equal(alone.magnE, runs[8][2].magnE)
-    again = list(subj.iter_simulate(coil, sites, magnitude=True, block_k=8))
+    again = list(subj.iter_simulate(coil, sites, block_k=8, **kw))
     for i in range(3):
         np.testing.assert_array_equal(again[i].magnE, runs[8][i].magnE)
     subj.free()
