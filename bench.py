@@ -200,9 +200,39 @@ def run_ours(args) -> dict:
     outs = {"transforms": d_T.data_ptr(), "summary": d_S.data_ptr()}
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def step():
+    warm_stats = None
+    if args.warm_start == "on":
+        from cunibs_b200.warmstart import train_warm_start
+
+        with torch.cuda.device(local):
+            model = train_warm_start(ctx, coil, n_train=args.train, rank=args.rank, seed=1)
+        warm_stats = {k: v for k, v in model.stats.items() if k != "loss_curve"}
+    d_used = torch.zeros(K_BLOCK, dtype=torch.int32, device=dev)
+    d_rel0 = torch.zeros(K_BLOCK, dtype=torch.float64, device=dev)
+    d_it = torch.zeros(K_BLOCK, dtype=torch.int32, device=dev)
+    outs.update({"warm_used": d_used.data_ptr(), "init_relres": d_rel0.data_ptr(), "iterations": d_it.data_ptr()})
+
+    def step(precision=_native.PREC_DEFAULT, warm=args.warm_start == "on"):
         return ctx.solve_block_device(d_pos.data_ptr(), d_mom.data_ptr(), coil.n_dipoles, d_c.data_ptr(),
-                                      d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, outs, recovery=args.recovery)
+                                      d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, outs, recovery=args.recovery,
+                                      precision=precision, warm_start=warm)
+
+    def timed(n, **kw):
+        """Device time of n steps (CUDA events on the library stream, L2 flushed before each)."""
+        ms, its = [], []
+        for _ in range(n):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            step(**kw)
+            with torch.cuda.stream(stream):
+                e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            its.append(float(d_it.float().mean().item()))
+        return float(sum(ms)), float(np.mean(its))
 
     for _ in range(args.warmup):
         step()
@@ -235,6 +265,16 @@ def run_ours(args) -> dict:
             dist.barrier()
     launches = _native.kernel_launches() - launches0
     total_ms = float(sum(step_ms))
+    warm_used = d_used.cpu().numpy().tolist()
+    warm_rel0 = d_rel0.cpu().numpy().tolist()
+    col_iters = float(d_it.float().mean().item())
+    # The same block on the same GPU without the learned guess: mixed precision, and plain FP64 PCG.
+    n_cmp = max(1, min(args.steps, 5))
+    for _ in range(2):
+        step(warm=False)
+        step(precision=_native.PREC_PLAIN_FP64, warm=False)
+    cold_ms, cold_it = timed(n_cmp, warm=False)
+    plain_ms, plain_it = timed(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
     if dist is not None:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -246,7 +286,8 @@ def run_ours(args) -> dict:
     for _ in range(max(1, min(args.steps, 5))):
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        res = ctx.solve_block(coil, centers, handles, dists, 1e6, recovery=args.recovery)
+        res = ctx.solve_block(coil, centers, handles, dists, 1e6, recovery=args.recovery,
+                              warm_start=args.warm_start == "on")
         e2e_ms.append((time.perf_counter() - t1) * 1e3)
     e2e_value = world * K_BLOCK / (statistics.median(e2e_ms) / 1e3)
     h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
@@ -279,14 +320,25 @@ def run_ours(args) -> dict:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 (FP32 PCG/V-cycle/dA-dt) with f64 refinement" if args.precision == "mixed" else "f64",
+        "dtype": ("f32 (FP32 PCG/V-cycle/dA-dt) with f64 refinement" if args.precision == "mixed" else "f64")
+                 + ("; bf16 tensor-core warm start" if args.warm_start == "on" else ""),
         "data": "synthetic: seeded sphere head and figure-8 coil",
         "config": config_dict(mesh, {"precision": args.precision, "recovery": args.recovery,
+                                     "warm_start": (f"MLP 6-4x512-{args.rank}, {args.train} plain-method training solves"
+                                                    if args.warm_start == "on" else "off"),
                                      "l2": "flushed (256 MB write) between steps",
                                      "parallelism": f"replicas x{world}"}),
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
+        "vs_plain_fp64": {"value": round(world * n_cmp * K_BLOCK / (plain_ms / 1e3), 3), "unit": "placements/s",
+                          "iterations": plain_it, "ratio": round((plain_ms / n_cmp) / (total_ms / args.steps), 3),
+                          "what": "plain FP64 zero-guess PCG, same block, same GPU"},
+        "ablation": {"mixed_zero_guess": {"value": round(world * n_cmp * K_BLOCK / (cold_ms / 1e3), 3),
+                                          "iterations": cold_it},
+                     "this_run": {"warm_start": args.warm_start, "iterations": col_iters,
+                                  "warm_used": warm_used, "init_relres": [round(v, 5) for v in warm_rel0]}},
+        "warm_start": warm_stats,
         "roofline": {"bound": "hbm", "kernel": "block PCG solve stage (SpMV-dominated iteration)",
                      "achieved": round(achieved, 1), "peak": hbm_peak, "unit": "GB/s",
                      "frac": round(achieved / hbm_peak, 4), "traffic": traffic,
@@ -368,6 +420,9 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
     ap.add_argument("--recovery", choices=["harmonic", "spr_tissue", "spr_global", "raw"], default="harmonic")
+    ap.add_argument("--warm-start", choices=["on", "off"], default="on")
+    ap.add_argument("--train", type=int, default=4096, help="training solves of the warm-start network")
+    ap.add_argument("--rank", type=int, default=512, help="reduced-basis size the network predicts")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     line = run_reference(args) if args.impl == "reference" else run_ours(args)

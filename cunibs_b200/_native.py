@@ -59,6 +59,7 @@ class SolveOpts(C.Structure):
         ("tolerance", C.c_double),
         ("max_iters", C.c_int),
         ("recovery", C.c_int),
+        ("warm_start", C.c_int),
     ]
 
 
@@ -84,6 +85,8 @@ class BlockOut(C.Structure):
         ("total_iterations", C.c_int),
         ("outer_steps", C.c_int),
         ("E_slots", _vp),
+        ("warm_used", _vp),
+        ("init_relres", _vp),
     ]
 
 
@@ -139,6 +142,14 @@ def load() -> C.CDLL:
         "cunibs_context_recovery": ([_vp, C.c_int, C.POINTER(RecoveryInfo)], C.c_int),
         "cunibs_context_recovery_array": ([_vp, C.c_int, C.c_char_p, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
         "cunibs_context_recover": ([_vp, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "cunibs_context_set_warmstart": ([_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
+        "cunibs_gemm_bf16": ([_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int, _vp,
+                              _vp, C.c_int, _vp, C.c_int, _vp], C.c_int),
+        "cunibs_mlp_colsum": ([_vp, C.c_int, C.c_int, C.c_int, _vp, _vp], C.c_int),
+        "cunibs_mlp_mse": ([_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
+        "cunibs_mlp_adam": ([_vp, _vp, _vp, _vp, C.c_longlong, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                             C.c_float, C.c_int, C.c_int, _vp, _vp, _vp], C.c_int),
+        "cunibs_mlp_features": ([_vp, C.c_int, _vp, _vp, _vp, C.c_int, _vp], C.c_int),
         "cunibs_context_set_timing": ([_vp, C.c_int], C.c_int),
         "cunibs_context_stage_times": ([_vp, dp, C.c_int], C.c_int),
         "cunibs_context_stream": ([_vp, C.POINTER(_vp)], C.c_int),
@@ -332,6 +343,17 @@ class Context:
                                                _p(slots), _p(E), _p(mag)))
         return slots, E, mag
 
+    def set_warm_start(self, depth, hidden, n_out, weights, biases, feature_mean, feature_std, coef_mean, coef_std,
+                       basis) -> None:
+        """Install a trained warm-start network (device pointers as ints); weights=None removes it."""
+        if weights is None:
+            check(self._lib.cunibs_context_set_warmstart(self.handle, 0, 0, 0, None, None, None, None, None, None, None))
+            return
+        w = (_vp * len(weights))(*weights)
+        b = (_vp * len(biases))(*biases)
+        check(self._lib.cunibs_context_set_warmstart(self.handle, int(depth), int(hidden), int(n_out), w, b,
+                                                     feature_mean, feature_std, coef_mean, coef_std, basis))
+
     def set_timing(self, on: bool = True) -> None:
         check(self._lib.cunibs_context_set_timing(self.handle, int(bool(on))))
 
@@ -346,12 +368,14 @@ class Context:
         return int(out.value or 0)
 
     def solve_block_device(self, pos, mom, n_dip, centers, handles, dists, k, didt, out_ptrs, *, block_width=0,
-                           precision=PREC_DEFAULT, tolerance=0.0, max_iters=0, recovery="raw") -> tuple[int, int]:
+                           precision=PREC_DEFAULT, tolerance=0.0, max_iters=0, recovery="raw",
+                           warm_start=False) -> tuple[int, int]:
         """cunibs_solve_block_device on raw device pointers (ints); out_ptrs maps output names to pointers."""
         out = BlockOut(out_ptrs.get("transforms"), out_ptrs.get("summary"), out_ptrs.get("iterations"),
                        out_ptrs.get("relres"), out_ptrs.get("magnE"), out_ptrs.get("E"), out_ptrs.get("v"), 0, 0,
-                       out_ptrs.get("E_slots"))
-        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery])
+                       out_ptrs.get("E_slots"), out_ptrs.get("warm_used"), out_ptrs.get("init_relres"))
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
+                         int(bool(warm_start)))
         check(self._lib.cunibs_solve_block_device(self.handle, pos, mom, int(n_dip), centers, handles, dists, int(k),
                                                   float(didt), C.byref(opts), C.byref(out)))
         return out.total_iterations, out.outer_steps
@@ -362,7 +386,7 @@ class Context:
 
     def solve_block(self, coil, centers, handles, dists, didt, *, block_width=0, precision=PREC_DEFAULT,
                     tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False,
-                    recovery="raw", nodal=False) -> dict:
+                    recovery="raw", nodal=False, warm_start=False) -> dict:
         """One block of k placements through cunibs_solve_block (host buffers in and out)."""
         centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
         k = centers.shape[0]
@@ -379,14 +403,18 @@ class Context:
             "E": np.empty((k, self.n_tets, 3), np.float32) if vectors else None,
             "v": np.empty((k, self.n_nodes)) if potential else None,
             "E_slots": None,
+            "warm_used": np.zeros(k, np.int32),
+            "init_relres": np.ones(k),
         }
         if nodal:
             if recovery == "raw":
                 raise ValueError("nodal=True needs a recovery mode")
             res["E_slots"] = np.empty((k, self.recovery(recovery)["n_slots"], 3), np.float32)
         out = BlockOut(_p(res["transform"]), _p(res["summary"]), _p(res["iterations"]), _p(res["relative_residual"]),
-                       _p(res["magnE"]), _p(res["E"]), _p(res["v"]), 0, 0, _p(res["E_slots"]))
-        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery])
+                       _p(res["magnE"]), _p(res["E"]), _p(res["v"]), 0, 0, _p(res["E_slots"]), _p(res["warm_used"]),
+                       _p(res["init_relres"]))
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
+                         int(bool(warm_start)))
         check(self._lib.cunibs_solve_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
                                            _p(dists), k, float(didt), C.byref(opts), C.byref(out)))
         res["total_iterations"] = out.total_iterations

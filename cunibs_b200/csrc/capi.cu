@@ -1,6 +1,7 @@
 // The C ABI (include/cunibs_b200.h): context lifetime, the block solve, stage-level entry points.
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "../../include/cunibs_b200.h"
 #include "internal.hpp"
@@ -64,6 +65,11 @@ struct cunibs_context {
     // Field-recovery operators, built on first use per mode, and their block workspace.
     std::unique_ptr<RecoveryOp> rec[4];
     DevArray<float> e_slots, e_raw;
+    // Learned warm start (installed by cunibs_context_set_warmstart) and its per-block outputs.
+    std::unique_ptr<WarmStart> warm;
+    DevArray<double> X0;
+    std::vector<int> warm_used;
+    std::vector<double> init_rel;
     // Stage timing (CUDA events on the context stream), enabled by cunibs_context_set_timing.
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -173,7 +179,18 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
     c->X.reserve(static_cast<std::size_t>(n_red) * K);
     rhs_block(m, c->dadt_elm.get(), k, K, c->B.get(), s);
     c->mark(3);
-    solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, prm, s, st);
+    const bool warm = opts && opts->warm_start;
+    c->warm_used.assign(k, 0);
+    c->init_rel.assign(k, 1.0);
+    if (warm) {
+        require(c->warm != nullptr, "warm_start requested but no warm-start network is installed");
+        require(c->warm->n_red == n_red, "the installed warm start was built for another mesh");
+        const DevCsr<double>& A0 = c->hier.levels.empty() ? c->hier.coarse : c->hier.levels[0].a;
+        c->X0.reserve(static_cast<std::size_t>(n_red) * K);
+        warm_start_guess(*c->warm, c->T.get(), k, K, A0, c->B.get(), c->X0.get(), c->warm_used.data(),
+                         c->init_rel.data(), s);
+    }
+    solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, prm, s, st, warm ? c->X0.get() : nullptr);
     // Columns that missed tolerance: one FP64 retry from their current iterate, then an error
     // (the rebuild-then-retry contract of fem/solve.py:528-551).
     std::vector<int> missed;
@@ -377,6 +394,8 @@ int cunibs_solve_block(cunibs_context* c, const double* dip_pos_m, const double*
         for (int i = 0; i < k; ++i) {
             if (out->iterations) out->iterations[i] = st.col_iters[i];
             if (out->relres) out->relres[i] = st.col_rel[i];
+            if (out->warm_used) out->warm_used[i] = c->warm_used[i];
+            if (out->init_relres) out->init_relres[i] = c->init_rel[i];
         }
         out->total_iterations = st.iterations;
         out->outer_steps = st.outer_steps;
@@ -407,6 +426,10 @@ int cunibs_solve_block_device(cunibs_context* c, const double* dip_pos_m, const 
             CUNIBS_CHECK(cudaMemcpy(out->iterations, st.col_iters.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
         if (out->relres)
             CUNIBS_CHECK(cudaMemcpy(out->relres, st.col_rel.data(), sizeof(double) * k, cudaMemcpyHostToDevice));
+        if (out->warm_used)
+            CUNIBS_CHECK(cudaMemcpy(out->warm_used, c->warm_used.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
+        if (out->init_relres)
+            CUNIBS_CHECK(cudaMemcpy(out->init_relres, c->init_rel.data(), sizeof(double) * k, cudaMemcpyHostToDevice));
         out->total_iterations = st.iterations;
         out->outer_steps = st.outer_steps;
     });
@@ -472,6 +495,52 @@ int cunibs_context_array(const cunibs_context* c, const char* name, int level, v
             const std::size_t nb = std::min<std::size_t>(count, static_cast<std::size_t>(cap)) * elem;
             CUNIBS_CHECK(cudaMemcpy(out, src, nb, cudaMemcpyDeviceToHost));
         }
+    });
+}
+
+int cunibs_context_set_warmstart(cunibs_context* c, int depth, int hidden, int n_out, const void* const* weights,
+                                 const float* const* biases, const float* feature_mean, const float* feature_std,
+                                 const float* coef_mean, const float* coef_std, const void* basis) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        DeviceGuard dg(c->device);
+        if (weights == nullptr) {
+            c->warm.reset();
+            return;
+        }
+        require(depth >= 1 && depth <= 16 && hidden >= 64 && hidden % 64 == 0 && n_out >= 1,
+                "depth in [1, 16], hidden a positive multiple of 64, n_out >= 1");
+        require(biases && feature_mean && feature_std && coef_mean && coef_std && basis, "NULL warm-start array");
+        cudaStream_t s = c->stream;
+        auto ws = std::make_unique<WarmStart>();
+        ws->depth = depth;
+        ws->hidden = hidden;
+        ws->n_out = n_out;
+        ws->n_out_pad = (n_out + 63) / 64 * 64;
+        ws->n_red = c->mesh.n_nodes - 1;
+        auto copy = [&](auto& dst, const void* src, std::size_t count) {
+            using T = std::remove_reference_t<decltype(*dst.get())>;
+            dst.resize(count);
+            CUNIBS_CHECK(cudaMemcpyAsync(dst.get(), src, count * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        };
+        for (int l = 0; l <= depth; ++l) {
+            require(weights[l] && biases[l], "NULL layer weights or bias");
+            const int in = l == 0 ? kWarmInPad : hidden;
+            const int out = l == depth ? ws->n_out_pad : hidden;
+            ws->w16.emplace_back();
+            ws->bias.emplace_back();
+            copy(ws->w16.back(), weights[l], static_cast<std::size_t>(out) * in);
+            copy(ws->bias.back(), biases[l], static_cast<std::size_t>(out));
+        }
+        copy(ws->in_mean, feature_mean, 6);
+        copy(ws->in_std, feature_std, 6);
+        copy(ws->out_mean, coef_mean, n_out);
+        copy(ws->out_std, coef_std, n_out);
+        copy(ws->basis, basis, static_cast<std::size_t>(ws->n_red) * 2 * ws->n_out_pad);
+        ws->error.resize(1);
+        ws->error.zero(s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        c->warm = std::move(ws);
     });
 }
 

@@ -1,0 +1,295 @@
+// BF16 tensor-core GEMM for sm_100a (B200): C[M,N] = A[M,K] . B[N,K]^T, FP32 accumulation in TMEM.
+//
+// The GEMMs of the learned warm start (forward, both backward products, and the prolongation of the
+// predicted coefficients) all take this one "both operands K-major" form; the network keeps the
+// transposed copies it needs (the epilogue writes them for free) instead of switching operand
+// majorness.
+//
+// One CTA per BM x BN output tile, 6 warps:
+//   warp 4       TMA producer: 128-byte-swizzled K-major tiles of A and B into a STAGES-deep ring,
+//                each stage guarded by a full/empty mbarrier pair (cp.async.bulk.tensor, no multicast);
+//   warp 5       allocates TMEM, and one elected lane issues tcgen05.mma (kind::f16, BF16 in, FP32
+//                accumulate) per 16-wide K step, releasing each stage with tcgen05.commit;
+//   warps 0..3   epilogue: tcgen05.ld of their 32 TMEM lanes (one output row per thread), then the
+//                fused tail (bias, SiLU or SiLU' gating) and the stores: FP32 and/or BF16 row-major and
+//                a BF16 transposed copy (coalesced: a warp's lanes are 32 consecutive rows).
+// Every mbarrier wait is bounded; on expiry the kernel records an error flag and winds down (the
+// TMEM allocation is always released).
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+
+#include "internal.hpp"
+
+namespace cunibs {
+namespace {
+
+constexpr int BM = 128;
+constexpr int BK = 64;  // one 128-byte swizzle atom of BF16 per row
+constexpr int STAGES = 4;
+constexpr int kThreads = 192;
+constexpr long kSpinLimit = 1L << 24;
+
+__device__ __forceinline__ std::uint32_t smem_u32(const void* p) {
+    return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(std::uint64_t* bar, std::uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(std::uint64_t* bar, std::uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(std::uint64_t* bar, std::uint32_t parity) {
+    std::uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, std::uint32_t parity) {
+    for (long i = 0; i < kSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(const CUtensorMap* map, std::uint64_t* bar, void* dst, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(reinterpret_cast<std::uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major, 128-byte-swizzled tile: rows 128 B apart, 8-row
+// groups 1024 B apart (SBO), descriptor version 1, layout type 2 (SWIZZLE_128B).
+__device__ __forceinline__ std::uint64_t sw128_desc(const void* tile) {
+    const std::uint64_t addr = smem_u32(tile);
+    std::uint64_t d = (addr & 0x3FFFF) >> 4;
+    d |= std::uint64_t{1} << 16;
+    d |= std::uint64_t{1024 >> 4} << 32;
+    d |= std::uint64_t{1} << 46;
+    d |= std::uint64_t{2} << 61;
+    return d;
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, M x N.
+template <int BN>
+__host__ __device__ constexpr std::uint32_t idesc_bf16() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<std::uint32_t>(BN >> 3) << 17) |
+           (static_cast<std::uint32_t>(BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_bf16(std::uint32_t tmem_d, std::uint64_t adesc, std::uint64_t bdesc,
+                                          std::uint32_t idesc, std::uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\ttcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(
+            tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(std::uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 16 consecutive FP32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(std::uint32_t taddr, float (&v)[16]) {
+    std::uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+          "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
+
+// d silu / dz = s (1 + z (1 - s)), s = sigmoid(z)
+__device__ __forceinline__ float silu_grad(float z) {
+    const float s = 1.0f / (1.0f + __expf(-z));
+    return s * (1.0f + z * (1.0f - s));
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_bf16_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                     GemmEpilogue ep, int M, int N, int K) {
+    constexpr std::uint32_t kABytes = BM * BK * 2;
+    constexpr std::uint32_t kBBytes = BN * BK * 2;
+    constexpr std::uint32_t kStageBytes = kABytes + kBBytes;
+    constexpr std::uint32_t kTmemCols = BN < 32 ? 32 : BN;
+    extern __shared__ unsigned char dyn_smem[];
+    // SWIZZLE_128B tiles want 1024-byte alignment.
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<std::uintptr_t>(dyn_smem) + 1023) &
+                                                          ~std::uintptr_t{1023});
+    std::uint64_t* full = reinterpret_cast<std::uint64_t*>(smem + STAGES * kStageBytes);
+    std::uint64_t* empty = full + STAGES;
+    std::uint64_t* accum = empty + STAGES;
+    std::uint32_t* tmem_slot = reinterpret_cast<std::uint32_t*>(accum + 1);
+    int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int num_kb = (K + BK - 1) / BK;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(accum, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const std::uint32_t tmem = *tmem_slot;
+
+    if (warp == 4 && lane == 0) {
+        // Producer.
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1)) {
+                *abort_flag = 1;
+                break;
+            }
+            unsigned char* st = smem + s * kStageBytes;
+            mbar_expect_tx(&full[s], kStageBytes);
+            tma_load_2d(&map_a, &full[s], st, kb * BK, m0);
+            tma_load_2d(&map_b, &full[s], st + kABytes, kb * BK, n0);
+        }
+    } else if (warp == 5 && lane == 0) {
+        // MMA issuer.
+        constexpr std::uint32_t idesc = idesc_bf16<BN>();
+        bool ok = true;
+        for (int kb = 0; kb < num_kb && ok; ++kb) {
+            const int s = kb % STAGES;
+            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            unsigned char* st = smem + s * kStageBytes;
+            const std::uint64_t adesc = sw128_desc(st), bdesc = sw128_desc(st + kABytes);
+#pragma unroll
+            for (int k = 0; k < BK / 16; ++k)
+                umma_bf16(tmem, adesc + 2 * k, bdesc + 2 * k, idesc, (kb > 0 || k > 0) ? 1u : 0u);
+            umma_commit(&empty[s]);
+        }
+        if (!ok) *abort_flag = 1;
+        umma_commit(accum);  // arrives once every MMA issued above has completed
+    } else if (warp < 4) {
+        // Epilogue: thread (warp, lane) owns output row m0 + 32 warp + lane.
+        const bool ready = mbar_wait(accum, 0);
+        tc_fence_after();
+        const int row = m0 + warp * 32 + lane;
+        if (ready) {
+#pragma unroll 1
+            for (int c = 0; c < BN; c += 16) {
+                float v[16];
+                tmem_ld16(tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c), v);
+                const bool row_ok = row < M;
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const int col = n0 + c + j;
+                    if (!row_ok || col >= N) continue;
+                    float z = v[j];
+                    if (ep.bias) z += ep.bias[col];
+                    const std::int64_t at = static_cast<std::int64_t>(row) * ep.ld_out + col;
+                    if (ep.gate) z *= silu_grad(ep.gate[static_cast<std::int64_t>(row) * ep.ld_gate + col]);
+                    if (ep.out32) ep.out32[at] = z;
+                    const float h = ep.act == 1 ? silu(z) : z;
+                    if (ep.out16) ep.out16[at] = __float2bfloat16_rn(h);
+                    if (ep.out16t) ep.out16t[static_cast<std::int64_t>(col) * ep.ld_t + row] = __float2bfloat16_rn(h);
+                }
+            }
+        } else {
+            *abort_flag = 1;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x == 0 && *abort_flag && ep.error) atomicExch(ep.error, 1);
+    if (warp == 5)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    if (!fn) fail(kECuda, "cuTensorMapEncodeTiled is unavailable");
+    return fn;
+}
+
+// Row-major [rows, cols] BF16 with leading dimension ld (elements), boxes of box_rows x 64.
+CUtensorMap make_map(const void* base, int rows, int cols, int ld, int box_rows) {
+    if (reinterpret_cast<std::uintptr_t>(base) % 16 != 0) fail(kEInval, "GEMM operand is not 16-byte aligned");
+    if (ld % 8 != 0) fail(kEInval, "GEMM leading dimension must be a multiple of 8 elements");
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(cols), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ld) * 2};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(BK), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult rc = encode_fn()(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rc != CUDA_SUCCESS) fail(kEInval, "cuTensorMapEncodeTiled rejected a GEMM operand");
+    return map;
+}
+
+template <int BN>
+void launch(const GemmProblem& p, cudaStream_t s) {
+    const CUtensorMap ma = make_map(p.a, p.M, p.K, p.lda, BM);
+    const CUtensorMap mb = make_map(p.b, p.N, p.K, p.ldb, BN);
+    constexpr std::size_t smem = STAGES * (BM + BN) * BK * 2 + 1024 + 256;
+    CUNIBS_CHECK(cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      static_cast<int>(smem)));
+    const dim3 grid((p.N + BN - 1) / BN, (p.M + BM - 1) / BM);
+    gemm_bf16_kernel<BN><<<grid, kThreads, smem, s>>>(ma, mb, p.ep, p.M, p.N, p.K);
+    count_launch();
+    CUNIBS_LAUNCH_CHECK("gemm_bf16");
+}
+
+}  // namespace
+
+void gemm_bf16(const GemmProblem& p, cudaStream_t s) {
+    if (p.M <= 0 || p.N <= 0 || p.K <= 0) fail(kEInval, "GEMM sizes must be positive");
+    if (p.K % 8 != 0) fail(kEInval, "GEMM K must be a multiple of 8");
+    if (p.ep.out16t && p.ep.ld_t < p.M) fail(kEInval, "transposed output leading dimension is below M");
+    if (p.N <= 16) launch<16>(p, s);
+    else if (p.N <= 32) launch<32>(p, s);
+    else launch<128>(p, s);
+}
+
+}  // namespace cunibs

@@ -1,6 +1,7 @@
 // Internal declarations shared by the cunibs_b200 translation units.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <array>
@@ -182,6 +183,58 @@ struct SummaryWork {
 };
 void gm_summary(const Mesh& m, const float* magnE, int k, double* summary_dev /* (k,16) */, SummaryWork& w,
                 cudaStream_t s);
+
+// BF16 tensor-core GEMM (gemm_tc.cu): C[M,N] = A[M,K] . B[N,K]^T, FP32 accumulation, fused tail:
+//   z = acc (+ bias[col]) (* silu'(gate[row, col]));  out32 = z;  h = act ? silu(z) : z;
+//   out16 = bf16(h) row-major;  out16t = bf16(h) transposed ([N, ld_t]).
+struct GemmEpilogue {
+    const float* bias = nullptr;
+    const float* gate = nullptr;
+    int ld_gate = 0;
+    int act = 0;
+    float* out32 = nullptr;
+    __nv_bfloat16* out16 = nullptr;
+    int ld_out = 0;
+    __nv_bfloat16* out16t = nullptr;
+    int ld_t = 0;
+    int* error = nullptr;  // set to 1 when a bounded wait expired
+};
+struct GemmProblem {
+    const __nv_bfloat16* a = nullptr;  // [M, lda], K-major
+    int lda = 0;
+    const __nv_bfloat16* b = nullptr;  // [N, ldb], K-major
+    int ldb = 0;
+    int M = 0, N = 0, K = 0;
+    GemmEpilogue ep;
+};
+void gemm_bf16(const GemmProblem& p, cudaStream_t s);
+
+// Learned warm start (warmstart.cu): an MLP from coil pose to the coefficients of a reduced basis of
+// the grounded potential, prolongated through the basis as the PCG initial guess.
+struct WarmStart {
+    int depth = 0;     // hidden layers
+    int hidden = 0;
+    int n_out = 0;     // basis size
+    int n_out_pad = 0;
+    int n_red = 0;     // rows of the basis (grounded system size)
+    std::vector<DevArray<__nv_bfloat16>> w16;  // per layer [out_pad, in_pad]
+    std::vector<DevArray<float>> bias;         // per layer [out_pad]
+    DevArray<float> in_mean, in_std, out_mean, out_std;
+    DevArray<__nv_bfloat16> basis;             // [n_red, n_out_pad]
+    // Inference workspace.
+    DevArray<__nv_bfloat16> x16, h16a, h16b, c16;
+    DevArray<float> pred, x0f;
+    DevArray<double> partials, norms;
+    DevArray<int> error;
+};
+constexpr int kWarmInPad = 64;  // pose features (6) padded to one BF16 swizzle row
+// Fills X0 (n_red, K) with the network's guess for the k placements whose coil transforms are T_dev
+// (k, 16), then zeroes every column whose initial residual is not below ||b||. used[c] (host) and
+// init_rel[c] (host) report, per column, whether the guess was kept and its relative residual.
+void warm_start_guess(WarmStart& ws, const double* T_dev, int k, int K, const DevCsr<double>& A, const double* B,
+                      double* X0, int* used, double* init_rel, cudaStream_t s);
+void pose_features(const double* T_dev, int k, const float* mean, const float* std, __nv_bfloat16* x16, int ld,
+                   cudaStream_t s);
 
 // Field recovery (recovery.cu). Modes match CUNIBS_RECOVERY_*.
 enum RecoveryMode : int { kRecRaw = 0, kRecSprGlobal = 1, kRecSprTissue = 2, kRecHarmonic = 3 };

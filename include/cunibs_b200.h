@@ -92,6 +92,7 @@ typedef struct {
     double tolerance;  /* <= 0: context default */
     int max_iters;     /* <= 0: context default */
     int recovery;      /* CUNIBS_RECOVERY_*; 0 = raw. magnE, E and the summary describe this field */
+    int warm_start;    /* 1: start PCG from the installed network's guess (cunibs_context_set_warmstart) */
 } cunibs_solve_opts;
 
 /* Outputs of a block solve of k placements. Required: transforms, summary. Optional (NULL to
@@ -108,6 +109,8 @@ typedef struct {
     int total_iterations; /* filled: iterations the block ran */
     int outer_steps;      /* filled: FP64 refinement steps (mixed) */
     float* E_slots;     /* (k, n_slots, 3) recovered field on its slots (NULL to skip; recovery only) */
+    int* warm_used;     /* (k) 1 where the warm-start guess was kept (its residual was below ||b||) */
+    double* init_relres;/* (k) relative residual of the initial guess (1 for the zero guess) */
 } cunibs_block_out;
 
 typedef struct {
@@ -216,6 +219,46 @@ int cunibs_context_recover(cunibs_context* ctx, int mode, int k, const double* v
 
 /* Gray-matter summary of one |E| field on the context's elements (RegionSlice.summarize). */
 int cunibs_context_summary(cunibs_context* ctx, const float* magnE, int k, double* summary);
+
+/* --- learned warm start ------------------------------------------------------------------
+ *
+ * No counterpart in the reference's solver. A network maps a coil pose (the coil origin / 100 mm
+ * and the handle axis: 6 numbers, standardised by feature_mean/std) through `depth` SiLU layers of
+ * width `hidden` to n_out standardised coefficients (coef_mean/std) of a reduced basis of the
+ * grounded potential; the guess is basis . coefficients. All products run on BF16 tensor cores with
+ * FP32 accumulation. Per column, a guess whose relative residual is not below 1 is dropped for the
+ * zero guess; PCG then runs to the same tolerance either way.
+ *
+ * cunibs_context_set_warmstart copies the network from device memory: weights[l] BF16 row-major
+ * [out_l, in_l] with in_0 = 64 (features zero-padded), in_l = hidden, out_l = hidden and
+ * out_depth = n_out rounded up to 64 (= r); biases[l] FP32 [out_l]; basis BF16 [n_nodes - 1, 2 r] in the
+ * grounded (Morton) row order, holding [V_hi | V_lo]: the basis V rounded to BF16 and the BF16
+ * rounding of its remainder (V_lo = bf16(V - V_hi)), so the guess keeps about 16 significant bits.
+ * weights == NULL removes the warm start. */
+int cunibs_context_set_warmstart(cunibs_context* ctx, int depth, int hidden, int n_out, const void* const* weights,
+                                 const float* const* biases, const float* feature_mean, const float* feature_std,
+                                 const float* coef_mean, const float* coef_std, const void* basis);
+
+/* The tensor-core kernels the network is trained with, on device pointers, queued on `stream`
+ * (a cudaStream_t). cunibs_gemm_bf16: C[M,N] = A[M,K] . B[N,K]^T (BF16, K-major, leading dimensions
+ * in elements, K a multiple of 8, 16-byte aligned bases) with FP32 accumulation and the fused tail
+ * z = acc + bias[col] (bias may be NULL), z *= silu'(gate[row, col]) (gate may be NULL),
+ * out32 = z, out16 = bf16(act ? silu(z) : z), out16t = its transpose [N, ld_t]; any output may be
+ * NULL. The others: column sums (bias gradients), mean-squared error and its gradient
+ * (2 (pred - target) / (rows * cols); scratch holds 296 floats), one Adam step with bias correction
+ * and decoupled weight decay that also refreshes BF16 copies [rows, cols] and [cols, rows], and the
+ * standardised BF16 pose features of k coil transforms (k, 16). */
+int cunibs_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int N, int K, const float* bias,
+                     const float* gate, int ld_gate, int act, float* out32, void* out16, int ld_out, void* out16t,
+                     int ld_t, void* stream);
+int cunibs_mlp_colsum(const float* x, int rows, int cols, int ld, float* out, void* stream);
+int cunibs_mlp_mse(const float* pred, const float* target, int rows, int cols, int ld, float* loss, float* d32,
+                   void* d16, void* d16t, int ld_t, float* scratch, void* stream);
+int cunibs_mlp_adam(float* param, float* m, float* v, const float* grad, long long n, float lr, float beta1,
+                    float beta2, float eps, int step, float weight_decay, int rows, int cols, void* w16, void* w16t,
+                    void* stream);
+int cunibs_mlp_features(const double* transforms, int k, const float* mean, const float* std, void* x16, int ld,
+                        void* stream);
 
 /* --- without device allocation ------------------------------------------------------------
  *

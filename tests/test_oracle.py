@@ -161,3 +161,36 @@ def test_summary_center_of_gravity_analytic():
                        np.array([[0.0, 0, 0], [4.0, 0, 0]]), np.array([2, 2], np.int32))
     np.testing.assert_allclose(s[4:7], [2.0, 0.0, 0.0])
     assert s[0] == 2.0 and s[7] == 3.0
+
+
+def test_bf16_restatement_matches_torch():
+    """The network checker's BF16 rounding (oracle/mlp.py) is round-to-nearest-even, as torch's."""
+    import torch
+
+    from oracle.mlp import bf16_round
+
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal(10000) * 10.0 ** rng.integers(-5, 5, 10000)
+    want = torch.tensor(a, dtype=torch.float32).to(torch.bfloat16).to(torch.float64).numpy()
+    np.testing.assert_array_equal(bf16_round(a), want)
+
+
+def test_mlp_restatement_gradients_match_finite_differences():
+    """The FP64 network restatement's backward pass against central differences (no BF16 rounding
+    in play: weights and inputs already BF16, perturbations along one weight)."""
+    from oracle.mlp import bf16_round, forward_backward
+
+    rng = np.random.default_rng(1)
+    W = [bf16_round(rng.standard_normal((16, 8)) * 0.5), bf16_round(rng.standard_normal((8, 16)) * 0.3)]
+    b = [rng.standard_normal(16) * 0.1, rng.standard_normal(8) * 0.1]
+    x = bf16_round(rng.standard_normal((12, 8)))
+    t = rng.standard_normal((12, 8))
+    _, _, dW, _ = forward_backward(W, b, x, t, 8)
+    i, j, h = 3, 2, 1e-6
+    Wp = [W[0], W[1].copy()]
+    Wm = [W[0], W[1].copy()]
+    Wp[1][i, j] += h
+    Wm[1][i, j] -= h
+    lp, *_ = forward_backward(Wp, b, x, t, 8)
+    lm, *_ = forward_backward(Wm, b, x, t, 8)
+    assert dW[1][i, j] == pytest.approx((lp - lm) / (2 * h), rel=1e-3)
