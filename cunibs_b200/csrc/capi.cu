@@ -185,12 +185,17 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
     if (warm) {
         require(c->warm != nullptr, "warm_start requested but no warm-start network is installed");
         require(c->warm->n_red == n_red, "the installed warm start was built for another mesh");
-        const DevCsr<double>& A0 = c->hier.levels.empty() ? c->hier.coarse : c->hier.levels[0].a;
         c->X0.reserve(static_cast<std::size_t>(n_red) * K);
-        warm_start_guess(*c->warm, c->T.get(), k, K, A0, c->B.get(), c->X0.get(), c->warm_used.data(),
-                         c->init_rel.data(), s);
+        warm_start_guess(*c->warm, c->T.get(), k, K, c->X0.get(), s);
     }
     solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, prm, s, st, warm ? c->X0.get() : nullptr);
+    if (warm) {
+        warm_start_check(*c->warm, s);
+        for (int i = 0; i < k; ++i) {
+            c->init_rel[i] = st.col_init_rel[i];
+            c->warm_used[i] = st.col_init_rel[i] < 1.0 ? 1 : 0;
+        }
+    }
     // Columns that missed tolerance: one FP64 retry from their current iterate, then an error
     // (the rebuild-then-retry contract of fem/solve.py:528-551).
     std::vector<int> missed;

@@ -9,6 +9,8 @@
 #include <cfloat>
 #include <climits>
 
+#include <algorithm>
+
 #include "internal.hpp"
 
 namespace cunibs {
@@ -57,26 +59,11 @@ __device__ double closest_on_tri(const double* p, const double* a, const double*
 
 // One block per placement: scan all skin triangles, reduce to the (d2, index) minimum, then
 // thread 0 builds the frame.
-__global__ void place_kernel(const double* __restrict__ nodes, const int* __restrict__ tris, int n_tri,
-                             const double* __restrict__ tnorm, const double* __restrict__ centers,
-                             const double* __restrict__ handles, const double* __restrict__ dists,
-                             double* __restrict__ out, int* __restrict__ degenerate) {
+// (distance^2, triangle) minimum of a block's threads, ties to the lower triangle index: an exact,
+// order-free reduction, so any split of the scan finds the same triangle.
+__device__ __forceinline__ void block_argmin(double& best, int& bi) {
     __shared__ double sd[kBlock];
     __shared__ int si[kBlock];
-    const int p = blockIdx.x;
-    const double center[3] = {centers[3 * p], centers[3 * p + 1], centers[3 * p + 2]};
-    double best = DBL_MAX;
-    int bi = INT_MAX;
-    double q[3];
-    for (int t = threadIdx.x; t < n_tri; t += blockDim.x) {
-        const double d2 = closest_on_tri(center, nodes + 3 * static_cast<long>(tris[3 * t]),
-                                         nodes + 3 * static_cast<long>(tris[3 * t + 1]),
-                                         nodes + 3 * static_cast<long>(tris[3 * t + 2]), q);
-        if (d2 < best) {
-            best = d2;
-            bi = t;
-        }
-    }
     sd[threadIdx.x] = best;
     si[threadIdx.x] = bi;
     __syncthreads();
@@ -91,8 +78,57 @@ __global__ void place_kernel(const double* __restrict__ nodes, const int* __rest
         }
         __syncthreads();
     }
+    best = sd[0];
+    bi = si[0];
+}
+
+// Closest skin triangle to each placement's centre: blockIdx.y = placement, blockIdx.x = one of
+// gridDim.x segments of the triangle list; each segment's minimum goes to part_d/part_i.
+__global__ void nearest_tri_kernel(const double* __restrict__ nodes, const int* __restrict__ tris, int n_tri,
+                                   const double* __restrict__ centers, double* __restrict__ part_d,
+                                   int* __restrict__ part_i) {
+    const int p = blockIdx.y;
+    const double center[3] = {centers[3 * p], centers[3 * p + 1], centers[3 * p + 2]};
+    double best = DBL_MAX;
+    int bi = INT_MAX;
+    double q[3];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tri; t += gridDim.x * blockDim.x) {
+        const double d2 = closest_on_tri(center, nodes + 3 * static_cast<long>(tris[3 * t]),
+                                         nodes + 3 * static_cast<long>(tris[3 * t + 1]),
+                                         nodes + 3 * static_cast<long>(tris[3 * t + 2]), q);
+        if (d2 < best) {
+            best = d2;
+            bi = t;
+        }
+    }
+    block_argmin(best, bi);
+    if (threadIdx.x == 0) {
+        part_d[p * gridDim.x + blockIdx.x] = best;
+        part_i[p * gridDim.x + blockIdx.x] = bi;
+    }
+}
+
+// One block per placement: the minimum over the segments, then the coil frame.
+__global__ void place_kernel(const double* __restrict__ nodes, const int* __restrict__ tris, int n_seg,
+                             const double* __restrict__ part_d, const int* __restrict__ part_i,
+                             const double* __restrict__ tnorm, const double* __restrict__ centers,
+                             const double* __restrict__ handles, const double* __restrict__ dists,
+                             double* __restrict__ out, int* __restrict__ degenerate) {
+    const int p = blockIdx.x;
+    const double center[3] = {centers[3 * p], centers[3 * p + 1], centers[3 * p + 2]};
+    double best = DBL_MAX;
+    int bi = INT_MAX;
+    for (int j = threadIdx.x; j < n_seg; j += blockDim.x) {
+        const double d = part_d[p * n_seg + j];
+        const int i = part_i[p * n_seg + j];
+        if (d < best || (d == best && i < bi)) {
+            best = d;
+            bi = i;
+        }
+    }
+    block_argmin(best, bi);
     if (threadIdx.x != 0) return;
-    const int tri = si[0];
+    const int tri = bi;
     double proj[3];
     closest_on_tri(center, nodes + 3 * static_cast<long>(tris[3 * tri]), nodes + 3 * static_cast<long>(tris[3 * tri + 1]),
                    nodes + 3 * static_cast<long>(tris[3 * tri + 2]), proj);
@@ -146,8 +182,15 @@ void place_transforms(const Mesh& m, const double* centers, const double* handle
                       double* transforms_dev, int* degenerate_dev, cudaStream_t s) {
     if (m.n_skin <= 0) fail(kEInval, "the mesh has no skin triangles to place a coil on");
     if (k <= 0) return;
-    place_kernel<<<k, kBlock, 0, s>>>(m.nodes.get(), m.skin.get(), m.n_skin, m.skin_normals.get(), centers, handles,
-                                      dists, transforms_dev, degenerate_dev); count_launch();
+    // Enough segments that the scan fills the GPU: about 2 x 148 blocks over all placements.
+    const int n_seg = std::max(1, std::min(static_cast<int>(grid_for(m.n_skin)), (296 + k - 1) / k));
+    m.place_d.reserve(static_cast<std::size_t>(n_seg) * k);
+    m.place_i.reserve(static_cast<std::size_t>(n_seg) * k);
+    nearest_tri_kernel<<<dim3(n_seg, k), kBlock, 0, s>>>(m.nodes.get(), m.skin.get(), m.n_skin, centers,
+                                                         m.place_d.get(), m.place_i.get());
+    place_kernel<<<k, kBlock, 0, s>>>(m.nodes.get(), m.skin.get(), n_seg, m.place_d.get(), m.place_i.get(),
+                                      m.skin_normals.get(), centers, handles, dists, transforms_dev, degenerate_dev);
+    count_launch(2);
     CUNIBS_LAUNCH_CHECK("place");
 }
 

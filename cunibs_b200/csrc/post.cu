@@ -57,16 +57,17 @@ __global__ void scatter_kernel(const double* __restrict__ x_red, int K, int grou
     v[q] = (i == ground) ? 0.0 : x_red[static_cast<long>(i - (i > ground ? 1 : 0)) * K + c];
 }
 
+// Sort keys of every placement's gray-matter |E|: (placement << 32) | bits(|E|). |E| >= 0, so its
+// IEEE bit pattern orders like its value, and one stable radix sort of all k segments together
+// orders each placement's values with ties kept in element order.
 __global__ void gm_gather_kernel(const float* __restrict__ magn, const int* __restrict__ gm, int n_gm, int n_tets, int k,
-                                 float* __restrict__ keys, int* __restrict__ vals, int* __restrict__ offsets) {
+                                 std::uint64_t* __restrict__ keys, int* __restrict__ vals) {
     const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q <= k) {
-        if (q <= k) offsets[q] = static_cast<int>(q * n_gm);
-    }
     if (q >= static_cast<long>(n_gm) * k) return;
     const int c = static_cast<int>(q / n_gm);
     const int i = static_cast<int>(q % n_gm);
-    keys[q] = magn[static_cast<long>(c) * n_tets + gm[i]];
+    const float v = magn[static_cast<long>(c) * n_tets + gm[i]];
+    keys[q] = (static_cast<std::uint64_t>(c) << 32) | __float_as_uint(v);
     vals[q] = i;
 }
 
@@ -74,9 +75,10 @@ constexpr int kScanTile = 1024;
 
 // Inclusive scan of the sorted FP64 volumes within each tile of each placement's segment: a
 // sequential walk per 8-element thread strip, then a fixed tree over the strips.
-__global__ void tile_scan_kernel(const int* __restrict__ sorted_idx, const int* __restrict__ gm,
-                                 const float* __restrict__ vols32, int n_gm, double* __restrict__ w_sorted,
-                                 double* __restrict__ cw, double* __restrict__ tile_tot) {
+__global__ void tile_scan_kernel(const int* __restrict__ sorted_idx, const std::uint64_t* __restrict__ sorted_keys,
+                                 const int* __restrict__ gm, const float* __restrict__ vols32, int n_gm,
+                                 float* __restrict__ values, double* __restrict__ w_sorted, double* __restrict__ cw,
+                                 double* __restrict__ tile_tot) {
     constexpr int kPer = kScanTile / 128;
     __shared__ double strip[128];
     const int c = blockIdx.y;
@@ -92,6 +94,7 @@ __global__ void tile_scan_kernel(const int* __restrict__ sorted_idx, const int* 
         if (i < n_gm) {
             w = static_cast<double>(vols32[gm[sorted_idx[base + i]]]);
             w_sorted[base + i] = w;
+            values[base + i] = __uint_as_float(static_cast<unsigned>(sorted_keys[base + i] & 0xffffffffu));
         }
         run += w;
         local[u] = run;
@@ -293,18 +296,20 @@ void gm_summary_impl(const Mesh& m, const float* magnE, int k, double* out, Summ
     w.cw.reserve(total);
     const int tiles = (n + kScanTile - 1) / kScanTile;
     w.tile_tot.reserve(static_cast<std::size_t>(tiles) * k);
-    gm_gather_kernel<<<grid_for(std::max<long>(total, k + 1)), kBlock, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, k,
-                                                                            w.keys.get(), w.vals.get(), w.offsets.get()); count_launch();
+    w.k64.reserve(total);
+    w.k64_s.reserve(total);
+    gm_gather_kernel<<<grid_for(total), kBlock, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, k, w.k64.get(),
+                                                        w.vals.get()); count_launch();
+    int seg_bits = 0;
+    while ((1 << seg_bits) < k) ++seg_bits;
     std::size_t bytes = 0;
-    CUNIBS_CHECK(cub::DeviceSegmentedRadixSort::SortPairs(nullptr, bytes, w.keys.get(), w.keys_s.get(), w.vals.get(),
-                                                         w.vals_s.get(), static_cast<int>(total), k, w.offsets.get(),
-                                                         w.offsets.get() + 1, 0, 32, s));
+    CUNIBS_CHECK(cub::DeviceRadixSort::SortPairs(nullptr, bytes, w.k64.get(), w.k64_s.get(), w.vals.get(),
+                                                 w.vals_s.get(), static_cast<int>(total), 0, 32 + seg_bits, s));
     w.temp.reserve(bytes ? bytes : 1);
-    CUNIBS_CHECK(cub::DeviceSegmentedRadixSort::SortPairs(w.temp.get(), bytes, w.keys.get(), w.keys_s.get(),
-                                                         w.vals.get(), w.vals_s.get(), static_cast<int>(total), k,
-                                                         w.offsets.get(), w.offsets.get() + 1, 0, 32, s));
-    tile_scan_kernel<<<dim3(tiles, k), 128, 0, s>>>(w.vals_s.get(), m.gm_index.get(), m.vols32.get(), n,
-                                                   w.w_sorted.get(), w.cw.get(), w.tile_tot.get()); count_launch();
+    CUNIBS_CHECK(cub::DeviceRadixSort::SortPairs(w.temp.get(), bytes, w.k64.get(), w.k64_s.get(), w.vals.get(),
+                                                 w.vals_s.get(), static_cast<int>(total), 0, 32 + seg_bits, s));
+    tile_scan_kernel<<<dim3(tiles, k), 128, 0, s>>>(w.vals_s.get(), w.k64_s.get(), m.gm_index.get(), m.vols32.get(), n,
+                                                   w.keys_s.get(), w.w_sorted.get(), w.cw.get(), w.tile_tot.get()); count_launch();
     tile_offset_kernel<<<dim3(tiles, k), 256, 0, s>>>(w.cw.get(), w.tile_tot.get(), n, tiles); count_launch();
     summary_kernel<<<k, 512, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, m.vols32.get(), m.bary.get(),
                                      w.keys_s.get(), w.w_sorted.get(), w.cw.get(), out); count_launch();

@@ -76,13 +76,38 @@ __device__ __forceinline__ void final_reduce(const double* __restrict__ partials
     __syncthreads();
 }
 
+// acc + sum of val[p] * x[col[p] * ld + c] over p = p0, p0 + S, ... < e, added in that order. The
+// row is taken eight terms at a time: every index and value load of a batch is issued, then every
+// gather, then the multiply-adds in order (predicated off past the row's end), so a lane has eight
+// index-then-gather chains in flight and a typical row of the finest operator (about 15 entries)
+// costs two rounds of memory latency. The additions, and so the result, keep the plain loop's order.
+template <typename T, int S>
+__device__ __forceinline__ T strided_dot(const int* __restrict__ col, const T* __restrict__ val,
+                                         const T* __restrict__ x, int p, int e, long ld, int c, T acc) {
+    constexpr int B = 8;
+    for (; p < e; p += B * S) {
+        int cj[B];
+        T vj[B], xj[B];
+#pragma unroll
+        for (int j = 0; j < B; ++j) {
+            const int q = p + j * S;
+            const bool ok = q < e;
+            cj[j] = ok ? col[q] : 0;
+            vj[j] = ok ? val[q] : T(0);
+        }
+#pragma unroll
+        for (int j = 0; j < B; ++j) xj[j] = (p + j * S < e) ? x[cj[j] * ld + c] : T(0);
+#pragma unroll
+        for (int j = 0; j < B; ++j)
+            if (p + j * S < e) acc += vj[j] * xj[j];
+    }
+    return acc;
+}
+
 template <typename T>
 __device__ __forceinline__ T row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
                                      const T* __restrict__ val, const T* __restrict__ x, int row, int c, int K) {
-    T s = T(0);
-    const int e = ptr[row + 1];
-    for (int p = ptr[row]; p < e; ++p) s += val[p] * x[static_cast<long>(col[p]) * K + c];
-    return s;
+    return strided_dot<T, 1>(col, val, x, ptr[row], ptr[row + 1], K, c, T(0));
 }
 
 // --- V-cycle kernels ---------------------------------------------------------------------
@@ -127,10 +152,7 @@ __device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const in
                                            const T* __restrict__ val, const T* __restrict__ x, int row, int r,
                                            int sub, int c, bool valid) {
     T acc = T(0);
-    if (valid) {
-        const int e = ptr[row + 1];
-        for (int p = ptr[row] + sub; p < e; p += TPR) acc += val[p] * x[static_cast<long>(col[p]) * K + c];
-    }
+    if (valid) acc = strided_dot<T, TPR>(col, val, x, ptr[row] + sub, ptr[row + 1], K, c, acc);
     if constexpr (TPR == 1) {
         return acc;
     } else if constexpr (TPR * K <= kWarp) {
@@ -402,10 +424,13 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
             const int cc = threadIdx.x;
             const double rel = sqrt(tot[cc]) / sqrt(ref[cc]);
             const double tc = tol_vec ? tol_vec[cc] : tol;
+            // frozen: 0 running, 2 met its target this iteration (its direction update still runs,
+            // so the sequence can resume after a residual replacement), 1 frozen before.
+            if (frozen[cc] == 2) frozen[cc] = 1;
             if (!frozen[cc]) {
                 if (record) rel_out[cc] = rel;
                 if (rel <= tc) {
-                    frozen[cc] = 1;
+                    frozen[cc] = 2;
                     if (record) conv_iter[cc] = it;
                 }
             }
@@ -424,15 +449,20 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
     }
 }
 
-// Finishes the beta update in the last block: rz_new = sum; beta = rz_new / rz (0 when frozen).
+// Finishes the beta update in the last block: rz_new = sum; beta = rz_new / rz. A column frozen
+// before this iteration (frozen == 1) keeps its rz and gets beta = 0 (its direction is not touched).
 template <int K>
 __device__ __forceinline__ void finish_beta(double* partials, double* rz, const int* frozen, double* beta) {
     __shared__ double tot[K];
     final_reduce<K>(partials, gridDim.x, tot);
     if (threadIdx.x < K) {
         const int cc = threadIdx.x;
-        beta[cc] = frozen[cc] ? 0.0 : tot[cc] / rz[cc];
-        rz[cc] = tot[cc];
+        if (frozen[cc] == 1) {
+            beta[cc] = 0.0;
+        } else {
+            beta[cc] = tot[cc] / rz[cc];
+            rz[cc] = tot[cc];
+        }
     }
 }
 
@@ -488,12 +518,15 @@ __global__ void __launch_bounds__(tile_threads<K>()) cheby_dot_kernel(
     if (last_block(counter)) finish_beta<K>(partials, rz, frozen, beta);
 }
 
+// p = z + beta p. A column frozen before this iteration keeps its direction, so a column that met
+// an inner target resumes the same Krylov sequence after the outer step replaces its residual.
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) update_p_kernel(int n, const double* __restrict__ beta,
-                                                                     const T* __restrict__ z, T* __restrict__ p) {
+                                                                     const T* __restrict__ z, T* __restrict__ p,
+                                                                     const int* __restrict__ frozen) {
     const int row = blockIdx.x * kTileRows + threadIdx.x / K;
     const int c = threadIdx.x % K;
-    if (row >= n) return;
+    if (row >= n || frozen[c] == 1) return;
     const long q = static_cast<long>(row) * K + c;
     p[q] = z[q] + static_cast<T>(beta[c]) * p[q];
 }
@@ -567,6 +600,25 @@ __global__ void __launch_bounds__(tile_threads<K>()) residual64_kernel(int n, co
     R[q] = B[q] - ax;
 }
 
+// The zero-guess fallback of a warm start: a column whose guess leaves ||R|| >= ||B|| restarts from
+// X = 0, R = B. init_rel[c] receives the kept guess's relative residual (1 when dropped).
+template <int K>
+__global__ void __launch_bounds__(tile_threads<K>()) guess_fallback_kernel(int n, double* __restrict__ X,
+                                                                           double* __restrict__ R,
+                                                                           const double* __restrict__ B,
+                                                                           const double* __restrict__ ref_sq,
+                                                                           const double* __restrict__ r0sq,
+                                                                           double* __restrict__ init_rel) {
+    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    const bool keep = r0sq[c] < ref_sq[c];
+    if (blockIdx.x == 0 && threadIdx.x < K) init_rel[c] = keep ? sqrt(r0sq[c] / ref_sq[c]) : 1.0;
+    if (row >= n || keep) return;
+    const long q = static_cast<long>(row) * K + c;
+    X[q] = 0.0;
+    R[q] = B[q];
+}
+
 template <int K>
 __global__ void __launch_bounds__(tile_threads<K>()) add_correction_kernel(int n, double* __restrict__ X,
                                                                            const float* __restrict__ d) {
@@ -605,7 +657,7 @@ class Solver {
     VWork<float> v32;
     VWork<double> v64;
     // Per-column scalars.
-    DevArray<double> rz, alpha, beta, ref_sq, rr0, rel, eta, partials;
+    DevArray<double> rz, alpha, beta, ref_sq, rr0, rel, eta, partials, r0sq, init_rel;
     DevArray<int> frozen, outer_conv, conv_iter, iter_counter;
     DevArray<unsigned> counter;
     int* h_flags = nullptr;   // pinned
@@ -649,7 +701,7 @@ class Solver {
         v32.cx.resize(mc);
         v64.cb.resize(mc);
         v64.cx.resize(mc);
-        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta}) a->resize(K);
+        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta, &r0sq, &init_rel}) a->resize(K);
         for (auto* a : {&frozen, &outer_conv, &conv_iter}) a->resize(K);
         iter_counter.resize(1);
         cap.resize(1);
@@ -766,7 +818,22 @@ class Solver {
     template <int K>
     void solve_plain(int k, const Params& prm, SolveStats& st, bool warm);
     template <int K>
-    void solve_mixed(int k, const Params& prm, SolveStats& st);
+    void solve_mixed(int k, const Params& prm, SolveStats& st, bool warm);
+    // R = B - A X in FP64 for a warm start, then the per-column zero-guess fallback.
+    template <int K>
+    void warm_residual(const DevCsr<double>& A) {
+        constexpr int TT = tile_threads<K>();
+        dispatch_tpr<K>(tpr0(), [&](auto tc) {
+            constexpr int TPR = decltype(tc)::value;
+            residual64_kernel<K, TPR><<<(n + ReduceTile<TPR>::kRows - 1) / ReduceTile<TPR>::kRows, TT, 0, stream>>>(
+                n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), R.get());
+        });
+        norm2_kernel<double, K><<<reduce_grid(n), TT, 0, stream>>>(n, R.get(), partials.get(), counter.get(),
+                                                                  r0sq.get());
+        guess_fallback_kernel<K><<<n_tiles(n), TT, 0, stream>>>(n, X.get(), R.get(), B.get(), ref_sq.get(),
+                                                                r0sq.get(), init_rel.get());
+        count_launch(3);
+    }
 
     template <typename Body>
     void run_graph(std::tuple<int, int, int> key, Body&& body) {
@@ -965,7 +1032,7 @@ void Solver::pcg_tail(T* r, T* z, T* p, bool jz_done) {
                                                                 frozen.get(), beta.get());
         count_launch();
     }
-    update_p_kernel<T, K><<<n_tiles(n), TT, 0, stream>>>(n, beta.get(), z, p);
+    update_p_kernel<T, K><<<n_tiles(n), TT, 0, stream>>>(n, beta.get(), z, p, frozen.get());
     count_launch();
 }
 
@@ -999,12 +1066,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     const std::size_t nk = static_cast<std::size_t>(n) * K;
     norm2_kernel<double, K><<<reduce_grid(n), TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
     if (warm) {
-        dispatch_tpr<K>(tpr0(), [&](auto tc) {
-            constexpr int TPR = decltype(tc)::value;
-            residual64_kernel<K, TPR><<<(n + ReduceTile<TPR>::kRows - 1) / ReduceTile<TPR>::kRows, TT, 0, s>>>(
-                n, A.ptr.get(), A.col.get(), A.val.get(), B.get(), X.get(), R.get());
-        });
-        count_launch();
+        warm_residual<K>(A);
     } else {
         X.zero(s);
         CUNIBS_CHECK(cudaMemcpyAsync(R.get(), B.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -1055,7 +1117,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
 }
 
 template <int K>
-void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
+void Solver::solve_mixed(int k, const Params& prm, SolveStats& st, bool warm) {
     constexpr int TT = tile_threads<K>();
     const unsigned g = n_tiles(n);
     cudaStream_t s = stream;
@@ -1064,6 +1126,7 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
     DevArray<float> coarse32;
     if (A32 == nullptr) fail(kEInval, "mixed precision needs at least one AMG level");
     norm2_kernel<double, K><<<reduce_grid(n), TT, 0, s>>>(n, B.get(), partials.get(), counter.get(), ref_sq.get()); count_launch();
+    if (warm) warm_residual<K>(A);
     outer_conv.zero(s);
     iter_counter.zero(s);
     CUNIBS_CHECK(cudaMemcpyAsync(h_dbl, ref_sq.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
@@ -1090,6 +1153,9 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st) {
         bool all = true;
         for (int c = 0; c < k; ++c) all = all && h_flags[c];
         if (all || total_inner >= prm.max_iters) break;
+        // Each inner solve starts a fresh FP32 Krylov sequence on the true residual. (Continuing the
+        // previous sequence across the replacement was measured: the FP32 recurrence drifts too far
+        // from the true residual for the old direction to stay useful.)
         d32.zero(s);
         p32.zero(s);
         fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
@@ -1173,8 +1239,15 @@ void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, con
         CUNIBS_CHECK(cudaMemcpyAsync(sv.B.get(), Bin, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
         if (X0) CUNIBS_CHECK(cudaMemcpyAsync(sv.X.get(), X0, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
         else sv.X.zero(sv.stream);
-        if (prm.precision == kMixed) sv.solve_mixed<KK>(k, prm, st);
+        if (prm.precision == kMixed) sv.solve_mixed<KK>(k, prm, st, X0 != nullptr);
         else sv.solve_plain<KK>(k, prm, st, X0 != nullptr);
+        if (X0) {
+            double h_init[16];
+            CUNIBS_CHECK(cudaMemcpyAsync(h_init, sv.init_rel.get(), sizeof(double) * KK, cudaMemcpyDeviceToHost,
+                                         sv.stream));
+            CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
+            st.col_init_rel.assign(h_init, h_init + k);
+        }
         CUNIBS_CHECK(cudaMemcpyAsync(Xout, sv.X.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
         CUNIBS_CHECK(cudaMemcpyAsync(sv.h_flags, sv.conv_iter.get(), sizeof(int) * KK, cudaMemcpyDeviceToHost, sv.stream));
         CUNIBS_CHECK(cudaMemcpyAsync(sv.h_dbl, sv.rel.get(), sizeof(double) * KK, cudaMemcpyDeviceToHost, sv.stream));

@@ -135,69 +135,6 @@ __global__ void widen_kernel(const float* __restrict__ x0f, int n, int ldf, int 
     X0[q] = c < k ? static_cast<double>(r[c]) + static_cast<double>(r[16 + c]) : 0.0;
 }
 
-// Per-column partial sums of ||B - A X0||^2 and ||B||^2: rows in a fixed grid-stride order per
-// thread, then a fixed tree per block; the column count does not change any column's order.
-__global__ void __launch_bounds__(kReduceThreads) init_residual_kernel(int n, const int* __restrict__ ptr,
-                                                                       const int* __restrict__ col,
-                                                                       const double* __restrict__ val,
-                                                                       const double* __restrict__ B,
-                                                                       const double* __restrict__ X, int K,
-                                                                       double* __restrict__ partial) {
-    __shared__ double red[kReduceThreads];
-    double rr[16], bb[16];
-#pragma unroll
-    for (int c = 0; c < 16; ++c) rr[c] = bb[c] = 0.0;
-    for (int row = blockIdx.x * blockDim.x + threadIdx.x; row < n; row += gridDim.x * blockDim.x) {
-        double ax[16];
-#pragma unroll
-        for (int c = 0; c < 16; ++c) ax[c] = 0.0;
-        for (int p = ptr[row]; p < ptr[row + 1]; ++p) {
-            const double a = val[p];
-            const double* xr = X + static_cast<std::int64_t>(col[p]) * K;
-#pragma unroll
-            for (int c = 0; c < 16; ++c)
-                if (c < K) ax[c] = fma(a, xr[c], ax[c]);
-        }
-        const double* br = B + static_cast<std::int64_t>(row) * K;
-#pragma unroll
-        for (int c = 0; c < 16; ++c)
-            if (c < K) {
-                const double r = br[c] - ax[c];
-                rr[c] = fma(r, r, rr[c]);
-                bb[c] = fma(br[c], br[c], bb[c]);
-            }
-    }
-    for (int c = 0; c < 2 * K; ++c) {
-        red[threadIdx.x] = c < K ? rr[c & 15] : bb[(c - K) & 15];
-        __syncthreads();
-        for (int off = kReduceThreads / 2; off > 0; off >>= 1) {
-            if (threadIdx.x < off) red[threadIdx.x] += red[threadIdx.x + off];
-            __syncthreads();
-        }
-        if (threadIdx.x == 0) partial[static_cast<std::int64_t>(c) * gridDim.x + blockIdx.x] = red[0];
-        __syncthreads();
-    }
-}
-
-// norms[c] = relative initial residual; a column whose guess is no better than zero is zeroed.
-__global__ void init_decide_kernel(const double* __restrict__ partial, int blocks, int K, int k,
-                                   double* __restrict__ norms) {
-    const int c = threadIdx.x;
-    if (c >= K) return;
-    double rr = 0.0, bb = 0.0;
-    for (int b = 0; b < blocks; ++b) {
-        rr += partial[static_cast<std::int64_t>(c) * blocks + b];
-        bb += partial[static_cast<std::int64_t>(K + c) * blocks + b];
-    }
-    norms[c] = (c < k && bb > 0.0) ? sqrt(rr / bb) : 2.0;
-}
-
-__global__ void drop_columns_kernel(double* __restrict__ X0, int n, int K, const double* __restrict__ norms) {
-    const std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q >= static_cast<std::int64_t>(n) * K) return;
-    if (!(norms[q % K] < 1.0)) X0[q] = 0.0;
-}
-
 }  // namespace
 
 void pose_features(const double* T_dev, int k, const float* mean, const float* std, __nv_bfloat16* x16, int ld,
@@ -207,8 +144,7 @@ void pose_features(const double* T_dev, int k, const float* mean, const float* s
     CUNIBS_LAUNCH_CHECK("pose features");
 }
 
-void warm_start_guess(WarmStart& ws, const double* T_dev, int k, int K, const DevCsr<double>& A, const double* B,
-                      double* X0, int* used, double* init_rel, cudaStream_t s) {
+void warm_start_guess(WarmStart& ws, const double* T_dev, int k, int K, double* X0, cudaStream_t s) {
     constexpr int kRowsPad = 16;  // the network's batch (k <= 16), one BN = 16 GEMM tile wide
     const int depth = ws.depth;
     ws.x16.reserve(kRowsPad * kWarmInPad);
@@ -277,26 +213,14 @@ void warm_start_guess(WarmStart& ws, const double* T_dev, int k, int K, const De
     const std::int64_t nk = static_cast<std::int64_t>(ws.n_red) * K;
     widen_kernel<<<grid_for(nk), kBlock, 0, s>>>(ws.x0f.get(), ws.n_red, 2 * kRowsPad, k, K, X0);
     count_launch();
-    // Fallback per column: keep the guess only where its residual is below ||b||.
-    ws.partials.reserve(static_cast<std::size_t>(2 * K) * kReduceBlocks);
-    init_residual_kernel<<<kReduceBlocks, kReduceThreads, 0, s>>>(A.n, A.ptr.get(), A.col.get(), A.val.get(), B, X0,
-                                                                  K, ws.partials.get());
-    count_launch();
-    init_decide_kernel<<<1, 32, 0, s>>>(ws.partials.get(), kReduceBlocks, K, k, ws.norms.get());
-    count_launch();
-    drop_columns_kernel<<<grid_for(nk), kBlock, 0, s>>>(X0, ws.n_red, K, ws.norms.get());
-    count_launch();
     CUNIBS_LAUNCH_CHECK("warm start");
-    double h_norms[16];
+}
+
+void warm_start_check(WarmStart& ws, cudaStream_t s) {
     int h_err = 0;
-    CUNIBS_CHECK(cudaMemcpyAsync(h_norms, ws.norms.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
     CUNIBS_CHECK(cudaMemcpyAsync(&h_err, ws.error.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
     CUNIBS_CHECK(cudaStreamSynchronize(s));
     if (h_err) fail(kETimeout, "a tensor-core GEMM of the warm start timed out waiting on its pipeline");
-    for (int c = 0; c < k; ++c) {
-        used[c] = h_norms[c] < 1.0 ? 1 : 0;
-        init_rel[c] = used[c] ? h_norms[c] : 1.0;
-    }
 }
 
 }  // namespace cunibs

@@ -313,6 +313,8 @@ def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: i
     # Training.
     t2 = time.perf_counter()
     mlp = PoseMLP(r, hidden, depth, seed)
+    if n_train < 2 * batch:
+        batch = max(8, (n_train // 2) // 8 * 8)
     n_hold = max(batch, n_train // 8)
     n_fit = (n_train - n_hold) // batch * batch
     gen = torch.Generator(device="cpu").manual_seed(seed + 1)

@@ -69,7 +69,7 @@ typedef struct {
     double tolerance;         /* ||r||/||b|| stopping criterion; DEFAULT_TOLERANCE = 1e-6 (fem/solve.py:56) */
     int max_iters;            /* DEFAULT_MAX_ITERS = 2000 */
     int precision;            /* CUNIBS_PREC_* */
-    double inner_reduction;   /* mixed: smallest residual reduction asked of one inner FP32 solve */
+    double inner_reduction;   /* mixed: deepest residual reduction asked of one inner FP32 solve */
     int inner_max_iters;      /* mixed: iteration cap of each inner FP32 solve */
     int iters_per_sync;       /* PCG iterations launched between host convergence checks */
 } cunibs_params;
