@@ -212,18 +212,49 @@ __global__ void __launch_bounds__(kThreads, 1)
                 float v[16];
                 tmem_ld16(tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c), v);
                 const bool row_ok = row < M;
+                const int col0 = n0 + c;
+                float z[16], h[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const int col = n0 + c + j;
-                    if (!row_ok || col >= N) continue;
-                    float z = v[j];
-                    if (ep.bias) z += ep.bias[col];
-                    const std::int64_t at = static_cast<std::int64_t>(row) * ep.ld_out + col;
-                    if (ep.gate) z *= silu_grad(ep.gate[static_cast<std::int64_t>(row) * ep.ld_gate + col]);
-                    if (ep.out32) ep.out32[at] = z;
-                    const float h = ep.act == 1 ? silu(z) : z;
-                    if (ep.out16) ep.out16[at] = __float2bfloat16_rn(h);
-                    if (ep.out16t) ep.out16t[static_cast<std::int64_t>(col) * ep.ld_t + row] = __float2bfloat16_rn(h);
+                    const int col = col0 + j;
+                    float t = v[j];
+                    if (row_ok && col < N) {
+                        if (ep.bias) t += ep.bias[col];
+                        if (ep.gate) t *= silu_grad(ep.gate[static_cast<std::int64_t>(row) * ep.ld_gate + col]);
+                    }
+                    z[j] = t;
+                    h[j] = ep.act == 1 ? silu(t) : t;
+                }
+                if (!row_ok) continue;
+                const std::int64_t at = static_cast<std::int64_t>(row) * ep.ld_out + col0;
+                // A full, aligned 16-column run goes out as 16-byte vector stores; the ragged edge
+                // (or an unaligned leading dimension) element by element.
+                const bool full = col0 + 16 <= N && (ep.ld_out % 8) == 0;
+                if (ep.out32) {
+                    if (full && (reinterpret_cast<std::uintptr_t>(ep.out32) & 15) == 0) {
+#pragma unroll
+                        for (int j = 0; j < 16; j += 4)
+                            *reinterpret_cast<float4*>(ep.out32 + at + j) = make_float4(z[j], z[j + 1], z[j + 2], z[j + 3]);
+                    } else {
+                        for (int j = 0; j < 16 && col0 + j < N; ++j) ep.out32[at + j] = z[j];
+                    }
+                }
+                if (ep.out16) {
+                    if (full && (reinterpret_cast<std::uintptr_t>(ep.out16) & 15) == 0) {
+#pragma unroll
+                        for (int j = 0; j < 16; j += 8) {
+                            __nv_bfloat162 q[4];
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) q[u] = __floats2bfloat162_rn(h[j + 2 * u], h[j + 2 * u + 1]);
+                            *reinterpret_cast<uint4*>(ep.out16 + at + j) = *reinterpret_cast<uint4*>(q);
+                        }
+                    } else {
+                        for (int j = 0; j < 16 && col0 + j < N; ++j) ep.out16[at + j] = __float2bfloat16_rn(h[j]);
+                    }
+                }
+                if (ep.out16t) {
+                    for (int j = 0; j < 16 && col0 + j < N; ++j)
+                        ep.out16t[static_cast<std::int64_t>(col0 + j) * ep.ld_t + row] = __float2bfloat16_rn(h[j]);
                 }
             }
         } else {

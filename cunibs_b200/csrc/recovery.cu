@@ -550,26 +550,13 @@ __global__ void harmonic_apply_kernel(const float4* __restrict__ wq, const int* 
     const int s = static_cast<int>(q / K), c = static_cast<int>(q % K);
     if (s >= n_slots || c >= k) return;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    // Eight patch entries per round: their records, then their potentials, then the multiply-adds in
-    // patch order (so the sums are the plain loop's).
-    constexpr int B = 8;
-    for (int p = pptr[s], end = pptr[s + 1]; p < end; p += B) {
-        float4 e[B];
-        double vm[B];
-#pragma unroll
-        for (int j = 0; j < B; ++j) e[j] = (p + j < end) ? wq[p + j] : make_float4(0.f, 0.f, 0.f, __int_as_float(ground));
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            const int m = __float_as_int(e[j].w);
-            vm[j] = (m == ground) ? 0.0 : x[static_cast<std::int64_t>(m - (m > ground ? 1 : 0)) * K + c];
-        }
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            if (p + j >= end) break;
-            ax = fma(static_cast<double>(e[j].x), vm[j], ax);
-            ay = fma(static_cast<double>(e[j].y), vm[j], ay);
-            az = fma(static_cast<double>(e[j].z), vm[j], az);
-        }
+    for (int p = pptr[s], end = pptr[s + 1]; p < end; ++p) {
+        const float4 e = wq[p];
+        const int m = __float_as_int(e.w);
+        const double vm = (m == ground) ? 0.0 : x[static_cast<std::int64_t>(m - (m > ground ? 1 : 0)) * K + c];
+        ax = fma(static_cast<double>(e.x), vm, ax);
+        ay = fma(static_cast<double>(e.y), vm, ay);
+        az = fma(static_cast<double>(e.z), vm, az);
     }
     const int node = slot_node[s];
     const float* da = dadt_nodes + (static_cast<std::int64_t>(c) * n_nodes + node) * 3;
@@ -588,30 +575,12 @@ __global__ void spr_apply_kernel(const float* __restrict__ w, const int* __restr
     const int c = static_cast<int>(q / n_slots), s = static_cast<int>(q % n_slots);
     const float* ec = e_elem + static_cast<std::int64_t>(c) * n_tets * 3;
     float ax = 0.f, ay = 0.f, az = 0.f;
-    constexpr int B = 8;
-    for (int p = ptr[s], end = ptr[s + 1]; p < end; p += B) {
-        float wp[B], ex[B], ey[B], ez[B];
-        int el[B];
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            const bool ok = p + j < end;
-            wp[j] = ok ? w[p + j] : 0.f;
-            el[j] = ok ? (idx[p + j] >> 2) : 0;
-        }
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            const float* ee = ec + 3 * static_cast<std::int64_t>(el[j]);
-            ex[j] = ee[0];
-            ey[j] = ee[1];
-            ez[j] = ee[2];
-        }
-#pragma unroll
-        for (int j = 0; j < B; ++j) {
-            if (p + j >= end) break;
-            ax = fmaf(wp[j], ex[j], ax);
-            ay = fmaf(wp[j], ey[j], ay);
-            az = fmaf(wp[j], ez[j], az);
-        }
+    for (int p = ptr[s], end = ptr[s + 1]; p < end; ++p) {
+        const float wp = w[p];
+        const float* ee = ec + 3 * static_cast<std::int64_t>(idx[p] >> 2);
+        ax = fmaf(wp, ee[0], ax);
+        ay = fmaf(wp, ee[1], ay);
+        az = fmaf(wp, ee[2], az);
     }
     float* o = e_slots + q * 3;
     o[0] = ax;

@@ -212,6 +212,13 @@ __global__ void conductivity_kernel(const int* __restrict__ tags, int m, double*
     if (threadIdx.x == 0 && c) atomicAdd(bad, c);
 }
 
+// -(vol * sigma) in FP32, the right-hand side's per-element weight (fem/solve.py:714).
+__global__ void neg_vc_kernel(const float* __restrict__ vols32, const double* __restrict__ cond, int m,
+                              float* __restrict__ neg_vc32) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < m) neg_vc32[e] = -(vols32[e] * static_cast<float>(cond[e]));
+}
+
 __global__ void resident_kernel(const double* __restrict__ g, const double* __restrict__ vols,
                                 const double* __restrict__ cond, const double* __restrict__ nodes,
                                 const int* __restrict__ tets, int m, float* __restrict__ g32,
@@ -603,6 +610,9 @@ void assemble_stiffness(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
         bad.zero(s);
         conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, m.cond.get(), bad.get()); count_launch();
         if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
+        // The right-hand side weighs each element by the same conductivity.
+        neg_vc_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.vols32.get(), m.cond.get(), m.n_tets, m.neg_vc32.get());
+        count_launch();
     }
     const std::int64_t Q = 16 * static_cast<std::int64_t>(m.n_tets);
     DevArray<double> ev(Q);

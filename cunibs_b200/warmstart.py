@@ -269,6 +269,7 @@ def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: i
     install it in the context. Returns the model with timing and loss statistics."""
     torch = _torch()
     t0 = time.perf_counter()
+    rank = min(rank, n_train)  # the POD of n_train solves has at most n_train modes
     centers, handles = cap_poses(n_train, radius_mm, z_min_mm, seed)
     T, X, iters = generate_solves(ctx, coil, centers, handles, tolerance=tolerance)
     torch.cuda.synchronize()

@@ -233,3 +233,33 @@ def test_invalid_inputs_raise(sphere_mesh):
 
         bad = HeadMesh([[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0]], [[0, 1, 2, 3]], [2], [[0, 1, 2]])
         _native.Context(bad.nodes_mm, bad.tet_nodes, bad.tet_tags, bad.skin_tris)
+
+
+def test_conductivity_resetup_scale_invariance(sphere_mesh):
+    """cunibs_context_set_conductivity (the per-sample step of a conductivity Monte Carlo): E depends
+    on conductivity ratios only, so scaling every tissue leaves the field unchanged, while changing
+    one tissue changes it; the default table restores the original field."""
+    from cunibs_b200.fem import TISSUE_CONDUCTIVITY
+
+    subj = Subject(sphere_mesh, tolerance=1e-10, precision="plain")
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    site = Placement(top, top + [0, 50, 0])
+    base = subj.simulate(coil, site, magnitude=True, recovery="raw").magnE.astype(np.float64)
+    sigma = np.zeros(11)
+    for tag, s in TISSUE_CONDUCTIVITY.items():
+        sigma[tag] = s
+    gm = subj.mesh.tet_tags == 2
+
+    def rel(a):
+        return np.linalg.norm(a[gm] - base[gm]) / np.linalg.norm(base[gm])
+
+    subj.context.set_conductivity(2.5 * sigma)
+    assert rel(subj.simulate(coil, site, magnitude=True, recovery="raw").magnE.astype(np.float64)) <= 1e-6
+    bumped = sigma.copy()
+    bumped[3] *= 3.0  # CSF
+    subj.context.set_conductivity(bumped)
+    assert rel(subj.simulate(coil, site, magnitude=True, recovery="raw").magnE.astype(np.float64)) >= 1e-3
+    subj.context.set_conductivity(sigma)
+    assert rel(subj.simulate(coil, site, magnitude=True, recovery="raw").magnE.astype(np.float64)) <= 1e-6
+    subj.free()

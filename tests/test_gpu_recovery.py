@@ -142,3 +142,23 @@ def test_nodal_field(patch_mesh, d70_coil, patch_placement, tmp_path):
     with pytest.raises(ValueError, match="nodal=True needs a recovery mode"):
         subj.simulate(d70_coil, patch_placement, nodal=True, recovery="raw")
     subj.free()
+
+
+def test_gpu_field_matches_the_closed_form_sphere():
+    """The GPU path (default harmonic recovery, mixed precision) on a 678k-tet five-shell sphere
+    against the closed-form field (oracle/analytic_sphere.py): measured 0.027 GM relative L2."""
+    from oracle.analytic_sphere import head_frame_dipoles, sphere_efield
+
+    mesh = sphere_head(3.0, 90.0, jitter_mm=0.0, seed=0)
+    subj = Subject(mesh, tolerance=1e-8)
+    coil = figure8_coil(256)
+    top = np.array([0.0, 0.0, 90.0])
+    r = subj.simulate(coil, Placement(top, top + [0, 50, 0]), vectors=True)
+    pos, mom = head_frame_dipoles(coil, r.transform)
+    ordered = subj.mesh
+    gm = ordered.tet_tags == 2
+    bary = ordered.tet_barycenters_mm[gm] * 1e-3
+    Ea = sphere_efield(bary, pos, mom)
+    Ef = r.E[gm].astype(np.float64)
+    assert np.linalg.norm(Ef - Ea) / np.linalg.norm(Ea) <= 0.05
+    subj.free()
