@@ -113,6 +113,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def job_throughput(local_ms: float, steps: int, world: int, dist=None, device="cpu") -> tuple[float, float]:
+    """Whole-job placements/s of `world` replicas that each timed `steps` blocks of K_BLOCK
+    placements: the slowest rank's time (max over ranks) bounds the job."""
+    import torch
+
+    total_ms = float(local_ms)
+    if dist is not None and world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    return total_ms, world * steps * K_BLOCK / (total_ms / 1e3)
+
+
 def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float]:
     """Algorithmic bytes of one PCG iteration and of one FP64 refinement step at block width K.
 
@@ -275,11 +288,9 @@ def run_ours(args) -> dict:
         step(precision=_native.PREC_PLAIN_FP64, warm=False)
     cold_ms, cold_it = timed(n_cmp, warm=False)
     plain_ms, plain_it = timed(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
-    if dist is not None:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * args.steps * K_BLOCK / (total_ms / 1e3)
+    total_ms, value = job_throughput(total_ms, args.steps, world, dist, dev)
+    cold_ms, cold_value = job_throughput(cold_ms, n_cmp, world, dist, dev)
+    plain_ms, plain_value = job_throughput(plain_ms, n_cmp, world, dist, dev)
 
     # End to end through the host C ABI (host buffers in and out).
     e2e_ms = []
@@ -331,10 +342,10 @@ def run_ours(args) -> dict:
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
-        "vs_plain_fp64": {"value": round(world * n_cmp * K_BLOCK / (plain_ms / 1e3), 3), "unit": "placements/s",
+        "vs_plain_fp64": {"value": round(plain_value, 3), "unit": "placements/s",
                           "iterations": plain_it, "ratio": round((plain_ms / n_cmp) / (total_ms / args.steps), 3),
                           "what": "plain FP64 zero-guess PCG, same block, same GPU"},
-        "ablation": {"mixed_zero_guess": {"value": round(world * n_cmp * K_BLOCK / (cold_ms / 1e3), 3),
+        "ablation": {"mixed_zero_guess": {"value": round(cold_value, 3),
                                           "iterations": cold_it},
                      "this_run": {"warm_start": args.warm_start, "iterations": col_iters,
                                   "warm_used": warm_used, "init_relres": [round(v, 5) for v in warm_rel0]}},
