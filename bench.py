@@ -8,7 +8,7 @@ one block (block_k = 8) to relative residual 1e-8. A step is one block of 8 plac
 placement, dA/dt, right-hand side, block PCG, field recovery (harmonic by default, as Subject.simulate)
 and gray-matter summary.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|plain]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision split|mixed|plain]
 
 Prints one JSON line (rank 0). ``value`` is device-timed with CUDA events on the library's stream,
 inputs resident in HBM, L2 flushed between steps; ``e2e`` goes through the host C ABI call
@@ -129,8 +129,8 @@ def job_throughput(local_ms: float, steps: int, world: int, dist=None, device="c
 def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float]:
     """Algorithmic bytes of one PCG iteration and of one FP64 refinement step at block width K.
 
-    Unique bytes each kernel must move, no reuse credit. v_b/v_x: value/vector bytes, 4 in the
-    mixed inner iteration, 8 in the plain one. On level l with n rows, nnz entries, a prolongator of
+    Unique bytes each kernel must move, no reuse credit. v_b/v_x: the V-cycle's value/vector bytes,
+    4 except in plain FP64; k_b/k_x: the Krylov body's, 4 only in mixed precision. On level l with n rows, nnz entries, a prolongator of
     pnnz entries and nc coarse rows:
       SpMV      nnz*(v_b+4) + 4*(n+1) + 2*v_x*K*n      (values, columns, row pointers, x and y)
       Chebyshev SpMV + 4*n + 4*v_x*K*n                  (+ dinv; x_cur, x_prev, b, out)
@@ -140,7 +140,9 @@ def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float
       coarse    v_b*nc^2 + 2*v_x*K*nc
     and the PCG body's BLAS-1 passes count each (n, K) vector read or written once.
     """
-    vb = vx = 4 if precision == "mixed" else 8
+    # The V-cycle streams FP32 copies except in plain FP64; the Krylov body is FP32 only in mixed.
+    vb = vx = 8 if precision == "plain" else 4
+    kb = kx = 4 if precision == "mixed" else 8
     sizes = ctx.levels()
     L = ctx.n_levels
     deg = 2
@@ -163,10 +165,12 @@ def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float
     total += vb * nc * nc + 2 * vx * K * nc
     n0 = sizes[0]
     nnz0 = ctx.array("a_col", 0).shape[0] if L > 0 else 0
-    total += nnz0 * (vb + 4) + 4 * (n0 + 1) + 2 * vx * K * n0  # Ap = A p (+ p.Ap)
-    total += 6 * vx * K * n0  # x += a p, r -= a Ap (+ ||r||)
+    total += nnz0 * (kb + 4) + 4 * (n0 + 1) + 2 * kx * K * n0  # Ap = A p (+ p.Ap)
+    total += 6 * kx * K * n0  # x += a p, r -= a Ap (+ ||r||)
+    if precision == "split":
+        total += vx * K * n0  # r rounded to FP32 for the V-cycle
     total += 2 * vx * K * n0  # r.z
-    total += 3 * vx * K * n0  # p = z + b p
+    total += (2 * kx + vx) * K * n0  # p = z + b p
     outer = nnz0 * 12 + 4 * (n0 + 1) + (8 + 8 + 4) * K * n0 + 20 * K * n0  # B - A X in FP64; X += d
     return float(total), float(outer)
 
@@ -192,7 +196,8 @@ def run_ours(args) -> dict:
     p = _native.default_params()
     p.device = local
     p.tolerance = TOL
-    p.precision = _native.PREC_MIXED if args.precision == "mixed" else _native.PREC_PLAIN_FP64
+    p.precision = {"mixed": _native.PREC_MIXED, "split": _native.PREC_SPLIT, "plain": _native.PREC_PLAIN_FP64}[
+        args.precision]
     t0 = time.perf_counter()
     ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
     setup_s = time.perf_counter() - t0
@@ -284,15 +289,19 @@ def run_ours(args) -> dict:
     warm_used = d_used.cpu().numpy().tolist()
     warm_rel0 = d_rel0.cpu().numpy().tolist()
     col_iters = float(d_it.float().mean().item())
-    # The same block on the same GPU without the learned guess: mixed precision, and plain FP64 PCG.
+    # The same block on the same GPU without the learned guess (this precision), with FP64
+    # iterative refinement around FP32 PCG, and with plain FP64 PCG.
     n_cmp = max(1, min(args.steps, 5))
     for _ in range(2):
         step(warm=False)
+        step(precision=_native.PREC_MIXED, warm=False)
         step(precision=_native.PREC_PLAIN_FP64, warm=False)
     cold_ms, cold_it = timed(n_cmp, warm=False)
+    mixed_ms, mixed_it = timed(n_cmp, precision=_native.PREC_MIXED, warm=False)
     plain_ms, plain_it = timed(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
     total_ms, value = job_throughput(total_ms, args.steps, world, dist, dev)
     cold_ms, cold_value = job_throughput(cold_ms, n_cmp, world, dist, dev)
+    mixed_ms, mixed_value = job_throughput(mixed_ms, n_cmp, world, dist, dev)
     plain_ms, plain_value = job_throughput(plain_ms, n_cmp, world, dist, dev)
 
     # End to end through the host C ABI (host buffers in and out).
@@ -336,7 +345,8 @@ def run_ours(args) -> dict:
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": ("f32 (FP32 PCG/V-cycle/dA-dt) with f64 refinement" if args.precision == "mixed" else "f64")
+        "dtype": {"mixed": "f32 (FP32 PCG/V-cycle/dA-dt) with f64 refinement",
+                  "split": "f64 PCG over an f32 V-cycle (f32 dA-dt)", "plain": "f64"}[args.precision]
                  + ("; bf16 tensor-core warm start" if args.warm_start == "on" else ""),
         "data": "synthetic: seeded sphere head and figure-8 coil",
         "config": config_dict(mesh, {"precision": args.precision, "recovery": args.recovery,
@@ -350,8 +360,10 @@ def run_ours(args) -> dict:
         "vs_plain_fp64": {"value": round(plain_value, 3), "unit": "placements/s",
                           "iterations": plain_it, "ratio": round((plain_ms / n_cmp) / (total_ms / args.steps), 3),
                           "what": "plain FP64 zero-guess PCG, same block, same GPU"},
-        "ablation": {"mixed_zero_guess": {"value": round(cold_value, 3),
-                                          "iterations": cold_it},
+        "ablation": {"zero_guess": {"value": round(cold_value, 3), "iterations": cold_it,
+                                    "what": f"{args.precision}, no learned guess"},
+                     "mixed_refinement_zero_guess": {"value": round(mixed_value, 3), "iterations": mixed_it,
+                                                     "what": "FP32 PCG + FP32 V-cycle inside FP64 refinement"},
                      "this_run": {"warm_start": args.warm_start, "iterations": col_iters,
                                   "warm_used": warm_used, "init_relres": [round(v, 5) for v in warm_rel0]}},
         "warm_start": warm_stats,
@@ -435,7 +447,7 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["mixed", "plain"], default="mixed")
+    ap.add_argument("--precision", choices=["split", "mixed", "plain"], default="split")
     ap.add_argument("--recovery", choices=["harmonic", "spr_tissue", "spr_global", "raw"], default="harmonic")
     ap.add_argument("--warm-start", choices=["on", "off"], default="on")
     ap.add_argument("--train", type=int, default=4096, help="training solves of the warm-start network")

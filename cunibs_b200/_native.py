@@ -15,7 +15,7 @@ _LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libcunibs_b200.so"
 _lib: C.CDLL | None = None
 
 OK, EINVAL, ENOMEM, ECUDA, ENOCONV, ETIMEOUT, EINTERNAL = range(7)
-PREC_DEFAULT, PREC_PLAIN_FP64, PREC_MIXED = 0, 1, 2
+PREC_DEFAULT, PREC_PLAIN_FP64, PREC_MIXED, PREC_SPLIT = 0, 1, 2, 3
 RECOVERY_CODES = {"raw": 0, "spr_global": 1, "spr_tissue": 2, "harmonic": 3}
 SUMMARY_LEN = 16
 

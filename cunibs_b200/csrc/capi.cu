@@ -36,7 +36,8 @@ void require(bool ok, const char* msg) {
 int to_internal_precision(int p) {
     if (p == CUNIBS_PREC_PLAIN_FP64) return kPlainFp64;
     if (p == CUNIBS_PREC_MIXED) return kMixed;
-    fail(kEInval, "precision must be CUNIBS_PREC_PLAIN_FP64 or CUNIBS_PREC_MIXED");
+    if (p == CUNIBS_PREC_SPLIT) return kFp64CgFp32Mg;
+    fail(kEInval, "precision must be CUNIBS_PREC_PLAIN_FP64, CUNIBS_PREC_MIXED or CUNIBS_PREC_SPLIT");
 }
 
 int pad_width(int k) {
@@ -278,7 +279,7 @@ int cunibs_params_default(cunibs_params* out) {
         out->cheby_lower_ratio = p.cheby_lower_ratio;
         out->tolerance = p.tolerance;
         out->max_iters = p.max_iters;
-        out->precision = CUNIBS_PREC_MIXED;
+        out->precision = CUNIBS_PREC_SPLIT;
         out->inner_reduction = p.inner_reduction;
         out->inner_max_iters = p.inner_max_iters;
         out->iters_per_sync = p.iters_per_sync;
@@ -305,7 +306,7 @@ int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_no
         c->prm.cheby_lower_ratio = p.cheby_lower_ratio;
         c->prm.tolerance = p.tolerance;
         c->prm.max_iters = p.max_iters;
-        c->prm.precision = to_internal_precision(p.precision == CUNIBS_PREC_DEFAULT ? CUNIBS_PREC_MIXED : p.precision);
+        c->prm.precision = to_internal_precision(p.precision == CUNIBS_PREC_DEFAULT ? CUNIBS_PREC_SPLIT : p.precision);
         c->prm.inner_reduction = p.inner_reduction;
         c->prm.inner_max_iters = p.inner_max_iters;
         c->prm.iters_per_sync = p.iters_per_sync > 0 ? p.iters_per_sync : 4;

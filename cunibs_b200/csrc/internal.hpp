@@ -29,7 +29,7 @@ struct Params {
     double cheby_lower_ratio = 12.0;
     double tolerance = 1e-6;
     int max_iters = 2000;
-    int precision = kMixed;
+    int precision = kFp64CgFp32Mg;
     double inner_reduction = 1e-4;  // deepest residual reduction asked of one inner FP32 solve
     int inner_max_iters = 60;
     int iters_per_sync = 4;         // PCG iterations launched between host convergence checks

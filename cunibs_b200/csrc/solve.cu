@@ -24,6 +24,7 @@
 #include <map>
 #include <memory>
 #include <tuple>
+#include <type_traits>
 
 #include "internal.hpp"
 
@@ -392,13 +393,16 @@ __global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
 // (tol_c = tol_vec[c] when given, else tol); the iteration it froze at and its relative residual
 // are recorded on the device. With z0 given, also writes the V-cycle's first smoothing step
 // z0 = alpha0*dinv*r from the new residual.
-template <typename T, int K>
+// With a V-cycle in a narrower type TZ than the Krylov vectors (FP64 PCG over an FP32 V-cycle),
+// r_lo receives the residual rounded to TZ, the V-cycle's input, and z0 is formed from it.
+template <typename T, typename TZ, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
     int n, const double* __restrict__ alpha, const T* __restrict__ p, const T* __restrict__ ap, T* __restrict__ x,
     T* __restrict__ r, double* partials, unsigned* counter, const double* __restrict__ ref, double tol,
     const double* __restrict__ tol_vec, int* __restrict__ frozen, int* __restrict__ iter_counter,
-    int* __restrict__ conv_iter, double* __restrict__ rel_out, int record, const T* __restrict__ dinv, T alpha0,
-    T* __restrict__ z0, cudaGraphConditionalHandle loop, int use_loop, const int* __restrict__ cap) {
+    int* __restrict__ conv_iter, double* __restrict__ rel_out, int record, const TZ* __restrict__ dinv, TZ alpha0,
+    TZ* __restrict__ z0, TZ* __restrict__ r_lo, cudaGraphConditionalHandle loop, int use_loop,
+    const int* __restrict__ cap) {
     const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
     const int tiles = n_tiles_dev(n);
@@ -411,7 +415,9 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
             x[q] += a * p[q];
             const T rn = r[q] - a * ap[q];
             r[q] = rn;
-            if (z0 != nullptr) z0[q] = alpha0 * dinv[row] * rn;
+            const TZ rl = static_cast<TZ>(rn);
+            if (r_lo != nullptr) r_lo[q] = rl;
+            if (z0 != nullptr) z0[q] = alpha0 * dinv[row] * rl;
             v += static_cast<double>(rn) * static_cast<double>(rn);
         }
     }
@@ -520,15 +526,22 @@ __global__ void __launch_bounds__(tile_threads<K>()) cheby_dot_kernel(
 
 // p = z + beta p. A column frozen before this iteration keeps its direction, so a column that met
 // an inner target resumes the same Krylov sequence after the outer step replaces its residual.
-template <typename T, int K>
+template <typename T, typename TZ, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) update_p_kernel(int n, const double* __restrict__ beta,
-                                                                     const T* __restrict__ z, T* __restrict__ p,
+                                                                     const TZ* __restrict__ z, T* __restrict__ p,
                                                                      const int* __restrict__ frozen) {
     const int row = blockIdx.x * kTileRows + threadIdx.x / K;
     const int c = threadIdx.x % K;
     if (row >= n || frozen[c] == 1) return;
     const long q = static_cast<long>(row) * K + c;
-    p[q] = z[q] + static_cast<T>(beta[c]) * p[q];
+    p[q] = static_cast<T>(z[q]) + static_cast<T>(beta[c]) * p[q];
+}
+
+// r_lo = r rounded to the V-cycle's type (the first V-cycle input of FP64 PCG over an FP32 V-cycle).
+template <typename T, typename TZ>
+__global__ void narrow_kernel(std::int64_t count, const T* __restrict__ r, TZ* __restrict__ r_lo) {
+    const std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q < count) r_lo[q] = static_cast<TZ>(r[q]);
 }
 
 // Mixed refinement outer step: R = B - A X in FP64; r32 = (float)R; per column the true relative
@@ -740,8 +753,9 @@ class Solver {
         VWork<T>& w = vw<T>();
         return (h->cheby.degree % 2) ? w.x[0].get() : w.r[0].get();
     }
-    template <typename T, int K>
-    void pcg_tail(T* r, T* z, T* p, bool jz_done);
+    // z = M r_v (V-cycle in TZ), beta, p = z + beta p (Krylov vectors in T).
+    template <typename T, typename TZ, int K>
+    void pcg_tail(TZ* r_v, TZ* z, T* p, bool jz_done);
     // Sub-lanes per row on the finest operator (the PCG's own matrix), capped where the reducing
     // kernels' 64/TPR-row tiles need at least four rows.
     int tpr0() const {
@@ -752,10 +766,12 @@ class Solver {
         h_flags[0] = v;
         CUNIBS_CHECK(cudaMemcpyAsync(cap.get(), h_flags, sizeof(int), cudaMemcpyHostToDevice, stream));
     }
-    template <typename T, int K>
-    void pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
-                       const double* tol_vec, const double* ref, int record, cudaGraphConditionalHandle loop = 0,
-                       int use_loop = 0);
+    // One PCG iteration with Krylov vectors in T and the V-cycle in TZ (r_v is r in TZ; the same
+    // buffer as r when the types agree).
+    template <typename T, typename TZ, int K>
+    void pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, TZ* r_v, TZ* z,
+                       double tol, const double* tol_vec, const double* ref, int record,
+                       cudaGraphConditionalHandle loop = 0, int use_loop = 0);
     DevArray<int> cap;
     // Device-side loop: body(handle) is captured once into the body of a conditional WHILE node and
     // replayed until a kernel in it clears the condition. Returns false when the driver cannot
@@ -815,7 +831,7 @@ class Solver {
         while_unsupported = true;
         return false;
     }
-    template <int K>
+    template <int K, typename TZ>
     void solve_plain(int k, const Params& prm, SolveStats& st, bool warm);
     template <int K>
     void solve_mixed(int k, const Params& prm, SolveStats& st, bool warm);
@@ -1023,23 +1039,23 @@ __global__ void fill_kernel(double* v, int n, double x) {
     if (i < n) v[i] = x;
 }
 
-template <typename T, int K>
-void Solver::pcg_tail(T* r, T* z, T* p, bool jz_done) {
+template <typename T, typename TZ, int K>
+void Solver::pcg_tail(TZ* r_v, TZ* z, T* p, bool jz_done) {
     constexpr int TT = tile_threads<K>();
-    const bool fused = vcycle<T, K>(r, z, jz_done, true);
+    const bool fused = vcycle<TZ, K>(r_v, z, jz_done, true);
     if (!fused) {
-        dot_beta_kernel<T, K><<<reduce_grid(n), TT, 0, stream>>>(n, r, z, partials.get(), counter.get(), rz.get(),
-                                                                frozen.get(), beta.get());
+        dot_beta_kernel<TZ, K><<<reduce_grid(n), TT, 0, stream>>>(n, r_v, z, partials.get(), counter.get(), rz.get(),
+                                                                 frozen.get(), beta.get());
         count_launch();
     }
-    update_p_kernel<T, K><<<n_tiles(n), TT, 0, stream>>>(n, beta.get(), z, p, frozen.get());
+    update_p_kernel<T, TZ, K><<<n_tiles(n), TT, 0, stream>>>(n, beta.get(), z, p, frozen.get());
     count_launch();
 }
 
-template <typename T, int K>
-void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, T* z, double tol,
-                           const double* tol_vec, const double* ref, int record, cudaGraphConditionalHandle loop,
-                           int use_loop) {
+template <typename T, typename TZ, int K>
+void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T* r, T* p, T* ap, TZ* r_v, TZ* z,
+                           double tol, const double* tol_vec, const double* ref, int record,
+                           cudaGraphConditionalHandle loop, int use_loop) {
     constexpr int TT = tile_threads<K>();
     const unsigned g = reduce_grid(n);
     dispatch_tpr<K>(tpr0(), [&](auto tc) {
@@ -1049,16 +1065,28 @@ void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T
     });
     count_launch();
     const bool has_levels = !h->levels.empty();
-    update_xr_kernel<T, K><<<g, TT, 0, stream>>>(
+    constexpr bool narrow = !std::is_same<T, TZ>::value;
+    update_xr_kernel<T, TZ, K><<<g, TT, 0, stream>>>(
         n, alpha.get(), p, ap, x, r, partials.get(), counter.get(), ref, tol, tol_vec, frozen.get(), iter_counter.get(),
-        conv_iter.get(), rel.get(), record, has_levels ? ldinv<T>(0) : nullptr, static_cast<T>(h->cheby.alpha0),
-        has_levels ? first0<T>() : nullptr, loop, use_loop, cap.get());
+        conv_iter.get(), rel.get(), record, has_levels ? ldinv<TZ>(0) : nullptr, static_cast<TZ>(h->cheby.alpha0),
+        has_levels ? first0<TZ>() : nullptr, narrow ? r_v : nullptr, loop, use_loop, cap.get());
     count_launch();
-    pcg_tail<T, K>(r, z, p, has_levels);
+    pcg_tail<T, TZ, K>(r_v, z, p, has_levels);
 }
 
-template <int K>
+template <int K, typename TZ>
 void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
+    constexpr bool narrow = !std::is_same<TZ, double>::value;
+    TZ* rv = nullptr;
+    TZ* zv = nullptr;
+    if constexpr (narrow) {
+        rv = r32.get();
+        zv = z32.get();
+    } else {
+        rv = R.get();
+        zv = Z.get();
+    }
+    const int key = narrow ? 4 : 2;
     constexpr int TT = tile_threads<K>();
     const unsigned g = n_tiles(n);
     cudaStream_t s = stream;
@@ -1083,13 +1111,18 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     rel.zero(s);
     fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
     count_launch();
-    pcg_tail<double, K>(R.get(), Z.get(), P.get(), false);
+    if constexpr (narrow) {
+        const std::int64_t count = static_cast<std::int64_t>(n) * K;
+        narrow_kernel<double, TZ><<<grid_for(count), kBlock, 0, s>>>(count, R.get(), rv);
+        count_launch();
+    }
+    pcg_tail<double, TZ, K>(rv, zv, P.get(), false);
     int it = 0;
     set_cap(prm.max_iters);
     long long nodes = 0;
-    const bool device_loop = run_while({2, K, 0}, [&](cudaGraphConditionalHandle hnd) {
-        pcg_iteration<double, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(), Z.get(),
-                                 prm.tolerance, nullptr, ref_sq.get(), 1, hnd, 1);
+    const bool device_loop = run_while({key, K, 0}, [&](cudaGraphConditionalHandle hnd) {
+        pcg_iteration<double, TZ, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(), rv,
+                                     zv, prm.tolerance, nullptr, ref_sq.get(), 1, hnd, 1);
     }, &nodes);
     if (device_loop) {
         CUNIBS_CHECK(cudaMemcpyAsync(h_flags, iter_counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1100,9 +1133,9 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     while (!device_loop && it < prm.max_iters) {
         const int m = std::min(prm.iters_per_sync, prm.max_iters - it);
         for (int j = 0; j < m; ++j) {
-            run_graph({0, K, 0}, [&] {
-                pcg_iteration<double, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(),
-                                         Z.get(), prm.tolerance, nullptr, ref_sq.get(), 1);
+            run_graph({key + 10, K, 0}, [&] {
+                pcg_iteration<double, TZ, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(),
+                                             AP.get(), rv, zv, prm.tolerance, nullptr, ref_sq.get(), 1);
             });
         }
         it += m;
@@ -1160,14 +1193,14 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st, bool warm) {
         p32.zero(s);
         fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
         count_launch();
-        pcg_tail<float, K>(r32.get(), z32.get(), p32.get(), false);
+        pcg_tail<float, float, K>(r32.get(), z32.get(), p32.get(), false);
         int it = 0;
         const int cap_n = std::min(prm.inner_max_iters, prm.max_iters - total_inner);
         set_cap(total_inner + cap_n);
         long long nodes = 0;
         const bool device_loop = run_while({3, K, 0}, [&](cudaGraphConditionalHandle hnd) {
-            pcg_iteration<float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
-                                    z32.get(), 0.0, eta.get(), rr0.get(), 0, hnd, 1);
+            pcg_iteration<float, float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
+                                           r32.get(), z32.get(), 0.0, eta.get(), rr0.get(), 0, hnd, 1);
         }, &nodes);
         if (device_loop) {
             CUNIBS_CHECK(cudaMemcpyAsync(h_flags, iter_counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1179,8 +1212,8 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st, bool warm) {
             const int m = std::min(prm.iters_per_sync, cap_n - it);
             for (int j = 0; j < m; ++j) {
                 run_graph({1, K, 0}, [&] {
-                    pcg_iteration<float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(), ap32.get(),
-                                            z32.get(), 0.0, eta.get(), rr0.get(), 0);
+                    pcg_iteration<float, float, K>(A.ptr.get(), A.col.get(), A32, d32.get(), r32.get(), p32.get(),
+                                                   ap32.get(), r32.get(), z32.get(), 0.0, eta.get(), rr0.get(), 0);
                 });
             }
             it += m;
@@ -1240,7 +1273,8 @@ void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, con
         if (X0) CUNIBS_CHECK(cudaMemcpyAsync(sv.X.get(), X0, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
         else sv.X.zero(sv.stream);
         if (prm.precision == kMixed) sv.solve_mixed<KK>(k, prm, st, X0 != nullptr);
-        else sv.solve_plain<KK>(k, prm, st, X0 != nullptr);
+        else if (prm.precision == kFp64CgFp32Mg) sv.solve_plain<KK, float>(k, prm, st, X0 != nullptr);
+        else sv.solve_plain<KK, double>(k, prm, st, X0 != nullptr);
         if (X0) {
             double h_init[16];
             CUNIBS_CHECK(cudaMemcpyAsync(h_init, sv.init_rel.get(), sizeof(double) * KK, cudaMemcpyDeviceToHost,

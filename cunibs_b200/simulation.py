@@ -61,7 +61,8 @@ from .fem import (  # noqa: E402
 from .mesh import HeadMesh, load_mesh  # noqa: E402
 
 _FORMAT_VERSION = 1
-Precision = Literal["mixed", "plain"]
+Precision = Literal["mixed", "split", "plain"]
+_PRECISION_CODES = {"mixed": _native.PREC_MIXED, "split": _native.PREC_SPLIT, "plain": _native.PREC_PLAIN_FP64}
 
 
 @dataclass(frozen=True)
@@ -86,14 +87,14 @@ class Subject:
     """A head mesh and its reusable GPU solver state (reference simulation.py:169-546).
 
     ``tolerance`` is the PCG stopping criterion ||r||/||b|| (the reference's DEFAULT_TOLERANCE is
-    1e-6). ``precision`` selects "mixed" (FP32 PCG and V-cycle inside FP64 refinement, the default)
-    or "plain" (FP64 throughout).
+    1e-6). ``precision`` selects "split" (FP64 PCG over an FP32 V-cycle, the default), "mixed"
+    (FP32 PCG and V-cycle inside FP64 iterative refinement) or "plain" (FP64 throughout).
     """
 
     def __init__(self, mesh: HeadMesh, *, tolerance: float = DEFAULT_TOLERANCE, max_iters: int = DEFAULT_MAX_ITERS,
-                 precision: Precision = "mixed", device: int = 0) -> None:
-        if precision not in ("mixed", "plain"):
-            raise ValueError("precision must be 'mixed' or 'plain'")
+                 precision: Precision = "split", device: int = 0) -> None:
+        if precision not in _PRECISION_CODES:
+            raise ValueError("precision must be 'mixed', 'split' or 'plain'")
         self._mesh = mesh
         self._ctx: _native.Context | None = None
         self._ordered: HeadMesh | None = None
@@ -134,7 +135,7 @@ class Subject:
                 p = _native.default_params()
                 p.tolerance = self._tolerance
                 p.max_iters = self._max_iters
-                p.precision = _native.PREC_MIXED if self._precision == "mixed" else _native.PREC_PLAIN_FP64
+                p.precision = _PRECISION_CODES[self._precision]
                 p.device = self._device
                 m = self._mesh
                 self._ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris, p)

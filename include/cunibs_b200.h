@@ -32,6 +32,7 @@ extern "C" {
 #define CUNIBS_PREC_DEFAULT 0    /* per-call option: use the context's precision */
 #define CUNIBS_PREC_PLAIN_FP64 1 /* FP64 PCG over an FP64 V-cycle */
 #define CUNIBS_PREC_MIXED 2      /* FP32 PCG + FP32 V-cycle inside FP64 iterative refinement */
+#define CUNIBS_PREC_SPLIT 3      /* FP64 PCG over an FP32 V-cycle (the default) */
 
 /* Field recovery: how the reported E is derived from the solve (fem/recovery.py:74-113).
  * RAW is the per-tetrahedron field; SPR_GLOBAL a linear patch fit per node; SPR_TISSUE the same per

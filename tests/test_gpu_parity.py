@@ -125,7 +125,7 @@ def test_dadt_matches_fp64_oracle(patch_pair, d70_coil, patch_placement, general
         assert np.abs(got[i] - want).max() <= 1e-5 * np.abs(want).max()
 
 
-@pytest.mark.parametrize("precision", [_native.PREC_PLAIN_FP64, _native.PREC_MIXED])
+@pytest.mark.parametrize("precision", [_native.PREC_PLAIN_FP64, _native.PREC_MIXED, _native.PREC_SPLIT])
 def test_linear_solve_matches_oracle_direct(sphere_pair, precision):
     ctx, orc = sphere_pair
     n = ctx.n_nodes - 1
@@ -157,7 +157,7 @@ def _compare_block(subject, orc, coil, sites, tol=1e-10, recovery="raw"):
     return res, ref
 
 
-@pytest.mark.parametrize("precision", ["mixed", "plain"])
+@pytest.mark.parametrize("precision", ["mixed", "split", "plain"])
 def test_patch_end_to_end_vs_oracle_and_reference_pin(patch_mesh, d70_coil, patch_placement, pins, precision):
     subj = Subject(patch_mesh, tolerance=1e-10, precision=precision)
     orc = Oracle(patch_mesh)
@@ -182,10 +182,11 @@ def test_sphere_block_vs_oracle(sphere_mesh):
     subj.free()
 
 
-@pytest.mark.parametrize("recovery", ["raw", "harmonic", "spr_tissue"])
-def test_block_width_and_batch_invariance_bitwise(sphere_mesh, recovery):
+@pytest.mark.parametrize("recovery,precision", [("raw", "mixed"), ("harmonic", "mixed"), ("spr_tissue", "mixed"),
+                                                ("harmonic", "split")])
+def test_block_width_and_batch_invariance_bitwise(sphere_mesh, recovery, precision):
     """A placement's result is bitwise independent of block_k and of its block-mates."""
-    subj = Subject(sphere_mesh, tolerance=1e-8)
+    subj = Subject(sphere_mesh, tolerance=1e-8, precision=precision)
     coil = figure8_coil(64)
     top = np.array([0.0, 0.0, 90.0])
     sites = [Placement(top + [dx, 0, 0], top + [dx, 50, 0]) for dx in (0.0, 10.0, -12.0)]
