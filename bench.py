@@ -10,9 +10,11 @@ and gray-matter summary.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision split|mixed|plain]
 
-Prints one JSON line (rank 0). ``value`` is device-timed with CUDA events on the library's stream,
-inputs resident in HBM, L2 flushed between steps; ``e2e`` goes through the host C ABI call
-(cunibs_solve_block) with host buffers, timed by the wall clock around the synchronous call.
+Prints one JSON line (rank 0). ``value`` is device-timed with CUDA events on the library's stream
+around all timed steps, inputs resident in HBM, L2 flushed before every step's solve, blocks
+submitted two deep as Subject.iter_simulate runs them (a block's placement, dA/dt and right-hand side
+beside the previous block's solve); ``e2e`` goes through the host C ABI (cunibs_submit_block /
+cunibs_finish_block) with host buffers, timed by the wall clock.
 """
 
 from __future__ import annotations
@@ -235,9 +237,44 @@ def run_ours(args) -> dict:
                                       d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, outs, recovery=args.recovery,
                                       precision=precision, warm_start=warm)
 
+    def submit(precision=_native.PREC_DEFAULT, warm=args.warm_start == "on"):
+        return ctx.submit_block_device(d_pos.data_ptr(), d_mom.data_ptr(), coil.n_dipoles, d_c.data_ptr(),
+                                       d_h.data_ptr(), d_d.data_ptr(), K_BLOCK, 1e6, recovery=args.recovery,
+                                       precision=precision, warm_start=warm)
+
+    def finish(ticket):
+        # L2 flushed on the library stream before every block's solve.
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        return ctx.finish_block_device(ticket, outs)
+
+    def pipelined(n, **kw):
+        """Device time of n steps submitted two deep, as Subject.iter_simulate runs its blocks: each
+        block's placement, dA/dt and right-hand side run beside the previous block's solve. CUDA
+        events on the library stream bracket all n steps (pipeline fill and drain included)."""
+        its, outer = [], []
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        tickets = [submit(**kw)]
+        for _ in range(n - 1):
+            tickets.append(submit(**kw))
+            it, o = finish(tickets.pop(0))
+            its.append(it)
+            outer.append(o)
+        it, o = finish(tickets.pop(0))
+        its.append(it)
+        outer.append(o)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), its, outer
+
     def timed(n, **kw):
-        """Device time of n steps (CUDA events on the library stream, L2 flushed before each)."""
-        ms, its = [], []
+        """Device time of n steps one at a time (CUDA events on the library stream around each,
+        L2 flushed before each), with the stage breakdown."""
+        ms, its, stages = [], [], np.zeros(5)
         for _ in range(n):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -250,69 +287,62 @@ def run_ours(args) -> dict:
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
             its.append(float(d_it.float().mean().item()))
-        return float(sum(ms)), float(np.mean(its))
+            stages += ctx.stage_times()
+        return float(sum(ms)), float(np.mean(its)), stages / n
 
-    for _ in range(args.warmup):
-        step()
+    pipelined(max(3, args.warmup))
     torch.cuda.synchronize()
     launches0 = _native.kernel_launches()
-    stage_sum = np.zeros(5)
-    iters = []
-    outers = []
-    step_ms = []
     with ClockSampler(local) as clocks:
         if dist is not None:
             dist.barrier()
         torch.cuda.synchronize()
         # An NVTX range around the timed steps lets a profiler capture exactly those launches.
         torch.cuda.nvtx.range_push("timed_steps")
-        for _ in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.zero_()
-                ev0 = torch.cuda.Event(enable_timing=True)
-                ev1 = torch.cuda.Event(enable_timing=True)
-                ev0.record(stream)
-            it, outer = step()
-            with torch.cuda.stream(stream):
-                ev1.record(stream)
-            ev1.synchronize()
-            step_ms.append(ev0.elapsed_time(ev1))
-            stage_sum += ctx.stage_times()
-            iters.append(it)
-            outers.append(outer)
+        total_ms, iters, outers = pipelined(args.steps)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
         if dist is not None:
             dist.barrier()
     launches = _native.kernel_launches() - launches0
-    total_ms = float(sum(step_ms))
     warm_used = d_used.cpu().numpy().tolist()
     warm_rel0 = d_rel0.cpu().numpy().tolist()
     col_iters = float(d_it.float().mean().item())
-    # The same block on the same GPU without the learned guess (this precision), with FP64
-    # iterative refinement around FP32 PCG, and with plain FP64 PCG.
-    n_cmp = max(1, min(args.steps, 5))
+    # The same blocks on the same GPU: one at a time (with the stage breakdown), without the
+    # learned guess (this precision), with FP64 iterative refinement around FP32 PCG, and with
+    # plain FP64 PCG; the comparison arms pipelined like the headline.
+    n_cmp = max(3, min(args.steps, 8))
     for _ in range(2):
-        step(warm=False)
-        step(precision=_native.PREC_MIXED, warm=False)
-        step(precision=_native.PREC_PLAIN_FP64, warm=False)
-    cold_ms, cold_it = timed(n_cmp, warm=False)
-    mixed_ms, mixed_it = timed(n_cmp, precision=_native.PREC_MIXED, warm=False)
-    plain_ms, plain_it = timed(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
+        step()
+    seq_ms, _, stage_avg = timed(n_cmp)
+    pipelined(2, warm=False)
+    cold_ms, cold_its, _ = pipelined(n_cmp, warm=False)
+    cold_it = float(d_it.float().mean().item())
+    pipelined(2, precision=_native.PREC_MIXED, warm=False)
+    mixed_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_MIXED, warm=False)
+    mixed_it = float(d_it.float().mean().item())
+    pipelined(2, precision=_native.PREC_PLAIN_FP64, warm=False)
+    plain_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
+    plain_it = float(d_it.float().mean().item())
     total_ms, value = job_throughput(total_ms, args.steps, world, dist, dev)
+    seq_ms, seq_value = job_throughput(seq_ms, n_cmp, world, dist, dev)
     cold_ms, cold_value = job_throughput(cold_ms, n_cmp, world, dist, dev)
     mixed_ms, mixed_value = job_throughput(mixed_ms, n_cmp, world, dist, dev)
     plain_ms, plain_value = job_throughput(plain_ms, n_cmp, world, dist, dev)
 
-    # End to end through the host C ABI (host buffers in and out).
-    e2e_ms = []
-    for _ in range(max(1, min(args.steps, 5))):
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        res = ctx.solve_block(coil, centers, handles, dists, 1e6, recovery=args.recovery,
-                              warm_start=args.warm_start == "on")
-        e2e_ms.append((time.perf_counter() - t1) * 1e3)
-    e2e_value = world * K_BLOCK / (statistics.median(e2e_ms) / 1e3)
+    # End to end through the host C ABI (host buffers in and out), blocks submitted two deep
+    # (cunibs_submit_block / cunibs_finish_block), timed by the wall clock around all of them.
+    n_e2e = max(3, min(args.steps, 8))
+    kw = dict(recovery=args.recovery, warm_start=args.warm_start == "on")
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    tickets = [ctx.submit_block(coil, centers, handles, dists, 1e6, **kw)]
+    for _ in range(n_e2e - 1):
+        tickets.append(ctx.submit_block(coil, centers, handles, dists, 1e6, **kw))
+        res = ctx.finish_block(tickets.pop(0))
+    res = ctx.finish_block(tickets.pop(0))
+    e2e_s = time.perf_counter() - t1
+    e2e_value = world * K_BLOCK * n_e2e / e2e_s
     h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
     d2h = res["transform"].nbytes + res["summary"].nbytes + res["iterations"].nbytes + res["relative_residual"].nbytes
 
@@ -322,7 +352,7 @@ def run_ours(args) -> dict:
     per_it, per_outer = solve_bytes_per_iteration(ctx, K_BLOCK, args.precision)
     mean_iters = float(np.mean(iters))
     mean_outer = float(np.mean(outers))
-    solve_ms = stage_sum[3] / args.steps
+    solve_ms = float(stage_avg[3])
     solve_bytes = per_it * mean_iters + per_outer * mean_outer
     achieved = solve_bytes / (solve_ms / 1e3) / 1e9
     # Measured DRAM bytes per PCG iteration (ncu over one timed block, warm L2), beside the
@@ -332,7 +362,7 @@ def run_ours(args) -> dict:
     if tp.exists():
         traffic = json.loads(tp.read_text()).get("dram_bytes_per_iteration")
     n_nodes = mesh.n_nodes
-    dadt_ms = stage_sum[1] / args.steps
+    dadt_ms = float(stage_avg[1])
     pair_evals = n_nodes * coil.n_dipoles * K_BLOCK
     line = {
         "metric": METRIC,
@@ -352,18 +382,22 @@ def run_ours(args) -> dict:
         "config": config_dict(mesh, {"precision": args.precision, "recovery": args.recovery,
                                      "warm_start": (f"MLP 6-4x512-{args.rank}, {args.train} plain-method training solves"
                                                     if args.warm_start == "on" else "off"),
-                                     "l2": "flushed (256 MB write) between steps",
+                                     "l2": "flushed (256 MB write) before every step's solve",
+                                     "pipeline": "blocks submitted two deep: placement/dA-dt/RHS of step i+1 "
+                                                 "beside the solve of step i",
                                      "parallelism": f"replicas x{world}"}),
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "vs_plain_fp64": {"value": round(plain_value, 3), "unit": "placements/s",
                           "iterations": plain_it, "ratio": round((plain_ms / n_cmp) / (total_ms / args.steps), 3),
-                          "what": "plain FP64 zero-guess PCG, same block, same GPU"},
+                          "what": "plain FP64 zero-guess PCG, same blocks, same pipeline, same GPU"},
         "ablation": {"zero_guess": {"value": round(cold_value, 3), "iterations": cold_it,
                                     "what": f"{args.precision}, no learned guess"},
                      "mixed_refinement_zero_guess": {"value": round(mixed_value, 3), "iterations": mixed_it,
                                                      "what": "FP32 PCG + FP32 V-cycle inside FP64 refinement"},
+                     "one_block_at_a_time": {"value": round(seq_value, 3),
+                                             "what": "this configuration without the two-deep pipeline"},
                      "this_run": {"warm_start": args.warm_start, "iterations": col_iters,
                                   "warm_used": warm_used, "init_relres": [round(v, 5) for v in warm_rel0]}},
         "warm_start": warm_stats,
@@ -373,8 +407,7 @@ def run_ours(args) -> dict:
                      "traffic_unit": "DRAM bytes per PCG iteration (ncu, warm L2)",
                      "bytes_per_iteration": per_it, "iterations": mean_iters, "outer_steps": mean_outer,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
-        "stages_ms": {k: round(v / args.steps, 4) for k, v in
-                      zip(["place", "dadt", "rhs", "solve", "post"], stage_sum)},
+        "stages_ms": {k: round(float(v), 4) for k, v in zip(["place", "dadt", "rhs", "solve", "post"], stage_avg)},
         "dadt": {"pair_evals_per_step": int(pair_evals), "ms": round(dadt_ms, 4),
                  "gpair_per_s": round(pair_evals / (dadt_ms / 1e3) / 1e9, 2)},
         "setup_s": round(setup_s, 3),

@@ -131,6 +131,15 @@ def load() -> C.CDLL:
         "cunibs_context_levels": ([_vp, ip, C.c_int], C.c_int),
         "cunibs_solve_block": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), C.POINTER(BlockOut)], C.c_int),
         "cunibs_solve_block_device": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), C.POINTER(BlockOut)], C.c_int),
+        "cunibs_submit_block": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts),
+                                 C.POINTER(C.c_longlong)], C.c_int),
+        "cunibs_finish_block": ([_vp, C.c_longlong, C.POINTER(BlockOut)], C.c_int),
+        "cunibs_submit_block_device": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double,
+                                        C.POINTER(SolveOpts), C.POINTER(C.c_longlong)], C.c_int),
+        "cunibs_finish_block_device": ([_vp, C.c_longlong, C.POINTER(BlockOut)], C.c_int),
+        "cunibs_cancel_block": ([_vp, C.c_longlong], C.c_int),
+        "cunibs_context_pending": ([_vp, C.POINTER(C.c_int)], C.c_int),
+        "cunibs_context_set_overlap": ([_vp, C.c_int], C.c_int),
         "cunibs_context_set_conductivity": ([_vp, dp], C.c_int),
         "cunibs_context_array": ([_vp, C.c_char_p, C.c_int, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
         "cunibs_context_place": ([_vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
@@ -215,6 +224,7 @@ class Context:
             _ip(skin) if skin.shape[0] else None, skin.shape[0], C.byref(prm), C.byref(h)))
         self._h = h
         self._lib = lib
+        self._submitted: dict[int, tuple] = {}
         self.params = prm
         info = Info()
         check(lib.cunibs_context_info(h, C.byref(info)))
@@ -380,20 +390,49 @@ class Context:
                                                   float(didt), C.byref(opts), C.byref(out)))
         return out.total_iterations, out.outer_steps
 
+    def submit_block_device(self, pos, mom, n_dip, centers, handles, dists, k, didt, *, block_width=0,
+                            precision=PREC_DEFAULT, tolerance=0.0, max_iters=0, recovery="raw",
+                            warm_start=False) -> int:
+        """cunibs_submit_block_device: prepare a block on raw device pointers (ints) without waiting;
+        returns its ticket."""
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
+                         int(bool(warm_start)))
+        t = C.c_longlong(0)
+        check(self._lib.cunibs_submit_block_device(self.handle, pos, mom, int(n_dip), centers, handles, dists, int(k),
+                                                   float(didt), C.byref(opts), C.byref(t)))
+        return t.value
+
+    def finish_block_device(self, ticket: int, out_ptrs) -> tuple[int, int]:
+        """cunibs_finish_block_device: solve a submitted block into out_ptrs (device pointers)."""
+        out = BlockOut(out_ptrs.get("transforms"), out_ptrs.get("summary"), out_ptrs.get("iterations"),
+                       out_ptrs.get("relres"), out_ptrs.get("magnE"), out_ptrs.get("E"), out_ptrs.get("v"), 0, 0,
+                       out_ptrs.get("E_slots"), out_ptrs.get("warm_used"), out_ptrs.get("init_relres"))
+        check(self._lib.cunibs_finish_block_device(self.handle, int(ticket), C.byref(out)))
+        return out.total_iterations, out.outer_steps
+
+    @property
+    def pending(self) -> int:
+        n = C.c_int(0)
+        check(self._lib.cunibs_context_pending(self.handle, C.byref(n)))
+        return n.value
+
+    def set_overlap(self, blocks_per_sm: int) -> None:
+        check(self._lib.cunibs_context_set_overlap(self.handle, int(blocks_per_sm)))
+
     def set_conductivity(self, sigma_by_tag) -> None:
         s = np.ascontiguousarray(sigma_by_tag, np.float64).reshape(11)
         check(self._lib.cunibs_context_set_conductivity(self.handle, s.ctypes.data_as(C.POINTER(C.c_double))))
 
-    def solve_block(self, coil, centers, handles, dists, didt, *, block_width=0, precision=PREC_DEFAULT,
-                    tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False,
-                    recovery="raw", nodal=False, warm_start=False) -> dict:
-        """One block of k placements through cunibs_solve_block (host buffers in and out)."""
+    @staticmethod
+    def _block_inputs(coil, centers, handles, dists):
         centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
-        k = centers.shape[0]
         handles = np.ascontiguousarray(handles, np.float64).reshape(-1, 3)
         dists = np.ascontiguousarray(dists, np.float64).reshape(-1)
         pos = np.ascontiguousarray(coil.positions_m, np.float64)
         mom = np.ascontiguousarray(coil.moments, np.float64)
+        return pos, mom, centers, handles, dists
+
+    def _block_outputs(self, k, magnitude, vectors, potential, recovery, nodal):
         res = {
             "transform": np.empty((k, 4, 4)),
             "summary": np.empty((k, SUMMARY_LEN)),
@@ -413,10 +452,50 @@ class Context:
         out = BlockOut(_p(res["transform"]), _p(res["summary"]), _p(res["iterations"]), _p(res["relative_residual"]),
                        _p(res["magnE"]), _p(res["E"]), _p(res["v"]), 0, 0, _p(res["E_slots"]), _p(res["warm_used"]),
                        _p(res["init_relres"]))
+        return res, out
+
+    def solve_block(self, coil, centers, handles, dists, didt, *, block_width=0, precision=PREC_DEFAULT,
+                    tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False,
+                    recovery="raw", nodal=False, warm_start=False) -> dict:
+        """One block of k placements through cunibs_solve_block (host buffers in and out)."""
+        pos, mom, centers, handles, dists = self._block_inputs(coil, centers, handles, dists)
+        k = centers.shape[0]
+        res, out = self._block_outputs(k, magnitude, vectors, potential, recovery, nodal)
         opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
                          int(bool(warm_start)))
         check(self._lib.cunibs_solve_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
                                            _p(dists), k, float(didt), C.byref(opts), C.byref(out)))
+        res["total_iterations"] = out.total_iterations
+        res["outer_steps"] = out.outer_steps
+        return res
+
+    def submit_block(self, coil, centers, handles, dists, didt, *, block_width=0, precision=PREC_DEFAULT,
+                     tolerance=0.0, max_iters=0, magnitude=False, vectors=False, potential=False,
+                     recovery="raw", nodal=False, warm_start=False) -> int:
+        """cunibs_submit_block: prepare a block (host inputs, copied now) without waiting for the
+        work; returns the ticket that finish_block takes. The outputs are chosen here."""
+        pos, mom, centers, handles, dists = self._block_inputs(coil, centers, handles, dists)
+        k = centers.shape[0]
+        if nodal and recovery == "raw":
+            raise ValueError("nodal=True needs a recovery mode")
+        opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
+                         int(bool(warm_start)))
+        t = C.c_longlong(0)
+        check(self._lib.cunibs_submit_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
+                                            _p(dists), k, float(didt), C.byref(opts), C.byref(t)))
+        self._submitted[t.value] = (k, magnitude, vectors, potential, recovery, nodal)
+        return t.value
+
+    def cancel_block(self, ticket: int) -> None:
+        """cunibs_cancel_block: drop a submitted block without solving it."""
+        self._submitted.pop(ticket, None)
+        check(self._lib.cunibs_cancel_block(self.handle, int(ticket)))
+
+    def finish_block(self, ticket: int) -> dict:
+        """cunibs_finish_block: solve a submitted block; the same dict as solve_block."""
+        k, magnitude, vectors, potential, recovery, nodal = self._submitted.pop(ticket)
+        res, out = self._block_outputs(k, magnitude, vectors, potential, recovery, nodal)
+        check(self._lib.cunibs_finish_block(self.handle, int(ticket), C.byref(out)))
         res["total_iterations"] = out.total_iterations
         res["outer_steps"] = out.outer_steps
         return res

@@ -1,5 +1,6 @@
 // The C ABI (include/cunibs_b200.h): context lifetime, the block solve, stage-level entry points.
 #include <cstring>
+#include <deque>
 #include <string>
 #include <type_traits>
 
@@ -50,25 +51,65 @@ int pad_width(int k) {
 
 void cunibs::set_last_error(const std::string& message) { g_last_error = message; }
 
+// What a block's preparation (placement, dA/dt, right-hand side) leaves for its solve. Two slots
+// let the next block be prepared while the previous one is solved.
+struct BlockSlot {
+    DevArray<double> in_pos, in_mom, in_centers, in_handles, in_dists;  // host-entry inputs, uploaded
+    DevArray<double> T, B, X0;  // X0: the learned initial guess
+    DevArray<int> deg;
+    DevArray<unsigned char> dip_packed;
+    DevArray<float> dadt_nodes, dadt_elm;
+    cudaEvent_t prepared = nullptr, placed = nullptr, guessed = nullptr;
+    int* h_deg = nullptr;  // pinned: the degenerate-placement flags
+};
+
+// Pinned host staging of a finished block's per-column statistics (device outputs).
+struct Staging {
+    int iters[16];
+    double rel[16];
+    int used[16];
+    double init[16];
+};
+
+struct PendingBlock {
+    long long ticket = 0;
+    int slot = 0, k = 0, K = 0;
+    bool has_opts = false, has_handles = false;
+    bool timed = false;  // stage events recorded (only for a block prepared with no other in flight)
+    cunibs_solve_opts opts{};
+};
+
 struct cunibs_context {
     int device = 0;
     Params prm;
+    // The solve and everything after it run on `stream`; block preparation runs on `prep`, at a
+    // lower priority, so that it fills what the latency-bound solve leaves of the SMs.
     cudaStream_t stream = nullptr;
+    cudaStream_t prep = nullptr;
     Mesh mesh;
     Hierarchy hier;
     SolverPtr solver;
     SummaryWork sw;
     // Block workspace, grown on demand.
-    DevArray<double> pos, mom, centers, handles, dists, T, B, X, summary, v;
-    DevArray<int> deg;
+    DevArray<double> pos, mom, centers, handles, dists, T, X, summary, v;
+    DevArray<int> deg, coil_flag;
     DevArray<unsigned char> dip_packed, zdip_packed;
-    DevArray<float> dadt_nodes, dadt_elm, magn, E;
+    DevArray<float> dadt_nodes, magn, E;
+    BlockSlot slots[2];
+    std::deque<PendingBlock> pending;
+    int next_slot = 0;
+    long long next_ticket = 1;
+    int* h_coil_flag = nullptr;  // pinned
+    Staging* staging = nullptr;  // pinned
+    cudaEvent_t ev_main = nullptr;
+    // Blocks per SM given to the dA/dt kernel while another block's solve may run beside it.
+    int overlap_blocks_per_sm = 2;
+    int sm_count = 0;
     // Field-recovery operators, built on first use per mode, and their block workspace.
     std::unique_ptr<RecoveryOp> rec[4];
     DevArray<float> e_slots, e_raw;
     // Learned warm start (installed by cunibs_context_set_warmstart) and its per-block outputs.
     std::unique_ptr<WarmStart> warm;
-    DevArray<double> X0;
     std::vector<int> warm_used;
     std::vector<double> init_rel;
     // Stage timing (CUDA events on the context stream), enabled by cunibs_context_set_timing.
@@ -76,8 +117,8 @@ struct cunibs_context {
     cudaEvent_t ev[6] = {};
     double stage_ms[5] = {};
 
-    void mark(int i) {
-        if (timing) CUNIBS_CHECK(cudaEventRecord(ev[i], stream));
+    void mark(int i, cudaStream_t on) {
+        if (timing) CUNIBS_CHECK(cudaEventRecord(ev[i], on));
     }
 
     RecoveryOp& recovery(int mode) {
@@ -102,7 +143,16 @@ struct cunibs_context {
     ~cunibs_context() {
         for (cudaEvent_t e : ev)
             if (e) cudaEventDestroy(e);
+        for (BlockSlot& sl : slots) {
+            for (cudaEvent_t e : {sl.prepared, sl.placed, sl.guessed})
+                if (e) cudaEventDestroy(e);
+            if (sl.h_deg) cudaFreeHost(sl.h_deg);
+        }
+        if (ev_main) cudaEventDestroy(ev_main);
+        if (h_coil_flag) cudaFreeHost(h_coil_flag);
+        if (staging) cudaFreeHost(staging);
         solver.reset();
+        if (prep) cudaStreamDestroy(prep);
         if (stream) cudaStreamDestroy(stream);
     }
 };
@@ -130,66 +180,151 @@ Params resolve(const cunibs_context* c, const cunibs_solve_opts* o) {
     return p;
 }
 
-// The block solve on device-resident inputs; outputs land in the context's workspace.
-void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, int n_dip, const double* centers,
-                     const double* handles, const double* dists, int k, double didt, const cunibs_solve_opts* opts,
-                     SolveStats& st, bool want_E, int& K_out) {
+constexpr int kMaxBlock = 16;
+
+void copy_out(void* dst, const void* src, std::size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
+std::size_t slot_bytes(const cunibs_context* c, const cunibs_solve_opts* opts, int k);
+
+// Block preparation on the preparation stream: the coil placement, dA/dt at the nodes and
+// elements, and the right-hand side, into a free slot. Device inputs are read asynchronously and
+// must stay valid until the block is finished; host inputs are copied into the slot first.
+// bounded_dadt gives the dA/dt kernel a bounded grid, for a preparation that runs beside another
+// block's solve. Returns the block's ticket.
+long long prepare_block(cunibs_context* c, const double* pos, const double* mom, int n_dip, const double* centers,
+                        const double* handles, const double* dists, int k, double didt, const cunibs_solve_opts* opts,
+                        bool host_inputs, bool bounded_dadt) {
     require(k >= 1, "need at least one placement");
     require(n_dip >= 1, "the coil needs at least one dipole");
+    require(pos && mom && centers && dists, "input arrays must not be NULL");
     const int K = (opts && opts->block_width > 0) ? opts->block_width : pad_width(k);
     require(K >= k, "block_width must be at least the number of placements");
-    K_out = K;
-    const Params prm = resolve(c, opts);
+    require(K <= kMaxBlock, "at most 16 placements per block");
     const int rec_mode = opts ? opts->recovery : kRecRaw;
     require(rec_mode >= kRecRaw && rec_mode <= kRecHarmonic, "unknown recovery mode");
+    const bool warm = opts && opts->warm_start;
+    if (warm) {
+        require(c->warm != nullptr, "warm_start requested but no warm-start network is installed");
+        require(c->warm->n_red == c->mesh.n_nodes - 1, "the installed warm start was built for another mesh");
+    }
+    int si = -1;
+    for (int t = 0; t < 2 && si < 0; ++t) {
+        const int cand = (c->next_slot + t) & 1;
+        bool used = false;
+        for (const PendingBlock& q : c->pending) used = used || q.slot == cand;
+        if (!used) si = cand;
+    }
+    require(si >= 0, "two blocks are already submitted: finish one before submitting another");
+    const bool beside_solve = bounded_dadt && !c->pending.empty();
+    BlockSlot& sl = c->slots[si];
+    Mesh& m = c->mesh;
+    cudaStream_t ps = c->prep;
+    const bool timed = c->timing && c->pending.empty();
+    auto mark = [&](int i) {
+        if (timed) c->mark(i, ps);
+    };
+    const int n_red = m.n_nodes - 1;
+    if (host_inputs) {
+        sl.in_pos.upload(pos, 3 * static_cast<std::size_t>(n_dip), ps);
+        sl.in_mom.upload(mom, 3 * static_cast<std::size_t>(n_dip), ps);
+        sl.in_centers.upload(centers, 3 * static_cast<std::size_t>(k), ps);
+        if (handles) sl.in_handles.upload(handles, 3 * static_cast<std::size_t>(k), ps);
+        sl.in_dists.upload(dists, static_cast<std::size_t>(k), ps);
+        pos = sl.in_pos.get();
+        mom = sl.in_mom.get();
+        centers = sl.in_centers.get();
+        handles = handles ? sl.in_handles.get() : nullptr;
+        dists = sl.in_dists.get();
+    }
+    // The coil's kind (all moments along its own z axis, or not) picks the dA/dt kernel.
+    c->zdip_packed.reserve(packed_zdipole_bytes() * static_cast<std::size_t>(n_dip));
+    c->coil_flag.reserve(1);
+    prep_zdipoles(pos, mom, n_dip, c->zdip_packed.get(), c->coil_flag.get(), ps);
+    CUNIBS_CHECK(cudaMemcpyAsync(c->h_coil_flag, c->coil_flag.get(), sizeof(int), cudaMemcpyDeviceToHost, ps));
+    CUNIBS_CHECK(cudaStreamSynchronize(ps));
+    const bool zcoil = *c->h_coil_flag == 0;
+    // The slot's previous block is finished on the context stream: start after what that stream
+    // holds so far.
+    CUNIBS_CHECK(cudaEventRecord(c->ev_main, c->stream));
+    CUNIBS_CHECK(cudaStreamWaitEvent(ps, c->ev_main, 0));
+    mark(0);
+    sl.T.reserve(16 * static_cast<std::size_t>(k));
+    sl.deg.reserve(k);
+    place_transforms(m, centers, handles, dists, k, sl.T.get(), sl.deg.get(), ps);
+    CUNIBS_CHECK(cudaMemcpyAsync(sl.h_deg, sl.deg.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, ps));
+    // The learned guess needs only the placement. Its GEMMs go on the context stream now, ahead
+    // of the solve of any block submitted earlier, and this block's dA/dt waits for them: the
+    // tensor-core tiles then find the SMs free of the long-lived dA/dt blocks.
+    if (warm) {
+        CUNIBS_CHECK(cudaEventRecord(sl.placed, ps));
+        CUNIBS_CHECK(cudaStreamWaitEvent(c->stream, sl.placed, 0));
+        sl.X0.reserve(static_cast<std::size_t>(n_red) * K);
+        warm_start_guess(*c->warm, sl.T.get(), k, K, sl.X0.get(), c->stream);
+        CUNIBS_CHECK(cudaEventRecord(sl.guessed, c->stream));
+        CUNIBS_CHECK(cudaStreamWaitEvent(ps, sl.guessed, 0));
+    }
+    sl.dadt_nodes.reserve(static_cast<std::size_t>(m.n_nodes) * 3 * k);
+    const int dadt_blocks = beside_solve ? c->overlap_blocks_per_sm * c->sm_count : 0;
+    if (zcoil) {
+        mark(1);
+        dadt_nodes_zcoil(m, c->zdip_packed.get(), n_dip, sl.T.get(), k, didt, sl.dadt_nodes.get(), ps, dadt_blocks);
+    } else {
+        sl.dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
+        prep_dipoles(pos, mom, n_dip, sl.T.get(), k, sl.dip_packed.get(), ps);
+        mark(1);
+        dadt_nodes(m, reinterpret_cast<const float*>(sl.dip_packed.get()), n_dip, sl.T.get(), k, didt,
+                   sl.dadt_nodes.get(), ps, dadt_blocks);
+    }
+    mark(2);
+    sl.dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
+    dadt_elements(m, sl.dadt_nodes.get(), k, sl.dadt_elm.get(), ps);
+    sl.B.reserve(static_cast<std::size_t>(n_red) * K);
+    rhs_block(m, sl.dadt_elm.get(), k, K, sl.B.get(), ps);
+    mark(3);
+    CUNIBS_CHECK(cudaEventRecord(sl.prepared, ps));
+    PendingBlock pb;
+    pb.slot = si;
+    pb.k = k;
+    pb.K = K;
+    pb.has_handles = handles != nullptr;
+    pb.has_opts = opts != nullptr;
+    pb.timed = timed;
+    if (opts) pb.opts = *opts;
+    pb.ticket = c->next_ticket++;
+    c->pending.push_back(pb);
+    c->next_slot = si ^ 1;
+    return pb.ticket;
+}
+
+// Solve, field recovery and summary of a prepared block, on the context stream; outputs land in
+// the context's workspace (and the slot's transforms). The block leaves the pending list whether
+// or not this succeeds.
+PendingBlock finish_block(cunibs_context* c, long long ticket, SolveStats& st, bool want_E) {
+    auto it = c->pending.begin();
+    while (it != c->pending.end() && it->ticket != ticket) ++it;
+    if (it == c->pending.end()) fail(kEInval, "no submitted block with ticket " + std::to_string(ticket));
+    const PendingBlock pb = *it;
+    c->pending.erase(it);
+    BlockSlot& sl = c->slots[pb.slot];
+    const int k = pb.k, K = pb.K;
+    const cunibs_solve_opts* opts = pb.has_opts ? &pb.opts : nullptr;
+    const Params prm = resolve(c, opts);
+    const int rec_mode = opts ? opts->recovery : kRecRaw;
     RecoveryOp* op = rec_mode == kRecRaw ? nullptr : &c->recovery(rec_mode);
     Mesh& m = c->mesh;
     cudaStream_t s = c->stream;
     const int n_red = m.n_nodes - 1;
-    c->T.reserve(16 * static_cast<std::size_t>(k));
-    c->deg.reserve(k);
-    c->mark(0);
-    c->deg.reserve(k + 1);
-    place_transforms(m, centers, handles, dists, k, c->T.get(), c->deg.get(), s);
-    c->zdip_packed.reserve(packed_zdipole_bytes() * static_cast<std::size_t>(n_dip));
-    prep_zdipoles(pos, mom, n_dip, c->zdip_packed.get(), c->deg.get() + k, s);
-    std::vector<int> deg(k + 1);
-    CUNIBS_CHECK(cudaMemcpyAsync(deg.data(), c->deg.get(), sizeof(int) * (k + 1), cudaMemcpyDeviceToHost, s));
-    CUNIBS_CHECK(cudaStreamSynchronize(s));
-    const bool zcoil = deg[k] == 0;
+    CUNIBS_CHECK(cudaEventSynchronize(sl.prepared));
     for (int i = 0; i < k; ++i)
-        if (handles != nullptr && deg[i])
+        if (pb.has_handles && sl.h_deg[i])
             fail(kEInval, "degenerate coil placement at index " + std::to_string(i) + " of " + std::to_string(k) +
                               ": the handle lies on the outward scalp normal through the projected centre, so the "
                               "coil's rotation about the normal is undefined");
-    c->dadt_nodes.reserve(static_cast<std::size_t>(m.n_nodes) * 3 * k);
-    if (zcoil) {
-        c->mark(1);
-        dadt_nodes_zcoil(m, c->zdip_packed.get(), n_dip, c->T.get(), k, didt, c->dadt_nodes.get(), s);
-    } else {
-        c->dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
-        prep_dipoles(pos, mom, n_dip, c->T.get(), k, c->dip_packed.get(), s);
-        c->mark(1);
-        dadt_nodes(m, reinterpret_cast<const float*>(c->dip_packed.get()), n_dip, c->T.get(), k, didt,
-                   c->dadt_nodes.get(), s);
-    }
-    c->mark(2);
-    c->dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
-    dadt_elements(m, c->dadt_nodes.get(), k, c->dadt_elm.get(), s);
-    c->B.reserve(static_cast<std::size_t>(n_red) * K);
+    CUNIBS_CHECK(cudaStreamWaitEvent(s, sl.prepared, 0));
     c->X.reserve(static_cast<std::size_t>(n_red) * K);
-    rhs_block(m, c->dadt_elm.get(), k, K, c->B.get(), s);
-    c->mark(3);
     const bool warm = opts && opts->warm_start;
     c->warm_used.assign(k, 0);
     c->init_rel.assign(k, 1.0);
-    if (warm) {
-        require(c->warm != nullptr, "warm_start requested but no warm-start network is installed");
-        require(c->warm->n_red == n_red, "the installed warm start was built for another mesh");
-        c->X0.reserve(static_cast<std::size_t>(n_red) * K);
-        warm_start_guess(*c->warm, c->T.get(), k, K, c->X0.get(), s);
-    }
-    solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, prm, s, st, warm ? c->X0.get() : nullptr);
+    solver_solve(*c->solver, sl.B.get(), c->X.get(), k, K, prm, s, st, warm ? sl.X0.get() : nullptr);
     if (warm) {
         warm_start_check(*c->warm, s);
         for (int i = 0; i < k; ++i) {
@@ -206,7 +341,7 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
         Params retry = prm;
         retry.precision = kPlainFp64;
         SolveStats st2;
-        solver_solve(*c->solver, c->B.get(), c->X.get(), k, K, retry, s, st2, c->X.get());
+        solver_solve(*c->solver, sl.B.get(), c->X.get(), k, K, retry, s, st2, c->X.get());
         for (int i : missed) {
             st.col_iters[i] += st2.col_iters[i];
             st.col_rel[i] = st2.col_rel[i];
@@ -218,27 +353,27 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
         }
         st.iterations += st2.iterations;
     }
-    c->mark(4);
+    if (pb.timed) c->mark(4, s);
     c->magn.reserve(static_cast<std::size_t>(m.n_tets) * k);
     if (want_E) c->E.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
     if (op == nullptr) {
-        reconstruct_block(m, c->X.get(), k, K, c->dadt_elm.get(), want_E ? c->E.get() : nullptr, c->magn.get(), s);
+        reconstruct_block(m, c->X.get(), k, K, sl.dadt_elm.get(), want_E ? c->E.get() : nullptr, c->magn.get(), s);
     } else {
         // The potential-consuming mode never forms the raw field (fem/solve.py:943-965).
         const float* e_elem = nullptr;
         if (rec_mode != kRecHarmonic) {
             c->e_raw.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
-            reconstruct_block(m, c->X.get(), k, K, c->dadt_elm.get(), c->e_raw.get(), c->magn.get(), s);
+            reconstruct_block(m, c->X.get(), k, K, sl.dadt_elm.get(), c->e_raw.get(), c->magn.get(), s);
             e_elem = c->e_raw.get();
         }
         c->e_slots.reserve(static_cast<std::size_t>(op->n_slots) * 3 * k);
-        apply_recovery(m, *op, c->X.get(), K, c->dadt_nodes.get(), e_elem, k, c->e_slots.get(),
+        apply_recovery(m, *op, c->X.get(), K, sl.dadt_nodes.get(), e_elem, k, c->e_slots.get(),
                        want_E ? c->E.get() : nullptr, c->magn.get(), s);
     }
     c->summary.reserve(static_cast<std::size_t>(kSummaryLen) * k);
     gm_summary(m, c->magn.get(), k, c->summary.get(), c->sw, s);
-    c->mark(5);
-    if (c->timing) {
+    if (pb.timed) c->mark(5, s);
+    if (pb.timed && c->timing) {
         CUNIBS_CHECK(cudaEventSynchronize(c->ev[5]));
         for (int i = 0; i < 5; ++i) {
             float ms = 0.0f;
@@ -246,6 +381,65 @@ void solve_block_dev(cunibs_context* c, const double* pos, const double* mom, in
             c->stage_ms[i] = ms;
         }
     }
+    return pb;
+}
+
+// Host outputs of a finished block (cunibs_block_out host pointers).
+void block_outputs_host(cunibs_context* c, const PendingBlock& pb, const SolveStats& st, cunibs_block_out* out) {
+    const Mesh& m = c->mesh;
+    cudaStream_t s = c->stream;
+    const int k = pb.k;
+    const cunibs_solve_opts* opts = pb.has_opts ? &pb.opts : nullptr;
+    copy_out(out->transforms, c->slots[pb.slot].T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToHost, s);
+    copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToHost, s);
+    copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
+    copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
+    copy_out(out->E_slots, c->e_slots.get(), slot_bytes(c, opts, k), cudaMemcpyDeviceToHost, s);
+    if (out->v) {
+        c->v.reserve(static_cast<std::size_t>(m.n_nodes) * k);
+        scatter_potential(m, c->X.get(), k, pb.K, c->v.get(), s);
+        copy_out(out->v, c->v.get(), sizeof(double) * static_cast<std::size_t>(m.n_nodes) * k, cudaMemcpyDeviceToHost, s);
+    }
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    for (int i = 0; i < k; ++i) {
+        if (out->iterations) out->iterations[i] = st.col_iters[i];
+        if (out->relres) out->relres[i] = st.col_rel[i];
+        if (out->warm_used) out->warm_used[i] = c->warm_used[i];
+        if (out->init_relres) out->init_relres[i] = c->init_rel[i];
+    }
+    out->total_iterations = st.iterations;
+    out->outer_steps = st.outer_steps;
+}
+
+// Device outputs of a finished block (cunibs_block_out device pointers).
+void block_outputs_device(cunibs_context* c, const PendingBlock& pb, const SolveStats& st, cunibs_block_out* out) {
+    const Mesh& m = c->mesh;
+    cudaStream_t s = c->stream;
+    const int k = pb.k;
+    const cunibs_solve_opts* opts = pb.has_opts ? &pb.opts : nullptr;
+    copy_out(out->transforms, c->slots[pb.slot].T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToDevice, s);
+    copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToDevice, s);
+    copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
+    copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
+    copy_out(out->E_slots, c->e_slots.get(), slot_bytes(c, opts, k), cudaMemcpyDeviceToDevice, s);
+    if (out->v) scatter_potential(m, c->X.get(), k, pb.K, out->v, s);
+    // Per-column statistics go up from pinned staging (no pageable-memory copies).
+    Staging& h = *c->staging;
+    for (int i = 0; i < k; ++i) {
+        h.iters[i] = st.col_iters[i];
+        h.rel[i] = st.col_rel[i];
+        h.used[i] = c->warm_used[i];
+        h.init[i] = c->init_rel[i];
+    }
+    copy_out(out->iterations, h.iters, sizeof(int) * k, cudaMemcpyHostToDevice, s);
+    copy_out(out->relres, h.rel, sizeof(double) * k, cudaMemcpyHostToDevice, s);
+    copy_out(out->warm_used, h.used, sizeof(int) * k, cudaMemcpyHostToDevice, s);
+    copy_out(out->init_relres, h.init, sizeof(double) * k, cudaMemcpyHostToDevice, s);
+    // Returning only once the outputs are complete measured faster in a two-deep pipeline than
+    // returning at once: the next submit then finds the previous block's work done.
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    out->total_iterations = st.iterations;
+    out->outer_steps = st.outer_steps;
 }
 
 void copy_out(void* dst, const void* src, std::size_t bytes, cudaMemcpyKind kind, cudaStream_t s) {
@@ -311,7 +505,20 @@ int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_no
         c->prm.inner_max_iters = p.inner_max_iters;
         c->prm.iters_per_sync = p.iters_per_sync > 0 ? p.iters_per_sync : 4;
         require(c->prm.tolerance > 0 && c->prm.max_iters > 0, "tolerance and max_iters must be positive");
-        CUNIBS_CHECK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        int least = 0, greatest = 0;
+        CUNIBS_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUNIBS_CHECK(cudaStreamCreateWithPriority(&c->stream, cudaStreamNonBlocking, greatest));
+        CUNIBS_CHECK(cudaStreamCreateWithPriority(&c->prep, cudaStreamNonBlocking, least));
+        CUNIBS_CHECK(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device));
+        CUNIBS_CHECK(cudaEventCreateWithFlags(&c->ev_main, cudaEventDisableTiming));
+        CUNIBS_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&c->h_coil_flag), sizeof(int), cudaHostAllocDefault));
+        CUNIBS_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&c->staging), sizeof(Staging), cudaHostAllocDefault));
+        for (BlockSlot& sl : c->slots) {
+            for (cudaEvent_t* e : {&sl.prepared, &sl.placed, &sl.guessed})
+                CUNIBS_CHECK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            CUNIBS_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&sl.h_deg), sizeof(int) * kMaxBlock,
+                                       cudaHostAllocDefault));
+        }
         build_mesh(c->mesh, nodes_mm, n_nodes, tet_nodes, tet_tags, n_tets, skin_tris, n_skin, c->stream);
         c->rebuild_hierarchy();
         *out = c.release();
@@ -322,6 +529,7 @@ int cunibs_context_destroy(cunibs_context* ctx) {
     return guarded([&] {
         if (!ctx) return;
         DeviceGuard dg(ctx->device);
+        CUNIBS_CHECK(cudaStreamSynchronize(ctx->prep));
         CUNIBS_CHECK(cudaStreamSynchronize(ctx->stream));
         delete ctx;
     });
@@ -375,36 +583,11 @@ int cunibs_solve_block(cunibs_context* c, const double* dip_pos_m, const double*
         require(dip_pos_m && dip_moment && centers_mm && handles_mm && dists_mm, "input arrays must not be NULL");
         require(out->transforms && out->summary, "out->transforms and out->summary are required");
         DeviceGuard dg(c->device);
-        cudaStream_t s = c->stream;
-        c->pos.upload(dip_pos_m, 3 * static_cast<std::size_t>(n_dip), s);
-        c->mom.upload(dip_moment, 3 * static_cast<std::size_t>(n_dip), s);
-        c->centers.upload(centers_mm, 3 * static_cast<std::size_t>(k), s);
-        c->handles.upload(handles_mm, 3 * static_cast<std::size_t>(k), s);
-        c->dists.upload(dists_mm, static_cast<std::size_t>(k), s);
+        const long long t = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k, didt,
+                                          opts, true, false);
         SolveStats st;
-        int K = 0;
-        solve_block_dev(c, c->pos.get(), c->mom.get(), n_dip, c->centers.get(), c->handles.get(), c->dists.get(), k,
-                        didt, opts, st, out->E != nullptr, K);
-        const Mesh& m = c->mesh;
-        copy_out(out->transforms, c->T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToHost, s);
-        copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToHost, s);
-        copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
-        copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToHost, s);
-        copy_out(out->E_slots, c->e_slots.get(), slot_bytes(c, opts, k), cudaMemcpyDeviceToHost, s);
-        if (out->v) {
-            c->v.reserve(static_cast<std::size_t>(m.n_nodes) * k);
-            scatter_potential(m, c->X.get(), k, K, c->v.get(), s);
-            copy_out(out->v, c->v.get(), sizeof(double) * static_cast<std::size_t>(m.n_nodes) * k, cudaMemcpyDeviceToHost, s);
-        }
-        CUNIBS_CHECK(cudaStreamSynchronize(s));
-        for (int i = 0; i < k; ++i) {
-            if (out->iterations) out->iterations[i] = st.col_iters[i];
-            if (out->relres) out->relres[i] = st.col_rel[i];
-            if (out->warm_used) out->warm_used[i] = c->warm_used[i];
-            if (out->init_relres) out->init_relres[i] = c->init_rel[i];
-        }
-        out->total_iterations = st.iterations;
-        out->outer_steps = st.outer_steps;
+        const PendingBlock pb = finish_block(c, t, st, out->E != nullptr);
+        block_outputs_host(c, pb, st, out);
     });
 }
 
@@ -415,29 +598,82 @@ int cunibs_solve_block_device(cunibs_context* c, const double* dip_pos_m, const 
         require(c && out, "NULL argument");
         require(out->transforms && out->summary, "out->transforms and out->summary are required");
         DeviceGuard dg(c->device);
-        cudaStream_t s = c->stream;
+        const long long t = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k, didt,
+                                          opts, false, false);
         SolveStats st;
-        int K = 0;
-        solve_block_dev(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k, didt, opts, st,
-                        out->E != nullptr, K);
-        const Mesh& m = c->mesh;
-        copy_out(out->transforms, c->T.get(), sizeof(double) * 16 * k, cudaMemcpyDeviceToDevice, s);
-        copy_out(out->summary, c->summary.get(), sizeof(double) * kSummaryLen * k, cudaMemcpyDeviceToDevice, s);
-        copy_out(out->magnE, c->magn.get(), sizeof(float) * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
-        copy_out(out->E, c->E.get(), sizeof(float) * 3 * static_cast<std::size_t>(m.n_tets) * k, cudaMemcpyDeviceToDevice, s);
-        copy_out(out->E_slots, c->e_slots.get(), slot_bytes(c, opts, k), cudaMemcpyDeviceToDevice, s);
-        if (out->v) scatter_potential(m, c->X.get(), k, K, out->v, s);
-        CUNIBS_CHECK(cudaStreamSynchronize(s));
-        if (out->iterations)
-            CUNIBS_CHECK(cudaMemcpy(out->iterations, st.col_iters.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
-        if (out->relres)
-            CUNIBS_CHECK(cudaMemcpy(out->relres, st.col_rel.data(), sizeof(double) * k, cudaMemcpyHostToDevice));
-        if (out->warm_used)
-            CUNIBS_CHECK(cudaMemcpy(out->warm_used, c->warm_used.data(), sizeof(int) * k, cudaMemcpyHostToDevice));
-        if (out->init_relres)
-            CUNIBS_CHECK(cudaMemcpy(out->init_relres, c->init_rel.data(), sizeof(double) * k, cudaMemcpyHostToDevice));
-        out->total_iterations = st.iterations;
-        out->outer_steps = st.outer_steps;
+        const PendingBlock pb = finish_block(c, t, st, out->E != nullptr);
+        block_outputs_device(c, pb, st, out);
+    });
+}
+
+int cunibs_submit_block(cunibs_context* c, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                        const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
+                        double didt, const cunibs_solve_opts* opts, long long* ticket) {
+    return guarded([&] {
+        require(c && ticket, "NULL argument");
+        require(dip_pos_m && dip_moment && centers_mm && handles_mm && dists_mm, "input arrays must not be NULL");
+        DeviceGuard dg(c->device);
+        *ticket = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k, didt, opts,
+                                true, true);
+    });
+}
+
+int cunibs_finish_block(cunibs_context* c, long long ticket, cunibs_block_out* out) {
+    return guarded([&] {
+        require(c && out, "NULL argument");
+        require(out->transforms && out->summary, "out->transforms and out->summary are required");
+        DeviceGuard dg(c->device);
+        SolveStats st;
+        const PendingBlock pb = finish_block(c, ticket, st, out->E != nullptr);
+        block_outputs_host(c, pb, st, out);
+    });
+}
+
+int cunibs_submit_block_device(cunibs_context* c, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                               const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
+                               double didt, const cunibs_solve_opts* opts, long long* ticket) {
+    return guarded([&] {
+        require(c && ticket, "NULL argument");
+        DeviceGuard dg(c->device);
+        *ticket = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k, didt, opts,
+                                false, true);
+    });
+}
+
+int cunibs_finish_block_device(cunibs_context* c, long long ticket, cunibs_block_out* out) {
+    return guarded([&] {
+        require(c && out, "NULL argument");
+        require(out->transforms && out->summary, "out->transforms and out->summary are required");
+        DeviceGuard dg(c->device);
+        SolveStats st;
+        const PendingBlock pb = finish_block(c, ticket, st, out->E != nullptr);
+        block_outputs_device(c, pb, st, out);
+    });
+}
+
+int cunibs_cancel_block(cunibs_context* c, long long ticket) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        auto it = c->pending.begin();
+        while (it != c->pending.end() && it->ticket != ticket) ++it;
+        if (it == c->pending.end()) fail(kEInval, "no submitted block with ticket " + std::to_string(ticket));
+        // The slot's buffers are next written on the preparation stream, behind this block's work.
+        c->pending.erase(it);
+    });
+}
+
+int cunibs_context_pending(const cunibs_context* c, int* n) {
+    return guarded([&] {
+        require(c && n, "NULL argument");
+        *n = static_cast<int>(c->pending.size());
+    });
+}
+
+int cunibs_context_set_overlap(cunibs_context* c, int blocks_per_sm) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        require(blocks_per_sm >= 1 && blocks_per_sm <= 16, "blocks_per_sm must be in [1, 16]");
+        c->overlap_blocks_per_sm = blocks_per_sm;
     });
 }
 

@@ -9,6 +9,7 @@
 // pairs so the arithmetic issues as sm_100 packed FP32 instructions (FFMA2/FADD2/FMUL2): two node
 // evaluations per instruction. The difference r - s is formed directly rather than through
 // |r|^2 + |s|^2 - 2 r.s, which costs no more here and loses nothing to cancellation.
+#include <algorithm>
 #include <cstdint>
 
 #include "internal.hpp"
@@ -51,18 +52,21 @@ __global__ void prep_dipoles_kernel(const double* __restrict__ pos, const double
 
 __device__ __forceinline__ float2 f2neg(float2 a) { return make_float2(-a.x, -a.y); }
 
-// grid = (ceil(N / (4*threads)), k). Node i of this thread: base + {0, 1, 2, 3} * stride, paired
-// as (0, 1) and (2, 3) into float2 lanes.
+// Work items are (node tile, placement) pairs, item = p * n_tiles + tile, walked by a grid of any
+// size (a bounded grid leaves room on every SM for kernels of other streams). Node i of this thread
+// in a tile: tile * threads + threadIdx + {0, 1, 2, 3} * n_tiles * threads, paired as (0, 1) and
+// (2, 3) into float2 lanes; the per-node arithmetic does not depend on the grid.
 __global__ void __launch_bounds__(kDadtThreads) dadt_kernel(const double* __restrict__ nodes_mm, int n_nodes,
                                                             const DipolePacked* __restrict__ dip, int n_dip,
                                                             const double* __restrict__ T, float scale,
-                                                            float* __restrict__ out) {
+                                                            float* __restrict__ out, int n_tiles, int n_items) {
     __shared__ DipolePacked tile[kDipTile];
-    const int p = blockIdx.y;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int p = item / n_tiles;
     const double* Tp = T + 16 * static_cast<long>(p);
     const double ox = Tp[3] * 1e-3, oy = Tp[7] * 1e-3, oz = Tp[11] * 1e-3;
-    const int stride = gridDim.x * blockDim.x;
-    const int base = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = n_tiles * blockDim.x;
+    const int base = (item - p * n_tiles) * blockDim.x + threadIdx.x;
     int node[4];
     float rxs[4], rys[4], rzs[4];
 #pragma unroll
@@ -133,6 +137,7 @@ __global__ void __launch_bounds__(kDadtThreads) dadt_kernel(const double* __rest
             o[3 * static_cast<long>(node[u]) + 2] = scale * az[u];
         }
     }
+    }
 }
 
 // dadt_elm[p][e] = 1/4 sum of the four nodal values (dadt_element.cu:6-31).
@@ -191,21 +196,42 @@ void prep_dipoles(const double* pos, const double* mom, int n_dip, const double*
 
 std::size_t packed_dipole_bytes() { return sizeof(DipolePacked); }
 
-void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k, double didt,
-                float* out, cudaStream_t s) {
+namespace {
+
+// Tiles of 4 * threads nodes; the grid is one block per (tile, placement) item, or max_blocks
+// blocks walking the items when max_blocks > 0.
+struct DadtGrid {
+    int n_tiles, n_items, blocks;
+};
+
+DadtGrid dadt_grid(int n_nodes, int k, int max_blocks) {
     const int per_block = 4 * kDadtThreads;
-    const dim3 grid((m.n_nodes + per_block - 1) / per_block, k);
-    dadt_kernel<<<grid, kDadtThreads, 0, s>>>(m.nodes.get(), m.n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
-                                             n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out); count_launch();
+    DadtGrid g;
+    g.n_tiles = (n_nodes + per_block - 1) / per_block;
+    g.n_items = g.n_tiles * k;
+    g.blocks = max_blocks > 0 ? std::min(g.n_items, max_blocks) : g.n_items;
+    return g;
+}
+
+}  // namespace
+
+void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k, double didt,
+                float* out, cudaStream_t s, int max_blocks) {
+    const DadtGrid g = dadt_grid(m.n_nodes, k, max_blocks);
+    dadt_kernel<<<g.blocks, kDadtThreads, 0, s>>>(m.nodes.get(), m.n_nodes,
+                                                 reinterpret_cast<const DipolePacked*>(dip_packed), n_dip,
+                                                 transforms_dev, static_cast<float>(didt * 1e-7), out, g.n_tiles,
+                                                 g.n_items);
+    count_launch();
     CUNIBS_LAUNCH_CHECK("dadt");
 }
 
 void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
                     const double* transforms_dev, int k, double didt, float* out, cudaStream_t s) {
-    const int per_block = 4 * kDadtThreads;
-    const dim3 grid((n_nodes + per_block - 1) / per_block, k);
-    dadt_kernel<<<grid, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
-                                             n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out);
+    const DadtGrid g = dadt_grid(n_nodes, k, 0);
+    dadt_kernel<<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
+                                                 n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out,
+                                                 g.n_tiles, g.n_items);
     count_launch();
 }
 
@@ -269,12 +295,14 @@ __global__ void prep_zdipoles_kernel(const double* __restrict__ pos, const doubl
     if (threadIdx.x == 0 && any) atomicOr(flag, 1);
 }
 
+// Work items and node order as dadt_kernel's.
 __global__ void __launch_bounds__(kDadtThreads) dadt_zcoil_kernel(const double* __restrict__ nodes_mm, int n_nodes,
                                                                   const ZDipolePacked* __restrict__ dip, int n_dip,
                                                                   const double* __restrict__ T, float scale,
-                                                                  float* __restrict__ out) {
+                                                                  float* __restrict__ out, int n_tiles, int n_items) {
     __shared__ ZDipolePacked tile[kDipTile];
-    const int p = blockIdx.y;
+    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
+    const int p = item / n_tiles;
     const double* Tp = T + 16 * static_cast<long>(p);
     // Columns of the rotation are the coil axes in head coordinates: R[a][b] = Tp[4a + b].
     double R[3][3];
@@ -283,8 +311,8 @@ __global__ void __launch_bounds__(kDadtThreads) dadt_zcoil_kernel(const double* 
 #pragma unroll
         for (int b = 0; b < 3; ++b) R[a][b] = Tp[4 * a + b];
     const double o[3] = {Tp[3] * 1e-3, Tp[7] * 1e-3, Tp[11] * 1e-3};
-    const int stride = gridDim.x * blockDim.x;
-    const int base = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = n_tiles * blockDim.x;
+    const int base = (item - p * n_tiles) * blockDim.x + threadIdx.x;
     int node[4];
     float px[4], py[4], pz[4];
 #pragma unroll
@@ -386,6 +414,7 @@ __global__ void __launch_bounds__(kDadtThreads) dadt_zcoil_kernel(const double* 
             o_p[3 * static_cast<long>(node[u]) + 2] = R20 * a0 + R21 * a1;
         }
     }
+    }
 }
 
 }  // namespace
@@ -402,11 +431,12 @@ void prep_zdipoles(const double* pos, const double* mom, int n_dip, void* zpacke
 }
 
 void dadt_nodes_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
-                      float* out, cudaStream_t s) {
-    const int per_block = 4 * kDadtThreads;
-    const dim3 grid((m.n_nodes + per_block - 1) / per_block, k);
-    dadt_zcoil_kernel<<<grid, kDadtThreads, 0, s>>>(m.nodes.get(), m.n_nodes, static_cast<const ZDipolePacked*>(zpacked),
-                                                   n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out);
+                      float* out, cudaStream_t s, int max_blocks) {
+    const DadtGrid g = dadt_grid(m.n_nodes, k, max_blocks);
+    dadt_zcoil_kernel<<<g.blocks, kDadtThreads, 0, s>>>(m.nodes.get(), m.n_nodes,
+                                                       static_cast<const ZDipolePacked*>(zpacked), n_dip,
+                                                       transforms_dev, static_cast<float>(didt * 1e-7), out,
+                                                       g.n_tiles, g.n_items);
     count_launch();
     CUNIBS_LAUNCH_CHECK("dadt z-coil");
 }

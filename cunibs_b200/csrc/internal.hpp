@@ -153,8 +153,10 @@ std::size_t packed_dipole_bytes();
 // Rotates the coil's dipoles into each placement's head frame: (k, n_dip) packed records.
 void prep_dipoles(const double* pos, const double* mom, int n_dip, const double* transforms_dev, int k, void* out,
                   cudaStream_t s);
+// max_blocks > 0 bounds the grid (blocks then walk the (node tile, placement) items), leaving SM
+// room for kernels of other streams; the result does not depend on it.
 void dadt_nodes(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k, double didt,
-                float* out /* (k, N, 3) */, cudaStream_t s);
+                float* out /* (k, N, 3) */, cudaStream_t s, int max_blocks = 0);
 // Coils whose moments all point along the coil's own z axis (every figure-8 and circular coil
 // model) take a cheaper path evaluated in each placement's coil frame. general_flag_dev receives 0
 // when the coil qualifies, 1 when some moment has an in-plane component; zpacked has room for
@@ -163,7 +165,7 @@ std::size_t packed_zdipole_bytes();
 void prep_zdipoles(const double* pos, const double* mom, int n_dip, void* zpacked, int* general_flag_dev,
                    cudaStream_t s);
 void dadt_nodes_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
-                      float* out /* (k, N, 3) */, cudaStream_t s);
+                      float* out /* (k, N, 3) */, cudaStream_t s, int max_blocks = 0);
 void dadt_elements(const Mesh& m, const float* dadt_nodes, int k, float* dadt_elm /* (k, M, 3) */, cudaStream_t s);
 // The general-moment dA/dt on raw device node coordinates (no Mesh), packed records from prep_dipoles.
 void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,

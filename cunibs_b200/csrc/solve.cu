@@ -675,6 +675,10 @@ class Solver {
     DevArray<unsigned> counter;
     int* h_flags = nullptr;   // pinned
     double* h_dbl = nullptr;  // pinned
+    // Deferred readbacks of the last solve_plain: h_dbl[2K..3K) holds the right-hand side norms
+    // (check_ref), h_flags[2K] the device loop's iteration count (st.iterations == -1).
+    bool check_ref = false;
+    long long loop_nodes = 0;
     std::map<std::tuple<int, int, int>, std::pair<cudaGraphExec_t, long long>> graphs;
 
     ~Solver() {
@@ -1034,6 +1038,19 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
 }
 
 // Before a first tail: p = 0 and rz = 1, so beta is finite and p becomes z.
+// Per-column start of a PCG solve: a zero right-hand side column starts (and stays) frozen at
+// iteration 0, so the loop never waits on it; the host reports it after the solve.
+__global__ void start_columns_kernel(const double* __restrict__ ref_sq, int K, int max_iters, int* __restrict__ frozen,
+                                     int* __restrict__ conv_iter, double* __restrict__ rel) {
+    const int c = threadIdx.x;
+    if (c < K) {
+        const bool live = ref_sq[c] > 0.0;
+        frozen[c] = live ? 0 : 1;
+        conv_iter[c] = live ? max_iters : 0;
+        rel[c] = 0.0;
+    }
+}
+
 __global__ void fill_kernel(double* v, int n, double x) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) v[i] = x;
@@ -1099,16 +1116,10 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
         X.zero(s);
         CUNIBS_CHECK(cudaMemcpyAsync(R.get(), B.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
-    frozen.zero(s);
     iter_counter.zero(s);
     P.zero(s);
-    CUNIBS_CHECK(cudaMemcpyAsync(h_dbl, ref_sq.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
-    CUNIBS_CHECK(cudaStreamSynchronize(s));
-    for (int c = 0; c < k; ++c)
-        if (!(h_dbl[c] > 0.0)) fail(kEInval, "zero right-hand side column " + std::to_string(c));
-    std::vector<int> init_iters(K, prm.max_iters);
-    CUNIBS_CHECK(cudaMemcpyAsync(conv_iter.get(), init_iters.data(), sizeof(int) * K, cudaMemcpyHostToDevice, s));
-    rel.zero(s);
+    start_columns_kernel<<<1, 32, 0, s>>>(ref_sq.get(), K, prm.max_iters, frozen.get(), conv_iter.get(), rel.get());
+    count_launch();
     fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
     count_launch();
     if constexpr (narrow) {
@@ -1124,13 +1135,18 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
         pcg_iteration<double, TZ, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(), rv,
                                      zv, prm.tolerance, nullptr, ref_sq.get(), 1, hnd, 1);
     }, &nodes);
+    // The right-hand side norms (zero columns) and, after a device loop, its iteration count are
+    // read with the caller's final readback: no host round trip of their own.
+    CUNIBS_CHECK(cudaMemcpyAsync(h_dbl + 2 * K, ref_sq.get(), sizeof(double) * K, cudaMemcpyDeviceToHost, s));
+    check_ref = true;
     if (device_loop) {
-        CUNIBS_CHECK(cudaMemcpyAsync(h_flags, iter_counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
-        CUNIBS_CHECK(cudaStreamSynchronize(s));
-        it = h_flags[0];
-        count_launch(nodes * it);
+        CUNIBS_CHECK(cudaMemcpyAsync(h_flags + 2 * K, iter_counter.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+        loop_nodes = nodes;
+        st.iterations = -1;
+        st.outer_steps = 1;
+        return;
     }
-    while (!device_loop && it < prm.max_iters) {
+    while (it < prm.max_iters) {
         const int m = std::min(prm.iters_per_sync, prm.max_iters - it);
         for (int j = 0; j < m; ++j) {
             run_graph({key + 10, K, 0}, [&] {
@@ -1241,7 +1257,10 @@ SolverPtr make_solver(const Hierarchy& h, const Params& p) {
     // device-side WHILE node, for profilers that do not step into conditional graph bodies.
     const char* host_loop = std::getenv("CUNIBS_SOLVER_HOST_LOOP");
     sv->while_unsupported = host_loop != nullptr && host_loop[0] == '1';
-    CUNIBS_CHECK(cudaStreamCreateWithFlags(&sv->stream, cudaStreamNonBlocking));
+    // The solver's kernels go at the highest stream priority: block preparation may run beside them.
+    int least = 0, greatest = 0;
+    CUNIBS_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    CUNIBS_CHECK(cudaStreamCreateWithPriority(&sv->stream, cudaStreamNonBlocking, greatest));
     return sv;
 }
 
@@ -1263,6 +1282,7 @@ void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, con
     dispatch_k(K, [&](auto kc) {
         constexpr int KK = decltype(kc)::value;
         sv.ensure(KK);
+        sv.check_ref = false;
         // Join the caller's stream.
         cudaEvent_t ev;
         CUNIBS_CHECK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -1275,13 +1295,9 @@ void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, con
         if (prm.precision == kMixed) sv.solve_mixed<KK>(k, prm, st, X0 != nullptr);
         else if (prm.precision == kFp64CgFp32Mg) sv.solve_plain<KK, float>(k, prm, st, X0 != nullptr);
         else sv.solve_plain<KK, double>(k, prm, st, X0 != nullptr);
-        if (X0) {
-            double h_init[16];
-            CUNIBS_CHECK(cudaMemcpyAsync(h_init, sv.init_rel.get(), sizeof(double) * KK, cudaMemcpyDeviceToHost,
-                                         sv.stream));
-            CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
-            st.col_init_rel.assign(h_init, h_init + k);
-        }
+        if (X0)
+            CUNIBS_CHECK(cudaMemcpyAsync(sv.h_dbl + 3 * KK, sv.init_rel.get(), sizeof(double) * KK,
+                                         cudaMemcpyDeviceToHost, sv.stream));
         CUNIBS_CHECK(cudaMemcpyAsync(Xout, sv.X.get(), nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
         CUNIBS_CHECK(cudaMemcpyAsync(sv.h_flags, sv.conv_iter.get(), sizeof(int) * KK, cudaMemcpyDeviceToHost, sv.stream));
         CUNIBS_CHECK(cudaMemcpyAsync(sv.h_dbl, sv.rel.get(), sizeof(double) * KK, cudaMemcpyDeviceToHost, sv.stream));
@@ -1291,6 +1307,16 @@ void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, con
         cudaEventDestroy(ev);
         st.col_iters.assign(sv.h_flags, sv.h_flags + k);
         st.col_rel.assign(sv.h_dbl, sv.h_dbl + k);
+        if (X0) st.col_init_rel.assign(sv.h_dbl + 3 * KK, sv.h_dbl + 3 * KK + k);
+        if (st.iterations < 0) {
+            st.iterations = sv.h_flags[2 * KK];
+            count_launch(sv.loop_nodes * st.iterations);
+        }
+        if (sv.check_ref) {
+            sv.check_ref = false;
+            for (int c = 0; c < k; ++c)
+                if (!(sv.h_dbl[2 * KK + c] > 0.0)) fail(kEInval, "zero right-hand side column " + std::to_string(c));
+        }
     });
 }
 

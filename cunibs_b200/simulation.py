@@ -2,6 +2,8 @@
 
 from __future__ import annotations
 
+from collections import deque
+
 from dataclasses import dataclass
 
 import numpy as np
@@ -189,41 +191,61 @@ class Subject:
         slot_node, slot_tag = self._host_slot_maps(recovery) if retain.nodal else (None, None)
         # Per-node slots need the connectivity to say which nodes a region touches.
         tet_nodes = self._host_tet_nodes() if retain.nodal and slot_tag is None else None
-        for start in range(0, len(sites), chunk_k):
-            chunk = sites[start : start + chunk_k]
+        chunks = [sites[i : i + chunk_k] for i in range(0, len(sites), chunk_k)]
+
+        def submit(chunk: Sequence[Placement]) -> int:
             centers = np.stack([s.center_mm for s in chunk])
             handles = np.stack([s.handle_mm for s in chunk])
             dists = np.array([s.distance_mm for s in chunk])
-            try:
-                with self._lock:
-                    out = ctx.solve_block(coil, centers, handles, dists, didt, magnitude=retain.magnitude,
-                                          vectors=retain.vectors, potential=retain.potential, recovery=recovery,
-                                          nodal=retain.nodal)
-            except _native.ConvergenceFailure as exc:
-                raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
-            host = self._host_metric_inputs() if (retain.magnitude or retain.nodal) else None
-            for i, site in enumerate(chunk):
-                yield FieldResult(
-                    summary=metrics.from_summary_row(out["summary"][i]),
-                    magnE=out["magnE"][i] if retain.magnitude else None,
-                    E=out["E"][i] if retain.vectors else None,
-                    v=out["v"][i] if retain.potential else None,
-                    transform=out["transform"][i],
-                    placement=site,
-                    coil_name=coil.name,
-                    didt=float(didt),
-                    vols=host[0] if host else None,
-                    tet_tags=host[1] if host else None,
-                    barycenters_mm=host[2] if host else None,
-                    recovery=recovery,
-                    iterations=int(out["iterations"][i]),
-                    relative_residual=float(out["relative_residual"][i]),
-                    n_nodes=ctx.n_nodes if retain.nodal else None,
-                    E_slots=out["E_slots"][i] if retain.nodal else None,
-                    slot_node=slot_node,
-                    slot_tag=slot_tag,
-                    tet_nodes=tet_nodes,
-                )
+            with self._lock:
+                return ctx.submit_block(coil, centers, handles, dists, didt, magnitude=retain.magnitude,
+                                        vectors=retain.vectors, potential=retain.potential, recovery=recovery,
+                                        nodal=retain.nodal)
+
+        # Blocks go through the context two deep: the next block's coil placement, dA/dt and
+        # right-hand side are prepared on the GPU beside this block's solve.
+        tickets: deque[int] = deque()
+        try:
+            if chunks:
+                tickets.append(submit(chunks[0]))
+            for b, chunk in enumerate(chunks):
+                if b + 1 < len(chunks):
+                    tickets.append(submit(chunks[b + 1]))
+                ticket = tickets.popleft()
+                try:
+                    with self._lock:
+                        out = ctx.finish_block(ticket)
+                except _native.ConvergenceFailure as exc:
+                    raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
+                host = self._host_metric_inputs() if (retain.magnitude or retain.nodal) else None
+                for i, site in enumerate(chunk):
+                    yield FieldResult(
+                        summary=metrics.from_summary_row(out["summary"][i]),
+                        magnE=out["magnE"][i] if retain.magnitude else None,
+                        E=out["E"][i] if retain.vectors else None,
+                        v=out["v"][i] if retain.potential else None,
+                        transform=out["transform"][i],
+                        placement=site,
+                        coil_name=coil.name,
+                        didt=float(didt),
+                        vols=host[0] if host else None,
+                        tet_tags=host[1] if host else None,
+                        barycenters_mm=host[2] if host else None,
+                        recovery=recovery,
+                        iterations=int(out["iterations"][i]),
+                        relative_residual=float(out["relative_residual"][i]),
+                        n_nodes=ctx.n_nodes if retain.nodal else None,
+                        E_slots=out["E_slots"][i] if retain.nodal else None,
+                        slot_node=slot_node,
+                        slot_tag=slot_tag,
+                        tet_nodes=tet_nodes,
+                    )
+        finally:
+            # A consumer that stops early (or an error) leaves submitted blocks: drop them.
+            with self._lock:
+                for ticket in tickets:
+                    if self._ctx is ctx:
+                        ctx.cancel_block(ticket)
 
     def iter_simulate(self, coil: Coil, placements: Sequence[Placement], didt: float = 1e6, *,
                       magnitude: bool = False, vectors: bool = False, potential: bool = False,

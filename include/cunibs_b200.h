@@ -159,6 +159,32 @@ int cunibs_solve_block_device(cunibs_context* ctx, const double* dip_pos_m, cons
                               const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
                               double didt, const cunibs_solve_opts* opts, cunibs_block_out* out);
 
+/* Two-stage form of the block solve, for a sequence of blocks (the block loop of
+ * Subject.iter_simulate, simulation.py:473-546). A submit prepares a block (coil placement, dA/dt,
+ * right-hand side) on the context's preparation stream and returns a ticket without waiting for
+ * the work; the finish of that ticket solves the block and writes its outputs exactly as the
+ * one-call entry does (same out fields, same host or device placement). At most two blocks are
+ * submitted and not finished; a block submitted while another waits to be finished is prepared
+ * beside that block's solve on the same GPU (its dA/dt kernel then takes a bounded grid,
+ * cunibs_context_set_overlap). Host inputs are copied at submit; device inputs must stay valid
+ * until their block is finished. Errors of a block (a degenerate placement, no convergence) are
+ * returned by its finish call; the block is dropped either way. Results are bitwise those of the
+ * one-call entries, which may be called while one block is submitted. */
+int cunibs_submit_block(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                        const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
+                        double didt, const cunibs_solve_opts* opts, long long* ticket);
+int cunibs_finish_block(cunibs_context* ctx, long long ticket, cunibs_block_out* out);
+int cunibs_submit_block_device(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                               const double* centers_mm, const double* handles_mm, const double* dists_mm, int k,
+                               double didt, const cunibs_solve_opts* opts, long long* ticket);
+int cunibs_finish_block_device(cunibs_context* ctx, long long ticket, cunibs_block_out* out);
+/* Drops a submitted block without solving it (a consumer that stops early). */
+int cunibs_cancel_block(cunibs_context* ctx, long long ticket);
+/* Number of submitted blocks not yet finished (0, 1 or 2). */
+int cunibs_context_pending(const cunibs_context* ctx, int* n);
+/* Blocks per SM the dA/dt kernel takes while another block's solve may run beside it (default 2). */
+int cunibs_context_set_overlap(cunibs_context* ctx, int blocks_per_sm);
+
 /* Re-assembles the stiffness with a new conductivity per tissue tag (sigma_by_tag[0..10], S/m;
  * index = tag) and rebuilds the AMG hierarchy: the per-sample step of a conductivity Monte Carlo
  * (uq/conductivity/run.py:324-361). */
