@@ -77,15 +77,18 @@ __device__ __forceinline__ void final_reduce(const double* __restrict__ partials
     __syncthreads();
 }
 
-// acc + sum of val[p] * x[col[p] * ld + c] over p = p0, p0 + S, ... < e, added in that order. The
-// row is taken eight terms at a time: every index and value load of a batch is issued, then every
-// gather, then the multiply-adds in order (predicated off past the row's end), so a lane has eight
-// index-then-gather chains in flight and a typical row of the finest operator (about 15 entries)
-// costs two rounds of memory latency. The additions, and so the result, keep the plain loop's order.
+// acc + sum of val[p] * x[col[p] * ld + c] over p = p0, p0 + S, ... < e, added in that order.
+// Operators walked by sub-lanes (S > 1, the coarse levels' long rows) take their terms eight at a
+// time: every index and value load of a batch is issued, then every gather, then the multiply-adds
+// in order (predicated off past the row's end). One lane per row (S = 1, the finest levels) takes
+// the plain loop: measured on the 1M-tet operator (178k rows, ~15 entries per row, 8 columns) the
+// batches of 4, 8, 12 and 16 cost registers and occupancy for more than the chains they put in
+// flight (PCG iteration 0.266 ms at 8, 0.247 ms plain). Both keep the plain loop's order of
+// additions, so the result does not depend on the batch.
 template <typename T, int S>
 __device__ __forceinline__ T strided_dot(const int* __restrict__ col, const T* __restrict__ val,
                                          const T* __restrict__ x, int p, int e, long ld, int c, T acc) {
-    constexpr int B = 8;
+    constexpr int B = S == 1 ? 1 : 8;
     for (; p < e; p += B * S) {
         int cj[B];
         T vj[B], xj[B];
