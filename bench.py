@@ -146,7 +146,8 @@ def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float
     vb = vx = 8 if precision == "plain" else 4
     kb = kx = 4 if precision == "mixed" else 8
     sizes = ctx.levels()
-    L = ctx.n_levels
+    L = ctx.vcycle_levels  # levels the V-cycle smooths; the one below is solved densely
+    sizes = list(sizes[:L]) + [ctx.bottom_rows]
     deg = 2
     total = 0.0
     for lev in range(L):
@@ -163,7 +164,7 @@ def solve_bytes_per_iteration(ctx, K: int, precision: str) -> tuple[float, float
             total += 4 * nc + vx * K * nc
         total += pnnz * (vb + 4) + 4 * (n + 1) + vx * K * (nc + 2 * n)
         total += deg * cheb
-    nc = ctx.coarse_rows
+    nc = ctx.bottom_rows
     total += vb * nc * nc + 2 * vx * K * nc
     n0 = sizes[0]
     nnz0 = ctx.array("a_col", 0).shape[0] if L > 0 else 0

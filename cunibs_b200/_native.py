@@ -36,6 +36,7 @@ class Params(C.Structure):
         ("inner_reduction", C.c_double),
         ("inner_max_iters", C.c_int),
         ("iters_per_sync", C.c_int),
+        ("dense_max_rows", C.c_int),
     ]
 
 
@@ -49,6 +50,8 @@ class Info(C.Structure):
         ("ground_node", C.c_int),
         ("n_levels", C.c_int),
         ("coarse_rows", C.c_int),
+        ("vcycle_levels", C.c_int),
+        ("bottom_rows", C.c_int),
     ]
 
 
@@ -236,6 +239,8 @@ class Context:
         self.ground_node = info.ground_node
         self.n_levels = info.n_levels
         self.coarse_rows = info.coarse_rows
+        self.vcycle_levels = info.vcycle_levels
+        self.bottom_rows = info.bottom_rows
 
     def close(self) -> None:
         h = getattr(self, "_h", None)

@@ -477,6 +477,7 @@ int cunibs_params_default(cunibs_params* out) {
         out->inner_reduction = p.inner_reduction;
         out->inner_max_iters = p.inner_max_iters;
         out->iters_per_sync = p.iters_per_sync;
+        out->dense_max_rows = p.dense_max_rows;
     });
 }
 
@@ -504,6 +505,8 @@ int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_no
         c->prm.inner_reduction = p.inner_reduction;
         c->prm.inner_max_iters = p.inner_max_iters;
         c->prm.iters_per_sync = p.iters_per_sync > 0 ? p.iters_per_sync : 4;
+        require(p.dense_max_rows >= 0 && p.dense_max_rows <= 4096, "dense_max_rows must be in [0, 4096]");
+        c->prm.dense_max_rows = p.dense_max_rows;
         require(c->prm.tolerance > 0 && c->prm.max_iters > 0, "tolerance and max_iters must be positive");
         int least = 0, greatest = 0;
         CUNIBS_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
@@ -546,6 +549,8 @@ int cunibs_context_info(const cunibs_context* c, cunibs_info* out) {
         out->ground_node = c->mesh.ground;
         out->n_levels = static_cast<int>(c->hier.levels.size());
         out->coarse_rows = c->hier.nc;
+        out->vcycle_levels = c->hier.vcycle_levels;
+        out->bottom_rows = c->hier.bottom_n;
     });
 }
 

@@ -33,6 +33,8 @@ struct Params {
     double inner_reduction = 1e-4;  // deepest residual reduction asked of one inner FP32 solve
     int inner_max_iters = 60;
     int iters_per_sync = 4;         // PCG iterations launched between host convergence checks
+    int dense_max_rows = 1024;      // the V-cycle ends in an exact dense solve at the first level
+                                    // below the finest with at most this many rows (0: at the coarsest)
 };
 
 struct Cheby {
@@ -73,6 +75,13 @@ struct Hierarchy {
     int nc = 0;
     DevArray<double> coarse_inv;   // dense (nc, nc), FP64 from a Cholesky factorisation
     DevArray<float> coarse_inv32;
+    // Where the V-cycle stops: it smooths levels [0, vcycle_levels) and solves the operator below
+    // them exactly with the dense inverse bottom_inv (bottom_n rows): levels[vcycle_levels].a, or
+    // the coarsest operator when vcycle_levels == levels.size() (then bottom_inv is coarse_inv).
+    int vcycle_levels = 0;
+    int bottom_n = 0;
+    DevArray<double> level_inv;    // dense inverse of levels[vcycle_levels].a when the V-cycle stops early
+    DevArray<float> level_inv32;
     std::vector<int> sizes;
     Cheby cheby;
 };

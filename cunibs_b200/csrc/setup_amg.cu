@@ -658,6 +658,24 @@ Cheby make_cheby(int degree, double lower_ratio) {
     return c;
 }
 
+// inv (and its FP32 copy) = the dense inverse of the SPD operator a, through a Cholesky factorisation.
+static void dense_inverse(const DevCsr<double>& a, DevArray<double>& inv, DevArray<float>& inv32, const char* what,
+                   cudaStream_t s) {
+    const int n = a.n;
+    DevArray<double> dense(static_cast<std::size_t>(n) * n), y(static_cast<std::size_t>(n) * n);
+    dense.zero(s);
+    densify_kernel<<<grid_for(n), kBlock, 0, s>>>(a.ptr.get(), a.col.get(), a.val.get(), n, dense.get());
+    count_launch();
+    DevArray<int> status(1);
+    cholesky_kernel<<<1, 1024, 0, s>>>(dense.get(), n, status.get()); count_launch();
+    if (read_scalar(status.get(), s)) fail(kEInternal, std::string(what) + " is not positive definite");
+    inv.resize(static_cast<std::size_t>(n) * n);
+    cholesky_inverse_kernel<<<grid_for(n, 64), 64, 0, s>>>(dense.get(), n, y.get(), inv.get()); count_launch();
+    to_f32(inv, static_cast<long>(n) * n, inv32, s);
+    CUNIBS_LAUNCH_CHECK("dense inverse");
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+}
+
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& prm, cudaStream_t s) {
     h.levels.clear();
     h.sizes.assign(1, a0.n);
@@ -698,18 +716,20 @@ void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& prm, cudaSt
     }
     h.nc = a.n;
     h.coarse = std::move(a);
-    const int nc = h.nc;
-    DevArray<double> dense(static_cast<std::size_t>(nc) * nc), y(static_cast<std::size_t>(nc) * nc);
-    dense.zero(s);
-    densify_kernel<<<grid_for(nc), kBlock, 0, s>>>(h.coarse.ptr.get(), h.coarse.col.get(), h.coarse.val.get(), nc,
-                                                   dense.get()); count_launch();
-    DevArray<int> status(1);
-    cholesky_kernel<<<1, 1024, 0, s>>>(dense.get(), nc, status.get()); count_launch();
-    if (read_scalar(status.get(), s)) fail(kEInternal, "coarsest AMG operator is not positive definite");
-    h.coarse_inv.resize(static_cast<std::size_t>(nc) * nc);
-    cholesky_inverse_kernel<<<grid_for(nc, 64), 64, 0, s>>>(dense.get(), nc, y.get(), h.coarse_inv.get()); count_launch();
-    to_f32(h.coarse_inv, static_cast<long>(nc) * nc, h.coarse_inv32, s);
-    CUNIBS_LAUNCH_CHECK("coarse inverse");
+    dense_inverse(h.coarse, h.coarse_inv, h.coarse_inv32, "coarsest AMG operator", s);
+    // The V-cycle's bottom: the first level below the finest small enough for a dense solve. Its
+    // exact inverse replaces the smoothing, restriction and prolongation of every level under it
+    // (a few latency-bound launches each per V-cycle) with one dense product.
+    h.vcycle_levels = static_cast<int>(h.levels.size());
+    h.bottom_n = h.nc;
+    for (int l = 1; l < static_cast<int>(h.levels.size()); ++l) {
+        if (prm.dense_max_rows > 0 && h.levels[l].n <= prm.dense_max_rows) {
+            h.vcycle_levels = l;
+            h.bottom_n = h.levels[l].n;
+            dense_inverse(h.levels[l].a, h.level_inv, h.level_inv32, "AMG level operator", s);
+            break;
+        }
+    }
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 

@@ -716,7 +716,7 @@ class Solver {
                 v64.b[l].resize(m);
             }
         }
-        const std::size_t mc = static_cast<std::size_t>(h->nc) * K;
+        const std::size_t mc = static_cast<std::size_t>(h->bottom_n) * K;
         v32.cb.resize(mc);
         v32.cx.resize(mc);
         v64.cb.resize(mc);
@@ -908,10 +908,15 @@ template <>
 const float* Solver::rval<float>(int l) const { return h->levels[l].r32.get(); }
 template <>
 const double* Solver::rval<double>(int l) const { return h->levels[l].r.val.get(); }
+// The dense inverse at the V-cycle's bottom (see Hierarchy::vcycle_levels).
 template <>
-const float* Solver::cinv<float>() const { return h->coarse_inv32.get(); }
+const float* Solver::cinv<float>() const {
+    return h->vcycle_levels < static_cast<int>(h->levels.size()) ? h->level_inv32.get() : h->coarse_inv32.get();
+}
 template <>
-const double* Solver::cinv<double>() const { return h->coarse_inv.get(); }
+const double* Solver::cinv<double>() const {
+    return h->vcycle_levels < static_cast<int>(h->levels.size()) ? h->level_inv.get() : h->coarse_inv.get();
+}
 template <>
 VWork<float>& Solver::vw<float>() { return v32; }
 template <>
@@ -921,12 +926,13 @@ template <typename T, int K>
 bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     const Hierarchy& H = *h;
     const Cheby& ch = H.cheby;
-    const int L = static_cast<int>(H.levels.size());
+    const int L = H.vcycle_levels;
+    const int n_bottom = H.bottom_n;
     VWork<T>& w = vw<T>();
     constexpr int TT = tile_threads<K>();
     cudaStream_t s = stream;
     if (L == 0) {
-        coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(), b, z); count_launch();
+        coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(n_bottom) * kWarp), kBlock, 0, s>>>(n_bottom, cinv<T>(), b, z); count_launch();
         return false;
     }
     const bool fuse_dot = dot && H.levels[0].tpr_a <= 16;
@@ -1019,8 +1025,9 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         });
         count_launch();
     }
-    coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(H.nc) * kWarp), kBlock, 0, s>>>(H.nc, cinv<T>(),
-                                                                                                 w.cb.get(), w.cx.get()); count_launch();
+    coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(n_bottom) * kWarp), kBlock, 0, s>>>(
+        n_bottom, cinv<T>(), w.cb.get(), w.cx.get());
+    count_launch();
     // Up-sweep.
     const T* xc = w.cx.get();
     for (int l = L - 1; l >= 0; --l) {

@@ -73,6 +73,9 @@ typedef struct {
     double inner_reduction;   /* mixed: deepest residual reduction asked of one inner FP32 solve */
     int inner_max_iters;      /* mixed: iteration cap of each inner FP32 solve */
     int iters_per_sync;       /* PCG iterations launched between host convergence checks */
+    int dense_max_rows;       /* the V-cycle ends in an exact dense solve at the first level below the
+                                 finest with at most this many rows (default 1024); 0: at the coarsest
+                                 level, as the reference's V-cycle does (vcycle.cu:420-663) */
 } cunibs_params;
 
 typedef struct {
@@ -84,6 +87,9 @@ typedef struct {
     int ground_node; /* in the context's (Morton) node order */
     int n_levels;    /* AMG levels above the dense coarse solve */
     int coarse_rows;
+    int vcycle_levels; /* levels the V-cycle smooths; the level below them (or the coarsest) is solved
+                          exactly (cunibs_params.dense_max_rows) */
+    int bottom_rows;   /* rows of that exactly solved operator */
 } cunibs_info;
 
 /* Per-call options of a block solve. Zero-initialise for the context defaults. */

@@ -77,15 +77,44 @@ def test_select_size4_bit_exact_on_level_operators(patch_pair):
     np.testing.assert_array_equal(agg_g, agg_o)
 
 
+@pytest.fixture(scope="module")
+def sphere_ref_cycle(sphere_mesh):
+    """A context whose V-cycle descends to the coarsest level, as the reference's does."""
+    m = sphere_mesh
+    p = _native.default_params()
+    p.dense_max_rows = 0
+    ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris, p)
+    yield ctx
+    ctx.close()
+
+
 @pytest.mark.parametrize("fp32,tol", [(False, 1e-11), (True, 2e-5)])
-def test_vcycle_matches_oracle(sphere_pair, fp32, tol):
-    ctx, orc = sphere_pair
+def test_vcycle_matches_oracle(sphere_ref_cycle, sphere_pair, fp32, tol):
+    ctx, orc = sphere_ref_cycle, sphere_pair[1]
+    assert ctx.vcycle_levels == ctx.n_levels and ctx.bottom_rows == ctx.coarse_rows
     rng = np.random.default_rng(0)
     r = rng.standard_normal((ctx.n_nodes - 1, 4))
     z_g = ctx.vcycle(r, fp32=fp32)
     z_o = orc.vcycle(r)
     for c in range(4):
         assert np.linalg.norm(z_g[:, c] - z_o[:, c]) / np.linalg.norm(z_o[:, c]) <= tol
+
+
+def test_dense_bottom_vcycle_is_a_symmetric_preconditioner(sphere_pair, sphere_ref_cycle):
+    """The default V-cycle stops at the first level below the finest with at most 1024 rows and
+    solves it exactly: the preconditioner stays symmetric positive definite (FP64), and PCG with it
+    needs no more iterations than with the full descent."""
+    ctx = sphere_pair[0]
+    assert 1 <= ctx.vcycle_levels < ctx.n_levels and ctx.bottom_rows <= 1024
+    rng = np.random.default_rng(3)
+    r = rng.standard_normal((ctx.n_nodes - 1, 2))
+    z = ctx.vcycle(r)
+    assert abs(r[:, 0] @ z[:, 1] - r[:, 1] @ z[:, 0]) <= 1e-10 * abs(r[:, 0] @ z[:, 1])
+    assert (np.einsum("ij,ij->j", r, z) > 0).all()
+    B = rng.standard_normal((ctx.n_nodes - 1, 4))
+    _, it_dense, rel = ctx.solve(B, 4, 4, tolerance=1e-10, max_iters=500)
+    _, it_full, _ = sphere_ref_cycle.solve(B, 4, 4, tolerance=1e-10, max_iters=500)
+    assert (rel <= 1e-10).all() and (it_dense <= it_full).all()
 
 
 def test_placement_matches_oracle(patch_pair, patch_placement):
