@@ -264,7 +264,7 @@ def _operator(ctx: _native.Context):
 def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: int = 512, hidden: int = 512,
                      depth: int = 4, epochs: int = 400, batch: int = 256, lr: float = 1e-3, seed: int = 0,
                      tolerance: float = 1e-8, z_min_mm: float = 40.0, radius_mm: float = 90.0,
-                     install: bool = True) -> WarmStartModel:
+                     install: bool = True, energy: bool = False) -> WarmStartModel:
     """Generate training solves, build the basis, train the network on the GPU and (optionally)
     install it in the context. Returns the model with timing and loss statistics."""
     torch = _torch()
@@ -286,6 +286,12 @@ def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: i
     Gal = V.T @ AV
     # Galerkin coefficients (V^T A V)^-1 V^T b with b = A x: V^T A x = (A V)^T x, A symmetric.
     coef = torch.linalg.solve(Gal, AV.T @ X.T).T.contiguous()  # [n_train, r]
+    if energy:
+        # A-orthonormal basis W = V L^-T (V^T A V = L L^T): the Galerkin coefficients are then
+        # W^T b, and their Euclidean error is the guess's A-norm error, the norm PCG converges in.
+        L = torch.linalg.cholesky(Gal)
+        V = torch.linalg.solve_triangular(L, V.T, upper=False).T.contiguous()
+        coef = (coef @ L).contiguous()  # V c = W L^T c, so the W-coefficients are L^T c
     del G, AV
     r = rank
     r_pad = (r + 63) // 64 * 64
