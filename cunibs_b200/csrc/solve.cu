@@ -85,13 +85,14 @@ __device__ __forceinline__ void final_reduce(const double* __restrict__ partials
 // batches of 4, 8, 12 and 16 cost registers and occupancy for more than the chains they put in
 // flight (PCG iteration 0.266 ms at 8, 0.247 ms plain). Both keep the plain loop's order of
 // additions, so the result does not depend on the batch.
-template <typename T, int S>
+template <typename T, int S, typename TX = T>
 __device__ __forceinline__ T strided_dot(const int* __restrict__ col, const T* __restrict__ val,
-                                         const T* __restrict__ x, int p, int e, long ld, int c, T acc) {
+                                         const TX* __restrict__ x, int p, int e, long ld, int c, T acc) {
     constexpr int B = S == 1 ? 1 : 8;
     for (; p < e; p += B * S) {
         int cj[B];
-        T vj[B], xj[B];
+        T vj[B];
+        TX xj[B];
 #pragma unroll
         for (int j = 0; j < B; ++j) {
             const int q = p + j * S;
@@ -100,10 +101,10 @@ __device__ __forceinline__ T strided_dot(const int* __restrict__ col, const T* _
             vj[j] = ok ? val[q] : T(0);
         }
 #pragma unroll
-        for (int j = 0; j < B; ++j) xj[j] = (p + j * S < e) ? x[cj[j] * ld + c] : T(0);
+        for (int j = 0; j < B; ++j) xj[j] = (p + j * S < e) ? x[cj[j] * ld + c] : TX(0);
 #pragma unroll
         for (int j = 0; j < B; ++j)
-            if (p + j * S < e) acc += vj[j] * xj[j];
+            if (p + j * S < e) acc += vj[j] * static_cast<T>(xj[j]);
     }
     return acc;
 }
@@ -151,12 +152,12 @@ struct RowSlot {
 // the same total, since each pair adds the same two values and addition is commutative), otherwise
 // by sub-lane 0 in shared memory. The tree depends on TPR alone, never on K. Every thread of the
 // block must call this.
-template <typename T, int K, int TPR, int ROWS>
+template <typename T, int K, int TPR, int ROWS, typename TX = T>
 __device__ __forceinline__ T group_row_dot(const int* __restrict__ ptr, const int* __restrict__ col,
-                                           const T* __restrict__ val, const T* __restrict__ x, int row, int r,
+                                           const T* __restrict__ val, const TX* __restrict__ x, int row, int r,
                                            int sub, int c, bool valid) {
     T acc = T(0);
-    if (valid) acc = strided_dot<T, TPR>(col, val, x, ptr[row] + sub, ptr[row + 1], K, c, acc);
+    if (valid) acc = strided_dot<T, TPR, TX>(col, val, x, ptr[row] + sub, ptr[row + 1], K, c, acc);
     if constexpr (TPR == 1) {
         return acc;
     } else if constexpr (TPR * K <= kWarp) {
@@ -286,25 +287,39 @@ unsigned group_grid(int n) {
 
 // x = Ainv b for the dense coarsest operator: a warp per row, lanes striding the row, a fixed
 // shuffle tree per column.
+// x = inv b for the dense bottom of the V-cycle: one block of kGemvThreads per row, each thread a
+// strided share of the row, warp sums then a fixed-order sum over the warps (deterministic, and
+// independent of K per column).
+constexpr int kGemvThreads = 128;
+
 template <typename T, int K>
-__global__ void coarse_gemv_kernel(int nc, const T* __restrict__ inv, const T* __restrict__ b, T* __restrict__ x) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / kWarp;
-    const int lane = threadIdx.x % kWarp;
+__global__ void __launch_bounds__(kGemvThreads) coarse_gemv_kernel(int nc, const T* __restrict__ inv,
+                                                                  const T* __restrict__ b, T* __restrict__ x) {
+    __shared__ T part[kGemvThreads / kWarp][K];
+    const int row = blockIdx.x;
     T acc[K];
 #pragma unroll
     for (int c = 0; c < K; ++c) acc[c] = T(0);
-    if (row < nc) {
-        for (int j = lane; j < nc; j += kWarp) {
-            const T a = inv[static_cast<long>(row) * nc + j];
+    const T* r = inv + static_cast<long>(row) * nc;
+#pragma unroll 4
+    for (int j = threadIdx.x; j < nc; j += kGemvThreads) {
+        const T a = r[j];
 #pragma unroll
-            for (int c = 0; c < K; ++c) acc[c] += a * b[static_cast<long>(j) * K + c];
-        }
+        for (int c = 0; c < K; ++c) acc[c] += a * b[static_cast<long>(j) * K + c];
     }
 #pragma unroll
     for (int c = 0; c < K; ++c) acc[c] = group_sum<kWarp>(acc[c]);
-    if (row < nc && lane == 0) {
+    const int warp = threadIdx.x / kWarp;
+    if (threadIdx.x % kWarp == 0) {
 #pragma unroll
-        for (int c = 0; c < K; ++c) x[static_cast<long>(row) * K + c] = acc[c];
+        for (int c = 0; c < K; ++c) part[warp][c] = acc[c];
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+        T v = part[0][threadIdx.x];
+#pragma unroll
+        for (int w = 1; w < kGemvThreads / kWarp; ++w) v += part[w][threadIdx.x];
+        x[static_cast<long>(row) * K + threadIdx.x] = v;
     }
 }
 
@@ -359,26 +374,38 @@ __global__ void __launch_bounds__(tile_threads<K>()) norm2_kernel(int n, const T
     }
 }
 
-// Ap = A p; pAp per column; alpha = rz / pAp (0 on a frozen column).
-template <typename T, int K, int TPR>
+// The search direction and its product, fused: p = z + beta p and Ap = A z + beta Ap (the product
+// carried by its recurrence, so the SpMV gathers the V-cycle's output z, FP32 under an FP32
+// V-cycle, instead of the FP64 direction), then pAp per column and alpha = rz / pAp. Columns frozen
+// before this iteration keep p and Ap; alpha is 0 on every frozen column.
+template <typename T, typename TZ, int K, int TPR>
 __global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
-    const T* __restrict__ p, T* __restrict__ ap, double* partials, unsigned* counter, const double* __restrict__ rz,
-    const int* __restrict__ frozen, double* __restrict__ alpha) {
+    const TZ* __restrict__ z, T* __restrict__ p, T* __restrict__ ap, double* partials, unsigned* counter,
+    const double* __restrict__ rz, const double* __restrict__ beta, const int* __restrict__ frozen,
+    double* __restrict__ alpha) {
     constexpr int ROWS = ReduceTile<TPR>::kRows;
     const int r = threadIdx.x / (TPR * K);
     const int sub = (threadIdx.x / K) % TPR;
     const int c = threadIdx.x % K;
     const int tiles = (n + ROWS - 1) / ROWS;
+    const bool update = frozen[c] != 1;
+    const T b = static_cast<T>(beta[c]);
     double v = 0.0;
     for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
         const int row = t * ROWS + r;
         const bool valid = row < n;
-        const T s = group_row_dot<T, K, TPR, ROWS>(ptr, col, val, p, row, r, sub, c, valid);
+        const T s = group_row_dot<T, K, TPR, ROWS, TZ>(ptr, col, val, z, row, r, sub, c, valid);
         if (valid && sub == 0) {
             const long q = static_cast<long>(row) * K + c;
-            ap[q] = s;
-            v += static_cast<double>(p[q]) * static_cast<double>(s);
+            T pq = p[q], aq = ap[q];
+            if (update) {
+                pq = static_cast<T>(z[q]) + b * pq;
+                aq = s + b * aq;
+                p[q] = pq;
+                ap[q] = aq;
+            }
+            v += static_cast<double>(pq) * static_cast<double>(aq);
         }
     }
     block_partial<K>(v, partials);
@@ -525,19 +552,6 @@ __global__ void __launch_bounds__(tile_threads<K>()) cheby_dot_kernel(
     }
     block_partial<K>(v, partials);
     if (last_block(counter)) finish_beta<K>(partials, rz, frozen, beta);
-}
-
-// p = z + beta p. A column frozen before this iteration keeps its direction, so a column that met
-// an inner target resumes the same Krylov sequence after the outer step replaces its residual.
-template <typename T, typename TZ, int K>
-__global__ void __launch_bounds__(tile_threads<K>()) update_p_kernel(int n, const double* __restrict__ beta,
-                                                                     const TZ* __restrict__ z, T* __restrict__ p,
-                                                                     const int* __restrict__ frozen) {
-    const int row = blockIdx.x * kTileRows + threadIdx.x / K;
-    const int c = threadIdx.x % K;
-    if (row >= n || frozen[c] == 1) return;
-    const long q = static_cast<long>(row) * K + c;
-    p[q] = static_cast<T>(z[q]) + static_cast<T>(beta[c]) * p[q];
 }
 
 // r_lo = r rounded to the V-cycle's type (the first V-cycle input of FP64 PCG over an FP32 V-cycle).
@@ -760,9 +774,9 @@ class Solver {
         VWork<T>& w = vw<T>();
         return (h->cheby.degree % 2) ? w.x[0].get() : w.r[0].get();
     }
-    // z = M r_v (V-cycle in TZ), beta, p = z + beta p (Krylov vectors in T).
-    template <typename T, typename TZ, int K>
-    void pcg_tail(TZ* r_v, TZ* z, T* p, bool jz_done);
+    // z = M r_v (V-cycle in TZ) and beta; the next iteration's SpMV forms p = z + beta p.
+    template <typename TZ, int K>
+    void pcg_tail(TZ* r_v, TZ* z, bool jz_done);
     // Sub-lanes per row on the finest operator (the PCG's own matrix), capped where the reducing
     // kernels' 64/TPR-row tiles need at least four rows.
     int tpr0() const {
@@ -932,7 +946,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     constexpr int TT = tile_threads<K>();
     cudaStream_t s = stream;
     if (L == 0) {
-        coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(n_bottom) * kWarp), kBlock, 0, s>>>(n_bottom, cinv<T>(), b, z); count_launch();
+        coarse_gemv_kernel<T, K><<<n_bottom, kGemvThreads, 0, s>>>(n_bottom, cinv<T>(), b, z); count_launch();
         return false;
     }
     const bool fuse_dot = dot && H.levels[0].tpr_a <= 16;
@@ -1025,8 +1039,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         });
         count_launch();
     }
-    coarse_gemv_kernel<T, K><<<grid_for(static_cast<std::int64_t>(n_bottom) * kWarp), kBlock, 0, s>>>(
-        n_bottom, cinv<T>(), w.cb.get(), w.cx.get());
+    coarse_gemv_kernel<T, K><<<n_bottom, kGemvThreads, 0, s>>>(n_bottom, cinv<T>(), w.cb.get(), w.cx.get());
     count_launch();
     // Up-sweep.
     const T* xc = w.cx.get();
@@ -1066,8 +1079,8 @@ __global__ void fill_kernel(double* v, int n, double x) {
     if (i < n) v[i] = x;
 }
 
-template <typename T, typename TZ, int K>
-void Solver::pcg_tail(TZ* r_v, TZ* z, T* p, bool jz_done) {
+template <typename TZ, int K>
+void Solver::pcg_tail(TZ* r_v, TZ* z, bool jz_done) {
     constexpr int TT = tile_threads<K>();
     const bool fused = vcycle<TZ, K>(r_v, z, jz_done, true);
     if (!fused) {
@@ -1075,8 +1088,6 @@ void Solver::pcg_tail(TZ* r_v, TZ* z, T* p, bool jz_done) {
                                                                  frozen.get(), beta.get());
         count_launch();
     }
-    update_p_kernel<T, TZ, K><<<n_tiles(n), TT, 0, stream>>>(n, beta.get(), z, p, frozen.get());
-    count_launch();
 }
 
 template <typename T, typename TZ, int K>
@@ -1087,8 +1098,9 @@ void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T
     const unsigned g = reduce_grid(n);
     dispatch_tpr<K>(tpr0(), [&](auto tc) {
         constexpr int TPR = decltype(tc)::value;
-        spmv_alpha_kernel<T, K, TPR><<<reduce_grid_rows<TPR>(n), TT, 0, stream>>>(
-            n, ptr, col, val, p, ap, partials.get(), counter.get(), rz.get(), frozen.get(), alpha.get());
+        spmv_alpha_kernel<T, TZ, K, TPR><<<reduce_grid_rows<TPR>(n), TT, 0, stream>>>(
+            n, ptr, col, val, z, p, ap, partials.get(), counter.get(), rz.get(), beta.get(), frozen.get(),
+            alpha.get());
     });
     count_launch();
     const bool has_levels = !h->levels.empty();
@@ -1098,7 +1110,7 @@ void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T
         conv_iter.get(), rel.get(), record, has_levels ? ldinv<TZ>(0) : nullptr, static_cast<TZ>(h->cheby.alpha0),
         has_levels ? first0<TZ>() : nullptr, narrow ? r_v : nullptr, loop, use_loop, cap.get());
     count_launch();
-    pcg_tail<T, TZ, K>(r_v, z, p, has_levels);
+    pcg_tail<TZ, K>(r_v, z, has_levels);
 }
 
 template <int K, typename TZ>
@@ -1128,6 +1140,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     }
     iter_counter.zero(s);
     P.zero(s);
+    AP.zero(s);  // the first iteration's Ap = A z + beta Ap reads it
     start_columns_kernel<<<1, 32, 0, s>>>(ref_sq.get(), K, prm.max_iters, frozen.get(), conv_iter.get(), rel.get());
     count_launch();
     fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
@@ -1137,7 +1150,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
         narrow_kernel<double, TZ><<<grid_for(count), kBlock, 0, s>>>(count, R.get(), rv);
         count_launch();
     }
-    pcg_tail<double, TZ, K>(rv, zv, P.get(), false);
+    pcg_tail<TZ, K>(rv, zv, false);
     int it = 0;
     set_cap(prm.max_iters);
     long long nodes = 0;
@@ -1217,9 +1230,10 @@ void Solver::solve_mixed(int k, const Params& prm, SolveStats& st, bool warm) {
         // from the true residual for the old direction to stay useful.)
         d32.zero(s);
         p32.zero(s);
+        ap32.zero(s);
         fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
         count_launch();
-        pcg_tail<float, float, K>(r32.get(), z32.get(), p32.get(), false);
+        pcg_tail<float, K>(r32.get(), z32.get(), false);
         int it = 0;
         const int cap_n = std::min(prm.inner_max_iters, prm.max_iters - total_inner);
         set_cap(total_inner + cap_n);
