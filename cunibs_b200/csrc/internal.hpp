@@ -195,7 +195,8 @@ struct SummaryWork {
     DevArray<std::uint64_t> k64, k64_s;
     DevArray<float> keys, keys_s;
     DevArray<int> vals, vals_s, offsets;
-    DevArray<double> w_sorted, cw, tile_tot;
+    DevArray<double> w_sorted, cw, tile_tot, part;
+    DevArray<int> part_i;
     DevArray<unsigned char> temp;
 };
 void gm_summary(const Mesh& m, const float* magnE, int k, double* summary_dev /* (k,16) */, SummaryWork& w,

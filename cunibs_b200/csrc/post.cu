@@ -152,22 +152,27 @@ __device__ double quantile(double q, const float* __restrict__ v, const double* 
     return slope * (q - x0) + static_cast<double>(v[lo]);
 }
 
-// One block per placement: peak/argmax, sums for mean/CoG, then variance; thread 0 finishes the
-// percentiles and focality from the sorted arrays.
-__global__ void summary_kernel(const float* __restrict__ magn, const int* __restrict__ gm, int n_gm, int n_tets,
-                               const float* __restrict__ vols32, const double* __restrict__ bary,
-                               const float* __restrict__ sorted_keys, const double* __restrict__ w_sorted,
-                               const double* __restrict__ cw, double* __restrict__ out) {
-    constexpr int kT = 512;
-    __shared__ double sv[kT], sw[kT], swm[kT], sx[kT], sy[kT], sz[kT];
-    __shared__ int si[kT];
-    __shared__ double mean_sh;
-    const int c = blockIdx.x;
+// Gray-matter summary of each placement (metrics.py:209-243) in three launches, so the element
+// passes spread over the GPU: kSumBlocks blocks per placement reduce fixed strided shares of the
+// elements in a fixed tree, and the partials are combined in a fixed sequential order (results
+// reproducible and independent of k). The peak is the largest |E|, the first in gray-matter order
+// among equals.
+constexpr int kSumBlocks = 64;
+constexpr int kSumT = 256;
+constexpr int kSumFields = 6;  // peak value, w, w*|E|, and the three w*|E|*barycentre sums
+
+__global__ void __launch_bounds__(kSumT) summary_stats_kernel(const float* __restrict__ magn, const int* __restrict__ gm,
+                                                             int n_gm, int n_tets, const float* __restrict__ vols32,
+                                                             const double* __restrict__ bary, double* __restrict__ part,
+                                                             int* __restrict__ part_i) {
+    __shared__ double sv[kSumT], sw[kSumT], swm[kSumT], sx[kSumT], sy[kSumT], sz[kSumT];
+    __shared__ int si[kSumT];
+    const int c = blockIdx.y;
     const float* m = magn + static_cast<long>(c) * n_tets;
     double best = -1.0;
     int bi = 0x7fffffff;
     double w_s = 0.0, wm_s = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
-    for (int i = threadIdx.x; i < n_gm; i += kT) {
+    for (int i = blockIdx.x * kSumT + threadIdx.x; i < n_gm; i += kSumBlocks * kSumT) {
         const int e = gm[i];
         const double mv = m[e];
         const double w = vols32[e];
@@ -182,80 +187,129 @@ __global__ void summary_kernel(const float* __restrict__ magn, const int* __rest
         cy += ww * bary[3 * static_cast<long>(e) + 1];
         cz += ww * bary[3 * static_cast<long>(e) + 2];
     }
-    sv[threadIdx.x] = best;
-    si[threadIdx.x] = bi;
-    sw[threadIdx.x] = w_s;
-    swm[threadIdx.x] = wm_s;
-    sx[threadIdx.x] = cx;
-    sy[threadIdx.x] = cy;
-    sz[threadIdx.x] = cz;
+    const int t = threadIdx.x;
+    sv[t] = best;
+    si[t] = bi;
+    sw[t] = w_s;
+    swm[t] = wm_s;
+    sx[t] = cx;
+    sy[t] = cy;
+    sz[t] = cz;
     __syncthreads();
-    for (int off = kT / 2; off > 0; off >>= 1) {
-        if (threadIdx.x < off) {
-            const int o = threadIdx.x + off;
-            if (sv[o] > sv[threadIdx.x] || (sv[o] == sv[threadIdx.x] && si[o] < si[threadIdx.x])) {
-                sv[threadIdx.x] = sv[o];
-                si[threadIdx.x] = si[o];
+    for (int off = kSumT / 2; off > 0; off >>= 1) {
+        if (t < off) {
+            const int o = t + off;
+            if (sv[o] > sv[t] || (sv[o] == sv[t] && si[o] < si[t])) {
+                sv[t] = sv[o];
+                si[t] = si[o];
             }
-            sw[threadIdx.x] += sw[o];
-            swm[threadIdx.x] += swm[o];
-            sx[threadIdx.x] += sx[o];
-            sy[threadIdx.x] += sy[o];
-            sz[threadIdx.x] += sz[o];
+            sw[t] += sw[o];
+            swm[t] += swm[o];
+            sx[t] += sx[o];
+            sy[t] += sy[o];
+            sz[t] += sz[o];
         }
         __syncthreads();
     }
-    double* o = out + static_cast<long>(c) * kSummaryLen;
-    if (threadIdx.x == 0) {
-        const int e = gm[si[0]];
+    if (t == 0) {
+        const long q = static_cast<long>(c) * kSumBlocks + blockIdx.x;
+        double* o = part + q * kSumFields;
         o[0] = sv[0];
-        o[1] = bary[3 * static_cast<long>(e)];
-        o[2] = bary[3 * static_cast<long>(e) + 1];
-        o[3] = bary[3 * static_cast<long>(e) + 2];
-        o[4] = sx[0] / swm[0];
-        o[5] = sy[0] / swm[0];
-        o[6] = sz[0] / swm[0];
-        o[7] = sw[0];
-        mean_sh = swm[0] / sw[0];
-        o[8] = mean_sh;
+        o[1] = sw[0];
+        o[2] = swm[0];
+        o[3] = sx[0];
+        o[4] = sy[0];
+        o[5] = sz[0];
+        part_i[q] = si[0];
     }
+}
+
+// Sum of field f over a placement's partials, in block order.
+__device__ __forceinline__ double part_sum(const double* part, int c, int f) {
+    double v = 0.0;
+    for (int b = 0; b < kSumBlocks; ++b) v += part[(static_cast<long>(c) * kSumBlocks + b) * kSumFields + f];
+    return v;
+}
+
+__global__ void __launch_bounds__(kSumT) summary_var_kernel(const float* __restrict__ magn, const int* __restrict__ gm,
+                                                           int n_gm, int n_tets, const float* __restrict__ vols32,
+                                                           const double* __restrict__ part,
+                                                           double* __restrict__ var_part) {
+    __shared__ double sv[kSumT];
+    __shared__ double mean_sh;
+    const int c = blockIdx.y;
+    if (threadIdx.x == 0) mean_sh = part_sum(part, c, 2) / part_sum(part, c, 1);
     __syncthreads();
     const double mean = mean_sh;
-    const double wtot = sw[0];
-    __syncthreads();
+    const float* m = magn + static_cast<long>(c) * n_tets;
     double var = 0.0;
-    for (int i = threadIdx.x; i < n_gm; i += kT) {
+    for (int i = blockIdx.x * kSumT + threadIdx.x; i < n_gm; i += kSumBlocks * kSumT) {
         const int e = gm[i];
         const double d = static_cast<double>(m[e]) - mean;
         var += static_cast<double>(vols32[e]) * d * d;
     }
     sv[threadIdx.x] = var;
     __syncthreads();
-    for (int off = kT / 2; off > 0; off >>= 1) {
+    for (int off = kSumT / 2; off > 0; off >>= 1) {
         if (threadIdx.x < off) sv[threadIdx.x] += sv[threadIdx.x + off];
         __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        o[9] = sqrt(sv[0] / wtot);
-        const long base = static_cast<long>(c) * n_gm;
-        const float* v = sorted_keys + base;
-        const double* w = w_sorted + base;
-        const double* cwp = cw + base;
-        const double qs[4] = {static_cast<double>(0.5f), static_cast<double>(0.95f), static_cast<double>(0.99f),
-                              static_cast<double>(0.999f)};
-        for (int j = 0; j < 4; ++j) o[10 + j] = quantile(qs[j], v, w, cwp, n_gm);
-        const double fr[2] = {0.5, 0.75};
-        for (int f = 0; f < 2; ++f) {
-            const double thr = fr[f] * o[13];
-            // First sorted slot with |E| >= thr; everything from there on is stimulated.
-            int lo = 0, hi = n_gm;
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if (static_cast<double>(v[mid]) >= thr) hi = mid;
-                else lo = mid + 1;
-            }
-            o[14 + f] = (lo == 0) ? cwp[n_gm - 1] : (cwp[n_gm - 1] - cwp[lo - 1]);
+    if (threadIdx.x == 0) var_part[static_cast<long>(c) * kSumBlocks + blockIdx.x] = sv[0];
+}
+
+// One thread per placement: partials in block order, then the weighted quantiles and focality
+// from the sorted |E| and its cumulative volume.
+__global__ void summary_final_kernel(int k, const int* __restrict__ gm, int n_gm, const double* __restrict__ bary,
+                                     const double* __restrict__ part, const int* __restrict__ part_i,
+                                     const double* __restrict__ var_part, const float* __restrict__ sorted_keys,
+                                     const double* __restrict__ w_sorted, const double* __restrict__ cw,
+                                     double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= k) return;
+    double best = -1.0;
+    int bi = 0x7fffffff;
+    for (int b = 0; b < kSumBlocks; ++b) {
+        const long q = static_cast<long>(c) * kSumBlocks + b;
+        const double v = part[q * kSumFields];
+        const int i = part_i[q];
+        if (v > best || (v == best && i < bi)) {
+            best = v;
+            bi = i;
         }
+    }
+    const double w_s = part_sum(part, c, 1), wm_s = part_sum(part, c, 2);
+    double var = 0.0;
+    for (int b = 0; b < kSumBlocks; ++b) var += var_part[static_cast<long>(c) * kSumBlocks + b];
+    double* o = out + static_cast<long>(c) * kSummaryLen;
+    const int e = gm[bi];
+    o[0] = best;
+    o[1] = bary[3 * static_cast<long>(e)];
+    o[2] = bary[3 * static_cast<long>(e) + 1];
+    o[3] = bary[3 * static_cast<long>(e) + 2];
+    o[4] = part_sum(part, c, 3) / wm_s;
+    o[5] = part_sum(part, c, 4) / wm_s;
+    o[6] = part_sum(part, c, 5) / wm_s;
+    o[7] = w_s;
+    o[8] = wm_s / w_s;
+    o[9] = sqrt(var / w_s);
+    const long base = static_cast<long>(c) * n_gm;
+    const float* v = sorted_keys + base;
+    const double* w = w_sorted + base;
+    const double* cwp = cw + base;
+    const double qs[4] = {static_cast<double>(0.5f), static_cast<double>(0.95f), static_cast<double>(0.99f),
+                          static_cast<double>(0.999f)};
+    for (int j = 0; j < 4; ++j) o[10 + j] = quantile(qs[j], v, w, cwp, n_gm);
+    const double fr[2] = {0.5, 0.75};
+    for (int f = 0; f < 2; ++f) {
+        const double thr = fr[f] * o[13];
+        // First sorted slot with |E| >= thr; everything from there on is stimulated.
+        int lo = 0, hi = n_gm;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (static_cast<double>(v[mid]) >= thr) hi = mid;
+            else lo = mid + 1;
+        }
+        o[14 + f] = (lo == 0) ? cwp[n_gm - 1] : (cwp[n_gm - 1] - cwp[lo - 1]);
     }
 }
 
@@ -311,8 +365,17 @@ void gm_summary_impl(const Mesh& m, const float* magnE, int k, double* out, Summ
     tile_scan_kernel<<<dim3(tiles, k), 128, 0, s>>>(w.vals_s.get(), w.k64_s.get(), m.gm_index.get(), m.vols32.get(), n,
                                                    w.keys_s.get(), w.w_sorted.get(), w.cw.get(), w.tile_tot.get()); count_launch();
     tile_offset_kernel<<<dim3(tiles, k), 256, 0, s>>>(w.cw.get(), w.tile_tot.get(), n, tiles); count_launch();
-    summary_kernel<<<k, 512, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, m.vols32.get(), m.bary.get(),
-                                     w.keys_s.get(), w.w_sorted.get(), w.cw.get(), out); count_launch();
+    w.part.reserve(static_cast<std::size_t>(k) * kSumBlocks * (kSumFields + 1));
+    w.part_i.reserve(static_cast<std::size_t>(k) * kSumBlocks);
+    double* part = w.part.get();
+    double* var_part = part + static_cast<std::size_t>(k) * kSumBlocks * kSumFields;
+    summary_stats_kernel<<<dim3(kSumBlocks, k), kSumT, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, m.vols32.get(),
+                                                               m.bary.get(), part, w.part_i.get());
+    summary_var_kernel<<<dim3(kSumBlocks, k), kSumT, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, m.vols32.get(),
+                                                             part, var_part);
+    summary_final_kernel<<<(k + 31) / 32, 32, 0, s>>>(k, m.gm_index.get(), n, m.bary.get(), part, w.part_i.get(), var_part,
+                                          w.keys_s.get(), w.w_sorted.get(), w.cw.get(), out);
+    count_launch(3);
     CUNIBS_LAUNCH_CHECK("gm summary");
 }
 
