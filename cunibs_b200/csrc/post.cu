@@ -134,24 +134,6 @@ __global__ void tile_offset_kernel(double* __restrict__ cw, const double* __rest
         cw[base + i] += off;
 }
 
-// interp(q, pos, v) with pos_i = (cw_i - w_i/2) / cw_last (metrics.py:82-95, numpy.interp).
-__device__ double quantile(double q, const float* __restrict__ v, const double* __restrict__ w,
-                           const double* __restrict__ cw, int n) {
-    const double total = cw[n - 1];
-    auto pos = [&](int i) { return (cw[i] - 0.5 * w[i]) / total; };
-    if (q <= pos(0)) return v[0];
-    if (q >= pos(n - 1)) return v[n - 1];
-    int lo = 0, hi = n - 1;  // pos(lo) <= q < pos(hi)
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (pos(mid) <= q) lo = mid;
-        else hi = mid;
-    }
-    const double x0 = pos(lo), x1 = pos(lo + 1);
-    const double slope = (static_cast<double>(v[lo + 1]) - static_cast<double>(v[lo])) / (x1 - x0);
-    return slope * (q - x0) + static_cast<double>(v[lo]);
-}
-
 // Gray-matter summary of each placement (metrics.py:209-243) in three launches, so the element
 // passes spread over the GPU: kSumBlocks blocks per placement reduce fixed strided shares of the
 // elements in a fixed tree, and the partials are combined in a fixed sequential order (results
@@ -257,59 +239,115 @@ __global__ void __launch_bounds__(kSumT) summary_var_kernel(const float* __restr
     if (threadIdx.x == 0) var_part[static_cast<long>(c) * kSumBlocks + blockIdx.x] = sv[0];
 }
 
-// One thread per placement: partials in block order, then the weighted quantiles and focality
-// from the sorted |E| and its cumulative volume.
-__global__ void summary_final_kernel(int k, const int* __restrict__ gm, int n_gm, const double* __restrict__ bary,
-                                     const double* __restrict__ part, const int* __restrict__ part_i,
-                                     const double* __restrict__ var_part, const float* __restrict__ sorted_keys,
-                                     const double* __restrict__ w_sorted, const double* __restrict__ cw,
-                                     double* __restrict__ out) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= k) return;
+// Largest i in [lo, hi) with pred(i) true, for a predicate true on a prefix of [lo, hi) and
+// pred(lo) true: 32 probes per step across the warp (about log32 n dependent loads instead of
+// log2 n). Every lane returns the same index, the one a binary search finds.
+template <typename Pred>
+__device__ __forceinline__ int warp_last_true(int lo, int hi, Pred pred) {
+    const int lane = threadIdx.x % kWarp;
+    while (hi - lo > 1) {
+        const long span = hi - lo;
+        const int probe = lo + static_cast<int>((span * (lane + 1)) / (kWarp + 1));
+        const bool ok = probe > lo && probe < hi && pred(probe);
+        const unsigned mask = __ballot_sync(0xffffffffu, ok || probe <= lo);
+        const int cnt = __popc(mask);  // probes are non-decreasing, so the true ones are a prefix
+        const int new_lo = cnt > 0 ? __shfl_sync(0xffffffffu, probe, cnt - 1) : lo;
+        const int new_hi = cnt < kWarp ? __shfl_sync(0xffffffffu, probe, cnt) : hi;
+        lo = max(lo, new_lo);
+        hi = (new_hi > lo) ? new_hi : lo + 1;
+    }
+    return lo;
+}
+
+// Weighted quantile of the sorted values v with weights w (cw: their cumulative sum):
+// interp(q, pos, v) with pos_i = (cw_i - w_i/2) / cw_last (metrics.py:82-95, numpy.interp), the
+// search spread over a warp.
+__device__ double warp_quantile(double q, const float* __restrict__ v, const double* __restrict__ w,
+                                const double* __restrict__ cw, int n) {
+    const double total = cw[n - 1];
+    auto pos = [&](int i) { return (cw[i] - 0.5 * w[i]) / total; };
+    if (q <= pos(0)) return v[0];
+    if (q >= pos(n - 1)) return v[n - 1];
+    const int lo = warp_last_true(0, n - 1, [&](int i) { return pos(i) <= q; });
+    const double x0 = pos(lo), x1 = pos(lo + 1);
+    const double slope = (static_cast<double>(v[lo + 1]) - static_cast<double>(v[lo])) / (x1 - x0);
+    return slope * (q - x0) + static_cast<double>(v[lo]);
+}
+
+// One warp per placement: partials combined in a fixed order (lane l takes blocks l and l + 32,
+// then a butterfly), the weighted quantiles and focality from the sorted |E| and its cumulative
+// volume with warp-wide searches.
+__global__ void __launch_bounds__(kWarp) summary_final_kernel(
+    int k, const int* __restrict__ gm, int n_gm, const double* __restrict__ bary, const double* __restrict__ part,
+    const int* __restrict__ part_i, const double* __restrict__ var_part, const float* __restrict__ sorted_keys,
+    const double* __restrict__ w_sorted, const double* __restrict__ cw, double* __restrict__ out) {
+    static_assert(kSumBlocks == 2 * kWarp, "two partials per lane");
+    const int c = blockIdx.x;
+    const int lane = threadIdx.x;
     double best = -1.0;
     int bi = 0x7fffffff;
-    for (int b = 0; b < kSumBlocks; ++b) {
-        const long q = static_cast<long>(c) * kSumBlocks + b;
+    double f[kSumFields] = {};
+    double var = 0.0;
+    for (int h = 0; h < 2; ++h) {
+        const long q = static_cast<long>(c) * kSumBlocks + lane + h * kWarp;
         const double v = part[q * kSumFields];
         const int i = part_i[q];
         if (v > best || (v == best && i < bi)) {
             best = v;
             bi = i;
         }
+#pragma unroll
+        for (int j = 1; j < kSumFields; ++j) f[j] += part[q * kSumFields + j];
+        var += var_part[q];
     }
-    const double w_s = part_sum(part, c, 1), wm_s = part_sum(part, c, 2);
-    double var = 0.0;
-    for (int b = 0; b < kSumBlocks; ++b) var += var_part[static_cast<long>(c) * kSumBlocks + b];
+#pragma unroll
+    for (int off = kWarp / 2; off > 0; off >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ov > best || (ov == best && oi < bi)) {
+            best = ov;
+            bi = oi;
+        }
+#pragma unroll
+        for (int j = 1; j < kSumFields; ++j) f[j] += __shfl_xor_sync(0xffffffffu, f[j], off);
+        var += __shfl_xor_sync(0xffffffffu, var, off);
+    }
     double* o = out + static_cast<long>(c) * kSummaryLen;
-    const int e = gm[bi];
-    o[0] = best;
-    o[1] = bary[3 * static_cast<long>(e)];
-    o[2] = bary[3 * static_cast<long>(e) + 1];
-    o[3] = bary[3 * static_cast<long>(e) + 2];
-    o[4] = part_sum(part, c, 3) / wm_s;
-    o[5] = part_sum(part, c, 4) / wm_s;
-    o[6] = part_sum(part, c, 5) / wm_s;
-    o[7] = w_s;
-    o[8] = wm_s / w_s;
-    o[9] = sqrt(var / w_s);
+    const double w_s = f[1], wm_s = f[2];
+    if (lane == 0) {
+        const int e = gm[bi];
+        o[0] = best;
+        o[1] = bary[3 * static_cast<long>(e)];
+        o[2] = bary[3 * static_cast<long>(e) + 1];
+        o[3] = bary[3 * static_cast<long>(e) + 2];
+        o[4] = f[3] / wm_s;
+        o[5] = f[4] / wm_s;
+        o[6] = f[5] / wm_s;
+        o[7] = w_s;
+        o[8] = wm_s / w_s;
+        o[9] = sqrt(var / w_s);
+    }
     const long base = static_cast<long>(c) * n_gm;
     const float* v = sorted_keys + base;
     const double* w = w_sorted + base;
     const double* cwp = cw + base;
     const double qs[4] = {static_cast<double>(0.5f), static_cast<double>(0.95f), static_cast<double>(0.99f),
                           static_cast<double>(0.999f)};
-    for (int j = 0; j < 4; ++j) o[10 + j] = quantile(qs[j], v, w, cwp, n_gm);
+    double p999 = 0.0;
+    for (int j = 0; j < 4; ++j) {
+        const double qv = warp_quantile(qs[j], v, w, cwp, n_gm);
+        if (lane == 0) o[10 + j] = qv;
+        p999 = qv;
+    }
     const double fr[2] = {0.5, 0.75};
-    for (int f = 0; f < 2; ++f) {
-        const double thr = fr[f] * o[13];
+    for (int g = 0; g < 2; ++g) {
+        const double thr = fr[g] * p999;
         // First sorted slot with |E| >= thr; everything from there on is stimulated.
-        int lo = 0, hi = n_gm;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (static_cast<double>(v[mid]) >= thr) hi = mid;
-            else lo = mid + 1;
-        }
-        o[14 + f] = (lo == 0) ? cwp[n_gm - 1] : (cwp[n_gm - 1] - cwp[lo - 1]);
+        int lo;
+        if (static_cast<double>(v[0]) >= thr) lo = 0;
+        else if (!(static_cast<double>(v[n_gm - 1]) >= thr)) lo = n_gm;
+        else lo = warp_last_true(0, n_gm - 1, [&](int i) { return !(static_cast<double>(v[i]) >= thr); }) + 1;
+        if (lane == 0) o[14 + g] = (lo == 0) ? cwp[n_gm - 1] : (cwp[n_gm - 1] - cwp[lo - 1]);
     }
 }
 
@@ -373,7 +411,7 @@ void gm_summary_impl(const Mesh& m, const float* magnE, int k, double* out, Summ
                                                                m.bary.get(), part, w.part_i.get());
     summary_var_kernel<<<dim3(kSumBlocks, k), kSumT, 0, s>>>(magnE, m.gm_index.get(), n, m.n_tets, m.vols32.get(),
                                                              part, var_part);
-    summary_final_kernel<<<(k + 31) / 32, 32, 0, s>>>(k, m.gm_index.get(), n, m.bary.get(), part, w.part_i.get(), var_part,
+    summary_final_kernel<<<k, kWarp, 0, s>>>(k, m.gm_index.get(), n, m.bary.get(), part, w.part_i.get(), var_part,
                                           w.keys_s.get(), w.w_sorted.get(), w.cw.get(), out);
     count_launch(3);
     CUNIBS_LAUNCH_CHECK("gm summary");
