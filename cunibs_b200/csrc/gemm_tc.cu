@@ -19,6 +19,7 @@
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
 
+#include <atomic>
 #include <mutex>
 
 #include "internal.hpp"
@@ -304,8 +305,17 @@ void launch(const GemmProblem& p, cudaStream_t s) {
     const CUtensorMap ma = make_map(p.a, p.M, p.K, p.lda, BM);
     const CUtensorMap mb = make_map(p.b, p.N, p.K, p.ldb, BN);
     constexpr std::size_t smem = STAGES * (BM + BN) * BK * 2 + 1024 + 256;
-    CUNIBS_CHECK(cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      static_cast<int>(smem)));
+    // The shared-memory opt-in is set once per device (a host call per launch costs more than a
+    // small GEMM's tiles).
+    static std::atomic<std::uint64_t> opted{0};
+    int dev = 0;
+    CUNIBS_CHECK(cudaGetDevice(&dev));
+    const std::uint64_t bit = std::uint64_t{1} << (dev & 63);
+    if (!(opted.load(std::memory_order_acquire) & bit)) {
+        CUNIBS_CHECK(cudaFuncSetAttribute(gemm_bf16_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)));
+        opted.fetch_or(bit, std::memory_order_acq_rel);
+    }
     const dim3 grid((p.N + BN - 1) / BN, (p.M + BM - 1) / BM);
     gemm_bf16_kernel<BN><<<grid, kThreads, smem, s>>>(ma, mb, p.ep, p.M, p.N, p.K);
     count_launch();
@@ -318,8 +328,10 @@ void gemm_bf16(const GemmProblem& p, cudaStream_t s) {
     if (p.M <= 0 || p.N <= 0 || p.K <= 0) fail(kEInval, "GEMM sizes must be positive");
     if (p.K % 8 != 0) fail(kEInval, "GEMM K must be a multiple of 8");
     if (p.ep.out16t && p.ep.ld_t < p.M) fail(kEInval, "transposed output leading dimension is below M");
+    // One row of tiles (M <= 128, the warm start's network at inference) is latency-bound: 32-wide
+    // tiles give 4x the CTAs and smaller stages (measured 20.5 -> 10.4 us for 16 x 512 x 512).
     if (p.N <= 16) launch<16>(p, s);
-    else if (p.N <= 32) launch<32>(p, s);
+    else if (p.N <= 32 || p.M <= BM) launch<32>(p, s);
     else launch<128>(p, s);
 }
 
