@@ -144,6 +144,7 @@ def load() -> C.CDLL:
         "cunibs_context_pending": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "cunibs_context_set_overlap": ([_vp, C.c_int], C.c_int),
         "cunibs_context_set_conductivity": ([_vp, dp], C.c_int),
+        "cunibs_context_set_conductivity_keep_coarse": ([_vp, dp], C.c_int),
         "cunibs_context_array": ([_vp, C.c_char_p, C.c_int, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
         "cunibs_context_place": ([_vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
         "cunibs_context_dadt": ([_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp], C.c_int),
@@ -424,9 +425,13 @@ class Context:
     def set_overlap(self, blocks_per_sm: int) -> None:
         check(self._lib.cunibs_context_set_overlap(self.handle, int(blocks_per_sm)))
 
-    def set_conductivity(self, sigma_by_tag) -> None:
+    def set_conductivity(self, sigma_by_tag, *, keep_coarse: bool = False) -> None:
+        """New conductivities (index = tissue tag). keep_coarse: refresh only the finest AMG level
+        (cunibs_context_set_conductivity_keep_coarse), the cheap per-sample step of a Monte Carlo."""
         s = np.ascontiguousarray(sigma_by_tag, np.float64).reshape(11)
-        check(self._lib.cunibs_context_set_conductivity(self.handle, s.ctypes.data_as(C.POINTER(C.c_double))))
+        fn = (self._lib.cunibs_context_set_conductivity_keep_coarse if keep_coarse
+              else self._lib.cunibs_context_set_conductivity)
+        check(fn(self.handle, s.ctypes.data_as(C.POINTER(C.c_double))))
 
     @staticmethod
     def _block_inputs(coil, centers, handles, dists):

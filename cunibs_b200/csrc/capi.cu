@@ -701,9 +701,23 @@ int cunibs_context_set_conductivity(cunibs_context* c, const double* sigma_by_ta
     return guarded([&] {
         require(c && sigma_by_tag, "NULL argument");
         for (int t = 1; t <= 10; ++t) require(sigma_by_tag[t] > 0.0, "conductivities must be positive");
+        require(c->pending.empty(), "finish the submitted blocks first");
         DeviceGuard dg(c->device);
         assemble_stiffness(c->mesh, sigma_by_tag, c->stream);
         c->rebuild_hierarchy();
+    });
+}
+
+int cunibs_context_set_conductivity_keep_coarse(cunibs_context* c, const double* sigma_by_tag) {
+    return guarded([&] {
+        require(c && sigma_by_tag, "NULL argument");
+        for (int t = 1; t <= 10; ++t) require(sigma_by_tag[t] > 0.0, "conductivities must be positive");
+        require(c->pending.empty(), "finish the submitted blocks first");
+        DeviceGuard dg(c->device);
+        assemble_stiffness(c->mesh, sigma_by_tag, c->stream);
+        DevCsr<double> a0;
+        reduce_grounded(c->mesh, a0, c->stream);
+        if (!refresh_finest_level(c->hier, a0, c->stream)) c->rebuild_hierarchy();
     });
 }
 

@@ -133,6 +133,7 @@ void reduce_grounded(const Mesh& m, DevCsr<double>& out, cudaStream_t s);
 // Hierarchy (setup_amg.cu).
 int select_size4(int n, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s);
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& p, cudaStream_t s);
+bool refresh_finest_level(Hierarchy& h, const DevCsr<double>& a0, cudaStream_t s);
 void spgemm(const DevCsr<double>& A, const DevCsr<double>& B, DevCsr<double>& C, cudaStream_t s);
 void transpose(const DevCsr<double>& A, DevCsr<double>& T, cudaStream_t s);
 void l1_dinv(const DevCsr<double>& a, DevArray<double>& dinv, cudaStream_t s);

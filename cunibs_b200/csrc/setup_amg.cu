@@ -676,6 +676,23 @@ static void dense_inverse(const DevCsr<double>& a, DevArray<double>& inv, DevArr
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 
+// New values for the finest operator (the same pattern: conductivity changes only values): copy
+// them, refresh the level's l1 smoother weights and FP32 copies, keep every coarser level,
+// prolongator and the dense bottom. False when the hierarchy has no level to refresh or the
+// pattern differs.
+bool refresh_finest_level(Hierarchy& h, const DevCsr<double>& a0, cudaStream_t s) {
+    if (h.levels.empty()) return false;
+    Level& L = h.levels[0];
+    if (L.a.n != a0.n || L.a.nnz != a0.nnz) return false;
+    CUNIBS_CHECK(cudaMemcpyAsync(L.a.val.get(), a0.val.get(), sizeof(double) * a0.nnz, cudaMemcpyDeviceToDevice, s));
+    l1_dinv(L.a, L.dinv, s);
+    to_f32(L.a.val, L.a.nnz, L.a32, s);
+    to_f32(L.dinv, L.n, L.dinv32, s);
+    CUNIBS_LAUNCH_CHECK("refresh finest level");
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    return true;
+}
+
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& prm, cudaStream_t s) {
     h.levels.clear();
     h.sizes.assign(1, a0.n);

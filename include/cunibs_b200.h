@@ -196,6 +196,15 @@ int cunibs_context_set_overlap(cunibs_context* ctx, int blocks_per_sm);
  * (uq/conductivity/run.py:324-361). */
 int cunibs_context_set_conductivity(cunibs_context* ctx, const double* sigma_by_tag);
 
+/* The cheap per-sample step: re-assembles the stiffness (and the right-hand side weights) for new
+ * conductivities and refreshes the finest AMG level's values and smoother weights, but keeps the
+ * coarser levels built for the earlier conductivities. PCG still solves the new operator to the
+ * same tolerance; the preconditioner is only slightly off. This is the reference's Monte Carlo
+ * scheme, which swaps the operator's values per draw and keeps the V-cycle built at the nominal
+ * conductivities (uq/conductivity/assembly.py:1-7,53-70; run.py:203-387). A draw that then misses
+ * the tolerance is the caller's cue for cunibs_context_set_conductivity. */
+int cunibs_context_set_conductivity_keep_coarse(cunibs_context* ctx, const double* sigma_by_tag);
+
 /* --- stage-level entry points (the reference's kernel exports, bindings.cpp) --------------- */
 
 /* Copies a named internal array to host memory. name / dtype:

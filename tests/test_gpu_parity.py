@@ -293,3 +293,39 @@ def test_conductivity_resetup_scale_invariance(sphere_mesh):
     subj.context.set_conductivity(sigma)
     assert rel(subj.simulate(coil, site, magnitude=True, recovery="raw").magnE.astype(np.float64)) <= 1e-6
     subj.free()
+
+
+def test_conductivity_keep_coarse_matches_full_resetup(sphere_mesh):
+    """cunibs_context_set_conductivity_keep_coarse (finest level refreshed, coarse levels kept)
+    solves the same operator as a full re-setup: the fields agree to the solve tolerance, at a
+    modest iteration cost, and the nominal table restores the original field."""
+    from cunibs_b200.fem import TISSUE_CONDUCTIVITY
+
+    sigma = np.zeros(11)
+    for tag, s in TISSUE_CONDUCTIVITY.items():
+        sigma[tag] = s
+    rng = np.random.default_rng(11)
+    draw = sigma.copy()
+    draw[1:] *= np.exp(0.25 * rng.standard_normal(10))  # lognormal, log-sd 0.25
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    sites = [Placement(top, top + [0, 50, 0]), Placement([30.0, 0, 84.8], [30.0, 50, 84.8])]
+    full = Subject(sphere_mesh, tolerance=1e-10)
+    kept = Subject(sphere_mesh, tolerance=1e-10)
+    base = [r.magnE.astype(np.float64) for r in kept.iter_simulate(coil, sites, magnitude=True, recovery="raw")]
+    full.context.set_conductivity(draw)
+    kept.context.set_conductivity(draw, keep_coarse=True)
+    gm = full.mesh.tet_tags == 2
+    a = list(full.iter_simulate(coil, sites, magnitude=True, recovery="raw"))
+    b = list(kept.iter_simulate(coil, sites, magnitude=True, recovery="raw"))
+    for ra, rb, r0 in zip(a, b, base):
+        x, y = ra.magnE.astype(np.float64)[gm], rb.magnE.astype(np.float64)[gm]
+        assert np.linalg.norm(x - y) / np.linalg.norm(x) <= 1e-7
+        assert np.linalg.norm(x - r0[gm]) / np.linalg.norm(r0[gm]) >= 1e-3  # the draw changed the field
+        assert rb.iterations <= 2 * ra.iterations
+    kept.context.set_conductivity(sigma, keep_coarse=True)
+    back = [r.magnE.astype(np.float64) for r in kept.iter_simulate(coil, sites, magnitude=True, recovery="raw")]
+    for r, r0 in zip(back, base):
+        assert np.linalg.norm(r[gm] - r0[gm]) / np.linalg.norm(r0[gm]) <= 1e-7
+    full.free()
+    kept.free()
