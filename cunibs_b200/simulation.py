@@ -279,6 +279,107 @@ class Subject:
                                        potential=potential, nodal=nodal, recovery=recovery, block_k=block_k)
         return result
 
+    def iter_simulate_conductivity_uq(self, coil: Coil, placements: Sequence[Placement], config, didt: float = 1e6,
+                                      *, moments: bool = False, recovery: str = "harmonic",
+                                      focality_frac: float = 0.5) -> Iterator:
+        """Stream a conductivity Monte Carlo per placement (reference simulation.py:594-630).
+
+        Every draw of ``config`` (:class:`cunibs_b200.uq.ConductivityUQConfig`) re-weights the
+        stiffness and right-hand side and solves the placement to the subject's tolerance; the
+        AMG hierarchy stays the nominal one (only its finest level follows the draw). Each
+        :class:`cunibs_b200.uq.ConductivityUQResult` carries the per-draw gray-matter peak,
+        focality (stimulated volume at ``focality_frac`` x p99.9, 0.5 or 0.75) and peak location;
+        ``moments=True`` adds per-tetrahedron mean/std/cov of |E| and the summary of the mean field.
+        The subject is back at the nominal conductivities afterwards.
+        """
+        from . import uq
+
+        sites = _sites(placements, "iter_simulate_conductivity_uq")
+        recovery = validate_recovery(recovery)
+        if not isinstance(coil, Coil):
+            raise TypeError("coil must be a cunibs_b200.Coil")
+        if focality_frac not in (0.5, 0.75):
+            raise ValueError("focality_frac must be 0.5 or 0.75 (the native summary's focality levels)")
+        if not isinstance(config, uq.ConductivityUQConfig) or config.n_samples < 1:
+            raise ValueError("config must be a ConductivityUQConfig with n_samples >= 1")
+        return self._iter_uq(coil, sites, config, float(didt), bool(moments), recovery, focality_frac)
+
+    def _iter_uq(self, coil, sites, config, didt, moments, recovery, focality_frac):
+        from . import uq
+
+        ctx = self.context
+        present = set(int(t) for t in np.unique(self.mesh.tet_tags))
+        tags = tuple(config.perturbed_tags) if config.perturbed_tags is not None else tuple(sorted(present))
+        for t in tags:
+            if t not in uq.DEFAULT_TISSUE_COV and t not in config.tissue_cov:
+                raise ValueError(f"no coefficient of variation for tissue tag {t}")
+        draws = uq.sample_conductivities(config, tags)
+        nominal = uq.nominal_sigma_table()
+        f_col = 14 if focality_frac == 0.5 else 15
+        host = self._host_metric_inputs() if moments else None
+        try:
+            for site in sites:
+                n = config.n_samples
+                peak = np.empty(n)
+                foc = np.empty(n)
+                loc = np.empty((n, 3))
+                its = np.empty(n, np.int32)
+                s1 = s2 = None
+                resetups = 0
+                for i in range(n):
+                    sigma = nominal.copy()
+                    sigma[list(tags)] = draws[i]
+                    with self._lock:
+                        ctx.set_conductivity(sigma, keep_coarse=True)
+                        args = (coil, site.center_mm[None], site.handle_mm[None], [site.distance_mm], didt)
+                        try:
+                            out = ctx.solve_block(*args, magnitude=moments, recovery=recovery)
+                        except _native.ConvergenceFailure:
+                            # The nominal preconditioner was too far from this draw: solve it
+                            # against its own hierarchy, then rebuild the nominal one.
+                            ctx.set_conductivity(sigma)
+                            try:
+                                out = ctx.solve_block(*args, magnitude=moments, recovery=recovery)
+                            except _native.ConvergenceFailure as exc:
+                                raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
+                            finally:
+                                ctx.set_conductivity(nominal)
+                            resetups += 1
+                    row = out["summary"][0]
+                    peak[i], foc[i], loc[i], its[i] = row[0], row[f_col], row[1:4], out["iterations"][0]
+                    if moments:
+                        m = out["magnE"][0].astype(np.float64)
+                        s1 = m.copy() if s1 is None else s1 + m
+                        s2 = m * m if s2 is None else s2 + m * m
+                mean = std = cov = None
+                if moments:
+                    mean = s1 / n
+                    std = np.sqrt(np.maximum(s2 / n - mean * mean, 0.0))
+                    cov = np.divide(std, mean, out=np.zeros_like(std), where=mean > 0)
+                res = uq.ConductivityUQResult(
+                    mean_magnE=mean, std_magnE=std, cov_magnE=cov, n_samples=n, perturbed_tags=tags,
+                    sigma_samples=draws, vols=host[0] if host else None, tet_tags=host[1] if host else None,
+                    barycenters_mm=host[2] if host else None, placement=site, coil_name=coil.name, didt=didt,
+                    peak_samples=peak, focality_samples=foc, peak_location_samples=loc, iteration_samples=its,
+                    recovery=recovery, full_resetups=resetups)
+                if moments:
+                    res.summary = res.compute_summary()
+                yield res
+        finally:
+            with self._lock:
+                if self._ctx is ctx:
+                    ctx.set_conductivity(nominal, keep_coarse=True)
+
+    def simulate_conductivity_uq(self, coil: Coil, placement: Placement, config, didt: float = 1e6, *,
+                                 moments: bool = False, recovery: str = "harmonic", focality_frac: float = 0.5):
+        """Conductivity Monte Carlo for a single placement (reference simulation.py:632-664)."""
+        if not isinstance(placement, Placement):
+            raise TypeError("simulate_conductivity_uq() takes a single Placement; use "
+                            "iter_simulate_conductivity_uq() for a sequence.")
+        (result,) = self.iter_simulate_conductivity_uq(coil, [placement], config, didt, moments=moments,
+                                                       recovery=recovery, focality_frac=focality_frac)
+        return result
+
 
 @dataclass
 class FieldResult:

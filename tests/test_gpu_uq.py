@@ -1,0 +1,52 @@
+"""Conductivity Monte Carlo on the GPU (Subject.simulate_conductivity_uq). Needs a B200.
+
+Each draw is solved with the nominal coarse AMG levels kept; its gray-matter peak must match a
+solve after a full re-setup for that draw, the moments must be the draws' mean and spread, and the
+subject must be back at the nominal conductivities afterwards, bit for bit.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from cunibs_b200 import Placement, Subject
+from cunibs_b200.synthetic import figure8_coil, sphere_head
+from cunibs_b200.uq import ConductivityUQConfig, nominal_sigma_table, sample_conductivities
+
+pytestmark = pytest.mark.gpu
+
+
+def test_conductivity_uq_matches_per_draw_full_resetup():
+    mesh = sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    site = Placement(top, top + [0, 50, 0])
+    cfg = ConductivityUQConfig(n_samples=5, seed=4)
+    subj = Subject(mesh, tolerance=1e-10)
+    before = subj.simulate(coil, site, magnitude=True, recovery="raw").magnE
+    res = subj.simulate_conductivity_uq(coil, site, cfg, moments=True, recovery="raw")
+    after = subj.simulate(coil, site, magnitude=True, recovery="raw").magnE
+    np.testing.assert_array_equal(after, before)
+    assert res.n_samples == 5 and res.full_resetups == 0
+    tags = res.perturbed_tags
+    np.testing.assert_array_equal(res.sigma_samples, sample_conductivities(cfg, tags))
+    ref = Subject(mesh, tolerance=1e-10)
+    fields = []
+    for i in range(cfg.n_samples):
+        sigma = nominal_sigma_table()
+        sigma[list(tags)] = res.sigma_samples[i]
+        ref.context.set_conductivity(sigma)
+        r = ref.simulate(coil, site, magnitude=True, recovery="raw")
+        assert res.peak_samples[i] == pytest.approx(r.peak_magnE(), rel=1e-6)
+        assert res.focality_samples[i] == pytest.approx(r.summary["focality_m3"]["0.5"], rel=1e-4)
+        fields.append(r.magnE.astype(np.float64))
+    f = np.stack(fields)
+    gm = res.tet_tags == 2
+    np.testing.assert_allclose(res.mean_magnE[gm], f.mean(0)[gm], rtol=1e-5)
+    np.testing.assert_allclose(res.std_magnE[gm], f.std(0)[gm], rtol=1e-3, atol=1e-6 * f.max())
+    assert res.summary is not None and res.max_local_cov() > 0
+    assert res.peak_mean_magnE() == pytest.approx(float(f.mean(0)[gm].max()), rel=1e-5)
+    assert np.isclose(sum(res.tissue_sensitivity().values()), 1.0, atol=0.5)
+    subj.free()
+    ref.free()
