@@ -264,7 +264,7 @@ def _operator(ctx: _native.Context):
 def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: int = 512, hidden: int = 512,
                      depth: int = 4, epochs: int = 400, batch: int = 256, lr: float = 1e-3, seed: int = 0,
                      tolerance: float = 1e-8, z_min_mm: float = 40.0, radius_mm: float = 90.0,
-                     install: bool = True, energy: bool = False) -> WarmStartModel:
+                     install: bool = True, energy: bool = True) -> WarmStartModel:
     """Generate training solves, build the basis, train the network on the GPU and (optionally)
     install it in the context. Returns the model with timing and loss statistics."""
     torch = _torch()

@@ -50,3 +50,26 @@ def test_conductivity_uq_matches_per_draw_full_resetup():
     assert np.isclose(sum(res.tissue_sensitivity().values()), 1.0, atol=0.5)
     subj.free()
     ref.free()
+
+
+def test_a_draw_the_kept_hierarchy_cannot_finish_gets_a_full_resetup():
+    """With a tight iteration budget and wide draws, the kept coarse levels miss it on some draws
+    (even after the solver's own FP64 retry, which grants a second budget): those are solved again
+    after a full re-setup, and the subject ends on its nominal hierarchy (the same field as
+    before, bit for bit)."""
+    mesh = sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    site = Placement(top, top + [0, 50, 0])
+    probe = Subject(mesh, tolerance=1e-8)
+    nominal_iters = probe.simulate(coil, site, recovery="raw").iterations
+    probe.free()
+    budget = nominal_iters // 2 + 2  # solve plus retry: about nominal + 3 iterations in all
+    subj = Subject(mesh, tolerance=1e-8, max_iters=budget)
+    before = subj.simulate(coil, site, magnitude=True, recovery="raw").magnE
+    cfg = ConductivityUQConfig(n_samples=6, seed=9, tissue_cov={t: 1.5 for t in range(1, 11)})
+    res = subj.simulate_conductivity_uq(coil, site, cfg, recovery="raw")
+    assert res.full_resetups >= 1
+    assert (res.iteration_samples <= 2 * budget).all()
+    np.testing.assert_array_equal(subj.simulate(coil, site, magnitude=True, recovery="raw").magnE, before)
+    subj.free()
