@@ -317,21 +317,29 @@ class Subject:
         nominal = uq.nominal_sigma_table()
         f_col = 14 if focality_frac == 0.5 else 15
         host = self._host_metric_inputs() if moments else None
+        n = config.n_samples
         try:
-            for site in sites:
-                n = config.n_samples
-                peak = np.empty(n)
-                foc = np.empty(n)
-                loc = np.empty((n, 3))
-                its = np.empty(n, np.int32)
+            # Every placement sees the same draws, so a chunk of up to MAX_BLOCK placements shares
+            # each draw's re-setup and one block solve; a placement's result does not depend on its
+            # block-mates, so it is the one a run of that placement alone gives.
+            for start in range(0, len(sites), MAX_BLOCK):
+                chunk = sites[start:start + MAX_BLOCK]
+                k = len(chunk)
+                centers = np.stack([s.center_mm for s in chunk])
+                handles = np.stack([s.handle_mm for s in chunk])
+                dists = np.array([s.distance_mm for s in chunk])
+                peak = np.empty((k, n))
+                foc = np.empty((k, n))
+                loc = np.empty((k, n, 3))
+                its = np.empty((k, n), np.int32)
                 s1 = s2 = None
-                resetups = 0
+                resetups = np.zeros(k, np.int64)
                 for i in range(n):
                     sigma = nominal.copy()
                     sigma[list(tags)] = draws[i]
                     with self._lock:
                         ctx.set_conductivity(sigma, keep_coarse=True)
-                        args = (coil, site.center_mm[None], site.handle_mm[None], [site.distance_mm], didt)
+                        args = (coil, centers, handles, dists, didt)
                         try:
                             out = ctx.solve_block(*args, magnitude=moments, recovery=recovery)
                         except _native.ConvergenceFailure:
@@ -345,26 +353,27 @@ class Subject:
                             finally:
                                 ctx.set_conductivity(nominal)
                             resetups += 1
-                    row = out["summary"][0]
-                    peak[i], foc[i], loc[i], its[i] = row[0], row[f_col], row[1:4], out["iterations"][0]
+                    rows = out["summary"]
+                    peak[:, i], foc[:, i], loc[:, i], its[:, i] = rows[:, 0], rows[:, f_col], rows[:, 1:4], out["iterations"]
                     if moments:
-                        m = out["magnE"][0].astype(np.float64)
+                        m = out["magnE"].astype(np.float64)
                         s1 = m.copy() if s1 is None else s1 + m
                         s2 = m * m if s2 is None else s2 + m * m
-                mean = std = cov = None
-                if moments:
-                    mean = s1 / n
-                    std = np.sqrt(np.maximum(s2 / n - mean * mean, 0.0))
-                    cov = np.divide(std, mean, out=np.zeros_like(std), where=mean > 0)
-                res = uq.ConductivityUQResult(
-                    mean_magnE=mean, std_magnE=std, cov_magnE=cov, n_samples=n, perturbed_tags=tags,
-                    sigma_samples=draws, vols=host[0] if host else None, tet_tags=host[1] if host else None,
-                    barycenters_mm=host[2] if host else None, placement=site, coil_name=coil.name, didt=didt,
-                    peak_samples=peak, focality_samples=foc, peak_location_samples=loc, iteration_samples=its,
-                    recovery=recovery, full_resetups=resetups)
-                if moments:
-                    res.summary = res.compute_summary()
-                yield res
+                for j, site in enumerate(chunk):
+                    mean = std = cov = None
+                    if moments:
+                        mean = s1[j] / n
+                        std = np.sqrt(np.maximum(s2[j] / n - mean * mean, 0.0))
+                        cov = np.divide(std, mean, out=np.zeros_like(std), where=mean > 0)
+                    res = uq.ConductivityUQResult(
+                        mean_magnE=mean, std_magnE=std, cov_magnE=cov, n_samples=n, perturbed_tags=tags,
+                        sigma_samples=draws, vols=host[0] if host else None, tet_tags=host[1] if host else None,
+                        barycenters_mm=host[2] if host else None, placement=site, coil_name=coil.name, didt=didt,
+                        peak_samples=peak[j], focality_samples=foc[j], peak_location_samples=loc[j],
+                        iteration_samples=its[j], recovery=recovery, full_resetups=int(resetups[j]))
+                    if moments:
+                        res.summary = res.compute_summary()
+                    yield res
         finally:
             with self._lock:
                 if self._ctx is ctx:

@@ -73,3 +73,22 @@ def test_a_draw_the_kept_hierarchy_cannot_finish_gets_a_full_resetup():
     assert (res.iteration_samples <= 2 * budget).all()
     np.testing.assert_array_equal(subj.simulate(coil, site, magnitude=True, recovery="raw").magnE, before)
     subj.free()
+
+
+def test_placements_batched_per_draw_match_single_runs():
+    """A sequence of placements shares every draw's re-setup and one block solve; each result is
+    the one a run of that placement alone gives, bit for bit."""
+    mesh = sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(64)
+    sites = [Placement([0.0, 0.0, 90.0], [0.0, 50.0, 90.0]), Placement([25.0, 0.0, 86.4], [25.0, 50.0, 86.4]),
+             Placement([0.0, -25.0, 86.4], [50.0, -25.0, 86.4])]
+    cfg = ConductivityUQConfig(n_samples=4, seed=2)
+    subj = Subject(mesh, tolerance=1e-8)
+    together = list(subj.iter_simulate_conductivity_uq(coil, sites, cfg, moments=True, recovery="harmonic"))
+    for site, r in zip(sites, together):
+        alone = subj.simulate_conductivity_uq(coil, site, cfg, moments=True, recovery="harmonic")
+        np.testing.assert_array_equal(r.peak_samples, alone.peak_samples)
+        np.testing.assert_array_equal(r.iteration_samples, alone.iteration_samples)
+        np.testing.assert_array_equal(r.mean_magnE, alone.mean_magnE)
+        assert r.placement is site
+    subj.free()
