@@ -1,5 +1,6 @@
 """The closed-form sphere field (oracle/analytic_sphere.py) as an independent check of the
-finite-element solution (not in the reference; a sanity bound, not the 1e-5 bar).
+finite-element solution (the reference has no such check; it bounds the discretisation error, so
+it is a sanity bound, not the 1e-5 parity bar against the FP64 oracle).
 
 The formula is first pinned by physics alone: inside a spherically symmetric conductor the induced
 field is tangential, divergence-free, and differs from -dA/dt by a gradient. The FEM then has to
