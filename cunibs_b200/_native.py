@@ -145,6 +145,11 @@ def load() -> C.CDLL:
         "cunibs_context_set_overlap": ([_vp, C.c_int], C.c_int),
         "cunibs_context_set_conductivity": ([_vp, dp], C.c_int),
         "cunibs_context_set_conductivity_keep_coarse": ([_vp, dp], C.c_int),
+        "cunibs_sigma_begin": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), dp, ip,
+                                C.c_int, C.c_double, ip], C.c_int),
+        "cunibs_sigma_draw": ([_vp, dp, C.POINTER(BlockOut), ip], C.c_int),
+        "cunibs_sigma_end": ([_vp], C.c_int),
+        "cunibs_sigma_coefficients": ([C.c_int, dp, dp, ip, C.c_double, dp, ip], C.c_int),
         "cunibs_context_array": ([_vp, C.c_char_p, C.c_int, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
         "cunibs_context_place": ([_vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
         "cunibs_context_dadt": ([_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp], C.c_int),
@@ -229,6 +234,7 @@ class Context:
         self._h = h
         self._lib = lib
         self._submitted: dict[int, tuple] = {}
+        self._study: tuple | None = None
         self.params = prm
         info = Info()
         check(lib.cunibs_context_info(h, C.byref(info)))
@@ -433,6 +439,47 @@ class Context:
               else self._lib.cunibs_context_set_conductivity)
         check(fn(self.handle, s.ctypes.data_as(C.POINTER(C.c_double))))
 
+    def sigma_begin(self, coil, centers, handles, dists, didt, sigma_nominal, tags, *, sensitivity_tol=1e-3,
+                    precision=PREC_DEFAULT, tolerance=0.0, max_iters=0, magnitude=False, vectors=False,
+                    potential=False, recovery="raw", nodal=False) -> np.ndarray:
+        """cunibs_sigma_begin: open a conductivity study of one block of placements; the outputs of
+        every draw are chosen here. Returns the sensitivity-subspace rank per placement."""
+        pos, mom, centers, handles, dists = self._block_inputs(coil, centers, handles, dists)
+        k = centers.shape[0]
+        if nodal and recovery == "raw":
+            raise ValueError("nodal=True needs a recovery mode")
+        opts = SolveOpts(0, int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery], 0)
+        sig = np.ascontiguousarray(sigma_nominal, np.float64).reshape(11)
+        tg = np.ascontiguousarray(tags, np.int32).reshape(-1)
+        rank = np.zeros(k, np.int32)
+        check(self._lib.cunibs_sigma_begin(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
+                                           _p(dists), k, float(didt), C.byref(opts),
+                                           sig.ctypes.data_as(C.POINTER(C.c_double)), _ip(tg), tg.shape[0],
+                                           float(sensitivity_tol), _ip(rank)))
+        self._study = (k, tg.shape[0], magnitude, vectors, potential, recovery, nodal)
+        return rank
+
+    def sigma_draw(self, sigma) -> dict:
+        """cunibs_sigma_draw: one draw (the perturbed tissues' conductivities, in the study's tag
+        order); the same dict as solve_block plus "resetup" (1 when the draw needed its own hierarchy)."""
+        if self._study is None:
+            raise ValueError("no conductivity study is open")
+        k, n_tags, magnitude, vectors, potential, recovery, nodal = self._study
+        s = np.ascontiguousarray(sigma, np.float64).reshape(n_tags)
+        res, out = self._block_outputs(k, magnitude, vectors, potential, recovery, nodal)
+        flag = C.c_int(0)
+        check(self._lib.cunibs_sigma_draw(self.handle, s.ctypes.data_as(C.POINTER(C.c_double)), C.byref(out),
+                                          C.byref(flag)))
+        res["total_iterations"] = out.total_iterations
+        res["outer_steps"] = out.outer_steps
+        res["resetup"] = flag.value
+        return res
+
+    def sigma_end(self) -> None:
+        """cunibs_sigma_end: close the study; the context is back at the nominal conductivities."""
+        self._study = None
+        check(self._lib.cunibs_sigma_end(self.handle))
+
     @staticmethod
     def _block_inputs(coil, centers, handles, dists):
         centers = np.ascontiguousarray(centers, np.float64).reshape(-1, 3)
@@ -513,6 +560,22 @@ class Context:
 
 def kernel_launches() -> int:
     return int(load().cunibs_kernel_launches())
+
+
+def sigma_coefficients(gram, proj, active, rtol: float = 1e-12):
+    """cunibs_sigma_coefficients (host only): the draw-coefficient map Z of one placement and the
+    rank of its sensitivity subspace."""
+    lib = load()
+    g = np.ascontiguousarray(gram, np.float64)
+    n = g.shape[0]
+    pr = np.ascontiguousarray(proj, np.float64).reshape(n, n)
+    act = np.ascontiguousarray(active, np.int32).reshape(n)
+    z = np.empty((n, n))
+    rank = C.c_int()
+    dp = C.POINTER(C.c_double)
+    check(lib.cunibs_sigma_coefficients(n, g.ctypes.data_as(dp), pr.ctypes.data_as(dp), _ip(act), float(rtol),
+                                        z.ctypes.data_as(dp), C.byref(rank)))
+    return z, rank.value
 
 
 def select_size4(row_ptr, col_idx, values):

@@ -1,4 +1,6 @@
 // The C ABI (include/cunibs_b200.h): context lifetime, the block solve, stage-level entry points.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <deque>
 #include <string>
@@ -77,7 +79,25 @@ struct PendingBlock {
     bool has_opts = false, has_handles = false;
     bool timed = false;  // stage events recorded (only for a block prepared with no other in flight)
     bool guess_due = false;  // a learned initial guess is wanted and not yet issued
+    bool x0_given = false;   // the slot's X0 already holds this block's initial guess
     cunibs_solve_opts opts{};
+};
+
+// A conductivity Monte Carlo over one block of placements (uq/conductivity/run.py:203-387): the
+// coil field of the block (held in one slot), the per-tissue operator components, the nominal
+// solution and its sensitivities, from cunibs_sigma_begin to cunibs_sigma_end.
+struct SigmaStudy {
+    int k = 0, K = 0, P = 0, slot = 0;
+    bool has_handles = false, has_opts = false;
+    cunibs_solve_opts opts{};
+    double nominal[11] = {};
+    int tags[kSigmaMaxTags] = {};
+    long nnz = 0;
+    DevArray<double> comp;   // (1 + P, nnz): the other tissues at nominal, then each tissue at unit sigma
+    DevArray<double> x_nom;  // (n_red, K) nominal potential
+    DevArray<double> S;      // (n_red, P, K) sensitivities
+    std::vector<double> Z;   // (K, P, P): y_j = Z_j (sigma - sigma_nom)
+    std::vector<int> rank;   // (k)
 };
 
 struct cunibs_context {
@@ -113,6 +133,8 @@ struct cunibs_context {
     std::unique_ptr<WarmStart> warm;
     std::vector<int> warm_used;
     std::vector<double> init_rel;
+    // The open conductivity study, if any (its block slot is reserved while it is open).
+    std::unique_ptr<SigmaStudy> study;
     // Stage timing (CUDA events on the context stream), enabled by cunibs_context_set_timing.
     bool timing = false;
     cudaEvent_t ev[6] = {};
@@ -181,6 +203,9 @@ Params resolve(const cunibs_context* c, const cunibs_solve_opts* o) {
 }
 
 constexpr int kMaxBlock = 16;
+// Eigenvalues of a placement's Jacobi-scaled sensitivity Gram kept for its draw guesses, relative
+// to the largest (the reference keeps singular values above 1e-8 of the largest, run.py:108-123).
+constexpr double kSigmaRtol = 1e-12;
 
 void copy_out(void* dst, const void* src, std::size_t bytes, cudaMemcpyKind kind, cudaStream_t s);
 std::size_t slot_bytes(const cunibs_context* c, const cunibs_solve_opts* opts, int k);
@@ -193,6 +218,7 @@ std::size_t slot_bytes(const cunibs_context* c, const cunibs_solve_opts* opts, i
 long long prepare_block(cunibs_context* c, const double* pos, const double* mom, int n_dip, const double* centers,
                         const double* handles, const double* dists, int k, double didt, const cunibs_solve_opts* opts,
                         bool host_inputs, bool bounded_dadt) {
+    require(!c->study, "a conductivity study is open: end it (cunibs_sigma_end) before solving other blocks");
     require(k >= 1, "need at least one placement");
     require(n_dip >= 1, "the coil needs at least one dipole");
     require(pos && mom && centers && dists, "input arrays must not be NULL");
@@ -324,12 +350,13 @@ PendingBlock finish_block(cunibs_context* c, long long ticket, SolveStats& st, b
     CUNIBS_CHECK(cudaStreamWaitEvent(s, sl.prepared, 0));
     c->X.reserve(static_cast<std::size_t>(n_red) * K);
     const bool warm = opts && opts->warm_start;
+    const bool guessed = warm || pb.x0_given;
     if (pb.guess_due) issue_guess(c, pb);
     c->warm_used.assign(k, 0);
     c->init_rel.assign(k, 1.0);
-    solver_solve(*c->solver, sl.B.get(), c->X.get(), k, K, prm, s, st, warm ? sl.X0.get() : nullptr);
-    if (warm) {
-        warm_start_check(*c->warm, s);
+    solver_solve(*c->solver, sl.B.get(), c->X.get(), k, K, prm, s, st, guessed ? sl.X0.get() : nullptr);
+    if (guessed) {
+        if (warm) warm_start_check(*c->warm, s);
         for (int i = 0; i < k; ++i) {
             c->init_rel[i] = st.col_init_rel[i];
             c->warm_used[i] = st.col_init_rel[i] < 1.0 ? 1 : 0;
@@ -700,6 +727,7 @@ int cunibs_context_set_overlap(cunibs_context* c, int blocks_per_sm) {
 int cunibs_context_set_conductivity(cunibs_context* c, const double* sigma_by_tag) {
     return guarded([&] {
         require(c && sigma_by_tag, "NULL argument");
+        require(!c->study, "a conductivity study is open: its draws set the conductivities until cunibs_sigma_end");
         for (int t = 1; t <= 10; ++t) require(sigma_by_tag[t] > 0.0, "conductivities must be positive");
         require(c->pending.empty(), "finish the submitted blocks first");
         DeviceGuard dg(c->device);
@@ -711,6 +739,7 @@ int cunibs_context_set_conductivity(cunibs_context* c, const double* sigma_by_ta
 int cunibs_context_set_conductivity_keep_coarse(cunibs_context* c, const double* sigma_by_tag) {
     return guarded([&] {
         require(c && sigma_by_tag, "NULL argument");
+        require(!c->study, "a conductivity study is open: its draws set the conductivities until cunibs_sigma_end");
         for (int t = 1; t <= 10; ++t) require(sigma_by_tag[t] > 0.0, "conductivities must be positive");
         require(c->pending.empty(), "finish the submitted blocks first");
         DeviceGuard dg(c->device);
@@ -718,6 +747,237 @@ int cunibs_context_set_conductivity_keep_coarse(cunibs_context* c, const double*
         DevCsr<double> a0;
         reduce_grounded(c->mesh, a0, c->stream);
         if (!refresh_finest_level(c->hier, a0, c->stream)) c->rebuild_hierarchy();
+    });
+}
+
+int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                       const double* centers_mm, const double* handles_mm, const double* dists_mm, int k, double didt,
+                       const cunibs_solve_opts* opts, const double* sigma_nominal, const int* tags, int n_tags,
+                       double sensitivity_tol, int* basis_rank) {
+    return guarded([&] {
+        require(c && sigma_nominal && tags, "NULL argument");
+        require(dip_pos_m && dip_moment && centers_mm && dists_mm, "input arrays must not be NULL");
+        require(!c->study, "a conductivity study is already open");
+        require(c->pending.empty(), "finish the submitted blocks first");
+        require(n_tags >= 1 && n_tags <= kSigmaMaxTags, "between 1 and 10 perturbed tissues");
+        require(sensitivity_tol > 0.0 && sensitivity_tol < 1.0, "sensitivity_tol must be in (0, 1)");
+        require(!(opts && opts->warm_start), "a conductivity study starts its draws from its own guess: warm_start must be 0");
+        for (int t = 1; t <= 10; ++t)
+            require(sigma_nominal[t] > 0.0 && std::isfinite(sigma_nominal[t]), "nominal conductivities must be positive");
+        auto st = std::make_unique<SigmaStudy>();
+        SigmaSlots slots{};
+        for (int& v : slots.slot) v = -1;
+        for (int a = 0; a < n_tags; ++a) {
+            require(tags[a] >= 1 && tags[a] <= 10, "perturbed tags must be in [1, 10]");
+            require(slots.slot[tags[a]] < 0, "perturbed tags must be distinct");
+            slots.slot[tags[a]] = a;
+            st->tags[a] = tags[a];
+        }
+        const int P = st->P = n_tags;
+        std::copy(sigma_nominal, sigma_nominal + 11, st->nominal);
+        DeviceGuard dg(c->device);
+        Mesh& m = c->mesh;
+        cudaStream_t s = c->stream;
+        // The context at the nominal conductivities, its coarse levels kept.
+        {
+            assemble_stiffness(m, st->nominal, s);
+            DevCsr<double> a0;
+            reduce_grounded(m, a0, s);
+            if (!refresh_finest_level(c->hier, a0, s)) c->rebuild_hierarchy();
+        }
+        require(!c->hier.levels.empty(), "the operator is too small for a conductivity study (it has no AMG level)");
+        const Level& L0 = c->hier.levels[0];
+        st->nnz = L0.a.nnz;
+        // Operator components on the grounded pattern (assembly.py:99-125): the unperturbed tissues at
+        // nominal, then each perturbed tissue at unit conductivity.
+        st->comp.resize(static_cast<std::size_t>(1 + P) * st->nnz);
+        double table[11];
+        for (int t = 0; t < 11; ++t) table[t] = (t >= 1 && slots.slot[t] < 0) ? st->nominal[t] : 0.0;
+        assemble_reduced_values(m, table, st->nnz, st->comp.get(), s);
+        for (int a = 0; a < P; ++a) {
+            for (double& v : table) v = 0.0;
+            table[st->tags[a]] = 1.0;
+            assemble_reduced_values(m, table, st->nnz, st->comp.get() + static_cast<std::size_t>(1 + a) * st->nnz, s);
+        }
+        // The components must give back the nominal operator (the gate of assembly.py:126-131).
+        {
+            SigmaWeights w{};
+            for (int a = 0; a < P; ++a) w.w[a] = st->nominal[st->tags[a]];
+            DevArray<double> recon(st->nnz);
+            sigma_combine(st->comp.get(), P, st->nnz, w, recon.get(), s);
+            const double rel = sigma_relative_difference(recon.get(), L0.a.val.get(), st->nnz, s);
+            if (!(rel <= 1e-10))
+                fail(kEInternal, "conductivity decomposition mismatch (relative difference " + std::to_string(rel) + ")");
+        }
+        // The block's coil field, kept in its slot for every draw, and the nominal solution.
+        const long long ticket = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k,
+                                               didt, opts, true, false);
+        st->slot = c->pending.back().slot;
+        SolveStats ss;
+        const PendingBlock pb = finish_block(c, ticket, ss, false);
+        st->k = pb.k;
+        st->K = pb.K;
+        st->has_handles = pb.has_handles;
+        st->has_opts = pb.has_opts;
+        st->opts = pb.opts;
+        const int K = st->K, n_red = m.n_nodes - 1;
+        const std::size_t npk = static_cast<std::size_t>(n_red) * P * K;
+        st->x_nom.resize(static_cast<std::size_t>(n_red) * K);
+        CUNIBS_CHECK(cudaMemcpyAsync(st->x_nom.get(), c->X.get(), sizeof(double) * n_red * K, cudaMemcpyDeviceToDevice, s));
+        // Sensitivity right-hand sides c_t = b_t - A_t x_nom, and which are nonzero (a tissue with no
+        // element gives none).
+        const BlockSlot& sl = c->slots[st->slot];
+        DevArray<double> C(npk);
+        sigma_sens_rhs(m, st->x_nom.get(), sl.dadt_elm.get(), st->k, K, slots, P, C.get(), s);
+        const std::vector<double> cc = sigma_gram(C.get(), C.get(), n_red, P, K, s);
+        std::vector<int> active(static_cast<std::size_t>(P) * K, 0);
+        std::vector<std::pair<int, int>> cols;
+        for (int j = 0; j < st->k; ++j)
+            for (int a = 0; a < P; ++a)
+                if (cc[(static_cast<std::size_t>(j) * P + a) * P + a] > 0.0) {
+                    active[static_cast<std::size_t>(j) * P + a] = 1;
+                    cols.emplace_back(a, j);
+                }
+        // Sensitivities s_t = A_nom^-1 c_t to a loose tolerance (run.py:44-49: they only span the
+        // guess's subspace; every draw is still solved to the full tolerance), 16 columns at a time.
+        st->S.resize(npk);
+        st->S.zero(s);
+        if (!cols.empty()) {
+            Params sp = resolve(c, opts);
+            sp.tolerance = sensitivity_tol;
+            DevArray<double> B16(static_cast<std::size_t>(n_red) * 16), X16(static_cast<std::size_t>(n_red) * 16);
+            for (std::size_t q0 = 0; q0 < cols.size(); q0 += 16) {
+                SigmaColumns cm{};
+                cm.count = static_cast<int>(std::min<std::size_t>(16, cols.size() - q0));
+                for (int l = 0; l < cm.count; ++l) {
+                    cm.a[l] = cols[q0 + l].first;
+                    cm.j[l] = cols[q0 + l].second;
+                }
+                sigma_pack(C.get(), n_red, P, K, cm, B16.get(), s);
+                SolveStats s16;
+                solver_solve(*c->solver, B16.get(), X16.get(), cm.count, 16, sp, s, s16);
+                sigma_unpack(X16.get(), n_red, P, K, cm, st->S.get(), s);
+            }
+        }
+        // Per placement: the A_nom-Gram of its sensitivities and their products with the c_t give
+        // the map from a draw's conductivity change to its subspace coefficients.
+        DevArray<double> AS(npk);
+        sigma_spmv(L0.a, st->S.get(), P * K, AS.get(), s);
+        const std::vector<double> G = sigma_gram(st->S.get(), AS.get(), n_red, P, K, s);
+        const std::vector<double> H = sigma_gram(st->S.get(), C.get(), n_red, P, K, s);
+        st->Z.assign(static_cast<std::size_t>(K) * P * P, 0.0);
+        st->rank.assign(st->k, 0);
+        const std::size_t pp = static_cast<std::size_t>(P) * P;
+        for (int j = 0; j < st->k; ++j)
+            st->rank[j] = sigma_coefficients(P, &G[j * pp], &H[j * pp], &active[static_cast<std::size_t>(j) * P],
+                                             kSigmaRtol, &st->Z[j * pp]);
+        if (basis_rank)
+            for (int j = 0; j < st->k; ++j) basis_rank[j] = st->rank[j];
+        c->study = std::move(st);
+    });
+}
+
+int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* out, int* resetup) {
+    return guarded([&] {
+        require(c && sigma && out, "NULL argument");
+        require(out->transforms && out->summary, "out->transforms and out->summary are required");
+        require(c->study != nullptr, "no conductivity study is open (cunibs_sigma_begin)");
+        SigmaStudy& st = *c->study;
+        const int P = st.P, k = st.k, K = st.K;
+        double table[11];
+        std::copy(st.nominal, st.nominal + 11, table);
+        SigmaWeights w{};
+        double dsig[kSigmaMaxTags] = {};
+        for (int a = 0; a < P; ++a) {
+            require(sigma[a] > 0.0 && std::isfinite(sigma[a]), "conductivities must be positive");
+            table[st.tags[a]] = sigma[a];
+            w.w[a] = sigma[a];
+            dsig[a] = sigma[a] - st.nominal[st.tags[a]];
+        }
+        SigmaDraw y{};
+        for (int j = 0; j < k; ++j)
+            for (int a = 0; a < P; ++a) {
+                double v = 0.0;
+                for (int t = 0; t < P; ++t) v += st.Z[(static_cast<std::size_t>(j) * P + a) * P + t] * dsig[t];
+                y.y[a * 16 + j] = v;
+            }
+        DeviceGuard dg(c->device);
+        Mesh& m = c->mesh;
+        cudaStream_t s = c->stream;
+        const int n_red = m.n_nodes - 1;
+        // The draw's finest operator (K(sigma) = K_base + sum sigma_t K_t), its smoother weights and
+        // the right-hand side weights; the coarse levels stay the nominal ones (run.py:244-247).
+        sigma_combine(st.comp.get(), P, st.nnz, w, c->hier.levels[0].a.val.get(), s);
+        refresh_finest_derived(c->hier, s);
+        set_element_conductivity(m, table, s);
+        BlockSlot& sl = c->slots[st.slot];
+        rhs_block(m, sl.dadt_elm.get(), k, K, sl.B.get(), s);
+        sl.X0.reserve(static_cast<std::size_t>(n_red) * K);
+        sigma_guess(st.x_nom.get(), st.S.get(), n_red, P, K, k, y, sl.X0.get(), s);
+        auto queue = [&] {
+            PendingBlock pb;
+            pb.slot = st.slot;
+            pb.k = k;
+            pb.K = K;
+            pb.has_handles = st.has_handles;
+            pb.has_opts = st.has_opts;
+            pb.opts = st.opts;
+            pb.x0_given = true;
+            pb.ticket = c->next_ticket++;
+            c->pending.push_back(pb);
+            return pb.ticket;
+        };
+        auto nominal_hierarchy = [&] {
+            assemble_stiffness(m, st.nominal, s);
+            c->rebuild_hierarchy();
+        };
+        SolveStats ss;
+        PendingBlock done;
+        int redone = 0;
+        try {
+            done = finish_block(c, queue(), ss, out->E != nullptr);
+        } catch (const Error& e) {
+            if (e.code != kENoConv) throw;
+            // The nominal coarse levels were too far from this draw: solve it against a hierarchy
+            // of its own (run.py:356-366), then rebuild the nominal one.
+            assemble_stiffness(m, table, s);
+            c->rebuild_hierarchy();
+            ss = SolveStats{};
+            try {
+                done = finish_block(c, queue(), ss, out->E != nullptr);
+            } catch (...) {
+                nominal_hierarchy();
+                throw;
+            }
+            nominal_hierarchy();
+            redone = 1;
+        }
+        block_outputs_host(c, done, ss, out);
+        if (resetup) *resetup = redone;
+    });
+}
+
+int cunibs_sigma_end(cunibs_context* c) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        if (!c->study) return;
+        DeviceGuard dg(c->device);
+        const std::unique_ptr<SigmaStudy> st = std::move(c->study);
+        assemble_stiffness(c->mesh, st->nominal, c->stream);
+        DevCsr<double> a0;
+        reduce_grounded(c->mesh, a0, c->stream);
+        if (!refresh_finest_level(c->hier, a0, c->stream)) c->rebuild_hierarchy();
+    });
+}
+
+int cunibs_sigma_coefficients(int n_tags, const double* gram, const double* proj, const int* active, double rtol,
+                              double* coef, int* rank) {
+    return guarded([&] {
+        require(gram && proj && active && coef, "NULL argument");
+        require(n_tags >= 1 && n_tags <= kSigmaMaxTags, "between 1 and 10 perturbed tissues");
+        require(rtol >= 0.0 && rtol < 1.0, "rtol must be in [0, 1)");
+        const int r = sigma_coefficients(n_tags, gram, proj, active, rtol, coef);
+        if (rank) *rank = r;
     });
 }
 

@@ -128,12 +128,21 @@ struct Mesh {
 void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, const int* tags, int n_tets,
                 const int* skin, int n_skin, cudaStream_t s);
 void assemble_stiffness(Mesh& m, const double* sigma_by_tag /* 11 entries or null */, cudaStream_t s);
+// Per-element conductivity and right-hand side weights of a conductivity table (11 entries).
+void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s);
+// Grounded (reduced) stiffness values of a conductivity table whose entries may be zero, into
+// out (nnz_red), without touching the mesh's own values; the table's linearity in sigma makes a
+// table with one unit entry give that tissue's share of the operator.
+void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, long nnz_red, double* out, cudaStream_t s);
 void reduce_grounded(const Mesh& m, DevCsr<double>& out, cudaStream_t s);
 
 // Hierarchy (setup_amg.cu).
 int select_size4(int n, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s);
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& p, cudaStream_t s);
 bool refresh_finest_level(Hierarchy& h, const DevCsr<double>& a0, cudaStream_t s);
+// The finest level's l1 smoother weights and FP32 copies, after its FP64 values were rewritten in
+// place (queued on s, no synchronisation).
+void refresh_finest_derived(Hierarchy& h, cudaStream_t s);
 void spgemm(const DevCsr<double>& A, const DevCsr<double>& B, DevCsr<double>& C, cudaStream_t s);
 void transpose(const DevCsr<double>& A, DevCsr<double>& T, cudaStream_t s);
 void l1_dinv(const DevCsr<double>& a, DevArray<double>& dinv, cudaStream_t s);
@@ -279,5 +288,42 @@ const int* recovery_slot_of_corner(const Mesh& m, const RecoveryOp& op);
 // Harmonic reads the solver block x_red (N-1, K) and dadt_nodes (k,N,3); SPR reads e_elem (k,M,3).
 void apply_recovery(const Mesh& m, const RecoveryOp& op, const double* x_red, int K, const float* dadt_nodes,
                     const float* e_elem, int k, float* e_slots, float* E, float* magn, cudaStream_t s);
+
+// Conductivity Monte Carlo (sigma.cu): per-draw operator values and the sensitivity-subspace guess.
+constexpr int kSigmaMaxTags = 10;
+struct SigmaWeights {
+    double w[kSigmaMaxTags];  // conductivity of each perturbed tissue, in study order
+};
+struct SigmaSlots {
+    int slot[11];  // study position of each tissue tag, -1 for a tag that is not perturbed
+};
+struct SigmaColumns {
+    int a[16], j[16];  // (tissue position, placement) of each lane of a 16-wide solve block
+    int count;
+};
+struct SigmaDraw {
+    double y[kSigmaMaxTags * 16];  // subspace coefficients, y[a * 16 + j]
+};
+// Values of the finest operator for one draw: comp[0] + sum_t w_t comp[1 + t] (comp (1 + n_tags, nnz)).
+void sigma_combine(const double* comp, int n_tags, long nnz, const SigmaWeights& w, double* out, cudaStream_t s);
+// Sensitivity right-hand sides c_t of the nominal potential x_red (n_red, K): c_out (n_red, P, K).
+void sigma_sens_rhs(const Mesh& m, const double* x_red, const float* dadt_elm, int k, int K, const SigmaSlots& slots,
+                    int P, double* c_out, cudaStream_t s);
+// Per-placement Gram blocks of two (n, P, K) arrays, (K, P, P) on the host; depends on n, not on K.
+std::vector<double> sigma_gram(const double* U, const double* V, long n, int P, int K, cudaStream_t s);
+// Y (n, W) = A X (n, W) in FP64.
+void sigma_spmv(const DevCsr<double>& A, const double* X, int W, double* Y, cudaStream_t s);
+void sigma_pack(const double* C, int n, int P, int K, const SigmaColumns& cm, double* B16, cudaStream_t s);
+void sigma_unpack(const double* X16, int n, int P, int K, const SigmaColumns& cm, double* S, cudaStream_t s);
+// X0 (n, K) = x_nom + S y per placement.
+void sigma_guess(const double* x_nom, const double* S, int n, int P, int K, int k, const SigmaDraw& y, double* X0,
+                 cudaStream_t s);
+// ||a - b|| / ||b|| over n entries (synchronises s).
+double sigma_relative_difference(const double* a, const double* b, long n, cudaStream_t s);
+// Host: the draw-coefficient map of one placement. gram (P, P) = S^T A S and proj (P, P) with
+// proj[a][t] = s_a . c_t over the active positions; Z (P, P) with y = Z (sigma - sigma_nom) the
+// A-Galerkin coefficients of the linearised residual. Returns the rank kept (eigenvalues of the
+// Jacobi-scaled Gram above rtol times the largest).
+int sigma_coefficients(int P, const double* gram, const double* proj, const int* active, double rtol, double* Z);
 
 }  // namespace cunibs

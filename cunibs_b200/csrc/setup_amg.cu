@@ -685,12 +685,17 @@ bool refresh_finest_level(Hierarchy& h, const DevCsr<double>& a0, cudaStream_t s
     Level& L = h.levels[0];
     if (L.a.n != a0.n || L.a.nnz != a0.nnz) return false;
     CUNIBS_CHECK(cudaMemcpyAsync(L.a.val.get(), a0.val.get(), sizeof(double) * a0.nnz, cudaMemcpyDeviceToDevice, s));
+    refresh_finest_derived(h, s);
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    return true;
+}
+
+void refresh_finest_derived(Hierarchy& h, cudaStream_t s) {
+    Level& L = h.levels[0];
     l1_dinv(L.a, L.dinv, s);
     to_f32(L.a.val, L.a.nnz, L.a32, s);
     to_f32(L.dinv, L.n, L.dinv32, s);
     CUNIBS_LAUNCH_CHECK("refresh finest level");
-    CUNIBS_CHECK(cudaStreamSynchronize(s));
-    return true;
 }
 
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& prm, cudaStream_t s) {

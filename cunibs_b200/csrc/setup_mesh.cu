@@ -603,17 +603,19 @@ void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, c
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 
+void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
+    CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
+    DevArray<int> bad(1);
+    bad.zero(s);
+    conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, m.cond.get(), bad.get()); count_launch();
+    if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
+    // The right-hand side weighs each element by the same conductivity.
+    neg_vc_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.vols32.get(), m.cond.get(), m.n_tets, m.neg_vc32.get());
+    count_launch();
+}
+
 void assemble_stiffness(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
-    if (sigma_by_tag != nullptr) {
-        CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
-        DevArray<int> bad(1);
-        bad.zero(s);
-        conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, m.cond.get(), bad.get()); count_launch();
-        if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
-        // The right-hand side weighs each element by the same conductivity.
-        neg_vc_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.vols32.get(), m.cond.get(), m.n_tets, m.neg_vc32.get());
-        count_launch();
-    }
+    if (sigma_by_tag != nullptr) set_element_conductivity(m, sigma_by_tag, s);
     const std::int64_t Q = 16 * static_cast<std::int64_t>(m.n_tets);
     DevArray<double> ev(Q);
     element_products_kernel<<<grid_for(Q), kBlock, 0, s>>>(m.g.get(), m.vols.get(), m.cond.get(), m.n_tets, ev.get()); count_launch();
@@ -621,6 +623,34 @@ void assemble_stiffness(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
     segmented_sum_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(ev.get(), m.contrib_ptr.get(), m.contrib_idx.get(),
                                                               m.k_nnz, m.k_val.get()); count_launch();
     CUNIBS_LAUNCH_CHECK("stiffness values");
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+}
+
+void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, long nnz_red, double* out, cudaStream_t s) {
+    CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
+    const int M = m.n_tets;
+    DevArray<double> cond(M);
+    DevArray<int> bad(1);
+    bad.zero(s);
+    conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), M, cond.get(), bad.get()); count_launch();
+    if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
+    const std::int64_t Q = 16 * static_cast<std::int64_t>(M);
+    DevArray<double> ev(Q), full(m.k_nnz);
+    element_products_kernel<<<grid_for(Q), kBlock, 0, s>>>(m.g.get(), m.vols.get(), cond.get(), M, ev.get()); count_launch();
+    segmented_sum_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(ev.get(), m.contrib_ptr.get(), m.contrib_idx.get(),
+                                                              m.k_nnz, full.get()); count_launch();
+    // The grounded pattern keeps each row's entries in order minus the ground column, so the
+    // reduced values are the full values with the ground row and column dropped.
+    DevArray<int> cnt(m.n_nodes), rptr(m.n_nodes);
+    CUNIBS_CHECK(cudaMemsetAsync(cnt.get() + (m.n_nodes - 1), 0, sizeof(int), s));
+    reduced_count_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), m.n_nodes, m.ground,
+                                                                    cnt.get()); count_launch();
+    exclusive_scan(cnt.get(), rptr.get(), m.n_nodes, s);
+    if (read_int(rptr.get() + (m.n_nodes - 1), s) != nnz_red) fail(kEInternal, "reduced stiffness pattern mismatch");
+    DevArray<int> rcol(nnz_red);
+    reduced_fill_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), full.get(), m.n_nodes,
+                                                                   m.ground, rptr.get(), rcol.get(), out); count_launch();
+    CUNIBS_LAUNCH_CHECK("reduced stiffness values");
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 

@@ -286,7 +286,9 @@ class Subject:
 
         Every draw of ``config`` (:class:`cunibs_b200.uq.ConductivityUQConfig`) re-weights the
         stiffness and right-hand side and solves the placement to the subject's tolerance; the
-        AMG hierarchy stays the nominal one (only its finest level follows the draw). Each
+        AMG hierarchy stays the nominal one (only its finest level follows the draw), the coil
+        field is evaluated once, and PCG starts from the nominal solution corrected within the
+        span of its conductivity sensitivities (cunibs_sigma_begin / cunibs_sigma_draw). Each
         :class:`cunibs_b200.uq.ConductivityUQResult` carries the per-draw gray-matter peak,
         focality (stimulated volume at ``focality_frac`` x p99.9, 0.5 or 0.75) and peak location;
         ``moments=True`` adds per-tetrahedron mean/std/cov of |E| and the summary of the mean field.
@@ -318,66 +320,58 @@ class Subject:
         f_col = 14 if focality_frac == 0.5 else 15
         host = self._host_metric_inputs() if moments else None
         n = config.n_samples
-        try:
-            # Every placement sees the same draws, so a chunk of up to MAX_BLOCK placements shares
-            # each draw's re-setup and one block solve; a placement's result does not depend on its
-            # block-mates, so it is the one a run of that placement alone gives.
-            for start in range(0, len(sites), MAX_BLOCK):
-                chunk = sites[start:start + MAX_BLOCK]
-                k = len(chunk)
-                centers = np.stack([s.center_mm for s in chunk])
-                handles = np.stack([s.handle_mm for s in chunk])
-                dists = np.array([s.distance_mm for s in chunk])
-                peak = np.empty((k, n))
-                foc = np.empty((k, n))
-                loc = np.empty((k, n, 3))
-                its = np.empty((k, n), np.int32)
-                s1 = s2 = None
-                resetups = np.zeros(k, np.int64)
-                for i in range(n):
-                    sigma = nominal.copy()
-                    sigma[list(tags)] = draws[i]
-                    with self._lock:
-                        ctx.set_conductivity(sigma, keep_coarse=True)
-                        args = (coil, centers, handles, dists, didt)
-                        try:
-                            out = ctx.solve_block(*args, magnitude=moments, recovery=recovery)
-                        except _native.ConvergenceFailure:
-                            # The nominal preconditioner was too far from this draw: solve it
-                            # against its own hierarchy, then rebuild the nominal one.
-                            ctx.set_conductivity(sigma)
-                            try:
-                                out = ctx.solve_block(*args, magnitude=moments, recovery=recovery)
-                            except _native.ConvergenceFailure as exc:
-                                raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
-                            finally:
-                                ctx.set_conductivity(nominal)
-                            resetups += 1
-                    rows = out["summary"]
-                    peak[:, i], foc[:, i], loc[:, i], its[:, i] = rows[:, 0], rows[:, f_col], rows[:, 1:4], out["iterations"]
-                    if moments:
-                        m = out["magnE"].astype(np.float64)
-                        s1 = m.copy() if s1 is None else s1 + m
-                        s2 = m * m if s2 is None else s2 + m * m
-                for j, site in enumerate(chunk):
-                    mean = std = cov = None
-                    if moments:
-                        mean = s1[j] / n
-                        std = np.sqrt(np.maximum(s2[j] / n - mean * mean, 0.0))
-                        cov = np.divide(std, mean, out=np.zeros_like(std), where=mean > 0)
-                    res = uq.ConductivityUQResult(
-                        mean_magnE=mean, std_magnE=std, cov_magnE=cov, n_samples=n, perturbed_tags=tags,
-                        sigma_samples=draws, vols=host[0] if host else None, tet_tags=host[1] if host else None,
-                        barycenters_mm=host[2] if host else None, placement=site, coil_name=coil.name, didt=didt,
-                        peak_samples=peak[j], focality_samples=foc[j], peak_location_samples=loc[j],
-                        iteration_samples=its[j], recovery=recovery, full_resetups=int(resetups[j]))
-                    if moments:
-                        res.summary = res.compute_summary()
-                    yield res
-        finally:
+        # Every placement sees the same draws, so a chunk of up to MAX_BLOCK placements shares each
+        # draw's operator update and one block solve; a placement's result does not depend on its
+        # block-mates, so it is the one a run of that placement alone gives.
+        for start in range(0, len(sites), MAX_BLOCK):
+            chunk = sites[start:start + MAX_BLOCK]
+            k = len(chunk)
+            centers = np.stack([s.center_mm for s in chunk])
+            handles = np.stack([s.handle_mm for s in chunk])
+            dists = np.array([s.distance_mm for s in chunk])
+            peak = np.empty((k, n))
+            foc = np.empty((k, n))
+            loc = np.empty((k, n, 3))
+            its = np.empty((k, n), np.int32)
+            s1 = s2 = None
+            resetups = 0
+            # The study holds the chunk's coil field, nominal solution and sensitivities; each draw
+            # swaps the finest operator's values and starts PCG from the sensitivity-subspace guess.
             with self._lock:
-                if self._ctx is ctx:
-                    ctx.set_conductivity(nominal, keep_coarse=True)
+                try:
+                    ctx.sigma_begin(coil, centers, handles, dists, didt, nominal, tags, magnitude=moments,
+                                    recovery=recovery)
+                    for i in range(n):
+                        try:
+                            out = ctx.sigma_draw(draws[i])
+                        except _native.ConvergenceFailure as exc:
+                            raise SolverConvergenceError.from_native(str(exc), self._tolerance) from exc
+                        resetups += out["resetup"]
+                        rows = out["summary"]
+                        peak[:, i], foc[:, i], loc[:, i] = rows[:, 0], rows[:, f_col], rows[:, 1:4]
+                        its[:, i] = out["iterations"]
+                        if moments:
+                            m = out["magnE"].astype(np.float64)
+                            s1 = m.copy() if s1 is None else s1 + m
+                            s2 = m * m if s2 is None else s2 + m * m
+                finally:
+                    if self._ctx is ctx:
+                        ctx.sigma_end()
+            for j, site in enumerate(chunk):
+                mean = std = cov = None
+                if moments:
+                    mean = s1[j] / n
+                    std = np.sqrt(np.maximum(s2[j] / n - mean * mean, 0.0))
+                    cov = np.divide(std, mean, out=np.zeros_like(std), where=mean > 0)
+                res = uq.ConductivityUQResult(
+                    mean_magnE=mean, std_magnE=std, cov_magnE=cov, n_samples=n, perturbed_tags=tags,
+                    sigma_samples=draws, vols=host[0] if host else None, tet_tags=host[1] if host else None,
+                    barycenters_mm=host[2] if host else None, placement=site, coil_name=coil.name, didt=didt,
+                    peak_samples=peak[j], focality_samples=foc[j], peak_location_samples=loc[j],
+                    iteration_samples=its[j], recovery=recovery, full_resetups=resetups)
+                if moments:
+                    res.summary = res.compute_summary()
+                yield res
 
     def simulate_conductivity_uq(self, coil: Coil, placement: Placement, config, didt: float = 1e6, *,
                                  moments: bool = False, recovery: str = "harmonic", focality_frac: float = 0.5):

@@ -1,13 +1,16 @@
 """Monte Carlo conductivity uncertainty for one or more coil placements (reference uq/conductivity).
 
 Every draw re-weights the stiffness and right-hand side by sampled tissue conductivities and solves
-the placement again. The context's AMG hierarchy stays the one built at the nominal conductivities;
-only the finest level's values and smoother weights follow each draw
-(``cunibs_context_set_conductivity_keep_coarse``), which is the reference's frozen-preconditioner
-scheme (uq/conductivity/assembly.py:1-70, run.py:203-387). PCG still solves each draw's operator to
-the subject's tolerance, so the preconditioner only changes the iteration count; a draw that misses
-the tolerance is solved again after a full re-setup for it, and the nominal hierarchy is then
-rebuilt, so accuracy never depends on the preconditioner tracking the draw.
+the placement again (the native study, ``cunibs_sigma_begin`` / ``cunibs_sigma_draw``). The
+stiffness is a fixed sum of per-tissue components, so a draw's operator is one combination of them;
+the context's AMG hierarchy stays the one built at the nominal conductivities, only the finest
+level's values and smoother weights following each draw, which is the reference's
+frozen-preconditioner scheme (uq/conductivity/assembly.py:1-70, run.py:203-387). Each draw starts
+from the nominal solution plus the Galerkin projection of its residual onto the span of the
+solution's conductivity sensitivities (run.py:105-200). PCG still solves each draw's operator to
+the subject's tolerance, so the preconditioner and the guess only change the iteration count; a
+draw that misses the tolerance is solved again after a full re-setup for it, and the nominal
+hierarchy is then rebuilt, so accuracy never depends on the preconditioner tracking the draw.
 """
 
 from __future__ import annotations

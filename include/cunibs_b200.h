@@ -205,6 +205,45 @@ int cunibs_context_set_conductivity(cunibs_context* ctx, const double* sigma_by_
  * the tolerance is the caller's cue for cunibs_context_set_conductivity. */
 int cunibs_context_set_conductivity_keep_coarse(cunibs_context* ctx, const double* sigma_by_tag);
 
+/* --- conductivity Monte Carlo of one block of placements (uq/conductivity/run.py:203-387) ---- */
+
+/* Opens a study (replaces build_conductivity_uq_precompute, uq/conductivity/assembly.py:73-140, and
+ * the per-placement set-up of run_conductivity_uq, run.py:236-314): sets the context to
+ * sigma_nominal (11 entries, index = tag; coarse AMG levels kept), splits the grounded stiffness
+ * into the unperturbed tissues plus one unit-conductivity component per tag in tags[0..n_tags)
+ * (checked to give back the nominal operator to 1e-10), places the k coil placements and
+ * evaluates their dA/dt once, solves the nominal block, and solves for the sensitivity of each
+ * placement's potential to each perturbed conductivity to sensitivity_tol (the reference uses
+ * 1e-3, run.py:44-49). basis_rank (k, may be NULL) receives the dimension of each placement's
+ * sensitivity subspace. opts as for cunibs_solve_block (warm_start must be 0). Until
+ * cunibs_sigma_end, block solves and cunibs_context_set_conductivity* are refused. */
+int cunibs_sigma_begin(cunibs_context* ctx, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                       const double* centers_mm, const double* handles_mm, const double* dists_mm, int k, double didt,
+                       const cunibs_solve_opts* opts, const double* sigma_nominal, const int* tags, int n_tags,
+                       double sensitivity_tol, int* basis_rank);
+
+/* One draw (the loop body of run.py:324-380): sigma (n_tags, in the order of tags) replaces the
+ * perturbed conductivities; the finest operator becomes the components' combination (its smoother
+ * weights follow, the coarse levels stay nominal), the right-hand side is re-weighted from the held
+ * dA/dt, and PCG starts from the nominal potential plus the A-Galerkin projection of the draw's
+ * linearised residual onto the sensitivity subspace (run.py:157-200), then runs to the study's
+ * tolerance. A draw the kept coarse levels cannot finish is solved again on a hierarchy built for
+ * it, after which the nominal hierarchy is rebuilt; *resetup (may be NULL) is then 1. Outputs as
+ * cunibs_solve_block (host buffers); out->init_relres is the guess's relative residual. */
+int cunibs_sigma_draw(cunibs_context* ctx, const double* sigma, cunibs_block_out* out, int* resetup);
+
+/* Closes the study and returns the context to the nominal conductivities (the same operator and
+ * hierarchy values as before cunibs_sigma_begin). A no-op when no study is open. */
+int cunibs_sigma_end(cunibs_context* ctx);
+
+/* The host step behind a placement's draw guess, exposed for testing: gram (n_tags, n_tags) =
+ * S^T A S of the sensitivities, proj (n_tags, n_tags) with proj[a][t] = s_a . c_t, active[a] = 0
+ * for a tissue with no sensitivity. coef (n_tags, n_tags) receives Z with the subspace coefficients
+ * y = Z (sigma - sigma_nominal): Z = G^+ proj, G^+ the pseudo-inverse of the Gram over its
+ * Jacobi-scaled eigenvalues above rtol times the largest; *rank (may be NULL) the count kept. */
+int cunibs_sigma_coefficients(int n_tags, const double* gram, const double* proj, const int* active, double rtol,
+                              double* coef, int* rank);
+
 /* --- stage-level entry points (the reference's kernel exports, bindings.cpp) --------------- */
 
 /* Copies a named internal array to host memory. name / dtype:

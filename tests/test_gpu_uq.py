@@ -1,8 +1,9 @@
-"""Conductivity Monte Carlo on the GPU (Subject.simulate_conductivity_uq). Needs a B200.
+"""Conductivity Monte Carlo on the GPU (Subject.simulate_conductivity_uq, cunibs_sigma_*). Needs a B200.
 
-Each draw is solved with the nominal coarse AMG levels kept; its gray-matter peak must match a
-solve after a full re-setup for that draw, the moments must be the draws' mean and spread, and the
-subject must be back at the nominal conductivities afterwards, bit for bit.
+Each draw is solved with the nominal coarse AMG levels kept, from the sensitivity-subspace guess;
+its gray-matter peak must match a solve after a full re-setup for that draw, the moments must be
+the draws' mean and spread, and the subject must be back at the nominal conductivities afterwards,
+bit for bit.
 """
 
 from __future__ import annotations
@@ -91,4 +92,44 @@ def test_placements_batched_per_draw_match_single_runs():
         np.testing.assert_array_equal(r.iteration_samples, alone.iteration_samples)
         np.testing.assert_array_equal(r.mean_magnE, alone.mean_magnE)
         assert r.placement is site
+    subj.free()
+
+
+def test_study_guess_cuts_iterations_against_the_zero_guess_on_the_same_hierarchy():
+    """cunibs_sigma_draw against cunibs_context_set_conductivity_keep_coarse + a zero-guess block
+    solve of the same draw: the same operator and coarse levels, so the same field to the solve
+    tolerance; the sensitivity-subspace guess starts well below the zero guess's residual and
+    needs fewer iterations."""
+    mesh = sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(64)
+    centers = np.array([[0.0, 0.0, 90.0], [25.0, 0.0, 86.4]])
+    handles = centers + [0.0, 50.0, 0.0]
+    dists = [4.0, 4.0]
+    subj = Subject(mesh, tolerance=1e-8)
+    ctx = subj.context
+    nominal = nominal_sigma_table()
+    tags = tuple(int(t) for t in np.unique(mesh.tet_tags))
+    draws = sample_conductivities(ConductivityUQConfig(n_samples=3, seed=5), tags)
+    ranks = ctx.sigma_begin(coil, centers, handles, dists, 1e6, nominal, tags, magnitude=True, recovery="raw")
+    assert (ranks >= 1).all() and (ranks <= len(tags)).all()
+    with pytest.raises(ValueError, match="conductivity study is open"):
+        ctx.solve_block(coil, centers, handles, dists, 1e6)
+    with pytest.raises(ValueError, match="conductivity study is open"):
+        ctx.set_conductivity(nominal)
+    outs = [ctx.sigma_draw(d) for d in draws]
+    ctx.sigma_end()
+    with pytest.raises(ValueError, match="no conductivity study"):
+        ctx.sigma_draw(draws[0])
+    for d, o in zip(draws, outs):
+        sigma = nominal.copy()
+        sigma[list(tags)] = d
+        ctx.set_conductivity(sigma, keep_coarse=True)
+        ref = ctx.solve_block(coil, centers, handles, dists, 1e6, magnitude=True, recovery="raw")
+        assert o["resetup"] == 0
+        assert (o["init_relres"] < 0.2).all(), o["init_relres"]
+        assert (o["iterations"] <= ref["iterations"]).all() and o["iterations"].sum() < ref["iterations"].sum()
+        np.testing.assert_allclose(o["summary"][:, 0], ref["summary"][:, 0], rtol=1e-6)
+        diff = np.linalg.norm(o["magnE"] - ref["magnE"], axis=1) / np.linalg.norm(ref["magnE"], axis=1)
+        assert (diff < 1e-6).all(), diff
+    ctx.set_conductivity(nominal, keep_coarse=True)
     subj.free()
