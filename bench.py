@@ -347,6 +347,8 @@ def run_ours(args) -> dict:
     h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
     d2h = res["transform"].nbytes + res["summary"].nbytes + res["iterations"].nbytes + res["relative_residual"].nbytes
 
+    draws = conductivity_draws(ctx, coil, centers[:4], handles[:4], dists[:4], args.recovery, stream)
+
     # Roofline of the SpMV-dominated iteration (solve stage).
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
     hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
@@ -412,6 +414,7 @@ def run_ours(args) -> dict:
         "dadt": {"pair_evals_per_step": int(pair_evals), "ms": round(dadt_ms, 4),
                  "gpair_per_s": round(pair_evals / (dadt_ms / 1e3) / 1e9, 2)},
         "setup_s": round(setup_s, 3),
+        "conductivity_draws": draws,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -419,6 +422,69 @@ def run_ours(args) -> dict:
     if dist is not None:
         dist.destroy_process_group()
     return line if rank == 0 else None
+
+
+def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_draws=12, seed=0) -> dict:
+    """Conductivity Monte Carlo on the same mesh: every tissue's conductivity lognormal with the
+    table value as median and log-sd 0.25 (seeded), one block of the first 4 placements. The study
+    (cunibs_sigma_begin once, then cunibs_sigma_draw per draw: operator components, coil field held,
+    sensitivity-subspace guess) against a keep-coarse re-assembly and a zero-guess block solve per
+    draw. Device time on the library stream around all draws (host API, outputs copied back each
+    draw); L2 not flushed."""
+    import torch
+
+    from cunibs_b200.uq import nominal_sigma_table
+
+    nominal = nominal_sigma_table()
+    tags = tuple(range(1, 11))
+    rng = np.random.default_rng(seed)
+    sig = nominal[list(tags)] * np.exp(0.25 * rng.standard_normal((n_draws, len(tags))))
+    k = centers.shape[0]
+
+    def device_ms(fn):
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        out = fn()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    def keep_coarse():
+        its = []
+        for s in sig:
+            table = nominal.copy()
+            table[list(tags)] = s
+            ctx.set_conductivity(table, keep_coarse=True)
+            its.append(ctx.solve_block(coil, centers, handles, dists, 1e6, recovery=recovery)["iterations"].mean())
+        ctx.set_conductivity(nominal, keep_coarse=True)
+        return its
+
+    def study():
+        its, rel0 = [], []
+        for s in sig:
+            r = ctx.sigma_draw(s)
+            its.append(r["iterations"].mean())
+            rel0.append(float(r["init_relres"].max()))
+        return its, rel0
+
+    old_ms, old_its = device_ms(keep_coarse)
+    begin_ms, ranks = device_ms(lambda: ctx.sigma_begin(coil, centers, handles, dists, 1e6, nominal, tags,
+                                                        recovery=recovery))
+    try:
+        new_ms, (new_its, rel0) = device_ms(study)
+    finally:
+        ctx.sigma_end()
+    return {"what": f"{n_draws} draws x {k} placements, 10 tissues lognormal (median = table, log-sd 0.25)",
+            "study_ms_per_draw": round(new_ms / n_draws, 4), "study_iterations": round(float(np.mean(new_its)), 2),
+            "study_begin_ms": round(begin_ms, 3), "subspace_rank": ranks.tolist(),
+            "guess_init_relres_max": round(max(rel0), 6),
+            "keep_coarse_zero_guess_ms_per_draw": round(old_ms / n_draws, 4),
+            "keep_coarse_iterations": round(float(np.mean(old_its)), 2),
+            "placement_draws_per_s": round(k * n_draws / (new_ms / 1e3), 2),
+            "ratio": round(old_ms / new_ms, 3)}
 
 
 def cpu_baseline(mesh, coil, sites, recovery, n_place=1) -> dict:
