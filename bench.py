@@ -464,10 +464,13 @@ def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_d
 
     def study():
         its, rel0 = [], []
+        # An NVTX range around the draws lets a profiler capture exactly their launches.
+        torch.cuda.nvtx.range_push("conductivity_draws")
         for s in sig:
             r = ctx.sigma_draw(s)
             its.append(r["iterations"].mean())
             rel0.append(float(r["init_relres"].max()))
+        torch.cuda.nvtx.range_pop()
         return its, rel0
 
     old_ms, old_its = device_ms(keep_coarse)

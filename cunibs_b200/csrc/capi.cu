@@ -155,6 +155,19 @@ struct cunibs_context {
         return *rec[mode];
     }
 
+    // The finest level takes the mesh's current stiffness values (same pattern), its smoother
+    // weights and FP32 copies follow; coarser levels are kept. Without levels: a full rebuild.
+    void keep_coarse_values() {
+        if (hier.levels.empty()) {
+            rebuild_hierarchy();
+            return;
+        }
+        Level& L0 = hier.levels[0];
+        reduce_grounded_values(mesh, L0.a, L0.a.val.get(), stream);
+        refresh_finest_derived(hier, stream);
+        CUNIBS_CHECK(cudaStreamSynchronize(stream));
+    }
+
     void rebuild_hierarchy() {
         solver.reset();
         DevCsr<double> a0;
@@ -744,9 +757,7 @@ int cunibs_context_set_conductivity_keep_coarse(cunibs_context* c, const double*
         require(c->pending.empty(), "finish the submitted blocks first");
         DeviceGuard dg(c->device);
         assemble_stiffness(c->mesh, sigma_by_tag, c->stream);
-        DevCsr<double> a0;
-        reduce_grounded(c->mesh, a0, c->stream);
-        if (!refresh_finest_level(c->hier, a0, c->stream)) c->rebuild_hierarchy();
+        c->keep_coarse_values();
     });
 }
 
@@ -779,12 +790,8 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         Mesh& m = c->mesh;
         cudaStream_t s = c->stream;
         // The context at the nominal conductivities, its coarse levels kept.
-        {
-            assemble_stiffness(m, st->nominal, s);
-            DevCsr<double> a0;
-            reduce_grounded(m, a0, s);
-            if (!refresh_finest_level(c->hier, a0, s)) c->rebuild_hierarchy();
-        }
+        assemble_stiffness(m, st->nominal, s);
+        c->keep_coarse_values();
         require(!c->hier.levels.empty(), "the operator is too small for a conductivity study (it has no AMG level)");
         const Level& L0 = c->hier.levels[0];
         st->nnz = L0.a.nnz;
@@ -793,11 +800,11 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         st->comp.resize(static_cast<std::size_t>(1 + P) * st->nnz);
         double table[11];
         for (int t = 0; t < 11; ++t) table[t] = (t >= 1 && slots.slot[t] < 0) ? st->nominal[t] : 0.0;
-        assemble_reduced_values(m, table, st->nnz, st->comp.get(), s);
+        assemble_reduced_values(m, table, L0.a, st->comp.get(), s);
         for (int a = 0; a < P; ++a) {
             for (double& v : table) v = 0.0;
             table[st->tags[a]] = 1.0;
-            assemble_reduced_values(m, table, st->nnz, st->comp.get() + static_cast<std::size_t>(1 + a) * st->nnz, s);
+            assemble_reduced_values(m, table, L0.a, st->comp.get() + static_cast<std::size_t>(1 + a) * st->nnz, s);
         }
         // The components must give back the nominal operator (the gate of assembly.py:126-131).
         {
@@ -909,7 +916,7 @@ int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* 
         // the right-hand side weights; the coarse levels stay the nominal ones (run.py:244-247).
         sigma_combine(st.comp.get(), P, st.nnz, w, c->hier.levels[0].a.val.get(), s);
         refresh_finest_derived(c->hier, s);
-        set_element_conductivity(m, table, s);
+        set_element_conductivity(m, table, s, false);  // the nominal table passed the check at begin
         BlockSlot& sl = c->slots[st.slot];
         rhs_block(m, sl.dadt_elm.get(), k, K, sl.B.get(), s);
         sl.X0.reserve(static_cast<std::size_t>(n_red) * K);
@@ -964,9 +971,7 @@ int cunibs_sigma_end(cunibs_context* c) {
         DeviceGuard dg(c->device);
         const std::unique_ptr<SigmaStudy> st = std::move(c->study);
         assemble_stiffness(c->mesh, st->nominal, c->stream);
-        DevCsr<double> a0;
-        reduce_grounded(c->mesh, a0, c->stream);
-        if (!refresh_finest_level(c->hier, a0, c->stream)) c->rebuild_hierarchy();
+        c->keep_coarse_values();
     });
 }
 

@@ -102,6 +102,7 @@ struct Mesh {
     DevArray<double> vols;      // (M) m^3
     DevArray<float> vols32;
     DevArray<double> cond;      // (M) S/m
+    DevArray<int> cond_bad;     // (1) elements whose tag the last conductivity table left undefined
     DevArray<float> neg_vc32;   // -(vol*sigma) in FP32
     DevArray<double> bary;      // (M,3) mm
     DevArray<int> n2c_ptr;      // (N+1)
@@ -129,17 +130,21 @@ void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, c
                 const int* skin, int n_skin, cudaStream_t s);
 void assemble_stiffness(Mesh& m, const double* sigma_by_tag /* 11 entries or null */, cudaStream_t s);
 // Per-element conductivity and right-hand side weights of a conductivity table (11 entries).
-void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s);
-// Grounded (reduced) stiffness values of a conductivity table whose entries may be zero, into
-// out (nnz_red), without touching the mesh's own values; the table's linearity in sigma makes a
-// table with one unit entry give that tissue's share of the operator.
-void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, long nnz_red, double* out, cudaStream_t s);
+// validate: fail when the table leaves a tag of the mesh undefined (a host synchronisation); a
+// caller whose table has passed that check once for the same tags may skip it.
+void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s, bool validate = true);
+// Grounded stiffness values of a conductivity table whose entries may be zero, on the grounded
+// pattern (out: pattern.nnz), without touching the mesh's own values; the operator's linearity in
+// sigma makes a table with one unit entry give that tissue's share of it.
+void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, const DevCsr<double>& pattern, double* out,
+                             cudaStream_t s);
 void reduce_grounded(const Mesh& m, DevCsr<double>& out, cudaStream_t s);
+// The grounded values of the mesh's stiffness on a grounded pattern already built (out: pattern.nnz).
+void reduce_grounded_values(const Mesh& m, const DevCsr<double>& pattern, double* out, cudaStream_t s);
 
 // Hierarchy (setup_amg.cu).
 int select_size4(int n, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s);
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& p, cudaStream_t s);
-bool refresh_finest_level(Hierarchy& h, const DevCsr<double>& a0, cudaStream_t s);
 // The finest level's l1 smoother weights and FP32 copies, after its FP64 values were rewritten in
 // place (queued on s, no synchronisation).
 void refresh_finest_derived(Hierarchy& h, cudaStream_t s);

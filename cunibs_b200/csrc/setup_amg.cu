@@ -676,20 +676,9 @@ static void dense_inverse(const DevCsr<double>& a, DevArray<double>& inv, DevArr
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 
-// New values for the finest operator (the same pattern: conductivity changes only values): copy
-// them, refresh the level's l1 smoother weights and FP32 copies, keep every coarser level,
-// prolongator and the dense bottom. False when the hierarchy has no level to refresh or the
-// pattern differs.
-bool refresh_finest_level(Hierarchy& h, const DevCsr<double>& a0, cudaStream_t s) {
-    if (h.levels.empty()) return false;
-    Level& L = h.levels[0];
-    if (L.a.n != a0.n || L.a.nnz != a0.nnz) return false;
-    CUNIBS_CHECK(cudaMemcpyAsync(L.a.val.get(), a0.val.get(), sizeof(double) * a0.nnz, cudaMemcpyDeviceToDevice, s));
-    refresh_finest_derived(h, s);
-    CUNIBS_CHECK(cudaStreamSynchronize(s));
-    return true;
-}
-
+// The finest level's smoother weights and FP32 copies after new values were written into it (the
+// same pattern: conductivity changes only values); every coarser level, prolongator and the dense
+// bottom are kept.
 void refresh_finest_derived(Hierarchy& h, cudaStream_t s) {
     Level& L = h.levels[0];
     l1_dinv(L.a, L.dinv, s);

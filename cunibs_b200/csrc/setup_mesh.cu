@@ -291,29 +291,42 @@ __global__ void pattern_fill_kernel(const std::uint64_t* __restrict__ keys, cons
 
 // Element matrices, a half-warp per element: lane l owns entry (l/4, l%4) and writes
 // vol*sigma*(g_i . g_j), products rounded one at a time, summed left to right.
-__global__ void element_products_kernel(const double* __restrict__ g, const double* __restrict__ vols,
-                                        const double* __restrict__ cond, int m, double* __restrict__ ev) {
-    const std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q >= 16 * static_cast<std::int64_t>(m)) return;
-    const std::int64_t e = q >> 4;
-    const int i = static_cast<int>((q >> 2) & 3);
-    const int j = static_cast<int>(q & 3);
-    const double* gi = g + 12 * e + 3 * i;
-    const double* gj = g + 12 * e + 3 * j;
-    const double dot = gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2];
-    const double s = vols[e] * cond[e];
-    ev[q] = s * dot;
-}
-
-// Deterministic segmented reduction: each CSR entry sums its element contributions in order.
-__global__ void segmented_sum_kernel(const double* __restrict__ ev, const int* __restrict__ contrib_ptr,
-                                     const int* __restrict__ contrib_idx, long nnz, double* __restrict__ out) {
+// Stiffness values, deterministically: each CSR entry sums its element contributions
+// vol_e sigma_e (g_ei . g_ej) in the order of contrib_idx (ascending element), with every product
+// and sum rounded on its own; nothing is staged per contribution.
+__global__ void assemble_entries_kernel(const double* __restrict__ g, const double* __restrict__ vols,
+                                        const double* __restrict__ cond, const int* __restrict__ contrib_ptr,
+                                        const int* __restrict__ contrib_idx, long nnz, double* __restrict__ out) {
     const long p = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (p >= nnz) return;
     double acc = 0.0;
     const int end = contrib_ptr[p + 1];
-    for (int q = contrib_ptr[p]; q < end; ++q) acc = acc + ev[contrib_idx[q]];
+    for (int q = contrib_ptr[p]; q < end; ++q) {
+        const int idx = contrib_idx[q];
+        const std::int64_t e = idx >> 4;
+        const double* gi = g + 12 * e + 3 * ((idx >> 2) & 3);
+        const double* gj = g + 12 * e + 3 * (idx & 3);
+        const double dot = gi[0] * gj[0] + gi[1] * gj[1] + gi[2] * gj[2];
+        const double sv = vols[e] * cond[e];
+        acc = acc + sv * dot;
+    }
     out[p] = acc;
+}
+
+// Grounded values on a known grounded pattern: row r of the reduced operator is row
+// i = r + (r >= ground) of the full one without the ground column, entries in order.
+__global__ void reduced_values_kernel(const int* __restrict__ ptr, const int* __restrict__ col,
+                                     const double* __restrict__ val, int n, int ground, const int* __restrict__ rptr,
+                                     double* __restrict__ rval) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n - 1) return;
+    const int i = r + (r >= ground ? 1 : 0);
+    int q = rptr[r];
+    for (int p = ptr[i]; p < ptr[i + 1]; ++p) {
+        if (col[p] == ground) continue;
+        rval[q] = val[p];
+        ++q;
+    }
 }
 
 // Lowest-z node, lowest index on ties: a min over the total order (z, index).
@@ -603,12 +616,13 @@ void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, c
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 
-void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
+void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s, bool validate) {
     CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
-    DevArray<int> bad(1);
-    bad.zero(s);
-    conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, m.cond.get(), bad.get()); count_launch();
-    if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
+    m.cond_bad.resize(1);
+    if (validate) m.cond_bad.zero(s);
+    conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, m.cond.get(), m.cond_bad.get());
+    count_launch();
+    if (validate && read_int(m.cond_bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
     // The right-hand side weighs each element by the same conductivity.
     neg_vc_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.vols32.get(), m.cond.get(), m.n_tets, m.neg_vc32.get());
     count_launch();
@@ -616,40 +630,38 @@ void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t 
 
 void assemble_stiffness(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
     if (sigma_by_tag != nullptr) set_element_conductivity(m, sigma_by_tag, s);
-    const std::int64_t Q = 16 * static_cast<std::int64_t>(m.n_tets);
-    DevArray<double> ev(Q);
-    element_products_kernel<<<grid_for(Q), kBlock, 0, s>>>(m.g.get(), m.vols.get(), m.cond.get(), m.n_tets, ev.get()); count_launch();
     m.k_val.resize(m.k_nnz);
-    segmented_sum_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(ev.get(), m.contrib_ptr.get(), m.contrib_idx.get(),
-                                                              m.k_nnz, m.k_val.get()); count_launch();
+    assemble_entries_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(m.g.get(), m.vols.get(), m.cond.get(),
+                                                                 m.contrib_ptr.get(), m.contrib_idx.get(), m.k_nnz,
+                                                                 m.k_val.get()); count_launch();
     CUNIBS_LAUNCH_CHECK("stiffness values");
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 
-void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, long nnz_red, double* out, cudaStream_t s) {
+void reduce_grounded_values(const Mesh& m, const DevCsr<double>& pattern, double* out, cudaStream_t s) {
+    if (pattern.n != m.n_nodes - 1) fail(kEInternal, "grounded pattern of another mesh");
+    reduced_values_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), m.k_val.get(),
+                                                                     m.n_nodes, m.ground, pattern.ptr.get(), out);
+    count_launch();
+    CUNIBS_LAUNCH_CHECK("grounded values");
+}
+
+void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, const DevCsr<double>& pattern, double* out,
+                             cudaStream_t s) {
     CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
     const int M = m.n_tets;
-    DevArray<double> cond(M);
+    DevArray<double> cond(M), full(m.k_nnz);
     DevArray<int> bad(1);
     bad.zero(s);
     conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), M, cond.get(), bad.get()); count_launch();
     if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
-    const std::int64_t Q = 16 * static_cast<std::int64_t>(M);
-    DevArray<double> ev(Q), full(m.k_nnz);
-    element_products_kernel<<<grid_for(Q), kBlock, 0, s>>>(m.g.get(), m.vols.get(), cond.get(), M, ev.get()); count_launch();
-    segmented_sum_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(ev.get(), m.contrib_ptr.get(), m.contrib_idx.get(),
-                                                              m.k_nnz, full.get()); count_launch();
-    // The grounded pattern keeps each row's entries in order minus the ground column, so the
-    // reduced values are the full values with the ground row and column dropped.
-    DevArray<int> cnt(m.n_nodes), rptr(m.n_nodes);
-    CUNIBS_CHECK(cudaMemsetAsync(cnt.get() + (m.n_nodes - 1), 0, sizeof(int), s));
-    reduced_count_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), m.n_nodes, m.ground,
-                                                                    cnt.get()); count_launch();
-    exclusive_scan(cnt.get(), rptr.get(), m.n_nodes, s);
-    if (read_int(rptr.get() + (m.n_nodes - 1), s) != nnz_red) fail(kEInternal, "reduced stiffness pattern mismatch");
-    DevArray<int> rcol(nnz_red);
-    reduced_fill_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), full.get(), m.n_nodes,
-                                                                   m.ground, rptr.get(), rcol.get(), out); count_launch();
+    assemble_entries_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(m.g.get(), m.vols.get(), cond.get(),
+                                                                 m.contrib_ptr.get(), m.contrib_idx.get(), m.k_nnz,
+                                                                 full.get()); count_launch();
+    if (pattern.n != m.n_nodes - 1) fail(kEInternal, "grounded pattern of another mesh");
+    reduced_values_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), full.get(),
+                                                                     m.n_nodes, m.ground, pattern.ptr.get(), out);
+    count_launch();
     CUNIBS_LAUNCH_CHECK("reduced stiffness values");
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
