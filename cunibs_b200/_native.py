@@ -150,6 +150,14 @@ def load() -> C.CDLL:
         "cunibs_sigma_draw": ([_vp, dp, C.POINTER(BlockOut), ip], C.c_int),
         "cunibs_sigma_end": ([_vp], C.c_int),
         "cunibs_sigma_coefficients": ([C.c_int, dp, dp, ip, C.c_double, dp, ip], C.c_int),
+        "cunibs_adm_create": ([_vp, ip, dp, C.c_int, dp, C.c_int, C.c_double, C.c_int, ip, dp, C.POINTER(_vp)],
+                              C.c_int),
+        "cunibs_adm_destroy": ([_vp], C.c_int),
+        "cunibs_adm_node_weights": ([_vp, dp], C.c_int),
+        "cunibs_adm_sample": ([_vp, dp, dp, ip], C.c_int),
+        "cunibs_adm_qfield": ([_vp, fp, C.c_longlong], C.c_int),
+        "cunibs_adm_evaluate": ([_vp, dp, dp, C.c_int, dp, C.c_int, C.c_double, dp], C.c_int),
+        "cunibs_adm_evaluate_exact": ([_vp, dp, dp, C.c_int, dp, C.c_int, C.c_double, dp, dp], C.c_int),
         "cunibs_context_array": ([_vp, C.c_char_p, C.c_int, _vp, C.c_longlong, C.POINTER(C.c_longlong)], C.c_int),
         "cunibs_context_place": ([_vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
         "cunibs_context_dadt": ([_vp, _vp, _vp, C.c_int, _vp, C.c_int, C.c_double, _vp], C.c_int),
@@ -560,6 +568,84 @@ class Context:
 
 def kernel_launches() -> int:
     return int(load().cunibs_kernel_launches())
+
+
+class Adm:
+    """An auxiliary-dipole-method handle (cunibs_adm_*): the adjoint state of one target functional
+    on a context, and the reciprocity field it last sampled. The context must stay open."""
+
+    def __init__(self, ctx: Context, elem_idx, weights, directions, tolerance: float, max_iters: int) -> None:
+        lib = load()
+        idx = np.ascontiguousarray(elem_idx, np.int32).reshape(-1)
+        w = np.ascontiguousarray(weights, np.float64).reshape(-1)
+        d = np.ascontiguousarray(directions, np.float64).reshape(-1, 3)
+        if idx.shape != w.shape:
+            raise ValueError("elem_idx and weights must have the same length")
+        self.n_dir = d.shape[0]
+        self.n_nodes = ctx.n_nodes
+        self.iterations = np.zeros(self.n_dir, np.int32)
+        self.relres = np.zeros(self.n_dir)
+        h = _vp()
+        dp = C.POINTER(C.c_double)
+        check(lib.cunibs_adm_create(ctx.handle, _ip(idx), w.ctypes.data_as(dp), idx.shape[0], d.ctypes.data_as(dp),
+                                    self.n_dir, float(tolerance), int(max_iters), _ip(self.iterations),
+                                    self.relres.ctypes.data_as(dp), C.byref(h)))
+        self._h = h
+        self._lib = lib
+        self._ctx = ctx  # keeps the context alive while the handle is
+        self.shape: tuple[int, int, int] | None = None
+        self.sample_id = 0
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            check(self._lib.cunibs_adm_destroy(self._h))
+            self._h = _vp()
+
+    def __del__(self) -> None:
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def node_weights(self) -> np.ndarray:
+        out = np.empty((self.n_dir, self.n_nodes, 3))
+        check(self._lib.cunibs_adm_node_weights(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def sample(self, origin_mm, spacing_mm, shape) -> int:
+        o = np.ascontiguousarray(origin_mm, np.float64).reshape(3)
+        sp = np.ascontiguousarray(spacing_mm, np.float64).reshape(3)
+        sh = np.ascontiguousarray(shape, np.int32).reshape(3)
+        dp = C.POINTER(C.c_double)
+        check(self._lib.cunibs_adm_sample(self._h, o.ctypes.data_as(dp), sp.ctypes.data_as(dp), _ip(sh)))
+        self.shape = tuple(int(v) for v in sh)
+        self.sample_id += 1
+        return self.sample_id
+
+    def qfield(self) -> np.ndarray:
+        if self.shape is None:
+            raise ValueError("the reciprocity field has not been sampled")
+        out = np.empty((self.n_dir, *self.shape, 3), np.float32)
+        check(self._lib.cunibs_adm_qfield(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out
+
+    def _eval(self, fn, coil, transforms, didt, *extra) -> np.ndarray:
+        T = np.ascontiguousarray(transforms, np.float64).reshape(-1, 16)
+        pos = np.ascontiguousarray(coil.positions_m, np.float64)
+        mom = np.ascontiguousarray(coil.moments, np.float64)
+        out = np.empty((T.shape[0], self.n_dir))
+        dp = C.POINTER(C.c_double)
+        check(fn(self._h, pos.ctypes.data_as(dp), mom.ctypes.data_as(dp), pos.shape[0], T.ctypes.data_as(dp),
+                 T.shape[0], float(didt), *extra, out.ctypes.data_as(dp)))
+        return out
+
+    def evaluate(self, coil, transforms, didt) -> np.ndarray:
+        return self._eval(self._lib.cunibs_adm_evaluate, coil, transforms, didt)
+
+    def evaluate_exact(self, coil, transforms, didt, center_mm=None) -> np.ndarray:
+        c = None if center_mm is None else np.ascontiguousarray(center_mm, np.float64).reshape(3)
+        cp_ = None if c is None else c.ctypes.data_as(C.POINTER(C.c_double))
+        return self._eval(self._lib.cunibs_adm_evaluate_exact, coil, transforms, didt, cp_)
 
 
 def sigma_coefficients(gram, proj, active, rtol: float = 1e-12):

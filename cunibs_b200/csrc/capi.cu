@@ -1,6 +1,8 @@
 // The C ABI (include/cunibs_b200.h): context lifetime, the block solve, stage-level entry points.
 #include <algorithm>
 #include <cmath>
+#include <climits>
+#include <cstdio>
 #include <cstring>
 #include <deque>
 #include <string>
@@ -983,6 +985,263 @@ int cunibs_sigma_coefficients(int n_tags, const double* gram, const double* proj
         require(rtol >= 0.0 && rtol < 1.0, "rtol must be in [0, 1)");
         const int r = sigma_coefficients(n_tags, gram, proj, active, rtol, coef);
         if (rank) *rank = r;
+    });
+}
+
+}  // extern "C"
+
+// A target functional's adjoint state on one context (adm/reciprocity.py:119-245): the nodal
+// reciprocity weights and, once sampled, the reciprocity field on a grid.
+struct cunibs_adm {
+    cunibs_context* ctx = nullptr;
+    AdmDirections dirs{};
+    DevArray<double> alpha;          // (n_tets) target weight per element
+    DevArray<double> W;              // (n_dir, n_nodes, 3)
+    std::vector<int> iterations;
+    std::vector<double> relres;
+    bool sampled = false;
+    AdmGrid grid{};
+    DevArray<float> Q;               // (n_dir, n_grid, 3)
+    DevArray<double> pos, mom, T, E; // evaluation workspace
+    DevArray<unsigned long long> bad;
+};
+
+namespace {
+
+// Reciprocity N-body sources: the nodes centred on center_mm with the weights of each direction as
+// moments, packed like rotated coil dipoles, and the matching (identity rotation, centre) frames.
+void adm_sources(cunibs_adm* a, const double* center_mm, DevArray<unsigned char>& packed, DevArray<double>& Td,
+                 cudaStream_t s) {
+    const Mesh& m = a->ctx->mesh;
+    const int nd = a->dirs.n;
+    DevArray<double> src(3 * static_cast<std::size_t>(m.n_nodes));
+    adm_centred_nodes(m, center_mm, src.get(), s);
+    std::vector<double> h(16 * static_cast<std::size_t>(nd), 0.0);
+    for (int d = 0; d < nd; ++d) {
+        double* t = &h[16 * d];
+        t[0] = t[5] = t[10] = t[15] = 1.0;
+        t[3] = center_mm[0];
+        t[7] = center_mm[1];
+        t[11] = center_mm[2];
+    }
+    Td.upload(h.data(), h.size(), s);
+    const std::size_t rec = packed_dipole_bytes();
+    packed.resize(rec * m.n_nodes * nd);
+    for (int d = 0; d < nd; ++d)
+        prep_dipoles(src.get(), a->W.get() + 3 * static_cast<std::size_t>(m.n_nodes) * d, m.n_nodes, Td.get() + 16 * d,
+                     1, packed.get() + rec * m.n_nodes * d, s);
+    CUNIBS_CHECK(cudaStreamSynchronize(s));  // h and src leave scope
+}
+
+void adm_inputs(cunibs_adm* a, const double* dip_pos_m, const double* dip_moment, int n_dip, const double* transforms,
+                int P, cudaStream_t s) {
+    require(dip_pos_m && dip_moment && transforms, "input arrays must not be NULL");
+    require(n_dip >= 1 && P >= 1, "need at least one dipole and one placement");
+    for (long i = 0; i < 16L * P; ++i) require(std::isfinite(transforms[i]), "transforms must be finite");
+    a->pos.upload(dip_pos_m, 3 * static_cast<std::size_t>(n_dip), s);
+    a->mom.upload(dip_moment, 3 * static_cast<std::size_t>(n_dip), s);
+    a->T.upload(transforms, 16 * static_cast<std::size_t>(P), s);
+    a->E.reserve(static_cast<std::size_t>(P) * a->dirs.n);
+}
+
+}  // namespace
+
+extern "C" {
+
+int cunibs_adm_create(cunibs_context* c, const int* elem_idx, const double* weights, int n_elem,
+                      const double* directions, int n_dir, double tolerance, int max_iters, int* iterations,
+                      double* relres, cunibs_adm** out) {
+    return guarded([&] {
+        require(c && elem_idx && weights && directions && out, "NULL argument");
+        *out = nullptr;
+        require(n_elem >= 1, "the target needs at least one element");
+        require(n_dir >= 1 && n_dir <= kAdmMaxDir, "between 1 and 3 adjoint directions");
+        require(tolerance > 0.0 && tolerance < 1.0 && max_iters >= 1, "tolerance in (0, 1) and max_iters >= 1");
+        require(!c->study, "a conductivity study is open: end it first");
+        require(c->pending.empty(), "finish the submitted blocks first");
+        Mesh& m = c->mesh;
+        std::vector<double> alpha(m.n_tets, 0.0);
+        for (int i = 0; i < n_elem; ++i) {
+            require(elem_idx[i] >= 0 && elem_idx[i] < m.n_tets, "target element index out of range");
+            require(std::isfinite(weights[i]), "target weights must be finite");
+            alpha[elem_idx[i]] += weights[i];
+        }
+        auto a = std::make_unique<cunibs_adm>();
+        a->ctx = c;
+        a->dirs.n = n_dir;
+        for (int d = 0; d < n_dir; ++d) {
+            double nrm = 0.0;
+            for (int x = 0; x < 3; ++x) {
+                a->dirs.e[d][x] = directions[3 * d + x];
+                nrm += directions[3 * d + x] * directions[3 * d + x];
+            }
+            require(nrm > 0.0 && std::isfinite(nrm), "directions must be finite and non-zero");
+        }
+        DeviceGuard dg(c->device);
+        cudaStream_t s = c->stream;
+        a->alpha.upload(alpha.data(), alpha.size(), s);
+        const int K = n_dir == 1 ? 1 : (n_dir == 2 ? 2 : 4);
+        const int n_red = m.n_nodes - 1;
+        DevArray<double> B(static_cast<std::size_t>(n_red) * K), X(static_cast<std::size_t>(n_red) * K);
+        adm_adjoint_rhs(m, a->alpha.get(), a->dirs, K, B.get(), s);
+        // All directions in one block solve (reciprocity.py:131-141 solves them one at a time).
+        Params prm = c->prm;
+        prm.tolerance = tolerance;
+        prm.max_iters = max_iters;
+        SolveStats st;
+        solver_solve(*c->solver, B.get(), X.get(), n_dir, K, prm, s, st);
+        bool missed = false;
+        for (int d = 0; d < n_dir; ++d) missed = missed || !(st.col_rel[d] <= tolerance);
+        if (missed) {
+            Params retry = prm;
+            retry.precision = kPlainFp64;
+            SolveStats st2;
+            solver_solve(*c->solver, B.get(), X.get(), n_dir, K, retry, s, st2, X.get());
+            for (int d = 0; d < n_dir; ++d) {
+                st.col_iters[d] += st2.col_iters[d];
+                st.col_rel[d] = st2.col_rel[d];
+                if (!(st2.col_rel[d] <= tolerance))
+                    fail(kENoConv, "adjoint solve did not converge (direction " + std::to_string(d) + "): relative "
+                                       "residual " + std::to_string(st2.col_rel[d]) + " > tolerance " +
+                                       std::to_string(tolerance));
+            }
+        }
+        a->W.resize(3 * static_cast<std::size_t>(m.n_nodes) * n_dir);
+        adm_node_weights(m, X.get(), K, a->alpha.get(), a->dirs, a->W.get(), s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        a->iterations.assign(st.col_iters.begin(), st.col_iters.end());
+        a->relres.assign(st.col_rel.begin(), st.col_rel.end());
+        for (int d = 0; d < n_dir; ++d) {
+            if (iterations) iterations[d] = a->iterations[d];
+            if (relres) relres[d] = a->relres[d];
+        }
+        *out = a.release();
+    });
+}
+
+int cunibs_adm_destroy(cunibs_adm* a) {
+    return guarded([&] {
+        if (!a) return;
+        DeviceGuard dg(a->ctx->device);
+        CUNIBS_CHECK(cudaStreamSynchronize(a->ctx->stream));
+        delete a;
+    });
+}
+
+int cunibs_adm_node_weights(const cunibs_adm* a, double* out) {
+    return guarded([&] {
+        require(a && out, "NULL argument");
+        DeviceGuard dg(a->ctx->device);
+        a->W.download(out, a->W.size(), a->ctx->stream);
+        CUNIBS_CHECK(cudaStreamSynchronize(a->ctx->stream));
+    });
+}
+
+int cunibs_adm_sample(cunibs_adm* a, const double* origin_mm, const double* spacing_mm, const int* shape) {
+    return guarded([&] {
+        require(a && origin_mm && spacing_mm && shape, "NULL argument");
+        AdmGrid gr{};
+        long long n_grid = 1;
+        for (int x = 0; x < 3; ++x) {
+            require(std::isfinite(origin_mm[x]), "grid origin must be finite");
+            require(spacing_mm[x] > 0.0 && std::isfinite(spacing_mm[x]), "grid spacing must be positive");
+            require(shape[x] >= 1 && shape[x] <= (1 << 16), "grid shape must be in [1, 65536] per axis");
+            gr.origin_mm[x] = origin_mm[x];
+            gr.spacing_mm[x] = spacing_mm[x];
+            gr.shape[x] = shape[x];
+            n_grid *= shape[x];
+        }
+        require(n_grid <= (1LL << 28), "at most 2^28 grid points");
+        DeviceGuard dg(a->ctx->device);
+        cudaStream_t s = a->ctx->stream;
+        double center[3];
+        for (int x = 0; x < 3; ++x) center[x] = gr.origin_mm[x] + 0.5 * gr.spacing_mm[x] * (gr.shape[x] - 1);
+        DevArray<double> pts(3 * static_cast<std::size_t>(n_grid)), Td;
+        adm_grid_points(gr, pts.get(), s);
+        DevArray<unsigned char> packed;
+        adm_sources(a, center, packed, Td, s);
+        a->sampled = false;
+        a->Q.resize(3 * static_cast<std::size_t>(n_grid) * a->dirs.n);
+        // Q_d on the grid: the coil-field N-body with the mesh nodes as sources (reciprocity.py:183-213).
+        dadt_nodes_raw(pts.get(), static_cast<int>(n_grid), reinterpret_cast<const float*>(packed.get()),
+                       a->ctx->mesh.n_nodes, Td.get(), a->dirs.n, 1.0, a->Q.get(), s);
+        CUNIBS_LAUNCH_CHECK("reciprocity field");
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        a->grid = gr;
+        a->sampled = true;
+    });
+}
+
+int cunibs_adm_qfield(const cunibs_adm* a, float* out, long long cap) {
+    return guarded([&] {
+        require(a && out, "NULL argument");
+        require(a->sampled, "the reciprocity field has not been sampled (cunibs_adm_sample)");
+        require(cap >= static_cast<long long>(a->Q.size()), "output buffer too small");
+        DeviceGuard dg(a->ctx->device);
+        a->Q.download(out, a->Q.size(), a->ctx->stream);
+        CUNIBS_CHECK(cudaStreamSynchronize(a->ctx->stream));
+    });
+}
+
+int cunibs_adm_evaluate(cunibs_adm* a, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                        const double* transforms, int P, double didt, double* E) {
+    return guarded([&] {
+        require(a && E, "NULL argument");
+        require(a->sampled, "the reciprocity field has not been sampled (cunibs_adm_sample)");
+        DeviceGuard dg(a->ctx->device);
+        cudaStream_t s = a->ctx->stream;
+        adm_inputs(a, dip_pos_m, dip_moment, n_dip, transforms, P, s);
+        a->bad.resize(3);
+        CUNIBS_CHECK(cudaMemsetAsync(a->bad.get(), 0xFF, 3 * sizeof(unsigned long long), s));
+        adm_evaluate(a->Q.get(), a->dirs.n, a->grid, a->pos.get(), a->mom.get(), n_dip, a->T.get(), P, didt,
+                     a->E.get(), a->bad.get(), s);
+        unsigned long long bad[3];
+        a->bad.download(bad, 3, s);
+        a->E.download(E, static_cast<std::size_t>(P) * a->dirs.n, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        for (int x = 0; x < 3; ++x) {
+            if (bad[x] == ULLONG_MAX) continue;
+            // The first axis with a dipole off the grid, and its first such sample (evaluate.py:49-79).
+            const long long p = static_cast<long long>(bad[x] / n_dip), j = static_cast<long long>(bad[x] % n_dip);
+            const double* Tp = transforms + 16 * p;
+            const double pos = Tp[4 * x] * dip_pos_m[3 * j] * 1e3 + Tp[4 * x + 1] * dip_pos_m[3 * j + 1] * 1e3 +
+                               Tp[4 * x + 2] * dip_pos_m[3 * j + 2] * 1e3 + Tp[4 * x + 3];
+            const double lo = a->grid.origin_mm[x], hi = lo + a->grid.spacing_mm[x] * (a->grid.shape[x] - 1);
+            char msg[512];
+            std::snprintf(msg, sizeof(msg),
+                          "A coil dipole falls outside the reciprocity grid: sample %lld of %d on axis %d (%c), dipole "
+                          "at %.3f mm against a grid spanning [%.3f, %.3f] mm (%.3f mm outside). Sample the "
+                          "reciprocity field on a grid that covers it: widen its coverage or margin, or evaluate at "
+                          "the coil distance the grid was built for.",
+                          p, P, x, "xyz"[x], pos, lo, hi, pos < lo ? lo - pos : pos - hi);
+            fail(kEInval, msg);
+        }
+    });
+}
+
+int cunibs_adm_evaluate_exact(cunibs_adm* a, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                              const double* transforms, int P, double didt, const double* center_mm, double* E) {
+    return guarded([&] {
+        require(a && E, "NULL argument");
+        require(static_cast<long long>(P) * n_dip <= (1LL << 26), "at most 2^26 placed dipoles per call");
+        DeviceGuard dg(a->ctx->device);
+        cudaStream_t s = a->ctx->stream;
+        adm_inputs(a, dip_pos_m, dip_moment, n_dip, transforms, P, s);
+        const double zero[3] = {0.0, 0.0, 0.0};
+        const double* c0 = center_mm ? center_mm : zero;
+        const std::size_t n_pts = static_cast<std::size_t>(P) * n_dip;
+        DevArray<double> s_mm(3 * n_pts), m_all(3 * n_pts), Td;
+        DevArray<float> Qx(3 * n_pts * a->dirs.n);
+        adm_placed_dipoles(a->pos.get(), a->mom.get(), n_dip, a->T.get(), P, s_mm.get(), m_all.get(), s);
+        DevArray<unsigned char> packed;
+        adm_sources(a, c0, packed, Td, s);
+        // Q evaluated at every placed dipole (no grid): evaluate.py:158-193.
+        dadt_nodes_raw(s_mm.get(), static_cast<int>(n_pts), reinterpret_cast<const float*>(packed.get()),
+                       a->ctx->mesh.n_nodes, Td.get(), a->dirs.n, 1.0, Qx.get(), s);
+        CUNIBS_LAUNCH_CHECK("reciprocity field at dipoles");
+        adm_exact_reduce(Qx.get(), a->dirs.n, P, n_dip, m_all.get(), didt, a->E.get(), s);
+        a->E.download(E, static_cast<std::size_t>(P) * a->dirs.n, s);
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
     });
 }
 

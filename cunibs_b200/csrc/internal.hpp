@@ -331,4 +331,33 @@ double sigma_relative_difference(const double* a, const double* b, long n, cudaS
 // Jacobi-scaled Gram above rtol times the largest).
 int sigma_coefficients(int P, const double* gram, const double* proj, const int* active, double rtol, double* Z);
 
+// Auxiliary dipole method (adm.cu): adjoint right-hand sides, nodal reciprocity weights and the
+// evaluation of placements against a reciprocity field sampled on a grid.
+constexpr int kAdmMaxDir = 3;
+struct AdmDirections {
+    double e[kAdmMaxDir][3];
+    int n;
+};
+struct AdmGrid {
+    double origin_mm[3];
+    double spacing_mm[3];
+    int shape[3];
+};
+// Adjoint right-hand sides (n_red, K) of the target weights alpha (per element, zero off target).
+void adm_adjoint_rhs(const Mesh& m, const double* alpha, const AdmDirections& dirs, int K, double* c_red,
+                     cudaStream_t s);
+// Nodal weights W (n_dir, n_nodes, 3) from the adjoint potentials lam (n_red, K).
+void adm_node_weights(const Mesh& m, const double* lam, int K, const double* alpha, const AdmDirections& dirs,
+                      double* W, cudaStream_t s);
+void adm_centred_nodes(const Mesh& m, const double* center_mm, double* out_m, cudaStream_t s);
+void adm_grid_points(const AdmGrid& gr, double* out /* (n_grid, 3) mm */, cudaStream_t s);
+// E (P, n_dir) from the sampled field Q (n_dir, n_grid, 3); bad[3] receives, per axis, the smallest
+// flat sample index p * n_dip + j of a dipole off the grid (left untouched when none is).
+void adm_evaluate(const float* Q, int n_dir, const AdmGrid& gr, const double* pos, const double* mom, int n_dip,
+                  const double* T, int P, double didt, double* E, unsigned long long* bad, cudaStream_t s);
+void adm_placed_dipoles(const double* pos, const double* mom, int n_dip, const double* T, int P, double* s_mm,
+                        double* m_out, cudaStream_t s);
+void adm_exact_reduce(const float* Qx, int n_dir, int P, int n_dip, const double* m_all, double didt, double* E,
+                      cudaStream_t s);
+
 }  // namespace cunibs

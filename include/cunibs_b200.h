@@ -244,6 +244,46 @@ int cunibs_sigma_end(cunibs_context* ctx);
 int cunibs_sigma_coefficients(int n_tags, const double* gram, const double* proj, const int* active, double rtol,
                               double* coef, int* rank);
 
+/* --- auxiliary dipole method (adm/reciprocity.py, evaluate.py) ---------------------------- */
+
+typedef struct cunibs_adm cunibs_adm;
+
+/* The adjoint (reciprocity) solves of a target functional J_d = sum_i weights[i] (dir_d . E_e),
+ * e = elem_idx[i] in the context's element order, for n_dir (1..3) directions (replaces
+ * solve_adjoint, reciprocity.py:119-141): K lambda_d = c_d, all directions in one block solve to
+ * tolerance (the reference's ADJOINT_TOLERANCE is 1e-9 with 3000 iterations), then the nodal
+ * weights W_d (reciprocity.py:91-116) with J_d = sum_n W_d[n] . dA/dt[n] exactly. iterations and
+ * relres (n_dir, may be NULL) receive the solve statistics. The context must outlive the handle
+ * and have no conductivity study open. */
+int cunibs_adm_create(cunibs_context* ctx, const int* elem_idx, const double* weights, int n_elem,
+                      const double* directions, int n_dir, double tolerance, int max_iters, int* iterations,
+                      double* relres, cunibs_adm** out);
+int cunibs_adm_destroy(cunibs_adm* adm);
+
+/* The nodal weights W (n_dir, n_nodes, 3), FP64, context node order. */
+int cunibs_adm_node_weights(const cunibs_adm* adm, double* out);
+
+/* Samples Q_d(g) = mu0/4pi sum_n W_d[n] x (g - r_n) / |g - r_n|^3 on a regular grid (origin and
+ * spacing in mm, shape per axis; C order, x slowest) with the FP32 dipole N-body centred on the
+ * grid's centre (replaces sample_qfield, reciprocity.py:183-213). The field stays on the device. */
+int cunibs_adm_sample(cunibs_adm* adm, const double* origin_mm, const double* spacing_mm, const int* shape);
+
+/* Copies the sampled field (n_dir, nx, ny, nz, 3) FP32 to host memory (cap: floats available). */
+int cunibs_adm_qfield(const cunibs_adm* adm, float* out, long long cap);
+
+/* E (P, n_dir) = didt sum_j m_j . Q_d(s_j) for the coil's dipoles placed by P coil-to-head affines
+ * (transforms (P, 4, 4), translation in mm), Q interpolated trilinearly on the sampled grid
+ * (replaces evaluate_frames, evaluate.py:82-152). One block per placement reduces in a fixed order,
+ * so a placement's value does not depend on the others. A dipole off the grid is CUNIBS_EINVAL
+ * naming the first offending sample. */
+int cunibs_adm_evaluate(cunibs_adm* adm, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                        const double* transforms, int P, double didt, double* E);
+
+/* The same functional with Q evaluated exactly at every placed dipole (no grid; evaluate.py:155-193),
+ * the N-body centred on center_mm (NULL: the origin). */
+int cunibs_adm_evaluate_exact(cunibs_adm* adm, const double* dip_pos_m, const double* dip_moment, int n_dip,
+                              const double* transforms, int P, double didt, const double* center_mm, double* E);
+
 /* --- stage-level entry points (the reference's kernel exports, bindings.cpp) --------------- */
 
 /* Copies a named internal array to host memory. name / dtype:
