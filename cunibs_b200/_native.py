@@ -7,6 +7,7 @@ be loaded, every entry point raises.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from pathlib import Path
 
 import numpy as np
@@ -243,6 +244,7 @@ class Context:
         self._lib = lib
         self._submitted: dict[int, tuple] = {}
         self._study: tuple | None = None
+        self._adms: weakref.WeakSet = weakref.WeakSet()
         self.params = prm
         info = Info()
         check(lib.cunibs_context_info(h, C.byref(info)))
@@ -258,6 +260,9 @@ class Context:
         self.bottom_rows = info.bottom_rows
 
     def close(self) -> None:
+        # Handles that live on this context (auxiliary-dipole-method state) go first.
+        for a in list(getattr(self, "_adms", ())):
+            a.close()
         h = getattr(self, "_h", None)
         if h is not None and h.value:
             self._lib.cunibs_context_destroy(h)
@@ -592,7 +597,8 @@ class Adm:
                                     self.relres.ctypes.data_as(dp), C.byref(h)))
         self._h = h
         self._lib = lib
-        self._ctx = ctx  # keeps the context alive while the handle is
+        self._ctx = ctx  # keeps the context object alive; closing the context closes this handle first
+        ctx._adms.add(self)
         self.shape: tuple[int, int, int] | None = None
         self.sample_id = 0
 
@@ -607,9 +613,15 @@ class Adm:
         except Exception:
             pass
 
+    @property
+    def handle(self):
+        if not self._h.value:
+            raise ValueError("the auxiliary-dipole-method handle has been closed (or its context freed)")
+        return self._h
+
     def node_weights(self) -> np.ndarray:
         out = np.empty((self.n_dir, self.n_nodes, 3))
-        check(self._lib.cunibs_adm_node_weights(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        check(self._lib.cunibs_adm_node_weights(self.handle, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
     def sample(self, origin_mm, spacing_mm, shape) -> int:
@@ -617,7 +629,7 @@ class Adm:
         sp = np.ascontiguousarray(spacing_mm, np.float64).reshape(3)
         sh = np.ascontiguousarray(shape, np.int32).reshape(3)
         dp = C.POINTER(C.c_double)
-        check(self._lib.cunibs_adm_sample(self._h, o.ctypes.data_as(dp), sp.ctypes.data_as(dp), _ip(sh)))
+        check(self._lib.cunibs_adm_sample(self.handle, o.ctypes.data_as(dp), sp.ctypes.data_as(dp), _ip(sh)))
         self.shape = tuple(int(v) for v in sh)
         self.sample_id += 1
         return self.sample_id
@@ -626,7 +638,7 @@ class Adm:
         if self.shape is None:
             raise ValueError("the reciprocity field has not been sampled")
         out = np.empty((self.n_dir, *self.shape, 3), np.float32)
-        check(self._lib.cunibs_adm_qfield(self._h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        check(self._lib.cunibs_adm_qfield(self.handle, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
         return out
 
     def _eval(self, fn, coil, transforms, didt, *extra) -> np.ndarray:
@@ -635,7 +647,7 @@ class Adm:
         mom = np.ascontiguousarray(coil.moments, np.float64)
         out = np.empty((T.shape[0], self.n_dir))
         dp = C.POINTER(C.c_double)
-        check(fn(self._h, pos.ctypes.data_as(dp), mom.ctypes.data_as(dp), pos.shape[0], T.ctypes.data_as(dp),
+        check(fn(self.handle, pos.ctypes.data_as(dp), mom.ctypes.data_as(dp), pos.shape[0], T.ctypes.data_as(dp),
                  T.shape[0], float(didt), *extra, out.ctypes.data_as(dp)))
         return out
 
