@@ -145,7 +145,8 @@ def test_resolve_target(setup):
     rt = adm.resolve_target(subj, adm.Target(point))
     assert rt.elem_idx.tolist() == [int(gm[np.argmin(np.linalg.norm(bary[gm] - point, axis=1))])]
     np.testing.assert_array_equal(rt.weights, [1.0])
-    rt = adm.resolve_target(subj, adm.Target(point, radius_mm=8.0))
+    inside = bary[rt.elem_idx[0]]  # a gray-matter barycentre: the ball around it holds its neighbours
+    rt = adm.resolve_target(subj, adm.Target(inside, radius_mm=8.0))
     assert rt.elem_idx.size > 1 and (tags[rt.elem_idx] == 2).all()
     np.testing.assert_allclose(rt.weights, vols[rt.elem_idx] / vols[rt.elem_idx].sum(), rtol=1e-14)
     np.testing.assert_allclose(rt.barycenter_mm, rt.weights @ bary[rt.elem_idx], rtol=1e-12)
