@@ -348,6 +348,7 @@ def run_ours(args) -> dict:
     d2h = res["transform"].nbytes + res["summary"].nbytes + res["iterations"].nbytes + res["relative_residual"].nbytes
 
     draws = conductivity_draws(ctx, coil, centers[:4], handles[:4], dists[:4], args.recovery, stream)
+    adm_line = adm_measure(ctx, coil, sites, stream)
 
     # Roofline of the SpMV-dominated iteration (solve stage).
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -415,6 +416,7 @@ def run_ours(args) -> dict:
                  "gpair_per_s": round(pair_evals / (dadt_ms / 1e3) / 1e9, 2)},
         "setup_s": round(setup_s, 3),
         "conductivity_draws": draws,
+        "adm": adm_line,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -488,6 +490,54 @@ def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_d
             "keep_coarse_iterations": round(float(np.mean(old_its)), 2),
             "placement_draws_per_s": round(k * n_draws / (new_ms / 1e3), 2),
             "ratio": round(old_ms / new_ms, 3)}
+
+
+def adm_measure(ctx, coil, sites, stream) -> dict:
+    """Auxiliary dipole method on the same head: a magnitude target 18 mm below the vertex (three
+    adjoint solves in one block at rel.res 1e-9), the reciprocity field on a 3 mm grid covering the
+    coil at any rotation on the 8 sites, then the target field of 8 sites x 360 rotations by grid
+    interpolation, and the optimiser over the 8 sites. Device time on the library stream (CUDA
+    events around each host call)."""
+    import torch
+
+    from cunibs_b200 import adm
+
+    def device_ms(fn):
+        with torch.cuda.stream(stream):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        out = fn()
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), out
+
+    centers = np.stack([c for c, _ in sites])
+    target = adm.resolve_target(ctx, adm.Target([0.0, 0.0, 72.0]))
+    adj_ms, adjoint = device_ms(lambda: adm.solve_adjoint(ctx, target))
+    grid = adm._coverage_grid(ctx, coil, centers, 4.0, 3.0, 8.0)
+    q_ms, recip = device_ms(lambda: adm.sample_qfield(adjoint, grid))
+    pairs = grid.n_points * ctx.n_nodes * target.directions.shape[0]
+    # 360 in-plane rotations per site: handle points around each site's own coil frame.
+    angles = np.radians(np.arange(360.0))
+    T0, _ = ctx.place(centers, np.stack([h for _, h in sites]), np.full(len(sites), 4.0))
+    rot = np.cos(angles)[None, :, None] * T0[:, None, :3, 1] + np.sin(angles)[None, :, None] * T0[:, None, :3, 0]
+    all_c = np.repeat(centers, 360, axis=0)
+    T, _ = ctx.place(all_c, all_c + 50.0 * rot.reshape(-1, 3), np.full(all_c.shape[0], 4.0))
+    adm.evaluate_frames(recip, coil, T[:8], 1e6)  # warm-up
+    ev_ms, e = device_ms(lambda: adm.evaluate_frames(recip, coil, T, 1e6))
+    opt_ms, res = device_ms(lambda: adm.optimize_placement(recip, coil, centers, n_samples=9))
+    out = {"what": "magnitude target (3 adjoint directions), 8 sites; grid 3 mm covering any rotation",
+           "adjoint_ms": round(adj_ms, 3), "adjoint_iterations": adjoint.iterations.tolist(),
+           "grid_points": int(grid.n_points), "qfield_ms": round(q_ms, 3),
+           "qfield_gpair_per_s": round(pairs / (q_ms / 1e3) / 1e9, 1),
+           "evaluate_placements": int(T.shape[0]), "evaluate_ms": round(ev_ms, 3),
+           "evaluate_placements_per_s": round(T.shape[0] / (ev_ms / 1e3), 1),
+           "optimize_ms": round(opt_ms, 3), "best_objective_v_per_m": round(res.best_objective, 4),
+           "sweep_max_v_per_m": round(float(np.linalg.norm(e, axis=1).max()), 4)}
+    adjoint.handle.close()
+    return out
 
 
 def cpu_baseline(mesh, coil, sites, recovery, n_place=1) -> dict:
