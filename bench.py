@@ -517,7 +517,9 @@ def adm_measure(ctx, coil, sites, stream) -> dict:
     target = adm.resolve_target(ctx, adm.Target([0.0, 0.0, 72.0]))
     adj_ms, adjoint = device_ms(lambda: adm.solve_adjoint(ctx, target))
     grid = adm._coverage_grid(ctx, coil, centers, 4.0, 3.0, 8.0)
+    torch.cuda.nvtx.range_push("adm_qfield")
     q_ms, recip = device_ms(lambda: adm.sample_qfield(adjoint, grid))
+    torch.cuda.nvtx.range_pop()
     pairs = grid.n_points * ctx.n_nodes * target.directions.shape[0]
     # 360 in-plane rotations per site: handle points around each site's own coil frame.
     angles = np.radians(np.arange(360.0))
@@ -526,7 +528,9 @@ def adm_measure(ctx, coil, sites, stream) -> dict:
     all_c = np.repeat(centers, 360, axis=0)
     T, _ = ctx.place(all_c, all_c + 50.0 * rot.reshape(-1, 3), np.full(all_c.shape[0], 4.0))
     adm.evaluate_frames(recip, coil, T[:8], 1e6)  # warm-up
+    torch.cuda.nvtx.range_push("adm_evaluate")  # lets a profiler capture exactly this launch
     ev_ms, e = device_ms(lambda: adm.evaluate_frames(recip, coil, T, 1e6))
+    torch.cuda.nvtx.range_pop()
     opt_ms, res = device_ms(lambda: adm.optimize_placement(recip, coil, centers, n_samples=9))
     out = {"what": "magnitude target (3 adjoint directions), 8 sites; grid 3 mm covering any rotation",
            "adjoint_ms": round(adj_ms, 3), "adjoint_iterations": adjoint.iterations.tolist(),
