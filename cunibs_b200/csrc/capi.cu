@@ -800,14 +800,10 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         // Operator components on the grounded pattern (assembly.py:99-125): the unperturbed tissues at
         // nominal, then each perturbed tissue at unit conductivity.
         st->comp.resize(static_cast<std::size_t>(1 + P) * st->nnz);
-        double table[11];
-        for (int t = 0; t < 11; ++t) table[t] = (t >= 1 && slots.slot[t] < 0) ? st->nominal[t] : 0.0;
-        assemble_reduced_values(m, table, L0.a, st->comp.get(), s);
-        for (int a = 0; a < P; ++a) {
-            for (double& v : table) v = 0.0;
-            table[st->tags[a]] = 1.0;
-            assemble_reduced_values(m, table, L0.a, st->comp.get() + static_cast<std::size_t>(1 + a) * st->nnz, s);
-        }
+        std::vector<double> tables(11 * static_cast<std::size_t>(1 + P), 0.0);
+        for (int t = 1; t < 11; ++t) tables[t] = slots.slot[t] < 0 ? st->nominal[t] : 0.0;
+        for (int a = 0; a < P; ++a) tables[11 * (1 + a) + st->tags[a]] = 1.0;
+        assemble_reduced_values(m, tables.data(), 1 + P, L0.a, st->comp.get(), s);
         // The components must give back the nominal operator (the gate of assembly.py:126-131).
         {
             SigmaWeights w{};
@@ -848,24 +844,26 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
                     cols.emplace_back(a, j);
                 }
         // Sensitivities s_t = A_nom^-1 c_t to a loose tolerance (run.py:44-49: they only span the
-        // guess's subspace; every draw is still solved to the full tolerance), 16 columns at a time.
+        // guess's subspace; every draw is still solved to the full tolerance), in blocks as wide as
+        // the solver's workspace already is (growing it would reallocate it and drop its graphs).
         st->S.resize(npk);
         st->S.zero(s);
         if (!cols.empty()) {
             Params sp = resolve(c, opts);
             sp.tolerance = sensitivity_tol;
-            DevArray<double> B16(static_cast<std::size_t>(n_red) * 16), X16(static_cast<std::size_t>(n_red) * 16);
-            for (std::size_t q0 = 0; q0 < cols.size(); q0 += 16) {
+            const int W = std::max(K, std::min(16, solver_width_capacity(*c->solver)));
+            DevArray<double> Bw(static_cast<std::size_t>(n_red) * W), Xw(static_cast<std::size_t>(n_red) * W);
+            for (std::size_t q0 = 0; q0 < cols.size(); q0 += W) {
                 SigmaColumns cm{};
-                cm.count = static_cast<int>(std::min<std::size_t>(16, cols.size() - q0));
+                cm.count = static_cast<int>(std::min<std::size_t>(W, cols.size() - q0));
                 for (int l = 0; l < cm.count; ++l) {
                     cm.a[l] = cols[q0 + l].first;
                     cm.j[l] = cols[q0 + l].second;
                 }
-                sigma_pack(C.get(), n_red, P, K, cm, B16.get(), s);
-                SolveStats s16;
-                solver_solve(*c->solver, B16.get(), X16.get(), cm.count, 16, sp, s, s16);
-                sigma_unpack(X16.get(), n_red, P, K, cm, st->S.get(), s);
+                sigma_pack(C.get(), n_red, P, K, cm, W, Bw.get(), s);
+                SolveStats sw;
+                solver_solve(*c->solver, Bw.get(), Xw.get(), cm.count, W, sp, s, sw);
+                sigma_unpack(Xw.get(), n_red, P, K, cm, W, st->S.get(), s);
             }
         }
         // Per placement: the A_nom-Gram of its sensitivities and their products with the c_t give

@@ -133,11 +133,11 @@ void assemble_stiffness(Mesh& m, const double* sigma_by_tag /* 11 entries or nul
 // validate: fail when the table leaves a tag of the mesh undefined (a host synchronisation); a
 // caller whose table has passed that check once for the same tags may skip it.
 void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s, bool validate = true);
-// Grounded stiffness values of a conductivity table whose entries may be zero, on the grounded
-// pattern (out: pattern.nnz), without touching the mesh's own values; the operator's linearity in
-// sigma makes a table with one unit entry give that tissue's share of it.
-void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, const DevCsr<double>& pattern, double* out,
-                             cudaStream_t s);
+// Grounded stiffness values of n_tables conductivity tables (11 entries each, zeros allowed) on the
+// grounded pattern, out (n_tables, pattern.nnz), without touching the mesh's own values; the
+// operator's linearity in sigma makes a table with one unit entry give that tissue's share of it.
+void assemble_reduced_values(const Mesh& m, const double* tables, int n_tables, const DevCsr<double>& pattern,
+                             double* out, cudaStream_t s);
 void reduce_grounded(const Mesh& m, DevCsr<double>& out, cudaStream_t s);
 // The grounded values of the mesh's stiffness on a grounded pattern already built (out: pattern.nnz).
 void reduce_grounded_values(const Mesh& m, const DevCsr<double>& pattern, double* out, cudaStream_t s);
@@ -169,6 +169,9 @@ SolverPtr make_solver(const Hierarchy& h, const Params& p);
 void solver_solve(Solver& sv, const double* B, double* X, int k, int k_pad, const Params& p, cudaStream_t s,
                   SolveStats& stats, const double* X0 = nullptr);
 void solver_vcycle(Solver& sv, const double* r, double* z, int k, bool fp32, cudaStream_t s);
+// The widest block the solver's workspace holds now (solving wider grows it: every workspace
+// array is reallocated and the captured loop graphs are dropped).
+int solver_width_capacity(const Solver& sv);
 
 // Coil and right-hand side (coil.cu).
 void place_transforms(const Mesh& m, const double* centers, const double* handles, const double* dists, int k,
@@ -318,8 +321,9 @@ void sigma_sens_rhs(const Mesh& m, const double* x_red, const float* dadt_elm, i
 std::vector<double> sigma_gram(const double* U, const double* V, long n, int P, int K, cudaStream_t s);
 // Y (n, W) = A X (n, W) in FP64.
 void sigma_spmv(const DevCsr<double>& A, const double* X, int W, double* Y, cudaStream_t s);
-void sigma_pack(const double* C, int n, int P, int K, const SigmaColumns& cm, double* B16, cudaStream_t s);
-void sigma_unpack(const double* X16, int n, int P, int K, const SigmaColumns& cm, double* S, cudaStream_t s);
+// A W-wide solve block (n, W) from the chosen columns of an (n, P, K) array, and back.
+void sigma_pack(const double* C, int n, int P, int K, const SigmaColumns& cm, int W, double* Bw, cudaStream_t s);
+void sigma_unpack(const double* Xw, int n, int P, int K, const SigmaColumns& cm, int W, double* S, cudaStream_t s);
 // X0 (n, K) = x_nom + S y per placement.
 void sigma_guess(const double* x_nom, const double* S, int n, int P, int K, int k, const SigmaDraw& y, double* X0,
                  cudaStream_t s);

@@ -646,22 +646,25 @@ void reduce_grounded_values(const Mesh& m, const DevCsr<double>& pattern, double
     CUNIBS_LAUNCH_CHECK("grounded values");
 }
 
-void assemble_reduced_values(const Mesh& m, const double* sigma_by_tag, const DevCsr<double>& pattern, double* out,
-                             cudaStream_t s) {
-    CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
+void assemble_reduced_values(const Mesh& m, const double* tables, int n_tables, const DevCsr<double>& pattern,
+                             double* out, cudaStream_t s) {
+    if (pattern.n != m.n_nodes - 1) fail(kEInternal, "grounded pattern of another mesh");
     const int M = m.n_tets;
     DevArray<double> cond(M), full(m.k_nnz);
     DevArray<int> bad(1);
-    bad.zero(s);
-    conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), M, cond.get(), bad.get()); count_launch();
-    if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
-    assemble_entries_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(m.g.get(), m.vols.get(), cond.get(),
-                                                                 m.contrib_ptr.get(), m.contrib_idx.get(), m.k_nnz,
-                                                                 full.get()); count_launch();
-    if (pattern.n != m.n_nodes - 1) fail(kEInternal, "grounded pattern of another mesh");
-    reduced_values_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), full.get(),
-                                                                     m.n_nodes, m.ground, pattern.ptr.get(), out);
-    count_launch();
+    for (int t = 0; t < n_tables; ++t) {
+        CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, tables + 11 * t, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
+        bad.zero(s);
+        conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), M, cond.get(), bad.get()); count_launch();
+        if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
+        assemble_entries_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(m.g.get(), m.vols.get(), cond.get(),
+                                                                     m.contrib_ptr.get(), m.contrib_idx.get(), m.k_nnz,
+                                                                     full.get()); count_launch();
+        reduced_values_kernel<<<grid_for(m.n_nodes - 1), kBlock, 0, s>>>(m.k_ptr.get(), m.k_col.get(), full.get(),
+                                                                         m.n_nodes, m.ground, pattern.ptr.get(),
+                                                                         out + static_cast<std::size_t>(t) * pattern.nnz);
+        count_launch();
+    }
     CUNIBS_LAUNCH_CHECK("reduced stiffness values");
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }

@@ -149,26 +149,26 @@ __global__ void spmv_cols_kernel(const int* __restrict__ ptr, const int* __restr
     Y[q] = acc;
 }
 
-// A 16-wide solve block from chosen (a, j) columns of an (n, P, K) array; lanes past count repeat
-// the last chosen column (the padding of a partial block).
-__global__ void pack_columns_kernel(const double* __restrict__ C, int n, int P, int K, SigmaColumns cm,
-                                    double* __restrict__ B16) {
+// A W-wide solve block (W <= 16) from chosen (a, j) columns of an (n, P, K) array; lanes past
+// count repeat the last chosen column (the padding of a partial block).
+__global__ void pack_columns_kernel(const double* __restrict__ C, int n, int P, int K, SigmaColumns cm, int W,
+                                    double* __restrict__ Bw) {
     const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q >= static_cast<long>(n) * 16) return;
-    const long r = q >> 4;
-    const int l = static_cast<int>(q & 15);
+    if (q >= static_cast<long>(n) * W) return;
+    const long r = q / W;
+    const int l = static_cast<int>(q % W);
     const int u = l < cm.count ? l : cm.count - 1;
-    B16[q] = C[(r * P + cm.a[u]) * K + cm.j[u]];
+    Bw[q] = C[(r * P + cm.a[u]) * K + cm.j[u]];
 }
 
-__global__ void unpack_columns_kernel(const double* __restrict__ X16, int n, int P, int K, SigmaColumns cm,
+__global__ void unpack_columns_kernel(const double* __restrict__ Xw, int n, int P, int K, SigmaColumns cm, int W,
                                       double* __restrict__ S) {
     const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (q >= static_cast<long>(n) * 16) return;
-    const long r = q >> 4;
-    const int l = static_cast<int>(q & 15);
+    if (q >= static_cast<long>(n) * W) return;
+    const long r = q / W;
+    const int l = static_cast<int>(q % W);
     if (l >= cm.count) return;
-    S[(r * P + cm.a[l]) * K + cm.j[l]] = X16[q];
+    S[(r * P + cm.a[l]) * K + cm.j[l]] = Xw[q];
 }
 
 // X0[r][j] = x_nom[r][j] + sum_a S[r][a][j] y[a][j] (columns past k repeat column k-1).
@@ -257,13 +257,15 @@ void sigma_spmv(const DevCsr<double>& A, const double* X, int W, double* Y, cuda
     CUNIBS_LAUNCH_CHECK("sigma spmv");
 }
 
-void sigma_pack(const double* C, int n, int P, int K, const SigmaColumns& cm, double* B16, cudaStream_t s) {
-    pack_columns_kernel<<<grid_for(static_cast<std::int64_t>(n) * 16), kBlock, 0, s>>>(C, n, P, K, cm, B16); count_launch();
+void sigma_pack(const double* C, int n, int P, int K, const SigmaColumns& cm, int W, double* Bw, cudaStream_t s) {
+    if (W < 1 || W > 16 || cm.count < 1 || cm.count > W) fail(kEInval, "sigma pack: 1 <= count <= W <= 16");
+    pack_columns_kernel<<<grid_for(static_cast<std::int64_t>(n) * W), kBlock, 0, s>>>(C, n, P, K, cm, W, Bw); count_launch();
     CUNIBS_LAUNCH_CHECK("sigma pack");
 }
 
-void sigma_unpack(const double* X16, int n, int P, int K, const SigmaColumns& cm, double* S, cudaStream_t s) {
-    unpack_columns_kernel<<<grid_for(static_cast<std::int64_t>(n) * 16), kBlock, 0, s>>>(X16, n, P, K, cm, S); count_launch();
+void sigma_unpack(const double* Xw, int n, int P, int K, const SigmaColumns& cm, int W, double* S, cudaStream_t s) {
+    if (W < 1 || W > 16 || cm.count < 1 || cm.count > W) fail(kEInval, "sigma unpack: 1 <= count <= W <= 16");
+    unpack_columns_kernel<<<grid_for(static_cast<std::int64_t>(n) * W), kBlock, 0, s>>>(Xw, n, P, K, cm, W, S); count_launch();
     CUNIBS_LAUNCH_CHECK("sigma unpack");
 }
 

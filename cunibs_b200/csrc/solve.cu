@@ -1344,6 +1344,8 @@ void solver_solve(Solver& sv, const double* Bin, double* Xout, int k, int K, con
     });
 }
 
+int solver_width_capacity(const Solver& sv) { return sv.kcap; }
+
 void solver_vcycle(Solver& sv, const double* r, double* z, int k, bool fp32, cudaStream_t s) {
     (void)fp32;
     dispatch_k(k, [&](auto kc) {
