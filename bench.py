@@ -319,6 +319,12 @@ def run_ours(args) -> dict:
     pipelined(2, warm=False)
     cold_ms, cold_its, _ = pipelined(n_cmp, warm=False)
     cold_it = float(d_it.float().mean().item())
+    proj = None
+    if args.warm_start == "on":
+        # The Galerkin projection of each block's right-hand sides onto the network's basis (no network).
+        pipelined(2, warm="projection")
+        proj_ms, _, _ = pipelined(n_cmp, warm="projection")
+        proj = (proj_ms, float(d_it.float().mean().item()), [round(v, 5) for v in d_rel0.cpu().numpy().tolist()])
     pipelined(2, precision=_native.PREC_MIXED, warm=False)
     mixed_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_MIXED, warm=False)
     mixed_it = float(d_it.float().mean().item())
@@ -402,6 +408,10 @@ def run_ours(args) -> dict:
                                                      "what": "FP32 PCG + FP32 V-cycle inside FP64 refinement"},
                      "one_block_at_a_time": {"value": round(seq_value, 3),
                                              "what": "this configuration without the two-deep pipeline"},
+                     "basis_projection_guess": None if proj is None else {
+                         "value": round(job_throughput(proj[0], n_cmp, world, dist, dev)[1], 3),
+                         "iterations": proj[1], "init_relres": proj[2],
+                         "what": "Galerkin projection of the right-hand sides onto the learned basis, no network"},
                      "this_run": {"warm_start": args.warm_start, "iterations": col_iters,
                                   "warm_used": warm_used, "init_relres": [round(v, 5) for v in warm_rel0]}},
         "warm_start": warm_stats,

@@ -203,6 +203,17 @@ def check(rc: int) -> None:
     raise NativeError(rc, msg)
 
 
+def _guess_code(warm_start) -> int:
+    """cunibs_solve_opts.warm_start: False/0 none, True/1 the network, "projection"/2 the Galerkin
+    projection onto the network's basis."""
+    if warm_start == "projection":
+        return 2
+    code = int(warm_start)
+    if code not in (0, 1, 2):
+        raise ValueError("warm_start must be False, True or 'projection'")
+    return code
+
+
 def _p(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(_vp)
 
@@ -410,7 +421,7 @@ class Context:
                        out_ptrs.get("relres"), out_ptrs.get("magnE"), out_ptrs.get("E"), out_ptrs.get("v"), 0, 0,
                        out_ptrs.get("E_slots"), out_ptrs.get("warm_used"), out_ptrs.get("init_relres"))
         opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
-                         int(bool(warm_start)))
+                         _guess_code(warm_start))
         check(self._lib.cunibs_solve_block_device(self.handle, pos, mom, int(n_dip), centers, handles, dists, int(k),
                                                   float(didt), C.byref(opts), C.byref(out)))
         return out.total_iterations, out.outer_steps
@@ -421,7 +432,7 @@ class Context:
         """cunibs_submit_block_device: prepare a block on raw device pointers (ints) without waiting;
         returns its ticket."""
         opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
-                         int(bool(warm_start)))
+                         _guess_code(warm_start))
         t = C.c_longlong(0)
         check(self._lib.cunibs_submit_block_device(self.handle, pos, mom, int(n_dip), centers, handles, dists, int(k),
                                                    float(didt), C.byref(opts), C.byref(t)))
@@ -532,7 +543,7 @@ class Context:
         k = centers.shape[0]
         res, out = self._block_outputs(k, magnitude, vectors, potential, recovery, nodal)
         opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
-                         int(bool(warm_start)))
+                         _guess_code(warm_start))
         check(self._lib.cunibs_solve_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
                                            _p(dists), k, float(didt), C.byref(opts), C.byref(out)))
         res["total_iterations"] = out.total_iterations
@@ -549,7 +560,7 @@ class Context:
         if nodal and recovery == "raw":
             raise ValueError("nodal=True needs a recovery mode")
         opts = SolveOpts(int(block_width), int(precision), float(tolerance), int(max_iters), RECOVERY_CODES[recovery],
-                         int(bool(warm_start)))
+                         _guess_code(warm_start))
         t = C.c_longlong(0)
         check(self._lib.cunibs_submit_block(self.handle, _p(pos), _p(mom), pos.shape[0], _p(centers), _p(handles),
                                             _p(dists), k, float(didt), C.byref(opts), C.byref(t)))

@@ -244,6 +244,8 @@ long long prepare_block(cunibs_context* c, const double* pos, const double* mom,
     require(rec_mode >= kRecRaw && rec_mode <= kRecHarmonic, "unknown recovery mode");
     const bool warm = opts && opts->warm_start;
     if (warm) {
+        require(opts->warm_start == kGuessNetwork || opts->warm_start == kGuessProjection,
+                "warm_start must be 0, 1 (network) or 2 (projection onto its basis)");
         require(c->warm != nullptr, "warm_start requested but no warm-start network is installed");
         require(c->warm->n_red == c->mesh.n_nodes - 1, "the installed warm start was built for another mesh");
     }
@@ -334,7 +336,7 @@ void issue_guess(cunibs_context* c, PendingBlock& q) {
     BlockSlot& ql = c->slots[q.slot];
     CUNIBS_CHECK(cudaStreamWaitEvent(c->stream, ql.prepared, 0));
     ql.X0.reserve(static_cast<std::size_t>(c->mesh.n_nodes - 1) * q.K);
-    warm_start_guess(*c->warm, ql.T.get(), q.k, q.K, ql.X0.get(), c->stream);
+    warm_start_guess(*c->warm, ql.T.get(), ql.B.get(), q.k, q.K, ql.X0.get(), q.opts.warm_start, c->stream);
     q.guess_due = false;
 }
 

@@ -268,7 +268,11 @@ constexpr int kWarmInPad = 64;  // pose features (6) padded to one BF16 swizzle 
 // (n_red, K); nothing waits on the host. The solver applies the per-column zero-guess fallback
 // (SolveStats::col_init_rel). warm_start_check (after the solve) raises if a GEMM's bounded wait
 // expired.
-void warm_start_guess(WarmStart& ws, const double* T_dev, int k, int K, double* X0, cudaStream_t s);
+// Guess sources (cunibs_solve_opts.warm_start): the network's coefficients from the coil pose, or
+// the Galerkin projection of the block's right-hand sides B (n_red, K) onto the same basis.
+enum GuessMode : int { kGuessNone = 0, kGuessNetwork = 1, kGuessProjection = 2 };
+void warm_start_guess(WarmStart& ws, const double* T_dev, const double* B, int k, int K, double* X0, int mode,
+                      cudaStream_t s);
 void warm_start_check(WarmStart& ws, cudaStream_t s);
 void pose_features(const double* T_dev, int k, const float* mean, const float* std, __nv_bfloat16* x16, int ld,
                    cudaStream_t s);

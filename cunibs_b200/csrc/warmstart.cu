@@ -126,6 +126,51 @@ __global__ void denorm_kernel(const float* __restrict__ pred, int k, int n_out, 
     c16[(16 + i) * w + ld + j] = __float2bfloat16_rn(0.0f);
 }
 
+// Galerkin coefficients of the right-hand sides in the A-orthonormal basis, c[j][a] = sum_n
+// W[n][a] b[n][j] with W = V_hi + V_lo (the stored split basis), partial sums over fixed row
+// ranges: block g takes rows g, g + grid, ... in order; thread t owns basis columns t, t + threads.
+constexpr int kProjThreads = 256;
+constexpr int kProjBlocks = 296;
+__global__ void __launch_bounds__(kProjThreads) project_kernel(const __nv_bfloat16* __restrict__ basis, int n, int ld,
+                                                               int n_out, const double* __restrict__ B, int K, int k,
+                                                               double* __restrict__ part) {
+    constexpr int kMaxK = 16;
+    for (int a = threadIdx.x; a < n_out; a += kProjThreads) {
+        double acc[kMaxK];
+#pragma unroll
+        for (int j = 0; j < kMaxK; ++j) acc[j] = 0.0;
+        for (int row = blockIdx.x; row < n; row += gridDim.x) {
+            const __nv_bfloat16* w = basis + static_cast<std::int64_t>(row) * 2 * ld;
+            const double wv = static_cast<double>(__bfloat162float(w[a])) + static_cast<double>(__bfloat162float(w[ld + a]));
+            const double* b = B + static_cast<std::int64_t>(row) * K;
+#pragma unroll
+            for (int j = 0; j < kMaxK; ++j)
+                if (j < k) acc[j] = fma(wv, b[j], acc[j]);
+        }
+        for (int j = 0; j < k; ++j) part[(static_cast<std::int64_t>(blockIdx.x) * k + j) * n_out + a] = acc[j];
+    }
+}
+
+// Sum of the per-block partials in block order, split into the prolongation operand (rows [c_hi | c_hi]
+// and [c_lo | 0], as denorm_kernel writes them).
+__global__ void project_final_kernel(const double* __restrict__ part, int blocks, int k, int n_out, int ld,
+                                     __nv_bfloat16* __restrict__ c16) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= 16 * ld) return;
+    const int i = q / ld, j = q % ld;
+    double v = 0.0;
+    if (i < k && j < n_out)
+        for (int g = 0; g < blocks; ++g) v += part[(static_cast<std::int64_t>(g) * k + i) * n_out + j];
+    const float vf = static_cast<float>(v);
+    const __nv_bfloat16 hi = __float2bfloat16_rn(vf);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(vf - __bfloat162float(hi));
+    const std::int64_t w = 2 * static_cast<std::int64_t>(ld);
+    c16[i * w + j] = hi;
+    c16[i * w + ld + j] = hi;
+    c16[(16 + i) * w + j] = lo;
+    c16[(16 + i) * w + ld + j] = __float2bfloat16_rn(0.0f);
+}
+
 // X0[row, c] (FP64, width K) = x0f[row, c] + x0f[row, 16 + c] for the k predicted columns.
 __global__ void widen_kernel(const float* __restrict__ x0f, int n, int ldf, int k, int K, double* __restrict__ X0) {
     const std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -144,59 +189,75 @@ void pose_features(const double* T_dev, int k, const float* mean, const float* s
     CUNIBS_LAUNCH_CHECK("pose features");
 }
 
-void warm_start_guess(WarmStart& ws, const double* T_dev, int k, int K, double* X0, cudaStream_t s) {
+void warm_start_guess(WarmStart& ws, const double* T_dev, const double* B, int k, int K, double* X0, int mode,
+                      cudaStream_t s) {
     constexpr int kRowsPad = 16;  // the network's batch (k <= 16), one BN = 16 GEMM tile wide
     const int depth = ws.depth;
-    ws.x16.reserve(kRowsPad * kWarmInPad);
-    ws.h16a.reserve(kRowsPad * ws.hidden);
-    ws.h16b.reserve(kRowsPad * ws.hidden);
-    ws.pred.reserve(static_cast<std::size_t>(kRowsPad) * ws.n_out_pad);
-    ws.c16.reserve(static_cast<std::size_t>(2 * kRowsPad) * 2 * ws.n_out_pad);
-    ws.x0f.reserve(static_cast<std::size_t>(ws.n_red) * 2 * kRowsPad);
-    ws.partials.reserve(1);
-    ws.norms.reserve(16);
-    ws.error.reserve(1);
-    CUNIBS_CHECK(cudaMemsetAsync(ws.x16.get(), 0, sizeof(__nv_bfloat16) * kRowsPad * kWarmInPad, s));
-    pose_features(T_dev, k, ws.in_mean.get(), ws.in_std.get(), ws.x16.get(), kWarmInPad, s);
-    // Hidden layers: h = silu(x W^T + b).
-    const __nv_bfloat16* in = ws.x16.get();
-    int in_dim = kWarmInPad;
-    for (int l = 0; l < depth; ++l) {
-        __nv_bfloat16* out = (l % 2 == 0) ? ws.h16a.get() : ws.h16b.get();
+    if (mode == kGuessProjection) {
+        // The Galerkin projection onto the basis: the A-norm-best guess it spans, from the
+        // right-hand sides themselves (no network).
+        ws.c16.reserve(static_cast<std::size_t>(2 * kRowsPad) * 2 * ws.n_out_pad);
+        ws.x0f.reserve(static_cast<std::size_t>(ws.n_red) * 2 * kRowsPad);
+        ws.error.reserve(1);
+        ws.partials.reserve(static_cast<std::size_t>(kProjBlocks) * k * ws.n_out);
+        project_kernel<<<kProjBlocks, kProjThreads, 0, s>>>(ws.basis.get(), ws.n_red, ws.n_out_pad, ws.n_out, B, K, k,
+                                                            ws.partials.get());
+        count_launch();
+        project_final_kernel<<<grid_for(16 * ws.n_out_pad), kBlock, 0, s>>>(ws.partials.get(), kProjBlocks, k, ws.n_out,
+                                                                            ws.n_out_pad, ws.c16.get());
+        count_launch();
+    } else {
+        ws.x16.reserve(kRowsPad * kWarmInPad);
+        ws.h16a.reserve(kRowsPad * ws.hidden);
+        ws.h16b.reserve(kRowsPad * ws.hidden);
+        ws.pred.reserve(static_cast<std::size_t>(kRowsPad) * ws.n_out_pad);
+        ws.c16.reserve(static_cast<std::size_t>(2 * kRowsPad) * 2 * ws.n_out_pad);
+        ws.x0f.reserve(static_cast<std::size_t>(ws.n_red) * 2 * kRowsPad);
+        ws.partials.reserve(1);
+        ws.norms.reserve(16);
+        ws.error.reserve(1);
+        CUNIBS_CHECK(cudaMemsetAsync(ws.x16.get(), 0, sizeof(__nv_bfloat16) * kRowsPad * kWarmInPad, s));
+        pose_features(T_dev, k, ws.in_mean.get(), ws.in_std.get(), ws.x16.get(), kWarmInPad, s);
+        // Hidden layers: h = silu(x W^T + b).
+        const __nv_bfloat16* in = ws.x16.get();
+        int in_dim = kWarmInPad;
+        for (int l = 0; l < depth; ++l) {
+            __nv_bfloat16* out = (l % 2 == 0) ? ws.h16a.get() : ws.h16b.get();
+            GemmProblem g;
+            g.a = in;
+            g.lda = in_dim;
+            g.b = ws.w16[l].get();
+            g.ldb = in_dim;
+            g.M = kRowsPad;
+            g.N = ws.hidden;
+            g.K = in_dim;
+            g.ep.bias = ws.bias[l].get();
+            g.ep.act = 1;
+            g.ep.out16 = out;
+            g.ep.ld_out = ws.hidden;
+            g.ep.error = ws.error.get();
+            gemm_bf16(g, s);
+            in = out;
+            in_dim = ws.hidden;
+        }
         GemmProblem g;
         g.a = in;
         g.lda = in_dim;
-        g.b = ws.w16[l].get();
+        g.b = ws.w16[depth].get();
         g.ldb = in_dim;
         g.M = kRowsPad;
-        g.N = ws.hidden;
+        g.N = ws.n_out_pad;
         g.K = in_dim;
-        g.ep.bias = ws.bias[l].get();
-        g.ep.act = 1;
-        g.ep.out16 = out;
-        g.ep.ld_out = ws.hidden;
+        g.ep.bias = ws.bias[depth].get();
+        g.ep.out32 = ws.pred.get();
+        g.ep.ld_out = ws.n_out_pad;
         g.ep.error = ws.error.get();
         gemm_bf16(g, s);
-        in = out;
-        in_dim = ws.hidden;
+        denorm_kernel<<<grid_for(kRowsPad * ws.n_out_pad), kBlock, 0, s>>>(ws.pred.get(), k, ws.n_out, ws.n_out_pad,
+                                                                            ws.out_mean.get(), ws.out_std.get(),
+                                                                            ws.c16.get());
+        count_launch();
     }
-    GemmProblem g;
-    g.a = in;
-    g.lda = in_dim;
-    g.b = ws.w16[depth].get();
-    g.ldb = in_dim;
-    g.M = kRowsPad;
-    g.N = ws.n_out_pad;
-    g.K = in_dim;
-    g.ep.bias = ws.bias[depth].get();
-    g.ep.out32 = ws.pred.get();
-    g.ep.ld_out = ws.n_out_pad;
-    g.ep.error = ws.error.get();
-    gemm_bf16(g, s);
-    denorm_kernel<<<grid_for(kRowsPad * ws.n_out_pad), kBlock, 0, s>>>(ws.pred.get(), k, ws.n_out, ws.n_out_pad,
-                                                                        ws.out_mean.get(), ws.out_std.get(),
-                                                                        ws.c16.get());
-    count_launch();
     // Prolongation through the basis: [n_red, 32] = [V_hi | V_lo] [n_red, 2r] . c16 [32, 2r]^T.
     GemmProblem p;
     p.a = ws.basis.get();

@@ -99,7 +99,9 @@ typedef struct {
     double tolerance;  /* <= 0: context default */
     int max_iters;     /* <= 0: context default */
     int recovery;      /* CUNIBS_RECOVERY_*; 0 = raw. magnE, E and the summary describe this field */
-    int warm_start;    /* 1: start PCG from the installed network's guess (cunibs_context_set_warmstart) */
+    int warm_start;    /* 1: start PCG from the installed network's guess (cunibs_context_set_warmstart);
+                          2: from the Galerkin projection of the right-hand sides onto that network's
+                          basis (no network: the A-norm-best guess the basis spans) */
 } cunibs_solve_opts;
 
 /* Outputs of a block solve of k placements. Required: transforms, summary. Optional (NULL to

@@ -162,6 +162,16 @@ def test_warm_start_cuts_iterations_and_keeps_the_answer(ws_subject):
             a, b = outs[True]["magnE"][:, gm].astype(np.float64), outs[False]["magnE"][:, gm].astype(np.float64)
             assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5
         gain[prec] = np.mean(iters[False]) - np.mean(iters[True])
+        if prec == _native.PREC_SPLIT:
+            # The Galerkin projection of the right-hand sides onto the same basis is the A-norm-best
+            # guess it spans: it needs no more iterations than the network's and gives the same answer.
+            proj = [ctx.solve_block(coil, centers[s:s + 8], handles[s:s + 8], dists, 1e6, magnitude=True,
+                                    warm_start="projection", precision=prec) for s in (0, 8)]
+            assert all(o["warm_used"].all() and (o["relative_residual"] <= 1e-8).all() for o in proj)
+            assert np.mean([o["iterations"] for o in proj]) <= np.mean(iters[True])
+            gm = ws_subject.mesh.tet_tags == 2
+            a = proj[1]["magnE"][:, gm].astype(np.float64)
+            assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5
     # The guess must save the FP64 Krylov methods (plain, and FP64 PCG over the FP32 V-cycle)
     # iterations. Iterative refinement restarts its FP32 inner solve at every step with a target
     # relative to the current residual (and carries Ap by its FP32 recurrence), so a better start
