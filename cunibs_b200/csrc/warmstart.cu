@@ -127,40 +127,75 @@ __global__ void denorm_kernel(const float* __restrict__ pred, int k, int n_out, 
 }
 
 // Galerkin coefficients of the right-hand sides in the A-orthonormal basis, c[j][a] = sum_n
-// W[n][a] b[n][j] with W = V_hi + V_lo (the stored split basis), partial sums over fixed row
-// ranges: block g takes rows g, g + grid, ... in order; thread t owns basis columns t, t + threads.
+// W[n][a] b[n][j] with W = V_hi + V_lo (the stored split basis). Block g takes the contiguous row
+// range [g * rows_per, (g + 1) * rows_per) in order, kProjUnroll rows per step with their basis loads
+// issued together; thread t owns basis column t (the basis is at most kProjThreads wide per pass,
+// wider bases loop). The block's right-hand-side rows are staged in shared memory.
 constexpr int kProjThreads = 256;
-constexpr int kProjBlocks = 296;
+constexpr int kProjBlocks = 592;
+constexpr int kProjUnroll = 8;
+constexpr int kProjStage = 64;  // right-hand-side rows staged per step (kProjStage x 16 doubles)
 __global__ void __launch_bounds__(kProjThreads) project_kernel(const __nv_bfloat16* __restrict__ basis, int n, int ld,
                                                                int n_out, const double* __restrict__ B, int K, int k,
-                                                               double* __restrict__ part) {
+                                                               int rows_per, double* __restrict__ part) {
     constexpr int kMaxK = 16;
-    for (int a = threadIdx.x; a < n_out; a += kProjThreads) {
+    __shared__ double sb[kProjStage][kMaxK];
+    const int r0 = blockIdx.x * rows_per;
+    const int r1 = min(n, r0 + rows_per);
+    for (int a0 = 0; a0 < n_out; a0 += kProjThreads) {
+        const int a = a0 + threadIdx.x;
         double acc[kMaxK];
 #pragma unroll
         for (int j = 0; j < kMaxK; ++j) acc[j] = 0.0;
-        for (int row = blockIdx.x; row < n; row += gridDim.x) {
-            const __nv_bfloat16* w = basis + static_cast<std::int64_t>(row) * 2 * ld;
-            const double wv = static_cast<double>(__bfloat162float(w[a])) + static_cast<double>(__bfloat162float(w[ld + a]));
-            const double* b = B + static_cast<std::int64_t>(row) * K;
+        for (int s0 = r0; s0 < r1; s0 += kProjStage) {
+            const int ns = min(kProjStage, r1 - s0);
+            __syncthreads();
+            for (int q = threadIdx.x; q < kProjStage * kMaxK; q += kProjThreads) {
+                const int rr = q / kMaxK, j = q % kMaxK;
+                sb[rr][j] = (rr < ns && j < k) ? B[static_cast<std::int64_t>(s0 + rr) * K + j] : 0.0;
+            }
+            __syncthreads();
+            if (a < n_out) {
+                for (int u0 = 0; u0 < ns; u0 += kProjUnroll) {
+                    double wv[kProjUnroll];
+#pragma unroll
+                    for (int u = 0; u < kProjUnroll; ++u) {
+                        wv[u] = 0.0;
+                        if (u0 + u < ns) {
+                            const __nv_bfloat16* w = basis + static_cast<std::int64_t>(s0 + u0 + u) * 2 * ld;
+                            wv[u] = static_cast<double>(__bfloat162float(w[a])) +
+                                    static_cast<double>(__bfloat162float(w[ld + a]));
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kProjUnroll; ++u)
+#pragma unroll
+                        for (int j = 0; j < kMaxK; ++j)
+                            if (j < k) acc[j] = fma(wv[u], sb[u0 + u < ns ? u0 + u : 0][j], acc[j]);
+                }
+            }
+        }
+        if (a < n_out)
 #pragma unroll
             for (int j = 0; j < kMaxK; ++j)
-                if (j < k) acc[j] = fma(wv, b[j], acc[j]);
-        }
-        for (int j = 0; j < k; ++j) part[(static_cast<std::int64_t>(blockIdx.x) * k + j) * n_out + a] = acc[j];
+                if (j < k) part[(static_cast<std::int64_t>(blockIdx.x) * k + j) * n_out + a] = acc[j];
     }
 }
 
-// Sum of the per-block partials in block order, split into the prolongation operand (rows [c_hi | c_hi]
-// and [c_lo | 0], as denorm_kernel writes them).
+// One warp per coefficient: the per-block partials summed in a fixed order (lane l takes blocks
+// l, l + 32, ..., then a fixed shuffle tree), then split into the prolongation operand (rows
+// [c_hi | c_hi] and [c_lo | 0], as denorm_kernel writes them).
 __global__ void project_final_kernel(const double* __restrict__ part, int blocks, int k, int n_out, int ld,
                                      __nv_bfloat16* __restrict__ c16) {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= 16 * ld) return;
-    const int i = q / ld, j = q % ld;
+    const int warp = static_cast<int>((static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) / kWarp);
+    const int lane = threadIdx.x % kWarp;
+    if (warp >= 16 * ld) return;
+    const int i = warp / ld, j = warp % ld;
     double v = 0.0;
     if (i < k && j < n_out)
-        for (int g = 0; g < blocks; ++g) v += part[(static_cast<std::int64_t>(g) * k + i) * n_out + j];
+        for (int g = lane; g < blocks; g += kWarp) v += part[(static_cast<std::int64_t>(g) * k + i) * n_out + j];
+    for (int off = kWarp / 2; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane != 0) return;
     const float vf = static_cast<float>(v);
     const __nv_bfloat16 hi = __float2bfloat16_rn(vf);
     const __nv_bfloat16 lo = __float2bfloat16_rn(vf - __bfloat162float(hi));
@@ -199,12 +234,14 @@ void warm_start_guess(WarmStart& ws, const double* T_dev, const double* B, int k
         ws.c16.reserve(static_cast<std::size_t>(2 * kRowsPad) * 2 * ws.n_out_pad);
         ws.x0f.reserve(static_cast<std::size_t>(ws.n_red) * 2 * kRowsPad);
         ws.error.reserve(1);
-        ws.partials.reserve(static_cast<std::size_t>(kProjBlocks) * k * ws.n_out);
-        project_kernel<<<kProjBlocks, kProjThreads, 0, s>>>(ws.basis.get(), ws.n_red, ws.n_out_pad, ws.n_out, B, K, k,
-                                                            ws.partials.get());
+        const int rows_per = (ws.n_red + kProjBlocks - 1) / kProjBlocks;
+        const int blocks = (ws.n_red + rows_per - 1) / rows_per;
+        ws.partials.reserve(static_cast<std::size_t>(blocks) * k * ws.n_out);
+        project_kernel<<<blocks, kProjThreads, 0, s>>>(ws.basis.get(), ws.n_red, ws.n_out_pad, ws.n_out, B, K, k,
+                                                       rows_per, ws.partials.get());
         count_launch();
-        project_final_kernel<<<grid_for(16 * ws.n_out_pad), kBlock, 0, s>>>(ws.partials.get(), kProjBlocks, k, ws.n_out,
-                                                                            ws.n_out_pad, ws.c16.get());
+        project_final_kernel<<<grid_for(static_cast<std::int64_t>(16) * ws.n_out_pad * kWarp), kBlock, 0, s>>>(
+            ws.partials.get(), blocks, k, ws.n_out, ws.n_out_pad, ws.c16.get());
         count_launch();
     } else {
         ws.x16.reserve(kRowsPad * kWarmInPad);
