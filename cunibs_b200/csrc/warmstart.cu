@@ -13,6 +13,8 @@
 #include <cmath>
 
 #include "../../include/cunibs_b200.h"
+#include <type_traits>
+
 #include "internal.hpp"
 
 namespace cunibs {
@@ -135,10 +137,10 @@ constexpr int kProjThreads = 256;
 constexpr int kProjBlocks = 592;
 constexpr int kProjUnroll = 8;
 constexpr int kProjStage = 64;  // right-hand-side rows staged per step (kProjStage x 16 doubles)
+template <int kMaxK>
 __global__ void __launch_bounds__(kProjThreads) project_kernel(const __nv_bfloat16* __restrict__ basis, int n, int ld,
                                                                int n_out, const double* __restrict__ B, int K, int k,
                                                                int rows_per, double* __restrict__ part) {
-    constexpr int kMaxK = 16;
     __shared__ double sb[kProjStage][kMaxK];
     const int r0 = blockIdx.x * rows_per;
     const int r1 = min(n, r0 + rows_per);
@@ -237,8 +239,17 @@ void warm_start_guess(WarmStart& ws, const double* T_dev, const double* B, int k
         const int rows_per = (ws.n_red + kProjBlocks - 1) / kProjBlocks;
         const int blocks = (ws.n_red + rows_per - 1) / rows_per;
         ws.partials.reserve(static_cast<std::size_t>(blocks) * k * ws.n_out);
-        project_kernel<<<blocks, kProjThreads, 0, s>>>(ws.basis.get(), ws.n_red, ws.n_out_pad, ws.n_out, B, K, k,
-                                                       rows_per, ws.partials.get());
+        // Accumulators for the block's own width only (K in {1, 2, 4, 8, 16}).
+        auto go = [&](auto kc) {
+            constexpr int KK = decltype(kc)::value;
+            project_kernel<KK><<<blocks, kProjThreads, 0, s>>>(ws.basis.get(), ws.n_red, ws.n_out_pad, ws.n_out, B, K,
+                                                               k, rows_per, ws.partials.get());
+        };
+        if (K <= 1) go(std::integral_constant<int, 1>{});
+        else if (K <= 2) go(std::integral_constant<int, 2>{});
+        else if (K <= 4) go(std::integral_constant<int, 4>{});
+        else if (K <= 8) go(std::integral_constant<int, 8>{});
+        else go(std::integral_constant<int, 16>{});
         count_launch();
         project_final_kernel<<<grid_for(static_cast<std::int64_t>(16) * ws.n_out_pad * kWarp), kBlock, 0, s>>>(
             ws.partials.get(), blocks, k, ws.n_out, ws.n_out_pad, ws.c16.get());
