@@ -617,7 +617,7 @@ def main() -> None:
     ap.add_argument("--precision", choices=["split", "mixed", "plain"], default="split")
     ap.add_argument("--recovery", choices=["harmonic", "spr_tissue", "spr_global", "raw"], default="harmonic")
     ap.add_argument("--warm-start", choices=["on", "off"], default="on")
-    ap.add_argument("--train", type=int, default=4096, help="training solves of the warm-start network")
+    ap.add_argument("--train", type=int, default=8192, help="training solves of the warm-start network")
     ap.add_argument("--rank", type=int, default=256, help="reduced-basis size the network predicts")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
