@@ -108,6 +108,8 @@ class Subject:
         self._precision = precision
         self._device = int(device)
         self._lock = threading.RLock()
+        self._block_k_default = MAX_BLOCK  # block width of block_k=None sweeps (autotune may lower it)
+        self._overlap = 2                  # dA/dt blocks per SM beside a running solve
 
     @classmethod
     def from_mesh(cls, mesh_file: str | Path, **kwargs) -> Subject:
@@ -141,7 +143,38 @@ class Subject:
                 p.device = self._device
                 m = self._mesh
                 self._ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris, p)
+                self._ctx.set_overlap(self._overlap)
             return self._ctx
+
+    @property
+    def block_k_default(self) -> int:
+        """Placements per block of a sweep called with ``block_k=None``."""
+        return self._block_k_default
+
+    @property
+    def overlap_blocks_per_sm(self) -> int:
+        return self._overlap
+
+    def set_sweep_defaults(self, *, block_k: int | None = None, overlap_blocks_per_sm: int | None = None) -> None:
+        """Settings that change no result bit: the block width of ``block_k=None`` sweeps (1 to
+        MAX_BLOCK) and the dA/dt blocks per SM that run beside a solve (1 to 16)."""
+        with self._lock:
+            if block_k is not None:
+                if not 1 <= int(block_k) <= MAX_BLOCK:
+                    raise ValueError(f"block_k must be in [1, {MAX_BLOCK}]")
+                self._block_k_default = int(block_k)
+            if overlap_blocks_per_sm is not None:
+                if not 1 <= int(overlap_blocks_per_sm) <= 16:
+                    raise ValueError("overlap_blocks_per_sm must be in [1, 16]")
+                self._overlap = int(overlap_blocks_per_sm)
+                if self._ctx is not None:
+                    self._ctx.set_overlap(self._overlap)
+
+    def autotune(self, coil: Coil, placements: Sequence[Placement], **kwargs):
+        """Choose the sweep defaults by timing them on these placements (cunibs_b200.tune.autotune)."""
+        from .tune import autotune
+
+        return autotune(self, coil, placements, **kwargs)
 
     @property
     def mesh(self) -> HeadMesh:
@@ -187,7 +220,7 @@ class Subject:
     def _iter_reduced(self, coil: Coil, sites: Sequence[Placement], didt: float, block_k: int | None,
                       retain: _Retain, recovery: str) -> Iterator[FieldResult]:
         ctx = self.context
-        chunk_k = MAX_BLOCK if block_k is None else max(1, min(MAX_BLOCK, int(block_k)))
+        chunk_k = self._block_k_default if block_k is None else max(1, min(MAX_BLOCK, int(block_k)))
         slot_node, slot_tag = self._host_slot_maps(recovery) if retain.nodal else (None, None)
         # Per-node slots need the connectivity to say which nodes a region touches.
         tet_nodes = self._host_tet_nodes() if retain.nodal and slot_tag is None else None
