@@ -196,15 +196,25 @@ __global__ void p1_gradients_kernel(const double* __restrict__ nodes, const int*
 }
 
 // Tissue conductivity table (fem/assembly.py:15-26); NaN marks an unknown tag.
-__constant__ double c_sigma[11];
+// A conductivity table (index = tissue tag) passed by value: contexts driven from several host
+// threads each launch with their own.
+struct SigmaTable {
+    double s[11];
+};
 
-__global__ void conductivity_kernel(const int* __restrict__ tags, int m, double* __restrict__ cond,
+SigmaTable sigma_table(const double* sigma_by_tag) {
+    SigmaTable t;
+    for (int i = 0; i < 11; ++i) t.s[i] = sigma_by_tag[i];
+    return t;
+}
+
+__global__ void conductivity_kernel(const int* __restrict__ tags, int m, SigmaTable table, double* __restrict__ cond,
                                     int* __restrict__ bad) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     int invalid = 0;
     if (e < m) {
         const int t = tags[e];
-        const double s = (t >= 0 && t <= 10) ? c_sigma[t] : NAN;
+        const double s = (t >= 0 && t <= 10) ? table.s[t] : NAN;
         cond[e] = s;
         invalid = isnan(s);
     }
@@ -537,10 +547,10 @@ void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, c
                           " zero or non-finite volume");
     }
     const double sigma[11] = {NAN, 0.126, 0.275, 1.654, 0.010, 0.465, 0.5, 0.008, 0.025, 0.6, 0.16};
-    CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma, sizeof(sigma), 0, cudaMemcpyHostToDevice, s));
     m.cond.resize(M);
     bad.zero(s);
-    conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), n_tets, m.cond.get(), bad.get()); count_launch();
+    conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), n_tets, sigma_table(sigma), m.cond.get(), bad.get());
+    count_launch();
     if (read_int(bad.get(), s)) fail(kEInval, "tetrahedra with unknown tissue tags");
 
     m.g32.resize(12 * M);
@@ -617,10 +627,10 @@ void build_mesh(Mesh& m, const double* nodes_mm, int n_nodes, const int* tets, c
 }
 
 void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t s, bool validate) {
-    CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, sigma_by_tag, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
     m.cond_bad.resize(1);
     if (validate) m.cond_bad.zero(s);
-    conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, m.cond.get(), m.cond_bad.get());
+    conductivity_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.tags.get(), m.n_tets, sigma_table(sigma_by_tag),
+                                                              m.cond.get(), m.cond_bad.get());
     count_launch();
     if (validate && read_int(m.cond_bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
     // The right-hand side weighs each element by the same conductivity.
@@ -653,9 +663,10 @@ void assemble_reduced_values(const Mesh& m, const double* tables, int n_tables, 
     DevArray<double> cond(M), full(m.k_nnz);
     DevArray<int> bad(1);
     for (int t = 0; t < n_tables; ++t) {
-        CUNIBS_CHECK(cudaMemcpyToSymbolAsync(c_sigma, tables + 11 * t, 11 * sizeof(double), 0, cudaMemcpyHostToDevice, s));
         bad.zero(s);
-        conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), M, cond.get(), bad.get()); count_launch();
+        conductivity_kernel<<<grid_for(M), kBlock, 0, s>>>(m.tags.get(), M, sigma_table(tables + 11 * t), cond.get(),
+                                                           bad.get());
+        count_launch();
         if (read_int(bad.get(), s)) fail(kEInval, "conductivity table leaves a tag undefined");
         assemble_entries_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(m.g.get(), m.vols.get(), cond.get(),
                                                                      m.contrib_ptr.get(), m.contrib_idx.get(), m.k_nnz,
