@@ -355,6 +355,7 @@ def run_ours(args) -> dict:
 
     draws = conductivity_draws(ctx, coil, centers[:4], handles[:4], dists[:4], args.recovery, stream)
     adm_line = adm_measure(ctx, coil, sites, stream)
+    multi = multi_subject_measure(coil, args.recovery) if world == 1 else None
 
     # Roofline of the SpMV-dominated iteration (solve stage).
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -427,6 +428,7 @@ def run_ours(args) -> dict:
         "setup_s": round(setup_s, 3),
         "conductivity_draws": draws,
         "adm": adm_line,
+        "multi_subject": multi,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -551,6 +553,42 @@ def adm_measure(ctx, coil, sites, stream) -> dict:
            "optimize_ms": round(opt_ms, 3), "best_objective_v_per_m": round(res.best_objective, 4),
            "sweep_max_v_per_m": round(float(np.linalg.norm(e, axis=1).max()), 4)}
     adjoint.handle.close()
+    return out
+
+
+def multi_subject_measure(coil, recovery, n_place=16) -> dict:
+    """Three subjects of uneven size (0.3M, 0.6M and 1.0M tetrahedra, the same 10-tissue sphere at
+    3.93, 3.12 and 2.63 mm) swept with 16 placements each: one after another, then side by side from
+    one host thread per subject (cunibs_b200.batch). Wall clock around each whole run (results
+    copied to the host); the per-subject results of the two runs are checked bitwise equal."""
+    from cunibs_b200 import Placement, Subject
+    from cunibs_b200.batch import SubjectJob, simulate_subjects
+
+    rng = np.random.default_rng(7)
+    sites = []
+    for _ in range(n_place):
+        th, ph = rng.uniform(0.0, np.radians(40.0)), rng.uniform(0.0, 2 * np.pi)
+        c = 90.0 * np.array([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+        sites.append(Placement(c, c + 50.0 * np.array([-np.sin(ph), np.cos(ph), 0.0])))
+    subjects = [Subject(sphere_head(h, 90.0, EIGHT_SHELLS, (EYE_CAP, MUSCLE_CAP), jitter_mm=0.2, seed=0), tolerance=TOL)
+                for h in (3.93, 3.12, 2.63)]
+    jobs = [SubjectJob(s, coil, sites, options=dict(recovery=recovery, magnitude=True)) for s in subjects]
+    for j in jobs:  # contexts, recovery operators and loop graphs built outside the timing
+        list(j.subject.iter_simulate(coil, sites[:8], recovery=recovery))
+    t0 = time.perf_counter()
+    alone = [list(j.subject.iter_simulate(coil, sites, recovery=recovery, magnitude=True)) for j in jobs]
+    seq_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    together = simulate_subjects(jobs)
+    con_s = time.perf_counter() - t0
+    same = all(np.array_equal(a.magnE, b.magnE) for ra, rb in zip(alone, together) for a, b in zip(ra, rb))
+    out = {"what": "3 subjects (0.3M / 0.6M / 1.0M tets) x 16 placements, harmonic recovery, |E| retained",
+           "n_tets": [int(s.context.n_tets) for s in subjects], "sequential_s": round(seq_s, 4),
+           "concurrent_s": round(con_s, 4), "placements_per_s_sequential": round(3 * n_place / seq_s, 1),
+           "placements_per_s_concurrent": round(3 * n_place / con_s, 1), "speedup": round(seq_s / con_s, 3),
+           "bitwise_equal": bool(same)}
+    for s in subjects:
+        s.free()
     return out
 
 
