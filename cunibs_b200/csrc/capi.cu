@@ -96,6 +96,7 @@ struct SigmaStudy {
     int tags[kSigmaMaxTags] = {};
     long nnz = 0;
     DevArray<double> comp;   // (1 + P, nnz): the other tissues at nominal, then each tissue at unit sigma
+    DevArray<double> rhs;    // (1 + P, n_red, K): the block's right-hand sides split the same way
     DevArray<double> x_nom;  // (n_red, K) nominal potential
     DevArray<double> S;      // (n_red, P, K) sensitivities
     std::vector<double> Z;   // (K, P, P): y_j = Z_j (sigma - sigma_nom)
@@ -829,6 +830,21 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         st->opts = pb.opts;
         const int K = st->K, n_red = m.n_nodes - 1;
         const std::size_t npk = static_cast<std::size_t>(n_red) * P * K;
+        // The right-hand side is linear in sigma like the operator (run.py:59-84): one block of
+        // right-hand sides per component table, so a draw's is one combination.
+        {
+            const BlockSlot& sl0 = c->slots[st->slot];
+            DevArray<double> td;
+            td.upload(tables.data(), tables.size(), s);
+            DevArray<float> wts(static_cast<std::size_t>(1 + P) * m.n_tets);
+            sigma_element_weights(m, td.get(), 1 + P, wts.get(), s);
+            const std::size_t nk = static_cast<std::size_t>(n_red) * K;
+            st->rhs.resize((1 + P) * nk);
+            for (int t = 0; t <= P; ++t)
+                rhs_block(m, sl0.dadt_elm.get(), st->k, K, st->rhs.get() + t * nk, s,
+                          wts.get() + static_cast<std::size_t>(t) * m.n_tets);
+            CUNIBS_CHECK(cudaStreamSynchronize(s));  // td and wts leave scope
+        }
         st->x_nom.resize(static_cast<std::size_t>(n_red) * K);
         CUNIBS_CHECK(cudaMemcpyAsync(st->x_nom.get(), c->X.get(), sizeof(double) * n_red * K, cudaMemcpyDeviceToDevice, s));
         // Sensitivity right-hand sides c_t = b_t - A_t x_nom, and which are nonzero (a tissue with no
@@ -920,7 +936,7 @@ int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* 
         refresh_finest_derived(c->hier, s);
         set_element_conductivity(m, table, s, false);  // the nominal table passed the check at begin
         BlockSlot& sl = c->slots[st.slot];
-        rhs_block(m, sl.dadt_elm.get(), k, K, sl.B.get(), s);
+        sigma_combine(st.rhs.get(), P, static_cast<long>(n_red) * K, w, sl.B.get(), s);
         sl.X0.reserve(static_cast<std::size_t>(n_red) * K);
         sigma_guess(st.x_nom.get(), st.S.get(), n_red, P, K, k, y, sl.X0.get(), s);
         auto queue = [&] {

@@ -241,11 +241,12 @@ void dadt_elements(const Mesh& m, const float* nodal, int k, float* elm, cudaStr
     CUNIBS_LAUNCH_CHECK("dadt element average");
 }
 
-void rhs_block(const Mesh& m, const float* elm, int k, int K, double* b_red, cudaStream_t s) {
+void rhs_block(const Mesh& m, const float* elm, int k, int K, double* b_red, cudaStream_t s, const float* neg_vc) {
     const unsigned g = (m.n_nodes - 1 + 63) / 64;
+    const float* w = neg_vc ? neg_vc : m.neg_vc32.get();
     auto go = [&](auto kc) {
         constexpr int KK = decltype(kc)::value;
-        rhs_kernel<KK><<<g, 64 * KK, 0, s>>>(elm, m.g32.get(), m.neg_vc32.get(), m.n2c_ptr.get(), m.n2c_idx.get(),
+        rhs_kernel<KK><<<g, 64 * KK, 0, s>>>(elm, m.g32.get(), w, m.n2c_ptr.get(), m.n2c_idx.get(),
                                              m.n_nodes, m.n_tets, k, m.ground, b_red); count_launch();
     };
     switch (K) {

@@ -200,8 +200,9 @@ void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed
 
 // Records the calling thread's message for cunibs_last_error.
 void set_last_error(const std::string& message);
+// neg_vc: the per-element weights -(vol * sigma) in FP32 (null: the mesh's own).
 void rhs_block(const Mesh& m, const float* dadt_elm, int k, int k_pad, double* b_red /* (N-1, k_pad) */,
-               cudaStream_t s);
+               cudaStream_t s, const float* neg_vc = nullptr);
 
 // Post-processing (post.cu).
 void reconstruct_block(const Mesh& m, const double* x_red /* (N-1,k_pad) */, int k, int k_pad,
@@ -318,6 +319,10 @@ struct SigmaDraw {
 };
 // Values of the finest operator for one draw: comp[0] + sum_t w_t comp[1 + t] (comp (1 + n_tags, nnz)).
 void sigma_combine(const double* comp, int n_tags, long nnz, const SigmaWeights& w, double* out, cudaStream_t s);
+// -vol of the elements of each table entry's tissue, zero elsewhere: out (n_tables, n_tets) FP32,
+// tables (n_tables, 11) of per-tag weights (the right-hand side's per-element weights of a
+// conductivity table whose entries are those weights).
+void sigma_element_weights(const Mesh& m, const double* tables_dev, int n_tables, float* out, cudaStream_t s);
 // Sensitivity right-hand sides c_t of the nominal potential x_red (n_red, K): c_out (n_red, P, K).
 void sigma_sens_rhs(const Mesh& m, const double* x_red, const float* dadt_elm, int k, int K, const SigmaSlots& slots,
                     int P, double* c_out, cudaStream_t s);

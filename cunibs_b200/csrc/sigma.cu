@@ -31,6 +31,18 @@ __global__ void combine_values_kernel(const double* __restrict__ comp, int n_tag
     out[p] = v;
 }
 
+// out[t][e] = -(vol_e * tables[t][tag_e]) in FP32, the right-hand side's element weights of table t
+// (the same rounding as the mesh's own weights of a full conductivity table).
+__global__ void element_weights_kernel(const float* __restrict__ vols32, const int* __restrict__ tags, int m,
+                                       const double* __restrict__ tables, int n_tables, float* __restrict__ out) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<long>(m) * n_tables) return;
+    const int t = static_cast<int>(q / m), e = static_cast<int>(q % m);
+    const int tag = tags[e];
+    const double w = (tag >= 0 && tag <= 10) ? tables[11 * t + tag] : 0.0;
+    out[q] = -(vols32[e] * static_cast<float>(w));
+}
+
 // c_out[r][a][j] = sum over the corners of node i whose element has tag tags_of_slot[a] of
 // vol_e (g_corner . E_e), E_e from the grounded potential x_red (n_red, K) and the element dA/dt of
 // placement j, accumulated in FP64 in node-to-corner order. Columns past k repeat column k-1.
@@ -215,6 +227,13 @@ __global__ void diff_norms_kernel(const double* __restrict__ a, const double* __
 void sigma_combine(const double* comp, int n_tags, long nnz, const SigmaWeights& w, double* out, cudaStream_t s) {
     combine_values_kernel<<<grid_for(nnz), kBlock, 0, s>>>(comp, n_tags, nnz, w, out); count_launch();
     CUNIBS_LAUNCH_CHECK("sigma combine");
+}
+
+void sigma_element_weights(const Mesh& m, const double* tables_dev, int n_tables, float* out, cudaStream_t s) {
+    const long total = static_cast<long>(m.n_tets) * n_tables;
+    element_weights_kernel<<<grid_for(total), kBlock, 0, s>>>(m.vols32.get(), m.tags.get(), m.n_tets, tables_dev,
+                                                             n_tables, out); count_launch();
+    CUNIBS_LAUNCH_CHECK("sigma element weights");
 }
 
 void sigma_sens_rhs(const Mesh& m, const double* x_red, const float* dadt_elm, int k, int K, const SigmaSlots& slots,
