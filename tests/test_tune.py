@@ -35,3 +35,11 @@ def test_autotune_rejects_bad_candidates_before_any_work(subject, kw, match):
 def test_autotune_needs_placements(subject):
     with pytest.raises(ValueError, match="at least one placement"):
         autotune(subject, figure8_coil(16), [])
+
+
+def test_simulate_subjects_rejects_a_shared_subject(subject):
+    from cunibs_b200.batch import SubjectJob, simulate_subjects
+
+    job = SubjectJob(subject, figure8_coil(16), [])
+    with pytest.raises(ValueError, match="its own subject"):
+        simulate_subjects([job, job])
