@@ -65,10 +65,10 @@ class Coil:
 
     @classmethod
     def load(cls, source: str | Path) -> Coil:
-        """Load a coil file: ``.ccd`` text, or ``.npz`` with ``positions_m``/``moments`` arrays.
-
-        The reference's bundled ``.h5`` coils need h5py, which this environment does not ship.
-        """
+        """Load a coil file (reference coil.py:67-82): the ``.h5`` files of the reference's coil
+        library (a ``dipoles`` (n, 6) dataset with the ``.ccd`` header as attributes), ``.ccd``
+        text, or ``.npz`` with ``positions_m``/``moments`` arrays. ``.h5`` files are read with h5py
+        where it is installed, else with this package's own reader (``cunibs_b200.h5lite``)."""
         p = Path(source)
         if p.suffix == ".ccd":
             return cls.from_ccd(p)
@@ -76,16 +76,28 @@ class Coil:
             with np.load(p) as z:
                 return cls(z["positions_m"], z["moments"], name=str(z.get("name", p.stem)))
         try:
-            import h5py  # noqa: F401
-        except ImportError as exc:  # pragma: no cover - depends on the environment
-            raise ImportError(f"reading {p.name} needs h5py, which is not installed") from exc
-        import h5py
+            import h5py
+        except ImportError:
+            from .h5lite import read_dataset
 
-        with h5py.File(p, "r") as h5f:
-            data = np.asarray(h5f["dipoles"], dtype=np.float64)
-            attrs = dict(h5f["dipoles"].attrs)
+            data, attrs = read_dataset(p, "dipoles")
+        else:
+            with h5py.File(p, "r") as h5f:
+                data = np.asarray(h5f["dipoles"], dtype=np.float64)
+                attrs = {k: _decode_attr(v) for k, v in h5f["dipoles"].attrs.items()}
+        data = np.asarray(data, dtype=np.float64)
         didt = attrs.get("dIdtmax")
         return cls(
             data[:, 0:3], data[:, 3:6], name=str(attrs.get("coilname", p.stem)),
             didt_max=None if didt is None else float(didt) * _CCD_DIDTMAX_TO_A_PER_S,
+            metadata=attrs,
         )
+
+
+def _decode_attr(v):
+    """An h5py attribute value as str, int or float."""
+    if isinstance(v, bytes):
+        return v.decode()
+    if isinstance(v, np.generic):
+        return v.item()
+    return v

@@ -1,0 +1,273 @@
+"""A small read-only HDF5 reader for the files the reference's coil library holds (h5py-written,
+default "earliest" format), so that its bundled ``.h5`` coils load where h5py is not installed.
+
+Written from the HDF5 File Format Specification (version 0 superblock), covering what such files
+use: a version-0 superblock with 8-byte offsets and lengths; groups as symbol tables (version-1
+B-tree of group nodes, symbol-table nodes, local heap); version-1 object headers with continuation
+blocks; the dataspace, datatype, data layout (version 3: compact, contiguous, chunked), filter
+pipeline (deflate, shuffle) and attribute messages; raw-data-chunk B-trees; numeric data
+(little- or big-endian integers and IEEE floats) and fixed- or variable-length strings (the latter
+through global-heap collections). Anything else raises ``ValueError`` naming what is missing.
+"""
+
+from __future__ import annotations
+
+import struct
+import zlib
+from pathlib import Path
+
+import numpy as np
+
+_SIGNATURE = b"\x89HDF\r\n\x1a\n"
+_UNDEF = 0xFFFFFFFFFFFFFFFF
+
+
+class _File:
+    def __init__(self, data: bytes) -> None:
+        self.d = data
+
+    def u(self, fmt: str, off: int):
+        return struct.unpack_from("<" + fmt, self.d, off)
+
+    def sig(self, off: int, s: bytes) -> None:
+        if self.d[off:off + len(s)] != s:
+            raise ValueError(f"HDF5: expected {s!r} at offset {off}")
+
+    # --- groups -----------------------------------------------------------------------------
+
+    def local_heap_name(self, heap: int, offset: int) -> str:
+        self.sig(heap, b"HEAP")
+        data_addr = self.u("Q", heap + 24)[0]
+        start = data_addr + offset
+        end = self.d.index(b"\x00", start)
+        return self.d[start:end].decode()
+
+    def group_entries(self, btree: int, heap: int) -> dict[str, int]:
+        """name -> object header address over a version-1 B-tree of group nodes."""
+        out: dict[str, int] = {}
+        self.sig(btree, b"TREE")
+        node_type, level, used = self.d[btree + 4], self.d[btree + 5], self.u("H", btree + 6)[0]
+        if node_type != 0:
+            raise ValueError("HDF5: a group B-tree must hold group nodes")
+        q = btree + 24 + 8  # past the header and key 0
+        for _ in range(used):
+            child = self.u("Q", q)[0]
+            q += 16  # child address, then the next key
+            if level > 0:
+                out.update(self.group_entries(child, heap))
+                continue
+            self.sig(child, b"SNOD")
+            n_sym = self.u("H", child + 6)[0]
+            for i in range(n_sym):
+                e = child + 8 + 40 * i
+                name_off, header = self.u("QQ", e)
+                out[self.local_heap_name(heap, name_off)] = header
+        return out
+
+    # --- object headers ---------------------------------------------------------------------
+
+    def messages(self, header: int) -> list[tuple[int, int, int]]:
+        """(type, offset of its data, size) of every message of a version-1 object header."""
+        if self.d[header] != 1:
+            raise ValueError("HDF5: only version-1 object headers are handled")
+        n_msg, _refs, size = self.u("HII", header + 2)
+        blocks = [(header + 16, size)]
+        out = []
+        while blocks and len(out) < n_msg:
+            start, length = blocks.pop(0)
+            q = start
+            while q + 8 <= start + length and len(out) < n_msg:
+                mtype, msize = self.u("HH", q)
+                if mtype == 0x10:  # continuation: another block of messages
+                    blocks.append(self.u("QQ", q + 8))
+                out.append((mtype, q + 8, msize))
+                q += 8 + msize
+        return out
+
+    def dataspace(self, off: int) -> tuple[int, ...]:
+        version, ndim, flags = self.d[off], self.d[off + 1], self.d[off + 2]
+        if version == 1:
+            dims_at = off + 8
+        elif version == 2:
+            dims_at = off + 4
+            if self.d[off + 3] == 0:  # scalar
+                return ()
+        else:
+            raise ValueError(f"HDF5: dataspace message version {version}")
+        return tuple(self.u(f"{ndim}Q", dims_at)) if ndim else ()
+
+    def datatype(self, off: int) -> dict:
+        cv = self.d[off]
+        cls = cv & 0x0F
+        bits = self.d[off + 1] | (self.d[off + 2] << 8) | (self.d[off + 3] << 16)
+        size = self.u("I", off + 4)[0]
+        order = ">" if bits & 1 else "<"
+        if cls == 0:
+            return {"kind": "num", "dtype": np.dtype(f"{order}{'i' if bits & 8 else 'u'}{size}"), "size": size}
+        if cls == 1:
+            return {"kind": "num", "dtype": np.dtype(f"{order}f{size}"), "size": size}
+        if cls == 3:
+            return {"kind": "fstr", "size": size}
+        if cls == 9:
+            if bits & 0x0F != 1:
+                raise ValueError("HDF5: variable-length sequences other than strings")
+            return {"kind": "vstr", "size": size}
+        raise ValueError(f"HDF5: datatype class {cls}")
+
+    def global_heap_object(self, collection: int, index: int) -> bytes:
+        self.sig(collection, b"GCOL")
+        total = self.u("Q", collection + 8)[0]
+        q, end = collection + 16, collection + total
+        while q + 16 <= end:
+            idx, _refs, _res, osize = self.u("HHIQ", q)
+            if idx == 0:
+                break
+            if idx == index:
+                return self.d[q + 16:q + 16 + osize]
+            q += 16 + ((osize + 7) // 8) * 8
+        raise ValueError("HDF5: global heap object not found")
+
+    def values(self, dtype: dict, shape: tuple[int, ...], off: int):
+        n = int(np.prod(shape)) if shape else 1
+        if dtype["kind"] == "num":
+            a = np.frombuffer(self.d, dtype=dtype["dtype"], count=n, offset=off)
+            a = a.astype(dtype["dtype"].newbyteorder("="))
+            return a.reshape(shape) if shape else a[0].item()
+        if dtype["kind"] == "fstr":
+            s = [self.d[off + i * dtype["size"]:off + (i + 1) * dtype["size"]].split(b"\x00")[0].decode()
+                 for i in range(n)]
+        else:
+            s = []
+            for i in range(n):
+                _length, coll, index = self.u("IQI", off + 16 * i)
+                s.append(self.global_heap_object(coll, index).decode())
+        return s if shape else s[0]
+
+    def attribute(self, off: int) -> tuple[str, object]:
+        version = self.d[off]
+        name_size, type_size, space_size = self.u("HHH", off + 2)
+        if version == 1:
+            pad = lambda x: (x + 7) // 8 * 8  # noqa: E731
+            q = off + 8
+        elif version in (2, 3):
+            pad = lambda x: x  # noqa: E731
+            q = off + 8 + (1 if version == 3 else 0)
+        else:
+            raise ValueError(f"HDF5: attribute message version {version}")
+        name = self.d[q:q + name_size].split(b"\x00")[0].decode()
+        q += pad(name_size)
+        dtype = self.datatype(q)
+        q += pad(type_size)
+        shape = self.dataspace(q)
+        q += pad(space_size)
+        return name, self.values(dtype, shape, q)
+
+    def chunk_index(self, btree: int, ndim: int) -> list[tuple[tuple[int, ...], int, int, int]]:
+        """(offset, filter mask, size, address) of every chunk of a raw-data-chunk B-tree."""
+        self.sig(btree, b"TREE")
+        node_type, level, used = self.d[btree + 4], self.d[btree + 5], self.u("H", btree + 6)[0]
+        if node_type != 1:
+            raise ValueError("HDF5: a chunk B-tree must hold raw-data chunks")
+        key = 8 + 8 * (ndim + 1)
+        out = []
+        q = btree + 24
+        for _ in range(used):
+            size, mask = self.u("II", q)
+            offs = self.u(f"{ndim}Q", q + 8)
+            child = self.u("Q", q + key)[0]
+            if level > 0:
+                out += self.chunk_index(child, ndim)
+            else:
+                out.append((offs, mask, size, child))
+            q += key + 8
+        return out
+
+    def dataset(self, header: int) -> tuple[np.ndarray, dict]:
+        shape = dtype = layout = None
+        filters: list[int] = []
+        attrs: dict = {}
+        for mtype, off, _size in self.messages(header):
+            if mtype == 0x01:
+                shape = self.dataspace(off)
+            elif mtype == 0x03:
+                dtype = self.datatype(off)
+            elif mtype == 0x08:
+                layout = off
+            elif mtype == 0x0B:
+                filters = self.filter_ids(off)
+            elif mtype == 0x0C:
+                k, v = self.attribute(off)
+                attrs[k] = v
+        if shape is None or dtype is None or layout is None or dtype["kind"] != "num":
+            raise ValueError("HDF5: not a numeric dataset")
+        return self.read_layout(layout, shape, dtype["dtype"], filters), attrs
+
+    def filter_ids(self, off: int) -> list[int]:
+        version, n = self.d[off], self.d[off + 1]
+        q = off + (8 if version == 1 else 2)
+        ids = []
+        for _ in range(n):
+            fid = self.u("H", q)[0]
+            if version == 1 or fid >= 256:
+                name_len, _flags, n_val = self.u("HHH", q + 2)
+                q += 8 + ((name_len + 7) // 8 * 8 if version == 1 else name_len)
+            else:
+                _flags, n_val = self.u("HH", q + 2)
+                q += 6
+            q += 4 * n_val + (4 if version == 1 and n_val % 2 else 0)
+            ids.append(fid)
+        return ids
+
+    def read_layout(self, off: int, shape: tuple[int, ...], dt: np.dtype, filters: list[int]) -> np.ndarray:
+        version, cls = self.d[off], self.d[off + 1]
+        if version != 3:
+            raise ValueError(f"HDF5: data layout message version {version}")
+        n = int(np.prod(shape))
+        if cls == 0:  # compact
+            size = self.u("H", off + 2)[0]
+            raw = self.d[off + 4:off + 4 + size]
+            return np.frombuffer(raw, dtype=dt, count=n).astype(dt.newbyteorder("=")).reshape(shape)
+        if cls == 1:  # contiguous
+            addr = self.u("Q", off + 2)[0]
+            return np.frombuffer(self.d, dtype=dt, count=n, offset=addr).astype(dt.newbyteorder("=")).reshape(shape)
+        if cls != 2:
+            raise ValueError(f"HDF5: layout class {cls}")
+        ndim = self.d[off + 2] - 1  # the last chunk dimension is the element size
+        btree = self.u("Q", off + 3)[0]
+        cdims = self.u(f"{ndim}I", off + 11)
+        out = np.zeros(shape, dtype=dt.newbyteorder("="))
+        if btree == _UNDEF:
+            return out
+        for offs, mask, size, addr in self.chunk_index(btree, ndim):
+            raw = self.d[addr:addr + size]
+            for i, fid in reversed(list(enumerate(filters))):
+                if mask & (1 << i):
+                    continue
+                if fid == 1:
+                    raw = zlib.decompress(raw)
+                elif fid == 2:  # shuffle: bytes grouped by position within the element
+                    raw = np.frombuffer(raw, np.uint8).reshape(dt.itemsize, -1).T.tobytes()
+                else:
+                    raise ValueError(f"HDF5: filter {fid}")
+            chunk = np.frombuffer(raw, dtype=dt).astype(dt.newbyteorder("=")).reshape(cdims)
+            sl = tuple(slice(o, min(o + c, s)) for o, c, s in zip(offs, cdims, shape))
+            out[sl] = chunk[tuple(slice(0, x.stop - x.start) for x in sl)]
+        return out
+
+
+def read_dataset(path: str | Path, name: str) -> tuple[np.ndarray, dict]:
+    """The dataset ``name`` of the root group of an HDF5 file and its attributes."""
+    f = _File(Path(path).read_bytes())
+    f.sig(0, _SIGNATURE)
+    if f.d[8] != 0:
+        raise ValueError(f"HDF5: superblock version {f.d[8]} (only version 0 is handled)")
+    if f.d[13] != 8 or f.d[14] != 8:
+        raise ValueError("HDF5: only 8-byte offsets and lengths are handled")
+    root_cache = f.u("I", 56 + 16)[0]
+    if root_cache != 1:
+        raise ValueError("HDF5: the root group has no cached symbol table")
+    btree, heap = f.u("QQ", 56 + 24)
+    entries = f.group_entries(btree, heap)
+    if name not in entries:
+        raise KeyError(f"{path}: no dataset {name!r} in the root group (has {sorted(entries)})")
+    return f.dataset(entries[name])
