@@ -226,7 +226,8 @@ def run_ours(args) -> dict:
         from cunibs_b200.warmstart import train_warm_start
 
         with torch.cuda.device(local):
-            model = train_warm_start(ctx, coil, n_train=args.train, rank=args.rank, seed=1)
+            model = train_warm_start(ctx, coil, n_train=args.train, rank=args.rank, hidden=args.hidden,
+                                     epochs=args.epochs, seed=1)
         warm_stats = {k: v for k, v in model.stats.items() if k != "loss_curve"}
     d_used = torch.zeros(K_BLOCK, dtype=torch.int32, device=dev)
     d_rel0 = torch.zeros(K_BLOCK, dtype=torch.float64, device=dev)
@@ -391,7 +392,8 @@ def run_ours(args) -> dict:
                  + ("; bf16 tensor-core warm start" if args.warm_start == "on" else ""),
         "data": "synthetic: seeded sphere head and figure-8 coil",
         "config": config_dict(mesh, {"precision": args.precision, "recovery": args.recovery,
-                                     "warm_start": (f"MLP 6-4x512-{args.rank}, {args.train} plain-method training solves"
+                                     "warm_start": (f"MLP 6-4x{args.hidden}-{args.rank}, {args.train} plain-method training solves, "
+                                                    f"{args.epochs} epochs"
                                                     if args.warm_start == "on" else "off"),
                                      "l2": "flushed (256 MB write) before every step's solve",
                                      "pipeline": "blocks submitted two deep: placement/dA-dt/RHS of step i+1 "
@@ -657,6 +659,8 @@ def main() -> None:
     ap.add_argument("--warm-start", choices=["on", "off"], default="on")
     ap.add_argument("--train", type=int, default=8192, help="training solves of the warm-start network")
     ap.add_argument("--rank", type=int, default=256, help="reduced-basis size the network predicts")
+    ap.add_argument("--hidden", type=int, default=512, help="width of the warm-start network's hidden layers")
+    ap.add_argument("--epochs", type=int, default=400, help="training epochs of the warm-start network")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     line = run_reference(args) if args.impl == "reference" else run_ours(args)
