@@ -115,6 +115,16 @@ __device__ __forceinline__ T row_dot(const int* __restrict__ ptr, const int* __r
     return strided_dot<T, 1>(col, val, x, ptr[row], ptr[row + 1], K, c, T(0));
 }
 
+// Programmatic dependent launch (sm_90 and later): a kernel of the solve loop launched with the
+// programmatic-serialization attribute may be scheduled while its predecessor in the stream drains.
+// It waits here, before touching any memory, for that predecessor to complete and its writes to be
+// visible, and at once lets its own successor be scheduled, so block dispatch and launch latency
+// overlap the previous kernel's tail. Launched without the attribute, both are no-ops.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // --- V-cycle kernels ---------------------------------------------------------------------
 //
 // A row group is TPR x K threads: K lanes per column-slot (lane = column, so a nonzero's K values
@@ -201,6 +211,7 @@ struct ReduceTile {
 template <typename T, int K>
 __global__ void __launch_bounds__(tile_threads<K>()) jz_kernel(int n, const T* __restrict__ dinv, const T* __restrict__ b,
                                                                T alpha0, T* __restrict__ x) {
+    pdl_enter();
     const int row = blockIdx.x * kTileRows + threadIdx.x / K;
     const int c = threadIdx.x % K;
     if (row < n) x[static_cast<long>(row) * K + c] = alpha0 * dinv[row] * b[static_cast<long>(row) * K + c];
@@ -213,6 +224,7 @@ __global__ void __launch_bounds__(Group<K, TPR>::kBlock) cheby_kernel(
     int n, const int* __restrict__ ptr, const int* __restrict__ col, const T* __restrict__ val,
     const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ x_cur, const T* x_prev, T c_cur,
     T c_prev, T alpha, T* out) {
+    pdl_enter();
     const RowSlot<T, K, TPR> s;
     const bool valid = s.row < n;
     const T ax = group_row_dot<T, K, TPR>(ptr, col, val, x_cur, s, valid);
@@ -230,6 +242,7 @@ __global__ void __launch_bounds__(Group<K, TPR>::kBlock) residual_kernel(int n, 
                                                                          const T* __restrict__ val,
                                                                          const T* __restrict__ x,
                                                                          const T* __restrict__ b, T* __restrict__ r) {
+    pdl_enter();
     const RowSlot<T, K, TPR> s;
     const bool valid = s.row < n;
     const T ax = group_row_dot<T, K, TPR>(ptr, col, val, x, s, valid);
@@ -246,6 +259,7 @@ __global__ void __launch_bounds__(Group<K, TPR>::kBlock) restrict_kernel(int nc,
                                                                          const T* __restrict__ rf, T* __restrict__ bc,
                                                                          const T* __restrict__ dinv_c, T alpha0,
                                                                          T* __restrict__ xc) {
+    pdl_enter();
     const RowSlot<T, K, TPR> s;
     const bool valid = s.row < nc;
     const T v = group_row_dot<T, K, TPR>(ptr, col, val, rf, s, valid);
@@ -260,6 +274,7 @@ __global__ void __launch_bounds__(Group<K, TPR>::kBlock) prolong_kernel(int n, c
                                                                         const int* __restrict__ col,
                                                                         const T* __restrict__ val,
                                                                         const T* __restrict__ xc, T* __restrict__ xf) {
+    pdl_enter();
     const RowSlot<T, K, TPR> s;
     const bool valid = s.row < n;
     const T v = group_row_dot<T, K, TPR>(ptr, col, val, xc, s, valid);
@@ -280,6 +295,27 @@ void dispatch_tpr(int tpr, F&& f) {
     }
 }
 
+// A solve-loop kernel launch, with programmatic stream serialization when `dep` is set (the
+// kernel then starts with pdl_enter()); a plain launch otherwise.
+template <typename... KArgs, typename... Args>
+void launch_loop(bool dep, void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+    if (!dep) {
+        kernel<<<grid, block, 0, s>>>(args...);
+        return;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUNIBS_CHECK(cudaLaunchKernelEx(&cfg, kernel, args...));
+}
+
 template <int K, int TPR>
 unsigned group_grid(int n) {
     return static_cast<unsigned>((n + Group<K, TPR>::kRows - 1) / Group<K, TPR>::kRows);
@@ -295,6 +331,7 @@ constexpr int kGemvThreads = 128;
 template <typename T, int K>
 __global__ void __launch_bounds__(kGemvThreads) coarse_gemv_kernel(int nc, const T* __restrict__ inv,
                                                                   const T* __restrict__ b, T* __restrict__ x) {
+    pdl_enter();
     __shared__ T part[kGemvThreads / kWarp][K];
     const int row = blockIdx.x;
     T acc[K];
@@ -384,6 +421,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) spmv_alpha_kernel(
     const TZ* __restrict__ z, T* __restrict__ p, T* __restrict__ ap, double* partials, unsigned* counter,
     const double* __restrict__ rz, const double* __restrict__ beta, const int* __restrict__ frozen,
     double* __restrict__ alpha) {
+    pdl_enter();
     constexpr int ROWS = ReduceTile<TPR>::kRows;
     const int r = threadIdx.x / (TPR * K);
     const int sub = (threadIdx.x / K) % TPR;
@@ -433,6 +471,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) update_xr_kernel(
     int* __restrict__ conv_iter, double* __restrict__ rel_out, int record, const TZ* __restrict__ dinv, TZ alpha0,
     TZ* __restrict__ z0, TZ* __restrict__ r_lo, cudaGraphConditionalHandle loop, int use_loop,
     const int* __restrict__ cap) {
+    pdl_enter();
     const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
     const int tiles = n_tiles_dev(n);
@@ -509,6 +548,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) dot_beta_kernel(int n, cons
                                                                      unsigned* counter, double* __restrict__ rz,
                                                                      const int* __restrict__ frozen,
                                                                      double* __restrict__ beta) {
+    pdl_enter();
     const int slot = threadIdx.x / K;
     const int c = threadIdx.x % K;
     const int tiles = n_tiles_dev(n);
@@ -532,6 +572,7 @@ __global__ void __launch_bounds__(tile_threads<K>()) cheby_dot_kernel(
     const T* __restrict__ dinv, const T* __restrict__ b, const T* __restrict__ x_cur, const T* __restrict__ x_prev,
     T c_cur, T c_prev, T alpha, T* __restrict__ z, double* partials, unsigned* counter, double* __restrict__ rz,
     const int* __restrict__ frozen, double* __restrict__ beta) {
+    pdl_enter();
     constexpr int ROWS = ReduceTile<TPR>::kRows;
     const int r = threadIdx.x / (TPR * K);
     const int sub = (threadIdx.x / K) % TPR;
@@ -679,6 +720,9 @@ class Solver {
     const Hierarchy* h = nullptr;
     int n = 0;
     int kcap = 0;
+    // Solve-loop kernels launched with programmatic stream serialization (pdl_enter); off with
+    // CUNIBS_PROGRAMMATIC_LAUNCH=0.
+    bool pdl = true;
     cudaStream_t stream = nullptr;
     // FP64 CG / outer workspace (n, kcap)
     DevArray<double> B, X, R, P, AP, Z;
@@ -946,7 +990,8 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     constexpr int TT = tile_threads<K>();
     cudaStream_t s = stream;
     if (L == 0) {
-        coarse_gemv_kernel<T, K><<<n_bottom, kGemvThreads, 0, s>>>(n_bottom, cinv<T>(), b, z); count_launch();
+        launch_loop(pdl, coarse_gemv_kernel<T, K>, n_bottom, kGemvThreads, s, n_bottom, cinv<T>(), b, z);
+        count_launch();
         return false;
     }
     const bool fuse_dot = dot && H.levels[0].tpr_a <= 16;
@@ -960,8 +1005,8 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         const Level& lv = H.levels[l];
         dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            cheby_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
-                lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al, out);
+            launch_loop(pdl, cheby_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
+                        lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al, out);
         });
         count_launch();
     };
@@ -988,10 +1033,10 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
                 const Level& lv = H.levels[0];
                 dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
                     constexpr int TPR = decltype(tc)::value;
-                    cheby_dot_kernel<T, K, TPR><<<reduce_grid_rows<TPR>(lv.n), TT, 0, s>>>(
-                        lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(0), ldinv<T>(0), bi, cur, prev,
-                        static_cast<T>(ch.c_cur[st - 1]), cp, static_cast<T>(ch.alpha[st - 1]), out, partials.get(),
-                        counter.get(), rz.get(), frozen.get(), beta.get());
+                    launch_loop(pdl, cheby_dot_kernel<T, K, TPR>, reduce_grid_rows<TPR>(lv.n), TT, s, lv.n,
+                                lv.a.ptr.get(), lv.a.col.get(), lval<T>(0), ldinv<T>(0), bi, cur, prev,
+                                static_cast<T>(ch.c_cur[st - 1]), cp, static_cast<T>(ch.alpha[st - 1]), out,
+                                partials.get(), counter.get(), rz.get(), frozen.get(), beta.get());
                 });
                 count_launch();
                 prev = cur;
@@ -1012,14 +1057,14 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         T* other = odd ? w.r[l].get() : w.x[l].get();
         const unsigned g = n_tiles(lv.n);
         if (l == 0 && !jz_done) {
-            jz_kernel<T, K><<<g, TT, 0, s>>>(lv.n, ldinv<T>(0), bi, static_cast<T>(ch.alpha0), first);
+            launch_loop(pdl, jz_kernel<T, K>, g, TT, s, lv.n, ldinv<T>(0), bi, static_cast<T>(ch.alpha0), first);
             count_launch();
         }
         sweep(l, bi, nullptr, first, other, nullptr);
         dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            residual_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
-                lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
+            launch_loop(pdl, residual_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
+                        lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
         });
         count_launch();
         const bool next_is_level = (l + 1 < L);
@@ -1033,13 +1078,13 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         }
         dispatch_tpr<K>(lv.tpr_r, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            restrict_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n_coarse), Group<K, TPR>::kBlock, 0, s>>>(
-                lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(), rval<T>(l), w.r[l].get(), nb, nd,
-                static_cast<T>(ch.alpha0), nx);
+            launch_loop(pdl, restrict_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n_coarse), Group<K, TPR>::kBlock, s,
+                        lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(), rval<T>(l), w.r[l].get(), nb, nd,
+                        static_cast<T>(ch.alpha0), nx);
         });
         count_launch();
     }
-    coarse_gemv_kernel<T, K><<<n_bottom, kGemvThreads, 0, s>>>(n_bottom, cinv<T>(), w.cb.get(), w.cx.get());
+    launch_loop(pdl, coarse_gemv_kernel<T, K>, n_bottom, kGemvThreads, s, n_bottom, cinv<T>(), w.cb.get(), w.cx.get());
     count_launch();
     // Up-sweep.
     const T* xc = w.cx.get();
@@ -1048,8 +1093,8 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         const T* bi = (l == 0) ? b : w.b[l].get();
         dispatch_tpr<K>(lv.tpr_p, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
-            prolong_kernel<T, K, TPR><<<group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, 0, s>>>(
-                lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
+            launch_loop(pdl, prolong_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
+                        lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
         });
         count_launch();
         // The level's smoothed correction stays wherever its sweep left it; the next finer
@@ -1084,8 +1129,8 @@ void Solver::pcg_tail(TZ* r_v, TZ* z, bool jz_done) {
     constexpr int TT = tile_threads<K>();
     const bool fused = vcycle<TZ, K>(r_v, z, jz_done, true);
     if (!fused) {
-        dot_beta_kernel<TZ, K><<<reduce_grid(n), TT, 0, stream>>>(n, r_v, z, partials.get(), counter.get(), rz.get(),
-                                                                 frozen.get(), beta.get());
+        launch_loop(pdl, dot_beta_kernel<TZ, K>, reduce_grid(n), TT, stream, n, r_v, z, partials.get(), counter.get(),
+                    rz.get(), frozen.get(), beta.get());
         count_launch();
     }
 }
@@ -1098,17 +1143,16 @@ void Solver::pcg_iteration(const int* ptr, const int* col, const T* val, T* x, T
     const unsigned g = reduce_grid(n);
     dispatch_tpr<K>(tpr0(), [&](auto tc) {
         constexpr int TPR = decltype(tc)::value;
-        spmv_alpha_kernel<T, TZ, K, TPR><<<reduce_grid_rows<TPR>(n), TT, 0, stream>>>(
-            n, ptr, col, val, z, p, ap, partials.get(), counter.get(), rz.get(), beta.get(), frozen.get(),
-            alpha.get());
+        launch_loop(pdl, spmv_alpha_kernel<T, TZ, K, TPR>, reduce_grid_rows<TPR>(n), TT, stream, n, ptr, col, val, z,
+                    p, ap, partials.get(), counter.get(), rz.get(), beta.get(), frozen.get(), alpha.get());
     });
     count_launch();
     const bool has_levels = !h->levels.empty();
     constexpr bool narrow = !std::is_same<T, TZ>::value;
-    update_xr_kernel<T, TZ, K><<<g, TT, 0, stream>>>(
-        n, alpha.get(), p, ap, x, r, partials.get(), counter.get(), ref, tol, tol_vec, frozen.get(), iter_counter.get(),
-        conv_iter.get(), rel.get(), record, has_levels ? ldinv<TZ>(0) : nullptr, static_cast<TZ>(h->cheby.alpha0),
-        has_levels ? first0<TZ>() : nullptr, narrow ? r_v : nullptr, loop, use_loop, cap.get());
+    launch_loop(pdl, update_xr_kernel<T, TZ, K>, g, TT, stream, n, alpha.get(), p, ap, x, r, partials.get(),
+                counter.get(), ref, tol, tol_vec, frozen.get(), iter_counter.get(), conv_iter.get(), rel.get(), record,
+                has_levels ? ldinv<TZ>(0) : nullptr, static_cast<TZ>(h->cheby.alpha0),
+                has_levels ? first0<TZ>() : nullptr, narrow ? r_v : nullptr, loop, use_loop, cap.get());
     count_launch();
     pcg_tail<TZ, K>(r_v, z, has_levels);
 }
@@ -1281,6 +1325,8 @@ SolverPtr make_solver(const Hierarchy& h, const Params& p) {
     // device-side WHILE node, for profilers that do not step into conditional graph bodies.
     const char* host_loop = std::getenv("CUNIBS_SOLVER_HOST_LOOP");
     sv->while_unsupported = host_loop != nullptr && host_loop[0] == '1';
+    const char* pdl = std::getenv("CUNIBS_PROGRAMMATIC_LAUNCH");
+    sv->pdl = !(pdl != nullptr && pdl[0] == '0');
     // The solver's kernels go at the highest stream priority: block preparation may run beside them.
     int least = 0, greatest = 0;
     CUNIBS_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
