@@ -324,7 +324,9 @@ def run_ours(args) -> dict:
     if args.warm_start == "on":
         # The Galerkin projection of each block's right-hand sides onto the network's basis (no network).
         pipelined(2, warm="projection")
+        torch.cuda.nvtx.range_push("projection_guess")  # lets a profiler capture exactly these blocks
         proj_ms, _, _ = pipelined(n_cmp, warm="projection")
+        torch.cuda.nvtx.range_pop()
         proj = (proj_ms, float(d_it.float().mean().item()), [round(v, 5) for v in d_rel0.cpu().numpy().tolist()])
     pipelined(2, precision=_native.PREC_MIXED, warm=False)
     mixed_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_MIXED, warm=False)
