@@ -132,48 +132,50 @@ __global__ void denorm_kernel(const float* __restrict__ pred, int k, int n_out, 
 // W[n][a] b[n][j] with W = V_hi + V_lo (the stored split basis). Block g takes the contiguous row
 // range [g * rows_per, (g + 1) * rows_per) in order, kProjUnroll rows per step with their basis loads
 // issued together; thread t owns basis column t (the basis is at most kProjThreads wide per pass,
-// wider bases loop). The block's right-hand-side rows are staged in shared memory.
+// wider bases loop). The block's right-hand-side rows are staged in shared memory. The partial sums
+// are FP32 (FP64 accumulation measured 174 us per block of 8 at the 1M-tet head, FP64-FMA bound):
+// the coefficients are rounded to a split BF16 pair (about 16 bits) before use, and the block
+// partials are summed in FP64.
 constexpr int kProjThreads = 256;
 constexpr int kProjBlocks = 592;
 constexpr int kProjUnroll = 8;
-constexpr int kProjStage = 64;  // right-hand-side rows staged per step (kProjStage x 16 doubles)
+constexpr int kProjStage = 64;  // right-hand-side rows staged per step (kProjStage x kMaxK floats)
 template <int kMaxK>
 __global__ void __launch_bounds__(kProjThreads) project_kernel(const __nv_bfloat16* __restrict__ basis, int n, int ld,
                                                                int n_out, const double* __restrict__ B, int K, int k,
                                                                int rows_per, double* __restrict__ part) {
-    __shared__ double sb[kProjStage][kMaxK];
+    __shared__ float sb[kProjStage][kMaxK];
     const int r0 = blockIdx.x * rows_per;
     const int r1 = min(n, r0 + rows_per);
     for (int a0 = 0; a0 < n_out; a0 += kProjThreads) {
         const int a = a0 + threadIdx.x;
-        double acc[kMaxK];
+        float acc[kMaxK];
 #pragma unroll
-        for (int j = 0; j < kMaxK; ++j) acc[j] = 0.0;
+        for (int j = 0; j < kMaxK; ++j) acc[j] = 0.0f;
         for (int s0 = r0; s0 < r1; s0 += kProjStage) {
             const int ns = min(kProjStage, r1 - s0);
             __syncthreads();
             for (int q = threadIdx.x; q < kProjStage * kMaxK; q += kProjThreads) {
                 const int rr = q / kMaxK, j = q % kMaxK;
-                sb[rr][j] = (rr < ns && j < k) ? B[static_cast<std::int64_t>(s0 + rr) * K + j] : 0.0;
+                sb[rr][j] = (rr < ns && j < k) ? static_cast<float>(B[static_cast<std::int64_t>(s0 + rr) * K + j]) : 0.0f;
             }
             __syncthreads();
             if (a < n_out) {
                 for (int u0 = 0; u0 < ns; u0 += kProjUnroll) {
-                    double wv[kProjUnroll];
+                    float wv[kProjUnroll];
 #pragma unroll
                     for (int u = 0; u < kProjUnroll; ++u) {
-                        wv[u] = 0.0;
+                        wv[u] = 0.0f;
                         if (u0 + u < ns) {
                             const __nv_bfloat16* w = basis + static_cast<std::int64_t>(s0 + u0 + u) * 2 * ld;
-                            wv[u] = static_cast<double>(__bfloat162float(w[a])) +
-                                    static_cast<double>(__bfloat162float(w[ld + a]));
+                            wv[u] = __bfloat162float(w[a]) + __bfloat162float(w[ld + a]);
                         }
                     }
 #pragma unroll
                     for (int u = 0; u < kProjUnroll; ++u)
 #pragma unroll
                         for (int j = 0; j < kMaxK; ++j)
-                            if (j < k) acc[j] = fma(wv[u], sb[u0 + u < ns ? u0 + u : 0][j], acc[j]);
+                            if (j < k) acc[j] = fmaf(wv[u], sb[u0 + u < ns ? u0 + u : 0][j], acc[j]);
                 }
             }
         }
