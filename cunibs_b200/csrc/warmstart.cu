@@ -161,21 +161,28 @@ __global__ void __launch_bounds__(kProjThreads) project_kernel(const __nv_bfloat
             }
             __syncthreads();
             if (a < n_out) {
-                for (int u0 = 0; u0 < ns; u0 += kProjUnroll) {
-                    float wv[kProjUnroll];
+                // Full steps without guards, so the step's basis loads issue together; then the tail.
+                int u0 = 0;
+                for (; u0 + kProjUnroll <= ns; u0 += kProjUnroll) {
+                    const __nv_bfloat16* w0 = basis + static_cast<std::int64_t>(s0 + u0) * 2 * ld + a;
+                    float hi[kProjUnroll], lo[kProjUnroll];
 #pragma unroll
                     for (int u = 0; u < kProjUnroll; ++u) {
-                        wv[u] = 0.0f;
-                        if (u0 + u < ns) {
-                            const __nv_bfloat16* w = basis + static_cast<std::int64_t>(s0 + u0 + u) * 2 * ld;
-                            wv[u] = __bfloat162float(w[a]) + __bfloat162float(w[ld + a]);
-                        }
+                        hi[u] = __bfloat162float(w0[static_cast<std::int64_t>(u) * 2 * ld]);
+                        lo[u] = __bfloat162float(w0[static_cast<std::int64_t>(u) * 2 * ld + ld]);
                     }
 #pragma unroll
-                    for (int u = 0; u < kProjUnroll; ++u)
+                    for (int u = 0; u < kProjUnroll; ++u) {
+                        const float wv = hi[u] + lo[u];
 #pragma unroll
-                        for (int j = 0; j < kMaxK; ++j)
-                            if (j < k) acc[j] = fmaf(wv[u], sb[u0 + u < ns ? u0 + u : 0][j], acc[j]);
+                        for (int j = 0; j < kMaxK; ++j) acc[j] = fmaf(wv, sb[u0 + u][j], acc[j]);
+                    }
+                }
+                for (; u0 < ns; ++u0) {
+                    const __nv_bfloat16* w = basis + static_cast<std::int64_t>(s0 + u0) * 2 * ld + a;
+                    const float wv = __bfloat162float(w[0]) + __bfloat162float(w[ld]);
+#pragma unroll
+                    for (int j = 0; j < kMaxK; ++j) acc[j] = fmaf(wv, sb[u0][j], acc[j]);
                 }
             }
         }
