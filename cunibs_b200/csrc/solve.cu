@@ -88,28 +88,6 @@ __device__ __forceinline__ void final_reduce(const double* __restrict__ partials
 template <typename T, int S, typename TX = T>
 __device__ __forceinline__ T strided_dot(const int* __restrict__ col, const T* __restrict__ val,
                                          const TX* __restrict__ x, int p, int e, long ld, int c, T acc) {
-    if constexpr (S == 1) {
-        // One lane per row: full batches of kPlainBatch entries with no bounds guards (their index,
-        // value and gather loads issue together), then the rest one by one; the additions stay in
-        // the row's order.
-        constexpr int kPlainBatch = 4;
-        for (; p + kPlainBatch <= e; p += kPlainBatch) {
-            int cj[kPlainBatch];
-            T vj[kPlainBatch];
-            TX xj[kPlainBatch];
-#pragma unroll
-            for (int j = 0; j < kPlainBatch; ++j) {
-                cj[j] = col[p + j];
-                vj[j] = val[p + j];
-            }
-#pragma unroll
-            for (int j = 0; j < kPlainBatch; ++j) xj[j] = x[cj[j] * ld + c];
-#pragma unroll
-            for (int j = 0; j < kPlainBatch; ++j) acc += vj[j] * static_cast<T>(xj[j]);
-        }
-        for (; p < e; ++p) acc += val[p] * static_cast<T>(x[col[p] * ld + c]);
-        return acc;
-    }
     constexpr int B = S == 1 ? 1 : 8;
     for (; p < e; p += B * S) {
         int cj[B];
