@@ -311,7 +311,7 @@ struct SigmaSlots {
     int slot[11];  // study position of each tissue tag, -1 for a tag that is not perturbed
 };
 struct SigmaColumns {
-    int a[16], j[16];  // (tissue position, placement) of each lane of a 16-wide solve block
+    int a[16], j[16];  // (tissue position, placement) of each lane of a solve block (at most 16 wide)
     int count;
 };
 struct SigmaDraw {
