@@ -344,17 +344,26 @@ def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: i
     # Held-out error of the standardised coefficients.
     xh = x16[n_fit:n_fit + n_hold // batch * batch].contiguous()
     held = []
+    mode_err = torch.zeros(r, dtype=torch.float64, device=coef.device)
     for s in range(0, xh.shape[0], batch):
         p = mlp.forward(xh[s:s + batch])
-        loss, *_ = mlp.loss_and_grad(p, target[n_fit + s:n_fit + s + batch].contiguous())
+        tb = target[n_fit + s:n_fit + s + batch].contiguous()
+        loss, *_ = mlp.loss_and_grad(p, tb)
         held.append(float(loss.item()))
+        mode_err += ((p[:, :r].double() - tb[:, :r].double()) ** 2).sum(0)
+    # Where the held-out error sits: its share in the leading modes (the guess's A-norm error is the
+    # coefficient error, the basis being A-orthonormal).
+    err_share = {}
+    if held:
+        cum = torch.cumsum(mode_err, 0) / mode_err.sum().clamp_min(1e-300)
+        err_share = {str(m): round(float(cum[m - 1]), 4) for m in (8, 16, 32, 64, 128) if m <= r}
     model = WarmStartModel(mlp, basis16, f_mean.contiguous(), f_std.contiguous(), c_mean.contiguous(),
                            c_std.contiguous(), r)
     model.stats = {"n_train": n_train, "rank": r, "train_iterations_mean": float(iters.mean()),
                    "data_s": round(t_data, 3), "basis_s": round(t_basis, 3), "train_s": round(t_train, 3),
                    "loss_curve": losses, "heldout_mse": float(np.mean(held)) if held else None,
                    "train_mse": losses[-1][1] if losses else None, "n_fit": n_fit, "epochs": epochs,
-                   "batch": batch}
+                   "batch": batch, "heldout_error_share_leading_modes": err_share}
     if install:
         model.install(ctx)
     return model
