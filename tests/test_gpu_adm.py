@@ -154,3 +154,15 @@ def test_resolve_target(setup):
     assert tiny.elem_idx.tolist() == adm.resolve_target(subj, adm.Target(point)).elem_idx.tolist()
     with pytest.raises(ValueError, match="contains no elements"):
         adm.resolve_target(subj, adm.Target(point, region="eye_balls"))
+
+
+def test_coverage_grid_holds_the_coil_at_every_rotation(setup):
+    subj, coil, _, _, tgt, bary = setup
+    centers = np.array([TOP, [20.0, 0.0, 87.7], [0.0, -20.0, 87.7]])
+    recip = adm.build_reciprocity(subj, coil, adm.Target(bary[tgt]), centers)
+    T, _ = subj.context.place(centers, None, np.full(3, DIST))
+    u, v = T[:, :3, 0], T[:, :3, 1]
+    for a in np.radians(np.arange(0.0, 360.0, 15.0)):
+        handles = centers + 50.0 * (np.cos(a) * v + np.sin(a) * u)
+        e = adm.evaluate(recip, coil, [Placement(c, hd, DIST) for c, hd in zip(centers, handles)], DIDT)
+        assert np.isfinite(e).all()

@@ -133,3 +133,50 @@ def test_study_guess_cuts_iterations_against_the_zero_guess_on_the_same_hierarch
         assert (diff < 1e-6).all(), diff
     ctx.set_conductivity(nominal, keep_coarse=True)
     subj.free()
+
+
+def test_study_properties_homogeneous_small_perturbation_subset_and_ensemble_size():
+    """Four properties of the reference's test_uq.py on the native study:
+    * a one-tissue head: scaling its only conductivity leaves the field as it was (and the nominal
+      solution is already the draw's, so the guess starts at the nominal solve's residual);
+    * a small perturbation: the first-order guess is nearly exact;
+    * a subset of perturbed tissues;
+    * draw i's result does not depend on how many draws the ensemble has."""
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    site = Placement(top, top + [0, 50, 0])
+    homog = Subject(sphere_head(8.0, 90.0, shells=((1.0, 2),), jitter_mm=0.3, seed=2), tolerance=1e-10)
+    res = homog.simulate_conductivity_uq(coil, site, ConductivityUQConfig(n_samples=3, seed=1), recovery="raw")
+    assert res.perturbed_tags == (2,)
+    np.testing.assert_allclose(res.peak_samples, res.peak_samples[0], rtol=1e-7)
+    homog.free()
+
+    subj = Subject(sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1), tolerance=1e-8)
+    ctx = subj.context
+    nominal = nominal_sigma_table()
+    c, h = top[None], (top + [0.0, 50.0, 0.0])[None]
+    tags = tuple(int(t) for t in np.unique(subj.mesh.tet_tags))
+    ctx.sigma_begin(coil, c, h, [4.0], 1e6, nominal, tags, recovery="raw")
+    try:
+        small = ctx.sigma_draw(nominal[list(tags)] * (1.0 + 1e-4 * np.arange(1, len(tags) + 1)))
+    finally:
+        ctx.sigma_end()
+    assert small["init_relres"][0] < 1e-5, small["init_relres"]
+
+    ctx.sigma_begin(coil, c, h, [4.0], 1e6, nominal, (3,), magnitude=True, recovery="raw")
+    try:
+        csf = ctx.sigma_draw([2.5])
+    finally:
+        ctx.sigma_end()
+    sigma = nominal.copy()
+    sigma[3] = 2.5
+    ctx.set_conductivity(sigma, keep_coarse=True)
+    ref = ctx.solve_block(coil, c, h, [4.0], 1e6, magnitude=True, recovery="raw")
+    ctx.set_conductivity(nominal, keep_coarse=True)
+    assert np.linalg.norm(csf["magnE"] - ref["magnE"]) / np.linalg.norm(ref["magnE"]) < 1e-6
+
+    three = subj.simulate_conductivity_uq(coil, site, ConductivityUQConfig(n_samples=3, seed=8), recovery="raw")
+    five = subj.simulate_conductivity_uq(coil, site, ConductivityUQConfig(n_samples=5, seed=8), recovery="raw")
+    np.testing.assert_array_equal(five.peak_samples[:3], three.peak_samples)
+    np.testing.assert_array_equal(five.iteration_samples[:3], three.iteration_samples)
+    subj.free()

@@ -65,3 +65,18 @@ def test_result_round_trip(tmp_path):
     assert set(back.tissue_sensitivity("focality")) == {2, 3}
     with pytest.raises(ValueError, match="Unknown output"):
         back.tissue_sensitivity("roi")
+
+
+def test_zero_cov_draws_are_the_nominal_conductivity():
+    tags = (2, 3)
+    for dist in ("lognormal", "normal"):
+        cfg = ConductivityUQConfig(n_samples=16, seed=5, tissue_cov={2: 0.0, 3: 0.0}, distribution=dist)
+        s = sample_conductivities(cfg, tags)
+        np.testing.assert_allclose(s, np.tile([TISSUE_CONDUCTIVITY[2], TISSUE_CONDUCTIVITY[3]], (16, 1)), rtol=1e-15)
+
+
+def test_draws_of_a_smaller_ensemble_are_a_prefix():
+    tags = (1, 2, 3)
+    small = sample_conductivities(ConductivityUQConfig(n_samples=3, seed=4), tags)
+    large = sample_conductivities(ConductivityUQConfig(n_samples=9, seed=4), tags)
+    np.testing.assert_array_equal(large[:3], small)
