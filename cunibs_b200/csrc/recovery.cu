@@ -550,31 +550,10 @@ __global__ void harmonic_apply_kernel(const float4* __restrict__ wq, const int* 
     const int s = static_cast<int>(q / K), c = static_cast<int>(q % K);
     if (s >= n_slots || c >= k) return;
     double ax = 0.0, ay = 0.0, az = 0.0;
-    auto value = [&](int m) {
-        return (m == ground) ? 0.0 : x[static_cast<std::int64_t>(m - (m > ground ? 1 : 0)) * K + c];
-    };
-    int p = pptr[s];
-    const int end = pptr[s + 1];
-    // Full batches of four entries without bounds guards, so their operator loads and potential
-    // gathers issue together; then the rest one by one. The additions keep the patch order.
-    constexpr int kBatch = 4;
-    for (; p + kBatch <= end; p += kBatch) {
-        float4 e[kBatch];
-        double vm[kBatch];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) e[j] = wq[p + j];
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) vm[j] = value(__float_as_int(e[j].w));
-#pragma unroll
-        for (int j = 0; j < kBatch; ++j) {
-            ax = fma(static_cast<double>(e[j].x), vm[j], ax);
-            ay = fma(static_cast<double>(e[j].y), vm[j], ay);
-            az = fma(static_cast<double>(e[j].z), vm[j], az);
-        }
-    }
-    for (; p < end; ++p) {
+    for (int p = pptr[s], end = pptr[s + 1]; p < end; ++p) {
         const float4 e = wq[p];
-        const double vm = value(__float_as_int(e.w));
+        const int m = __float_as_int(e.w);
+        const double vm = (m == ground) ? 0.0 : x[static_cast<std::int64_t>(m - (m > ground ? 1 : 0)) * K + c];
         ax = fma(static_cast<double>(e.x), vm, ax);
         ay = fma(static_cast<double>(e.y), vm, ay);
         az = fma(static_cast<double>(e.z), vm, az);
