@@ -312,9 +312,30 @@ class Subject:
                                        potential=potential, nodal=nodal, recovery=recovery, block_k=block_k)
         return result
 
+    def roi(self, point_mm, radius_mm: float = 0.0, region: metrics.Region = "gray_matter"):
+        """Volume-weighted ROI of ``region`` elements around ``point_mm`` (the nearest one when the
+        radius is 0), usable as a ``record_rois`` probe or an auxiliary-dipole-method target
+        (reference simulation.py:233-248)."""
+        from . import adm
+
+        return adm.resolve_target(self, adm.Target(point_mm, region=region, radius_mm=radius_mm))
+
+    def depth_probes(self, cortical_point_mm, inward_dir, depths_mm: Sequence[float], radius_mm: float = 0.0,
+                     region: metrics.Region = "all") -> list:
+        """ROIs at increasing depth along ``inward_dir`` from a cortical point (simulation.py:250-267)."""
+        p = np.array(cortical_point_mm, dtype=np.float64).reshape(-1)
+        d = np.array(inward_dir, dtype=np.float64).reshape(-1)
+        if p.shape != (3,) or d.shape != (3,):
+            raise ValueError("cortical_point_mm and inward_dir must be 3-vectors")
+        norm = float(np.linalg.norm(d))
+        if not np.isfinite(norm) or norm == 0.0:
+            raise ValueError("inward_dir must be a non-zero, finite 3-vector.")
+        d = d / norm
+        return [self.roi(p + depth * d, radius_mm=radius_mm, region=region) for depth in depths_mm]
+
     def iter_simulate_conductivity_uq(self, coil: Coil, placements: Sequence[Placement], config, didt: float = 1e6,
                                       *, moments: bool = False, recovery: str = "harmonic",
-                                      focality_frac: float = 0.5) -> Iterator:
+                                      focality_frac: float = 0.5, record_rois=None) -> Iterator:
         """Stream a conductivity Monte Carlo per placement (reference simulation.py:594-630).
 
         Every draw of ``config`` (:class:`cunibs_b200.uq.ConductivityUQConfig`) re-weights the
@@ -325,7 +346,8 @@ class Subject:
         :class:`cunibs_b200.uq.ConductivityUQResult` carries the per-draw gray-matter peak,
         focality (stimulated volume at ``focality_frac`` x p99.9, 0.5 or 0.75) and peak location;
         ``moments=True`` adds per-tetrahedron mean/std/cov of |E| and the summary of the mean field.
-        The subject is back at the nominal conductivities afterwards.
+        ``record_rois`` ({name: ROI from :meth:`roi`}) adds each draw's volume-weighted mean |E| per
+        ROI (``roi_samples``). The subject is back at the nominal conductivities afterwards.
         """
         from . import uq
 
@@ -337,9 +359,13 @@ class Subject:
             raise ValueError("focality_frac must be 0.5 or 0.75 (the native summary's focality levels)")
         if not isinstance(config, uq.ConductivityUQConfig) or config.n_samples < 1:
             raise ValueError("config must be a ConductivityUQConfig with n_samples >= 1")
-        return self._iter_uq(coil, sites, config, float(didt), bool(moments), recovery, focality_frac)
+        rois = dict(record_rois or {})
+        for name, r in rois.items():
+            if not hasattr(r, "elem_idx") or not hasattr(r, "weights"):
+                raise TypeError(f"record_rois[{name!r}] must be an ROI from Subject.roi")
+        return self._iter_uq(coil, sites, config, float(didt), bool(moments), recovery, focality_frac, rois)
 
-    def _iter_uq(self, coil, sites, config, didt, moments, recovery, focality_frac):
+    def _iter_uq(self, coil, sites, config, didt, moments, recovery, focality_frac, rois):
         from . import uq
 
         ctx = self.context
@@ -366,14 +392,15 @@ class Subject:
             foc = np.empty((k, n))
             loc = np.empty((k, n, 3))
             its = np.empty((k, n), np.int32)
+            roi_s = {name: np.empty((k, n)) for name in rois}
             s1 = s2 = None
             resetups = 0
             # The study holds the chunk's coil field, nominal solution and sensitivities; each draw
             # swaps the finest operator's values and starts PCG from the sensitivity-subspace guess.
             with self._lock:
                 try:
-                    ctx.sigma_begin(coil, centers, handles, dists, didt, nominal, tags, magnitude=moments,
-                                    recovery=recovery)
+                    ctx.sigma_begin(coil, centers, handles, dists, didt, nominal, tags,
+                                    magnitude=moments or bool(rois), recovery=recovery)
                     for i in range(n):
                         try:
                             out = ctx.sigma_draw(draws[i])
@@ -383,6 +410,8 @@ class Subject:
                         rows = out["summary"]
                         peak[:, i], foc[:, i], loc[:, i] = rows[:, 0], rows[:, f_col], rows[:, 1:4]
                         its[:, i] = out["iterations"]
+                        for name, r in rois.items():  # volume-weighted ROI means (run.py:378-379)
+                            roi_s[name][:, i] = out["magnE"][:, r.elem_idx].astype(np.float64) @ r.weights
                         if moments:
                             m = out["magnE"].astype(np.float64)
                             s1 = m.copy() if s1 is None else s1 + m
@@ -401,19 +430,22 @@ class Subject:
                     sigma_samples=draws, vols=host[0] if host else None, tet_tags=host[1] if host else None,
                     barycenters_mm=host[2] if host else None, placement=site, coil_name=coil.name, didt=didt,
                     peak_samples=peak[j], focality_samples=foc[j], peak_location_samples=loc[j],
-                    iteration_samples=its[j], recovery=recovery, full_resetups=resetups)
+                    iteration_samples=its[j], recovery=recovery, full_resetups=resetups,
+                    roi_samples={name: roi_s[name][j].copy() for name in rois})
                 if moments:
                     res.summary = res.compute_summary()
                 yield res
 
     def simulate_conductivity_uq(self, coil: Coil, placement: Placement, config, didt: float = 1e6, *,
-                                 moments: bool = False, recovery: str = "harmonic", focality_frac: float = 0.5):
+                                 moments: bool = False, recovery: str = "harmonic", focality_frac: float = 0.5,
+                                 record_rois=None):
         """Conductivity Monte Carlo for a single placement (reference simulation.py:632-664)."""
         if not isinstance(placement, Placement):
             raise TypeError("simulate_conductivity_uq() takes a single Placement; use "
                             "iter_simulate_conductivity_uq() for a sequence.")
         (result,) = self.iter_simulate_conductivity_uq(coil, [placement], config, didt, moments=moments,
-                                                       recovery=recovery, focality_frac=focality_frac)
+                                                       recovery=recovery, focality_frac=focality_frac,
+                                                       record_rois=record_rois)
         return result
 
 

@@ -118,6 +118,7 @@ class ConductivityUQResult:
     summary: ConductivityUQSummary | None = None
     recovery: str = "raw"
     full_resetups: int = 0  # draws solved again after a full re-setup
+    roi_samples: dict[str, npt.NDArray[np.float64]] = field(default_factory=dict)  # name -> per-draw ROI mean |E|
 
     def compute_summary(self, region: metrics.Region = "gray_matter") -> ConductivityUQSummary:
         if self.mean_magnE is None or self.cov_magnE is None:
@@ -144,12 +145,17 @@ class ConductivityUQResult:
         return self._summary_for(region).max_local_cov
 
     def tissue_sensitivity(self, output: str = "peak") -> dict[int, float]:
+        """Variance shares of the perturbed tissues in a per-draw output (result.py:31-62): "peak",
+        "focality" or the name of an ROI recorded with ``record_rois``."""
         if output == "peak":
             y = self.peak_samples
         elif output == "focality":
             y = self.focality_samples
+        elif output in self.roi_samples:
+            y = self.roi_samples[output]
         else:
-            raise ValueError(f"Unknown output {output!r}; expected 'peak' or 'focality'.")
+            raise ValueError(f"Unknown output {output!r}; expected 'peak', 'focality', or a recorded ROI name "
+                             f"(available: {['peak', 'focality', *self.roi_samples]}).")
         return tissue_sensitivity(self.sigma_samples, y, self.perturbed_tags)
 
     def save(self, path: str | Path) -> None:
@@ -163,7 +169,10 @@ class ConductivityUQResult:
             placement_distance_mm=self.placement.distance_mm, coil_name=self.coil_name, didt=self.didt,
             peak_samples=self.peak_samples, focality_samples=self.focality_samples,
             peak_location_samples=self.peak_location_samples, iteration_samples=self.iteration_samples,
-            recovery=self.recovery, full_resetups=self.full_resetups, **arrays)
+            recovery=self.recovery, full_resetups=self.full_resetups,
+            roi_names=np.array(list(self.roi_samples), dtype=np.str_),
+            roi_samples=np.stack([self.roi_samples[k] for k in self.roi_samples]) if self.roi_samples
+            else np.zeros((0, self.n_samples)), **arrays)
 
     @classmethod
     def load(cls, path: str | Path) -> ConductivityUQResult:
@@ -184,7 +193,9 @@ class ConductivityUQResult:
                 focality_samples=np.asarray(z["focality_samples"]),
                 peak_location_samples=np.asarray(z["peak_location_samples"]),
                 iteration_samples=np.asarray(z["iteration_samples"]), recovery=str(z["recovery"]),
-                full_resetups=int(z["full_resetups"]))
+                full_resetups=int(z["full_resetups"]),
+                roi_samples={str(n): np.asarray(v) for n, v in zip(z["roi_names"], z["roi_samples"])}
+                if "roi_names" in z.files else {})
         if res.mean_magnE is not None:
             res.summary = res.compute_summary()
         return res

@@ -180,3 +180,26 @@ def test_study_properties_homogeneous_small_perturbation_subset_and_ensemble_siz
     np.testing.assert_array_equal(five.peak_samples[:3], three.peak_samples)
     np.testing.assert_array_equal(five.iteration_samples[:3], three.iteration_samples)
     subj.free()
+
+
+def test_record_rois_and_depth_probes():
+    """Per-draw ROI means (record_rois) are the volume-weighted |E| of the ROI in each draw: their
+    ensemble mean is the ROI's weighted mean of the per-element mean field."""
+    mesh = sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    site = Placement(top, top + [0, 50, 0])
+    subj = Subject(mesh, tolerance=1e-8)
+    rois = {"vertex": subj.roi([0.0, 0.0, 72.0], radius_mm=8.0), "one": subj.roi([10.0, 0.0, 70.0])}
+    probes = subj.depth_probes([0.0, 0.0, 76.0], [0.0, 0.0, -1.0], [0.0, 10.0, 20.0], radius_mm=5.0)
+    assert len(probes) == 3 and len({tuple(p.elem_idx[:3]) for p in probes}) == 3
+    with pytest.raises(ValueError, match="non-zero"):
+        subj.depth_probes([0.0, 0.0, 76.0], [0.0, 0.0, 0.0], [0.0])
+    res = subj.simulate_conductivity_uq(coil, site, ConductivityUQConfig(n_samples=4, seed=6), moments=True,
+                                        recovery="raw", record_rois=rois)
+    for name, r in rois.items():
+        s = res.roi_samples[name]
+        assert s.shape == (4,) and (s > 0).all()
+        assert s.mean() == pytest.approx(float(res.mean_magnE[r.elem_idx] @ r.weights), rel=1e-9)
+    assert set(res.tissue_sensitivity("vertex")) == set(res.perturbed_tags)
+    subj.free()

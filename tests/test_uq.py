@@ -80,3 +80,25 @@ def test_draws_of_a_smaller_ensemble_are_a_prefix():
     small = sample_conductivities(ConductivityUQConfig(n_samples=3, seed=4), tags)
     large = sample_conductivities(ConductivityUQConfig(n_samples=9, seed=4), tags)
     np.testing.assert_array_equal(large[:3], small)
+
+
+def test_roi_samples_round_trip_and_feed_the_sensitivity(tmp_path):
+    rng = np.random.default_rng(3)
+    n, tags = 64, (2, 3)
+    sig = np.exp(rng.normal(0.0, 0.2, size=(n, 2)))
+    roi = np.exp(0.8 * np.log(sig[:, 1]))  # driven by tag 3 alone
+    res = ConductivityUQResult(
+        mean_magnE=None, std_magnE=None, cov_magnE=None, n_samples=n, perturbed_tags=tags, sigma_samples=sig,
+        vols=None, tet_tags=None, barycenters_mm=None, placement=Placement([0, 0, 90.0], [0, 50, 90.0]),
+        coil_name="fig8", didt=1e6, peak_samples=np.ones(n), focality_samples=np.ones(n),
+        peak_location_samples=np.zeros((n, 3)), iteration_samples=np.zeros(n, np.int32),
+        roi_samples={"M1": roi})
+    share = res.tissue_sensitivity("M1")
+    assert share[3] == pytest.approx(1.0, abs=1e-9) and share[2] == pytest.approx(0.0, abs=1e-9)
+    assert res.tissue_sensitivity("peak") == {2: 0.0, 3: 0.0}
+    with pytest.raises(ValueError, match="available"):
+        res.tissue_sensitivity("V1")
+    res.save(tmp_path / "r.npz")
+    back = ConductivityUQResult.load(tmp_path / "r.npz")
+    assert list(back.roi_samples) == ["M1"]
+    np.testing.assert_array_equal(back.roi_samples["M1"], roi)
