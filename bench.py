@@ -560,11 +560,12 @@ def adm_measure(ctx, coil, sites, stream) -> dict:
     return out
 
 
-def multi_subject_measure(coil, recovery, n_place=16) -> dict:
+def multi_subject_measure(coil, recovery, n_place=16, repeats=3) -> dict:
     """Three subjects of uneven size (0.3M, 0.6M and 1.0M tetrahedra, the same 10-tissue sphere at
     3.93, 3.12 and 2.63 mm) swept with 16 placements each: one after another, then side by side from
     one host thread per subject (cunibs_b200.batch). Wall clock around each whole run (results
-    copied to the host); the per-subject results of the two runs are checked bitwise equal."""
+    copied to the host), three repetitions of each alternating, the median kept; the per-subject results
+    of the two runs are checked bitwise equal."""
     from cunibs_b200 import Placement, Subject
     from cunibs_b200.batch import SubjectJob, simulate_subjects
 
@@ -579,16 +580,21 @@ def multi_subject_measure(coil, recovery, n_place=16) -> dict:
     jobs = [SubjectJob(s, coil, sites, options=dict(recovery=recovery, magnitude=True)) for s in subjects]
     for j in jobs:  # contexts, recovery operators and loop graphs built outside the timing
         list(j.subject.iter_simulate(coil, sites[:8], recovery=recovery))
-    t0 = time.perf_counter()
-    alone = [list(j.subject.iter_simulate(coil, sites, recovery=recovery, magnitude=True)) for j in jobs]
-    seq_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    together = simulate_subjects(jobs)
-    con_s = time.perf_counter() - t0
-    same = all(np.array_equal(a.magnE, b.magnE) for ra, rb in zip(alone, together) for a, b in zip(ra, rb))
+    seq, con, same = [], [], True
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        alone = [list(j.subject.iter_simulate(coil, sites, recovery=recovery, magnitude=True)) for j in jobs]
+        seq.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        together = simulate_subjects(jobs)
+        con.append(time.perf_counter() - t0)
+        same = same and all(np.array_equal(a.magnE, b.magnE) for ra, rb in zip(alone, together) for a, b in zip(ra, rb))
+    seq_s, con_s = float(np.median(seq)), float(np.median(con))
     out = {"what": "3 subjects (0.3M / 0.6M / 1.0M tets) x 16 placements, harmonic recovery, |E| retained",
            "n_tets": [int(s.context.n_tets) for s in subjects], "sequential_s": round(seq_s, 4),
-           "concurrent_s": round(con_s, 4), "placements_per_s_sequential": round(3 * n_place / seq_s, 1),
+           "concurrent_s": round(con_s, 4), "repeats_s": {"sequential": [round(t, 4) for t in seq],
+                                                          "concurrent": [round(t, 4) for t in con]},
+           "placements_per_s_sequential": round(3 * n_place / seq_s, 1),
            "placements_per_s_concurrent": round(3 * n_place / con_s, 1), "speedup": round(seq_s / con_s, 3),
            "bitwise_equal": bool(same)}
     for s in subjects:
