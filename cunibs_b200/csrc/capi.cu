@@ -1178,9 +1178,10 @@ int cunibs_adm_sample(cunibs_adm* a, const double* origin_mm, const double* spac
         adm_sources(a, center, packed, Td, s);
         a->sampled = false;
         a->Q.resize(3 * static_cast<std::size_t>(n_grid) * a->dirs.n);
-        // Q_d on the grid: the coil-field N-body with the mesh nodes as sources (reciprocity.py:183-213).
-        dadt_nodes_raw(pts.get(), static_cast<int>(n_grid), reinterpret_cast<const float*>(packed.get()),
-                       a->ctx->mesh.n_nodes, Td.get(), a->dirs.n, 1.0, a->Q.get(), s);
+        // Q_d on the grid: the coil-field N-body with the mesh nodes as sources (reciprocity.py:183-213),
+        // every direction in one pass over the sources.
+        dadt_nodes_shared(pts.get(), static_cast<int>(n_grid), reinterpret_cast<const float*>(packed.get()),
+                          a->ctx->mesh.n_nodes, Td.get(), a->dirs.n, 1.0, a->Q.get(), s);
         CUNIBS_LAUNCH_CHECK("reciprocity field");
         CUNIBS_CHECK(cudaStreamSynchronize(s));
         a->grid = gr;

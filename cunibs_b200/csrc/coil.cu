@@ -140,6 +140,110 @@ __global__ void __launch_bounds__(kDadtThreads) dadt_kernel(const double* __rest
     }
 }
 
+// ND source sets that share their positions and differ only in their moments (the mesh nodes as
+// the sources of an adjoint's ND directions). One shared-memory record per source holds the
+// position once and every set's moment.
+template <int ND>
+struct __align__(16) SharedSource {
+    float2 sx, sy, sz;
+    float2 m[ND][3];
+};
+
+// The field of ND source sets at common positions (records d * n_dip + j of prep_dipoles, all
+// prepared with the one transform T): per (target, source) pair the difference and 1/|d|^3 are
+// formed once and used for every set. Per set the arithmetic and the order over sources are
+// dadt_kernel's, so set d's field is bitwise what dadt_kernel gives for it as one placement.
+// Work items are node tiles only; node order within a tile as dadt_kernel's.
+template <int ND>
+__global__ void __launch_bounds__(kDadtThreads) dadt_shared_kernel(const double* __restrict__ nodes_mm, int n_nodes,
+                                                                   const DipolePacked* __restrict__ dip, int n_dip,
+                                                                   const double* __restrict__ T, float scale,
+                                                                   float* __restrict__ out, int n_tiles) {
+    __shared__ SharedSource<ND> tile[kDipTile];
+    const double ox = T[3] * 1e-3, oy = T[7] * 1e-3, oz = T[11] * 1e-3;
+    const int stride = n_tiles * blockDim.x;
+    for (int item = blockIdx.x; item < n_tiles; item += gridDim.x) {
+    const int base = item * blockDim.x + threadIdx.x;
+    int node[4];
+    float rxs[4], rys[4], rzs[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        node[u] = base + u * stride;
+        const int i = node[u] < n_nodes ? node[u] : n_nodes - 1;
+        rxs[u] = static_cast<float>(nodes_mm[3 * static_cast<long>(i)] * 1e-3 - ox);
+        rys[u] = static_cast<float>(nodes_mm[3 * static_cast<long>(i) + 1] * 1e-3 - oy);
+        rzs[u] = static_cast<float>(nodes_mm[3 * static_cast<long>(i) + 2] * 1e-3 - oz);
+    }
+    const float2 rx[2] = {make_float2(rxs[0], rxs[1]), make_float2(rxs[2], rxs[3])};
+    const float2 ry[2] = {make_float2(rys[0], rys[1]), make_float2(rys[2], rys[3])};
+    const float2 rz[2] = {make_float2(rzs[0], rzs[1]), make_float2(rzs[2], rzs[3])};
+    float2 ax[ND][2], ay[ND][2], az[ND][2];
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) ax[d][q] = ay[d][q] = az[d][q] = make_float2(0.f, 0.f);
+    for (int t0 = 0; t0 < n_dip; t0 += kDipTile) {
+        const int nt = min(kDipTile, n_dip - t0);
+        __syncthreads();
+        for (int j = threadIdx.x; j < nt; j += blockDim.x) {
+            const DipolePacked p0 = dip[t0 + j];
+            SharedSource<ND> r;
+            r.sx = p0.sx;
+            r.sy = p0.sy;
+            r.sz = p0.sz;
+#pragma unroll
+            for (int d = 0; d < ND; ++d) {
+                const DipolePacked pd = dip[static_cast<long>(d) * n_dip + t0 + j];
+                r.m[d][0] = pd.mx;
+                r.m[d][1] = pd.my;
+                r.m[d][2] = pd.mz;
+            }
+            tile[j] = r;
+        }
+        __syncthreads();
+        for (int j = 0; j < nt; ++j) {
+            const float2 sx = tile[j].sx, sy = tile[j].sy, sz = tile[j].sz;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const float2 dx = __fadd2_rn(rx[q], f2neg(sx));
+                const float2 dy = __fadd2_rn(ry[q], f2neg(sy));
+                const float2 dz = __fadd2_rn(rz[q], f2neg(sz));
+                float2 d2 = __fmul2_rn(dx, dx);
+                d2 = __ffma2_rn(dy, dy, d2);
+                d2 = __ffma2_rn(dz, dz, d2);
+                const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+                const float2 w = __fmul2_rn(__fmul2_rn(inv, inv), inv);
+#pragma unroll
+                for (int d = 0; d < ND; ++d) {
+                    const float2 mx = tile[j].m[d][0], my = tile[j].m[d][1], mz = tile[j].m[d][2];
+                    const float2 cx = __ffma2_rn(my, dz, __fmul2_rn(f2neg(mz), dy));
+                    const float2 cy = __ffma2_rn(mz, dx, __fmul2_rn(f2neg(mx), dz));
+                    const float2 cz = __ffma2_rn(mx, dy, __fmul2_rn(f2neg(my), dx));
+                    ax[d][q] = __ffma2_rn(w, cx, ax[d][q]);
+                    ay[d][q] = __ffma2_rn(w, cy, ay[d][q]);
+                    az[d][q] = __ffma2_rn(w, cz, az[d][q]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+        const float vx[4] = {ax[d][0].x, ax[d][0].y, ax[d][1].x, ax[d][1].y};
+        const float vy[4] = {ay[d][0].x, ay[d][0].y, ay[d][1].x, ay[d][1].y};
+        const float vz[4] = {az[d][0].x, az[d][0].y, az[d][1].x, az[d][1].y};
+        float* o = out + static_cast<long>(d) * n_nodes * 3;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (node[u] < n_nodes) {
+                o[3 * static_cast<long>(node[u])] = scale * vx[u];
+                o[3 * static_cast<long>(node[u]) + 1] = scale * vy[u];
+                o[3 * static_cast<long>(node[u]) + 2] = scale * vz[u];
+            }
+        }
+    }
+    }
+}
+
 // dadt_elm[p][e] = 1/4 sum of the four nodal values (dadt_element.cu:6-31).
 __global__ void element_average_kernel(const float* __restrict__ nodal, const int* __restrict__ tets, int n_nodes,
                                        int n_tets, int k, float* __restrict__ elm) {
@@ -232,6 +336,20 @@ void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed
     dadt_kernel<<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
                                                  n_dip, transforms_dev, static_cast<float>(didt * 1e-7), out,
                                                  g.n_tiles, g.n_items);
+    count_launch();
+}
+
+void dadt_nodes_shared(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
+                       const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s) {
+    const DadtGrid g = dadt_grid(n_nodes, 1, 0);
+    const float scale = static_cast<float>(didt * 1e-7);
+    const auto* dp = reinterpret_cast<const DipolePacked*>(dip_packed);
+    switch (n_sets) {
+        case 1: dadt_shared_kernel<1><<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles); break;
+        case 2: dadt_shared_kernel<2><<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles); break;
+        case 3: dadt_shared_kernel<3><<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles); break;
+        default: fail(kEInval, "between 1 and 3 source sets");
+    }
     count_launch();
 }
 

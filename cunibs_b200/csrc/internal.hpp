@@ -197,6 +197,11 @@ void dadt_elements(const Mesh& m, const float* dadt_nodes, int k, float* dadt_el
 // The general-moment dA/dt on raw device node coordinates (no Mesh), packed records from prep_dipoles.
 void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
                     const double* transforms_dev, int k, double didt, float* out, cudaStream_t s);
+// n_sets (1..3) source sets at common positions, records set * n_dip + j of prep_dipoles all made
+// with the one transform transform_dev; out (n_sets, n_nodes, 3). Set d's field is bitwise
+// dadt_nodes_raw's for that set alone; each pair's geometry is formed once for all sets.
+void dadt_nodes_shared(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
+                       const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s);
 
 // Records the calling thread's message for cunibs_last_error.
 void set_last_error(const std::string& message);

@@ -86,6 +86,26 @@ def test_qfield_exact_and_grid_interpolation_converge_to_the_functional(setup):
     assert errors[1] <= 5e-3 and errors[2] <= 3e-3, errors
 
 
+def test_qfield_directions_from_one_pass_equal_each_direction_alone(setup):
+    """A magnitude target's three Q fields come from one pass over the sources, each pair's
+    geometry shared by the directions; each equals the field of its direction's target alone,
+    bitwise where the two adjoints' node weights are bitwise equal."""
+    subj, coil, _, _, tgt, bary = setup
+    grid = adm.grid_for_placements(subj, coil, [Placement(TOP, HANDLE, DIST)], spacing_mm=4.0, margin_mm=8.0)
+    mag = adm.solve_adjoint(subj, adm.resolve_target(subj, adm.Target(bary[tgt])))
+    assert np.array_equal(mag.target.directions, np.eye(3))
+    w3, q3 = mag.node_weights, adm.sample_qfield(mag, grid).q
+    assert q3.shape == (3, *grid.shape, 3) and np.isfinite(q3).all()
+    for d in range(3):
+        one = adm.solve_adjoint(subj, adm.resolve_target(subj, adm.Target(bary[tgt], np.eye(3)[d])))
+        w1, q1 = one.node_weights, adm.sample_qfield(one, grid).q
+        np.testing.assert_allclose(w1[0], w3[d], rtol=1e-9, atol=1e-12 * np.abs(w3[d]).max())
+        if np.array_equal(w1[0], w3[d]):
+            np.testing.assert_array_equal(q1[0], q3[d])
+        else:
+            np.testing.assert_allclose(q1[0], q3[d], rtol=1e-5, atol=1e-6 * np.abs(q3[d]).max())
+
+
 def test_optimum_matches_a_forward_solve_there(setup):
     subj, coil, res, _, tgt, bary = setup
     T = res["transform"][0]
