@@ -62,57 +62,109 @@ def config_dict(mesh, extra=None):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, sampled from before the warm-up to the end of the
+    comparison arms. Each sample carries nvidia-smi's own timestamp, so the summary holds the
+    samples taken inside the timed region. nvidia-smi starts slowly and a short timed region may
+    hold fewer than three samples; the summary then takes the three nearest to it and reports how
+    far outside the region they lie (slack_ms). Throttle reasons seen anywhere in the sampled
+    window are reported as well."""
 
-    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, device: int) -> None:
+    def __init__(self, device: int, command: str = "nvidia-smi") -> None:
         self.device = device
+        self.command = command
         self.proc = None
         self.lines: list[str] = []
         self.t = None
+        self.region: tuple[float, float] | None = None
 
-    def __enter__(self):
+    def start(self, wait_s: float = 5.0) -> "ClockSampler":
+        """Starts sampling every 100 ms and waits (at most wait_s) for the first sample."""
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                [self.command, "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except (FileNotFoundError, OSError):
             self.proc = None
+            return self
+        import atexit
+
+        atexit.register(self.stop)
+        t_end = time.time() + wait_s
+        while not self.lines and self.proc.poll() is None and time.time() < t_end:
+            time.sleep(0.02)
         return self
 
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def __exit__(self, *exc):
-        if self.proc is not None:
+    def mark(self, t0: float, t1: float) -> None:
+        """The timed region's start and end (time.time())."""
+        self.region = (t0, t1)
+
+    def stop(self) -> None:
+        if self.proc is not None and self.proc.poll() is None:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+            if self.t is not None:
+                self.t.join(timeout=5)
 
-    def summary(self) -> dict:
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 6:
-                continue
+    @staticmethod
+    def _when(stamp: str) -> float | None:
+        import datetime
+
+        for fmt in ("%Y/%m/%d %H:%M:%S.%f", "%Y/%m/%d %H:%M:%S"):
             try:
-                sm.append(float(parts[0]))
-                mx.append(float(parts[1]))
+                return datetime.datetime.strptime(stamp.strip(), fmt).timestamp()
             except ValueError:
                 continue
-            for name, val in zip(names, parts[2:6]):
-                if val.lower() == "active":
-                    reasons.add(name)
+        return None
+
+    def _samples(self) -> list[tuple[float | None, float, float, set]]:
+        out = []
+        for line in list(self.lines):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm, mx = float(parts[1]), float(parts[2])
+            except ValueError:
+                continue
+            reasons = {n for n, v in zip(self.REASONS, parts[3:7]) if v.lower() == "active"}
+            out.append((self._when(parts[0]), sm, mx, reasons))
+        return out
+
+    def summary(self) -> dict:
+        samples = self._samples()
+        window = sorted(set().union(*(r for *_, r in samples))) if samples else []
+        chosen, inside, slack = samples, None, None
+        timed = [x for x in samples if x[0] is not None]
+        if self.region is not None and timed and len(timed) == len(samples):
+            t0, t1 = self.region
+            dist = [max(t0 - x[0], x[0] - t1, 0.0) for x in timed]
+            inside = sum(d == 0.0 for d in dist)
+            order = sorted(range(len(timed)), key=lambda i: dist[i])
+            keep = [i for i in order if dist[i] == 0.0]
+            if len(keep) < 3:
+                keep = order[:3]
+            chosen = [timed[i] for i in keep]
+            slack = round(max(dist[i] for i in keep) * 1e3, 1)
+        sm = [x[1] for x in chosen]
+        mx = [x[2] for x in chosen]
+        reasons = sorted(set().union(*(x[3] for x in chosen))) if chosen else []
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": reasons, "samples": len(chosen), "in_region": inside, "slack_ms": slack,
+                "window_samples": len(samples), "window_reasons": window}
 
 
 def job_throughput(local_ms: float, steps: int, world: int, dist=None, device="cpu") -> tuple[float, float]:
@@ -292,20 +344,22 @@ def run_ours(args) -> dict:
             stages += ctx.stage_times()
         return float(sum(ms)), float(np.mean(its)), stages / n
 
+    clocks = ClockSampler(local).start()
     pipelined(max(3, args.warmup))
     torch.cuda.synchronize()
     launches0 = _native.kernel_launches()
-    with ClockSampler(local) as clocks:
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-        # An NVTX range around the timed steps lets a profiler capture exactly those launches.
-        torch.cuda.nvtx.range_push("timed_steps")
-        total_ms, iters, outers = pipelined(args.steps)
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
-        if dist is not None:
-            dist.barrier()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t_region = time.time()
+    # An NVTX range around the timed steps lets a profiler capture exactly those launches.
+    torch.cuda.nvtx.range_push("timed_steps")
+    total_ms, iters, outers = pipelined(args.steps)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    clocks.mark(t_region, time.time())
+    if dist is not None:
+        dist.barrier()
     launches = _native.kernel_launches() - launches0
     warm_used = d_used.cpu().numpy().tolist()
     warm_rel0 = d_rel0.cpu().numpy().tolist()
@@ -334,6 +388,7 @@ def run_ours(args) -> dict:
     pipelined(2, precision=_native.PREC_PLAIN_FP64, warm=False)
     plain_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
     plain_it = float(d_it.float().mean().item())
+    clocks.stop()
     total_ms, value = job_throughput(total_ms, args.steps, world, dist, dev)
     seq_ms, seq_value = job_throughput(seq_ms, n_cmp, world, dist, dev)
     cold_ms, cold_value = job_throughput(cold_ms, n_cmp, world, dist, dev)
