@@ -1,5 +1,7 @@
-"""A small read-only HDF5 reader for the files the reference's coil library holds (h5py-written,
-default "earliest" format), so that its bundled ``.h5`` coils load where h5py is not installed.
+"""A small read-only HDF5 reader for files in h5py's default ("earliest") format: the reference's
+bundled ``.h5`` coils and its ``.h5`` field results load where h5py is not installed.
+``read_dataset`` reads one dataset of the root group; ``read_tree`` reads the whole file (groups,
+their attributes, numeric datasets).
 
 Written from the HDF5 File Format Specification (version 0 superblock), covering what such files
 use: a version-0 superblock with 8-byte offsets and lengths; groups as symbol tables (version-1
@@ -255,14 +257,46 @@ class _File:
         return out
 
 
-def read_dataset(path: str | Path, name: str) -> tuple[np.ndarray, dict]:
-    """The dataset ``name`` of the root group of an HDF5 file and its attributes."""
+    def group(self, header: int, depth: int = 0) -> dict:
+        """A group's attributes, datasets (array, attributes) and subgroups, read recursively."""
+        if depth > 32:
+            raise ValueError("HDF5: groups nested deeper than 32 levels")
+        table, attrs = None, {}
+        for mtype, off, _size in self.messages(header):
+            if mtype == 0x11:
+                table = self.u("QQ", off)
+            elif mtype == 0x0C:
+                k, v = self.attribute(off)
+                attrs[k] = v
+        if table is None:
+            raise ValueError("HDF5: a group object header without a symbol table message")
+        out = {"attrs": attrs, "datasets": {}, "groups": {}}
+        for name, child in self.group_entries(*table).items():
+            if any(mtype == 0x11 for mtype, _, _ in self.messages(child)):
+                out["groups"][name] = self.group(child, depth + 1)
+            else:
+                out["datasets"][name] = self.dataset(child)
+        return out
+
+
+def _open(path: str | Path) -> _File:
     f = _File(Path(path).read_bytes())
     f.sig(0, _SIGNATURE)
     if f.d[8] != 0:
         raise ValueError(f"HDF5: superblock version {f.d[8]} (only version 0 is handled)")
     if f.d[13] != 8 or f.d[14] != 8:
         raise ValueError("HDF5: only 8-byte offsets and lengths are handled")
+    return f
+
+
+def is_hdf5(path: str | Path) -> bool:
+    with open(path, "rb") as fh:
+        return fh.read(len(_SIGNATURE)) == _SIGNATURE
+
+
+def read_dataset(path: str | Path, name: str) -> tuple[np.ndarray, dict]:
+    """The dataset ``name`` of the root group of an HDF5 file and its attributes."""
+    f = _open(path)
     root_cache = f.u("I", 56 + 16)[0]
     if root_cache != 1:
         raise ValueError("HDF5: the root group has no cached symbol table")
@@ -271,3 +305,10 @@ def read_dataset(path: str | Path, name: str) -> tuple[np.ndarray, dict]:
     if name not in entries:
         raise KeyError(f"{path}: no dataset {name!r} in the root group (has {sorted(entries)})")
     return f.dataset(entries[name])
+
+
+def read_tree(path: str | Path) -> dict:
+    """The whole file from the root group: ``{"attrs": {...}, "datasets": {name: (array, attrs)},
+    "groups": {name: <the same for the subgroup>}}``."""
+    f = _open(path)
+    return f.group(f.u("Q", 56 + 8)[0])

@@ -555,6 +555,13 @@ class FieldResult:
 
     @classmethod
     def load(cls, path: str | Path) -> FieldResult:
+        """Read a result saved by :meth:`save` (``.npz``), or an HDF5 result file in the reference's
+        layout (simulation.py:805-870: datasets and attributes of the root group, the metrics in a
+        ``summary`` group), recognised by its signature."""
+        from . import h5lite
+
+        if h5lite.is_hdf5(path):
+            return cls._load_hdf5(path, _hdf5_tree(path))
         with np.load(Path(path), allow_pickle=False) as z:
             if int(z["format_version"]) != _FORMAT_VERSION:
                 raise ValueError(f"{path}: file format version {int(z['format_version'])} is not readable (expected {_FORMAT_VERSION}).")
@@ -575,3 +582,64 @@ class FieldResult:
                        iterations=int(z["iterations"]), relative_residual=float(z["relative_residual"]),
                        n_nodes=int(z["n_nodes"]) if "n_nodes" in z.files else None, E_slots=opt("E_slots"),
                        slot_node=opt("slot_node"), slot_tag=opt("slot_tag"), tet_nodes=opt("tet_nodes"))
+
+    @classmethod
+    def _load_hdf5(cls, path, tree: dict) -> FieldResult:
+        """The reference's HDF5 layout (simulation.py:839-870, _read_metrics 68-77) as a tree of
+        ``{"attrs", "datasets", "groups"}`` dictionaries."""
+        attrs, data = tree["attrs"], tree["datasets"]
+        stored = int(attrs.get("format_version", 0))
+        if stored != _FORMAT_VERSION:
+            raise ValueError(f"{path}: file format version {stored} is not readable (expected {_FORMAT_VERSION}).")
+        opt = lambda k: np.asarray(data[k][0]) if k in data else None  # noqa: E731
+        grp = tree["groups"]["summary"]
+        summary: metrics.FieldMetrics = {
+            "region": str(grp["attrs"]["region"]),
+            "peak_magnE": float(grp["attrs"]["peak_magnE"]),
+            "peak_location_mm": np.asarray(grp["datasets"]["peak_location_mm"][0]),
+            "center_of_gravity_mm": np.asarray(grp["datasets"]["center_of_gravity_mm"][0]),
+            "region_volume_m3": float(grp["attrs"]["region_volume_m3"]),
+            "focality_m3": {str(k): float(v) for k, v in grp["groups"]["focality_m3"]["attrs"].items()},
+            "distribution": {str(k): float(v) for k, v in grp["groups"]["distribution"]["attrs"].items()},
+        }
+        return cls(summary=summary, magnE=opt("magnE"), E=opt("E"), v=opt("v"), transform=np.asarray(data["transform"][0]),
+                   placement=Placement(np.asarray(attrs["placement_center_mm"], np.float64),
+                                       np.asarray(attrs["placement_handle_mm"], np.float64),
+                                       float(attrs["placement_distance_mm"])),
+                   coil_name=str(attrs["coil_name"]), didt=float(attrs["didt"]), vols=opt("vols"),
+                   tet_tags=opt("tet_tags"), barycenters_mm=opt("barycenters_mm"),
+                   recovery=str(attrs.get("recovery", "raw")),
+                   n_nodes=int(attrs["n_nodes"]) if "n_nodes" in attrs else None, E_slots=opt("E_slots"),
+                   slot_node=opt("slot_node"), slot_tag=opt("slot_tag"), tet_nodes=opt("tet_nodes"))
+
+
+def _hdf5_tree(path) -> dict:
+    """An HDF5 file as nested ``{"attrs", "datasets": {name: (array, attrs)}, "groups"}``
+    dictionaries: through h5py where it is installed, else through the built-in reader (files in
+    h5py's default format)."""
+    try:
+        import h5py
+    except ImportError:
+        from . import h5lite
+
+        return h5lite.read_tree(path)
+
+    def walk(g) -> dict:
+        out = {"attrs": {k: _h5_value(v) for k, v in g.attrs.items()}, "datasets": {}, "groups": {}}
+        for name, obj in g.items():
+            if isinstance(obj, h5py.Group):
+                out["groups"][name] = walk(obj)
+            else:
+                out["datasets"][name] = (np.asarray(obj), {k: _h5_value(v) for k, v in obj.attrs.items()})
+        return out
+
+    with h5py.File(path, "r") as f:
+        return walk(f)
+
+
+def _h5_value(v):
+    if isinstance(v, bytes):
+        return v.decode()
+    if isinstance(v, np.ndarray) and v.shape == ():
+        return v.item()
+    return v

@@ -41,3 +41,85 @@ def test_h5lite_rejects_other_files(tmp_path):
     bad.write_bytes(b"not an hdf5 file at all")
     with pytest.raises(ValueError, match="HDF5"):
         read_dataset(bad, "dipoles")
+
+
+@pytest.mark.skipif(not COILS.is_dir(), reason="the reference's coil library is not mounted")
+def test_tree_reader_agrees_with_the_dataset_reader_on_every_coil():
+    from cunibs_b200 import h5lite
+
+    for f in sorted(COILS.glob("*.h5")):
+        assert h5lite.is_hdf5(f)
+        tree = h5lite.read_tree(f)
+        a, attrs = h5lite.read_dataset(f, "dipoles")
+        b, battrs = tree["datasets"]["dipoles"]
+        np.testing.assert_array_equal(a, b)
+        assert attrs == battrs and tree["groups"] == {}
+
+
+def _result():
+    from cunibs_b200 import Placement
+    from cunibs_b200.simulation import FieldResult
+
+    rng = np.random.default_rng(5)
+    summary = {"region": "gray_matter", "peak_magnE": 101.5, "peak_location_mm": np.array([1.0, 2.0, 80.0]),
+               "center_of_gravity_mm": np.array([0.5, 1.5, 78.0]), "region_volume_m3": 3.2e-4,
+               "focality_m3": {"50": 1.1e-6, "75": 4.0e-7}, "distribution": {"p50": 20.0, "p99": 90.0}}
+    return FieldResult(summary=summary, magnE=rng.random(40, dtype=np.float32), E=None, v=rng.random(12),
+                       transform=np.eye(4), placement=Placement([0.0, 0.0, 90.0], [0.0, 50.0, 90.0], 4.0),
+                       coil_name="D70", didt=1e6, vols=rng.random(40, dtype=np.float32),
+                       tet_tags=np.full(40, 2, np.int32), barycenters_mm=rng.random((40, 3)), recovery="harmonic",
+                       n_nodes=12, E_slots=rng.random((12, 3), dtype=np.float32), slot_node=np.arange(12, dtype=np.int32))
+
+
+def _reference_layout(r) -> dict:
+    """The tree the reference's FieldResult.save writes (simulation.py:805-837, _write_metrics 56-65)."""
+    data = {k: (getattr(r, k), {}) for k in ("magnE", "E", "v", "vols", "tet_tags", "barycenters_mm", "E_slots",
+                                              "slot_node", "slot_tag", "tet_nodes") if getattr(r, k) is not None}
+    data["transform"] = (r.transform, {})
+    s = r.summary
+    summary = {"attrs": {"region": s["region"], "peak_magnE": s["peak_magnE"], "region_volume_m3": s["region_volume_m3"]},
+               "datasets": {"peak_location_mm": (s["peak_location_mm"], {}),
+                            "center_of_gravity_mm": (s["center_of_gravity_mm"], {})},
+               "groups": {"focality_m3": {"attrs": dict(s["focality_m3"]), "datasets": {}, "groups": {}},
+                          "distribution": {"attrs": dict(s["distribution"]), "datasets": {}, "groups": {}}}}
+    attrs = {"format_version": 1, "recovery": r.recovery, "n_nodes": r.n_nodes, "coil_name": r.coil_name,
+             "didt": r.didt, "placement_center_mm": r.placement.center_mm, "placement_handle_mm": r.placement.handle_mm,
+             "placement_distance_mm": r.placement.distance_mm}
+    return {"attrs": attrs, "datasets": data, "groups": {"summary": summary}}
+
+
+def test_field_result_loads_the_reference_hdf5_layout(tmp_path, monkeypatch):
+    from cunibs_b200 import simulation
+
+    r = _result()
+    tree = _reference_layout(r)
+    f = tmp_path / "result.h5"
+    f.write_bytes(b"\x89HDF\r\n\x1a\n" + bytes(64))  # the signature routes load() to the HDF5 reader
+    monkeypatch.setattr(simulation, "_hdf5_tree", lambda path: tree)
+    got = simulation.FieldResult.load(f)
+    for k in ("magnE", "v", "vols", "tet_tags", "barycenters_mm", "E_slots", "slot_node", "transform"):
+        np.testing.assert_array_equal(getattr(got, k), getattr(r, k))
+    assert got.E is None and got.slot_tag is None and got.tet_nodes is None
+    assert (got.coil_name, got.didt, got.recovery, got.n_nodes) == ("D70", 1e6, "harmonic", 12)
+    np.testing.assert_array_equal(got.placement.center_mm, r.placement.center_mm)
+    assert got.placement.distance_mm == 4.0
+    assert got.summary["region"] == "gray_matter" and got.summary["focality_m3"] == r.summary["focality_m3"]
+    assert got.summary["distribution"] == r.summary["distribution"]
+    np.testing.assert_array_equal(got.summary["peak_location_mm"], r.summary["peak_location_mm"])
+    # The same result through the .npz path matches too.
+    r.save(tmp_path / "result.npz")
+    back = simulation.FieldResult.load(tmp_path / "result.npz")
+    np.testing.assert_array_equal(back.magnE, got.magnE)
+    assert back.summary["peak_magnE"] == got.summary["peak_magnE"]
+
+
+def test_field_result_hdf5_version_is_checked(tmp_path, monkeypatch):
+    from cunibs_b200 import simulation
+
+    tree = _reference_layout(_result())
+    tree["attrs"]["format_version"] = 2
+    f = tmp_path / "result.h5"
+    f.write_bytes(b"\x89HDF\r\n\x1a\n" + bytes(64))
+    monkeypatch.setattr(simulation, "_hdf5_tree", lambda path: tree)
+    with pytest.raises(ValueError, match="format version 2"):
+        simulation.FieldResult.load(f)
