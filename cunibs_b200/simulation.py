@@ -592,16 +592,7 @@ class FieldResult:
         if stored != _FORMAT_VERSION:
             raise ValueError(f"{path}: file format version {stored} is not readable (expected {_FORMAT_VERSION}).")
         opt = lambda k: np.asarray(data[k][0]) if k in data else None  # noqa: E731
-        grp = tree["groups"]["summary"]
-        summary: metrics.FieldMetrics = {
-            "region": str(grp["attrs"]["region"]),
-            "peak_magnE": float(grp["attrs"]["peak_magnE"]),
-            "peak_location_mm": np.asarray(grp["datasets"]["peak_location_mm"][0]),
-            "center_of_gravity_mm": np.asarray(grp["datasets"]["center_of_gravity_mm"][0]),
-            "region_volume_m3": float(grp["attrs"]["region_volume_m3"]),
-            "focality_m3": {str(k): float(v) for k, v in grp["groups"]["focality_m3"]["attrs"].items()},
-            "distribution": {str(k): float(v) for k, v in grp["groups"]["distribution"]["attrs"].items()},
-        }
+        summary = _metrics_from_tree(tree["groups"]["summary"])
         return cls(summary=summary, magnE=opt("magnE"), E=opt("E"), v=opt("v"), transform=np.asarray(data["transform"][0]),
                    placement=Placement(np.asarray(attrs["placement_center_mm"], np.float64),
                                        np.asarray(attrs["placement_handle_mm"], np.float64),
@@ -611,6 +602,19 @@ class FieldResult:
                    recovery=str(attrs.get("recovery", "raw")),
                    n_nodes=int(attrs["n_nodes"]) if "n_nodes" in attrs else None, E_slots=opt("E_slots"),
                    slot_node=opt("slot_node"), slot_tag=opt("slot_tag"), tet_nodes=opt("tet_nodes"))
+
+
+def _metrics_from_tree(grp: dict) -> metrics.FieldMetrics:
+    """FieldMetrics from a group in the reference's metrics layout (simulation.py:56-77)."""
+    return {
+        "region": str(grp["attrs"]["region"]),
+        "peak_magnE": float(grp["attrs"]["peak_magnE"]),
+        "peak_location_mm": np.asarray(grp["datasets"]["peak_location_mm"][0]),
+        "center_of_gravity_mm": np.asarray(grp["datasets"]["center_of_gravity_mm"][0]),
+        "region_volume_m3": float(grp["attrs"]["region_volume_m3"]),
+        "focality_m3": {str(k): float(v) for k, v in grp["groups"]["focality_m3"]["attrs"].items()},
+        "distribution": {str(k): float(v) for k, v in grp["groups"]["distribution"]["attrs"].items()},
+    }
 
 
 def _hdf5_tree(path) -> dict:

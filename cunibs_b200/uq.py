@@ -176,8 +176,13 @@ class ConductivityUQResult:
 
     @classmethod
     def load(cls, path: str | Path) -> ConductivityUQResult:
-        from .simulation import Placement
+        """Read a result saved by :meth:`save` (``.npz``), or an HDF5 result file in the reference's
+        layout (result.py:182-262), recognised by its signature."""
+        from . import h5lite
+        from .simulation import Placement, _hdf5_tree
 
+        if h5lite.is_hdf5(path):
+            return cls._load_hdf5(path, _hdf5_tree(path))
         with np.load(Path(path), allow_pickle=False) as z:
             if int(z["format_version"]) != _FORMAT_VERSION:
                 raise ValueError(f"{path}: file format version {int(z['format_version'])} is not readable.")
@@ -199,6 +204,36 @@ class ConductivityUQResult:
         if res.mean_magnE is not None:
             res.summary = res.compute_summary()
         return res
+
+    @classmethod
+    def _load_hdf5(cls, path, tree: dict) -> ConductivityUQResult:
+        """The reference's HDF5 layout (result.py:193-262) as a tree of ``{"attrs", "datasets",
+        "groups"}`` dictionaries. Its files hold no per-draw iteration counts: those load as -1."""
+        from .simulation import Placement, _metrics_from_tree
+
+        attrs, data, groups = tree["attrs"], tree["datasets"], tree["groups"]
+        stored = int(attrs.get("format_version", 0))
+        if stored != _FORMAT_VERSION:
+            raise ValueError(f"{path}: file format version {stored} is not readable (expected {_FORMAT_VERSION}).")
+        opt = lambda k: np.asarray(data[k][0]) if k in data else None  # noqa: E731
+        n = int(attrs["n_samples"])
+        summary = groups["summary"]
+        roi = groups.get("roi_samples", {"datasets": {}})["datasets"]
+        return cls(
+            mean_magnE=opt("mean_magnE"), std_magnE=opt("std_magnE"), cov_magnE=opt("cov_magnE"), n_samples=n,
+            perturbed_tags=tuple(int(t) for t in np.atleast_1d(attrs["perturbed_tags"])),
+            sigma_samples=np.asarray(data["sigma_samples"][0]), vols=opt("vols"), tet_tags=opt("tet_tags"),
+            barycenters_mm=opt("barycenters_mm"),
+            placement=Placement(np.asarray(attrs["placement_center_mm"], np.float64),
+                                np.asarray(attrs["placement_handle_mm"], np.float64),
+                                float(attrs["placement_distance_mm"])),
+            coil_name=str(attrs["coil_name"]), didt=float(attrs["didt"]),
+            peak_samples=np.asarray(data["peak_samples"][0]), focality_samples=np.asarray(data["focality_samples"][0]),
+            peak_location_samples=np.asarray(data["peak_location_samples"][0]),
+            iteration_samples=np.full(n, -1, np.int32), recovery=str(attrs.get("recovery", "raw")),
+            summary=ConductivityUQSummary(mean_field=_metrics_from_tree(summary["groups"]["mean_field"]),
+                                          max_local_cov=float(summary["attrs"]["max_local_cov"])),
+            roi_samples={str(k): np.asarray(v[0]) for k, v in roi.items()})
 
 
 def nominal_sigma_table() -> np.ndarray:

@@ -123,3 +123,37 @@ def test_field_result_hdf5_version_is_checked(tmp_path, monkeypatch):
     monkeypatch.setattr(simulation, "_hdf5_tree", lambda path: tree)
     with pytest.raises(ValueError, match="format version 2"):
         simulation.FieldResult.load(f)
+
+
+def test_conductivity_result_loads_the_reference_hdf5_layout(tmp_path, monkeypatch):
+    from cunibs_b200 import simulation
+    from cunibs_b200.uq import ConductivityUQResult
+
+    rng = np.random.default_rng(9)
+    n, m = 16, 40
+    metrics_grp = _reference_layout(_result())["groups"]["summary"]
+    tree = {
+        "attrs": {"format_version": 1, "recovery": "harmonic", "n_samples": n,
+                  "perturbed_tags": np.array([1, 2, 3], np.int32), "coil_name": "D70", "didt": 1e6,
+                  "placement_center_mm": np.array([0.0, 0.0, 90.0]), "placement_handle_mm": np.array([0.0, 50.0, 90.0]),
+                  "placement_distance_mm": 4.0},
+        "datasets": {"mean_magnE": (rng.random(m), {}), "std_magnE": (rng.random(m), {}), "cov_magnE": (rng.random(m), {}),
+                     "vols": (rng.random(m), {}), "tet_tags": (np.full(m, 2, np.int32), {}),
+                     "barycenters_mm": (rng.random((m, 3)), {}), "sigma_samples": (rng.random((n, 3)), {}),
+                     "peak_samples": (rng.random(n), {}), "focality_samples": (rng.random(n), {}),
+                     "peak_location_samples": (rng.random((n, 3)), {})},
+        "groups": {"summary": {"attrs": {"max_local_cov": 0.31}, "datasets": {}, "groups": {"mean_field": metrics_grp}},
+                   "roi_samples": {"attrs": {}, "datasets": {"m1": (rng.random(n), {})}, "groups": {}}},
+    }
+    f = tmp_path / "uq.h5"
+    f.write_bytes(b"\x89HDF\r\n\x1a\n" + bytes(64))
+    monkeypatch.setattr(simulation, "_hdf5_tree", lambda path: tree)
+    got = ConductivityUQResult.load(f)
+    assert got.n_samples == n and got.perturbed_tags == (1, 2, 3) and got.recovery == "harmonic"
+    for k in ("mean_magnE", "std_magnE", "cov_magnE", "vols", "tet_tags", "barycenters_mm", "sigma_samples",
+              "peak_samples", "focality_samples", "peak_location_samples"):
+        np.testing.assert_array_equal(getattr(got, k), tree["datasets"][k][0])
+    np.testing.assert_array_equal(got.roi_samples["m1"], tree["groups"]["roi_samples"]["datasets"]["m1"][0])
+    assert got.summary.max_local_cov == 0.31 and got.summary.mean_field["region"] == "gray_matter"
+    assert (got.iteration_samples == -1).all() and got.iteration_samples.shape == (n,)
+    assert set(got.tissue_sensitivity("m1")) == {1, 2, 3}
