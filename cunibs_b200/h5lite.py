@@ -294,6 +294,21 @@ def is_hdf5(path: str | Path) -> bool:
         return fh.read(len(_SIGNATURE)) == _SIGNATURE
 
 
+def _malformed(fn):
+    """Reads past the end of the file, or zlib errors, surface as ValueError naming the file."""
+    import functools
+
+    @functools.wraps(fn)
+    def wrapper(path, *args):
+        try:
+            return fn(path, *args)
+        except (struct.error, IndexError, zlib.error) as exc:
+            raise ValueError(f"HDF5: {path} is truncated or malformed ({exc})") from exc
+
+    return wrapper
+
+
+@_malformed
 def read_dataset(path: str | Path, name: str) -> tuple[np.ndarray, dict]:
     """The dataset ``name`` of the root group of an HDF5 file and its attributes."""
     f = _open(path)
@@ -307,6 +322,7 @@ def read_dataset(path: str | Path, name: str) -> tuple[np.ndarray, dict]:
     return f.dataset(entries[name])
 
 
+@_malformed
 def read_tree(path: str | Path) -> dict:
     """The whole file from the root group: ``{"attrs": {...}, "datasets": {name: (array, attrs)},
     "groups": {name: <the same for the subgroup>}}``."""

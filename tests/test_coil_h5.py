@@ -157,3 +157,16 @@ def test_conductivity_result_loads_the_reference_hdf5_layout(tmp_path, monkeypat
     assert got.summary.max_local_cov == 0.31 and got.summary.mean_field["region"] == "gray_matter"
     assert (got.iteration_samples == -1).all() and got.iteration_samples.shape == (n,)
     assert set(got.tissue_sensitivity("m1")) == {1, 2, 3}
+
+
+@pytest.mark.skipif(not COILS.is_dir(), reason="the reference's coil library is not mounted")
+def test_truncated_files_raise_value_errors(tmp_path):
+    from cunibs_b200 import h5lite
+
+    data = (COILS / "MagStim_D70.h5").read_bytes()
+    for n in (100, 900, 2000, 5000, len(data) - 64):
+        p = tmp_path / f"cut{n}.h5"
+        p.write_bytes(data[:n])
+        for read in (lambda: h5lite.read_tree(p), lambda: h5lite.read_dataset(p, "dipoles")):
+            with pytest.raises(ValueError, match="HDF5"):
+                read()
