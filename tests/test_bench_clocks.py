@@ -55,7 +55,7 @@ def test_short_region_takes_the_nearest_three(tmp_path):
     c.stop()
     s = c.summary()
     assert s["samples"] == 3 and s["in_region"] <= 1
-    assert 0.0 < s["slack_ms"] < 200.0
+    assert 0.0 < s["slack_ms"] < 1000.0  # about 50-100 ms; loose for a loaded host
     assert s["reasons"] == ["sw_power_cap"] and s["window_reasons"] == ["sw_power_cap"]
 
 
