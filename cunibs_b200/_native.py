@@ -53,6 +53,7 @@ class Info(C.Structure):
         ("coarse_rows", C.c_int),
         ("vcycle_levels", C.c_int),
         ("bottom_rows", C.c_int),
+        ("hierarchy_builds", C.c_int),
     ]
 
 
@@ -172,6 +173,8 @@ def load() -> C.CDLL:
         "cunibs_context_set_warmstart": ([_vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp], C.c_int),
         "cunibs_gemm_bf16": ([_vp, C.c_int, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp, C.c_int, C.c_int, _vp,
                               _vp, C.c_int, _vp, C.c_int, _vp], C.c_int),
+        "cunibs_gemm_status": ([_vp, C.POINTER(C.c_int)], C.c_int),
+        "cunibs_debug_gemm_waits": ([C.c_longlong, C.c_longlong, C.c_int], C.c_int),
         "cunibs_mlp_colsum": ([_vp, C.c_int, C.c_int, C.c_int, _vp, _vp], C.c_int),
         "cunibs_mlp_mse": ([_vp, _vp, C.c_int, C.c_int, C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp], C.c_int),
         "cunibs_mlp_adam": ([_vp, _vp, _vp, _vp, C.c_longlong, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
@@ -269,6 +272,13 @@ class Context:
         self.coarse_rows = info.coarse_rows
         self.vcycle_levels = info.vcycle_levels
         self.bottom_rows = info.bottom_rows
+
+    @property
+    def hierarchy_builds(self) -> int:
+        """AMG hierarchy builds over the context's life (1 at create; each rebuild adds one)."""
+        info = Info()
+        check(self._lib.cunibs_context_info(self.handle, C.byref(info)))
+        return int(info.hierarchy_builds)
 
     def close(self) -> None:
         # Handles that live on this context (auxiliary-dipole-method state) go first.

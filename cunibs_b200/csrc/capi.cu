@@ -171,7 +171,11 @@ struct cunibs_context {
         CUNIBS_CHECK(cudaStreamSynchronize(stream));
     }
 
+    // Hierarchy builds over the context's life (the first at create); cunibs_context_info reports it.
+    int hierarchy_builds = 0;
+
     void rebuild_hierarchy() {
+        ++hierarchy_builds;
         solver.reset();
         DevCsr<double> a0;
         reduce_grounded(mesh, a0, stream);
@@ -380,12 +384,16 @@ PendingBlock finish_block(cunibs_context* c, long long ticket, SolveStats& st, b
             c->warm_used[i] = st.col_init_rel[i] < 1.0 ? 1 : 0;
         }
     }
-    // Columns that missed tolerance: one FP64 retry from their current iterate, then an error
-    // (the rebuild-then-retry contract of fem/solve.py:528-551).
+    // Columns that missed tolerance: the hierarchy is rebuilt at the operator's current values (a
+    // V-cycle kept from other conductivities may be what failed), then one FP64 retry from their
+    // current iterate, then an error (the rebuild-then-retry contract of fem/solve.py:528-551).
+    // Inside a conductivity study the mesh's assembled values are the nominal ones, not the draw's,
+    // so the draw's own failure path (cunibs_sigma_draw) does its rebuild instead.
     std::vector<int> missed;
     for (int i = 0; i < k; ++i)
         if (!(st.col_rel[i] <= prm.tolerance)) missed.push_back(i);
     if (!missed.empty()) {
+        if (!c->study) c->rebuild_hierarchy();
         Params retry = prm;
         retry.precision = kPlainFp64;
         SolveStats st2;
@@ -611,6 +619,7 @@ int cunibs_context_info(const cunibs_context* c, cunibs_info* out) {
         out->coarse_rows = c->hier.nc;
         out->vcycle_levels = c->hier.vcycle_levels;
         out->bottom_rows = c->hier.bottom_n;
+        out->hierarchy_builds = c->hierarchy_builds;
     });
 }
 

@@ -31,7 +31,10 @@ constexpr int BM = 128;
 constexpr int BK = 64;  // one 128-byte swizzle atom of BF16 per row
 constexpr int STAGES = 4;
 constexpr int kThreads = 192;
-constexpr long kSpinLimit = 1L << 24;
+// Every mbarrier wait gives up after this many polls or this much %globaltimer time, whichever
+// comes first (a stage's loads land within microseconds; these only bound a failure).
+constexpr long long kSpinLimit = 1LL << 24;
+constexpr unsigned long long kWaitLimitNs = 2000000000ULL;
 
 __device__ __forceinline__ std::uint32_t smem_u32(const void* p) {
     return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
@@ -55,10 +58,21 @@ __device__ __forceinline__ bool mbar_try_wait(std::uint64_t* bar, std::uint32_t 
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, std::uint32_t parity) {
-    for (long i = 0; i < kSpinLimit; ++i)
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity to complete: at most `polls` polls and at most
+// `limit_ns` of global time.
+__device__ __forceinline__ bool mbar_wait(std::uint64_t* bar, std::uint32_t parity, long long polls,
+                                          unsigned long long limit_ns) {
+    const unsigned long long t0 = global_ns();
+    for (long long i = 0; i < polls; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 255) == 255 && global_ns() - t0 > limit_ns) return false;
+    }
     return false;
 }
 
@@ -171,9 +185,11 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     if (warp == 4 && lane == 0) {
         // Producer.
-        for (int kb = 0; kb < num_kb; ++kb) {
+        // ep.withhold_loads (a test of the timeout path) issues no loads: the MMA warp's first wait
+        // can then only run out.
+        for (int kb = 0; kb < num_kb && !ep.withhold_loads; ++kb) {
             const int s = kb % STAGES;
-            if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1)) {
+            if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) & 1) ^ 1, ep.wait_polls, ep.wait_ns)) {
                 *abort_flag = 1;
                 break;
             }
@@ -188,7 +204,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         bool ok = true;
         for (int kb = 0; kb < num_kb && ok; ++kb) {
             const int s = kb % STAGES;
-            if (!mbar_wait(&full[s], (kb / STAGES) & 1)) {
+            if (!mbar_wait(&full[s], (kb / STAGES) & 1, ep.wait_polls, ep.wait_ns)) {
                 ok = false;
                 break;
             }
@@ -204,7 +220,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         umma_commit(accum);  // arrives once every MMA issued above has completed
     } else if (warp < 4) {
         // Epilogue: thread (warp, lane) owns output row m0 + 32 warp + lane.
-        const bool ready = mbar_wait(accum, 0);
+        const bool ready = mbar_wait(accum, 0, ep.wait_polls, ep.wait_ns);
         tc_fence_after();
         const int row = m0 + warp * 32 + lane;
         if (ready) {
@@ -322,17 +338,68 @@ void launch(const GemmProblem& p, cudaStream_t s) {
     CUNIBS_LAUNCH_CHECK("gemm_bf16");
 }
 
+// The wait bounds every launch gets (cunibs_debug_gemm_waits changes them for tests of the
+// timeout path), and the per-device word that launches without an error flag of their own report
+// an expired wait to (read and cleared by gemm_status).
+std::atomic<long long> g_wait_polls{kSpinLimit};
+std::atomic<unsigned long long> g_wait_ns{kWaitLimitNs};
+std::atomic<int> g_withhold{0};
+constexpr int kMaxDevices = 64;
+std::mutex g_status_mu;
+int* g_status[kMaxDevices] = {};
+
+int* status_word(int dev) {
+    if (dev < 0 || dev >= kMaxDevices) fail(kEInval, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_status_mu);
+    if (!g_status[dev]) {
+        int* p = nullptr;
+        CUNIBS_CHECK(cudaMalloc(&p, sizeof(int)));
+        CUNIBS_CHECK(cudaMemset(p, 0, sizeof(int)));
+        g_status[dev] = p;
+    }
+    return g_status[dev];
+}
+
 }  // namespace
 
-void gemm_bf16(const GemmProblem& p, cudaStream_t s) {
-    if (p.M <= 0 || p.N <= 0 || p.K <= 0) fail(kEInval, "GEMM sizes must be positive");
-    if (p.K % 8 != 0) fail(kEInval, "GEMM K must be a multiple of 8");
-    if (p.ep.out16t && p.ep.ld_t < p.M) fail(kEInval, "transposed output leading dimension is below M");
+void gemm_bf16(const GemmProblem& p_in, cudaStream_t s) {
+    if (p_in.M <= 0 || p_in.N <= 0 || p_in.K <= 0) fail(kEInval, "GEMM sizes must be positive");
+    if (p_in.K % 8 != 0) fail(kEInval, "GEMM K must be a multiple of 8");
+    if (p_in.ep.out16t && p_in.ep.ld_t < p_in.M) fail(kEInval, "transposed output leading dimension is below M");
+    GemmProblem p = p_in;
+    p.ep.wait_polls = g_wait_polls.load(std::memory_order_relaxed);
+    p.ep.wait_ns = g_wait_ns.load(std::memory_order_relaxed);
+    p.ep.withhold_loads = g_withhold.load(std::memory_order_relaxed);
+    if (!p.ep.error) {
+        int dev = 0;
+        CUNIBS_CHECK(cudaGetDevice(&dev));
+        p.ep.error = status_word(dev);
+    }
     // One row of tiles (M <= 128, the warm start's network at inference) is latency-bound: 32-wide
     // tiles give 4x the CTAs and smaller stages (measured 20.5 -> 10.4 us for 16 x 512 x 512).
     if (p.N <= 16) launch<16>(p, s);
     else if (p.N <= 32 || p.M <= BM) launch<32>(p, s);
     else launch<128>(p, s);
+}
+
+bool gemm_status(cudaStream_t s) {
+    int dev = 0;
+    CUNIBS_CHECK(cudaGetDevice(&dev));
+    int* w = status_word(dev);
+    int h = 0;
+    CUNIBS_CHECK(cudaMemcpyAsync(&h, w, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUNIBS_CHECK(cudaStreamSynchronize(s));
+    if (h) {
+        CUNIBS_CHECK(cudaMemsetAsync(w, 0, sizeof(int), s));
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+    }
+    return h != 0;
+}
+
+void gemm_set_waits(long long polls, unsigned long long limit_ns, int withhold_loads) {
+    g_wait_polls.store(polls > 0 ? polls : kSpinLimit, std::memory_order_relaxed);
+    g_wait_ns.store(limit_ns > 0 ? limit_ns : kWaitLimitNs, std::memory_order_relaxed);
+    g_withhold.store(withhold_loads ? 1 : 0, std::memory_order_relaxed);
 }
 
 }  // namespace cunibs

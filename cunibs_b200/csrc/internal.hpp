@@ -239,7 +239,11 @@ struct GemmEpilogue {
     int ld_out = 0;
     __nv_bfloat16* out16t = nullptr;
     int ld_t = 0;
-    int* error = nullptr;  // set to 1 when a bounded wait expired
+    int* error = nullptr;  // set to 1 when a bounded wait expired (NULL: the device's status word)
+    // Filled by gemm_bf16 from the library's wait settings.
+    long long wait_polls = 0;
+    unsigned long long wait_ns = 0;
+    int withhold_loads = 0;
 };
 struct GemmProblem {
     const __nv_bfloat16* a = nullptr;  // [M, lda], K-major
@@ -250,6 +254,12 @@ struct GemmProblem {
     GemmEpilogue ep;
 };
 void gemm_bf16(const GemmProblem& p, cudaStream_t s);
+// Whether a GEMM launched without an error flag of its own had a wait expire on the current device
+// since the last call (synchronises `s`, then clears the word).
+bool gemm_status(cudaStream_t s);
+// Wait bounds of later GEMM launches (<= 0: the defaults); withhold_loads makes the producer issue
+// no loads, for tests of the timeout path.
+void gemm_set_waits(long long polls, unsigned long long limit_ns, int withhold_loads);
 
 // Learned warm start (warmstart.cu): an MLP from coil pose to the coefficients of a reduced basis of
 // the grounded potential, prolongated through the basis as the PCG initial guess.

@@ -392,6 +392,20 @@ int cunibs_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int 
     });
 }
 
+int cunibs_gemm_status(void* stream, int* expired) {
+    return guarded_call([&] {
+        const bool e = gemm_status(static_cast<cudaStream_t>(stream));
+        if (expired) *expired = e ? 1 : 0;
+        if (e) fail(kETimeout, "a bounded mbarrier wait of a tensor-core GEMM expired; its outputs are invalid");
+    });
+}
+
+int cunibs_debug_gemm_waits(long long max_polls, long long max_ns, int withhold_loads) {
+    return guarded_call([&] {
+        gemm_set_waits(max_polls, max_ns > 0 ? static_cast<unsigned long long>(max_ns) : 0ULL, withhold_loads);
+    });
+}
+
 int cunibs_mlp_colsum(const float* x, int rows, int cols, int ld, float* out, void* stream) {
     return guarded_call([&] {
         if (!x || !out || rows < 1 || cols < 1 || ld < cols) fail(kEInval, "bad colsum arguments");

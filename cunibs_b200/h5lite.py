@@ -44,8 +44,13 @@ class _File:
         end = self.d.index(b"\x00", start)
         return self.d[start:end].decode()
 
-    def group_entries(self, btree: int, heap: int) -> dict[str, int]:
-        """name -> object header address over a version-1 B-tree of group nodes."""
+    def group_entries(self, btree: int, heap: int, _seen: set[int] | None = None) -> dict[str, int]:
+        """name -> object header address over a version-1 B-tree of group nodes. A node reached a
+        second time (a cycle in a malformed file) raises ValueError."""
+        seen = set() if _seen is None else _seen
+        if btree in seen:
+            raise ValueError(f"HDF5: group B-tree node at {btree} is reached twice")
+        seen.add(btree)
         out: dict[str, int] = {}
         self.sig(btree, b"TREE")
         node_type, level, used = self.d[btree + 4], self.d[btree + 5], self.u("H", btree + 6)[0]
@@ -56,7 +61,7 @@ class _File:
             child = self.u("Q", q)[0]
             q += 16  # child address, then the next key
             if level > 0:
-                out.update(self.group_entries(child, heap))
+                out.update(self.group_entries(child, heap, seen))
                 continue
             self.sig(child, b"SNOD")
             n_sym = self.u("H", child + 6)[0]
@@ -257,10 +262,15 @@ class _File:
         return out
 
 
-    def group(self, header: int, depth: int = 0) -> dict:
-        """A group's attributes, datasets (array, attributes) and subgroups, read recursively."""
+    def group(self, header: int, depth: int = 0, _seen: set[int] | None = None) -> dict:
+        """A group's attributes, datasets (array, attributes) and subgroups, read recursively. A group
+        whose object header comes round again (links forming a cycle) raises ValueError."""
         if depth > 32:
             raise ValueError("HDF5: groups nested deeper than 32 levels")
+        seen = set() if _seen is None else _seen
+        if header in seen:
+            raise ValueError(f"HDF5: the group object header at {header} is reached twice (a cycle)")
+        seen.add(header)
         table, attrs = None, {}
         for mtype, off, _size in self.messages(header):
             if mtype == 0x11:
@@ -273,7 +283,7 @@ class _File:
         out = {"attrs": attrs, "datasets": {}, "groups": {}}
         for name, child in self.group_entries(*table).items():
             if any(mtype == 0x11 for mtype, _, _ in self.messages(child)):
-                out["groups"][name] = self.group(child, depth + 1)
+                out["groups"][name] = self.group(child, depth + 1, seen)
             else:
                 out["datasets"][name] = self.dataset(child)
         return out
@@ -295,15 +305,20 @@ def is_hdf5(path: str | Path) -> bool:
 
 
 def _malformed(fn):
-    """Reads past the end of the file, or zlib errors, surface as ValueError naming the file."""
+    """Reads past the end of the file, zlib errors, runaway recursion and the reader's own
+    structural errors surface as ValueError naming the file."""
     import functools
 
     @functools.wraps(fn)
     def wrapper(path, *args):
         try:
             return fn(path, *args)
-        except (struct.error, IndexError, zlib.error) as exc:
+        except (struct.error, IndexError, zlib.error, RecursionError) as exc:
             raise ValueError(f"HDF5: {path} is truncated or malformed ({exc})") from exc
+        except ValueError as exc:
+            if str(path) in str(exc):
+                raise
+            raise ValueError(f"HDF5: {path} is malformed ({exc})") from exc
 
     return wrapper
 

@@ -357,6 +357,9 @@ def train_warm_start(ctx: _native.Context, coil, *, n_train: int = 4096, rank: i
     if held:
         cum = torch.cumsum(mode_err, 0) / mode_err.sum().clamp_min(1e-300)
         err_share = {str(m): round(float(cum[m - 1]), 4) for m in (8, 16, 32, 64, 128) if m <= r}
+    # Every GEMM of the training and the held-out pass reports an expired barrier wait to the
+    # device's status word: a network trained on invalid products is refused here.
+    _native.check(_native.load().cunibs_gemm_status(_stream(), None))
     model = WarmStartModel(mlp, basis16, f_mean.contiguous(), f_std.contiguous(), c_mean.contiguous(),
                            c_std.contiguous(), r)
     model.stats = {"n_train": n_train, "rank": r, "train_iterations_mean": float(iters.mean()),

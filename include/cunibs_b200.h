@@ -90,6 +90,9 @@ typedef struct {
     int vcycle_levels; /* levels the V-cycle smooths; the level below them (or the coarsest) is solved
                           exactly (cunibs_params.dense_max_rows) */
     int bottom_rows;   /* rows of that exactly solved operator */
+    int hierarchy_builds; /* AMG hierarchy builds over the context's life: 1 at create, +1 for each
+                             conductivity re-setup that rebuilds it and for each rebuild before the
+                             FP64 retry of a block that missed tolerance */
 } cunibs_info;
 
 /* Per-call options of a block solve. Zero-initialise for the context defaults. */
@@ -375,6 +378,16 @@ int cunibs_gemm_bf16(const void* A, int lda, const void* B, int ldb, int M, int 
                      const float* gate, int ld_gate, int act, float* out32, void* out16, int ld_out, void* out16t,
                      int ld_t, void* stream);
 int cunibs_mlp_colsum(const float* x, int rows, int cols, int ld, float* out, void* stream);
+/* Every mbarrier wait of the GEMM is bounded (2^24 polls or 2 s). A GEMM queued through
+ * cunibs_gemm_bf16 records an expired wait in a per-device status word; cunibs_gemm_status
+ * synchronises `stream`, reads and clears that word, sets *expired (may be NULL) and returns
+ * CUNIBS_ETIMEOUT if a wait expired since the last read (that GEMM's outputs are invalid), else OK.
+ * No counterpart in the reference (its kernels do not wait on barriers). */
+int cunibs_gemm_status(void* stream, int* expired);
+/* For tests of the timeout path only: later GEMM launches give up their waits after max_polls polls
+ * or max_ns nanoseconds (<= 0: the defaults), and with withhold_loads = 1 the producer issues no
+ * loads, so the MMA warp's first wait can only run out. Process-wide; restore with (0, 0, 0). */
+int cunibs_debug_gemm_waits(long long max_polls, long long max_ns, int withhold_loads);
 int cunibs_mlp_mse(const float* pred, const float* target, int rows, int cols, int ld, float* loss, float* d32,
                    void* d16, void* d16t, int ld_t, float* scratch, void* stream);
 int cunibs_mlp_adam(float* param, float* m, float* v, const float* grad, long long n, float lr, float beta1,
@@ -394,12 +407,23 @@ int cunibs_mlp_features(const double* transforms, int k, const float* mean, cons
  * transforms (k, 4, 4) and out (k, n_nodes, 3) are all device pointers on the current device, and the
  * work is queued on `stream` (a cudaStream_t; NULL is the legacy default stream). The function
  * allocates nothing: its scratch -- k * n_dip rotated dipole records -- is a fixed array of
- * CUNIBS_DADT_NOALLOC_MAX_RECORDS records (768 KiB) compiled into the library, which every GPU that
- * loads the library holds until the process exits. Larger k * n_dip is rejected with CUNIBS_EINVAL.
- * The first call on a device looks up that array's device address (a one-time cudaGetSymbolAddress,
- * made with the device current); make that first call before any stream capture. All calls share
- * the one array, so calls that may overlap on the GPU (different streams, or different host
- * threads) race on it: order them on one stream. */
+ * CUNIBS_DADT_NOALLOC_MAX_RECORDS records (768 KiB) compiled into the library. Larger k * n_dip is
+ * rejected with CUNIBS_EINVAL.
+ * When the array takes device memory: it belongs to the library's CUDA module. Under the runtime's
+ * default lazy module loading (CUDA_MODULE_LOADING=LAZY) a device receives the module -- the array
+ * and the kernel code -- at the first call on that device, and that first call can fail with
+ * CUNIBS_ECUDA (out of memory) if another allocator has already reserved all of the device's memory.
+ * So make one call on each device before the other allocator reserves its memory, or run with
+ * CUDA_MODULE_LOADING=EAGER (the module is then loaded with the context). The device holds it until
+ * the process exits.
+ * The first call on a device also looks up the array's device address (cudaGetSymbolAddress, made
+ * with the device current); make that first call before any stream capture. The address is kept per
+ * device and looked up again when the device's context changes (after cudaDeviceReset, or with a
+ * different driver-API context current).
+ * A CUDA error already pending from the caller's earlier work is reported as such (CUNIBS_ECUDA) and
+ * left pending; nothing is launched.
+ * All calls share the one array, so calls that may overlap on the GPU (different streams, or
+ * different host threads) race on it: order them on one stream. */
 #define CUNIBS_DADT_NOALLOC_MAX_RECORDS 16384
 int cunibs_dadt_noalloc(const double* nodes_mm, int n_nodes, const double* dip_pos_m, const double* dip_moment,
                         int n_dip, const double* transforms, int k, double didt, float* out, void* stream);

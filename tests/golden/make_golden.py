@@ -17,6 +17,7 @@ test file and line they come from.
 from __future__ import annotations
 
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -58,4 +59,7 @@ def main(reference: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CUNIBS_REFERENCE_ROOT", "")
+    if not root:
+        raise SystemExit("usage: make_golden.py <reference checkout> (or set CUNIBS_REFERENCE_ROOT)")
+    main(Path(root))

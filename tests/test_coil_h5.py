@@ -7,6 +7,7 @@ present, every bundled coil is read and the D70 is checked against the fixture b
 
 from __future__ import annotations
 
+import os
 from pathlib import Path
 
 import numpy as np
@@ -15,7 +16,10 @@ import pytest
 from cunibs_b200 import Coil
 
 GOLDEN = Path(__file__).resolve().parent / "golden" / "magstim_d70.npz"
-COILS = Path("/root/reference/src/cunibs/coils")
+# The reference checkout, when mounted, is named by CUNIBS_REFERENCE_ROOT; the tests that read its
+# coil library are skipped otherwise.
+_REF = os.environ.get("CUNIBS_REFERENCE_ROOT", "")
+COILS = Path(_REF) / "src" / "cunibs" / "coils" if _REF else Path("/nonexistent")
 
 
 @pytest.mark.skipif(not COILS.is_dir(), reason="the reference's coil library is not mounted")

@@ -68,6 +68,45 @@ def test_noalloc_matches_regular_entry_point_on_two_calls():
     ctx.close()
 
 
+def test_noalloc_call_leaves_free_device_memory_unchanged():
+    """After a first call (which, under lazy module loading, places the library's module on the
+    device), further calls take no device memory: the device's free memory is the same before and
+    after them."""
+    torch = pytest.importorskip("torch")
+    lib = _native.load()
+    lib.cunibs_dadt_noalloc.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                        C.c_double, C.c_void_p, C.c_void_p]
+    lib.cunibs_dadt_noalloc.restype = C.c_int
+    dev = torch.device("cuda", 0)
+    coil = figure8_coil(128)
+    n_nodes, k = 4096, 4
+    rng = np.random.default_rng(7)
+    d_nodes = torch.tensor(rng.uniform(-80.0, 80.0, (n_nodes, 3)), dtype=torch.float64, device=dev)
+    d_pos = torch.tensor(coil.positions_m, dtype=torch.float64, device=dev)
+    d_mom = torch.tensor(coil.moments, dtype=torch.float64, device=dev)
+    T = np.tile(np.eye(4), (k, 1, 1))
+    T[:, :3, 3] = [[0.0, 0.0, 94.0], [10.0, 0.0, 93.0], [0.0, 10.0, 93.0], [-10.0, 0.0, 93.0]]  # mm
+    d_T = torch.tensor(T.reshape(-1, 16), dtype=torch.float64, device=dev)
+    d_out = torch.empty((k, n_nodes, 3), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def call():
+        rc = lib.cunibs_dadt_noalloc(
+            C.c_void_p(d_nodes.data_ptr()), n_nodes, C.c_void_p(d_pos.data_ptr()), C.c_void_p(d_mom.data_ptr()),
+            coil.n_dipoles, C.c_void_p(d_T.data_ptr()), k, C.c_double(1e6), C.c_void_p(d_out.data_ptr()),
+            C.c_void_p(stream.cuda_stream))
+        _native.check(rc)
+        stream.synchronize()
+
+    call()
+    free_before, _ = torch.cuda.mem_get_info(dev)
+    for _ in range(3):
+        call()
+    free_after, _ = torch.cuda.mem_get_info(dev)
+    assert free_after == free_before
+    assert torch.isfinite(d_out).all()
+
+
 def test_noalloc_rejects_more_records_than_its_scratch():
     torch = pytest.importorskip("torch")
     lib = _native.load()
