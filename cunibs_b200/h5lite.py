@@ -236,6 +236,8 @@ class _File:
             return np.frombuffer(raw, dtype=dt, count=n).astype(dt.newbyteorder("=")).reshape(shape)
         if cls == 1:  # contiguous
             addr = self.u("Q", off + 2)[0]
+            if n == 0 or addr == _UNDEF:  # no storage allocated: empty, or never written (fill value 0)
+                return np.zeros(shape, dtype=dt.newbyteorder("="))
             return np.frombuffer(self.d, dtype=dt, count=n, offset=addr).astype(dt.newbyteorder("=")).reshape(shape)
         if cls != 2:
             raise ValueError(f"HDF5: layout class {cls}")
@@ -343,3 +345,202 @@ def read_tree(path: str | Path) -> dict:
     "groups": {name: <the same for the subgroup>}}``."""
     f = _open(path)
     return f.group(f.u("Q", 56 + 8)[0])
+
+
+# --- writing -------------------------------------------------------------------------------------
+#
+# The writer produces the same structures the reader handles and h5py's default ("earliest")
+# format uses, as the bundled coil files show them: a version-0 superblock (8-byte offsets and
+# lengths, group leaf K 4, internal K 16); each group an object header holding a symbol-table
+# message and its attributes, with a one-node version-1 B-tree (allocated at full size), symbol
+# table nodes of up to 8 entries, names sorted, and a local heap; each dataset an object header with
+# dataspace (version 1), datatype, fill value (version 2) and contiguous layout (version 3)
+# messages and its attributes; strings as variable-length UTF-8 strings in one global heap
+# collection, as h5py writes Python strings. Numeric data is written little-endian.
+
+_GROUP_LEAF_K = 4
+_GROUP_INTERNAL_K = 16
+_BTREE_NODE_BYTES = 24 + (2 * _GROUP_INTERNAL_K + 1) * 8 + 2 * _GROUP_INTERNAL_K * 8
+_SNOD_BYTES = 8 + 2 * _GROUP_LEAF_K * 40
+_VLEN_STR_TYPE = bytes.fromhex("1901010010000000") + bytes.fromhex("100000000100000000000800")
+
+
+def _pad8(b: bytes) -> bytes:
+    return b + b"\x00" * (-len(b) % 8)
+
+
+def _dtype_message(dt: np.dtype) -> bytes:
+    dt = np.dtype(dt).newbyteorder("<") if np.dtype(dt).byteorder == ">" else np.dtype(dt)
+    size = dt.itemsize
+    if dt.kind == "f":
+        if size == 8:
+            bits, exp_loc, exp_size, mant_size, bias = 0x3F20, 52, 11, 52, 1023
+        elif size == 4:
+            bits, exp_loc, exp_size, mant_size, bias = 0x1F20, 23, 8, 23, 127
+        else:
+            raise ValueError(f"HDF5 writer: float of {size} bytes")
+        return struct.pack("<B3sI", 0x11, bits.to_bytes(3, "little"), size) + struct.pack(
+            "<HHBBBBI", 0, 8 * size, exp_loc, exp_size, 0, mant_size, bias)
+    if dt.kind in "iu" or dt.kind == "b":
+        signed = 0x08 if dt.kind == "i" else 0x00
+        return struct.pack("<B3sI", 0x10, bytes([signed, 0, 0]), size) + struct.pack("<HH", 0, 8 * size)
+    raise ValueError(f"HDF5 writer: dtype {dt}")
+
+
+def _dataspace_message(shape: tuple[int, ...]) -> bytes:
+    return struct.pack("<BBBBI", 1, len(shape), 0, 0, 0) + b"".join(struct.pack("<Q", int(n)) for n in shape)
+
+
+class _Writer:
+    def __init__(self) -> None:
+        self.buf = bytearray(96)  # the superblock goes first, written last
+        self.strings: list[bytes] = []
+        self.gcol_at: int | None = None
+        self.pending_vlen: list[tuple[int, int]] = []  # (where a heap ID's address goes, string index)
+
+    def alloc(self, data: bytes) -> int:
+        at = len(self.buf)
+        self.buf += _pad8(bytes(data))
+        return at
+
+    def vlen_string(self, s: str) -> bytes:
+        """The 16-byte on-disk reference to a global-heap string (address patched at the end)."""
+        b = s.encode()
+        self.strings.append(b)
+        return struct.pack("<IQI", len(b), 0, len(self.strings))
+
+    def attribute_message(self, name: str, value) -> bytes:
+        nm = name.encode() + b"\x00"
+        vlen_slots = []
+        if isinstance(value, str):
+            dtm, space = _VLEN_STR_TYPE, _dataspace_message(())
+            data = self.vlen_string(value)
+            vlen_slots.append(4)
+        elif isinstance(value, (list, tuple)) and value and all(isinstance(v, str) for v in value):
+            dtm, space = _VLEN_STR_TYPE, _dataspace_message((len(value),))
+            parts = []
+            for i, v in enumerate(value):
+                parts.append(self.vlen_string(v))
+                vlen_slots.append(16 * i + 4)
+            data = b"".join(parts)
+        else:
+            a = np.asarray(value)
+            if a.dtype == bool:
+                a = a.astype(np.int8)
+            if a.dtype.kind not in "iuf":
+                raise ValueError(f"HDF5 writer: attribute {name!r} of type {a.dtype}")
+            a = a.astype(a.dtype.newbyteorder("<"))
+            dtm, space, data = _dtype_message(a.dtype), _dataspace_message(a.shape), a.tobytes()
+        head = struct.pack("<BBHHH", 1, 0, len(nm), len(dtm), len(space))
+        body = head + _pad8(nm) + _pad8(dtm) + _pad8(space)
+        data_at = len(body)
+        msg = _pad8(body + data)
+        return msg, [data_at + s for s in vlen_slots]
+
+    def object_header(self, messages: list[tuple[int, bytes, int]], vlen_fixups: list[list[int]]) -> int:
+        """messages: (type, data, flags); vlen_fixups[i]: offsets in message i's data that hold a
+        global-heap collection address. Returns the header's address."""
+        block = bytearray()
+        fix_at = []
+        for (mtype, data, flags), fixes in zip(messages, vlen_fixups):
+            data = _pad8(data)
+            start = len(block) + 8
+            block += struct.pack("<HHB3x", mtype, len(data), flags) + data
+            fix_at += [start + f for f in fixes]
+        prefix = struct.pack("<BBHII4x", 1, 0, len(messages), 1, len(block))
+        at = self.alloc(prefix + bytes(block))
+        self.pending_vlen += [(at + 16 + f, 0) for f in fix_at]
+        return at
+
+    def dataset(self, arr: np.ndarray, attrs: dict) -> int:
+        a = np.ascontiguousarray(arr)
+        if a.dtype == bool:
+            a = a.astype(np.int8)
+        a = a.astype(a.dtype.newbyteorder("<"))
+        raw_at = self.alloc(a.tobytes()) if a.nbytes else _UNDEF
+        msgs = [(0x01, _dataspace_message(a.shape), 0), (0x03, _dtype_message(a.dtype), 1),
+                (0x05, bytes([2, 2, 2, 0]), 1),
+                (0x08, struct.pack("<BBQQ", 3, 1, raw_at, a.nbytes), 0)]
+        fixes: list[list[int]] = [[], [], [], []]
+        for k, v in attrs.items():
+            m, f = self.attribute_message(k, v)
+            msgs.append((0x0C, m, 0))
+            fixes.append(f)
+        return self.object_header(msgs, fixes)
+
+    def group(self, tree: dict) -> tuple[int, int, int]:
+        """Writes a group and everything under it; returns (header, B-tree, local heap) addresses."""
+        children: dict[str, tuple[int, bool, tuple[int, int]]] = {}
+        for name, item in tree.get("datasets", {}).items():
+            arr, attrs = item if isinstance(item, tuple) else (item, {})
+            children[name] = (self.dataset(arr, attrs), False, (0, 0))
+        for name, sub in tree.get("groups", {}).items():
+            hdr, bt, hp = self.group(sub)
+            children[name] = (hdr, True, (bt, hp))
+        names = sorted(children, key=lambda s: s.encode())
+        if len(names) > 2 * _GROUP_LEAF_K * 2 * _GROUP_INTERNAL_K:
+            raise ValueError("HDF5 writer: more than 256 members in one group")
+        # Local heap: "" at 0, then the names, each null-terminated and padded to 8 bytes.
+        heap_data = bytearray(8)
+        offset = {}
+        for n in names:
+            offset[n] = len(heap_data)
+            heap_data += _pad8(n.encode() + b"\x00")
+        # Symbol table nodes of up to 2 * leaf K entries each.
+        snods, keys = [], [0]
+        for s in range(0, len(names), 2 * _GROUP_LEAF_K):
+            part = names[s:s + 2 * _GROUP_LEAF_K]
+            node = bytearray(b"SNOD" + struct.pack("<BBH", 1, 0, len(part)))
+            for n in part:
+                hdr, is_group, (bt, hp) = children[n]
+                node += struct.pack("<QQII", offset[n], hdr, 1 if is_group else 0, 0)
+                node += struct.pack("<QQ", bt, hp) if is_group else bytes(16)
+            node += bytes(_SNOD_BYTES - len(node))
+            snods.append(self.alloc(bytes(node)))
+            keys.append(offset[part[-1]])
+        btree = bytearray(b"TREE" + struct.pack("<BBHQQ", 0, 0, len(snods), _UNDEF, _UNDEF))
+        for i, child in enumerate(snods):
+            btree += struct.pack("<QQ", keys[i], child)
+        btree += struct.pack("<Q", keys[len(snods)])
+        btree += bytes(_BTREE_NODE_BYTES - len(btree))
+        bt_at = self.alloc(bytes(btree))
+        heap_at = len(self.buf)
+        self.alloc(b"HEAP" + struct.pack("<B3xQQQ", 0, len(heap_data), _UNDEF, heap_at + 32))
+        self.alloc(bytes(heap_data))
+        msgs = [(0x11, struct.pack("<QQ", bt_at, heap_at), 0)]
+        fixes: list[list[int]] = [[]]
+        for k, v in tree.get("attrs", {}).items():
+            m, f = self.attribute_message(k, v)
+            msgs.append((0x0C, m, 0))
+            fixes.append(f)
+        return self.object_header(msgs, fixes), bt_at, heap_at
+
+    def finish(self, root: tuple[int, int, int]) -> bytes:
+        if self.strings:
+            objs = bytearray()
+            for i, b in enumerate(self.strings, start=1):
+                objs += struct.pack("<HHIQ", i, 0, 0, len(b)) + _pad8(b)
+            size = max(4096, 16 + len(objs) + 16)
+            gcol = bytearray(b"GCOL" + struct.pack("<B3xQ", 1, size)) + objs
+            free = size - len(gcol)
+            gcol += struct.pack("<HHIQ", 0, 0, 0, free) + bytes(free - 16)
+            self.gcol_at = self.alloc(bytes(gcol))
+            for where, _ in self.pending_vlen:
+                struct.pack_into("<Q", self.buf, where, self.gcol_at)
+        hdr, bt, hp = root
+        sb = bytearray(_SIGNATURE + bytes([0, 0, 0, 0, 0, 8, 8, 0]))
+        sb += struct.pack("<HHI", _GROUP_LEAF_K, _GROUP_INTERNAL_K, 0)
+        sb += struct.pack("<QQQQ", 0, _UNDEF, len(self.buf), _UNDEF)
+        sb += struct.pack("<QQII", 0, hdr, 1, 0) + struct.pack("<QQ", bt, hp)
+        self.buf[0:96] = sb
+        return bytes(self.buf)
+
+
+def write_tree(path: str | Path, tree: dict) -> None:
+    """Writes ``tree`` -- ``{"attrs": {...}, "datasets": {name: array or (array, attrs)},
+    "groups": {name: <the same>}}``, the form ``read_tree`` returns -- as an HDF5 file. Attribute
+    values may be str (stored as variable-length UTF-8 strings), lists of str, or numbers and
+    numeric arrays; datasets are numeric arrays (stored contiguous, uncompressed)."""
+    w = _Writer()
+    root = w.group(tree)
+    Path(path).write_bytes(w.finish(root))

@@ -535,7 +535,12 @@ class FieldResult:
         return self._summaries[region]
 
     def save(self, path: str | Path) -> None:
-        """Write the result to a self-contained ``.npz`` (arrays not retained are absent)."""
+        """Write the result to a self-contained file (arrays not retained are absent). A ``.h5`` or
+        ``.hdf5`` path gets the reference's HDF5 layout (simulation.py:805-838), written through h5py
+        where it is installed, else through the built-in writer; any other path a ``.npz``."""
+        if Path(path).suffix.lower() in (".h5", ".hdf5"):
+            _write_hdf5_tree(path, self._hdf5_tree())
+            return
         arrays = {k: getattr(self, k) for k in ("magnE", "E", "v", "vols", "tet_tags", "barycenters_mm", "E_slots",
                                                   "slot_node", "slot_tag", "tet_nodes")
                   if getattr(self, k) is not None}
@@ -583,6 +588,21 @@ class FieldResult:
                        n_nodes=int(z["n_nodes"]) if "n_nodes" in z.files else None, E_slots=opt("E_slots"),
                        slot_node=opt("slot_node"), slot_tag=opt("slot_tag"), tet_nodes=opt("tet_nodes"))
 
+    def _hdf5_tree(self) -> dict:
+        """The reference's HDF5 layout of this result (simulation.py:805-838) as a tree."""
+        data = {k: getattr(self, k) for k in ("magnE", "E", "v", "vols", "tet_tags", "barycenters_mm", "E_slots",
+                                               "slot_node", "slot_tag", "tet_nodes") if getattr(self, k) is not None}
+        data["transform"] = self.transform
+        attrs: dict = {"format_version": _FORMAT_VERSION, "recovery": self.recovery}
+        if self.n_nodes is not None:
+            attrs["n_nodes"] = int(self.n_nodes)
+        attrs.update({"coil_name": self.coil_name, "didt": float(self.didt),
+                      "placement_center_mm": np.asarray(self.placement.center_mm, np.float64),
+                      "placement_handle_mm": np.asarray(self.placement.handle_mm, np.float64),
+                      "placement_distance_mm": float(self.placement.distance_mm)})
+        return {"attrs": attrs, "datasets": {k: (np.asarray(v), {}) for k, v in data.items()},
+                "groups": {"summary": _metrics_tree(self.summary)}}
+
     @classmethod
     def _load_hdf5(cls, path, tree: dict) -> FieldResult:
         """The reference's HDF5 layout (simulation.py:839-870, _read_metrics 68-77) as a tree of
@@ -602,6 +622,42 @@ class FieldResult:
                    recovery=str(attrs.get("recovery", "raw")),
                    n_nodes=int(attrs["n_nodes"]) if "n_nodes" in attrs else None, E_slots=opt("E_slots"),
                    slot_node=opt("slot_node"), slot_tag=opt("slot_tag"), tet_nodes=opt("tet_nodes"))
+
+
+def _metrics_tree(m: metrics.FieldMetrics) -> dict:
+    """The reference's metrics group layout (simulation.py:56-65) as a tree."""
+    return {"attrs": {"region": str(m["region"]), "peak_magnE": float(m["peak_magnE"]),
+                      "region_volume_m3": float(m["region_volume_m3"])},
+            "datasets": {"peak_location_mm": (np.asarray(m["peak_location_mm"], np.float64), {}),
+                         "center_of_gravity_mm": (np.asarray(m["center_of_gravity_mm"], np.float64), {})},
+            "groups": {name: {"attrs": {str(k): float(v) for k, v in m[name].items()}, "datasets": {}, "groups": {}}
+                       for name in ("focality_m3", "distribution")}}
+
+
+def _write_hdf5_tree(path, tree: dict) -> None:
+    """Writes a ``{"attrs", "datasets": {name: (array, attrs)}, "groups"}`` tree as an HDF5 file:
+    through h5py where it is installed (datasets gzip-compressed, as the reference writes them), else
+    through the built-in writer (contiguous datasets, strings as variable-length UTF-8)."""
+    try:
+        import h5py
+    except ImportError:
+        from . import h5lite
+
+        h5lite.write_tree(path, tree)
+        return
+
+    def put(g, t: dict) -> None:
+        for k, v in t.get("attrs", {}).items():
+            g.attrs[k] = v
+        for name, (arr, attrs) in t.get("datasets", {}).items():
+            d = g.create_dataset(name, data=arr, compression="gzip" if np.asarray(arr).size > 16 else None)
+            for k, v in attrs.items():
+                d.attrs[k] = v
+        for name, sub in t.get("groups", {}).items():
+            put(g.create_group(name), sub)
+
+    with h5py.File(path, "w") as f:
+        put(f, tree)
 
 
 def _metrics_from_tree(grp: dict) -> metrics.FieldMetrics:

@@ -159,7 +159,14 @@ class ConductivityUQResult:
         return tissue_sensitivity(self.sigma_samples, y, self.perturbed_tags)
 
     def save(self, path: str | Path) -> None:
-        """Write the result to a self-contained ``.npz`` (moment arrays only when retained)."""
+        """Write the result to a self-contained file (moment arrays only when retained). A ``.h5``
+        or ``.hdf5`` path gets the reference's HDF5 layout (result.py:182-222; its files hold no
+        per-draw iteration counts or re-setup count), any other path a ``.npz``."""
+        if Path(path).suffix.lower() in (".h5", ".hdf5"):
+            from .simulation import _write_hdf5_tree
+
+            _write_hdf5_tree(path, self._hdf5_tree())
+            return
         arrays = {k: getattr(self, k) for k in ("mean_magnE", "std_magnE", "cov_magnE", "vols", "tet_tags",
                                                   "barycenters_mm") if getattr(self, k) is not None}
         np.savez_compressed(
@@ -204,6 +211,28 @@ class ConductivityUQResult:
         if res.mean_magnE is not None:
             res.summary = res.compute_summary()
         return res
+
+    def _hdf5_tree(self) -> dict:
+        """The reference's HDF5 layout of this result (result.py:182-222) as a tree."""
+        from .simulation import _metrics_tree
+
+        if self.summary is None:
+            raise ValueError("This result has no summary to save; call compute_summary() first.")
+        data = {k: getattr(self, k) for k in ("mean_magnE", "std_magnE", "cov_magnE", "vols", "tet_tags",
+                                               "barycenters_mm") if getattr(self, k) is not None}
+        data["sigma_samples"] = self.sigma_samples
+        for k in ("peak_samples", "focality_samples", "peak_location_samples"):
+            data[k] = getattr(self, k)
+        summary = {"attrs": {"max_local_cov": float(self.summary.max_local_cov)}, "datasets": {},
+                   "groups": {"mean_field": _metrics_tree(self.summary.mean_field)}}
+        roi = {"attrs": {}, "datasets": {k: (np.asarray(v), {}) for k, v in self.roi_samples.items()}, "groups": {}}
+        attrs = {"format_version": _FORMAT_VERSION, "recovery": self.recovery, "n_samples": int(self.n_samples),
+                 "perturbed_tags": np.asarray(self.perturbed_tags, dtype=np.int32), "coil_name": self.coil_name,
+                 "didt": float(self.didt), "placement_center_mm": np.asarray(self.placement.center_mm, np.float64),
+                 "placement_handle_mm": np.asarray(self.placement.handle_mm, np.float64),
+                 "placement_distance_mm": float(self.placement.distance_mm)}
+        return {"attrs": attrs, "datasets": {k: (np.asarray(v), {}) for k, v in data.items()},
+                "groups": {"summary": summary, "roi_samples": roi}}
 
     @classmethod
     def _load_hdf5(cls, path, tree: dict) -> ConductivityUQResult:

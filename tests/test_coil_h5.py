@@ -174,3 +174,130 @@ def test_truncated_files_raise_value_errors(tmp_path):
         for read in (lambda: h5lite.read_tree(p), lambda: h5lite.read_dataset(p, "dipoles")):
             with pytest.raises(ValueError, match="HDF5"):
                 read()
+
+
+def test_field_result_hdf5_save_round_trip(tmp_path):
+    """FieldResult.save to .h5 writes the reference's layout (simulation.py:805-838); the built-in
+    reader reads it back as that layout and load() restores every retained array and the summary."""
+    from cunibs_b200 import h5lite, simulation
+
+    r = _result()
+    path = tmp_path / "result.h5"
+    r.save(path)
+    assert h5lite.is_hdf5(path)
+    tree = h5lite.read_tree(path)
+    want = _reference_layout(r)
+    assert set(tree["datasets"]) == set(want["datasets"])
+    assert set(tree["attrs"]) == set(want["attrs"])
+    assert set(tree["groups"]["summary"]["groups"]) == {"focality_m3", "distribution"}
+    got = simulation.FieldResult.load(path)
+    for k in ("magnE", "v", "vols", "tet_tags", "barycenters_mm", "E_slots", "slot_node", "transform"):
+        a, b = getattr(got, k), getattr(r, k)
+        np.testing.assert_array_equal(a, b)
+        assert a.dtype == np.asarray(b).dtype
+    assert got.E is None and got.slot_tag is None and got.tet_nodes is None
+    assert (got.coil_name, got.didt, got.recovery, got.n_nodes) == (r.coil_name, r.didt, r.recovery, r.n_nodes)
+    np.testing.assert_array_equal(got.placement.handle_mm, r.placement.handle_mm)
+    assert got.summary["focality_m3"] == r.summary["focality_m3"]
+    assert got.summary["distribution"] == r.summary["distribution"]
+    assert got.summary["peak_magnE"] == r.summary["peak_magnE"]
+
+
+def test_conductivity_result_hdf5_save_round_trip(tmp_path):
+    from cunibs_b200 import h5lite
+    from cunibs_b200.simulation import Placement
+    from cunibs_b200.uq import ConductivityUQResult, ConductivityUQSummary
+
+    rng = np.random.default_rng(4)
+    n, m = 6, 40
+    mean = rng.random(m).astype(np.float32)
+    summary = ConductivityUQSummary(mean_field=_result().summary, max_local_cov=0.31)
+    res = ConductivityUQResult(
+        mean_magnE=mean, std_magnE=mean * 0.1, cov_magnE=None, n_samples=n, perturbed_tags=(1, 2, 3),
+        sigma_samples=rng.random((n, 3)), vols=rng.random(m), tet_tags=np.full(m, 2, np.int32),
+        barycenters_mm=rng.random((m, 3)), placement=Placement([0.0, 0.0, 90.0], [0.0, 50.0, 90.0]),
+        coil_name="fig8", didt=1e6, peak_samples=rng.random(n), focality_samples=rng.random((n, 2)),
+        peak_location_samples=rng.random((n, 3)), iteration_samples=np.full(n, 12, np.int32), recovery="raw",
+        summary=summary, roi_samples={"m1": rng.random(n), "s1": rng.random(n)})
+    path = tmp_path / "uq.h5"
+    res.save(path)
+    tree = h5lite.read_tree(path)
+    assert set(tree["groups"]) == {"summary", "roi_samples"}
+    assert tree["attrs"]["perturbed_tags"].dtype == np.int32
+    got = ConductivityUQResult.load(path)
+    for k in ("mean_magnE", "std_magnE", "sigma_samples", "peak_samples", "focality_samples",
+              "peak_location_samples", "vols", "tet_tags", "barycenters_mm"):
+        np.testing.assert_array_equal(getattr(got, k), getattr(res, k))
+    assert got.cov_magnE is None and got.perturbed_tags == (1, 2, 3) and got.n_samples == n
+    assert set(got.roi_samples) == {"m1", "s1"}
+    np.testing.assert_array_equal(got.roi_samples["s1"], res.roi_samples["s1"])
+    assert got.summary.max_local_cov == 0.31
+
+
+def test_writer_covers_types_shapes_and_many_members(tmp_path):
+    """Every attribute kind the layouts use, empty and 0-d datasets, nested groups, and a group with
+    more members than one symbol-table node holds (several nodes under one B-tree node)."""
+    from cunibs_b200 import h5lite
+
+    rng = np.random.default_rng(1)
+    tree = {"attrs": {"s": "text with ü", "i": 7, "f": 2.5, "v": np.array([1.0, 2.0, 3.0]),
+                      "ti": np.array([1, 2], np.int32), "strs": ["a", "bc"]},
+            "datasets": {f"d{i:02d}": (rng.random((3, i + 1)).astype(np.float32 if i % 2 else np.float64),
+                                       {"k": i}) for i in range(20)},
+            "groups": {"g": {"attrs": {"x": 1.0}, "datasets": {"empty": (np.zeros((0, 3)), {}),
+                                                                "ints": (np.arange(10, dtype=np.int64), {})},
+                             "groups": {"h": {"attrs": {}, "datasets": {}, "groups": {}}}}}}
+    path = tmp_path / "t.h5"
+    h5lite.write_tree(path, tree)
+    got = h5lite.read_tree(path)
+    assert got["attrs"]["s"] == "text with ü" and got["attrs"]["i"] == 7 and got["attrs"]["f"] == 2.5
+    np.testing.assert_array_equal(got["attrs"]["v"], [1.0, 2.0, 3.0])
+    assert got["attrs"]["ti"].dtype == np.int32 and got["attrs"]["strs"] == ["a", "bc"]
+    assert sorted(got["datasets"]) == sorted(tree["datasets"])
+    for name, (arr, attrs) in tree["datasets"].items():
+        back, battrs = got["datasets"][name]
+        np.testing.assert_array_equal(back, arr)
+        assert back.dtype == arr.dtype and battrs == attrs
+        np.testing.assert_array_equal(h5lite.read_dataset(path, name)[0], arr)
+    g = got["groups"]["g"]
+    assert g["attrs"] == {"x": 1.0} and g["datasets"]["empty"][0].shape == (0, 3)
+    np.testing.assert_array_equal(g["datasets"]["ints"][0], np.arange(10))
+    assert g["groups"]["h"] == {"attrs": {}, "datasets": {}, "groups": {}}
+
+
+@pytest.mark.skipif(not COILS.is_dir(), reason="the reference's coil library is not mounted")
+def test_writer_matches_a_bundled_coil_structure(tmp_path):
+    """A coil file rewritten by the built-in writer reads back (through both readers) equal to the
+    bundled one: the same dataset, attributes and string encoding."""
+    from cunibs_b200 import h5lite
+
+    src = COILS / "MagStim_D70.h5"
+    tree = h5lite.read_tree(src)
+    out = tmp_path / "d70.h5"
+    h5lite.write_tree(out, tree)
+    again = h5lite.read_tree(out)
+    a, aa = tree["datasets"]["dipoles"]
+    b, ba = again["datasets"]["dipoles"]
+    np.testing.assert_array_equal(a, b)
+    assert aa == ba and again["attrs"] == tree["attrs"]
+    np.testing.assert_array_equal(h5lite.read_dataset(out, "dipoles")[0], a)
+    c = Coil.load(out)
+    assert c.name == "D70" and c.n_dipoles == a.shape[0]
+
+
+def test_group_cycle_raises_value_error_naming_the_file(tmp_path):
+    """A malformed file whose group links form a cycle: a subgroup's symbol-table entry pointing back
+    at the root group's object header."""
+    import struct
+
+    from cunibs_b200 import h5lite
+
+    path = tmp_path / "cycle.h5"
+    h5lite.write_tree(path, {"attrs": {}, "datasets": {}, "groups": {"sub": {"attrs": {}, "datasets": {}, "groups": {}}}})
+    data = bytearray(path.read_bytes())
+    root_header = struct.unpack_from("<Q", data, 64)[0]
+    snod = data.index(b"SNOD")
+    struct.pack_into("<Q", data, snod + 8 + 8, root_header)  # entry 0's object header -> the root
+    path.write_bytes(bytes(data))
+    with pytest.raises(ValueError, match=f"{path}.*reached twice"):
+        h5lite.read_tree(path)
