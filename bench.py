@@ -415,6 +415,15 @@ def run_ours(args) -> dict:
     draws = conductivity_draws(ctx, coil, centers[:4], handles[:4], dists[:4], args.recovery, stream)
     adm_line = adm_measure(ctx, coil, sites, stream)
     multi = multi_subject_measure(coil, args.recovery) if world == 1 else None
+    # The other benchmark configurations, each a line of its own (one GPU; rank 0 of a replica run).
+    configs = None
+    if args.configs == "all" and rank == 0:
+        configs = {}
+        if args.warm_start == "on":
+            configs["learned_heldout"] = config_learned_heldout(ctx, coil, stream, n_train=args.train)
+        configs["small_plain"] = config_small_plain(local, not args.no_cpu_baseline)
+        configs["batched_uneven"] = config_batched_uneven()
+        configs["conductivity_3_5m"] = config_conductivity_3_5m(local, not args.no_cpu_baseline)
 
     # Roofline of the SpMV-dominated iteration (solve stage).
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -495,6 +504,7 @@ def run_ours(args) -> dict:
         "conductivity_draws": draws,
         "adm": adm_line,
         "multi_subject": multi,
+        "configs": configs,
         "clocks": clocks.summary(),
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -558,15 +568,24 @@ def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_d
         return its, rel0
 
     old_ms, old_its = device_ms(keep_coarse)
-    begin_ms, ranks = device_ms(lambda: ctx.sigma_begin(coil, centers, handles, dists, 1e6, nominal, tags,
-                                                        recovery=recovery))
+    # Opening the study twice, with the wall clock beside the device time of each: a first call that
+    # alone is slow, or a host time far above the device time, locates one-off costs.
+    begin_runs = []
+    for rep in range(2):
+        t0 = time.perf_counter()
+        begin_ms, ranks = device_ms(lambda: ctx.sigma_begin(coil, centers, handles, dists, 1e6, nominal, tags,
+                                                            recovery=recovery))
+        begin_runs.append((round(begin_ms, 3), round(1e3 * (time.perf_counter() - t0), 3)))
+        if rep == 0:
+            ctx.sigma_end()
     try:
         new_ms, (new_its, rel0) = device_ms(study)
     finally:
         ctx.sigma_end()
     return {"what": f"{n_draws} draws x {k} placements, 10 tissues lognormal (median = table, log-sd 0.25)",
             "study_ms_per_draw": round(new_ms / n_draws, 4), "study_iterations": round(float(np.mean(new_its)), 2),
-            "study_begin_ms": round(begin_ms, 3), "subspace_rank": ranks.tolist(),
+            "study_begin_ms": round(begin_ms, 3), "study_begin_device_host_ms": begin_runs,
+            "subspace_rank": ranks.tolist(),
             "guess_init_relres_max": round(max(rel0), 6),
             "keep_coarse_zero_guess_ms_per_draw": round(old_ms / n_draws, 4),
             "keep_coarse_iterations": round(float(np.mean(old_its)), 2),
@@ -600,7 +619,11 @@ def adm_measure(ctx, coil, sites, stream) -> dict:
     adj_ms, adjoint = device_ms(lambda: adm.solve_adjoint(ctx, target))
     grid = adm._coverage_grid(ctx, coil, centers, 4.0, 3.0, 8.0)
     torch.cuda.nvtx.range_push("adm_qfield")
-    q_ms, recip = device_ms(lambda: adm.sample_qfield(adjoint, grid))
+    q_runs = []
+    for _ in range(2):  # the first and a repeat, device and wall clock (one-off costs show in the first)
+        t0 = time.perf_counter()
+        q_ms, recip = device_ms(lambda: adm.sample_qfield(adjoint, grid))
+        q_runs.append((round(q_ms, 3), round(1e3 * (time.perf_counter() - t0), 3)))
     torch.cuda.nvtx.range_pop()
     pairs = grid.n_points * ctx.n_nodes * target.directions.shape[0]
     # 360 in-plane rotations per site: handle points around each site's own coil frame.
@@ -616,7 +639,7 @@ def adm_measure(ctx, coil, sites, stream) -> dict:
     opt_ms, res = device_ms(lambda: adm.optimize_placement(recip, coil, centers, n_samples=9))
     out = {"what": "magnitude target (3 adjoint directions), 8 sites; grid 3 mm covering any rotation",
            "adjoint_ms": round(adj_ms, 3), "adjoint_iterations": adjoint.iterations.tolist(),
-           "grid_points": int(grid.n_points), "qfield_ms": round(q_ms, 3),
+           "grid_points": int(grid.n_points), "qfield_ms": round(q_ms, 3), "qfield_device_host_ms": q_runs,
            "qfield_gpair_per_s": round(pairs / (q_ms / 1e3) / 1e9, 1),
            "evaluate_placements": int(T.shape[0]), "evaluate_ms": round(ev_ms, 3),
            "evaluate_placements_per_s": round(T.shape[0] / (ev_ms / 1e3), 1),
@@ -665,6 +688,226 @@ def multi_subject_measure(coil, recovery, n_place=16, repeats=3) -> dict:
            "bitwise_equal": bool(same)}
     for s in subjects:
         s.free()
+    return out
+
+
+def _device_ms(stream, fn):
+    """CUDA-event time of fn() on the library stream (events on either side, synchronised)."""
+    import torch
+
+    with torch.cuda.stream(stream):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+    out = fn()
+    with torch.cuda.stream(stream):
+        e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1), out
+
+
+def _gm_parity(gpu_magnE, gpu_peak, ref, tags) -> tuple[float, float]:
+    gm = tags == 2
+    a, b = np.asarray(gpu_magnE, np.float64)[gm], np.asarray(ref["magnE"][0], np.float64)[gm]
+    return (float(np.linalg.norm(a - b) / np.linalg.norm(b)),
+            float(abs(gpu_peak - ref["summary"][0][0]) / ref["summary"][0][0]))
+
+
+def config_small_plain(local: int, with_oracle: bool, reps: int = 10) -> dict:
+    """The plain-method small case: 64^3 lattice at 3 mm clipped to r <= 90 mm (five shells), a
+    figure-8 of 2 x 512 z-dipoles 4 mm above the vertex, dI/dt 1e6, one placement per block
+    (block_k 1), relative residual 1e-10. Context set-up time, then device time of `reps` one-placement
+    blocks (host C ABI, harmonic recovery) for plain FP64 and the split default; parity of each
+    against the FP64 oracle at 1e-12 (rank 0)."""
+    import torch
+
+    from cunibs_b200 import _native
+    from cunibs_b200.synthetic import FIVE_SHELLS
+
+    mesh = sphere_head(3.0, 90.0, FIVE_SHELLS, cells=64)
+    coil = figure8_coil(512)
+    c = np.array([[0.0, 0.0, 90.0]])
+    h = c + [0.0, 50.0, 0.0]
+    out = {"what": "64^3 x 3 mm sphere (5 shells), 2x512 z-dipole figure-8 4 mm above the vertex, "
+                   "k = 1, rel.res 1e-10, harmonic recovery", "n_tets": int(mesh.n_tets)}
+    ref = None
+    if with_oracle:
+        from oracle import Oracle
+
+        orc = Oracle(mesh)
+        ref = orc.solve(coil, c, h, [4.0], 1e6, tolerance=1e-12, recovery="harmonic")
+    for name, prec in (("plain_fp64", _native.PREC_PLAIN_FP64), ("split", _native.PREC_SPLIT)):
+        p = _native.default_params()
+        p.device = local
+        p.tolerance = 1e-10
+        p.precision = prec
+        t0 = time.perf_counter()
+        ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
+        torch.cuda.synchronize()
+        setup_s = time.perf_counter() - t0
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+        first = ctx.solve_block(coil, c, h, [4.0], 1e6, magnitude=True, recovery="harmonic")  # recovery operator
+        ms, its = _device_ms(stream, lambda: [ctx.solve_block(coil, c, h, [4.0], 1e6, recovery="harmonic")[
+            "iterations"][0] for _ in range(reps)])
+        row = {"setup_s": round(setup_s, 3), "placements_per_s": round(reps / (ms / 1e3), 2),
+               "ms_per_placement": round(ms / reps, 3), "iterations": int(its[0])}
+        if ref is not None:
+            # The oracle's element order is the context's (the same Morton layout, bit for bit).
+            rel, peak = _gm_parity(first["magnE"][0], first["summary"][0][0], ref, ctx.array("tet_tags"))
+            row["parity"] = {"gm_rel_l2": float(f"{rel:.3e}"), "peak_rel": float(f"{peak:.3e}"), "bar": 1e-5}
+        out[name] = row
+        ctx.close()
+    return out
+
+
+def config_batched_uneven(n_place: int = 64) -> dict:
+    """Four sphere heads of uneven size (0.3M, 0.9M, 1.8M and 3.5M tets at outer radii 85, 88, 92 and
+    95 mm), 64 placements each (uniform random centres on the scalp cap above z = 40 mm, handle
+    azimuth uniform), harmonic recovery: each subject's block width and dA/dt overlap autotuned (widths
+    4, 8, 16) on its own first 16 placements, then the four sweeps one after another and side by side
+    (one host thread per subject). Wall clock around each whole run, results copied to the host; the
+    side-by-side results are checked bitwise against the sequential ones."""
+    from cunibs_b200 import Placement, Subject
+    from cunibs_b200.batch import SubjectJob, simulate_subjects
+    from cunibs_b200.synthetic import cap_placements
+
+    coil = figure8_coil(2048)
+    specs = [(3.71, 85.0, 11), (2.68, 88.0, 12), (2.23, 92.0, 13), (1.83, 95.0, 14)]
+    subjects, jobs, tuned = [], [], []
+    for spacing, radius, seed in specs:
+        mesh = sphere_head(spacing, radius, EIGHT_SHELLS, (EYE_CAP, MUSCLE_CAP), jitter_mm=0.2, seed=0)
+        subj = Subject(mesh, tolerance=TOL)
+        sites = [Placement(cc, hh) for cc, hh in cap_placements(radius, n_place, 40.0, seed=seed)]
+        res = subj.autotune(coil, sites[:16], widths=(4, 8, 16), overlaps=(1, 2), repeats=1)
+        tuned.append({"block_k": res.block_k, "overlap": res.overlap_blocks_per_sm})
+        subjects.append(subj)
+        jobs.append(SubjectJob(subj, coil, sites, options=dict(recovery="harmonic", magnitude=True)))
+    for j in jobs:  # loop graphs of the tuned width captured outside the timing
+        list(j.subject.iter_simulate(coil, j.placements[:16], recovery="harmonic"))
+    t0 = time.perf_counter()
+    alone = [list(j.subject.iter_simulate(coil, j.placements, recovery="harmonic", magnitude=True)) for j in jobs]
+    seq_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    together = simulate_subjects(jobs)
+    con_s = time.perf_counter() - t0
+    same = all(np.array_equal(a.magnE, b.magnE) for ra, rb in zip(alone, together) for a, b in zip(ra, rb))
+    total = n_place * len(jobs)
+    out = {"what": "4 subjects (0.3/0.9/1.8/3.5M tets, r 85-95 mm) x 64 cap placements, autotuned width "
+                   "and overlap per subject, harmonic recovery, |E| retained",
+           "n_tets": [int(s.context.n_tets) for s in subjects], "tuned": tuned,
+           "sequential_s": round(seq_s, 4), "concurrent_s": round(con_s, 4),
+           "placements_per_s_sequential": round(total / seq_s, 1),
+           "placements_per_s_concurrent": round(total / con_s, 1), "bitwise_equal": bool(same)}
+    for s in subjects:
+        s.free()
+    return out
+
+
+def config_learned_heldout(ctx, coil, stream, n_held: int = 1024, n_train: int = 0) -> dict:
+    """The learned warm start on held-out poses: 1024 random cap poses (a seed the training never
+    used), solved in blocks of 8 to rel.res 1e-8 with the installed network's guess and with the zero
+    guess, both two deep; mean PCG iterations, the guess's initial residual, and device-timed
+    placements/s of each."""
+    from cunibs_b200.synthetic import cap_placements
+
+    poses = cap_placements(90.0, n_held, 40.0, seed=991)
+    c = np.stack([p[0] for p in poses])
+    h = np.stack([p[1] for p in poses])
+    d = np.full(K_BLOCK, 4.0)
+
+    def sweep(warm):
+        its, rel0 = [], []
+        tickets = [ctx.submit_block(coil, c[:K_BLOCK], h[:K_BLOCK], d, 1e6, warm_start=warm)]
+        for b in range(1, n_held // K_BLOCK + 1):
+            if b < n_held // K_BLOCK:
+                s = slice(b * K_BLOCK, (b + 1) * K_BLOCK)
+                tickets.append(ctx.submit_block(coil, c[s], h[s], d, 1e6, warm_start=warm))
+            r = ctx.finish_block(tickets.pop(0))
+            its += r["iterations"].tolist()
+            rel0 += r["init_relres"].tolist()
+        return its, rel0
+
+    sweep(True)  # graphs
+    ms_w, (its_w, rel_w) = _device_ms(stream, lambda: sweep(True))
+    ms_z, (its_z, _) = _device_ms(stream, lambda: sweep(False))
+    return {"what": f"{n_held} held-out cap poses, blocks of 8, rel.res 1e-8, harmonic recovery off (summary only)",
+            "n_train": n_train, "iterations_learned": round(float(np.mean(its_w)), 3),
+            "iterations_zero_guess": round(float(np.mean(its_z)), 3),
+            "init_relres_median": round(float(np.median(rel_w)), 5), "init_relres_max": round(float(np.max(rel_w)), 5),
+            "guess_kept_fraction": round(float(np.mean(np.array(rel_w) < 1.0)), 4),
+            "placements_per_s_learned": round(n_held / (ms_w / 1e3), 1),
+            "placements_per_s_zero_guess": round(n_held / (ms_z / 1e3), 1)}
+
+
+def config_conductivity_3_5m(local: int, with_oracle: bool, n_draws: int = 512, seed: int = 0) -> dict:
+    """The conductivity study at 3.5M tets: the ten-tissue sphere at 1.73 mm (90 mm), four cap
+    placements, 512 draws with every tissue lognormal (median = table value, log-sd 0.25), mixed
+    precision (FP64 PCG over the FP32 V-cycle) to rel.res 1e-8, harmonic recovery. Device time of
+    the draws; the distribution of each placement's gray-matter peak |E| and p99 over the draws; the
+    first two draws of the first placement against the FP64 oracle assembled with their tables (rank 0)."""
+    import torch
+
+    from cunibs_b200 import _native
+    from cunibs_b200.synthetic import cap_placements
+    from cunibs_b200.uq import nominal_sigma_table
+
+    mesh = sphere_head(1.73, 90.0, EIGHT_SHELLS, (EYE_CAP, MUSCLE_CAP), jitter_mm=0.2, seed=0)
+    coil = figure8_coil(2048)
+    poses = cap_placements(90.0, 4, 40.0, seed=21)
+    c = np.stack([p[0] for p in poses])
+    h = np.stack([p[1] for p in poses])
+    p = _native.default_params()
+    p.device = local
+    p.tolerance = TOL
+    ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+    nominal = nominal_sigma_table()
+    tags = tuple(range(1, 11))
+    rng = np.random.default_rng(seed)
+    sig = nominal[list(tags)] * np.exp(0.25 * rng.standard_normal((n_draws, len(tags))))
+    ctx.solve_block(coil, c, h, [4.0] * 4, 1e6, recovery="harmonic")  # recovery operator and graphs
+    begin_ms, _ = _device_ms(stream, lambda: ctx.sigma_begin(coil, c, h, [4.0] * 4, 1e6, nominal, tags,
+                                                               magnitude=True, recovery="harmonic"))
+    first = []
+    try:
+        def draws():
+            peaks, p99, its, resetups = [], [], [], 0
+            for i, s in enumerate(sig):
+                r = ctx.sigma_draw(s)
+                peaks.append(r["summary"][:, 0].copy())
+                p99.append(r["summary"][:, 12].copy())
+                its.append(float(r["iterations"].mean()))
+                resetups += int(r["resetup"])
+                if i < 2:
+                    first.append((r["magnE"][0].copy(), float(r["summary"][0][0])))
+            return np.array(peaks), np.array(p99), its, resetups
+        ms, (peaks, p99, its, resetups) = _device_ms(stream, draws)
+    finally:
+        ctx.sigma_end()
+    q = lambda a: {"mean": float(f"{a.mean():.6g}"), "std": float(f"{a.std():.6g}"),  # noqa: E731
+                   "p5": float(f"{np.percentile(a, 5):.6g}"), "p50": float(f"{np.percentile(a, 50):.6g}"),
+                   "p95": float(f"{np.percentile(a, 95):.6g}")}
+    out = {"what": f"3.5M-tet ten-tissue head, 4 cap placements x {n_draws} draws (all 10 tissues lognormal, "
+                   "log-sd 0.25), rel.res 1e-8, harmonic recovery", "n_tets": int(mesh.n_tets),
+           "begin_ms": round(begin_ms, 2), "ms_per_draw": round(ms / n_draws, 3),
+           "draws_per_s": round(n_draws / (ms / 1e3), 2), "placement_draws_per_s": round(4 * n_draws / (ms / 1e3), 1),
+           "iterations_mean": round(float(np.mean(its)), 2), "full_resetups": resetups,
+           "gm_peak_magnE": [q(peaks[:, j]) for j in range(4)], "gm_p99_magnE": [q(p99[:, j]) for j in range(4)]}
+    if with_oracle:
+        from oracle import Oracle, OracleParams
+
+        worst_rel, worst_peak = 0.0, 0.0
+        tet_tags = ctx.array("tet_tags")
+        for i, (m, pk) in enumerate(first):
+            table = nominal.copy()
+            table[list(tags)] = sig[i]
+            ref = Oracle(mesh, OracleParams(sigma_by_tag=tuple(table))).solve(
+                coil, c[:1], h[:1], [4.0], 1e6, tolerance=1e-12, recovery="harmonic")
+            rel, peak = _gm_parity(m, pk, ref, tet_tags)
+            worst_rel, worst_peak = max(worst_rel, rel), max(worst_peak, peak)
+        out["parity_first_draws"] = {"draws": len(first), "gm_rel_l2": float(f"{worst_rel:.3e}"),
+                                     "peak_rel": float(f"{worst_peak:.3e}"), "bar": 1e-5}
+    ctx.close()
     return out
 
 
@@ -771,6 +1014,9 @@ def main() -> None:
     ap.add_argument("--hidden", type=int, default=512, help="width of the warm-start network's hidden layers")
     ap.add_argument("--epochs", type=int, default=400, help="training epochs of the warm-start network")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--configs", choices=["all", "none"], default="all",
+                    help="also measure the other benchmark configurations (small plain case, uneven subjects, "
+                         "held-out learned guess, conductivity study at 3.5M tets)")
     args = ap.parse_args()
     line = run_reference(args) if args.impl == "reference" else run_ours(args)
     if line is not None:

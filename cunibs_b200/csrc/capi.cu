@@ -1576,7 +1576,7 @@ int cunibs_select_size4(int n, const int* row_ptr, const int* col_idx, const flo
         rp.upload(row_ptr, n + 1, s);
         ci.upload(col_idx, nnz, s);
         va.upload(values, nnz, s);
-        *n_coarse = select_size4(n, rp.get(), ci.get(), va.get(), agg.get(), s);
+        *n_coarse = select_size4(n, nnz, rp.get(), ci.get(), va.get(), agg.get(), s);
         agg.download(aggregates, n, s);
         CUNIBS_CHECK(cudaStreamSynchronize(s));
     });

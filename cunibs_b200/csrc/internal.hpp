@@ -143,7 +143,7 @@ void reduce_grounded(const Mesh& m, DevCsr<double>& out, cudaStream_t s);
 void reduce_grounded_values(const Mesh& m, const DevCsr<double>& pattern, double* out, cudaStream_t s);
 
 // Hierarchy (setup_amg.cu).
-int select_size4(int n, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s);
+int select_size4(int n, long nnz, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s);
 void build_hierarchy(Hierarchy& h, DevCsr<double>& a0, const Params& p, cudaStream_t s);
 // The finest level's l1 smoother weights and FP32 copies, after its FP64 values were rewritten in
 // place (queued on s, no synchronisation).
@@ -215,13 +215,21 @@ void reconstruct_block(const Mesh& m, const double* x_red /* (N-1,k_pad) */, int
                        cudaStream_t s);
 void scatter_potential(const Mesh& m, const double* x_red, int k, int k_pad, double* v /* (k,N) */, cudaStream_t s);
 constexpr int kSummaryLen = 16;
+// Workspace of the gray-matter summary (post.cu): fixed-point volumes of the mesh's gray matter,
+// the radix select's histograms, ranges and candidates, and the statistics' partial sums.
 struct SummaryWork {
-    DevArray<std::uint64_t> k64, k64_s;
-    DevArray<float> keys, keys_s;
-    DevArray<int> vals, vals_s, offsets;
-    DevArray<double> w_sorted, cw, tile_tot, part;
+    int wfix_n = -1;
+    DevArray<long long> wfix;
+    DevArray<unsigned char> sel_mesh, sel_state, edges;
+    DevArray<float> gv;
+    DevArray<unsigned> hcnt;
+    DevArray<unsigned long long> hw, cand;
+    DevArray<int> cand_n, ticket;
+    bool hist_clear = false;
+    int hist_k = 0;
+    DevArray<double> qval, part;
+    DevArray<long long> foc;
     DevArray<int> part_i;
-    DevArray<unsigned char> temp;
 };
 void gm_summary(const Mesh& m, const float* magnE, int k, double* summary_dev /* (k,16) */, SummaryWork& w,
                 cudaStream_t s);

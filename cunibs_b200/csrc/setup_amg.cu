@@ -59,205 +59,378 @@ T read_scalar(const T* dev, cudaStream_t s) {
 }
 
 // --- SIZE_4 aggregation -------------------------------------------------------------------
+//
+// The matching rules are the AMGx SIZE_4 selector's as the reference applies them (aggregate.cu):
+// edge weight |a_ij| / max(|a_ii|, |a_jj|) perturbed by a hash of the unordered pair; round 1
+// pairs rows with their strongest unpaired neighbour on a mutual choice, round 2 merges pairs
+// into quads the same way, leftovers join their strongest aggregated neighbour, and labels are
+// renumbered in order. What is this project's own is how it runs on the GPU:
+//
+// * Edge keys. Every CSR entry carries one 64-bit key, (bits of its weight) << 32 | (column + 1),
+//   or 0 when the entry can never be chosen (the diagonal, a column outside the level, a NaN
+//   weight). Weights are >= 0, whose IEEE bit patterns order like the values, so "strongest
+//   neighbour, highest column on equal weight" is the plain maximum of the eligible keys, and
+//   key 0 is "no neighbour". A scan reads one word per entry.
+// * Group-per-row scans. G lanes (G from the level's mean row length) stride over a row's keys
+//   and combine their maxima with shuffles; the maximum of a set does not depend on the order it
+//   is taken in, so the result equals a sequential fold over the row.
+// * Device-side loop control. Each matching round is queued as its full schedule of iterations
+//   up front. The last block of an iteration's final kernel (ticket counter) adds up the rows
+//   left unmatched and sets the round's `done` word when the round's exit rule holds; every
+//   later kernel of the round reads `done` first and returns at once. The host waits only once,
+//   for the number of aggregates.
 
-__device__ __forceinline__ unsigned agg_hash(unsigned a, unsigned seed) {
-    a ^= seed;
-    a = (a + 0x7ed55d16u) + (a << 12);
-    a = (a ^ 0xc761c23cu) + (a >> 19);
-    a = (a + 0x165667b1u) + (a << 5);
-    a = (a ^ 0xd3a2646cu) + (a << 9);
-    a = (a + 0xfd7046c5u) + (a << 3);
-    a = (a ^ 0xb55a4f09u) + (a >> 16);
-    return a;
+// One step of the hash: x = (x op c) + (x shift s), op add or xor, shift left or right.
+struct HashStep {
+    bool use_xor;
+    unsigned c;
+    bool left;
+    int shift;
+};
+
+// Robert Jenkins' 32-bit integer hash (six add/xor-shift steps), seeded by xor: the perturbation
+// AMGx applies to edge weights, which the bit-exact partition requires as is.
+__device__ __forceinline__ unsigned pair_hash(unsigned lo, unsigned hi) {
+    constexpr HashStep steps[6] = {{false, 0x7ed55d16u, true, 12}, {true, 0xc761c23cu, false, 19},
+                                   {false, 0x165667b1u, true, 5},  {true, 0xd3a2646cu, true, 9},
+                                   {false, 0xfd7046c5u, true, 3},  {true, 0xb55a4f09u, false, 16}};
+    unsigned x = lo ^ hi;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const unsigned mixed = steps[k].use_xor ? (x ^ steps[k].c) : (x + steps[k].c);
+        x = mixed + (steps[k].left ? (x << steps[k].shift) : (x >> steps[k].shift));
+    }
+    return x;
 }
 
-__device__ __forceinline__ bool is_candidate(int col, int row, int n) {
-    return col != row && static_cast<unsigned>(col) < static_cast<unsigned>(n);
+__device__ __forceinline__ unsigned long long edge_key(float w, int col) {
+    return (static_cast<unsigned long long>(__float_as_uint(w)) << 32) | static_cast<unsigned>(col + 1);
 }
+__device__ __forceinline__ int key_col(unsigned long long k) { return static_cast<int>(k & 0xffffffffu) - 1; }
+__device__ __forceinline__ float key_weight(unsigned long long k) { return __uint_as_float(static_cast<unsigned>(k >> 32)); }
 
-// Lexicographic max of (weight, column) from (0, -1); NaN weights never win.
-__device__ __forceinline__ void best_take(float& bw, int& bc, float w, int col) {
-    if (w > bw || (w == bw && col > bc)) {
-        bw = w;
-        bc = col;
+// The lanes of this thread's row group (G consecutive lanes; the groups tile the warp). A group
+// leaves or stays as a whole, so its mask names exactly the lanes that take part.
+template <int G>
+__device__ __forceinline__ unsigned group_mask() {
+    if constexpr (G == 32) {
+        return 0xffffffffu;
+    } else {
+        return ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
     }
 }
 
-__device__ __forceinline__ void count_block(int pred, int* counter) {
-    const int n = __syncthreads_count(pred);
-    if (threadIdx.x == 0 && n) atomicAdd(counter, n);
+// Maximum over the G lanes of a row group.
+template <int G>
+__device__ __forceinline__ unsigned long long group_max(unsigned long long v) {
+    const unsigned m = group_mask<G>();
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) {
+        const unsigned long long u = __shfl_xor_sync(m, v, o, G);
+        v = u > v ? u : v;
+    }
+    return v;
 }
 
-__global__ void agg_diag_weights_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                        const float* __restrict__ va, float* __restrict__ diag) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// Loop control shared by the kernels of one matching round.
+struct MatchCtl {
+    int unmatched;  // rows left unmatched by the current iteration (summed by its blocks)
+    int arrived;    // blocks of the current iteration's final kernel that have added their count
+    int previous;   // rows left unmatched by the previous iteration (n before the first)
+    int done;       // 1 once the round's exit rule held
+};
+
+// Which rule ends a round: round 1 stops when every row is paired or an iteration pairs none;
+// round 2 also stops once fewer than 5% of the rows are left.
+enum class ExitRule { kPairs, kQuads };
+
+// Called by every thread of a block of a round's final kernel, `left` its row's "still unmatched".
+template <ExitRule R>
+__device__ void close_iteration(int left, int n, MatchCtl* ctl) {
+    __shared__ int block_left;
+    __shared__ bool last;
+    if (threadIdx.x == 0) block_left = 0;
+    __syncthreads();
+    if (left) atomicAdd(&block_left, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (block_left) atomicAdd(&ctl->unmatched, block_left);
+        __threadfence();
+        last = atomicAdd(&ctl->arrived, 1) == static_cast<int>(gridDim.x) - 1;
+    }
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        const int now = atomicAdd(&ctl->unmatched, 0);
+        bool stop = now == 0 || now == ctl->previous;
+        if (R == ExitRule::kQuads) stop = stop || static_cast<float>(now) / static_cast<float>(n) < 0.05f;
+        ctl->previous = now;
+        ctl->unmatched = 0;
+        ctl->arrived = 0;
+        if (stop) ctl->done = 1;
+    }
+}
+
+__global__ void match_ctl_reset_kernel(MatchCtl* ctl, int n) {
+    ctl->unmatched = 0;
+    ctl->arrived = 0;
+    ctl->previous = n;
+    ctl->done = 0;
+}
+
+// |diagonal| of every row (0 when the row stores none): the first diagonal entry the row holds.
+template <int G>
+__global__ void row_diag_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                const float* __restrict__ va, float* __restrict__ adiag) {
+    const int lane = threadIdx.x % G;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    const unsigned gmask = group_mask<G>();
+    if (row >= n) return;  // whole groups leave together (n rows x G lanes)
     float d = 0.0f;
-    for (int j = rp[i]; j < rp[i + 1]; ++j)
-        if (ci[j] == i) {
-            d = va[j];
+    for (int base = rp[row]; base < rp[row + 1]; base += G) {
+        const int j = base + lane;
+        const bool hit = j < rp[row + 1] && ci[j] == row;
+        const unsigned m = __ballot_sync(gmask, hit) & gmask;
+        if (m) {
+            const int first = __ffs(m) - 1;  // lowest lane: the first such entry of the row
+            d = __shfl_sync(gmask, hit ? va[j] : 0.0f, first & (G - 1), G);
             break;
         }
-    diag[i] = d;
+    }
+    if (lane == 0) adiag[row] = fabsf(d);
 }
 
-// w_ij = |a_ij| / max(|a_ii|, |a_jj|), perturbed by a hash of the unordered pair to break ties.
-__global__ void agg_edge_weight_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                       const float* __restrict__ va, const float* __restrict__ diag,
-                                       float* __restrict__ w) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float di = fabsf(diag[i]);
-    for (int j = rp[i]; j < rp[i + 1]; ++j) {
-        const int jc = ci[j];
-        if (!is_candidate(jc, i, n)) {
-            w[j] = -1.0f;
-            continue;
+// The edge keys of every entry of a row.
+__global__ void edge_keys_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                 const float* __restrict__ va, const float* __restrict__ adiag,
+                                 unsigned long long* __restrict__ key) {
+    const int row = blockIdx.x * blockDim.x + threadIdx.x;
+    if (row >= n) return;
+    const float di = adiag[row];
+    for (int j = rp[row]; j < rp[row + 1]; ++j) {
+        const int c = ci[j];
+        unsigned long long k = 0;
+        if (c != row && static_cast<unsigned>(c) < static_cast<unsigned>(n)) {
+            const float ed = fabsf(va[j]) / fmaxf(di, adiag[c]);
+            const unsigned h = pair_hash(static_cast<unsigned>(min(row, c)), static_cast<unsigned>(max(row, c)));
+            const float frac = 1e-5f * static_cast<float>(h) / 4294967295.0f;
+            const float w = __fmaf_rn(frac, ed, ed);
+            if (!(w != w)) k = edge_key(w, c);  // a NaN weight never wins
         }
-        const float den = fmaxf(di, fabsf(diag[jc]));
-        const float ed = fabsf(va[j]) / den;
-        const unsigned lo = static_cast<unsigned>(min(i, jc));
-        const unsigned hi = static_cast<unsigned>(max(i, jc));
-        const float frac = 1e-5f * static_cast<float>(agg_hash(lo, hi)) / 4294967295.0f;
-        w[j] = __fmaf_rn(frac, ed, ed);
+        key[j] = k;
     }
 }
 
-__global__ void agg_init_kernel(int n, int* __restrict__ agg, int* __restrict__ partner, int* __restrict__ strongest) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    agg[i] = i;
-    partner[i] = -1;
-    strongest[i] = -1;
+__global__ void match_init_kernel(int n, int* __restrict__ agg, int* __restrict__ partner, int* __restrict__ choice) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    agg[t] = t;
+    partner[t] = -1;
+    choice[t] = -1;
 }
 
-__global__ void agg_r1_find_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                   const float* __restrict__ w, const int* __restrict__ partner,
-                                   int* __restrict__ strongest) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n || partner[t] != -1) return;
-    float bw = 0.0f;
-    int bc = -1;
-    for (int j = rp[t]; j < rp[t + 1]; ++j) {
-        const int jc = ci[j];
-        if (!is_candidate(jc, t, n) || partner[jc] != -1) continue;
-        best_take(bw, bc, w[j], jc);
+// Round 1, propose: an unpaired row names its strongest unpaired neighbour. A row that sees none
+// keeps its earlier proposal (the reference's behaviour, which gives a coarser hierarchy).
+template <int G>
+__global__ void pair_propose_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
+                                    const unsigned long long* __restrict__ key, const int* __restrict__ partner,
+                                    int* __restrict__ choice, const MatchCtl* __restrict__ ctl) {
+    if (ctl->done) return;
+    const int lane = threadIdx.x % G;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    if (row >= n || partner[row] != -1) return;  // whole groups leave together
+    unsigned long long best = 0;
+    for (int j = rp[row] + lane; j < rp[row + 1]; j += G) {
+        const unsigned long long k = key[j];
+        if (k > best && partner[key_col(k)] == -1) best = k;
     }
-    if (bc != -1) strongest[t] = bc;
+    best = group_max<G>(best);
+    if (lane == 0 && best) choice[row] = key_col(best);
 }
 
-__global__ void agg_r1_match_kernel(int n, int* __restrict__ partner, int* __restrict__ agg,
-                                    const int* __restrict__ strongest, int* __restrict__ remaining) {
+// Round 1, accept: two rows that named each other become a pair labelled by the smaller index.
+__global__ void pair_accept_kernel(int n, int* __restrict__ partner, int* __restrict__ agg,
+                                   const int* __restrict__ choice, MatchCtl* __restrict__ ctl) {
+    if (ctl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int un = 0;
+    int left = 0;
     if (t < n && partner[t] == -1) {
-        const int pm = strongest[t];
-        if (pm != -1 && strongest[pm] == t) {
-            partner[t] = pm;
-            agg[t] = min(pm, t);
+        const int c = choice[t];
+        if (c != -1 && choice[c] == t) {
+            partner[t] = c;
+            agg[t] = min(t, c);
         } else {
-            un = 1;
+            left = 1;
         }
     }
-    count_block(un, remaining);
+    close_iteration<ExitRule::kPairs>(left, n, ctl);
 }
 
-__global__ void agg_r2_init_kernel(int n, int* __restrict__ partner, float* __restrict__ wsn,
-                                   int* __restrict__ aggregated) {
+// Between the rounds: unpaired rows pair with themselves; nothing is merged yet.
+__global__ void quad_init_kernel(int n, int* __restrict__ partner, float* __restrict__ offer,
+                                 int* __restrict__ merged) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     if (partner[t] == -1) partner[t] = t;
-    wsn[t] = -1.0f;
-    aggregated[t] = -1;
+    offer[t] = -1.0f;
+    merged[t] = -1;
 }
 
-__global__ void agg_r2_find_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                   const float* __restrict__ w, const int* __restrict__ aggregated,
-                                   const int* __restrict__ agg, const int* __restrict__ partner,
-                                   int* __restrict__ strongest, float* __restrict__ wsn) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n || aggregated[t] != -1) return;
-    const int p = partner[t];
-    float bw = 0.0f;
-    int bc = -1;
-    for (int j = rp[t]; j < rp[t + 1]; ++j) {
-        const int jc = ci[j];
-        if (!is_candidate(jc, t, n)) continue;
-        if (aggregated[jc] != -1 || jc == p) continue;
-        best_take(bw, bc, w[j], jc);
+// Round 2, propose: a row of an unmerged pair names the pair of its strongest unmerged neighbour
+// outside its own pair, and records that edge's weight as its offer.
+template <int G>
+__global__ void quad_propose_kernel(int n, const int* __restrict__ rp, const unsigned long long* __restrict__ key,
+                                    const int* __restrict__ merged, const int* __restrict__ agg,
+                                    const int* __restrict__ partner, int* __restrict__ choice,
+                                    float* __restrict__ offer, const MatchCtl* __restrict__ ctl) {
+    if (ctl->done) return;
+    const int lane = threadIdx.x % G;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    if (row >= n || merged[row] != -1) return;  // whole groups leave together
+    const int mate = partner[row];
+    unsigned long long best = 0;
+    for (int j = rp[row] + lane; j < rp[row + 1]; j += G) {
+        const unsigned long long k = key[j];
+        if (k <= best) continue;
+        const int c = key_col(k);
+        if (c != mate && merged[c] == -1) best = k;
     }
-    if (bc != -1) {
-        wsn[t] = bw;
-        strongest[t] = agg[bc];
-    }
-}
-
-// Both members of a pair adopt one proposal. Row t writes its own slot only, and reads its
-// partner's only when the partner's proposal is strictly stronger, in which case the partner
-// writes nothing: the read never races a write.
-__global__ void agg_r2_agree_kernel(int n, int* __restrict__ aggregated, int* __restrict__ strongest,
-                                    const float* __restrict__ wsn, const int* __restrict__ partner) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n || aggregated[t] != -1) return;
-    const int p = partner[t];
-    const float mine = wsn[t];
-    const float theirs = (p != -1) ? wsn[p] : -1.0f;
-    if (mine < 0.0f && theirs < 0.0f) {
-        aggregated[t] = 1;
-        strongest[t] = -1;
-    } else if (mine < theirs) {
-        strongest[t] = strongest[p];
+    best = group_max<G>(best);
+    if (lane == 0 && best) {
+        offer[row] = key_weight(best);
+        choice[row] = agg[key_col(best)];
     }
 }
 
-__global__ void agg_r2_match_kernel(int n, int* __restrict__ agg, int* __restrict__ aggregated,
-                                    const int* __restrict__ strongest, int* __restrict__ remaining) {
+// Round 2, settle: the two rows of a pair adopt the stronger of their two proposals; a pair whose
+// rows both have no offer stops here as a pair. A row reads its mate's choice only when the
+// mate's offer is strictly stronger, and then the mate writes nothing, so no read races a write.
+__global__ void quad_settle_kernel(int n, int* __restrict__ merged, int* __restrict__ choice,
+                                   const float* __restrict__ offer, const int* __restrict__ partner,
+                                   const MatchCtl* __restrict__ ctl) {
+    if (ctl->done) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int un = 0;
-    if (t < n && aggregated[t] == -1) {
-        const int pm = strongest[t];
-        const int mine = agg[t];
-        if (pm != -1 && strongest[pm] == mine) {
-            aggregated[t] = 1;
-            agg[t] = min(pm, mine);
+    if (t >= n || merged[t] != -1) return;
+    const int mate = partner[t];
+    const float own = offer[t];
+    const float other = mate != -1 ? offer[mate] : -1.0f;
+    if (own < 0.0f && other < 0.0f) {
+        merged[t] = 1;
+        choice[t] = -1;
+    } else if (own < other) {
+        choice[t] = choice[mate];
+    }
+}
+
+// Round 2, accept: two pairs that named each other merge, labelled by the smaller label.
+__global__ void quad_accept_kernel(int n, int* __restrict__ agg, int* __restrict__ merged,
+                                   const int* __restrict__ choice, MatchCtl* __restrict__ ctl) {
+    if (ctl->done) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    int left = 0;
+    if (t < n && merged[t] == -1) {
+        const int c = choice[t];
+        const int label = agg[t];
+        if (c != -1 && choice[c] == label) {
+            merged[t] = 1;
+            agg[t] = min(c, label);
         } else {
-            un = 1;
+            left = 1;
         }
     }
-    count_block(un, remaining);
+    close_iteration<ExitRule::kQuads>(left, n, ctl);
 }
 
-__global__ void agg_merge_kernel(int n, const int* __restrict__ rp, const int* __restrict__ ci,
-                                 const float* __restrict__ w, const int* __restrict__ agg,
-                                 const int* __restrict__ aggregated, int* __restrict__ cand) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n || aggregated[t] != -1) return;
-    float bw = 0.0f;
-    int bc = -1;
-    for (int j = rp[t]; j < rp[t + 1]; ++j) {
-        const int jc = ci[j];
-        if (!is_candidate(jc, t, n) || aggregated[jc] == -1) continue;
-        best_take(bw, bc, w[j], jc);
+// Leftovers (rows still unmerged when round 2 ended): each picks the label of its strongest merged
+// neighbour, or its own index when it has none; the picks are applied in a second kernel so every
+// row sees the same merged set.
+template <int G>
+__global__ void leftover_pick_kernel(int n, const int* __restrict__ rp, const unsigned long long* __restrict__ key,
+                                     const int* __restrict__ agg, const int* __restrict__ merged,
+                                     int* __restrict__ pick) {
+    const int lane = threadIdx.x % G;
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) / G;
+    if (row >= n || merged[row] != -1) return;  // whole groups leave together
+    unsigned long long best = 0;
+    for (int j = rp[row] + lane; j < rp[row + 1]; j += G) {
+        const unsigned long long k = key[j];
+        if (k > best && merged[key_col(k)] != -1) best = k;
     }
-    cand[t] = (bc != -1) ? agg[bc] : t;
+    best = group_max<G>(best);
+    if (lane == 0) pick[row] = best ? agg[key_col(best)] : row;
 }
 
-__global__ void agg_join_kernel(int n, int* __restrict__ agg, int* __restrict__ aggregated, const int* __restrict__ cand) {
+__global__ void leftover_apply_kernel(int n, int* __restrict__ agg, int* __restrict__ merged,
+                                      const int* __restrict__ pick) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n && aggregated[t] == -1) {
-        agg[t] = cand[t];
-        aggregated[t] = 1;
+    if (t < n && merged[t] == -1) {
+        agg[t] = pick[t];
+        merged[t] = 1;
     }
 }
 
-__global__ void agg_mark_kernel(int n, const int* __restrict__ agg, int* __restrict__ used) {
+// Labels in use, then each row's label replaced by the number of used labels below it.
+__global__ void label_used_kernel(int n, const int* __restrict__ agg, int* __restrict__ used) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) used[agg[t]] = 1;
 }
 
-__global__ void agg_relabel_kernel(int n, int* __restrict__ agg, const int* __restrict__ excl) {
+__global__ void label_renumber_kernel(int n, int* __restrict__ agg, const int* __restrict__ below) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) agg[t] = excl[agg[t]];
+    if (t < n) agg[t] = below[agg[t]];
+}
+
+// Lanes per row of the scanning kernels, from the level's mean row length.
+int group_lanes(int n, long nnz) {
+    const double per = n > 0 ? static_cast<double>(nnz) / n : 0.0;
+    return per <= 12.0 ? 4 : per <= 24.0 ? 8 : per <= 48.0 ? 16 : 32;
+}
+
+unsigned group_grid(int n, int G) {
+    const long threads = static_cast<long>(n) * G;
+    return static_cast<unsigned>((threads + kBlock - 1) / kBlock);
+}
+
+// Runs the whole selection on `s` and returns the number of aggregates (the one host wait).
+template <int G>
+int run_matching(int n, long nnz, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s) {
+    constexpr int kMaxIterations = 16;  // per round, as the reference's selector
+    const unsigned rows = grid_for(n), groups = group_grid(n, G);
+    DevArray<float> adiag(n), offer(n);
+    DevArray<unsigned long long> key(nnz > 0 ? nnz : 1);
+    DevArray<int> partner(n), choice(n), merged(n), pick(n), used(n + 1), below(n + 1);
+    DevArray<MatchCtl> ctl(1);
+    row_diag_kernel<G><<<groups, kBlock, 0, s>>>(n, rp, ci, va, adiag.get()); count_launch();
+    edge_keys_kernel<<<rows, kBlock, 0, s>>>(n, rp, ci, va, adiag.get(), key.get()); count_launch();
+    match_init_kernel<<<rows, kBlock, 0, s>>>(n, agg, partner.get(), choice.get()); count_launch();
+    match_ctl_reset_kernel<<<1, 1, 0, s>>>(ctl.get(), n); count_launch();
+    CUNIBS_LAUNCH_CHECK("aggregation set-up");
+    for (int it = 0; it < kMaxIterations; ++it) {
+        pair_propose_kernel<G><<<groups, kBlock, 0, s>>>(n, rp, ci, key.get(), partner.get(), choice.get(), ctl.get());
+        pair_accept_kernel<<<rows, kBlock, 0, s>>>(n, partner.get(), agg, choice.get(), ctl.get());
+        count_launch(2);
+    }
+    CUNIBS_LAUNCH_CHECK("aggregation pairs");
+    quad_init_kernel<<<rows, kBlock, 0, s>>>(n, partner.get(), offer.get(), merged.get()); count_launch();
+    match_ctl_reset_kernel<<<1, 1, 0, s>>>(ctl.get(), n); count_launch();
+    for (int it = 0; it < kMaxIterations; ++it) {
+        quad_propose_kernel<G><<<groups, kBlock, 0, s>>>(n, rp, key.get(), merged.get(), agg, partner.get(),
+                                                          choice.get(), offer.get(), ctl.get());
+        quad_settle_kernel<<<rows, kBlock, 0, s>>>(n, merged.get(), choice.get(), offer.get(), partner.get(), ctl.get());
+        quad_accept_kernel<<<rows, kBlock, 0, s>>>(n, agg, merged.get(), choice.get(), ctl.get());
+        count_launch(3);
+    }
+    CUNIBS_LAUNCH_CHECK("aggregation quads");
+    // With no row left unmerged both kernels find nothing to do.
+    leftover_pick_kernel<G><<<groups, kBlock, 0, s>>>(n, rp, key.get(), agg, merged.get(), pick.get());
+    leftover_apply_kernel<<<rows, kBlock, 0, s>>>(n, agg, merged.get(), pick.get());
+    count_launch(2);
+    used.zero(s);
+    label_used_kernel<<<rows, kBlock, 0, s>>>(n, agg, used.get()); count_launch();
+    exclusive_scan(used.get(), below.get(), n + 1, s);
+    label_renumber_kernel<<<rows, kBlock, 0, s>>>(n, agg, below.get()); count_launch();
+    CUNIBS_LAUNCH_CHECK("aggregation labels");
+    return read_scalar(below.get() + n, s);
 }
 
 // --- sparse products ----------------------------------------------------------------------
@@ -493,7 +666,7 @@ int aggregate_level(const DevCsr<double>& a, const Params& prm, DevArray<int>& a
         DevArray<float> v32(cur->nnz ? cur->nnz : 1);
         to_f32_kernel<<<grid_for(cur->nnz), kBlock, 0, s>>>(cur->val.get(), cur->nnz, v32.get()); count_launch();
         DevArray<int> step(cur->n);
-        const int nc = select_size4(cur->n, cur->ptr.get(), cur->col.get(), v32.get(), step.get(), s);
+        const int nc = select_size4(cur->n, cur->nnz, cur->ptr.get(), cur->col.get(), v32.get(), step.get(), s);
         if (nc == cur->n || nc < prm.min_coarse_rows) break;
         if (!have) {
             agg.resize(a.n);
@@ -521,54 +694,14 @@ void to_f32(const DevArray<double>& in, long n, DevArray<float>& out, cudaStream
 
 }  // namespace
 
-int select_size4(int n, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s) {
+int select_size4(int n, long nnz, const int* rp, const int* ci, const float* va, int* agg, cudaStream_t s) {
     if (n <= 0) return 0;
-    const int nnz = read_scalar(rp + n, s);
-    DevArray<float> diag(n), w(nnz > 0 ? nnz : 1), wsn(n);
-    DevArray<int> partner(n), strongest(n), aggregated(n), cand(n), counter(1), used(n + 1), excl(n + 1);
-    const unsigned blocks = grid_for(n);
-    agg_diag_weights_kernel<<<blocks, kBlock, 0, s>>>(n, rp, ci, va, diag.get()); count_launch();
-    if (nnz > 0) {
-        agg_edge_weight_kernel<<<blocks, kBlock, 0, s>>>(n, rp, ci, va, diag.get(), w.get());
-        count_launch();
+    switch (group_lanes(n, nnz)) {
+        case 4: return run_matching<4>(n, nnz, rp, ci, va, agg, s);
+        case 8: return run_matching<8>(n, nnz, rp, ci, va, agg, s);
+        case 16: return run_matching<16>(n, nnz, rp, ci, va, agg, s);
+        default: return run_matching<32>(n, nnz, rp, ci, va, agg, s);
     }
-    agg_init_kernel<<<blocks, kBlock, 0, s>>>(n, agg, partner.get(), strongest.get()); count_launch();
-    CUNIBS_LAUNCH_CHECK("aggregation init");
-    int unassigned = n;
-    for (int iter = 0; iter <= 15; ++iter) {
-        counter.zero(s);
-        agg_r1_find_kernel<<<blocks, kBlock, 0, s>>>(n, rp, ci, w.get(), partner.get(), strongest.get()); count_launch();
-        agg_r1_match_kernel<<<blocks, kBlock, 0, s>>>(n, partner.get(), agg, strongest.get(), counter.get()); count_launch();
-        CUNIBS_LAUNCH_CHECK("aggregation round 1");
-        const int prev = unassigned;
-        unassigned = read_scalar(counter.get(), s);
-        if (unassigned == 0 || unassigned == prev) break;
-    }
-    agg_r2_init_kernel<<<blocks, kBlock, 0, s>>>(n, partner.get(), wsn.get(), aggregated.get()); count_launch();
-    unassigned = n;
-    for (int iter = 0; iter <= 15; ++iter) {
-        counter.zero(s);
-        agg_r2_find_kernel<<<blocks, kBlock, 0, s>>>(n, rp, ci, w.get(), aggregated.get(), agg, partner.get(),
-                                                    strongest.get(), wsn.get()); count_launch();
-        agg_r2_agree_kernel<<<blocks, kBlock, 0, s>>>(n, aggregated.get(), strongest.get(), wsn.get(), partner.get()); count_launch();
-        agg_r2_match_kernel<<<blocks, kBlock, 0, s>>>(n, agg, aggregated.get(), strongest.get(), counter.get()); count_launch();
-        CUNIBS_LAUNCH_CHECK("aggregation round 2");
-        const int prev = unassigned;
-        unassigned = read_scalar(counter.get(), s);
-        if (unassigned == 0 || unassigned == prev ||
-            static_cast<float>(unassigned) / static_cast<float>(n) < 0.05f)
-            break;
-    }
-    if (unassigned != 0) {
-        agg_merge_kernel<<<blocks, kBlock, 0, s>>>(n, rp, ci, w.get(), agg, aggregated.get(), cand.get()); count_launch();
-        agg_join_kernel<<<blocks, kBlock, 0, s>>>(n, agg, aggregated.get(), cand.get()); count_launch();
-    }
-    used.zero(s);
-    agg_mark_kernel<<<blocks, kBlock, 0, s>>>(n, agg, used.get()); count_launch();
-    exclusive_scan(used.get(), excl.get(), n + 1, s);
-    agg_relabel_kernel<<<blocks, kBlock, 0, s>>>(n, agg, excl.get()); count_launch();
-    CUNIBS_LAUNCH_CHECK("aggregation relabel");
-    return read_scalar(excl.get() + n, s);
 }
 
 void spgemm(const DevCsr<double>& A, const DevCsr<double>& B, DevCsr<double>& C, cudaStream_t s) {

@@ -732,6 +732,10 @@ class Solver {
     VWork<double> v64;
     // Per-column scalars.
     DevArray<double> rz, alpha, beta, ref_sq, rr0, rel, eta, partials, r0sq, init_rel;
+    // The call's tolerance per column, written before every solve: the cached loop graphs read it
+    // from here, so a call with another tolerance than the one the graph was captured under still
+    // stops at its own.
+    DevArray<double> tolv;
     DevArray<int> frozen, outer_conv, conv_iter, iter_counter;
     DevArray<unsigned> counter;
     int* h_flags = nullptr;   // pinned
@@ -779,7 +783,7 @@ class Solver {
         v32.cx.resize(mc);
         v64.cb.resize(mc);
         v64.cx.resize(mc);
-        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta, &r0sq, &init_rel}) a->resize(K);
+        for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta, &r0sq, &init_rel, &tolv}) a->resize(K);
         for (auto* a : {&frozen, &outer_conv, &conv_iter}) a->resize(K);
         iter_counter.resize(1);
         cap.resize(1);
@@ -1188,7 +1192,8 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     start_columns_kernel<<<1, 32, 0, s>>>(ref_sq.get(), K, prm.max_iters, frozen.get(), conv_iter.get(), rel.get());
     count_launch();
     fill_kernel<<<1, 32, 0, s>>>(rz.get(), K, 1.0);
-    count_launch();
+    fill_kernel<<<1, 32, 0, s>>>(tolv.get(), K, prm.tolerance);
+    count_launch(2);
     if constexpr (narrow) {
         const std::int64_t count = static_cast<std::int64_t>(n) * K;
         narrow_kernel<double, TZ><<<grid_for(count), kBlock, 0, s>>>(count, R.get(), rv);
@@ -1200,7 +1205,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
     long long nodes = 0;
     const bool device_loop = run_while({key, K, 0}, [&](cudaGraphConditionalHandle hnd) {
         pcg_iteration<double, TZ, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(), AP.get(), rv,
-                                     zv, prm.tolerance, nullptr, ref_sq.get(), 1, hnd, 1);
+                                     zv, 0.0, tolv.get(), ref_sq.get(), 1, hnd, 1);
     }, &nodes);
     // The right-hand side norms (zero columns) and, after a device loop, its iteration count are
     // read with the caller's final readback: no host round trip of their own.
@@ -1218,7 +1223,7 @@ void Solver::solve_plain(int k, const Params& prm, SolveStats& st, bool warm) {
         for (int j = 0; j < m; ++j) {
             run_graph({key + 10, K, 0}, [&] {
                 pcg_iteration<double, TZ, K>(A.ptr.get(), A.col.get(), A.val.get(), X.get(), R.get(), P.get(),
-                                             AP.get(), rv, zv, prm.tolerance, nullptr, ref_sq.get(), 1);
+                                             AP.get(), rv, zv, 0.0, tolv.get(), ref_sq.get(), 1);
             });
         }
         it += m;

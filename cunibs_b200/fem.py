@@ -9,8 +9,13 @@ from typing import NamedTuple
 DEFAULT_TOLERANCE = 1e-6
 DEFAULT_MAX_ITERS = 2000
 BLOCK_SIZES = (1, 2, 4, 8, 16)
-# Widest block the Subject API chunks a sweep into (the reference's MAX_BLOCK is 8).
+# Widest block the Subject API chunks a sweep into for an explicit block_k (the reference's
+# MAX_BLOCK is 8).
 MAX_BLOCK = 8
+# Widest block the native solver takes (cunibs_solve_opts.block_width). A sweep called with
+# block_k=None may run this wide once the autotuner has chosen it: a placement's result does not
+# depend on the block width, bit for bit.
+SWEEP_MAX_BLOCK = 16
 
 TISSUE_CONDUCTIVITY: dict[int, float] = {
     1: 0.126, 2: 0.275, 3: 1.654, 4: 0.010, 5: 0.465, 6: 0.5, 7: 0.008, 8: 0.025, 9: 0.6, 10: 0.16,

@@ -57,6 +57,7 @@ from .fem import (  # noqa: E402
     DEFAULT_MAX_ITERS,
     DEFAULT_TOLERANCE,
     MAX_BLOCK,
+    SWEEP_MAX_BLOCK,
     SolverConvergenceError,
     validate_recovery,
 )
@@ -157,11 +158,12 @@ class Subject:
 
     def set_sweep_defaults(self, *, block_k: int | None = None, overlap_blocks_per_sm: int | None = None) -> None:
         """Settings that change no result bit: the block width of ``block_k=None`` sweeps (1 to
-        MAX_BLOCK) and the dA/dt blocks per SM that run beside a solve (1 to 16)."""
+        SWEEP_MAX_BLOCK, 16: wider than an explicit block_k may ask, since the result does not
+        depend on it) and the dA/dt blocks per SM that run beside a solve (1 to 16)."""
         with self._lock:
             if block_k is not None:
-                if not 1 <= int(block_k) <= MAX_BLOCK:
-                    raise ValueError(f"block_k must be in [1, {MAX_BLOCK}]")
+                if not 1 <= int(block_k) <= SWEEP_MAX_BLOCK:
+                    raise ValueError(f"block_k must be in [1, {SWEEP_MAX_BLOCK}]")
                 self._block_k_default = int(block_k)
             if overlap_blocks_per_sm is not None:
                 if not 1 <= int(overlap_blocks_per_sm) <= 16:

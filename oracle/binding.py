@@ -28,6 +28,8 @@ class _Params(C.Structure):
         ("cheby_degree", C.c_int),
         ("cheby_lower_ratio", C.c_double),
         ("n_threads", C.c_int),
+        ("has_sigma", C.c_int),
+        ("sigma_by_tag", C.c_double * 11),
     ]
 
 
@@ -39,6 +41,7 @@ class OracleParams:
     cheby_degree: int = 2
     cheby_lower_ratio: float = 12.0
     n_threads: int = 0
+    sigma_by_tag: tuple[float, ...] | None = None  # 11 entries indexed by tag: a conductivity draw
 
 
 def build_oracle() -> Path:
@@ -89,7 +92,9 @@ class Oracle:
     def __init__(self, mesh, params: OracleParams | None = None) -> None:
         lib = _load()
         p = params or OracleParams()
-        cp = _Params(p.min_coarse_rows, p.max_levels, p.agg_rounds, p.cheby_degree, p.cheby_lower_ratio, p.n_threads)
+        sig = (C.c_double * 11)(*(p.sigma_by_tag if p.sigma_by_tag is not None else [0.0] * 11))
+        cp = _Params(p.min_coarse_rows, p.max_levels, p.agg_rounds, p.cheby_degree, p.cheby_lower_ratio, p.n_threads,
+                     1 if p.sigma_by_tag is not None else 0, sig)
         err = C.create_string_buffer(512)
         nodes = np.ascontiguousarray(mesh.nodes_mm, dtype=np.float64)
         tets = np.ascontiguousarray(mesh.tet_nodes, dtype=np.int32)

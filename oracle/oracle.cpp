@@ -1437,6 +1437,8 @@ void orc_params_default(orc_params* p) {
     p->cheby_degree = 2;
     p->cheby_lower_ratio = 12.0;
     p->n_threads = 0;
+    p->has_sigma = 0;
+    for (double& v : p->sigma_by_tag) v = 0.0;
 }
 
 void* orc_ctx_create(const double* nodes_mm, int n_nodes, const int* tet_nodes, const int* tet_tags,
@@ -1488,6 +1490,7 @@ void* orc_ctx_create(const double* nodes_mm, int n_nodes, const int* tet_nodes, 
         for (int e = 0; e < n_tets; ++e) {
             c->cond[e] = tissue_sigma(c->tags[e]);
             if (std::isnan(c->cond[e])) throw std::invalid_argument("unknown tissue tag");
+            if (c->prm.has_sigma) c->cond[e] = c->prm.sigma_by_tag[c->tags[e]];  // a conductivity draw
         }
         node2corner(c->tets, 4, n_nodes, c->n2c_ptr, c->n2c_idx);
         c->stiff = assemble_stiffness(*c);

@@ -22,6 +22,8 @@ typedef struct {
     int cheby_degree;         /* fem/solve.py:167 SmootherParams.degree = 2 */
     double cheby_lower_ratio; /* fem/solve.py:168 = 12 */
     int n_threads;            /* OpenMP threads; <= 0 means all */
+    int has_sigma;            /* nonzero: conductivity per tag from sigma_by_tag, not the table */
+    double sigma_by_tag[11];  /* S/m indexed by tag (1..10); a conductivity draw */
 } orc_params;
 
 /* Summary layout shared with the CUDA C-ABI (cunibs_b200.h CUNIBS_SUMMARY_*). */

@@ -1,7 +1,7 @@
 """Failure contracts, made to happen on the host side or by a wait that runs out. Needs a B200.
 
 * Forward non-convergence (reference tests/test_block_solve.py:321-376, contract at
-  fem/solve.py:368-392,528-551): an unreachable tolerance with a small iteration budget makes every
+  fem/solve.py:368-392,528-551): a tolerance out of reach of a small iteration budget makes every
   column of a block miss; the library rebuilds the hierarchy at the operator's current values, retries
   in FP64 from the failed iterate, and then raises SolverConvergenceError naming the column. The
   subject stays usable afterwards.
@@ -42,8 +42,10 @@ def test_unreachable_tolerance_rebuilds_then_raises_block(small_sphere, precisio
     want = [r.magnE for r in good.iter_simulate(coil, sites, magnitude=True)]
     good.free()
 
-    # 1e-30 is out of reach in FP64 (PCG stalls near 1e-17) and 25 iterations are far too few.
-    subj = Subject(small_sphere, tolerance=1e-30, max_iters=25, precision=precision)
+    # Five iterations cannot reach 1e-12 (this head needs about 20), and neither can the FP64 retry's
+    # five. (A tiny tolerance with a larger budget is not enough: on a small head the recursively
+    # updated residual keeps falling far below machine precision, even to zero.)
+    subj = Subject(small_sphere, tolerance=1e-12, max_iters=5, precision=precision)
     ctx = subj.context
     builds = ctx.hierarchy_builds
     assert builds == 1
@@ -52,14 +54,14 @@ def test_unreachable_tolerance_rebuilds_then_raises_block(small_sphere, precisio
     err = excinfo.value
     assert ctx.hierarchy_builds == builds + 1, "the hierarchy was not rebuilt before the retry"
     assert err.column in range(len(sites)), "the failing column must be attributable"
-    assert err.tolerance == 1e-30
-    assert err.relative_residual > 0.0
-    assert err.iterations >= 25
-    assert ctx.pending() == 0  # the block submitted behind the failed one was dropped
+    assert err.tolerance == 1e-12
+    assert err.relative_residual > 1e-12
+    assert err.iterations >= 5
+    assert ctx.pending == 0  # nothing is left submitted
 
     # The subject still solves: a block at a reachable tolerance matches a fresh subject's.
     out = ctx.solve_block(coil, np.stack([s.center_mm for s in sites]), np.stack([s.handle_mm for s in sites]),
-                          [4.0] * len(sites), 1e6, tolerance=1e-8, max_iters=2000, magnitude=True,
+                          [4.0] * len(sites), 1e6, tolerance=1e-8, max_iters=2000, magnitude=True, recovery="harmonic",
                           precision={"split": _native.PREC_SPLIT, "plain": _native.PREC_PLAIN_FP64}[precision])
     assert (out["relative_residual"] <= 1e-8).all()
     for i in range(len(sites)):

@@ -329,3 +329,60 @@ def test_conductivity_keep_coarse_matches_full_resetup(sphere_mesh):
         assert np.linalg.norm(r[gm] - r0[gm]) / np.linalg.norm(r0[gm]) <= 1e-7
     full.free()
     kept.free()
+
+
+def test_hierarchy_rebuild_and_plain_solve_are_bit_reproducible(sphere_mesh):
+    """A full re-setup at unchanged conductivities rebuilds the same hierarchy bit for bit, and a
+    plain FP64 block solve gives the same field before it, twice in a row, and after it."""
+    from cunibs_b200.fem import TISSUE_CONDUCTIVITY
+
+    m = sphere_mesh
+    p = _native.default_params()
+    p.precision = _native.PREC_PLAIN_FP64
+    p.tolerance = 1e-8
+    ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris, p)
+    coil = figure8_coil(64)
+    c = np.array([[0.0, 0.0, 90.0], [10.0, 0.0, 89.4]])
+    h = c + [0.0, 50.0, 0.0]
+
+    def arrays():
+        out = {}
+        for lev in range(ctx.n_levels):
+            for name in ("a_val", "p_val", "dinv", "a_col", "agg"):
+                out[(name, lev)] = ctx.array(name, lev).copy()
+        return out
+
+    def field():
+        return ctx.solve_block(coil, c, h, [4.0, 4.0], 1e6, magnitude=True, recovery="harmonic")["magnE"].copy()
+
+    before, f0, f1 = arrays(), field(), field()
+    np.testing.assert_array_equal(f1, f0)
+    sigma = np.zeros(11)
+    for tag, s in TISSUE_CONDUCTIVITY.items():
+        sigma[tag] = s
+    ctx.set_conductivity(sigma)  # full rebuild at the same values
+    after = arrays()
+    for key in before:
+        np.testing.assert_array_equal(after[key], before[key], err_msg=str(key))
+    np.testing.assert_array_equal(field(), f0)
+    ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["split", "plain"])
+def test_per_call_tolerance_is_honoured_by_the_cached_loop_graph(sphere_mesh, precision):
+    """The PCG loop is captured once per block width and replayed; each call's own tolerance must
+    still govern it: loose, then tight, then loose again on one context, each stopping at its own."""
+    subj = Subject(sphere_mesh, tolerance=1e-8, precision=precision)
+    ctx = subj.context
+    coil = figure8_coil(64)
+    c = np.array([[0.0, 0.0, 90.0], [10.0, 0.0, 89.4]])
+    h = c + [0.0, 50.0, 0.0]
+    runs = {}
+    for tol in (1e-3, 1e-11, 1e-3):
+        r = ctx.solve_block(coil, c, h, [4.0, 4.0], 1e6, tolerance=tol, max_iters=500)
+        assert (r["relative_residual"] <= tol).all(), (tol, r["relative_residual"])
+        runs.setdefault(tol, []).append(r["iterations"].copy())
+    loose, tight = runs[1e-3][0], runs[1e-11][0]
+    assert (tight > loose + 5).all()
+    np.testing.assert_array_equal(runs[1e-3][1], loose)
+    subj.free()

@@ -98,3 +98,29 @@ def test_1m_head_block_of_8_vs_oracle(head_1m, precision):
         assert rel <= GM_REL_L2, f"placement {i}: GM rel-L2 {rel:.2e}"
         assert peak <= PEAK_REL, f"placement {i}: peak rel {peak:.2e}"
     subj.free()
+
+
+def test_summary_percentiles_at_full_size_vs_oracle(head_1m):
+    """The gray-matter summary (radix-selected percentiles, focality) on the 1M-tet head's ~330k
+    gray-matter elements, three fields in one call: continuous values, values rounded to 1/64
+    (long runs of ties, kept in element order), and a constant field."""
+    from cunibs_b200 import _native
+    from oracle import oracle_summary
+
+    m = head_1m
+    ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris)
+    orc = Oracle(m)
+    rng = np.random.default_rng(9)
+    f = np.empty((3, ctx.n_tets), np.float32)
+    f[0] = rng.gamma(2.0, 0.3, ctx.n_tets)
+    f[1] = np.round(rng.gamma(2.0, 0.3, ctx.n_tets) * 64.0) / 64.0
+    f[2] = 0.25
+    got = ctx.summary(f)
+    vols32 = orc.f64("vols").astype(np.float32)
+    bary, tags = orc.f64("bary").reshape(-1, 3), orc.i32("tet_tags")
+    for i in range(3):
+        want = oracle_summary(f[i], vols32, bary, tags)
+        np.testing.assert_allclose(got[i], want, rtol=1e-10, atol=0, err_msg=f"field {i}")
+    again = ctx.summary(f)
+    np.testing.assert_array_equal(again, got)  # reproducible run to run
+    ctx.close()

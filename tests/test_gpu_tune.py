@@ -34,3 +34,23 @@ def test_autotune_picks_a_measured_setting_and_changes_no_result():
     for a, b in zip(after, before):
         np.testing.assert_array_equal(a, b)
     subj.free()
+
+
+def test_sweep_sixteen_wide_matches_eight_wide_bitwise():
+    """A block_k=None sweep may run 16 placements per block (the native solver's widest), wider
+    than an explicit block_k may ask; every result is bitwise the 8-wide sweep's."""
+    subj = Subject(sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1), tolerance=1e-8)
+    coil = figure8_coil(64)
+    rng = np.random.default_rng(5)
+    sites = []
+    for _ in range(20):
+        th, ph = rng.uniform(0.0, 0.5), rng.uniform(0.0, 2 * np.pi)
+        c = 90.0 * np.array([np.sin(th) * np.cos(ph), np.sin(th) * np.sin(ph), np.cos(th)])
+        sites.append(Placement(c, c + [-50.0 * np.sin(ph), 50.0 * np.cos(ph), 0.0]))
+    eight = list(subj.iter_simulate(coil, sites, magnitude=True))
+    subj.set_sweep_defaults(block_k=16)
+    sixteen = list(subj.iter_simulate(coil, sites, magnitude=True))
+    for a, b in zip(sixteen, eight):
+        np.testing.assert_array_equal(a.magnE, b.magnE)
+        assert a.summary["distribution"] == b.summary["distribution"]
+    subj.free()

@@ -194,3 +194,30 @@ def test_mlp_restatement_gradients_match_finite_differences():
     lp, *_ = forward_backward(Wp, b, x, t, 8)
     lm, *_ = forward_backward(Wm, b, x, t, 8)
     assert dW[1][i, j] == pytest.approx((lp - lm) / (2 * h), rel=1e-3)
+
+
+def test_oracle_conductivity_table_parameter():
+    """The oracle's conductivity table: the default table given explicitly changes nothing bit for
+    bit; every conductivity scaled by one factor leaves |E| unchanged (it depends on ratios only);
+    one tissue changed moves it."""
+    from cunibs_b200.fem import TISSUE_CONDUCTIVITY
+    from cunibs_b200.synthetic import figure8_coil, sphere_head
+    from oracle import Oracle, OracleParams
+
+    mesh = sphere_head(10.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(32)
+    c = np.array([[0.0, 0.0, 90.0]])
+    h = c + [0.0, 50.0, 0.0]
+    table = [0.0] * 11
+    for tag, s in TISSUE_CONDUCTIVITY.items():
+        table[tag] = s
+    base = Oracle(mesh).solve(coil, c, h, [4.0], 1e6, tolerance=1e-12)["magnE"][0].astype(np.float64)
+    same = Oracle(mesh, OracleParams(sigma_by_tag=tuple(table))).solve(coil, c, h, [4.0], 1e6, tolerance=1e-12)
+    np.testing.assert_array_equal(same["magnE"][0], base)
+    scaled = Oracle(mesh, OracleParams(sigma_by_tag=tuple(2.5 * s for s in table))).solve(coil, c, h, [4.0], 1e6,
+                                                                                            tolerance=1e-12)
+    assert np.linalg.norm(scaled["magnE"][0] - base) / np.linalg.norm(base) <= 1e-8
+    bumped = list(table)
+    bumped[3] *= 3.0
+    moved = Oracle(mesh, OracleParams(sigma_by_tag=tuple(bumped))).solve(coil, c, h, [4.0], 1e6, tolerance=1e-12)
+    assert np.linalg.norm(moved["magnE"][0] - base) / np.linalg.norm(base) >= 1e-3

@@ -17,15 +17,17 @@ def subject():
 def test_sweep_defaults_are_validated(subject):
     assert subject.block_k_default == 8 and subject.overlap_blocks_per_sm == 2
     with pytest.raises(ValueError, match="block_k"):
-        subject.set_sweep_defaults(block_k=9)
+        subject.set_sweep_defaults(block_k=17)
     with pytest.raises(ValueError, match="overlap"):
         subject.set_sweep_defaults(overlap_blocks_per_sm=0)
     subject.set_sweep_defaults(block_k=4)
     assert subject.block_k_default == 4
+    subject.set_sweep_defaults(block_k=16)  # a block_k=None sweep may run wider than an explicit block_k
+    assert subject.block_k_default == 16
     subject.set_sweep_defaults(block_k=8)
 
 
-@pytest.mark.parametrize("kw, match", [(dict(widths=(0, 4)), "block widths"), (dict(widths=(16,)), "block widths"),
+@pytest.mark.parametrize("kw, match", [(dict(widths=(0, 4)), "block widths"), (dict(widths=(32,)), "block widths"),
                                        (dict(overlaps=(17,)), "overlaps"), (dict(repeats=0), "repeats")])
 def test_autotune_rejects_bad_candidates_before_any_work(subject, kw, match):
     with pytest.raises(ValueError, match=match):
