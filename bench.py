@@ -578,8 +578,17 @@ def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_d
         begin_runs.append((round(begin_ms, 3), round(1e3 * (time.perf_counter() - t0), 3)))
         if rep == 0:
             ctx.sigma_end()
+    guesses = {}
     try:
         new_ms, (new_its, rel0) = device_ms(study)
+        # The same draws from the nominal potential alone (what a predictor of the nominal solution
+        # per pose can give at best) and from zero, on the same kept hierarchy.
+        for mode in ("nominal", "zero"):
+            ctx.sigma_set_guess(mode)
+            g_ms, (g_its, g_rel0) = device_ms(study)
+            guesses[mode] = {"ms_per_draw": round(g_ms / n_draws, 4), "iterations": round(float(np.mean(g_its)), 2),
+                             "init_relres_max": round(max(g_rel0), 6)}
+        ctx.sigma_set_guess("subspace")
     finally:
         ctx.sigma_end()
     return {"what": f"{n_draws} draws x {k} placements, 10 tissues lognormal (median = table, log-sd 0.25)",
@@ -590,7 +599,10 @@ def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_d
             "keep_coarse_zero_guess_ms_per_draw": round(old_ms / n_draws, 4),
             "keep_coarse_iterations": round(float(np.mean(old_its)), 2),
             "placement_draws_per_s": round(k * n_draws / (new_ms / 1e3), 2),
-            "ratio": round(old_ms / new_ms, 3)}
+            "ratio": round(old_ms / new_ms, 3),
+            "guess_comparison": {"subspace": {"ms_per_draw": round(new_ms / n_draws, 4),
+                                              "iterations": round(float(np.mean(new_its)), 2),
+                                              "init_relres_max": round(max(rel0), 6)}, **guesses}}
 
 
 def adm_measure(ctx, coil, sites, stream) -> dict:

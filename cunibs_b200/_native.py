@@ -151,6 +151,7 @@ def load() -> C.CDLL:
                                 C.c_int, C.c_double, ip], C.c_int),
         "cunibs_sigma_draw": ([_vp, dp, C.POINTER(BlockOut), ip], C.c_int),
         "cunibs_sigma_end": ([_vp], C.c_int),
+        "cunibs_sigma_set_guess": ([_vp, C.c_int], C.c_int),
         "cunibs_sigma_coefficients": ([C.c_int, dp, dp, ip, C.c_double, dp, ip], C.c_int),
         "cunibs_adm_create": ([_vp, ip, dp, C.c_int, dp, C.c_int, C.c_double, C.c_int, ip, dp, C.POINTER(_vp)],
                               C.c_int),
@@ -508,6 +509,14 @@ class Context:
         res["outer_steps"] = out.outer_steps
         res["resetup"] = flag.value
         return res
+
+    def sigma_set_guess(self, mode: str) -> None:
+        """cunibs_sigma_set_guess: the initial guess of the following draws ("subspace", the default;
+        "nominal", the nominal potential alone; "zero")."""
+        codes = {"subspace": 0, "nominal": 1, "zero": 2}
+        if mode not in codes:
+            raise ValueError("guess mode must be 'subspace', 'nominal' or 'zero'")
+        check(self._lib.cunibs_sigma_set_guess(self.handle, codes[mode]))
 
     def sigma_end(self) -> None:
         """cunibs_sigma_end: close the study; the context is back at the nominal conductivities."""

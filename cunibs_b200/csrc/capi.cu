@@ -101,6 +101,7 @@ struct SigmaStudy {
     DevArray<double> S;      // (n_red, P, K) sensitivities
     std::vector<double> Z;   // (K, P, P): y_j = Z_j (sigma - sigma_nom)
     std::vector<int> rank;   // (k)
+    int guess_mode = 0;      // 0 subspace guess, 1 the nominal potential alone, 2 zero (cunibs_sigma_set_guess)
 };
 
 struct cunibs_context {
@@ -929,12 +930,14 @@ int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* 
             dsig[a] = sigma[a] - st.nominal[st.tags[a]];
         }
         SigmaDraw y{};
-        for (int j = 0; j < k; ++j)
-            for (int a = 0; a < P; ++a) {
-                double v = 0.0;
-                for (int t = 0; t < P; ++t) v += st.Z[(static_cast<std::size_t>(j) * P + a) * P + t] * dsig[t];
-                y.y[a * 16 + j] = v;
-            }
+        if (st.guess_mode == 0) {
+            for (int j = 0; j < k; ++j)
+                for (int a = 0; a < P; ++a) {
+                    double v = 0.0;
+                    for (int t = 0; t < P; ++t) v += st.Z[(static_cast<std::size_t>(j) * P + a) * P + t] * dsig[t];
+                    y.y[a * 16 + j] = v;
+                }
+        }
         DeviceGuard dg(c->device);
         Mesh& m = c->mesh;
         cudaStream_t s = c->stream;
@@ -947,7 +950,7 @@ int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* 
         BlockSlot& sl = c->slots[st.slot];
         sigma_combine(st.rhs.get(), P, static_cast<long>(n_red) * K, w, sl.B.get(), s);
         sl.X0.reserve(static_cast<std::size_t>(n_red) * K);
-        sigma_guess(st.x_nom.get(), st.S.get(), n_red, P, K, k, y, sl.X0.get(), s);
+        if (st.guess_mode != 2) sigma_guess(st.x_nom.get(), st.S.get(), n_red, P, K, k, y, sl.X0.get(), s);
         auto queue = [&] {
             PendingBlock pb;
             pb.slot = st.slot;
@@ -956,7 +959,7 @@ int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* 
             pb.has_handles = st.has_handles;
             pb.has_opts = st.has_opts;
             pb.opts = st.opts;
-            pb.x0_given = true;
+            pb.x0_given = st.guess_mode != 2;
             pb.ticket = c->next_ticket++;
             c->pending.push_back(pb);
             return pb.ticket;
@@ -988,6 +991,15 @@ int cunibs_sigma_draw(cunibs_context* c, const double* sigma, cunibs_block_out* 
         }
         block_outputs_host(c, done, ss, out);
         if (resetup) *resetup = redone;
+    });
+}
+
+int cunibs_sigma_set_guess(cunibs_context* c, int mode) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        require(c->study != nullptr, "no conductivity study is open (cunibs_sigma_begin)");
+        require(mode >= 0 && mode <= 2, "guess mode must be 0 (subspace), 1 (nominal potential) or 2 (zero)");
+        c->study->guess_mode = mode;
     });
 }
 

@@ -237,6 +237,12 @@ int cunibs_sigma_begin(cunibs_context* ctx, const double* dip_pos_m, const doubl
  * cunibs_solve_block (host buffers); out->init_relres is the guess's relative residual. */
 int cunibs_sigma_draw(cunibs_context* ctx, const double* sigma, cunibs_block_out* out, int* resetup);
 
+/* The initial guess of the following draws, for comparisons of guesses (the results are the same
+ * to the tolerance): 0 the sensitivity-subspace guess above (the default, the reference's
+ * _InitialGuess, run.py:105-200), 1 the nominal potential alone, 2 the zero guess. No counterpart
+ * in the reference. */
+int cunibs_sigma_set_guess(cunibs_context* ctx, int mode);
+
 /* Closes the study and returns the context to the nominal conductivities (the same operator and
  * hierarchy values as before cunibs_sigma_begin). A no-op when no study is open. */
 int cunibs_sigma_end(cunibs_context* ctx);

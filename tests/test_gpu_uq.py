@@ -238,3 +238,34 @@ def test_conductivity_draws_match_the_fp64_oracle_with_the_draws_table():
             assert np.linalg.norm(a - b) / np.linalg.norm(b) <= 1e-5
             assert abs(g["summary"][i][0] - ref["summary"][i][0]) <= 1e-5 * ref["summary"][i][0]
     subj.free()
+
+
+def test_draw_guess_modes_agree_and_rank():
+    """The draws from the subspace guess, from the nominal potential alone and from zero reach the
+    same field to the tolerance; the subspace guess starts closest and needs the fewest iterations."""
+    mesh = sphere_head(6.0, 90.0, jitter_mm=0.3, seed=1)
+    coil = figure8_coil(64)
+    top = np.array([0.0, 0.0, 90.0])
+    c = np.stack([top, top + [15.0, 0.0, -1.3]])
+    h = c + [0.0, 50.0, 0.0]
+    subj = Subject(mesh, tolerance=1e-10)
+    ctx = subj.context
+    nominal = nominal_sigma_table()
+    tags = tuple(int(t) for t in np.unique(mesh.tet_tags))
+    draw = nominal[list(tags)] * np.exp(0.25 * np.random.default_rng(8).standard_normal(len(tags)))
+    ctx.sigma_begin(coil, c, h, [4.0, 4.0], 1e6, nominal, tags, magnitude=True, recovery="raw")
+    out = {}
+    try:
+        for mode in ("subspace", "nominal", "zero"):
+            ctx.sigma_set_guess(mode)
+            out[mode] = ctx.sigma_draw(draw)
+    finally:
+        ctx.sigma_end()
+    base = out["zero"]["magnE"].astype(np.float64)
+    for mode in ("subspace", "nominal"):
+        m = out[mode]["magnE"].astype(np.float64)
+        assert np.linalg.norm(m - base) / np.linalg.norm(base) <= 1e-7
+    assert (out["subspace"]["init_relres"] < out["nominal"]["init_relres"]).all()
+    assert (out["zero"]["init_relres"] == 1.0).all()
+    assert out["subspace"]["iterations"].sum() <= out["nominal"]["iterations"].sum() <= out["zero"]["iterations"].sum()
+    subj.free()
