@@ -20,6 +20,7 @@
 #include <cudaTypedefs.h>
 
 #include <atomic>
+#include <cstdlib>
 #include <mutex>
 
 #include "internal.hpp"
@@ -286,6 +287,178 @@ __global__ void __launch_bounds__(kThreads, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+// Tall, narrow products streamed by persistent CTAs: C[M, BN] = A[M, K] . B[BN, K]^T with K at most
+// kStreamMaxKB * BK and only an FP32 output (the prolongation of the network's coefficients through
+// the basis: M = nodes, K = 2 x rank, a 183 MB A read once). One CTA per SM walks the M tiles
+// tile = blockIdx.x, + gridDim.x, ...:
+//   warp 4   loads B once (it stays in shared memory), then streams A's 128 x 64 tiles through a
+//            kStreamStages-deep ring without a break between M tiles;
+//   warp 5   issues the MMAs of tile t into one of two TMEM accumulators (t & 1), so tile t + 1
+//            accumulates while the epilogue drains tile t;
+//   warps 0-3 read a finished accumulator, release it (one arrive per warp) and store its rows.
+// Every wait is bounded; an expired wait sets the abort word, every role leaves its loop at its next
+// check, and before TMEM is freed the MMA issuer waits (bounded) for its issued MMAs and the producer
+// for its last issued loads.
+constexpr int kStreamStages = 8;
+constexpr int kStreamMaxKB = 8;
+
+template <int BN>
+__global__ void __launch_bounds__(kThreads, 1)
+    gemm_stream_kernel(const __grid_constant__ CUtensorMap map_a, const __grid_constant__ CUtensorMap map_b,
+                       float* __restrict__ out32, int ld_out, int M, int N, int K, int* error, long long wait_polls,
+                       unsigned long long wait_ns, int withhold_loads) {
+    constexpr std::uint32_t kABytes = BM * BK * 2;
+    constexpr std::uint32_t kBBytes = BN * BK * 2;
+    constexpr std::uint32_t kTmemCols = 2 * BN < 32 ? 32 : 2 * BN;
+    extern __shared__ unsigned char dyn_smem[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>((reinterpret_cast<std::uintptr_t>(dyn_smem) + 1023) &
+                                                          ~std::uintptr_t{1023});
+    unsigned char* a_ring = smem;                                    // kStreamStages x kABytes
+    unsigned char* b_res = smem + kStreamStages * kABytes;           // kStreamMaxKB x kBBytes
+    std::uint64_t* full = reinterpret_cast<std::uint64_t*>(b_res + kStreamMaxKB * kBBytes);
+    std::uint64_t* empty = full + kStreamStages;
+    std::uint64_t* acc_full = empty + kStreamStages;  // [2]
+    std::uint64_t* acc_empty = acc_full + 2;          // [2]
+    std::uint64_t* b_full = acc_empty + 2;
+    std::uint64_t* drain = b_full + 1;
+    std::uint32_t* tmem_slot = reinterpret_cast<std::uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int num_kb = (K + BK - 1) / BK;
+    const int n_tiles = (M + BM - 1) / BM;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kStreamStages; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 4);  // one arrive per epilogue warp
+        }
+        mbar_init(b_full, 1);
+        mbar_init(drain, 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 5) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const std::uint32_t tmem = *tmem_slot;
+
+    if (warp == 4 && lane == 0) {
+        // Producer.
+        long long issued = 0;  // A k-blocks issued over all tiles
+        if (!withhold_loads) {
+            mbar_expect_tx(b_full, kBBytes * num_kb);
+            for (int kb = 0; kb < num_kb; ++kb) tma_load_2d(&map_b, b_full, b_res + kb * kBBytes, kb * BK, 0);
+            for (int tile = blockIdx.x; tile < n_tiles && !*abort_flag; tile += gridDim.x) {
+                for (int kb = 0; kb < num_kb; ++kb, ++issued) {
+                    const int sidx = static_cast<int>(issued % kStreamStages);
+                    if (issued >= kStreamStages &&
+                        !mbar_wait(&empty[sidx], static_cast<std::uint32_t>(((issued / kStreamStages) & 1) ^ 1),
+                                   wait_polls, wait_ns)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    mbar_expect_tx(&full[sidx], kABytes);
+                    tma_load_2d(&map_a, &full[sidx], a_ring + sidx * kABytes, kb * BK, tile * BM);
+                }
+            }
+            // Before the shared memory goes: the last loads issued into each stage have landed.
+            for (long long g = issued > kStreamStages ? issued - kStreamStages : 0; g < issued; ++g)
+                (void)mbar_wait(&full[g % kStreamStages], static_cast<std::uint32_t>((g / kStreamStages) & 1),
+                                wait_polls, wait_ns);
+            (void)mbar_wait(b_full, 0, wait_polls, wait_ns);
+        }
+    } else if (warp == 5 && lane == 0) {
+        // MMA issuer.
+        constexpr std::uint32_t idesc = idesc_bf16<BN>();
+        bool ok = mbar_wait(b_full, 0, wait_polls, wait_ns);
+        long long used = 0;  // A k-blocks consumed over all tiles
+        int t = 0;           // this CTA's tile count
+        for (int tile = blockIdx.x; ok && tile < n_tiles; tile += gridDim.x, ++t) {
+            const int a = t & 1;
+            if (t >= 2 && !mbar_wait(&acc_empty[a], static_cast<std::uint32_t>(((t >> 1) & 1) ^ 1), wait_polls, wait_ns)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            for (int kb = 0; kb < num_kb; ++kb, ++used) {
+                const int sidx = static_cast<int>(used % kStreamStages);
+                if (*abort_flag || !mbar_wait(&full[sidx], static_cast<std::uint32_t>((used / kStreamStages) & 1),
+                                              wait_polls, wait_ns)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const std::uint64_t adesc = sw128_desc(a_ring + sidx * kABytes);
+                const std::uint64_t bdesc = sw128_desc(b_res + kb * kBBytes);
+#pragma unroll
+                for (int k = 0; k < BK / 16; ++k)
+                    umma_bf16(tmem + static_cast<std::uint32_t>(a * BN), adesc + 2 * k, bdesc + 2 * k, idesc,
+                              (kb > 0 || k > 0) ? 1u : 0u);
+                umma_commit(&empty[sidx]);
+            }
+            if (!ok) break;
+            umma_commit(&acc_full[a]);
+        }
+        if (!ok) *abort_flag = 1;
+        // Every MMA issued above has completed before the final barrier frees TMEM.
+        umma_commit(drain);
+        (void)mbar_wait(drain, 0, wait_polls, wait_ns);
+    } else if (warp < 4) {
+        // Epilogue: thread (warp, lane) owns row 32 warp + lane of each tile.
+        int t = 0;
+        for (int tile = blockIdx.x; tile < n_tiles; tile += gridDim.x, ++t) {
+            const int a = t & 1;
+            if (*abort_flag || !mbar_wait(&acc_full[a], static_cast<std::uint32_t>((t >> 1) & 1), wait_polls, wait_ns)) {
+                *abort_flag = 1;
+                break;
+            }
+            tc_fence_after();
+            float v[BN];
+#pragma unroll
+            for (int c = 0; c < BN; c += 16) {
+                float part[16];
+                tmem_ld16(tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(a * BN + c),
+                          part);
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[c + j] = part[j];
+            }
+            // The accumulator is in registers: hand it back to the MMA issuer.
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[a])) : "memory");
+            const int row = tile * BM + warp * 32 + lane;
+            if (row < M) {
+                float* o = out32 + static_cast<std::int64_t>(row) * ld_out;
+                if (N == BN && (ld_out % 4) == 0 && (reinterpret_cast<std::uintptr_t>(out32) & 15) == 0) {
+#pragma unroll
+                    for (int j = 0; j < BN; j += 4)
+                        *reinterpret_cast<float4*>(o + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < BN; ++j)
+                        if (j < N) o[j] = v[j];
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (threadIdx.x == 0 && *abort_flag && error) atomicExch(error, 1);
+    if (warp == 5)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -360,6 +533,37 @@ int* status_word(int dev) {
     return g_status[dev];
 }
 
+// The streamed form of a tall, narrow product with an FP32 output only: one persistent CTA per SM.
+void launch_stream(const GemmProblem& p, cudaStream_t s) {
+    constexpr int BN = 32;
+    const CUtensorMap ma = make_map(p.a, p.M, p.K, p.lda, BM);
+    const CUtensorMap mb = make_map(p.b, p.N, p.K, p.ldb, BN);
+    constexpr std::size_t smem = kStreamStages * BM * BK * 2 + kStreamMaxKB * BN * BK * 2 + 1024 + 256;
+    static std::atomic<std::uint64_t> opted{0};
+    int dev = 0;
+    CUNIBS_CHECK(cudaGetDevice(&dev));
+    const std::uint64_t bit = std::uint64_t{1} << (dev & 63);
+    if (!(opted.load(std::memory_order_acquire) & bit)) {
+        CUNIBS_CHECK(cudaFuncSetAttribute(gemm_stream_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(smem)));
+        opted.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    int sms = 0;
+    CUNIBS_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int n_tiles = (p.M + BM - 1) / BM;
+    gemm_stream_kernel<BN><<<std::min(n_tiles, sms), kThreads, smem, s>>>(
+        ma, mb, p.ep.out32, p.ep.ld_out, p.M, p.N, p.K, p.ep.error, p.ep.wait_polls, p.ep.wait_ns,
+        p.ep.withhold_loads);
+    count_launch();
+    CUNIBS_LAUNCH_CHECK("gemm_bf16 stream");
+}
+
+bool streams(const GemmProblem& p) {
+    const GemmEpilogue& e = p.ep;
+    const bool plain = e.out32 && !e.out16 && !e.out16t && !e.bias && !e.gate && e.act == 0;
+    return plain && p.N <= 32 && p.K <= kStreamMaxKB * BK && p.M >= 64 * BM;
+}
+
 }  // namespace
 
 void gemm_bf16(const GemmProblem& p_in, cudaStream_t s) {
@@ -374,6 +578,11 @@ void gemm_bf16(const GemmProblem& p_in, cudaStream_t s) {
         int dev = 0;
         CUNIBS_CHECK(cudaGetDevice(&dev));
         p.ep.error = status_word(dev);
+    }
+    // A tall, narrow product with a plain FP32 output streams through persistent CTAs.
+    if (streams(p) && std::getenv("CUNIBS_GEMM_TILED") == nullptr) {
+        launch_stream(p, s);
+        return;
     }
     // One row of tiles (M <= 128, the warm start's network at inference) is latency-bound: 32-wide
     // tiles give 4x the CTAs and smaller stages (measured 20.5 -> 10.4 us for 16 x 512 x 512).

@@ -69,14 +69,16 @@ def test_unreachable_tolerance_rebuilds_then_raises_block(small_sphere, precisio
     subj.free()
 
 
-def test_gemm_wait_runs_out_and_reports_timeout():
+@pytest.mark.parametrize("M", [256, 16384])
+def test_gemm_wait_runs_out_and_reports_timeout(M):
     torch = pytest.importorskip("torch")
     from cunibs_b200.warmstart import gemm
 
     lib = _native.load()
     dev = torch.device("cuda", 0)
     g = torch.Generator(device="cpu").manual_seed(3)
-    M, N, K = 256, 128, 512
+    # 256 rows: the tiled kernel; 16384 rows and 32 columns: the streamed one (persistent CTAs).
+    N, K = (128 if M == 256 else 32), 512
     a = torch.randn(M, K, generator=g).to(torch.bfloat16).to(dev)
     b = torch.randn(N, K, generator=g).to(torch.bfloat16).to(dev)
     out = torch.zeros(M, N, dtype=torch.float32, device=dev)

@@ -212,3 +212,31 @@ def test_a_useless_guess_falls_back_to_the_zero_guess(ws_subject):
     ctx.set_warm_start(0, 0, 0, None, None, None, None, None, None, None)
     with pytest.raises(ValueError, match="no warm-start network"):
         ctx.solve_block(coil, c, h, [4.0, 4.0], 1e6, warm_start=True)
+
+
+@pytest.mark.parametrize("M,N", [(178636, 32), (20000, 16), (8192 + 77, 32)])
+def test_streamed_tall_gemm_matches_tiled_bitwise_and_fp64(M, N, monkeypatch):
+    """The tall, narrow product (the basis prolongation) runs on persistent CTAs that stream A and
+    keep two TMEM accumulators; it issues the same MMAs in the same order as the tiled kernel, so
+    the two agree bit for bit, and both match FP64 to accumulation rounding."""
+    import ctypes as C
+
+    from cunibs_b200 import _native
+    from cunibs_b200.warmstart import gemm
+
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device="cpu").manual_seed(M)
+    K = 512
+    a = torch.randn(M, K, generator=g).to(torch.bfloat16).to(dev)
+    b = torch.randn(N, K, generator=g).to(torch.bfloat16).to(dev)
+    streamed = torch.full((M, N), float("nan"), dtype=torch.float32, device=dev)
+    gemm(a, b, out32=streamed)
+    monkeypatch.setenv("CUNIBS_GEMM_TILED", "1")
+    tiled = torch.full((M, N), float("nan"), dtype=torch.float32, device=dev)
+    gemm(a, b, out32=tiled)
+    lib = _native.load()
+    _native.check(lib.cunibs_gemm_status(C.c_void_p(torch.cuda.current_stream().cuda_stream), None))
+    assert torch.equal(streamed, tiled)
+    want = a.double() @ b.double().T
+    rel = float((streamed.double() - want).norm() / want.norm())
+    assert rel <= 2e-6, rel
