@@ -258,6 +258,8 @@ def run_ours(args) -> dict:
     ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
     setup_s = time.perf_counter() - t0
     ctx.set_timing(True)
+    if args.overlap > 0:
+        ctx.set_overlap(args.overlap)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
 
     centers = np.stack([c for c, _ in sites])
@@ -471,6 +473,7 @@ def run_ours(args) -> dict:
                                      "l2": "flushed (256 MB write) before every step's solve",
                                      "pipeline": "blocks submitted two deep: placement/dA-dt/RHS of step i+1 "
                                                  "beside the solve of step i",
+                                     "overlap_blocks_per_sm": args.overlap if args.overlap > 0 else 2,
                                      "parallelism": f"replicas x{world}"}),
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -1026,6 +1029,8 @@ def main() -> None:
     ap.add_argument("--hidden", type=int, default=512, help="width of the warm-start network's hidden layers")
     ap.add_argument("--epochs", type=int, default=400, help="training epochs of the warm-start network")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--overlap", type=int, default=0,
+                    help="dA/dt blocks per SM beside a running solve (0: the context's default, 2)")
     ap.add_argument("--configs", choices=["all", "none"], default="all",
                     help="also measure the other benchmark configurations (small plain case, uneven subjects, "
                          "held-out learned guess, conductivity study at 3.5M tets)")
