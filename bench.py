@@ -254,12 +254,16 @@ def run_ours(args) -> dict:
     p.tolerance = TOL
     p.precision = {"mixed": _native.PREC_MIXED, "split": _native.PREC_SPLIT, "plain": _native.PREC_PLAIN_FP64}[
         args.precision]
+    if args.cheby_degree > 0:
+        p.cheby_degree = args.cheby_degree
     t0 = time.perf_counter()
     ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
     setup_s = time.perf_counter() - t0
     ctx.set_timing(True)
     if args.overlap > 0:
         ctx.set_overlap(args.overlap)
+    use_table = args.coil_field == "table"
+    ctx.set_coil_table(use_table)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
 
     centers = np.stack([c for c, _ in sites])
@@ -374,6 +378,19 @@ def run_ours(args) -> dict:
     for _ in range(2):
         step()
     seq_ms, _, stage_avg = timed(n_cmp)
+    table_info = ctx.coil_table_info()
+    # The same configuration with the dipole sum at every node (the reference's dA/dt), and the
+    # plain method as the reference runs it: plain FP64 zero-guess PCG over the dipole sum.
+    ctx.set_coil_table(False)
+    for _ in range(2):
+        step()
+    _, _, stage_direct = timed(n_cmp)
+    pipelined(2)
+    direct_ms, _, _ = pipelined(n_cmp)
+    pipelined(2, precision=_native.PREC_PLAIN_FP64, warm=False)
+    plain_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
+    plain_it = float(d_it.float().mean().item())
+    ctx.set_coil_table(use_table)
     pipelined(2, warm=False)
     cold_ms, cold_its, _ = pipelined(n_cmp, warm=False)
     cold_it = float(d_it.float().mean().item())
@@ -389,14 +406,15 @@ def run_ours(args) -> dict:
     mixed_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_MIXED, warm=False)
     mixed_it = float(d_it.float().mean().item())
     pipelined(2, precision=_native.PREC_PLAIN_FP64, warm=False)
-    plain_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
-    plain_it = float(d_it.float().mean().item())
+    plain_table_ms, _, _ = pipelined(n_cmp, precision=_native.PREC_PLAIN_FP64, warm=False)
     clocks.stop()
     total_ms, value = job_throughput(total_ms, args.steps, world, dist, dev)
     seq_ms, seq_value = job_throughput(seq_ms, n_cmp, world, dist, dev)
     cold_ms, cold_value = job_throughput(cold_ms, n_cmp, world, dist, dev)
     mixed_ms, mixed_value = job_throughput(mixed_ms, n_cmp, world, dist, dev)
     plain_ms, plain_value = job_throughput(plain_ms, n_cmp, world, dist, dev)
+    direct_ms, direct_value = job_throughput(direct_ms, n_cmp, world, dist, dev)
+    plain_table_ms, plain_table_value = job_throughput(plain_table_ms, n_cmp, world, dist, dev)
 
     # End to end through the host C ABI (host buffers in and out), blocks submitted two deep
     # (cunibs_submit_block / cunibs_finish_block), timed by the wall clock around all of them.
@@ -474,17 +492,26 @@ def run_ours(args) -> dict:
                                      "pipeline": "blocks submitted two deep: placement/dA-dt/RHS of step i+1 "
                                                  "beside the solve of step i",
                                      "overlap_blocks_per_sm": args.overlap if args.overlap > 0 else 2,
+                                     "cheby_degree": int(p.cheby_degree),
+                                     "coil_field": ("table (coil-frame samples, tricubic) beyond 15 mm of the "
+                                                    "coil, dipole sum nearer" if use_table
+                                                    else "dipole sum at every node"),
                                      "parallelism": f"replicas x{world}"}),
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "vs_plain_fp64": {"value": round(plain_value, 3), "unit": "placements/s",
                           "iterations": plain_it, "ratio": round((plain_ms / n_cmp) / (total_ms / args.steps), 3),
-                          "what": "plain FP64 zero-guess PCG, same blocks, same pipeline, same GPU"},
+                          "what": "plain FP64 zero-guess PCG with the dipole sum at every node (the "
+                                  "reference's method), same blocks, same pipeline, same GPU"},
         "ablation": {"zero_guess": {"value": round(cold_value, 3), "iterations": cold_it,
                                     "what": f"{args.precision}, no learned guess"},
                      "mixed_refinement_zero_guess": {"value": round(mixed_value, 3), "iterations": mixed_it,
                                                      "what": "FP32 PCG + FP32 V-cycle inside FP64 refinement"},
+                     "dipole_sum_every_node": {"value": round(direct_value, 3),
+                                               "what": "this configuration with the coil table off"},
+                     "plain_fp64_zero_guess_table": {"value": round(plain_table_value, 3),
+                                                     "what": "plain FP64 zero-guess PCG with the coil table"},
                      "one_block_at_a_time": {"value": round(seq_value, 3),
                                              "what": "this configuration without the two-deep pipeline"},
                      "basis_projection_guess": None if proj is None else {
@@ -501,8 +528,13 @@ def run_ours(args) -> dict:
                      "bytes_per_iteration": per_it, "iterations": mean_iters, "outer_steps": mean_outer,
                      "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"},
         "stages_ms": {k: round(float(v), 4) for k, v in zip(["place", "dadt", "rhs", "solve", "post"], stage_avg)},
-        "dadt": {"pair_evals_per_step": int(pair_evals), "ms": round(dadt_ms, 4),
-                 "gpair_per_s": round(pair_evals / (dadt_ms / 1e3) / 1e9, 2)},
+        "dadt": {"ms": round(dadt_ms, 4), "ms_dipole_sum": round(float(stage_direct[1]), 4),
+                 "pair_evals_per_step_dipole_sum": int(pair_evals),
+                 "gpair_per_s_dipole_sum": round(pair_evals / (float(stage_direct[1]) / 1e3) / 1e9, 2),
+                 "table": {"in_use": table_info["in_use"], "points": table_info["points"],
+                           "layers": table_info["layers"], "check_rel_l2": table_info["check_rel_l2"],
+                           "near_fraction": (round(table_info["last_near_nodes"] / table_info["last_node_placements"], 5)
+                                             if table_info["last_near_nodes"] >= 0 else None)}},
         "setup_s": round(setup_s, 3),
         "conductivity_draws": draws,
         "adm": adm_line,
@@ -1029,6 +1061,10 @@ def main() -> None:
     ap.add_argument("--hidden", type=int, default=512, help="width of the warm-start network's hidden layers")
     ap.add_argument("--epochs", type=int, default=400, help="training epochs of the warm-start network")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cheby-degree", type=int, default=0,
+                    help="Chebyshev smoother degree of the V-cycle (0: the reference's default, 2)")
+    ap.add_argument("--coil-field", choices=["table", "direct"], default="table",
+                    help="dA/dt from the coil table beyond 15 mm of the coil (default) or the dipole sum everywhere")
     ap.add_argument("--overlap", type=int, default=0,
                     help="dA/dt blocks per SM beside a running solve (0: the context's default, 2)")
     ap.add_argument("--configs", choices=["all", "none"], default="all",

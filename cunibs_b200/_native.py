@@ -145,6 +145,8 @@ def load() -> C.CDLL:
         "cunibs_cancel_block": ([_vp, C.c_longlong], C.c_int),
         "cunibs_context_pending": ([_vp, C.POINTER(C.c_int)], C.c_int),
         "cunibs_context_set_overlap": ([_vp, C.c_int], C.c_int),
+        "cunibs_context_set_coil_table": ([_vp, C.c_int, C.c_double, C.c_double], C.c_int),
+        "cunibs_context_coil_table_info": ([_vp, _vp], C.c_int),
         "cunibs_context_set_conductivity": ([_vp, dp], C.c_int),
         "cunibs_context_set_conductivity_keep_coarse": ([_vp, dp], C.c_int),
         "cunibs_sigma_begin": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), dp, ip,
@@ -465,6 +467,20 @@ class Context:
 
     def set_overlap(self, blocks_per_sm: int) -> None:
         check(self._lib.cunibs_context_set_overlap(self.handle, int(blocks_per_sm)))
+
+    def set_coil_table(self, enabled: bool = True, near_mm: float = 15.0, step: float = 0.035) -> None:
+        """cunibs_context_set_coil_table: the block entries read the coil's field from a table sampled
+        once per coil for nodes deeper than near_mm below the coil (enabled), or sum every dipole at
+        every node (not enabled)."""
+        check(self._lib.cunibs_context_set_coil_table(self.handle, 1 if enabled else 0, float(near_mm), float(step)))
+
+    def coil_table_info(self) -> dict:
+        """cunibs_context_coil_table_info as a dict."""
+        out = np.zeros(8, np.float64)
+        check(self._lib.cunibs_context_coil_table_info(self.handle, out.ctypes.data))
+        return {"mode": int(out[0]), "in_use": bool(out[1]), "points": int(out[2]), "layers": int(out[3]),
+                "check_rel_l2": float(out[4]), "builds": int(out[5]), "last_near_nodes": int(out[6]),
+                "last_node_placements": int(out[7])}
 
     def set_conductivity(self, sigma_by_tag, *, keep_coarse: bool = False) -> None:
         """New conductivities (index = tissue tag). keep_coarse: refresh only the finest AMG level

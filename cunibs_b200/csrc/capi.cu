@@ -63,8 +63,12 @@ struct BlockSlot {
     DevArray<int> deg;
     DevArray<unsigned char> dip_packed;
     DevArray<float> dadt_nodes, dadt_elm;
+    // Nodes the coil table does not cover, per placement (p * N + ...), and their counts.
+    DevArray<int> near_list, near_cnt;
     cudaEvent_t prepared = nullptr;
-    int* h_deg = nullptr;  // pinned: the degenerate-placement flags
+    int* h_deg = nullptr;   // pinned: the degenerate-placement flags
+    int* h_near = nullptr;  // pinned: near_cnt, copied when the block's dA/dt read the table
+    bool near_valid = false;
 };
 
 // Pinned host staging of a finished block's per-column statistics (device outputs).
@@ -129,6 +133,13 @@ struct cunibs_context {
     cudaEvent_t ev_main = nullptr;
     // Blocks per SM given to the dA/dt kernel while another block's solve may run beside it.
     int overlap_blocks_per_sm = 2;
+    // The coil field table (cunibs_context_set_coil_table): mode 1 reads it for nodes deeper than
+    // table_near_m below the coil, mode 0 sums every dipole at every node.
+    CoilTable coil_table;
+    int table_mode = 1;
+    double table_near_m = 0.015, table_step = 0.035;
+    double mesh_rho_m = 0.0;  // largest distance of a node from the centre of the mesh's bounding box
+    long long last_near = -1, last_near_of = 0;  // direct-sum nodes of the last finished block
     int sm_count = 0;
     // Field-recovery operators, built on first use per mode, and their block workspace.
     std::unique_ptr<RecoveryOp> rec[4];
@@ -190,6 +201,7 @@ struct cunibs_context {
         for (BlockSlot& sl : slots) {
             if (sl.prepared) cudaEventDestroy(sl.prepared);
             if (sl.h_deg) cudaFreeHost(sl.h_deg);
+            if (sl.h_near) cudaFreeHost(sl.h_near);
         }
         if (ev_main) cudaEventDestroy(ev_main);
         if (h_coil_flag) cudaFreeHost(h_coil_flag);
@@ -288,9 +300,21 @@ long long prepare_block(cunibs_context* c, const double* pos, const double* mom,
     c->zdip_packed.reserve(packed_zdipole_bytes() * static_cast<std::size_t>(n_dip));
     c->coil_flag.reserve(1);
     prep_zdipoles(pos, mom, n_dip, c->zdip_packed.get(), c->coil_flag.get(), ps);
+    CoilTable& tb = c->coil_table;
+    const bool want_table = c->table_mode != 0;
+    if (want_table && tb.built && tb.n_dip == n_dip) coil_compare(pos, mom, n_dip, tb, c->coil_flag.get(), ps);
     CUNIBS_CHECK(cudaMemcpyAsync(c->h_coil_flag, c->coil_flag.get(), sizeof(int), cudaMemcpyDeviceToHost, ps));
     CUNIBS_CHECK(cudaStreamSynchronize(ps));
-    const bool zcoil = *c->h_coil_flag == 0;
+    const bool zcoil = (*c->h_coil_flag & 1) == 0;
+    // The table follows the coil: rebuilt (once) when the coil, its kind or the table's parameters
+    // change.
+    if (want_table && (!tb.built || tb.n_dip != n_dip || (*c->h_coil_flag & 2) || tb.nc != (zcoil ? 2 : 3) ||
+                       tb.near_m != c->table_near_m || tb.step != c->table_step)) {
+        const double rho = std::max(c->mesh_rho_m, c->table_near_m);
+        build_coil_table(tb, pos, mom, n_dip, zcoil, c->zdip_packed.get(), c->table_near_m, c->table_step, 1.1 * rho,
+                         2.5 * rho + 0.05, kCoilTableMaxPoints, ps);
+    }
+    const bool use_table = want_table && tb.valid;
     // The slot's previous block is finished on the context stream: start after what that stream
     // holds so far.
     CUNIBS_CHECK(cudaEventRecord(c->ev_main, c->stream));
@@ -302,16 +326,38 @@ long long prepare_block(cunibs_context* c, const double* pos, const double* mom,
     CUNIBS_CHECK(cudaMemcpyAsync(sl.h_deg, sl.deg.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, ps));
     sl.dadt_nodes.reserve(static_cast<std::size_t>(m.n_nodes) * 3 * k);
     const int dadt_blocks = beside_solve ? c->overlap_blocks_per_sm * c->sm_count : 0;
+    if (use_table) {
+        sl.near_list.reserve(static_cast<std::size_t>(m.n_nodes) * k);
+        sl.near_cnt.reserve(kMaxBlock);
+    }
+    sl.near_valid = use_table;
     if (zcoil) {
         mark(1);
-        dadt_nodes_zcoil(m, c->zdip_packed.get(), n_dip, sl.T.get(), k, didt, sl.dadt_nodes.get(), ps, dadt_blocks);
+        if (use_table) {
+            dadt_table(m, tb, sl.T.get(), k, didt, sl.dadt_nodes.get(), sl.near_list.get(), sl.near_cnt.get(), ps,
+                       dadt_blocks);
+            dadt_near_zcoil(m, c->zdip_packed.get(), n_dip, sl.T.get(), k, didt, sl.dadt_nodes.get(),
+                            sl.near_list.get(), sl.near_cnt.get(), ps, dadt_blocks);
+        } else {
+            dadt_nodes_zcoil(m, c->zdip_packed.get(), n_dip, sl.T.get(), k, didt, sl.dadt_nodes.get(), ps,
+                             dadt_blocks);
+        }
     } else {
         sl.dip_packed.reserve(packed_dipole_bytes() * static_cast<std::size_t>(n_dip) * k);
         prep_dipoles(pos, mom, n_dip, sl.T.get(), k, sl.dip_packed.get(), ps);
         mark(1);
-        dadt_nodes(m, reinterpret_cast<const float*>(sl.dip_packed.get()), n_dip, sl.T.get(), k, didt,
-                   sl.dadt_nodes.get(), ps, dadt_blocks);
+        if (use_table) {
+            dadt_table(m, tb, sl.T.get(), k, didt, sl.dadt_nodes.get(), sl.near_list.get(), sl.near_cnt.get(), ps,
+                       dadt_blocks);
+            dadt_near_general(m, reinterpret_cast<const float*>(sl.dip_packed.get()), n_dip, sl.T.get(), k, didt,
+                              sl.dadt_nodes.get(), sl.near_list.get(), sl.near_cnt.get(), ps, dadt_blocks);
+        } else {
+            dadt_nodes(m, reinterpret_cast<const float*>(sl.dip_packed.get()), n_dip, sl.T.get(), k, didt,
+                       sl.dadt_nodes.get(), ps, dadt_blocks);
+        }
     }
+    if (use_table)
+        CUNIBS_CHECK(cudaMemcpyAsync(sl.h_near, sl.near_cnt.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, ps));
     mark(2);
     sl.dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
     dadt_elements(m, sl.dadt_nodes.get(), k, sl.dadt_elm.get(), ps);
@@ -365,6 +411,12 @@ PendingBlock finish_block(cunibs_context* c, long long ticket, SolveStats& st, b
     cudaStream_t s = c->stream;
     const int n_red = m.n_nodes - 1;
     CUNIBS_CHECK(cudaEventSynchronize(sl.prepared));
+    c->last_near = -1;
+    if (sl.near_valid) {
+        c->last_near = 0;
+        for (int i = 0; i < k; ++i) c->last_near += sl.h_near[i];
+    }
+    c->last_near_of = static_cast<long long>(m.n_nodes) * k;
     for (int i = 0; i < k; ++i)
         if (pb.has_handles && sl.h_deg[i])
             fail(kEInval, "degenerate coil placement at index " + std::to_string(i) + " of " + std::to_string(k) +
@@ -590,6 +642,26 @@ int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_no
             CUNIBS_CHECK(cudaEventCreateWithFlags(&sl.prepared, cudaEventDisableTiming));
             CUNIBS_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&sl.h_deg), sizeof(int) * kMaxBlock,
                                        cudaHostAllocDefault));
+            CUNIBS_CHECK(cudaHostAlloc(reinterpret_cast<void**>(&sl.h_near), sizeof(int) * kMaxBlock,
+                                       cudaHostAllocDefault));
+        }
+        {
+            double lo[3] = {nodes_mm[0], nodes_mm[1], nodes_mm[2]}, hi[3] = {lo[0], lo[1], lo[2]};
+            for (int i = 1; i < n_nodes; ++i)
+                for (int a = 0; a < 3; ++a) {
+                    lo[a] = std::min(lo[a], nodes_mm[3 * static_cast<long>(i) + a]);
+                    hi[a] = std::max(hi[a], nodes_mm[3 * static_cast<long>(i) + a]);
+                }
+            double r2 = 0.0;
+            for (int i = 0; i < n_nodes; ++i) {
+                double d2 = 0.0;
+                for (int a = 0; a < 3; ++a) {
+                    const double d = nodes_mm[3 * static_cast<long>(i) + a] - 0.5 * (lo[a] + hi[a]);
+                    d2 += d * d;
+                }
+                r2 = std::max(r2, d2);
+            }
+            c->mesh_rho_m = std::sqrt(r2) * 1e-3;
         }
         build_mesh(c->mesh, nodes_mm, n_nodes, tet_nodes, tet_tags, n_tets, skin_tris, n_skin, c->stream);
         c->rebuild_hierarchy();
@@ -741,6 +813,33 @@ int cunibs_context_pending(const cunibs_context* c, int* n) {
     return guarded([&] {
         require(c && n, "NULL argument");
         *n = static_cast<int>(c->pending.size());
+    });
+}
+
+int cunibs_context_set_coil_table(cunibs_context* c, int mode, double near_mm, double step) {
+    return guarded([&] {
+        require(c != nullptr, "NULL context");
+        require(mode == 0 || mode == 1, "mode must be 0 (direct sums) or 1 (coil table)");
+        require(near_mm > 0.0 && near_mm <= 1000.0, "near_mm must be in (0, 1000]");
+        require(step > 0.0 && step <= 0.5, "step must be in (0, 0.5]");
+        c->table_mode = mode;
+        c->table_near_m = near_mm * 1e-3;
+        c->table_step = step;
+    });
+}
+
+int cunibs_context_coil_table_info(const cunibs_context* c, double* out) {
+    return guarded([&] {
+        require(c != nullptr && out != nullptr, "NULL argument");
+        const CoilTable& tb = c->coil_table;
+        out[0] = c->table_mode;
+        out[1] = tb.valid ? 1.0 : 0.0;
+        out[2] = static_cast<double>(tb.built ? tb.points : 0);
+        out[3] = tb.built ? tb.n_layers : 0;
+        out[4] = tb.check_rel;
+        out[5] = tb.builds;
+        out[6] = static_cast<double>(c->last_near);
+        out[7] = static_cast<double>(c->last_near_of);
     });
 }
 

@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cstdint>
 
+#include "coil_packed.cuh"
 #include "internal.hpp"
 
 namespace cunibs {
@@ -19,12 +20,6 @@ namespace {
 
 constexpr int kDadtThreads = 128;
 constexpr int kDipTile = 256;
-
-// One placement's dipoles in the head frame, centred on the coil origin, each component stored
-// twice so a shared-memory load yields a ready float2 broadcast: {s,s}, {m,m} per axis.
-struct __align__(16) DipolePacked {
-    float2 sx, sy, sz, mx, my, mz;
-};
 
 // Per (placement, dipole): s' = R pos (metres), m' = R mom, where R is the transform's rotation.
 // The translation cancels against the centring at the coil origin.
@@ -391,10 +386,6 @@ void rhs_block(const Mesh& m, const float* elm, int k, int K, double* b_red, cud
 namespace cunibs {
 namespace {
 
-struct __align__(16) ZDipolePacked {
-    float2 sx, sy, sz, m;
-};
-
 __global__ void prep_zdipoles_kernel(const double* __restrict__ pos, const double* __restrict__ mom, int n_dip,
                                      ZDipolePacked* __restrict__ out, int* __restrict__ flag) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -586,15 +577,28 @@ void prep_zdipoles(const double* pos, const double* mom, int n_dip, void* zpacke
     CUNIBS_LAUNCH_CHECK("prep z-dipoles");
 }
 
-void dadt_nodes_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
-                      float* out, cudaStream_t s, int max_blocks) {
-    const DadtGrid g = dadt_grid(m.n_nodes, k, max_blocks);
-    dadt_zcoil_kernel<<<g.blocks, kDadtThreads, 0, s>>>(m.nodes.get(), m.n_nodes,
-                                                       static_cast<const ZDipolePacked*>(zpacked), n_dip,
-                                                       transforms_dev, static_cast<float>(didt * 1e-7), out,
-                                                       g.n_tiles, g.n_items);
+void dadt_zcoil_raw(const double* nodes_mm, int n_nodes, const void* zpacked, int n_dip, const double* transforms_dev,
+                    int k, float scale, float* out, cudaStream_t s, int max_blocks) {
+    const DadtGrid g = dadt_grid(n_nodes, k, max_blocks);
+    dadt_zcoil_kernel<<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, static_cast<const ZDipolePacked*>(zpacked),
+                                                       n_dip, transforms_dev, scale, out, g.n_tiles, g.n_items);
     count_launch();
     CUNIBS_LAUNCH_CHECK("dadt z-coil");
+}
+
+void dadt_nodes_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
+                      float* out, cudaStream_t s, int max_blocks) {
+    dadt_zcoil_raw(m.nodes.get(), m.n_nodes, zpacked, n_dip, transforms_dev, k, static_cast<float>(didt * 1e-7), out, s,
+                   max_blocks);
+}
+
+void dadt_general_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
+                      const double* transforms_dev, int k, float scale, float* out, cudaStream_t s) {
+    const DadtGrid g = dadt_grid(n_nodes, k, 0);
+    dadt_kernel<<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, reinterpret_cast<const DipolePacked*>(dip_packed),
+                                                 n_dip, transforms_dev, scale, out, g.n_tiles, g.n_items);
+    count_launch();
+    CUNIBS_LAUNCH_CHECK("dadt");
 }
 
 }  // namespace cunibs

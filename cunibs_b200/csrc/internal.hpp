@@ -202,6 +202,66 @@ void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed
 // dadt_nodes_raw's for that set alone; each pair's geometry is formed once for all sets.
 void dadt_nodes_shared(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
                        const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s);
+// The two direct sums on raw node coordinates with an explicit FP32 scale (1: the bare dipole sum).
+void dadt_zcoil_raw(const double* nodes_mm, int n_nodes, const void* zpacked, int n_dip, const double* transforms_dev,
+                    int k, float scale, float* out, cudaStream_t s, int max_blocks = 0);
+void dadt_general_raw(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
+                      const double* transforms_dev, int k, float scale, float* out, cudaStream_t s);
+
+// --- coil field table (coil_table.cu) ----------------------------------------------------------
+// The coil's bare dipole sum sampled once per coil on a grid in its own frame, in layers below the
+// deepest dipole whose depths grow geometrically, z_j = z0 (1 + step)^(j - 1), each layer a square
+// grid of spacing step * z_j. A node deeper than z0 inside the grid takes the tricubic Lagrange
+// interpolant of the table (four layers, four rows, four points); the others, the nodes near the coil,
+// take the direct sum.
+struct CoilTableLayer {
+    float inv_h;       // grid lines at x = (i - half) / inv_h and y = (j - half) / inv_h, metres
+    float z;           // depth below the deepest dipole, metres
+    int half;          // index of the line through x = 0 (and y = 0)
+    int n;             // points per row, rows per layer
+    long long offset;  // first point of the layer in the table
+};
+
+constexpr int kCoilTableMaxLayers = 256;
+// Tables above this many points (a mesh far larger than a head, or a tiny near depth) are not built.
+constexpr long long kCoilTableMaxPoints = 16LL << 20;
+
+struct CoilTable {
+    bool built = false;   // built for the coil in pos/mom and the parameters below
+    bool valid = false;   // and its check passed: the dA/dt path may read it
+    int nc = 0;           // components per point: 2 (moments along the coil's z: A_z = 0) or 3
+    int n_dip = 0;
+    int n_layers = 0;
+    long long points = 0;
+    float z_top = 0.f;    // the deepest dipole's z in the coil frame (z points into the head), metres
+    float z0 = 0.f, inv_z0 = 0.f, inv_log_step = 0.f;
+    double near_m = 0.0, step = 0.0, lateral_m = 0.0;
+    double check_rel = 0.0;  // relative L2 error of the interpolant at the check points
+    int builds = 0;
+    DevArray<CoilTableLayer> layers;
+    DevArray<float> data;       // per point: 2 floats (nc 2) or 4 (nc 3, the fourth zero)
+    DevArray<double> pos, mom;  // the coil it was built for
+};
+
+// Sets bit 1 of *flag when pos/mom differ from the table's coil (same n_dip).
+void coil_compare(const double* pos, const double* mom, int n_dip, const CoilTable& tb, int* flag, cudaStream_t s);
+// Builds (and checks) the table for the coil on the device in pos/mom; lateral_m is the half-width
+// of the layers, depth_m the deepest depth sampled. Synchronises s. Leaves tb.valid false when the
+// check fails or the table would exceed max_points.
+void build_coil_table(CoilTable& tb, const double* pos, const double* mom, int n_dip, bool zcoil, const void* zpacked,
+                      double near_m, double step, double lateral_m, double depth_m, long long max_points,
+                      cudaStream_t s);
+// dA/dt of every node the table covers, for k placements; the others are appended to their
+// placement's list near_list[p * N + ...], counted in near_cnt[p] (zeroed here).
+void dadt_table(const Mesh& m, const CoilTable& tb, const double* transforms_dev, int k, double didt, float* out,
+                int* near_list, int* near_cnt, cudaStream_t s, int max_blocks = 0);
+// The direct sum for the listed nodes: eight warps per block split the dipoles, their partial sums
+// added in warp order (the result does not depend on the list's order or the grid).
+void dadt_near_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
+                     float* out, const int* near_list, const int* near_cnt, cudaStream_t s, int max_blocks = 0);
+void dadt_near_general(const Mesh& m, const float* dip_packed, int n_dip, const double* transforms_dev, int k,
+                       double didt, float* out, const int* near_list, const int* near_cnt, cudaStream_t s,
+                       int max_blocks = 0);
 
 // Records the calling thread's message for cunibs_last_error.
 void set_last_error(const std::string& message);

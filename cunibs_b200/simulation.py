@@ -95,9 +95,12 @@ class Subject:
     """
 
     def __init__(self, mesh: HeadMesh, *, tolerance: float = DEFAULT_TOLERANCE, max_iters: int = DEFAULT_MAX_ITERS,
-                 precision: Precision = "split", device: int = 0) -> None:
+                 precision: Precision = "split", device: int = 0,
+                 coil_field: Literal["table", "direct"] = "table") -> None:
         if precision not in _PRECISION_CODES:
             raise ValueError("precision must be 'mixed', 'split' or 'plain'")
+        if coil_field not in ("table", "direct"):
+            raise ValueError("coil_field must be 'table' or 'direct'")
         self._mesh = mesh
         self._ctx: _native.Context | None = None
         self._ordered: HeadMesh | None = None
@@ -111,6 +114,9 @@ class Subject:
         self._lock = threading.RLock()
         self._block_k_default = MAX_BLOCK  # block width of block_k=None sweeps (autotune may lower it)
         self._overlap = 2                  # dA/dt blocks per SM beside a running solve
+        # "table": nodes away from the coil read its field from a table sampled once per coil (about
+        # 1e-7 relative); "direct": every node sums every dipole, as the reference does.
+        self._coil_field = coil_field
 
     @classmethod
     def from_mesh(cls, mesh_file: str | Path, **kwargs) -> Subject:
@@ -145,12 +151,18 @@ class Subject:
                 m = self._mesh
                 self._ctx = _native.Context(m.nodes_mm, m.tet_nodes, m.tet_tags, m.skin_tris, p)
                 self._ctx.set_overlap(self._overlap)
+                self._ctx.set_coil_table(self._coil_field == "table")
             return self._ctx
 
     @property
     def block_k_default(self) -> int:
         """Placements per block of a sweep called with ``block_k=None``."""
         return self._block_k_default
+
+    @property
+    def coil_field(self) -> str:
+        """How the coil's dA/dt reaches the nodes: "table" or "direct" (see ``__init__``)."""
+        return self._coil_field
 
     @property
     def overlap_blocks_per_sm(self) -> int:

@@ -195,6 +195,21 @@ int cunibs_cancel_block(cunibs_context* ctx, long long ticket);
 int cunibs_context_pending(const cunibs_context* ctx, int* n);
 /* Blocks per SM the dA/dt kernel takes while another block's solve may run beside it (default 2). */
 int cunibs_context_set_overlap(cunibs_context* ctx, int blocks_per_sm);
+/* How the block entries form the coil dA/dt at the nodes (fem/placement.py:279-317 sums every
+ * dipole at every node, solver/coil/dadt.cu:27-113).
+ *   mode 1 (default): a table of the coil's field, sampled once per coil in its own frame in layers
+ *     below the coil whose spacing grows with depth (`step` times the depth, default 0.035), gives
+ *     every node deeper than near_mm (default 15) below the coil by tricubic interpolation; nodes
+ *     nearer the coil keep the dipole sum. The table is rebuilt when the coil changes, and checked
+ *     when built against the dipole sum (relative L2 error at most 2e-6 at cell centres, else the
+ *     dipole sum is used everywhere); its interpolation error is about 1e-7 relative at step 0.035.
+ *   mode 0: the dipole sum at every node.
+ * cunibs_dadt, cunibs_dadt_noalloc and the auxiliary dipole method always sum every dipole. */
+int cunibs_context_set_coil_table(cunibs_context* ctx, int mode, double near_mm, double step);
+/* out[8]: mode, table in use (0/1), table points, layers, check error (relative L2), builds, nodes
+ * given the dipole sum in the last finished block (-1 when it did not read the table), nodes x
+ * placements of that block. */
+int cunibs_context_coil_table_info(const cunibs_context* ctx, double* out);
 
 /* Re-assembles the stiffness with a new conductivity per tissue tag (sigma_by_tag[0..10], S/m;
  * index = tag) and rebuilds the AMG hierarchy: the per-sample step of a conductivity Monte Carlo
