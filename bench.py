@@ -432,9 +432,11 @@ def run_ours(args) -> dict:
     h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
     d2h = res["transform"].nbytes + res["summary"].nbytes + res["iterations"].nbytes + res["relative_residual"].nbytes
 
-    draws = conductivity_draws(ctx, coil, centers[:4], handles[:4], dists[:4], args.recovery, stream)
-    adm_line = adm_measure(ctx, coil, sites, stream)
-    multi = multi_subject_measure(coil, args.recovery) if world == 1 else None
+    draws = adm_line = multi = None
+    if args.extras == "all":
+        draws = conductivity_draws(ctx, coil, centers[:4], handles[:4], dists[:4], args.recovery, stream)
+        adm_line = adm_measure(ctx, coil, sites, stream)
+        multi = multi_subject_measure(coil, args.recovery) if world == 1 else None
     # The other benchmark configurations, each a line of its own (one GPU; rank 0 of a replica run).
     configs = None
     if args.configs == "all" and rank == 0:
@@ -1067,6 +1069,9 @@ def main() -> None:
                     help="dA/dt from the coil table beyond 15 mm of the coil (default) or the dipole sum everywhere")
     ap.add_argument("--overlap", type=int, default=0,
                     help="dA/dt blocks per SM beside a running solve (0: the context's default, 2)")
+    ap.add_argument("--extras", choices=["all", "none"], default="all",
+                    help="also measure the conductivity draws, the auxiliary dipole method and the side-by-side "
+                         "subjects on the headline head")
     ap.add_argument("--configs", choices=["all", "none"], default="all",
                     help="also measure the other benchmark configurations (small plain case, uneven subjects, "
                          "held-out learned guess, conductivity study at 3.5M tets)")

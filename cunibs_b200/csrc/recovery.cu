@@ -19,6 +19,8 @@
 // B200 layout: the harmonic operator is one float4 per patch entry {w_x, w_y, w_z, node} so the
 // apply streams one 16-byte load per entry, shared by the K column lanes of a slot (a broadcast);
 // the potential is read from the solver's row-major (n, K) block, one 8-byte lane per column.
+#include <cstdlib>
+
 #include <cub/cub.cuh>
 
 #include "internal.hpp"
@@ -566,6 +568,43 @@ __global__ void harmonic_apply_kernel(const float4* __restrict__ wq, const int* 
     o[2] = static_cast<float>(-az - static_cast<double>(da[2]));
 }
 
+// The same with one thread per (slot, column pair): one operator load serves both columns and the
+// potential pair is one 16-byte gather; each column's sums are bitwise the one-column kernel's.
+__global__ void harmonic_apply_pair_kernel(const float4* __restrict__ wq, const int* __restrict__ pptr,
+                                           const int* __restrict__ slot_node, int n_slots,
+                                           const double* __restrict__ x, int K, int ground,
+                                           const float* __restrict__ dadt_nodes, int n_nodes, int k,
+                                           float* __restrict__ e_slots) {
+    const std::int64_t q = static_cast<std::int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const int L = K / 2;
+    const int s = static_cast<int>(q / L), c0 = 2 * static_cast<int>(q % L);
+    if (s >= n_slots || c0 >= k) return;
+    const double2* xv = reinterpret_cast<const double2*>(x);
+    double ax0 = 0.0, ay0 = 0.0, az0 = 0.0, ax1 = 0.0, ay1 = 0.0, az1 = 0.0;
+    for (int p = pptr[s], end = pptr[s + 1]; p < end; ++p) {
+        const float4 e = wq[p];
+        const int m = __float_as_int(e.w);
+        const double2 vm = (m == ground) ? make_double2(0.0, 0.0)
+                                         : xv[static_cast<std::int64_t>(m - (m > ground ? 1 : 0)) * L + c0 / 2];
+        ax0 = fma(static_cast<double>(e.x), vm.x, ax0);
+        ay0 = fma(static_cast<double>(e.y), vm.x, ay0);
+        az0 = fma(static_cast<double>(e.z), vm.x, az0);
+        ax1 = fma(static_cast<double>(e.x), vm.y, ax1);
+        ay1 = fma(static_cast<double>(e.y), vm.y, ay1);
+        az1 = fma(static_cast<double>(e.z), vm.y, az1);
+    }
+    const int node = slot_node[s];
+    const double a[2][3] = {{ax0, ay0, az0}, {ax1, ay1, az1}};
+    for (int h = 0; h < 2 && c0 + h < k; ++h) {
+        const int c = c0 + h;
+        const float* da = dadt_nodes + (static_cast<std::int64_t>(c) * n_nodes + node) * 3;
+        float* o = e_slots + (static_cast<std::int64_t>(c) * n_slots + s) * 3;
+        o[0] = static_cast<float>(-a[h][0] - static_cast<double>(da[0]));
+        o[1] = static_cast<float>(-a[h][1] - static_cast<double>(da[1]));
+        o[2] = static_cast<float>(-a[h][2] - static_cast<double>(da[2]));
+    }
+}
+
 // SPR: E_s = sum_c w_c E_{e(c)}, FP32 accumulation in slot order; one thread per (slot, column).
 __global__ void spr_apply_kernel(const float* __restrict__ w, const int* __restrict__ ptr,
                                  const int* __restrict__ idx, int n_slots, const float* __restrict__ e_elem,
@@ -786,10 +825,18 @@ const int* recovery_slot_of_corner(const Mesh& m, const RecoveryOp& op) {
 void apply_recovery(const Mesh& m, const RecoveryOp& op, const double* x_red, int K, const float* dadt_nodes,
                     const float* e_elem, int k, float* e_slots, float* E, float* magn, cudaStream_t s) {
     if (op.mode == kRecHarmonic) {
-        const std::int64_t n = static_cast<std::int64_t>(op.n_slots) * K;
-        harmonic_apply_kernel<<<grid_for(n), kBlock, 0, s>>>(op.wq.get(), op.ptr.get(), op.slot_node.get(),
-                                                             op.n_slots, x_red, K, m.ground, dadt_nodes, m.n_nodes, k,
-                                                             e_slots);
+        const char* lanes = std::getenv("CUNIBS_LANE_COLUMNS");
+        if (K % 2 == 0 && !(lanes != nullptr && lanes[0] == '1')) {
+            const std::int64_t n = static_cast<std::int64_t>(op.n_slots) * (K / 2);
+            harmonic_apply_pair_kernel<<<grid_for(n), kBlock, 0, s>>>(op.wq.get(), op.ptr.get(), op.slot_node.get(),
+                                                                      op.n_slots, x_red, K, m.ground, dadt_nodes,
+                                                                      m.n_nodes, k, e_slots);
+        } else {
+            const std::int64_t n = static_cast<std::int64_t>(op.n_slots) * K;
+            harmonic_apply_kernel<<<grid_for(n), kBlock, 0, s>>>(op.wq.get(), op.ptr.get(), op.slot_node.get(),
+                                                                 op.n_slots, x_red, K, m.ground, dadt_nodes, m.n_nodes,
+                                                                 k, e_slots);
+        }
     } else {
         const bool nodes = op.mode == kRecSprGlobal;
         const std::int64_t n = static_cast<std::int64_t>(op.n_slots) * k;

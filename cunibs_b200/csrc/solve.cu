@@ -282,6 +282,151 @@ __global__ void __launch_bounds__(Group<K, TPR>::kBlock) prolong_kernel(int n, c
     xf[static_cast<long>(s.row) * K + s.c] += v;
 }
 
+// --- one lane per row and C adjacent columns (operators walked by one lane per row) -------------
+//
+// A lane takes C adjacent columns of its row (C = 2 or 4): one index and one value load per nonzero
+// serve them all, and the gather is one 8- or 16-byte load (FP32; FP64 takes 16-byte pairs). A
+// C-th of the lanes carry the same memory work, so each has C times the loads in flight at the same
+// occupancy. Each column's terms are added in CSR order exactly as by strided_dot<T, 1> (one fused
+// multiply-add per term), so the results are bitwise those of the one-column kernels.
+template <typename T, int C>
+struct ColGroup;
+template <>
+struct ColGroup<float, 2> {
+    using V = float2;
+    __device__ static void split(const V& v, float* o) { o[0] = v.x; o[1] = v.y; }
+};
+template <>
+struct ColGroup<float, 4> {
+    using V = float4;
+    __device__ static void split(const V& v, float* o) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+};
+template <>
+struct ColGroup<double, 2> {
+    using V = double2;
+    __device__ static void split(const V& v, double* o) { o[0] = v.x; o[1] = v.y; }
+};
+
+constexpr int kColBlock = 256;
+
+template <int K, int C>
+struct ColLanes {
+    static constexpr int kLanes = K / C;                // lanes per row
+    static constexpr int kRows = kColBlock / kLanes;    // rows per block
+};
+
+template <int K, int C>
+unsigned col_grid(int n) {
+    return static_cast<unsigned>((n + ColLanes<K, C>::kRows - 1) / ColLanes<K, C>::kRows);
+}
+
+// The C columns' gathers of row j: x[j * K + g * C + 0 .. C-1].
+template <typename T, int K, int C>
+__device__ __forceinline__ void gather_cols(const T* __restrict__ x, long j, int g, T out[C]) {
+    if constexpr (std::is_same<T, double>::value && C == 4) {
+        const double2* xv = reinterpret_cast<const double2*>(x + j * K + g * C);
+        const double2 a = xv[0], b = xv[1];
+        out[0] = a.x;
+        out[1] = a.y;
+        out[2] = b.x;
+        out[3] = b.y;
+    } else {
+        using G = ColGroup<T, C>;
+        G::split(reinterpret_cast<const typename G::V*>(x)[j * (K / C) + g], out);
+    }
+}
+
+template <typename T, int K, int C>
+__device__ __forceinline__ void row_dot_cols(const int* __restrict__ ptr, const int* __restrict__ col,
+                                             const T* __restrict__ val, const T* __restrict__ x, int row, int g,
+                                             T acc[C]) {
+#pragma unroll
+    for (int u = 0; u < C; ++u) acc[u] = T(0);
+    const int e = ptr[row + 1];
+    for (int p = ptr[row]; p < e; ++p) {
+        const int j = col[p];
+        const T v = val[p];
+        T xx[C];
+        gather_cols<T, K, C>(x, j, g, xx);
+#pragma unroll
+        for (int u = 0; u < C; ++u) acc[u] += v * xx[u];
+    }
+}
+
+template <typename T, int K, int C>
+__global__ void __launch_bounds__(kColBlock) cheby_cols_kernel(int n, const int* __restrict__ ptr,
+                                                               const int* __restrict__ col, const T* __restrict__ val,
+                                                               const T* __restrict__ dinv, const T* __restrict__ b,
+                                                               const T* __restrict__ x_cur, const T* x_prev, T c_cur,
+                                                               T c_prev, T alpha, T* out) {
+    pdl_enter();
+    const int row = blockIdx.x * ColLanes<K, C>::kRows + threadIdx.x / ColLanes<K, C>::kLanes;
+    const int g = threadIdx.x % ColLanes<K, C>::kLanes;
+    if (row >= n) return;
+    T ax[C];
+    row_dot_cols<T, K, C>(ptr, col, val, x_cur, row, g, ax);
+    const long q = static_cast<long>(row) * K + g * C;
+    const T d = dinv[row];
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+        const T cur = x_cur[q + u];
+        const T prev = x_prev[q + u];
+        const T rhs = b[q + u];
+        out[q + u] = c_cur * cur + c_prev * prev + alpha * d * (rhs - ax[u]);
+    }
+}
+
+template <typename T, int K, int C>
+__global__ void __launch_bounds__(kColBlock) residual_cols_kernel(int n, const int* __restrict__ ptr,
+                                                                  const int* __restrict__ col,
+                                                                  const T* __restrict__ val, const T* __restrict__ x,
+                                                                  const T* __restrict__ b, T* __restrict__ r) {
+    pdl_enter();
+    const int row = blockIdx.x * ColLanes<K, C>::kRows + threadIdx.x / ColLanes<K, C>::kLanes;
+    const int g = threadIdx.x % ColLanes<K, C>::kLanes;
+    if (row >= n) return;
+    T ax[C];
+    row_dot_cols<T, K, C>(ptr, col, val, x, row, g, ax);
+    const long q = static_cast<long>(row) * K + g * C;
+#pragma unroll
+    for (int u = 0; u < C; ++u) r[q + u] = b[q + u] - ax[u];
+}
+
+template <typename T, int K, int C>
+__global__ void __launch_bounds__(kColBlock) prolong_cols_kernel(int n, const int* __restrict__ ptr,
+                                                                 const int* __restrict__ col,
+                                                                 const T* __restrict__ val, const T* __restrict__ xc,
+                                                                 T* __restrict__ xf) {
+    pdl_enter();
+    const int row = blockIdx.x * ColLanes<K, C>::kRows + threadIdx.x / ColLanes<K, C>::kLanes;
+    const int g = threadIdx.x % ColLanes<K, C>::kLanes;
+    if (row >= n) return;
+    T v[C];
+    row_dot_cols<T, K, C>(ptr, col, val, xc, row, g, v);
+    const long q = static_cast<long>(row) * K + g * C;
+#pragma unroll
+    for (int u = 0; u < C; ++u) xf[q + u] += v[u];
+}
+
+// Calls f(std::integral_constant<int, C>) with the widest lane width C <= lane_cols that divides K
+// (C > 1), and returns whether it did.
+template <int K, typename F>
+bool dispatch_cols(int lane_cols, F&& f) {
+    if constexpr (K % 4 == 0) {
+        if (lane_cols >= 4) {
+            f(std::integral_constant<int, 4>{});
+            return true;
+        }
+    }
+    if constexpr (K % 2 == 0) {
+        if (lane_cols >= 2) {
+            f(std::integral_constant<int, 2>{});
+            return true;
+        }
+    }
+    return false;
+}
+
 template <int K, typename F>
 void dispatch_tpr(int tpr, F&& f) {
     switch (tpr) {
@@ -723,6 +868,9 @@ class Solver {
     // Solve-loop kernels launched with programmatic stream serialization (pdl_enter); off with
     // CUNIBS_PROGRAMMATIC_LAUNCH=0.
     bool pdl = true;
+    // Columns per lane of the one-lane-per-row operators (the *_cols kernels; bitwise the same
+    // results): 2 by default, CUNIBS_LANE_COLUMNS=1 or 4 to choose.
+    int lane_cols = 2;
     cudaStream_t stream = nullptr;
     // FP64 CG / outer workspace (n, kcap)
     DevArray<double> B, X, R, P, AP, Z;
@@ -999,6 +1147,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         return false;
     }
     const bool fuse_dot = dot && H.levels[0].tpr_a <= 16;
+    const int cols = lane_cols;
     const int deg = ch.degree;
     const bool odd = (deg % 2) != 0;
     // One Chebyshev sweep of `deg` steps (vcycle.cu:585-617 buffer discipline). x0 == nullptr is a
@@ -1007,6 +1156,21 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     // the buffer that holds x_{i-1}, which the step kernel reads only at the row it writes.
     auto launch_cheby = [&](int l, const T* bi, const T* cur, const T* prev, T cc, T cp, T al, T* out) {
         const Level& lv = H.levels[l];
+        if (lv.tpr_a == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
+                constexpr int C = decltype(cc_)::value;
+                if constexpr (std::is_same<T, double>::value && C == 4) {
+                    launch_loop(pdl, cheby_cols_kernel<T, K, 2>, col_grid<K, 2>(lv.n), kColBlock, s, lv.n,
+                                lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al,
+                                out);
+                } else {
+                    launch_loop(pdl, cheby_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n,
+                                lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al,
+                                out);
+                }
+            })) {
+            count_launch();
+            return;
+        }
         dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
             launch_loop(pdl, cheby_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
@@ -1065,11 +1229,18 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
             count_launch();
         }
         sweep(l, bi, nullptr, first, other, nullptr);
-        dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
-            constexpr int TPR = decltype(tc)::value;
-            launch_loop(pdl, residual_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
-                        lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
+        const bool grouped = lv.tpr_a == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
+            constexpr int C = (std::is_same<T, double>::value && decltype(cc_)::value == 4) ? 2 : decltype(cc_)::value;
+            launch_loop(pdl, residual_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n, lv.a.ptr.get(),
+                        lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
         });
+        if (!grouped) {
+            dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
+                constexpr int TPR = decltype(tc)::value;
+                launch_loop(pdl, residual_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s,
+                            lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
+            });
+        }
         count_launch();
         const bool next_is_level = (l + 1 < L);
         T* nb = next_is_level ? w.b[l + 1].get() : w.cb.get();
@@ -1095,11 +1266,18 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     for (int l = L - 1; l >= 0; --l) {
         const Level& lv = H.levels[l];
         const T* bi = (l == 0) ? b : w.b[l].get();
-        dispatch_tpr<K>(lv.tpr_p, [&](auto tc) {
-            constexpr int TPR = decltype(tc)::value;
-            launch_loop(pdl, prolong_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
-                        lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
+        const bool grouped = lv.tpr_p == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
+            constexpr int C = (std::is_same<T, double>::value && decltype(cc_)::value == 4) ? 2 : decltype(cc_)::value;
+            launch_loop(pdl, prolong_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n, lv.p.ptr.get(),
+                        lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
         });
+        if (!grouped) {
+            dispatch_tpr<K>(lv.tpr_p, [&](auto tc) {
+                constexpr int TPR = decltype(tc)::value;
+                launch_loop(pdl, prolong_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s,
+                            lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
+            });
+        }
         count_launch();
         // The level's smoothed correction stays wherever its sweep left it; the next finer
         // prolongation reads it from there.
@@ -1332,6 +1510,8 @@ SolverPtr make_solver(const Hierarchy& h, const Params& p) {
     sv->while_unsupported = host_loop != nullptr && host_loop[0] == '1';
     const char* pdl = std::getenv("CUNIBS_PROGRAMMATIC_LAUNCH");
     sv->pdl = !(pdl != nullptr && pdl[0] == '0');
+    const char* lanes = std::getenv("CUNIBS_LANE_COLUMNS");
+    if (lanes != nullptr && (lanes[0] == '1' || lanes[0] == '2' || lanes[0] == '4')) sv->lane_cols = lanes[0] - '0';
     // The solver's kernels go at the highest stream priority: block preparation may run beside them.
     int least = 0, greatest = 0;
     CUNIBS_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
