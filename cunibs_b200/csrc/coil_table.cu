@@ -193,58 +193,102 @@ __global__ void __launch_bounds__(kTableThreads) dadt_table_kernel(const double*
     }
 }
 
-// Items (tile of 32 listed nodes, placement), tile-major so that the occupied tiles of every
-// placement come first; a tile past its placement's count is skipped (uniformly per block). Warp w
-// sums dipoles [w * chunk, (w + 1) * chunk) for the tile's 32 nodes; warp 0 adds the eight partial
-// sums in warp order.
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+
+// Items (tile of 64 listed nodes, placement), tile-major so that the occupied tiles of every
+// placement come first; a tile past its placement's count is skipped (uniformly per block). Lane l of
+// every warp carries the tile's nodes l and l + 32 as one float2 pair (packed FP32 arithmetic); warp
+// w sums dipoles [w * chunk, (w + 1) * chunk) through a 32-dipole shared-memory stage, and a stage
+// whose dipoles share their plane and moment (a figure-8 wing) takes the 8-operation form of
+// dadt_zcoil_kernel; warp 0 adds the eight partial sums in warp order.
 __global__ void __launch_bounds__(32 * kNearWarps) dadt_near_zcoil_kernel(
     const double* __restrict__ nodes_mm, int n_nodes, const ZDipolePacked* __restrict__ dip, int n_dip,
     const double* __restrict__ T, int k, float scale, float* __restrict__ out, const int* __restrict__ near_list,
     const int* __restrict__ near_cnt) {
-    __shared__ float part[kNearWarps][2][32];
+    __shared__ ZDipolePacked stage[kNearWarps][32];
+    __shared__ float part[kNearWarps][2][64];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int chunk = (n_dip + kNearWarps - 1) / kNearWarps;
     const int j_lo = min(n_dip, w * chunk), j_hi = min(n_dip, j_lo + chunk);
-    const int tiles = (n_nodes + 31) / 32;
+    const int tiles = (n_nodes + 63) / 64;
     for (int item = blockIdx.x; item < tiles * k; item += gridDim.x) {
         const int tile = item / k, p = item - tile * k;
         const int cnt = near_cnt[p];
-        if (tile * 32 >= cnt) continue;
-        const int e = tile * 32 + lane;
-        const bool valid = e < cnt;
+        if (tile * 64 >= cnt) continue;
+        const int e0 = tile * 64 + lane, e1 = e0 + 32;
         const int* lp = near_list + static_cast<long long>(p) * n_nodes;
-        const int i = lp[valid ? e : tile * 32];
-        double R[3][3];
-        float px, py, pz;
-        coil_frame(nodes_mm, i, T + 16 * static_cast<long>(p), R, px, py, pz);
-        float ax = 0.f, ay = 0.f;
-        const float4* d4 = reinterpret_cast<const float4*>(dip);
-        for (int j = j_lo; j < j_hi; ++j) {
-            const float4 a = __ldg(d4 + 2 * j);      // sx.x sx.y sy.x sy.y
-            const float4 b = __ldg(d4 + 2 * j + 1);  // sz.x sz.y m.x m.y
-            const float dx = px - a.x, dy = py - a.z, dz = pz - b.x;
-            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float inv = rsqrtf(d2);
-            const float wm = (inv * b.z) * (inv * inv);
-            ax = fmaf(wm, dy, ax);
-            ay = fmaf(wm, dx, ay);
+        const int i0 = lp[e0 < cnt ? e0 : tile * 64], i1 = lp[e1 < cnt ? e1 : tile * 64];
+        const double* Tp = T + 16 * static_cast<long>(p);
+        float2 rx, ry, rz;
+        {
+            double R[3][3];
+            float px0, py0, pz0, px1, py1, pz1;
+            coil_frame(nodes_mm, i0, Tp, R, px0, py0, pz0);
+            coil_frame(nodes_mm, i1, Tp, R, px1, py1, pz1);
+            rx = make_float2(px0, px1);
+            ry = make_float2(py0, py1);
+            rz = make_float2(pz0, pz1);
         }
-        part[w][0][lane] = ax;
-        part[w][1][lane] = ay;
-        __syncthreads();
-        if (w == 0 && valid) {
-            float sx = 0.f, sy = 0.f;
-#pragma unroll
-            for (int u = 0; u < kNearWarps; ++u) {
-                sx += part[u][0][lane];
-                sy += part[u][1][lane];
+        float2 ax = make_float2(0.f, 0.f), ay = ax;
+        for (int t0 = j_lo; t0 < j_hi; t0 += 32) {
+            const int nt = min(32, j_hi - t0);
+            __syncwarp();
+            if (lane < nt) stage[w][lane] = dip[t0 + lane];
+            __syncwarp();
+            const float z_first = stage[w][0].sz.x, m_first = stage[w][0].m.x;
+            const bool same = lane >= nt || (stage[w][lane].sz.x == z_first && stage[w][lane].m.x == m_first);
+            if (__all_sync(0xffffffffu, same)) {
+                const float2 dz = f2sub(rz, stage[w][0].sz);
+                const float2 zz = __fmul2_rn(dz, dz);
+                float2 tx = make_float2(0.f, 0.f), ty = tx;
+                for (int j = 0; j < nt; ++j) {
+                    const ZDipolePacked d = stage[w][j];
+                    const float2 dx = f2sub(rx, d.sx), dy = f2sub(ry, d.sy);
+                    const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, zz));
+                    const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+                    const float2 w3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
+                    tx = __ffma2_rn(w3, dy, tx);
+                    ty = __ffma2_rn(w3, dx, ty);
+                }
+                const float2 mt = stage[w][0].m;
+                ax = __ffma2_rn(mt, tx, ax);
+                ay = __ffma2_rn(mt, ty, ay);
+            } else {
+                for (int j = 0; j < nt; ++j) {
+                    const ZDipolePacked d = stage[w][j];
+                    const float2 dx = f2sub(rx, d.sx), dy = f2sub(ry, d.sy), dz = f2sub(rz, d.sz);
+                    const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+                    const float2 inv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+                    const float2 wm = __fmul2_rn(__fmul2_rn(inv, d.m), __fmul2_rn(inv, inv));
+                    ax = __ffma2_rn(wm, dy, ax);
+                    ay = __ffma2_rn(wm, dx, ay);
+                }
             }
-            // A' = (-sum wm dy, sum wm dx, 0); A = R A'.
-            const float a0 = -scale * sx, a1 = scale * sy;
-            float* o = out + (static_cast<long long>(p) * n_nodes + i) * 3;
-            o[0] = static_cast<float>(R[0][0]) * a0 + static_cast<float>(R[0][1]) * a1;
-            o[1] = static_cast<float>(R[1][0]) * a0 + static_cast<float>(R[1][1]) * a1;
-            o[2] = static_cast<float>(R[2][0]) * a0 + static_cast<float>(R[2][1]) * a1;
+        }
+        part[w][0][lane] = ax.x;
+        part[w][0][lane + 32] = ax.y;
+        part[w][1][lane] = ay.x;
+        part[w][1][lane + 32] = ay.y;
+        __syncthreads();
+        if (w == 0) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int e = h == 0 ? e0 : e1;
+                if (e >= cnt) continue;
+                const int slot = lane + 32 * h;
+                float sx = 0.f, sy = 0.f;
+#pragma unroll
+                for (int u = 0; u < kNearWarps; ++u) {
+                    sx += part[u][0][slot];
+                    sy += part[u][1][slot];
+                }
+                // A' = (-sum wm dy, sum wm dx, 0); A = R A' (rotation columns = coil axes, Tp[4a + b]).
+                const float a0 = -scale * sx, a1 = scale * sy;
+                float* o = out + (static_cast<long long>(p) * n_nodes + (h == 0 ? i0 : i1)) * 3;
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    o[r] = static_cast<float>(Tp[4 * r]) * a0 + static_cast<float>(Tp[4 * r + 1]) * a1;
+            }
         }
         __syncthreads();
     }
@@ -537,8 +581,8 @@ void dadt_table(const Mesh& m, const CoilTable& tb, const double* transforms_dev
 
 void dadt_near_zcoil(const Mesh& m, const void* zpacked, int n_dip, const double* transforms_dev, int k, double didt,
                      float* out, const int* near_list, const int* near_cnt, cudaStream_t s, int max_blocks) {
-    const long long items = static_cast<long long>((m.n_nodes + 31) / 32) * k;
-    dadt_near_zcoil_kernel<<<bounded(items, max_blocks, 4096), 32 * kNearWarps, 0, s>>>(
+    const long long items = static_cast<long long>((m.n_nodes + 63) / 64) * k;
+    dadt_near_zcoil_kernel<<<bounded(items, max_blocks, 1184), 32 * kNearWarps, 0, s>>>(
         m.nodes.get(), m.n_nodes, static_cast<const ZDipolePacked*>(zpacked), n_dip, transforms_dev, k,
         static_cast<float>(didt * 1e-7), out, near_list, near_cnt);
     count_launch();
