@@ -408,6 +408,156 @@ __global__ void __launch_bounds__(kColBlock) prolong_cols_kernel(int n, const in
     for (int u = 0; u < C; ++u) xf[q + u] += v[u];
 }
 
+// The same for operators walked by TPR sub-lanes per row (coarse levels, long rows), when a row's
+// TPR x K/C threads fit in one warp: each sub-lane takes its strided share of the row eight entries
+// at a time (index and value loads, then the gathers, then the multiply-adds in order, as
+// strided_dot<T, TPR>), and the shares are combined by the XOR butterfly of group_row_dot: the same
+// pairing tree per column, so the sums are bitwise those of the one-column kernels.
+template <int K, int TPR, int C>
+struct SubColLanes {
+    static constexpr int kLanes = K / C;                     // column groups per row
+    static constexpr int kThreads = TPR * kLanes;            // threads per row (<= 32)
+    static constexpr int kRows = kColBlock / kThreads;       // rows per block
+};
+
+template <int K, int TPR, int C>
+unsigned subcol_grid(int n) {
+    return static_cast<unsigned>((n + SubColLanes<K, TPR, C>::kRows - 1) / SubColLanes<K, TPR, C>::kRows);
+}
+
+template <typename T, int K, int TPR, int C>
+__device__ __forceinline__ void sub_row_dot_cols(const int* __restrict__ ptr, const int* __restrict__ col,
+                                                 const T* __restrict__ val, const T* __restrict__ x, int row,
+                                                 bool valid, int sub, int g, T acc[C]) {
+    constexpr int B = 8;
+#pragma unroll
+    for (int u = 0; u < C; ++u) acc[u] = T(0);
+    if (valid) {
+        const int e = ptr[row + 1];
+        for (int p = ptr[row] + sub; p < e; p += B * TPR) {
+            int cj[B];
+            T vj[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                const int q = p + j * TPR;
+                const bool ok = q < e;
+                cj[j] = ok ? col[q] : 0;
+                vj[j] = ok ? val[q] : T(0);
+            }
+            T xj[B][C];
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                if (p + j * TPR < e) {
+                    gather_cols<T, K, C>(x, cj[j], g, xj[j]);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < C; ++u) xj[j][u] = T(0);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < B; ++j)
+                if (p + j * TPR < e) {
+#pragma unroll
+                    for (int u = 0; u < C; ++u) acc[u] += vj[j] * xj[j][u];
+                }
+        }
+    }
+#pragma unroll
+    for (int off = TPR / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int u = 0; u < C; ++u) acc[u] += __shfl_xor_sync(0xffffffffu, acc[u], off * (K / C));
+}
+
+template <typename T, int K, int TPR, int C>
+struct SubColSlot {
+    int row, sub, g;
+    __device__ __forceinline__ SubColSlot() {
+        using S = SubColLanes<K, TPR, C>;
+        const int t = threadIdx.x;
+        row = blockIdx.x * S::kRows + t / S::kThreads;
+        sub = (t / S::kLanes) % TPR;
+        g = t % S::kLanes;
+    }
+};
+
+template <typename T, int K, int TPR, int C>
+__global__ void __launch_bounds__(kColBlock) cheby_subcols_kernel(int n, const int* __restrict__ ptr,
+                                                                  const int* __restrict__ col,
+                                                                  const T* __restrict__ val,
+                                                                  const T* __restrict__ dinv, const T* __restrict__ b,
+                                                                  const T* __restrict__ x_cur, const T* x_prev,
+                                                                  T c_cur, T c_prev, T alpha, T* out) {
+    pdl_enter();
+    const SubColSlot<T, K, TPR, C> s;
+    const bool valid = s.row < n;
+    T ax[C];
+    sub_row_dot_cols<T, K, TPR, C>(ptr, col, val, x_cur, s.row, valid, s.sub, s.g, ax);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.g * C;
+    const T d = dinv[s.row];
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+        const T cur = x_cur[q + u];
+        const T prev = x_prev[q + u];
+        const T rhs = b[q + u];
+        out[q + u] = c_cur * cur + c_prev * prev + alpha * d * (rhs - ax[u]);
+    }
+}
+
+template <typename T, int K, int TPR, int C>
+__global__ void __launch_bounds__(kColBlock) residual_subcols_kernel(int n, const int* __restrict__ ptr,
+                                                                     const int* __restrict__ col,
+                                                                     const T* __restrict__ val,
+                                                                     const T* __restrict__ x, const T* __restrict__ b,
+                                                                     T* __restrict__ r) {
+    pdl_enter();
+    const SubColSlot<T, K, TPR, C> s;
+    const bool valid = s.row < n;
+    T ax[C];
+    sub_row_dot_cols<T, K, TPR, C>(ptr, col, val, x, s.row, valid, s.sub, s.g, ax);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.g * C;
+#pragma unroll
+    for (int u = 0; u < C; ++u) r[q + u] = b[q + u] - ax[u];
+}
+
+template <typename T, int K, int TPR, int C>
+__global__ void __launch_bounds__(kColBlock) restrict_subcols_kernel(int nc, const int* __restrict__ ptr,
+                                                                     const int* __restrict__ col,
+                                                                     const T* __restrict__ val,
+                                                                     const T* __restrict__ rf, T* __restrict__ bc,
+                                                                     const T* __restrict__ dinv_c, T alpha0,
+                                                                     T* __restrict__ xc) {
+    pdl_enter();
+    const SubColSlot<T, K, TPR, C> s;
+    const bool valid = s.row < nc;
+    T v[C];
+    sub_row_dot_cols<T, K, TPR, C>(ptr, col, val, rf, s.row, valid, s.sub, s.g, v);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.g * C;
+#pragma unroll
+    for (int u = 0; u < C; ++u) {
+        bc[q + u] = v[u];
+        if (dinv_c != nullptr) xc[q + u] = alpha0 * dinv_c[s.row] * v[u];
+    }
+}
+
+template <typename T, int K, int TPR, int C>
+__global__ void __launch_bounds__(kColBlock) prolong_subcols_kernel(int n, const int* __restrict__ ptr,
+                                                                    const int* __restrict__ col,
+                                                                    const T* __restrict__ val,
+                                                                    const T* __restrict__ xc, T* __restrict__ xf) {
+    pdl_enter();
+    const SubColSlot<T, K, TPR, C> s;
+    const bool valid = s.row < n;
+    T v[C];
+    sub_row_dot_cols<T, K, TPR, C>(ptr, col, val, xc, s.row, valid, s.sub, s.g, v);
+    if (!valid || s.sub != 0) return;
+    const long q = static_cast<long>(s.row) * K + s.g * C;
+#pragma unroll
+    for (int u = 0; u < C; ++u) xf[q + u] += v[u];
+}
+
 // Calls f(std::integral_constant<int, C>) with the widest lane width C <= lane_cols that divides K
 // (C > 1), and returns whether it did.
 template <int K, typename F>
@@ -425,6 +575,39 @@ bool dispatch_cols(int lane_cols, F&& f) {
         }
     }
     return false;
+}
+
+// Calls f(std::integral_constant<int, TPR>, std::integral_constant<int, 2>) when an operator walked by
+// tpr > 1 sub-lanes takes column pairs (lane_cols >= 2, K even, a row's threads within one warp),
+// and returns whether it did.
+template <int K, typename F>
+bool dispatch_subcols(int tpr, int lane_cols, F&& f) {
+    if constexpr (K % 2 == 0) {
+        if (lane_cols < 2) return false;
+        constexpr int L = K / 2;
+        auto go = [&](auto tc) {
+            constexpr int TPR = decltype(tc)::value;
+            if constexpr (TPR * L <= 32) {
+                f(tc, std::integral_constant<int, 2>{});
+                return true;
+            } else {
+                return false;
+            }
+        };
+        switch (tpr) {
+            case 2: return go(std::integral_constant<int, 2>{});
+            case 4: return go(std::integral_constant<int, 4>{});
+            case 8: return go(std::integral_constant<int, 8>{});
+            case 16: return go(std::integral_constant<int, 16>{});
+            case 32: return go(std::integral_constant<int, 32>{});
+            default: return false;
+        }
+    } else {
+        (void)tpr;
+        (void)lane_cols;
+        (void)f;
+        return false;
+    }
 }
 
 template <int K, typename F>
@@ -1171,6 +1354,15 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
             count_launch();
             return;
         }
+        if (lv.tpr_a > 1 && dispatch_subcols<K>(lv.tpr_a, cols, [&](auto tc, auto cc_) {
+                constexpr int TPR = decltype(tc)::value;
+                constexpr int C = decltype(cc_)::value;
+                launch_loop(pdl, cheby_subcols_kernel<T, K, TPR, C>, subcol_grid<K, TPR, C>(lv.n), kColBlock, s, lv.n,
+                            lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), ldinv<T>(l), bi, cur, prev, cc, cp, al, out);
+            })) {
+            count_launch();
+            return;
+        }
         dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
             launch_loop(pdl, cheby_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n), Group<K, TPR>::kBlock, s, lv.n,
@@ -1229,11 +1421,19 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
             count_launch();
         }
         sweep(l, bi, nullptr, first, other, nullptr);
-        const bool grouped = lv.tpr_a == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
-            constexpr int C = (std::is_same<T, double>::value && decltype(cc_)::value == 4) ? 2 : decltype(cc_)::value;
-            launch_loop(pdl, residual_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n, lv.a.ptr.get(),
-                        lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
-        });
+        const bool grouped =
+            (lv.tpr_a == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
+                 constexpr int C =
+                     (std::is_same<T, double>::value && decltype(cc_)::value == 4) ? 2 : decltype(cc_)::value;
+                 launch_loop(pdl, residual_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n,
+                             lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
+             })) ||
+            (lv.tpr_a > 1 && dispatch_subcols<K>(lv.tpr_a, cols, [&](auto tc, auto cc_) {
+                 constexpr int TPR = decltype(tc)::value;
+                 constexpr int C = decltype(cc_)::value;
+                 launch_loop(pdl, residual_subcols_kernel<T, K, TPR, C>, subcol_grid<K, TPR, C>(lv.n), kColBlock, s,
+                             lv.n, lv.a.ptr.get(), lv.a.col.get(), lval<T>(l), w.x[l].get(), bi, w.r[l].get());
+             }));
         if (!grouped) {
             dispatch_tpr<K>(lv.tpr_a, [&](auto tc) {
                 constexpr int TPR = decltype(tc)::value;
@@ -1251,7 +1451,14 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
             nx = nodd ? w.x[l + 1].get() : w.r[l + 1].get();
             nd = ldinv<T>(l + 1);
         }
-        dispatch_tpr<K>(lv.tpr_r, [&](auto tc) {
+        const bool rgrouped = lv.tpr_r > 1 && dispatch_subcols<K>(lv.tpr_r, cols, [&](auto tc, auto cc_) {
+            constexpr int TPR = decltype(tc)::value;
+            constexpr int C = decltype(cc_)::value;
+            launch_loop(pdl, restrict_subcols_kernel<T, K, TPR, C>, subcol_grid<K, TPR, C>(lv.n_coarse), kColBlock, s,
+                        lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(), rval<T>(l), w.r[l].get(), nb, nd,
+                        static_cast<T>(ch.alpha0), nx);
+        });
+        if (!rgrouped) dispatch_tpr<K>(lv.tpr_r, [&](auto tc) {
             constexpr int TPR = decltype(tc)::value;
             launch_loop(pdl, restrict_kernel<T, K, TPR>, group_grid<K, TPR>(lv.n_coarse), Group<K, TPR>::kBlock, s,
                         lv.n_coarse, lv.r.ptr.get(), lv.r.col.get(), rval<T>(l), w.r[l].get(), nb, nd,
@@ -1266,11 +1473,19 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     for (int l = L - 1; l >= 0; --l) {
         const Level& lv = H.levels[l];
         const T* bi = (l == 0) ? b : w.b[l].get();
-        const bool grouped = lv.tpr_p == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
-            constexpr int C = (std::is_same<T, double>::value && decltype(cc_)::value == 4) ? 2 : decltype(cc_)::value;
-            launch_loop(pdl, prolong_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n, lv.p.ptr.get(),
-                        lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
-        });
+        const bool grouped =
+            (lv.tpr_p == 1 && dispatch_cols<K>(cols, [&](auto cc_) {
+                 constexpr int C =
+                     (std::is_same<T, double>::value && decltype(cc_)::value == 4) ? 2 : decltype(cc_)::value;
+                 launch_loop(pdl, prolong_cols_kernel<T, K, C>, col_grid<K, C>(lv.n), kColBlock, s, lv.n,
+                             lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
+             })) ||
+            (lv.tpr_p > 1 && dispatch_subcols<K>(lv.tpr_p, cols, [&](auto tc, auto cc_) {
+                 constexpr int TPR = decltype(tc)::value;
+                 constexpr int C = decltype(cc_)::value;
+                 launch_loop(pdl, prolong_subcols_kernel<T, K, TPR, C>, subcol_grid<K, TPR, C>(lv.n), kColBlock, s,
+                             lv.n, lv.p.ptr.get(), lv.p.col.get(), pval<T>(l), xc, w.x[l].get());
+             }));
         if (!grouped) {
             dispatch_tpr<K>(lv.tpr_p, [&](auto tc) {
                 constexpr int TPR = decltype(tc)::value;
