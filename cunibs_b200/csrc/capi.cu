@@ -247,10 +247,11 @@ std::size_t slot_bytes(const cunibs_context* c, const cunibs_solve_opts* opts, i
 // elements, and the right-hand side, into a free slot. Device inputs are read asynchronously and
 // must stay valid until the block is finished; host inputs are copied into the slot first.
 // bounded_dadt gives the dA/dt kernel a bounded grid, for a preparation that runs beside another
-// block's solve. Returns the block's ticket.
+// block's solve. The element average of dA/dt is formed when the block's recovery reads it (raw and
+// SPR) or keep_elements asks for it (a conductivity study's block). Returns the block's ticket.
 long long prepare_block(cunibs_context* c, const double* pos, const double* mom, int n_dip, const double* centers,
                         const double* handles, const double* dists, int k, double didt, const cunibs_solve_opts* opts,
-                        bool host_inputs, bool bounded_dadt) {
+                        bool host_inputs, bool bounded_dadt, bool keep_elements = false) {
     require(!c->study, "a conductivity study is open: end it (cunibs_sigma_end) before solving other blocks");
     require(k >= 1, "need at least one placement");
     require(n_dip >= 1, "the coil needs at least one dipole");
@@ -359,10 +360,15 @@ long long prepare_block(cunibs_context* c, const double* pos, const double* mom,
     if (use_table)
         CUNIBS_CHECK(cudaMemcpyAsync(sl.h_near, sl.near_cnt.get(), sizeof(int) * k, cudaMemcpyDeviceToHost, ps));
     mark(2);
-    sl.dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
-    dadt_elements(m, sl.dadt_nodes.get(), k, sl.dadt_elm.get(), ps);
+    if (keep_elements || rec_mode != kRecHarmonic) {
+        sl.dadt_elm.reserve(static_cast<std::size_t>(m.n_tets) * 3 * k);
+        dadt_elements(m, sl.dadt_nodes.get(), k, sl.dadt_elm.get(), ps);
+    }
     sl.B.reserve(static_cast<std::size_t>(n_red) * K);
-    rhs_block(m, sl.dadt_elm.get(), k, K, sl.B.get(), ps);
+    // A conductivity study forms every draw's right-hand side from the element average, its nominal
+    // one included; other blocks take it from the nodal field directly.
+    if (keep_elements) rhs_block(m, sl.dadt_elm.get(), k, K, sl.B.get(), ps);
+    else rhs_block_nodes(m, sl.dadt_nodes.get(), k, K, sl.B.get(), ps);
     mark(3);
     CUNIBS_CHECK(cudaEventRecord(sl.prepared, ps));
     PendingBlock pb;
@@ -928,7 +934,7 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         }
         // The block's coil field, kept in its slot for every draw, and the nominal solution.
         const long long ticket = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k,
-                                               didt, opts, true, false);
+                                               didt, opts, true, false, true);
         st->slot = c->pending.back().slot;
         SolveStats ss;
         const PendingBlock pb = finish_block(c, ticket, ss, false);

@@ -283,6 +283,50 @@ __global__ void __launch_bounds__(64 * K) rhs_kernel(const float* __restrict__ e
     b_red[static_cast<long>(r) * K + c] = acc;
 }
 
+// w_ij = sum over entry (i, j)'s element contributions (ascending element) of 1/4 neg_vc[e] g[e, i]:
+// b_i = sum_{corners of i} neg_vc[e] (1/4 sum_{n in e} A_n) . g[e, i] = sum_j w_ij . A_j.
+__global__ void rhs_weights_kernel(const float* __restrict__ g32, const float* __restrict__ neg_vc,
+                                   const int* __restrict__ contrib_ptr, const int* __restrict__ contrib_idx, long nnz,
+                                   float* __restrict__ w) {
+    const long p = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (p >= nnz) return;
+    double ax = 0.0, ay = 0.0, az = 0.0;
+    for (int q = contrib_ptr[p], end = contrib_ptr[p + 1]; q < end; ++q) {
+        const int idx = contrib_idx[q];
+        const long e = idx >> 4;
+        const float* gi = g32 + 12 * e + 3 * ((idx >> 2) & 3);
+        const double sv = 0.25 * static_cast<double>(neg_vc[e]);
+        ax += sv * static_cast<double>(gi[0]);
+        ay += sv * static_cast<double>(gi[1]);
+        az += sv * static_cast<double>(gi[2]);
+    }
+    w[3 * p] = static_cast<float>(ax);
+    w[3 * p + 1] = static_cast<float>(ay);
+    w[3 * p + 2] = static_cast<float>(az);
+}
+
+// b_red[r][c] = sum over row i's stiffness entries of w_ij . dadt_nodes[c][j] in FP64 (entry
+// order), i = r skipping the grounded node; columns past k repeat column k-1.
+template <int K>
+__global__ void __launch_bounds__(64 * K) rhs_nodes_kernel(const float* __restrict__ nodal, const float* __restrict__ w,
+                                                           const int* __restrict__ ptr, const int* __restrict__ col,
+                                                           int n_nodes, int k, int ground, double* __restrict__ b_red) {
+    const int r = blockIdx.x * 64 + threadIdx.x / K;
+    const int c = threadIdx.x % K;
+    if (r >= n_nodes - 1) return;
+    const int i = r + (r >= ground ? 1 : 0);
+    const int src = c < k ? c : k - 1;
+    const float* a = nodal + static_cast<long>(src) * n_nodes * 3;
+    double acc = 0.0;
+    for (int q = ptr[i]; q < ptr[i + 1]; ++q) {
+        const long j = col[q];
+        const float* wq = w + 3 * static_cast<long>(q);
+        acc += static_cast<double>(wq[0]) * a[3 * j] + static_cast<double>(wq[1]) * a[3 * j + 1] +
+               static_cast<double>(wq[2]) * a[3 * j + 2];
+    }
+    b_red[static_cast<long>(r) * K + c] = acc;
+}
+
 }  // namespace
 
 void prep_dipoles(const double* pos, const double* mom, int n_dip, const double* transforms_dev, int k, void* out,
@@ -352,6 +396,33 @@ void dadt_elements(const Mesh& m, const float* nodal, int k, float* elm, cudaStr
     const long total = static_cast<long>(m.n_tets) * k;
     element_average_kernel<<<grid_for(total), kBlock, 0, s>>>(nodal, m.tets.get(), m.n_nodes, m.n_tets, k, elm); count_launch();
     CUNIBS_LAUNCH_CHECK("dadt element average");
+}
+
+void rhs_block_nodes(Mesh& m, const float* nodal, int k, int K, double* b_red, cudaStream_t s) {
+    if (!m.rhs_w_ok) {
+        m.rhs_w.resize(3 * static_cast<std::size_t>(m.k_nnz));
+        rhs_weights_kernel<<<grid_for(m.k_nnz), kBlock, 0, s>>>(m.g32.get(), m.neg_vc32.get(), m.contrib_ptr.get(),
+                                                                m.contrib_idx.get(), m.k_nnz, m.rhs_w.get());
+        count_launch();
+        CUNIBS_LAUNCH_CHECK("rhs weights");
+        m.rhs_w_ok = true;
+    }
+    const unsigned g = (m.n_nodes - 1 + 63) / 64;
+    auto go = [&](auto kc) {
+        constexpr int KK = decltype(kc)::value;
+        rhs_nodes_kernel<KK><<<g, 64 * KK, 0, s>>>(nodal, m.rhs_w.get(), m.k_ptr.get(), m.k_col.get(), m.n_nodes, k,
+                                                   m.ground, b_red);
+        count_launch();
+    };
+    switch (K) {
+        case 1: go(std::integral_constant<int, 1>{}); break;
+        case 2: go(std::integral_constant<int, 2>{}); break;
+        case 4: go(std::integral_constant<int, 4>{}); break;
+        case 8: go(std::integral_constant<int, 8>{}); break;
+        case 16: go(std::integral_constant<int, 16>{}); break;
+        default: fail(kEInval, "block width must be one of {1, 2, 4, 8, 16}");
+    }
+    CUNIBS_LAUNCH_CHECK("rhs from nodes");
 }
 
 void rhs_block(const Mesh& m, const float* elm, int k, int K, double* b_red, cudaStream_t s, const float* neg_vc) {

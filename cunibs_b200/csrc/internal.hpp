@@ -115,6 +115,12 @@ struct Mesh {
     DevArray<int> contrib_idx;  // (16M) e*16 + i*4 + j, ascending e within each entry
     DevArray<double> k_val;     // (nnz) FP64
     long k_nnz = 0;
+    // Right-hand side weights per stiffness entry (i, j): w_ij = sum over the elements e holding both
+    // of 1/4 neg_vc32[e] g32[e, i] (3 components, FP32 from an FP64 sum in contribution order), so the
+    // block right-hand side is b_i = sum_j w_ij . dA/dt_j from the nodal field. Built on first use,
+    // stale (rhs_w_ok false) once the element conductivities change.
+    DevArray<float> rhs_w;
+    bool rhs_w_ok = false;
     int ground = 0;
     // Gray-matter slice (tag 2): element index, FP32 volumes, barycentres.
     DevArray<int> gm_index;
@@ -268,6 +274,9 @@ void set_last_error(const std::string& message);
 // neg_vc: the per-element weights -(vol * sigma) in FP32 (null: the mesh's own).
 void rhs_block(const Mesh& m, const float* dadt_elm, int k, int k_pad, double* b_red /* (N-1, k_pad) */,
                cudaStream_t s, const float* neg_vc = nullptr);
+// The same right-hand side from the nodal dA/dt (k, N, 3) through the mesh's rhs_w (built here when
+// stale): equal to rhs_block of the element average up to rounding, with no element pass.
+void rhs_block_nodes(Mesh& m, const float* dadt_nodes, int k, int k_pad, double* b_red, cudaStream_t s);
 
 // Post-processing (post.cu).
 void reconstruct_block(const Mesh& m, const double* x_red /* (N-1,k_pad) */, int k, int k_pad,

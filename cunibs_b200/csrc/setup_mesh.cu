@@ -636,6 +636,7 @@ void set_element_conductivity(Mesh& m, const double* sigma_by_tag, cudaStream_t 
     // The right-hand side weighs each element by the same conductivity.
     neg_vc_kernel<<<grid_for(m.n_tets), kBlock, 0, s>>>(m.vols32.get(), m.cond.get(), m.n_tets, m.neg_vc32.get());
     count_launch();
+    m.rhs_w_ok = false;
 }
 
 void assemble_stiffness(Mesh& m, const double* sigma_by_tag, cudaStream_t s) {
