@@ -612,7 +612,7 @@ def conductivity_draws(ctx, coil, centers, handles, dists, recovery, stream, n_d
         t0 = time.perf_counter()
         begin_ms, ranks = device_ms(lambda: ctx.sigma_begin(coil, centers, handles, dists, 1e6, nominal, tags,
                                                             recovery=recovery))
-        begin_runs.append((round(begin_ms, 3), round(1e3 * (time.perf_counter() - t0), 3)))
+        begin_runs.append((round(begin_ms, 3), round(1e3 * (time.perf_counter() - t0), 3), ctx.phase_times()))
         if rep == 0:
             ctx.sigma_end()
     guesses = {}

@@ -147,6 +147,7 @@ def load() -> C.CDLL:
         "cunibs_context_set_overlap": ([_vp, C.c_int], C.c_int),
         "cunibs_context_set_coil_table": ([_vp, C.c_int, C.c_double, C.c_double], C.c_int),
         "cunibs_context_coil_table_info": ([_vp, _vp], C.c_int),
+        "cunibs_context_phase_times": ([_vp, _vp], C.c_int),
         "cunibs_context_set_conductivity": ([_vp, dp], C.c_int),
         "cunibs_context_set_conductivity_keep_coarse": ([_vp, dp], C.c_int),
         "cunibs_sigma_begin": ([_vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.c_int, C.c_double, C.POINTER(SolveOpts), dp, ip,
@@ -473,6 +474,13 @@ class Context:
         once per coil for nodes deeper than near_mm below the coil (enabled), or sum every dipole at
         every node (not enabled)."""
         check(self._lib.cunibs_context_set_coil_table(self.handle, 1 if enabled else 0, float(near_mm), float(step)))
+
+    def phase_times(self) -> list[float]:
+        """cunibs_context_phase_times: host milliseconds to the end of each phase of the last
+        cunibs_sigma_begin."""
+        out = np.zeros(8, np.float64)
+        check(self._lib.cunibs_context_phase_times(self.handle, out.ctypes.data))
+        return [round(float(v), 3) for v in out]
 
     def coil_table_info(self) -> dict:
         """cunibs_context_coil_table_info as a dict."""

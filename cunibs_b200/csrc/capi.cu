@@ -1,5 +1,6 @@
 // The C ABI (include/cunibs_b200.h): context lifetime, the block solve, stage-level entry points.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <climits>
 #include <cstdio>
@@ -140,6 +141,9 @@ struct cunibs_context {
     double table_near_m = 0.015, table_step = 0.035;
     double mesh_rho_m = 0.0;  // largest distance of a node from the centre of the mesh's bounding box
     long long last_near = -1, last_near_of = 0;  // direct-sum nodes of the last finished block
+    // Host wall-clock milliseconds from the start of the last cunibs_sigma_begin to the end of each of
+    // its phases (cunibs_context_phase_times).
+    double phase_ms[8] = {};
     int sm_count = 0;
     // Field-recovery operators, built on first use per mode, and their block workspace.
     std::unique_ptr<RecoveryOp> rec[4];
@@ -822,6 +826,13 @@ int cunibs_context_pending(const cunibs_context* c, int* n) {
     });
 }
 
+int cunibs_context_phase_times(const cunibs_context* c, double* out) {
+    return guarded([&] {
+        require(c != nullptr && out != nullptr, "NULL argument");
+        std::copy(c->phase_ms, c->phase_ms + 8, out);
+    });
+}
+
 int cunibs_context_set_coil_table(cunibs_context* c, int mode, double near_mm, double step) {
     return guarded([&] {
         require(c != nullptr, "NULL context");
@@ -909,9 +920,16 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         DeviceGuard dg(c->device);
         Mesh& m = c->mesh;
         cudaStream_t s = c->stream;
+        const auto t_begin = std::chrono::steady_clock::now();
+        auto phase = [&](int i) {
+            c->phase_ms[i] =
+                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+        };
+        for (double& v : c->phase_ms) v = 0.0;
         // The context at the nominal conductivities, its coarse levels kept.
         assemble_stiffness(m, st->nominal, s);
         c->keep_coarse_values();
+        phase(0);
         require(!c->hier.levels.empty(), "the operator is too small for a conductivity study (it has no AMG level)");
         const Level& L0 = c->hier.levels[0];
         st->nnz = L0.a.nnz;
@@ -932,12 +950,16 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
             if (!(rel <= 1e-10))
                 fail(kEInternal, "conductivity decomposition mismatch (relative difference " + std::to_string(rel) + ")");
         }
+        phase(1);
         // The block's coil field, kept in its slot for every draw, and the nominal solution.
         const long long ticket = prepare_block(c, dip_pos_m, dip_moment, n_dip, centers_mm, handles_mm, dists_mm, k,
                                                didt, opts, true, false, true);
         st->slot = c->pending.back().slot;
+        CUNIBS_CHECK(cudaStreamSynchronize(c->prep));
+        phase(2);
         SolveStats ss;
         const PendingBlock pb = finish_block(c, ticket, ss, false);
+        phase(3);
         st->k = pb.k;
         st->K = pb.K;
         st->has_handles = pb.has_handles;
@@ -960,6 +982,7 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
                           wts.get() + static_cast<std::size_t>(t) * m.n_tets);
             CUNIBS_CHECK(cudaStreamSynchronize(s));  // td and wts leave scope
         }
+        phase(4);
         st->x_nom.resize(static_cast<std::size_t>(n_red) * K);
         CUNIBS_CHECK(cudaMemcpyAsync(st->x_nom.get(), c->X.get(), sizeof(double) * n_red * K, cudaMemcpyDeviceToDevice, s));
         // Sensitivity right-hand sides c_t = b_t - A_t x_nom, and which are nonzero (a tissue with no
@@ -976,6 +999,7 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
                     active[static_cast<std::size_t>(j) * P + a] = 1;
                     cols.emplace_back(a, j);
                 }
+        phase(5);
         // Sensitivities s_t = A_nom^-1 c_t to a loose tolerance (run.py:44-49: they only span the
         // guess's subspace; every draw is still solved to the full tolerance), in blocks as wide as
         // the solver's workspace already is (growing it would reallocate it and drop its graphs).
@@ -999,6 +1023,8 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
                 sigma_unpack(Xw.get(), n_red, P, K, cm, W, st->S.get(), s);
             }
         }
+        CUNIBS_CHECK(cudaStreamSynchronize(s));
+        phase(6);
         // Per placement: the A_nom-Gram of its sensitivities and their products with the c_t give
         // the map from a draw's conductivity change to its subspace coefficients.
         DevArray<double> AS(npk);
@@ -1014,6 +1040,7 @@ int cunibs_sigma_begin(cunibs_context* c, const double* dip_pos_m, const double*
         if (basis_rank)
             for (int j = 0; j < st->k; ++j) basis_rank[j] = st->rank[j];
         c->study = std::move(st);
+        phase(7);
     });
 }
 

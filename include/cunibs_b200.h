@@ -210,6 +210,12 @@ int cunibs_context_set_coil_table(cunibs_context* ctx, int mode, double near_mm,
  * given the dipole sum in the last finished block (-1 when it did not read the table), nodes x
  * placements of that block. */
 int cunibs_context_coil_table_info(const cunibs_context* ctx, double* out);
+/* Diagnostics of the last cunibs_sigma_begin on this context (no counterpart in the reference):
+ * out[8] = host wall-clock milliseconds from the call's start to the end of each phase: 0 nominal
+ * assembly and kept hierarchy, 1 operator components, 2 the block's coil field, 3 its nominal solve,
+ * 4 per-tissue right-hand sides, 5 sensitivity right-hand sides, 6 sensitivity solves, 7 the guess
+ * coefficients. */
+int cunibs_context_phase_times(const cunibs_context* ctx, double* out);
 
 /* Re-assembles the stiffness with a new conductivity per tissue tag (sigma_by_tag[0..10], S/m;
  * index = tag) and rebuilds the AMG hierarchy: the per-sample step of a conductivity Monte Carlo
