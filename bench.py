@@ -256,6 +256,8 @@ def run_ours(args) -> dict:
         args.precision]
     if args.cheby_degree > 0:
         p.cheby_degree = args.cheby_degree
+    if args.cheby_lower_ratio > 0:
+        p.cheby_lower_ratio = args.cheby_lower_ratio
     t0 = time.perf_counter()
     ctx = _native.Context(mesh.nodes_mm, mesh.tet_nodes, mesh.tet_tags, mesh.skin_tris, p)
     setup_s = time.perf_counter() - t0
@@ -495,6 +497,7 @@ def run_ours(args) -> dict:
                                                  "beside the solve of step i",
                                      "overlap_blocks_per_sm": args.overlap if args.overlap > 0 else 2,
                                      "cheby_degree": int(p.cheby_degree),
+                                     "cheby_lower_ratio": float(p.cheby_lower_ratio),
                                      "coil_field": ("table (coil-frame samples, tricubic) beyond 15 mm of the "
                                                     "coil, dipole sum nearer" if use_table
                                                     else "dipole sum at every node"),
@@ -1063,6 +1066,8 @@ def main() -> None:
     ap.add_argument("--hidden", type=int, default=512, help="width of the warm-start network's hidden layers")
     ap.add_argument("--epochs", type=int, default=400, help="training epochs of the warm-start network")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cheby-lower-ratio", type=float, default=0.0,
+                    help="Chebyshev smoother's interval [lambda_max / ratio, lambda_max] (0: the reference's 12)")
     ap.add_argument("--cheby-degree", type=int, default=0,
                     help="Chebyshev smoother degree of the V-cycle (0: the reference's default, 2)")
     ap.add_argument("--coil-field", choices=["table", "direct"], default="table",
