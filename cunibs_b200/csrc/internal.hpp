@@ -66,7 +66,7 @@ struct Level {
 };
 
 // Sub-lanes per row for an SpMV-shaped kernel over n_rows rows and nnz entries: one while the rows
-// alone fill the GPU, otherwise enough that each walks about eight entries (a power of two up to 32).
+// alone fill the GPU, otherwise enough that each walks about sixteen entries (a power of two up to 32).
 int choose_tpr(int n_rows, long nnz);
 
 struct Hierarchy {
