@@ -637,7 +637,7 @@ int cunibs_context_create(const double* nodes_mm, int n_nodes, const int* tet_no
         c->prm.inner_reduction = p.inner_reduction;
         c->prm.inner_max_iters = p.inner_max_iters;
         c->prm.iters_per_sync = p.iters_per_sync > 0 ? p.iters_per_sync : 4;
-        require(p.dense_max_rows >= 0 && p.dense_max_rows <= 4096, "dense_max_rows must be in [0, 4096]");
+        require(p.dense_max_rows >= 0 && p.dense_max_rows <= 16384, "dense_max_rows must be in [0, 16384]");
         c->prm.dense_max_rows = p.dense_max_rows;
         require(c->prm.tolerance > 0 && c->prm.max_iters > 0, "tolerance and max_iters must be positive");
         int least = 0, greatest = 0;
@@ -1425,6 +1425,7 @@ int cunibs_context_array(const cunibs_context* c, const char* name, int level, v
         const std::string n(name);
         const void* src = nullptr;
         std::size_t count = 0, elem = 4;
+        std::size_t pitch = 0, row_bytes = 0;  // a dense matrix stored with padded rows
         auto pick = [&](const void* p, std::size_t cnt, std::size_t es) {
             src = p;
             count = cnt;
@@ -1450,7 +1451,11 @@ int cunibs_context_array(const cunibs_context* c, const char* name, int level, v
         else if (n == "coarse_ptr") pick(h.coarse.ptr.get(), h.nc + 1, 4);
         else if (n == "coarse_col") pick(h.coarse.col.get(), h.coarse.nnz, 4);
         else if (n == "coarse_val") pick(h.coarse.val.get(), h.coarse.nnz, 8);
-        else if (n == "coarse_inv") pick(h.coarse_inv.get(), static_cast<std::size_t>(h.nc) * h.nc, 8);
+        else if (n == "coarse_inv") {
+            pick(h.coarse_inv.get(), static_cast<std::size_t>(h.nc) * h.nc, 8);
+            pitch = static_cast<std::size_t>(dense_ld(h.nc)) * 8;
+            row_bytes = static_cast<std::size_t>(h.nc) * 8;
+        }
         else if (lv_ok && n == "a_ptr") pick(h.levels[level].a.ptr.get(), h.levels[level].n + 1, 4);
         else if (lv_ok && n == "a_col") pick(h.levels[level].a.col.get(), h.levels[level].a.nnz, 4);
         else if (lv_ok && n == "a_val") pick(h.levels[level].a.val.get(), h.levels[level].a.nnz, 8);
@@ -1461,7 +1466,10 @@ int cunibs_context_array(const cunibs_context* c, const char* name, int level, v
         else if (lv_ok && n == "dinv") pick(h.levels[level].dinv.get(), h.levels[level].n, 8);
         else fail(kEInval, "unknown array name or level: " + n);
         *len = static_cast<long long>(count);
-        if (out && count) {
+        if (out && count && pitch) {
+            const std::size_t rows = std::min<std::size_t>(count, static_cast<std::size_t>(cap)) * elem / row_bytes;
+            CUNIBS_CHECK(cudaMemcpy2D(out, row_bytes, src, pitch, row_bytes, rows, cudaMemcpyDeviceToHost));
+        } else if (out && count) {
             const std::size_t nb = std::min<std::size_t>(count, static_cast<std::size_t>(cap)) * elem;
             CUNIBS_CHECK(cudaMemcpy(out, src, nb, cudaMemcpyDeviceToHost));
         }

@@ -33,7 +33,7 @@ struct Params {
     double inner_reduction = 1e-4;  // deepest residual reduction asked of one inner FP32 solve
     int inner_max_iters = 60;
     int iters_per_sync = 4;         // PCG iterations launched between host convergence checks
-    int dense_max_rows = 1024;      // the V-cycle ends in an exact dense solve at the first level
+    int dense_max_rows = 12288;     // the V-cycle ends in an exact dense solve at the first level
                                     // below the finest with at most this many rows (0: at the coarsest)
 };
 
@@ -69,11 +69,15 @@ struct Level {
 // alone fill the GPU, otherwise enough that each walks about sixteen entries (a power of two up to 32).
 int choose_tpr(int n_rows, long nnz);
 
+// Row length (entries) of a dense inverse of n rows: rows start on 32-byte boundaries in FP64 and
+// 16-byte boundaries in FP32, padded with zeros past column n.
+inline int dense_ld(int n) { return (n + 3) / 4 * 4; }
+
 struct Hierarchy {
     std::vector<Level> levels;
     DevCsr<double> coarse;
     int nc = 0;
-    DevArray<double> coarse_inv;   // dense (nc, nc), FP64 from a Cholesky factorisation
+    DevArray<double> coarse_inv;   // dense (nc, dense_ld(nc)), FP64
     DevArray<float> coarse_inv32;
     // Where the V-cycle stops: it smooths levels [0, vcycle_levels) and solves the operator below
     // them exactly with the dense inverse bottom_inv (bottom_n rows): levels[vcycle_levels].a, or
@@ -81,6 +85,7 @@ struct Hierarchy {
     int vcycle_levels = 0;
     int bottom_n = 0;
     DevArray<double> level_inv;    // dense inverse of levels[vcycle_levels].a when the V-cycle stops early
+                                   // (bottom_n, dense_ld(bottom_n))
     DevArray<float> level_inv32;
     std::vector<int> sizes;
     Cheby cheby;

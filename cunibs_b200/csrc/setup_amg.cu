@@ -575,62 +575,202 @@ __global__ void compose_kernel(int* __restrict__ agg, const int* __restrict__ st
     if (i < n) agg[i] = step[agg[i]];
 }
 
-// --- coarse Cholesky inverse --------------------------------------------------------------
+// --- dense inverse of the V-cycle's bottom operator ----------------------------------------
+//
+// A blocked sweep (Gauss-Jordan elimination without pivoting, which an SPD matrix never needs) on
+// the lower triangle of the matrix padded to a multiple of kSweepB with an identity block. Sweeping
+// pivot block k with P = A_kk^-1 maps
+//   A_kk -> -P,  A_ik -> C_i = A_ik P,  A_ij -> A_ij - C_i A_kj   (i, j != k),
+// and after every block has been swept the matrix holds -A^-1. Only tiles on or below the block
+// diagonal are stored and updated (A_kj for j > k is read as A_jk^T), so a step is one SYRK-shaped
+// product of about n^2 kSweepB multiply-adds; the whole inverse costs n^3 of them, on every SM.
 
-__global__ void densify_kernel(const int* __restrict__ ptr, const int* __restrict__ col,
-                               const double* __restrict__ val, int n, double* __restrict__ m) {
+constexpr int kSweepB = 64;
+
+__global__ void densify_lower_kernel(const int* __restrict__ ptr, const int* __restrict__ col,
+                                     const double* __restrict__ val, int n, int N, double* __restrict__ m) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    for (int p = ptr[i]; p < ptr[i + 1]; ++p) m[static_cast<long>(i) * n + col[p]] = val[p];
+    if (i >= N) return;
+    if (i >= n) {
+        m[static_cast<long>(i) * N + i] = 1.0;  // identity padding
+        return;
+    }
+    for (int p = ptr[i]; p < ptr[i + 1]; ++p) m[static_cast<long>(i) * N + col[p]] = val[p];
 }
 
-// Left-looking Cholesky L L^T of a dense SPD matrix in place, one block; column j's diagonal by
-// thread 0, then the column below it in parallel. Sums run in ascending k like the CPU restatement.
-__global__ void cholesky_kernel(double* __restrict__ m, int n, int* __restrict__ status) {
-    __shared__ double d_sh;
-    __shared__ int bad;
-    if (threadIdx.x == 0) bad = 0;
+// Tile (I, J) of the symmetric matrix as stored (lower triangle): element (r, c) of the tile.
+__device__ __forceinline__ double sym_tile(const double* __restrict__ m, int N, int I, int J, int r, int c) {
+    const long row = static_cast<long>(I) * kSweepB + r, col = static_cast<long>(J) * kSweepB + c;
+    return (I > J || (I == J && r >= c)) ? m[row * N + col] : m[col * N + row];
+}
+
+// acc (per thread a 4 x 4 patch of a 64 x 64 tile) = X (64 x 64, rows ldx apart) * Y (64 x 64, rows
+// ldy apart); the reduction dimension in chunks of 32 staged (coalesced loads) in `stage`, a
+// shared-memory buffer of kStageDoubles.
+constexpr int kStageDoubles = kSweepB * 33 + 32 * kSweepB;
+
+__device__ __forceinline__ void tile_product(const double* X, long ldx, const double* Y, long ldy, double acc[4][4],
+                                             double* stage) {
+    double (*xs)[33] = reinterpret_cast<double (*)[33]>(stage);
+    double (*ys)[kSweepB] = reinterpret_cast<double (*)[kSweepB]>(stage + kSweepB * 33);
+    const int t = threadIdx.x, ty = t / 16, tx = t % 16;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+    for (int k0 = 0; k0 < kSweepB; k0 += 32) {
+        for (int q = t; q < kSweepB * 32; q += blockDim.x) {
+            xs[q / 32][q % 32] = X[(q / 32) * ldx + k0 + q % 32];
+            ys[q / kSweepB][q % kSweepB] = Y[(k0 + q / kSweepB) * ldy + q % kSweepB];
+        }
+        __syncthreads();
+#pragma unroll 8
+        for (int kk = 0; kk < 32; ++kk) {
+            double xa[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) xa[a] = xs[ty * 4 + a][kk];
+            const double2 y0 = *reinterpret_cast<const double2*>(&ys[kk][tx * 4]);
+            const double2 y1 = *reinterpret_cast<const double2*>(&ys[kk][tx * 4 + 2]);
+            const double yb[4] = {y0.x, y0.y, y1.x, y1.y};
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = fma(xa[a], yb[b], acc[a][b]);
+        }
+        __syncthreads();
+    }
+}
+
+// P = A_kk^-1 of the current pivot block, by a scalar sweep of its 64 pivots in shared memory
+// (which leaves -A_kk^-1). status = 1 when a pivot is not positive (not SPD).
+__global__ void __launch_bounds__(256) sweep_pivot_kernel(const double* __restrict__ m, int N, int k,
+                                                          double* __restrict__ pinv, int* __restrict__ status) {
+    __shared__ double b[kSweepB][kSweepB + 1];
+    __shared__ double dsh;
+    for (int q = threadIdx.x; q < kSweepB * kSweepB; q += blockDim.x)
+        b[q / kSweepB][q % kSweepB] = sym_tile(m, N, k, k, q / kSweepB, q % kSweepB);
     __syncthreads();
-    for (int j = 0; j < n; ++j) {
+    for (int p = 0; p < kSweepB; ++p) {
         if (threadIdx.x == 0) {
-            double d = m[static_cast<long>(j) * n + j];
-            for (int k = 0; k < j; ++k) d -= m[static_cast<long>(j) * n + k] * m[static_cast<long>(j) * n + k];
+            double d = b[p][p];
             if (!(d > 0.0)) {
-                bad = 1;
+                *status = 1;
                 d = 1.0;
             }
-            d = sqrt(d);
-            m[static_cast<long>(j) * n + j] = d;
-            d_sh = d;
+            dsh = d;
         }
         __syncthreads();
-        const double d = d_sh;
-        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
-            double s = m[static_cast<long>(i) * n + j];
-            for (int k = 0; k < j; ++k) s -= m[static_cast<long>(i) * n + k] * m[static_cast<long>(j) * n + k];
-            m[static_cast<long>(i) * n + j] = s / d;
+        const double d = dsh;
+        for (int q = threadIdx.x; q < kSweepB * kSweepB; q += blockDim.x) {
+            const int i = q / kSweepB, j = q % kSweepB;
+            if (i != p && j != p) b[i][j] -= b[i][p] * b[p][j] / d;
         }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kSweepB; i += blockDim.x) {
+            if (i != p) {
+                b[i][p] /= d;
+                b[p][i] /= d;
+            }
+        }
+        if (threadIdx.x == 0) b[p][p] = -1.0 / d;
         __syncthreads();
     }
-    if (threadIdx.x == 0) *status = bad;
+    // P is symmetric; its two rounded halves are averaged so that it is so exactly.
+    for (int q = threadIdx.x; q < kSweepB * kSweepB; q += blockDim.x) {
+        const int i = q / kSweepB, j = q % kSweepB;
+        pinv[q] = -0.5 * (b[i][j] + b[j][i]);
+    }
 }
 
-// inv = L^-T L^-1, one thread per column of the identity.
-__global__ void cholesky_inverse_kernel(const double* __restrict__ L, int n, double* __restrict__ y,
-                                        double* __restrict__ inv) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= n) return;
-    double* yc = y + static_cast<long>(c) * n;
-    for (int i = 0; i < n; ++i) {
-        double s = (i == c) ? 1.0 : 0.0;
-        for (int k = 0; k < i; ++k) s -= L[static_cast<long>(i) * n + k] * yc[k];
-        yc[i] = s / L[static_cast<long>(i) * n + i];
+// For every block row I != k (blockIdx.x = I): the old row panel rbuf[:, I] = A_kI (64 x N, rows N
+// apart) and C_I = A_Ik P into cbuf (N x 64), formed as C_I^T = P A_kI (P is symmetric).
+__global__ void __launch_bounds__(256) sweep_panel_kernel(const double* __restrict__ m, int N, int k,
+                                                          const double* __restrict__ pinv, double* __restrict__ cbuf,
+                                                          double* __restrict__ rbuf) {
+    __shared__ __align__(16) double buf[kStageDoubles];
+    static_assert(kStageDoubles >= kSweepB * (kSweepB + 1), "the staging buffer holds one padded tile");
+    double (*tile)[kSweepB + 1] = reinterpret_cast<double (*)[kSweepB + 1]>(buf);  // A_kI
+    const int I = blockIdx.x;
+    if (I == k) return;
+    for (int q = threadIdx.x; q < kSweepB * kSweepB; q += blockDim.x) {
+        // Read along the stored rows: A_kI itself above the diagonal block, A_Ik below it.
+        if (I < k) {
+            const int r = q / kSweepB, c = q % kSweepB;
+            tile[r][c] = m[(static_cast<long>(k) * kSweepB + r) * N + static_cast<long>(I) * kSweepB + c];
+        } else {
+            const int c = q / kSweepB, r = q % kSweepB;
+            tile[r][c] = m[(static_cast<long>(I) * kSweepB + c) * N + static_cast<long>(k) * kSweepB + r];
+        }
     }
-    for (int i = n - 1; i >= 0; --i) {
-        double s = yc[i];
-        for (int k = i + 1; k < n; ++k) s -= L[static_cast<long>(k) * n + i] * inv[static_cast<long>(k) * n + c];
-        inv[static_cast<long>(i) * n + c] = s / L[static_cast<long>(i) * n + i];
+    __syncthreads();
+    for (int q = threadIdx.x; q < kSweepB * kSweepB; q += blockDim.x) {
+        const int r = q / kSweepB, c = q % kSweepB;
+        rbuf[static_cast<long>(r) * N + static_cast<long>(I) * kSweepB + c] = tile[r][c];
     }
+    __syncthreads();
+    double acc[4][4];
+    tile_product(pinv, kSweepB, rbuf + static_cast<long>(I) * kSweepB, N, acc, buf);
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+            cbuf[(static_cast<long>(I) * kSweepB + tx * 4 + b) * kSweepB + ty * 4 + a] = acc[a][b];
+}
+
+// A_IJ -= C_I A_kJ for the stored tiles I >= J with I, J != k (blockIdx = (J, I)).
+__global__ void __launch_bounds__(256) sweep_update_kernel(double* __restrict__ m, int N, int k,
+                                                           const double* __restrict__ cbuf,
+                                                           const double* __restrict__ rbuf) {
+    __shared__ __align__(16) double buf[kStageDoubles];
+    const int J = blockIdx.x, I = blockIdx.y;
+    if (I < J || I == k || J == k) return;
+    double acc[4][4];
+    tile_product(cbuf + static_cast<long>(I) * kSweepB * kSweepB, kSweepB, rbuf + static_cast<long>(J) * kSweepB, N,
+                 acc, buf);
+    const int ty = threadIdx.x / 16, tx = threadIdx.x % 16;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        double* row = m + (static_cast<long>(I) * kSweepB + ty * 4 + a) * N + static_cast<long>(J) * kSweepB + tx * 4;
+        double2 v0 = *reinterpret_cast<double2*>(row), v1 = *reinterpret_cast<double2*>(row + 2);
+        v0.x -= acc[a][0];
+        v0.y -= acc[a][1];
+        v1.x -= acc[a][2];
+        v1.y -= acc[a][3];
+        *reinterpret_cast<double2*>(row) = v0;
+        *reinterpret_cast<double2*>(row + 2) = v1;
+    }
+}
+
+// The swept pivot row and column: A_Ik = C_I (stored as A_kI = C_I^T above the diagonal), A_kk = -P.
+__global__ void __launch_bounds__(256) sweep_finish_kernel(double* __restrict__ m, int N, int k,
+                                                           const double* __restrict__ pinv,
+                                                           const double* __restrict__ cbuf) {
+    const int I = blockIdx.x;
+    for (int q = threadIdx.x; q < kSweepB * kSweepB; q += blockDim.x) {
+        const int r = q / kSweepB, c = q % kSweepB;
+        if (I == k) {
+            m[(static_cast<long>(k) * kSweepB + r) * N + static_cast<long>(k) * kSweepB + c] = -pinv[q];
+        } else if (I > k) {
+            m[(static_cast<long>(I) * kSweepB + r) * N + static_cast<long>(k) * kSweepB + c] =
+                cbuf[(static_cast<long>(I) * kSweepB + r) * kSweepB + c];
+        } else {
+            m[(static_cast<long>(k) * kSweepB + c) * N + static_cast<long>(I) * kSweepB + r] =
+                cbuf[(static_cast<long>(I) * kSweepB + r) * kSweepB + c];
+        }
+    }
+}
+
+// inv = A^-1 (n x n, rows of ld entries, zero past column n) and its FP32 copy, from the swept
+// lower triangle (-A^-1).
+__global__ void sweep_extract_kernel(const double* __restrict__ m, int N, int n, int ld, double* __restrict__ inv,
+                                     float* __restrict__ inv32) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= static_cast<long>(n) * ld) return;
+    const int i = static_cast<int>(q / ld), j = static_cast<int>(q % ld);
+    const double v = j < n ? -m[static_cast<long>(i >= j ? i : j) * N + (i >= j ? j : i)] : 0.0;
+    inv[q] = v;
+    inv32[q] = static_cast<float>(v);
 }
 
 void tentative(const DevArray<int>& agg, int n, int nc, DevCsr<double>& pt, cudaStream_t s) {
@@ -794,21 +934,36 @@ Cheby make_cheby(int degree, double lower_ratio) {
     return c;
 }
 
-// inv (and its FP32 copy) = the dense inverse of the SPD operator a, through a Cholesky factorisation.
+// inv (and its FP32 copy) = the dense inverse of the SPD operator a, by the blocked sweep; rows of
+// dense_ld(a.n) entries.
 static void dense_inverse(const DevCsr<double>& a, DevArray<double>& inv, DevArray<float>& inv32, const char* what,
-                   cudaStream_t s) {
+                          cudaStream_t s) {
     const int n = a.n;
-    DevArray<double> dense(static_cast<std::size_t>(n) * n), y(static_cast<std::size_t>(n) * n);
-    dense.zero(s);
-    densify_kernel<<<grid_for(n), kBlock, 0, s>>>(a.ptr.get(), a.col.get(), a.val.get(), n, dense.get());
+    const int T = (n + kSweepB - 1) / kSweepB;
+    const int N = T * kSweepB;
+    DevArray<double> m(static_cast<std::size_t>(N) * N), pinv(kSweepB * kSweepB),
+        cbuf(static_cast<std::size_t>(N) * kSweepB), rbuf(static_cast<std::size_t>(N) * kSweepB);
+    m.zero(s);
+    densify_lower_kernel<<<grid_for(N), kBlock, 0, s>>>(a.ptr.get(), a.col.get(), a.val.get(), n, N, m.get());
     count_launch();
     DevArray<int> status(1);
-    cholesky_kernel<<<1, 1024, 0, s>>>(dense.get(), n, status.get()); count_launch();
-    if (read_scalar(status.get(), s)) fail(kEInternal, std::string(what) + " is not positive definite");
-    inv.resize(static_cast<std::size_t>(n) * n);
-    cholesky_inverse_kernel<<<grid_for(n, 64), 64, 0, s>>>(dense.get(), n, y.get(), inv.get()); count_launch();
-    to_f32(inv, static_cast<long>(n) * n, inv32, s);
+    status.zero(s);
+    for (int k = 0; k < T; ++k) {
+        sweep_pivot_kernel<<<1, 256, 0, s>>>(m.get(), N, k, pinv.get(), status.get());
+        sweep_panel_kernel<<<T, 256, 0, s>>>(m.get(), N, k, pinv.get(), cbuf.get(), rbuf.get());
+        sweep_update_kernel<<<dim3(T, T), 256, 0, s>>>(m.get(), N, k, cbuf.get(), rbuf.get());
+        sweep_finish_kernel<<<T, 256, 0, s>>>(m.get(), N, k, pinv.get(), cbuf.get());
+        count_launch(4);
+    }
     CUNIBS_LAUNCH_CHECK("dense inverse");
+    if (read_scalar(status.get(), s)) fail(kEInternal, std::string(what) + " is not positive definite");
+    const int ld = dense_ld(n);
+    inv.resize(static_cast<std::size_t>(n) * ld);
+    inv32.resize(static_cast<std::size_t>(n) * ld);
+    sweep_extract_kernel<<<grid_for(static_cast<std::int64_t>(n) * ld), kBlock, 0, s>>>(m.get(), N, n, ld, inv.get(),
+                                                                                      inv32.get());
+    count_launch();
+    CUNIBS_LAUNCH_CHECK("dense inverse extract");
     CUNIBS_CHECK(cudaStreamSynchronize(s));
 }
 

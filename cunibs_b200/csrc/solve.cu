@@ -22,6 +22,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <tuple>
 #include <type_traits>
@@ -626,13 +627,13 @@ void dispatch_tpr(int tpr, F&& f) {
 // A solve-loop kernel launch, with programmatic stream serialization when `dep` is set (the
 // kernel then starts with pdl_enter()); a plain launch otherwise.
 template <typename... KArgs, typename... Args>
-void launch_loop(bool dep, void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, Args... args) {
+void launch_loop(bool dep, void (*kernel)(KArgs...), dim3 grid, unsigned block, cudaStream_t s, Args... args) {
     if (!dep) {
         kernel<<<grid, block, 0, s>>>(args...);
         return;
     }
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
+    cfg.gridDim = grid;
     cfg.blockDim = dim3(block);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
@@ -649,43 +650,158 @@ unsigned group_grid(int n) {
     return static_cast<unsigned>((n + Group<K, TPR>::kRows - 1) / Group<K, TPR>::kRows);
 }
 
-// x = Ainv b for the dense coarsest operator: a warp per row, lanes striding the row, a fixed
-// shuffle tree per column.
-// x = inv b for the dense bottom of the V-cycle: one block of kGemvThreads per row, each thread a
-// strided share of the row, warp sums then a fixed-order sum over the warps (deterministic, and
-// independent of K per column).
-constexpr int kGemvThreads = 128;
+// x = inv b for the dense bottom of the V-cycle (n rows of ld entries, zero past column n). inv is
+// symmetric, so x_i = sum_j inv[j][i] b_j: a lane owns V consecutive outputs i and walks rows j of
+// inv, every warp load 512 contiguous bytes of one row, with no reduction across lanes. Pass 1: the
+// grid is about one block per SM (DenseGrid): block (I, S) owns the outputs of column block I and
+// the rows j of split S, and streams them once. Each thread copies its own 16 bytes of each row
+// into a private ring of shared-memory slots with asynchronous copies (cp.async, kDenseRing stages
+// of kDenseRows rows ahead), so the bytes in flight do not take registers, and a thread only ever
+// waits for its own copies (cp.async.wait_group: no barrier, no spinning). b's rows of the split are
+// staged once in shared memory and read as broadcasts. Pass 2 adds the splits' partials in order.
+// Every (output, column of b) sum runs over the same terms in the same order whatever K is (the
+// grid depends on n, the type and the GPU only), so a column's result does not depend on the block
+// width.
+constexpr int kDenseMaxThreads = 512;
+constexpr int kDenseRows = 8;
+constexpr std::size_t kDenseSmemBudget = 220 * 1024;
+
+template <typename T>
+struct DenseGrid {
+    static constexpr int V = 16 / static_cast<int>(sizeof(T));  // outputs per lane (one 16-byte load)
+    static constexpr int kRing = sizeof(T) == 8 ? 2 : 3;         // stages in flight
+    int col_blocks = 1, cols = 0, threads = 0, splits = 1, split_rows = 0;
+    std::size_t ring_bytes = 0, b_bytes = 0;
+    DenseGrid(int n, int K, int sm_count) {
+        const int ld = dense_ld(n);
+        col_blocks = (ld + kDenseMaxThreads * V - 1) / (kDenseMaxThreads * V);
+        const int span = kWarp * V;
+        cols = ((ld + col_blocks - 1) / col_blocks + span - 1) / span * span;
+        threads = cols / V;
+        ring_bytes = static_cast<std::size_t>(kRing) * kDenseRows * threads * 16;
+        splits = std::max(1, std::min(sm_count / col_blocks, (n + 15) / 16));
+        // b's rows of a split share the block's shared memory with the ring; the splits are sized
+        // for the widest block (16 columns) so that they never depend on K.
+        const std::size_t widest = 16 * sizeof(T);
+        const std::size_t room = kDenseSmemBudget - ring_bytes;
+        splits = std::max<int>(splits, static_cast<int>((static_cast<std::size_t>(n) * widest + room - 1) / room));
+        split_rows = (n + splits - 1) / splits;
+        b_bytes = static_cast<std::size_t>(split_rows) * K * sizeof(T);
+    }
+    std::size_t smem() const { return ring_bytes + b_bytes; }
+};
+
+// The inverse streams past L2 marked evict-first, so that it does not push the finest level's
+// operator and vectors (which stay L2-resident from one PCG iteration to the next) out of L2.
+__device__ __forceinline__ std::uint64_t evict_first_policy() {
+    std::uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid, std::uint64_t policy) {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;" ::"r"(dst), "l"(gmem),
+                 "r"(valid ? 16 : 0), "l"(policy)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ void load16(const T* p, T* o);
+template <>
+__device__ __forceinline__ void load16<float>(const float* p, float* o) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+    o[2] = v.z;
+    o[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void load16<double>(const double* p, double* o) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    o[0] = v.x;
+    o[1] = v.y;
+}
 
 template <typename T, int K>
-__global__ void __launch_bounds__(kGemvThreads) coarse_gemv_kernel(int nc, const T* __restrict__ inv,
-                                                                  const T* __restrict__ b, T* __restrict__ x) {
+__global__ void __launch_bounds__(kDenseMaxThreads) dense_part_kernel(int n, int ld, int cols, int split_rows,
+                                                                      const T* __restrict__ inv,
+                                                                      const T* __restrict__ b,
+                                                                      T* __restrict__ part) {
     pdl_enter();
-    __shared__ T part[kGemvThreads / kWarp][K];
-    const int row = blockIdx.x;
-    T acc[K];
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = T(0);
-    const T* r = inv + static_cast<long>(row) * nc;
-#pragma unroll 4
-    for (int j = threadIdx.x; j < nc; j += kGemvThreads) {
-        const T a = r[j];
-#pragma unroll
-        for (int c = 0; c < K; ++c) acc[c] += a * b[static_cast<long>(j) * K + c];
-    }
-#pragma unroll
-    for (int c = 0; c < K; ++c) acc[c] = group_sum<kWarp>(acc[c]);
-    const int warp = threadIdx.x / kWarp;
-    if (threadIdx.x % kWarp == 0) {
-#pragma unroll
-        for (int c = 0; c < K; ++c) part[warp][c] = acc[c];
-    }
+    constexpr int V = DenseGrid<T>::V, R = DenseGrid<T>::kRing, U = kDenseRows;
+    extern __shared__ __align__(16) unsigned char dense_smem[];
+    // Ring slot (stage, row t) of thread x: 16 bytes at ((stage * U + t) * blockDim.x + x) * 16.
+    uint4* ring = reinterpret_cast<uint4*>(dense_smem);
+    T* bs = reinterpret_cast<T*>(dense_smem + static_cast<std::size_t>(R) * U * blockDim.x * 16);
+    const int j0 = blockIdx.y * split_rows;
+    const int j1 = min(n, j0 + split_rows);
+    for (int q = threadIdx.x; q < (j1 - j0) * K; q += blockDim.x) bs[q] = b[static_cast<long>(j0) * K + q];
     __syncthreads();
-    if (threadIdx.x < K) {
-        T v = part[0][threadIdx.x];
+    const int i0 = blockIdx.x * cols + threadIdx.x * V;
+    if (i0 >= ld) return;
+    const T* col = inv + i0;
+    const std::uint64_t policy = evict_first_policy();
+    const int stages = (j1 - j0 + U - 1) / U;
+    // Stage st holds rows j0 + st U + t (t < U); rows past j1 are zero-filled without a read.
+    auto issue = [&](int st) {
+        if (st < stages) {
 #pragma unroll
-        for (int w = 1; w < kGemvThreads / kWarp; ++w) v += part[w][threadIdx.x];
-        x[static_cast<long>(row) * K + threadIdx.x] = v;
+            for (int t = 0; t < U; ++t) {
+                const int j = j0 + st * U + t;
+                cp_async16(&ring[((st % R) * U + t) * blockDim.x + threadIdx.x],
+                           col + static_cast<long>(j < j1 ? j : j0) * ld, j < j1, policy);
+            }
+        }
+        cp_async_commit();  // an empty group past the last stage keeps the group count uniform
+    };
+#pragma unroll
+    for (int st = 0; st < R; ++st) issue(st);
+    T acc[V][K];
+#pragma unroll
+    for (int u = 0; u < V; ++u)
+#pragma unroll
+        for (int c = 0; c < K; ++c) acc[u][c] = T(0);
+    for (int st = 0; st < stages; ++st) {
+        cp_async_wait<R - 1>();  // this thread's copies of stage st have landed
+        const int rows = min(U, j1 - j0 - st * U);
+#pragma unroll
+        for (int t = 0; t < U; ++t) {
+            if (t < rows) {
+                T a[V];
+                load16<T>(reinterpret_cast<const T*>(&ring[((st % R) * U + t) * blockDim.x + threadIdx.x]), a);
+                const T* bj = bs + (st * U + t) * K;
+#pragma unroll
+                for (int c = 0; c < K; ++c)
+#pragma unroll
+                    for (int u = 0; u < V; ++u) acc[u][c] = fma(a[u], bj[c], acc[u][c]);
+            }
+        }
+        issue(st + R);  // into the slots just read (this thread's own)
     }
+    cp_async_wait<0>();
+    T* out = part + (static_cast<long>(blockIdx.y) * n + i0) * K;
+#pragma unroll
+    for (int u = 0; u < V; ++u)
+        if (i0 + u < n)
+#pragma unroll
+            for (int c = 0; c < K; ++c) out[u * K + c] = acc[u][c];
+}
+
+template <typename T, int K>
+__global__ void __launch_bounds__(kBlock) dense_sum_kernel(int n, int blocks, const T* __restrict__ part,
+                                                          T* __restrict__ x) {
+    pdl_enter();
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const long nk = static_cast<long>(n) * K;
+    if (q >= nk) return;
+    T v = part[q];
+    for (int J = 1; J < blocks; ++J) v += part[J * nk + q];
+    x[q] = v;
 }
 
 // --- PCG kernels -------------------------------------------------------------------------
@@ -1041,6 +1157,7 @@ template <typename T>
 struct VWork {
     std::vector<DevArray<T>> x, r, b;
     DevArray<T> cb, cx;
+    DevArray<T> part;  // the dense bottom's per-column-block partial sums
 };
 
 class Solver {
@@ -1048,12 +1165,15 @@ class Solver {
     const Hierarchy* h = nullptr;
     int n = 0;
     int kcap = 0;
-    // Solve-loop kernels launched with programmatic stream serialization (pdl_enter); off with
-    // CUNIBS_PROGRAMMATIC_LAUNCH=0.
-    bool pdl = true;
+    // Solve-loop kernels launched with programmatic stream serialization (pdl_enter): off by default,
+    // on with CUNIBS_PROGRAMMATIC_LAUNCH=1. With the V-cycle's bottom at level 1 the loop is mostly
+    // multi-wave finest-level kernels, whose early-resident successors take their later waves'
+    // slots: split solve 3.38 ms per block of 8 with it, 3.26 ms without.
+    bool pdl = false;
     // Columns per lane of the one-lane-per-row operators (the *_cols kernels; bitwise the same
     // results): 2 by default, CUNIBS_LANE_COLUMNS=1 or 4 to choose.
     int lane_cols = 2;
+    int sm_count = 148;
     cudaStream_t stream = nullptr;
     // FP64 CG / outer workspace (n, kcap)
     DevArray<double> B, X, R, P, AP, Z;
@@ -1114,6 +1234,8 @@ class Solver {
         v32.cx.resize(mc);
         v64.cb.resize(mc);
         v64.cx.resize(mc);
+        v32.part.resize(mc * DenseGrid<float>(h->bottom_n, K, sm_count).splits);
+        v64.part.resize(mc * DenseGrid<double>(h->bottom_n, K, sm_count).splits);
         for (auto* a : {&rz, &alpha, &beta, &ref_sq, &rr0, &rel, &eta, &r0sq, &init_rel, &tolv}) a->resize(K);
         for (auto* a : {&frozen, &outer_conv, &conv_iter}) a->resize(K);
         iter_counter.resize(1);
@@ -1148,6 +1270,9 @@ class Solver {
     // per row); returns whether it did.
     template <typename T, int K>
     bool vcycle(const T* b, T* z, bool jz_done = false, bool dot = false);
+    // x = inv b at the V-cycle's bottom (bottom_n rows, K columns).
+    template <typename T, int K>
+    void dense_bottom(const T* b, T* x);
     template <typename T>
     T* first0() {
         VWork<T>& w = vw<T>();
@@ -1316,17 +1441,44 @@ template <>
 VWork<double>& Solver::vw<double>() { return v64; }
 
 template <typename T, int K>
+void Solver::dense_bottom(const T* b, T* x) {
+    const int nb = h->bottom_n;
+    const DenseGrid<T> g(nb, K, sm_count);
+    const std::size_t smem = g.smem();
+    if (smem > 48 * 1024) {
+        static std::once_flag opt_in;
+        std::call_once(opt_in, [] {
+            CUNIBS_CHECK(cudaFuncSetAttribute(dense_part_kernel<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              static_cast<int>(kDenseSmemBudget)));
+        });
+        if (smem > kDenseSmemBudget) fail(kEInternal, "dense bottom split too large for shared memory");
+    }
+    T* part = vw<T>().part.get();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(static_cast<unsigned>(g.col_blocks), static_cast<unsigned>(g.splits));
+    cfg.blockDim = dim3(static_cast<unsigned>(g.threads));
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    // Launched without programmatic serialization: its blocks (one per SM, most of the SM's shared
+    // memory) would otherwise be made resident early and wait beside the restriction that feeds it.
+    cfg.numAttrs = 0;
+    CUNIBS_CHECK(cudaLaunchKernelEx(&cfg, dense_part_kernel<T, K>, nb, dense_ld(nb), g.cols, g.split_rows, cinv<T>(), b,
+                                    part));
+    launch_loop(pdl, dense_sum_kernel<T, K>, grid_for(static_cast<std::int64_t>(nb) * K), kBlock, stream, nb, g.splits,
+                static_cast<const T*>(part), x);
+    count_launch(2);
+}
+
+template <typename T, int K>
 bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
     const Hierarchy& H = *h;
     const Cheby& ch = H.cheby;
     const int L = H.vcycle_levels;
-    const int n_bottom = H.bottom_n;
     VWork<T>& w = vw<T>();
     constexpr int TT = tile_threads<K>();
     cudaStream_t s = stream;
     if (L == 0) {
-        launch_loop(pdl, coarse_gemv_kernel<T, K>, n_bottom, kGemvThreads, s, n_bottom, cinv<T>(), b, z);
-        count_launch();
+        dense_bottom<T, K>(b, z);
         return false;
     }
     const bool fuse_dot = dot && H.levels[0].tpr_a <= 16;
@@ -1466,8 +1618,7 @@ bool Solver::vcycle(const T* b, T* z, bool jz_done, bool dot) {
         });
         count_launch();
     }
-    launch_loop(pdl, coarse_gemv_kernel<T, K>, n_bottom, kGemvThreads, s, n_bottom, cinv<T>(), w.cb.get(), w.cx.get());
-    count_launch();
+    dense_bottom<T, K>(w.cb.get(), w.cx.get());
     // Up-sweep.
     const T* xc = w.cx.get();
     for (int l = L - 1; l >= 0; --l) {
@@ -1724,9 +1875,12 @@ SolverPtr make_solver(const Hierarchy& h, const Params& p) {
     const char* host_loop = std::getenv("CUNIBS_SOLVER_HOST_LOOP");
     sv->while_unsupported = host_loop != nullptr && host_loop[0] == '1';
     const char* pdl = std::getenv("CUNIBS_PROGRAMMATIC_LAUNCH");
-    sv->pdl = !(pdl != nullptr && pdl[0] == '0');
+    sv->pdl = pdl != nullptr && pdl[0] == '1';
     const char* lanes = std::getenv("CUNIBS_LANE_COLUMNS");
     if (lanes != nullptr && (lanes[0] == '1' || lanes[0] == '2' || lanes[0] == '4')) sv->lane_cols = lanes[0] - '0';
+    int dev = 0;
+    CUNIBS_CHECK(cudaGetDevice(&dev));
+    CUNIBS_CHECK(cudaDeviceGetAttribute(&sv->sm_count, cudaDevAttrMultiProcessorCount, dev));
     // The solver's kernels go at the highest stream priority: block preparation may run beside them.
     int least = 0, greatest = 0;
     CUNIBS_CHECK(cudaDeviceGetStreamPriorityRange(&least, &greatest));

@@ -74,7 +74,8 @@ typedef struct {
     int inner_max_iters;      /* mixed: iteration cap of each inner FP32 solve */
     int iters_per_sync;       /* PCG iterations launched between host convergence checks */
     int dense_max_rows;       /* the V-cycle ends in an exact dense solve at the first level below the
-                                 finest with at most this many rows (default 1024); 0: at the coarsest
+                                 finest with at most this many rows (default 12288, at most 16384;
+                                 its dense inverse takes 12 bytes per entry); 0: at the coarsest
                                  level, as the reference's V-cycle does (vcycle.cu:420-663) */
 } cunibs_params;
 
