@@ -1455,6 +1455,11 @@ int cunibs_context_array(const cunibs_context* c, const char* name, int level, v
             pick(h.coarse_inv.get(), static_cast<std::size_t>(h.nc) * h.nc, 8);
             pitch = static_cast<std::size_t>(dense_ld(h.nc)) * 8;
             row_bytes = static_cast<std::size_t>(h.nc) * 8;
+        } else if (n == "bottom_inv") {  // the dense inverse the V-cycle ends in (bottom_rows square)
+            const bool early = h.vcycle_levels < static_cast<int>(h.levels.size());
+            pick(early ? h.level_inv.get() : h.coarse_inv.get(), static_cast<std::size_t>(h.bottom_n) * h.bottom_n, 8);
+            pitch = static_cast<std::size_t>(dense_ld(h.bottom_n)) * 8;
+            row_bytes = static_cast<std::size_t>(h.bottom_n) * 8;
         }
         else if (lv_ok && n == "a_ptr") pick(h.levels[level].a.ptr.get(), h.levels[level].n + 1, 4);
         else if (lv_ok && n == "a_col") pick(h.levels[level].a.col.get(), h.levels[level].a.nnz, 4);

@@ -727,6 +727,50 @@ __device__ __forceinline__ void load16<double>(const double* p, double* o) {
     o[1] = v.y;
 }
 
+// A lane's V outputs += a (its V entries of one row of inv) * b_j, for each of b's K columns. FP32 pairs
+// the outputs for packed FMAs (FFMA2, each lane an fmaf rounded once: the same sums as scalar).
+template <typename T, int K>
+struct DenseAcc {
+    static constexpr int V = DenseGrid<T>::V;
+    T v[V][K];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int u = 0; u < V; ++u)
+#pragma unroll
+            for (int c = 0; c < K; ++c) v[u][c] = T(0);
+    }
+    __device__ __forceinline__ void add(const T* a, const T* bj) {
+#pragma unroll
+        for (int c = 0; c < K; ++c)
+#pragma unroll
+            for (int u = 0; u < V; ++u) v[u][c] = fma(a[u], bj[c], v[u][c]);
+    }
+    __device__ __forceinline__ T get(int u, int c) const { return v[u][c]; }
+};
+template <int K>
+struct DenseAcc<float, K> {
+    float2 v[2][K];  // outputs (0, 1) and (2, 3)
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int c = 0; c < K; ++c) v[h][c] = make_float2(0.0f, 0.0f);
+    }
+    __device__ __forceinline__ void add(const float* a, const float* bj) {
+        const float2 a01 = make_float2(a[0], a[1]), a23 = make_float2(a[2], a[3]);
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+            const float2 bb = make_float2(bj[c], bj[c]);
+            v[0][c] = __ffma2_rn(a01, bb, v[0][c]);
+            v[1][c] = __ffma2_rn(a23, bb, v[1][c]);
+        }
+    }
+    __device__ __forceinline__ float get(int u, int c) const {
+        const float2 p = v[u >> 1][c];
+        return (u & 1) ? p.y : p.x;
+    }
+};
+
 template <typename T, int K>
 __global__ void __launch_bounds__(kDenseMaxThreads) dense_part_kernel(int n, int ld, int cols, int split_rows,
                                                                       const T* __restrict__ inv,
@@ -744,41 +788,37 @@ __global__ void __launch_bounds__(kDenseMaxThreads) dense_part_kernel(int n, int
     __syncthreads();
     const int i0 = blockIdx.x * cols + threadIdx.x * V;
     if (i0 >= ld) return;
-    const T* col = inv + i0;
+    const T* src = inv + static_cast<long>(j0) * ld + i0;  // this thread's 16 bytes of row j0
+    uint4* mine = ring + threadIdx.x;
+    const int stride = blockDim.x;  // slots from one row of a stage to the next
     const std::uint64_t policy = evict_first_policy();
     const int stages = (j1 - j0 + U - 1) / U;
     // Stage st holds rows j0 + st U + t (t < U); rows past j1 are zero-filled without a read.
     auto issue = [&](int st) {
         if (st < stages) {
+            const T* s = src + static_cast<long>(st) * U * ld;
+            uint4* d = mine + (st % R) * U * stride;
+            const int left = j1 - j0 - st * U;
 #pragma unroll
-            for (int t = 0; t < U; ++t) {
-                const int j = j0 + st * U + t;
-                cp_async16(&ring[((st % R) * U + t) * blockDim.x + threadIdx.x],
-                           col + static_cast<long>(j < j1 ? j : j0) * ld, j < j1, policy);
-            }
+            for (int t = 0; t < U; ++t) cp_async16(d + t * stride, t < left ? s + static_cast<long>(t) * ld : src, t < left, policy);
         }
         cp_async_commit();  // an empty group past the last stage keeps the group count uniform
     };
 #pragma unroll
     for (int st = 0; st < R; ++st) issue(st);
-    T acc[V][K];
-#pragma unroll
-    for (int u = 0; u < V; ++u)
-#pragma unroll
-        for (int c = 0; c < K; ++c) acc[u][c] = T(0);
+    DenseAcc<T, K> acc;
+    acc.zero();
     for (int st = 0; st < stages; ++st) {
         cp_async_wait<R - 1>();  // this thread's copies of stage st have landed
         const int rows = min(U, j1 - j0 - st * U);
+        const uint4* d = mine + (st % R) * U * stride;
+        const T* bj = bs + st * U * K;
 #pragma unroll
         for (int t = 0; t < U; ++t) {
             if (t < rows) {
                 T a[V];
-                load16<T>(reinterpret_cast<const T*>(&ring[((st % R) * U + t) * blockDim.x + threadIdx.x]), a);
-                const T* bj = bs + (st * U + t) * K;
-#pragma unroll
-                for (int c = 0; c < K; ++c)
-#pragma unroll
-                    for (int u = 0; u < V; ++u) acc[u][c] = fma(a[u], bj[c], acc[u][c]);
+                load16<T>(reinterpret_cast<const T*>(d + t * stride), a);
+                acc.add(a, bj + t * K);
             }
         }
         issue(st + R);  // into the slots just read (this thread's own)
@@ -789,7 +829,7 @@ __global__ void __launch_bounds__(kDenseMaxThreads) dense_part_kernel(int n, int
     for (int u = 0; u < V; ++u)
         if (i0 + u < n)
 #pragma unroll
-            for (int c = 0; c < K; ++c) out[u * K + c] = acc[u][c];
+            for (int c = 0; c < K; ++c) out[u * K + c] = acc.get(u, c);
 }
 
 template <typename T, int K>

@@ -324,6 +324,7 @@ int cunibs_adm_evaluate_exact(cunibs_adm* adm, const double* dip_pos_m, const do
  *            "stiff_ptr" "stiff_col" "gm_index" and per level "a_ptr" "a_col" "agg" "p_ptr" "p_col"
  *            "coarse_ptr" "coarse_col"
  *   float64: "nodes_mm" "g" "vols" "bary" "stiff_val" "skin_normals" "coarse_val" "coarse_inv"
+ *            "bottom_inv" (the dense inverse the V-cycle ends in, bottom_rows square)
  *            and per level "a_val" "p_val" "dinv"
  * *len receives the element count; at most cap elements are written. */
 int cunibs_context_array(const cunibs_context* ctx, const char* name, int level, void* out, long long cap,

@@ -101,11 +101,11 @@ def test_vcycle_matches_oracle(sphere_ref_cycle, sphere_pair, fp32, tol):
 
 
 def test_dense_bottom_vcycle_is_a_symmetric_preconditioner(sphere_pair, sphere_ref_cycle):
-    """The default V-cycle stops at the first level below the finest with at most 1024 rows and
+    """The default V-cycle stops at the first level below the finest with at most 12,288 rows and
     solves it exactly: the preconditioner stays symmetric positive definite (FP64), and PCG with it
     needs no more iterations than with the full descent."""
     ctx = sphere_pair[0]
-    assert 1 <= ctx.vcycle_levels < ctx.n_levels and ctx.bottom_rows <= 1024
+    assert 1 <= ctx.vcycle_levels < ctx.n_levels and ctx.bottom_rows <= 12288
     rng = np.random.default_rng(3)
     r = rng.standard_normal((ctx.n_nodes - 1, 2))
     z = ctx.vcycle(r)
