@@ -1172,6 +1172,7 @@ struct cunibs_adm {
     AdmGrid grid{};
     DevArray<float> Q;               // (n_dir, n_grid, 3)
     DevArray<double> pos, mom, T, E; // evaluation workspace
+    DevArray<float> q_part;          // the reciprocity field's per-chunk partials
     DevArray<unsigned long long> bad;
 };
 
@@ -1334,7 +1335,7 @@ int cunibs_adm_sample(cunibs_adm* a, const double* origin_mm, const double* spac
         // Q_d on the grid: the coil-field N-body with the mesh nodes as sources (reciprocity.py:183-213),
         // every direction in one pass over the sources.
         dadt_nodes_shared(pts.get(), static_cast<int>(n_grid), reinterpret_cast<const float*>(packed.get()),
-                          a->ctx->mesh.n_nodes, Td.get(), a->dirs.n, 1.0, a->Q.get(), s);
+                          a->ctx->mesh.n_nodes, Td.get(), a->dirs.n, 1.0, a->Q.get(), s, a->q_part);
         CUNIBS_LAUNCH_CHECK("reciprocity field");
         CUNIBS_CHECK(cudaStreamSynchronize(s));
         a->grid = gr;

@@ -146,18 +146,25 @@ struct __align__(16) SharedSource {
 
 // The field of ND source sets at common positions (records d * n_dip + j of prep_dipoles, all
 // prepared with the one transform T): per (target, source) pair the difference and 1/|d|^3 are
-// formed once and used for every set. Per set the arithmetic and the order over sources are
-// dadt_kernel's, so set d's field is bitwise what dadt_kernel gives for it as one placement.
-// Work items are node tiles only; node order within a tile as dadt_kernel's.
+// formed once and used for every set, with dadt_kernel's per-set arithmetic. Work items are
+// (node tile, source chunk) pairs, item = chunk * n_tiles + tile, so that few targets (a grid of a
+// few hundred thousand points) still fill the GPU: with one chunk a thread sums every source in
+// order and writes the scaled field (dadt_kernel's order, bitwise its result for one set); with
+// several it writes the chunk's unscaled partial to part[chunk][set][node][3], and
+// shared_sum_kernel adds the chunks in order. The chunks depend on the sizes only, never on ND.
+// Node order within a tile as dadt_kernel's.
 template <int ND>
 __global__ void __launch_bounds__(kDadtThreads) dadt_shared_kernel(const double* __restrict__ nodes_mm, int n_nodes,
                                                                    const DipolePacked* __restrict__ dip, int n_dip,
                                                                    const double* __restrict__ T, float scale,
-                                                                   float* __restrict__ out, int n_tiles) {
+                                                                   float* __restrict__ out, int n_tiles, int chunk,
+                                                                   int n_items, float* __restrict__ part) {
     __shared__ SharedSource<ND> tile[kDipTile];
     const double ox = T[3] * 1e-3, oy = T[7] * 1e-3, oz = T[11] * 1e-3;
     const int stride = n_tiles * blockDim.x;
-    for (int item = blockIdx.x; item < n_tiles; item += gridDim.x) {
+    for (int work = blockIdx.x; work < n_items; work += gridDim.x) {
+    const int item = work % n_tiles, ch = work / n_tiles;
+    const int j_begin = ch * chunk, j_end = min(n_dip, j_begin + chunk);
     const int base = item * blockDim.x + threadIdx.x;
     int node[4];
     float rxs[4], rys[4], rzs[4];
@@ -177,8 +184,8 @@ __global__ void __launch_bounds__(kDadtThreads) dadt_shared_kernel(const double*
     for (int d = 0; d < ND; ++d)
 #pragma unroll
         for (int q = 0; q < 2; ++q) ax[d][q] = ay[d][q] = az[d][q] = make_float2(0.f, 0.f);
-    for (int t0 = 0; t0 < n_dip; t0 += kDipTile) {
-        const int nt = min(kDipTile, n_dip - t0);
+    for (int t0 = j_begin; t0 < j_end; t0 += kDipTile) {
+        const int nt = min(kDipTile, j_end - t0);
         __syncthreads();
         for (int j = threadIdx.x; j < nt; j += blockDim.x) {
             const DipolePacked p0 = dip[t0 + j];
@@ -226,17 +233,28 @@ __global__ void __launch_bounds__(kDadtThreads) dadt_shared_kernel(const double*
         const float vx[4] = {ax[d][0].x, ax[d][0].y, ax[d][1].x, ax[d][1].y};
         const float vy[4] = {ay[d][0].x, ay[d][0].y, ay[d][1].x, ay[d][1].y};
         const float vz[4] = {az[d][0].x, az[d][0].y, az[d][1].x, az[d][1].y};
-        float* o = out + static_cast<long>(d) * n_nodes * 3;
+        float* o = part ? part + (static_cast<long>(ch) * ND + d) * n_nodes * 3 : out + static_cast<long>(d) * n_nodes * 3;
+        const float sc = part ? 1.0f : scale;
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             if (node[u] < n_nodes) {
-                o[3 * static_cast<long>(node[u])] = scale * vx[u];
-                o[3 * static_cast<long>(node[u]) + 1] = scale * vy[u];
-                o[3 * static_cast<long>(node[u]) + 2] = scale * vz[u];
+                o[3 * static_cast<long>(node[u])] = sc * vx[u];
+                o[3 * static_cast<long>(node[u]) + 1] = sc * vy[u];
+                o[3 * static_cast<long>(node[u]) + 2] = sc * vz[u];
             }
         }
     }
     }
+}
+
+// out = scale * (the chunks' partials added in chunk order).
+__global__ void shared_sum_kernel(long count, int chunks, const float* __restrict__ part, float scale,
+                                  float* __restrict__ out) {
+    const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (q >= count) return;
+    float v = part[q];
+    for (int c = 1; c < chunks; ++c) v += part[c * count + q];
+    out[q] = scale * v;
 }
 
 // dadt_elm[p][e] = 1/4 sum of the four nodal values (dadt_element.cu:6-31).
@@ -379,17 +397,37 @@ void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed
 }
 
 void dadt_nodes_shared(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
-                       const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s) {
+                       const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s,
+                       DevArray<float>& scratch) {
     const DadtGrid g = dadt_grid(n_nodes, 1, 0);
     const float scale = static_cast<float>(didt * 1e-7);
     const auto* dp = reinterpret_cast<const DipolePacked*>(dip_packed);
+    if (n_sets < 1 || n_sets > 3) fail(kEInval, "between 1 and 3 source sets");
+    // Source chunks: about two waves of resident blocks when the targets alone leave the GPU short
+    // of them (kDipTile-multiples of sources, at least one tile each); one chunk otherwise.
+    int dev = 0, sms = 0;
+    CUNIBS_CHECK(cudaGetDevice(&dev));
+    CUNIBS_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int resident = sms * (2048 / kDadtThreads);
+    int chunks = 1;
+    if (g.n_tiles < resident) chunks = std::min((2 * resident + g.n_tiles - 1) / g.n_tiles, (n_dip + kDipTile - 1) / kDipTile);
+    chunks = std::max(chunks, 1);
+    const int chunk = ((n_dip + chunks - 1) / chunks + kDipTile - 1) / kDipTile * kDipTile;
+    chunks = (n_dip + chunk - 1) / chunk;
+    const int n_items = g.n_tiles * chunks;
+    if (chunks > 1) scratch.reserve(static_cast<std::size_t>(chunks) * n_sets * n_nodes * 3);
+    float* pp = chunks > 1 ? scratch.get() : nullptr;
     switch (n_sets) {
-        case 1: dadt_shared_kernel<1><<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles); break;
-        case 2: dadt_shared_kernel<2><<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles); break;
-        case 3: dadt_shared_kernel<3><<<g.blocks, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles); break;
-        default: fail(kEInval, "between 1 and 3 source sets");
+        case 1: dadt_shared_kernel<1><<<n_items, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles, chunk, n_items, pp); break;
+        case 2: dadt_shared_kernel<2><<<n_items, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles, chunk, n_items, pp); break;
+        default: dadt_shared_kernel<3><<<n_items, kDadtThreads, 0, s>>>(nodes_mm, n_nodes, dp, n_dip, transform_dev, scale, out, g.n_tiles, chunk, n_items, pp); break;
     }
     count_launch();
+    if (chunks > 1) {
+        const long count = static_cast<long>(n_sets) * n_nodes * 3;
+        shared_sum_kernel<<<grid_for(count), kBlock, 0, s>>>(count, chunks, pp, scale, out);
+        count_launch();
+    }
 }
 
 void dadt_elements(const Mesh& m, const float* nodal, int k, float* elm, cudaStream_t s) {

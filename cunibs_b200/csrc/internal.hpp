@@ -211,8 +211,11 @@ void dadt_nodes_raw(const double* nodes_mm, int n_nodes, const float* dip_packed
 // n_sets (1..3) source sets at common positions, records set * n_dip + j of prep_dipoles all made
 // with the one transform transform_dev; out (n_sets, n_nodes, 3). Set d's field is bitwise
 // dadt_nodes_raw's for that set alone; each pair's geometry is formed once for all sets.
+// scratch holds the source chunks' partial fields when the targets alone do not fill the GPU (grown
+// on demand and kept by the caller, so repeated calls allocate nothing).
 void dadt_nodes_shared(const double* nodes_mm, int n_nodes, const float* dip_packed, int n_dip,
-                       const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s);
+                       const double* transform_dev, int n_sets, double didt, float* out, cudaStream_t s,
+                       DevArray<float>& scratch);
 // The two direct sums on raw node coordinates with an explicit FP32 scale (1: the bare dipole sum).
 void dadt_zcoil_raw(const double* nodes_mm, int n_nodes, const void* zpacked, int n_dip, const double* transforms_dev,
                     int k, float scale, float* out, cudaStream_t s, int max_blocks = 0);
