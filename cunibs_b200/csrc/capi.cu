@@ -1172,7 +1172,12 @@ struct cunibs_adm {
     AdmGrid grid{};
     DevArray<float> Q;               // (n_dir, n_grid, 3)
     DevArray<double> pos, mom, T, E; // evaluation workspace
-    DevArray<float> q_part;          // the reciprocity field's per-chunk partials
+    // Sampling workspace, grown on demand and kept, so that a repeated sampling allocates nothing:
+    // the grid points, the sources' centred positions, their packed records and frames, and the
+    // per-chunk partial fields.
+    DevArray<double> q_pts, q_src, q_T;
+    DevArray<unsigned char> q_packed;
+    DevArray<float> q_part;
     DevArray<unsigned long long> bad;
 };
 
@@ -1184,7 +1189,8 @@ void adm_sources(cunibs_adm* a, const double* center_mm, DevArray<unsigned char>
                  cudaStream_t s) {
     const Mesh& m = a->ctx->mesh;
     const int nd = a->dirs.n;
-    DevArray<double> src(3 * static_cast<std::size_t>(m.n_nodes));
+    DevArray<double>& src = a->q_src;
+    src.reserve(3 * static_cast<std::size_t>(m.n_nodes));
     adm_centred_nodes(m, center_mm, src.get(), s);
     std::vector<double> h(16 * static_cast<std::size_t>(nd), 0.0);
     for (int d = 0; d < nd; ++d) {
@@ -1194,13 +1200,14 @@ void adm_sources(cunibs_adm* a, const double* center_mm, DevArray<unsigned char>
         t[7] = center_mm[1];
         t[11] = center_mm[2];
     }
-    Td.upload(h.data(), h.size(), s);
+    Td.reserve(h.size());
+    CUNIBS_CHECK(cudaMemcpyAsync(Td.get(), h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, s));
     const std::size_t rec = packed_dipole_bytes();
-    packed.resize(rec * m.n_nodes * nd);
+    packed.reserve(rec * m.n_nodes * nd);
     for (int d = 0; d < nd; ++d)
         prep_dipoles(src.get(), a->W.get() + 3 * static_cast<std::size_t>(m.n_nodes) * d, m.n_nodes, Td.get() + 16 * d,
                      1, packed.get() + rec * m.n_nodes * d, s);
-    CUNIBS_CHECK(cudaStreamSynchronize(s));  // h and src leave scope
+    CUNIBS_CHECK(cudaStreamSynchronize(s));  // h leaves scope
 }
 
 void adm_inputs(cunibs_adm* a, const double* dip_pos_m, const double* dip_moment, int n_dip, const double* transforms,
@@ -1326,9 +1333,11 @@ int cunibs_adm_sample(cunibs_adm* a, const double* origin_mm, const double* spac
         cudaStream_t s = a->ctx->stream;
         double center[3];
         for (int x = 0; x < 3; ++x) center[x] = gr.origin_mm[x] + 0.5 * gr.spacing_mm[x] * (gr.shape[x] - 1);
-        DevArray<double> pts(3 * static_cast<std::size_t>(n_grid)), Td;
+        DevArray<double>& pts = a->q_pts;
+        DevArray<double>& Td = a->q_T;
+        DevArray<unsigned char>& packed = a->q_packed;
+        pts.reserve(3 * static_cast<std::size_t>(n_grid));
         adm_grid_points(gr, pts.get(), s);
-        DevArray<unsigned char> packed;
         adm_sources(a, center, packed, Td, s);
         a->sampled = false;
         a->Q.resize(3 * static_cast<std::size_t>(n_grid) * a->dirs.n);
