@@ -1994,16 +1994,20 @@ void solver_vcycle(Solver& sv, const double* r, double* z, int k, bool fp32, cud
         CUNIBS_CHECK(cudaStreamSynchronize(s));
         const std::size_t nk = static_cast<std::size_t>(sv.n) * KK;
         if (fp32) {
-            // r (FP64) -> FP32, cycle, back to FP64.
+            // r (FP64) -> FP32, cycle, back to FP64. Every copy goes on the solver's stream: a plain
+            // cudaMemcpy from pageable memory may return before its DMA has landed, and the solver's
+            // non-blocking stream would not wait for it.
             std::vector<double> hr(nk);
-            CUNIBS_CHECK(cudaMemcpy(hr.data(), r, nk * sizeof(double), cudaMemcpyDeviceToHost));
-            std::vector<float> hf(hr.begin(), hr.end());
-            CUNIBS_CHECK(cudaMemcpy(sv.r32.get(), hf.data(), nk * sizeof(float), cudaMemcpyHostToDevice));
-            sv.vcycle<float, KK>(sv.r32.get(), sv.z32.get());
+            CUNIBS_CHECK(cudaMemcpyAsync(hr.data(), r, nk * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
             CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
-            CUNIBS_CHECK(cudaMemcpy(hf.data(), sv.z32.get(), nk * sizeof(float), cudaMemcpyDeviceToHost));
+            std::vector<float> hf(hr.begin(), hr.end());
+            CUNIBS_CHECK(cudaMemcpyAsync(sv.r32.get(), hf.data(), nk * sizeof(float), cudaMemcpyHostToDevice, sv.stream));
+            sv.vcycle<float, KK>(sv.r32.get(), sv.z32.get());
+            CUNIBS_CHECK(cudaMemcpyAsync(hf.data(), sv.z32.get(), nk * sizeof(float), cudaMemcpyDeviceToHost, sv.stream));
+            CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
             std::vector<double> hz(hf.begin(), hf.end());
-            CUNIBS_CHECK(cudaMemcpy(z, hz.data(), nk * sizeof(double), cudaMemcpyHostToDevice));
+            CUNIBS_CHECK(cudaMemcpyAsync(z, hz.data(), nk * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+            CUNIBS_CHECK(cudaStreamSynchronize(sv.stream));
         } else {
             CUNIBS_CHECK(cudaMemcpyAsync(sv.R.get(), r, nk * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
             sv.vcycle<double, KK>(sv.R.get(), sv.Z.get());
