@@ -57,6 +57,12 @@ inline unsigned grid_for(std::int64_t n, int per_block = kBlock) {
     return static_cast<unsigned>((n + per_block - 1) / per_block);
 }
 
+// Device memory for DevArray (devmem.cu): freed blocks are cached per device and size and reused.
+// dev_alloc throws Error on failure; dev_free synchronises the block's device before the block can
+// be handed out again.
+void* dev_alloc(std::size_t bytes);
+void dev_free(void* p) noexcept;
+
 // Owning device allocation. Move-only; frees on destruction.
 template <typename T>
 class DevArray {
@@ -85,9 +91,7 @@ class DevArray {
         if (n == n_ && p_ != nullptr) return;
         release();
         if (n == 0) return;
-        void* p = nullptr;
-        check(cudaMalloc(&p, n * sizeof(T)), "cudaMalloc");
-        p_ = static_cast<T*>(p);
+        p_ = static_cast<T*>(dev_alloc(n * sizeof(T)));
         n_ = n;
     }
     // Grow-only resize: keeps the allocation when it is already large enough.
@@ -95,7 +99,7 @@ class DevArray {
         if (n > n_) resize(n);
     }
     void release() noexcept {
-        if (p_) cudaFree(p_);
+        if (p_) dev_free(p_);
         p_ = nullptr;
         n_ = 0;
     }
