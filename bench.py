@@ -419,17 +419,21 @@ def run_ours(args) -> dict:
     plain_table_ms, plain_table_value = job_throughput(plain_table_ms, n_cmp, world, dist, dev)
 
     # End to end through the host C ABI (host buffers in and out), blocks submitted two deep
-    # (cunibs_submit_block / cunibs_finish_block), timed by the wall clock around all of them.
+    # (cunibs_submit_block / cunibs_finish_block), timed by the wall clock around all of them. The
+    # wall clock also sees the host, so the run is repeated three times and the median kept.
     n_e2e = max(3, args.steps)
     kw = dict(recovery=args.recovery, warm_start=args.warm_start == "on")
-    torch.cuda.synchronize()
-    t1 = time.perf_counter()
-    tickets = [ctx.submit_block(coil, centers, handles, dists, 1e6, **kw)]
-    for _ in range(n_e2e - 1):
-        tickets.append(ctx.submit_block(coil, centers, handles, dists, 1e6, **kw))
+    e2e_runs = []
+    for _ in range(3):
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        tickets = [ctx.submit_block(coil, centers, handles, dists, 1e6, **kw)]
+        for _ in range(n_e2e - 1):
+            tickets.append(ctx.submit_block(coil, centers, handles, dists, 1e6, **kw))
+            res = ctx.finish_block(tickets.pop(0))
         res = ctx.finish_block(tickets.pop(0))
-    res = ctx.finish_block(tickets.pop(0))
-    e2e_s = time.perf_counter() - t1
+        e2e_runs.append(time.perf_counter() - t1)
+    e2e_s = float(np.median(e2e_runs))
     _, e2e_value = job_throughput(e2e_s * 1e3, n_e2e, world, dist, dev)
     h2d = coil.positions_m.nbytes + coil.moments.nbytes + centers.nbytes + handles.nbytes + dists.nbytes
     d2h = res["transform"].nbytes + res["summary"].nbytes + res["iterations"].nbytes + res["relative_residual"].nbytes
@@ -503,7 +507,8 @@ def run_ours(args) -> dict:
                                                     else "dipole sum at every node"),
                                      "parallelism": f"replicas x{world}"}),
         "e2e": {"value": round(e2e_value, 3), "unit": "placements/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
+                "d2h_bytes_per_step": int(d2h), "runs_s": [round(x, 5) for x in e2e_runs],
+                "what": f"median of 3 wall-clock runs of {n_e2e} blocks through the host C ABI"},
         "gpu_launches": int(launches),
         "vs_plain_fp64": {"value": round(plain_value, 3), "unit": "placements/s",
                           "iterations": plain_it, "ratio": round((plain_ms / n_cmp) / (total_ms / args.steps), 3),

@@ -698,10 +698,9 @@ __device__ __forceinline__ std::uint64_t evict_first_policy() {
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
     return p;
 }
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid, std::uint64_t policy) {
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, std::uint64_t policy) {
     const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2, %3;" ::"r"(dst), "l"(gmem),
-                 "r"(valid ? 16 : 0), "l"(policy)
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;" ::"r"(dst), "l"(gmem), "l"(policy)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -793,14 +792,15 @@ __global__ void __launch_bounds__(kDenseMaxThreads) dense_part_kernel(int n, int
     const int stride = blockDim.x;  // slots from one row of a stage to the next
     const std::uint64_t policy = evict_first_policy();
     const int stages = (j1 - j0 + U - 1) / U;
-    // Stage st holds rows j0 + st U + t (t < U); rows past j1 are zero-filled without a read.
+    // Stage st holds rows j0 + st U + t (t < U); slots of rows past j1 are neither filled nor read.
     auto issue = [&](int st) {
         if (st < stages) {
             const T* s = src + static_cast<long>(st) * U * ld;
             uint4* d = mine + (st % R) * U * stride;
             const int left = j1 - j0 - st * U;
 #pragma unroll
-            for (int t = 0; t < U; ++t) cp_async16(d + t * stride, t < left ? s + static_cast<long>(t) * ld : src, t < left, policy);
+            for (int t = 0; t < U; ++t)
+                if (t < left) cp_async16(d + t * stride, s + static_cast<long>(t) * ld, policy);
         }
         cp_async_commit();  // an empty group past the last stage keeps the group count uniform
     };
